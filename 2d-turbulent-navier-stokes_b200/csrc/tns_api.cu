@@ -1,0 +1,594 @@
+// tns_api.cu -- host runtime behind the C ABI of include/tnsgpu.h.
+//
+// tns_create validates the Fortran arrays, finds the structured i x j block the cells
+// form (faces 1..4 = j-, i+, j+, i- as the reference's generators number them), and
+// lays the mesh out on the device in (i, j) order with the ghosts in four side arrays.
+// tns_run replays one RK4 iteration (turbnstwod.f90:95-168) as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tnsgpu.h"
+#include "tns_kernels.h"
+
+using tns::Mesh;
+using tns::Params;
+
+namespace {
+
+enum KernelId { K_DISS = 0, K_STAGE1 = 1, K_STAGE = 2, K_DTMIN = 3, K_GPORT = 4, K_NKERNEL = 5 };
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        n = count;
+        return cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+};
+
+}  // namespace
+
+struct tns_handle {
+    std::string err;
+    Params P{};
+    Mesh M{};
+    int ni = 0, nj = 0, neles = 0, nods = 0, nghosts = 0, maxid = 0;
+    std::vector<int> cell_of;   // structured index k -> 0-based original cell id
+    bool identity = true;
+    std::vector<int> ghost_line;  // device ghost index -> bc.in line
+    std::vector<int> ghost_id;    // bc.in line -> Fortran ghost id
+    std::vector<int> port_ghosts;
+    std::vector<double> hX, hY, hcfldl, hgxc, hgyc, hginj;  // host layout (device order)
+    std::vector<int> hgtype, hgrank;
+    cudaStream_t own = nullptr, stream = nullptr;
+    DevBuf<double> x, y, cfldl, gxc, gyc, ginj, gport, qa, qb, qc, d, vis, dt, dtmin, partial,
+        primout;
+    DevBuf<int> gtype, grank, ports;
+    DevBuf<unsigned int> counter, status;
+    DevBuf<unsigned long long> cdiff;
+    double* pinned = nullptr;  // 5*ncell staging
+    bool have_state = false, have_run = false;
+    cudaGraphExec_t graph = nullptr;
+    bool profile = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    double kms[K_NKERNEL] = {0};
+    long long kcount[K_NKERNEL] = {0};
+    long long launches = 0;
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return TNS_OK;
+        return fail(TNS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+    size_t ncell() const { return (size_t)ni * nj; }
+};
+
+namespace {
+
+// Derived scalars exactly as the Fortran main forms them (turbnstwod.f90:37-42,
+// 63/84 for RTOLERANCE), plus constants folded in the Fortran's left-to-right order.
+Params make_params(const tns_params& p) {
+    Params P{};
+    P.gama = p.gama; P.amol = p.amol; P.cfl = p.cfl; P.prandtl = p.prandtl;
+    P.prandtlt = p.prandtlt; P.p0 = p.p0; P.t0 = p.t0; P.pamb = p.pamb; P.rtred = p.rtred;
+    P.rinit = p.rinit; P.tflame = p.tflame; P.ancomb = p.ancomb; P.acomb = p.acomb;
+    P.rhoprop = p.rhoprop; P.pinf = p.pinf; P.aminf = p.aminf; P.deltabl = p.deltabl;
+    P.local = p.local; P.npseudo = p.npseudo; P.iaxis = p.iaxis;
+    P.rr = 8314.0 / p.amol;
+    P.cv = P.rr / (p.gama - 1.0);
+    P.cp = P.cv * p.gama;
+    const double rho0 = p.p0 / (P.rr * p.t0);
+    P.s0 = p.p0 / std::pow(rho0, p.gama);
+    P.tinf = p.t0 / (1.0 + 0.5 * (p.gama - 1.0) * p.aminf * p.aminf);
+    P.rtol = p.rinit * p.rtred;
+    P.gamrr = p.gama * P.rr;
+    P.suth_amol = 0.00000011848 * std::sqrt(p.amol);
+    P.div23 = 2.0 / 3.0;
+    P.fr2k = std::sqrt(2.0 * std::sqrt(0.09));
+    P.inv1mg = 1.0 / (1.0 - p.gama);
+    P.gth08 = std::pow(35.0, 0.8);
+    P.rtol_rtred = P.rtol * p.rtred;
+    P.bl_u = 2.0 * p.aminf * std::sqrt(P.gamrr * P.tinf);
+    P.bl_exp = 1.0 / 7.0;
+    return P;
+}
+
+int build_mesh(tns_handle* h, const tns_mesh* m) {
+    const int ne = m->neles, ng = m->nghosts, nn = m->nods;
+    if (ne <= 0 || nn <= 0 || ng < 0 || !m->x || !m->y || !m->nod || !m->nc1 || !m->nc2 ||
+        !m->nc3 || !m->nc4 || (ng > 0 && (!m->nparent || !m->nghost || !m->ntype || !m->nside)))
+        return h->fail(TNS_ERR_ARG, "tns_create: missing mesh arrays or sizes");
+    if (m->ld_nod < ne) return h->fail(TNS_ERR_ARG, "tns_create: ld_nod < NELES");
+    const int* ncs[4] = {m->nc1, m->nc2, m->nc3, m->nc4};
+    auto NOD = [&](int cell0, int k) { return m->nod[(size_t)k * m->ld_nod + cell0]; };
+    // ghost lines
+    std::unordered_map<int, int> line_of;
+    line_of.reserve((size_t)ng * 2 + 1);
+    int maxid = ne;
+    for (int L = 0; L < ng; L++) {
+        const int gid = m->nghost[L], par = m->nparent[L], ty = m->ntype[L], sd = m->nside[L];
+        if (gid >= 1 && gid <= ne)
+            return h->fail(TNS_ERR_MESH, "bc.in line %d: ghost id %d collides with a cell", L + 1, gid);
+        if (gid < 1) return h->fail(TNS_ERR_MESH, "bc.in line %d: bad ghost id %d", L + 1, gid);
+        if (!line_of.emplace(gid, L).second)
+            return h->fail(TNS_ERR_MESH, "bc.in line %d: ghost id %d repeated", L + 1, gid);
+        if (par < 1 || par > ne)
+            return h->fail(TNS_ERR_MESH, "bc.in line %d: parent %d out of range", L + 1, par);
+        if (sd < 1 || sd > 4) return h->fail(TNS_ERR_MESH, "bc.in line %d: side %d", L + 1, sd);
+        if (ty < 2 || ty > 7)
+            return h->fail(TNS_ERR_MESH, "bc.in line %d: BC type %d is not one of 2..7", L + 1, ty);
+        if (ncs[sd - 1][par - 1] != gid)
+            return h->fail(TNS_ERR_MESH, "bc.in line %d: NC%d(%d)=%d is not ghost %d", L + 1, sd,
+                           par, ncs[sd - 1][par - 1], gid);
+        maxid = std::max(maxid, gid);
+    }
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) {
+            const int v = ncs[k][c];
+            if (v >= 1 && v <= ne) continue;
+            auto it = line_of.find(v);
+            if (it == line_of.end())
+                return h->fail(TNS_ERR_MESH, "cell %d face %d: neighbour %d is neither a cell nor a ghost",
+                               c + 1, k + 1, v);
+            const int L = it->second;
+            if (m->nparent[L] != c + 1 || m->nside[L] != k + 1)
+                return h->fail(TNS_ERR_MESH, "ghost %d is referenced by cell %d face %d but belongs to cell %d side %d",
+                               v, c + 1, k + 1, m->nparent[L], m->nside[L]);
+            const int n1 = NOD(c, k);
+            (void)n1;
+        }
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) {
+            const int v = NOD(c, k);
+            if (v < 1 || v > nn) return h->fail(TNS_ERR_MESH, "cell %d node %d: id %d out of range", c + 1, k + 1, v);
+        }
+    auto is_cell = [&](int v) { return v >= 1 && v <= ne; };
+    // corner cell: ghosts on faces 1 and 4
+    int corner = -1, ncorner = 0;
+    for (int c = 0; c < ne; c++)
+        if (!is_cell(m->nc1[c]) && !is_cell(m->nc4[c])) { corner = c; ncorner++; }
+    if (ncorner != 1)
+        return h->fail(TNS_ERR_UNSUPPORTED,
+                       "mesh is not one structured i x j block (%d cells with ghosts on faces 1 and 4)", ncorner);
+    int nj = 1, ni = 1;
+    for (int c = corner; is_cell(m->nc3[c]); c = m->nc3[c] - 1) {
+        if (++nj > ne) return h->fail(TNS_ERR_UNSUPPORTED, "face-3 walk does not end");
+    }
+    for (int c = corner; is_cell(m->nc2[c]); c = m->nc2[c] - 1) {
+        if (++ni > ne) return h->fail(TNS_ERR_UNSUPPORTED, "face-2 walk does not end");
+    }
+    if ((long long)ni * nj != ne)
+        return h->fail(TNS_ERR_UNSUPPORTED, "mesh is not one structured block (%d x %d != %d cells)", ni, nj, ne);
+    if (ni < 2 || nj < 2) return h->fail(TNS_ERR_UNSUPPORTED, "need at least 2 x 2 cells (got %d x %d)", ni, nj);
+    std::vector<int> cell_of((size_t)ne, -1), seen((size_t)ne, 0);
+    int start = corner;
+    for (int i = 0; i < ni; i++) {
+        int c = start;
+        for (int j = 0; j < nj; j++) {
+            if (c < 0 || c >= ne || seen[c])
+                return h->fail(TNS_ERR_UNSUPPORTED, "cells do not form an i x j block (at %d,%d)", i, j);
+            seen[c] = 1;
+            cell_of[(size_t)i * nj + j] = c;
+            if (j + 1 < nj) c = is_cell(m->nc3[c]) ? m->nc3[c] - 1 : -1;
+        }
+        if (i + 1 < ni) start = is_cell(m->nc2[start]) ? m->nc2[start] - 1 : -1;
+    }
+    // adjacency and node consistency
+    std::vector<int> node_of((size_t)(ni + 1) * (nj + 1), 0);
+    auto set_node = [&](int a, int b, int id) {
+        int& slot = node_of[(size_t)a * (nj + 1) + b];
+        if (slot == 0) slot = id;
+        return slot == id;
+    };
+    for (int i = 0; i < ni; i++)
+        for (int j = 0; j < nj; j++) {
+            const int c = cell_of[(size_t)i * nj + j];
+            const int want[4] = {j > 0 ? cell_of[(size_t)i * nj + j - 1] + 1 : 0,
+                                 i + 1 < ni ? cell_of[(size_t)(i + 1) * nj + j] + 1 : 0,
+                                 j + 1 < nj ? cell_of[(size_t)i * nj + j + 1] + 1 : 0,
+                                 i > 0 ? cell_of[(size_t)(i - 1) * nj + j] + 1 : 0};
+            for (int k = 0; k < 4; k++) {
+                const int v = ncs[k][c];
+                if (want[k] ? v != want[k] : is_cell(v))
+                    return h->fail(TNS_ERR_UNSUPPORTED, "cell %d face %d breaks the i x j block", c + 1, k + 1);
+            }
+            if (!set_node(i, j, NOD(c, 0)) || !set_node(i + 1, j, NOD(c, 1)) ||
+                !set_node(i + 1, j + 1, NOD(c, 2)) || !set_node(i, j + 1, NOD(c, 3)))
+                return h->fail(TNS_ERR_UNSUPPORTED, "cell %d: nodes are not shared as in an i x j block", c + 1);
+        }
+    h->ni = ni; h->nj = nj; h->neles = ne; h->nods = nn; h->nghosts = ng; h->maxid = maxid;
+    h->identity = true;
+    for (int k = 0; k < ne; k++)
+        if (cell_of[k] != k) { h->identity = false; break; }
+    h->cell_of.swap(cell_of);
+
+    // device-order host arrays
+    const size_t nnode = (size_t)(ni + 1) * (nj + 1), ncell = (size_t)ne;
+    const int ngs = 2 * (ni + nj);
+    if (ngs != ng)
+        return h->fail(TNS_ERR_MESH, "expected %d ghosts for a %d x %d block, bc.in has %d", ngs, ni, nj, ng);
+    std::vector<double> X(nnode), Y(nnode), cfldl(ncell), gxc(ngs), gyc(ngs), ginj(ngs, 1.0);
+    std::vector<int> gtype(ngs), grank(ngs);
+    for (size_t a = 0; a < nnode; a++) {
+        X[a] = m->x[node_of[a] - 1];
+        Y[a] = m->y[node_of[a] - 1];
+    }
+    h->M.ni = ni;
+    h->M.nj = nj;
+    h->ghost_line.assign(ngs, -1);
+    h->ghost_id.assign(ng, 0);
+    for (int L = 0; L < ng; L++) h->ghost_id[L] = m->nghost[L];
+    for (int i = 0; i < ni; i++)
+        for (int j = 0; j < nj; j++) {
+            const size_t k = (size_t)i * nj + j;
+            const int c = h->cell_of[k];
+            const size_t n1 = (size_t)i * (nj + 1) + j;
+            const double X1 = X[n1], X2 = X[n1 + nj + 1], X3 = X[n1 + nj + 2], X4 = X[n1 + 1];
+            const double Y1 = Y[n1], Y2 = Y[n1 + nj + 1], Y3 = Y[n1 + nj + 2], Y4 = Y[n1 + 1];
+            // geometry.f90:70-74
+            const double DL12 = std::sqrt((X1 - X2) * (X1 - X2) + (Y1 - Y2) * (Y1 - Y2));
+            const double DL23 = std::sqrt((X2 - X3) * (X2 - X3) + (Y2 - Y3) * (Y2 - Y3));
+            const double DL34 = std::sqrt((X3 - X4) * (X3 - X4) + (Y3 - Y4) * (Y3 - Y4));
+            const double DL41 = std::sqrt((X4 - X1) * (X4 - X1) + (Y4 - Y1) * (Y4 - Y1));
+            const double DL = std::min(std::min(std::min(DL12, DL23), DL34), DL41);
+            cfldl[k] = h->P.cfl * DL;
+            const double xcc = (X1 + X2 + X3 + X4) * 0.25, ycc = (Y1 + Y2 + Y3 + Y4) * 0.25;
+            for (int s = 1; s <= 4; s++) {
+                const bool bnd = (s == 1 && j == 0) || (s == 2 && i == ni - 1) ||
+                                 (s == 3 && j == nj - 1) || (s == 4 && i == 0);
+                if (!bnd) continue;
+                const int g = h->M.ghost_index(s, (s == 1 || s == 3) ? i : j);
+                const int L = line_of.at(ncs[s - 1][c]);
+                h->ghost_line[g] = L;
+                gtype[g] = m->ntype[L];
+                grank[g] = L;
+                // geometry.f90:114-142
+                double xf, yf;
+                if (s == 1) { xf = 0.5 * (X1 + X2); yf = 0.5 * (Y1 + Y2); }
+                else if (s == 2) { xf = 0.5 * (X2 + X3); yf = 0.5 * (Y2 + Y3); }
+                else if (s == 3) { xf = 0.5 * (X3 + X4); yf = 0.5 * (Y3 + Y4); }
+                else { xf = 0.5 * (X4 + X1); yf = 0.5 * (Y4 + Y1); }
+                gxc[g] = 2.0 * xf - xcc;
+                gyc[g] = 2.0 * yf - ycc;
+                if (gtype[g] == 6) h->port_ghosts.push_back(g);
+            }
+        }
+    for (int g = 0; g < ngs; g++)
+        if (h->ghost_line[g] < 0) return h->fail(TNS_ERR_MESH, "boundary face %d has no bc.in line", g);
+    h->hX.swap(X); h->hY.swap(Y); h->hcfldl.swap(cfldl); h->hgxc.swap(gxc); h->hgyc.swap(gyc);
+    h->hginj.swap(ginj); h->hgtype.swap(gtype); h->hgrank.swap(grank);
+    return TNS_OK;
+}
+
+// Device copy of the layout built by build_mesh.
+int upload_mesh(tns_handle* h) {
+    const size_t nnode = h->hX.size(), ncell = h->hcfldl.size(), ngs = h->hgxc.size();
+    int rc;
+    if ((rc = h->cuda(h->x.alloc(nnode), "cudaMalloc")) || (rc = h->cuda(h->y.alloc(nnode), "cudaMalloc")) ||
+        (rc = h->cuda(h->cfldl.alloc(ncell), "cudaMalloc")) || (rc = h->cuda(h->gxc.alloc(ngs), "cudaMalloc")) ||
+        (rc = h->cuda(h->gyc.alloc(ngs), "cudaMalloc")) || (rc = h->cuda(h->ginj.alloc(ngs), "cudaMalloc")) ||
+        (rc = h->cuda(h->gport.alloc(ngs), "cudaMalloc")) || (rc = h->cuda(h->gtype.alloc(ngs), "cudaMalloc")) ||
+        (rc = h->cuda(h->grank.alloc(ngs), "cudaMalloc")) ||
+        (rc = h->cuda(h->ports.alloc(h->port_ghosts.size()), "cudaMalloc")))
+        return rc;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return h->cuda(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+    };
+    if ((rc = up(h->x.p, h->hX.data(), nnode * 8)) || (rc = up(h->y.p, h->hY.data(), nnode * 8)) ||
+        (rc = up(h->cfldl.p, h->hcfldl.data(), ncell * 8)) ||
+        (rc = up(h->gxc.p, h->hgxc.data(), ngs * 8)) || (rc = up(h->gyc.p, h->hgyc.data(), ngs * 8)) ||
+        (rc = up(h->ginj.p, h->hginj.data(), ngs * 8)) ||
+        (rc = up(h->gtype.p, h->hgtype.data(), ngs * 4)) ||
+        (rc = up(h->grank.p, h->hgrank.data(), ngs * 4)))
+        return rc;
+    if (!h->port_ghosts.empty() &&
+        (rc = up(h->ports.p, h->port_ghosts.data(), h->port_ghosts.size() * 4)))
+        return rc;
+    if ((rc = h->cuda(cudaMemset(h->gport.p, 0, ngs * 8), "cudaMemset"))) return rc;
+    Mesh& M = h->M;
+    M.ni = h->ni; M.nj = h->nj; M.x = h->x.p; M.y = h->y.p; M.cfldl = h->cfldl.p; M.gtype = h->gtype.p;
+    M.grank = h->grank.p; M.gxc = h->gxc.p; M.gyc = h->gyc.p; M.ginj = h->ginj.p;
+    M.gport = h->gport.p;
+    return TNS_OK;
+}
+
+int alloc_state(tns_handle* h) {
+    const size_t nc = h->ncell();
+    int rc;
+    if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qb.alloc(5 * nc), "cudaMalloc")) ||
+        (rc = h->cuda(h->qc.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->d.alloc(5 * nc), "cudaMalloc")) ||
+        (rc = h->cuda(h->vis.alloc(4 * nc), "cudaMalloc")) || (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc")) ||
+        (rc = h->cuda(h->dtmin.alloc(1), "cudaMalloc")) ||
+        (rc = h->cuda(h->partial.alloc((size_t)tns::dtmin_blocks(h->M)), "cudaMalloc")) ||
+        (rc = h->cuda(h->counter.alloc(1), "cudaMalloc")) || (rc = h->cuda(h->status.alloc(1), "cudaMalloc")) ||
+        (rc = h->cuda(h->cdiff.alloc(5), "cudaMalloc")))
+        return rc;
+    if ((rc = h->cuda(cudaMemset(h->counter.p, 0, 4), "cudaMemset")) ||
+        (rc = h->cuda(cudaMemset(h->status.p, 0, 4), "cudaMemset")) ||
+        (rc = h->cuda(cudaMemset(h->dt.p, 0, nc * 8), "cudaMemset")) ||
+        (rc = h->cuda(cudaMemset(h->vis.p, 0, 4 * nc * 8), "cudaMemset")))
+        return rc;
+    return h->cuda(cudaMallocHost((void**)&h->pinned, 5 * nc * sizeof(double)), "cudaMallocHost");
+}
+
+// Timed launch wrapper: events around the launch when profiling.
+template <class F>
+void launch(tns_handle* h, int kid, F&& f) {
+    if (h->profile) cudaEventRecord(h->ev[0], h->stream);
+    f();
+    h->launches++;
+    if (h->profile) {
+        cudaEventRecord(h->ev[1], h->stream);
+        cudaEventSynchronize(h->ev[1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        h->kms[kid] += ms;
+        h->kcount[kid]++;
+    }
+}
+
+// One RK4 iteration (turbnstwod.f90:97-168).  Buffers: A = state, B/C = stage scratch;
+// stage 4 writes A in place (each cell reads only its own COLD there).
+void enqueue_iteration(tns_handle* h, bool monitor) {
+    const Params& P = h->P;
+    const Mesh& M = h->M;
+    cudaStream_t s = h->stream;
+    double *A = h->qa.p, *B = h->qb.p, *Cq = h->qc.p;
+    const int np = (int)h->port_ghosts.size();
+    if (!P.local)
+        launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
+    launch(h, K_DISS, [&] { tns::launch_dissipation(P, M, A, h->d.p, h->dt.p, h->dtmin.p, s); });
+    static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
+    const double* in[4] = {A, B, Cq, B};
+    double* out[4] = {B, Cq, B, A};
+    if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
+    for (int st = 0; st < 4; st++) {
+        if (np) launch(h, K_GPORT, [&] { tns::launch_gport(P, M, in[st], h->ports.p, np, h->gport.p, s); });
+        launch(h, st == 0 ? K_STAGE1 : K_STAGE, [&] {
+            tns::launch_stage(P, M, st == 0, in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
+                              alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
+                              st == 3 ? h->status.p : nullptr, s);
+        });
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out) {
+    if (!out) return TNS_ERR_ARG;
+    *out = nullptr;
+    if (!mesh || !params) return TNS_ERR_ARG;
+    tns_handle* h = new tns_handle();
+    *out = h;
+    if (params->precision != 0) return h->fail(TNS_ERR_ARG, "precision mode %d is not available", params->precision);
+    if (!(params->gama > 1.0) || !(params->amol > 0.0) || !(params->cfl > 0.0))
+        return h->fail(TNS_ERR_ARG, "GAMA must exceed 1, AMOL and CFL must be positive");
+    h->P = make_params(*params);
+    int rc;
+    // host-side validation and layout first: mesh errors are reported without a GPU
+    if ((rc = build_mesh(h, mesh))) return rc;
+    if ((rc = h->cuda(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    h->stream = h->own;
+    if ((rc = h->cuda(tns::configure_kernels(), "cudaFuncSetAttribute"))) return rc;
+    if ((rc = upload_mesh(h))) return rc;
+    if ((rc = alloc_state(h))) return rc;
+    cudaEventCreate(&h->ev[0]);
+    cudaEventCreate(&h->ev[1]);
+    return TNS_OK;
+}
+
+int tns_set_injection_scale(tns_handle* h, const double* scale) {
+    if (!h || !scale) return TNS_ERR_ARG;
+    std::vector<double> g((size_t)h->M.nghosts(), 1.0);
+    for (size_t k = 0; k < g.size(); k++) g[k] = scale[h->ghost_line[k]];
+    return h->cuda(cudaMemcpy(h->ginj.p, g.data(), g.size() * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const double* c3,
+                     const double* c4, const double* c5) {
+    if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
+    const size_t nc = h->ncell();
+    const double* src[5] = {c1, c2, c3, c4, c5};
+    for (int m = 0; m < 5; m++) {
+        double* dst = h->pinned + m * nc;
+        if (h->identity) std::memcpy(dst, src[m], nc * 8);
+        else
+            for (size_t k = 0; k < nc; k++) dst[k] = src[m][h->cell_of[k]];
+    }
+    int rc = h->cuda(cudaMemcpyAsync(h->qa.p, h->pinned, 5 * nc * 8, cudaMemcpyHostToDevice, h->stream),
+                     "cudaMemcpyAsync");
+    if (rc) return rc;
+    rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    if (rc) return rc;
+    h->have_state = true;
+    return TNS_OK;
+}
+
+int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int max_records,
+            int* n_records) {
+    if (!h) return TNS_ERR_ARG;
+    if (n_records) *n_records = 0;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_run: no state uploaded");
+    if (niter <= 0) return TNS_OK;
+    int nrec = 0, rc;
+    const bool use_graph = !h->profile;
+    if (use_graph && !h->graph) {
+        cudaGraph_t g;
+        if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture")))
+            return rc;
+        const long long before = h->launches;
+        enqueue_iteration(h, false);
+        h->launches = before;
+        if ((rc = h->cuda(cudaStreamEndCapture(h->stream, &g), "capture"))) return rc;
+        rc = h->cuda(cudaGraphInstantiate(&h->graph, g, 0), "cudaGraphInstantiate");
+        cudaGraphDestroy(g);
+        if (rc) return rc;
+    }
+    const long long per_iter = 1 + (h->P.local ? 0 : 1) + 4 + 4 * (h->port_ghosts.empty() ? 0 : 1);
+    for (int it = 1; it <= niter; it++) {
+        const bool mon = monitor_every > 0 && it % monitor_every == 0;
+        if (mon || !use_graph) {
+            enqueue_iteration(h, mon);
+        } else {
+            if ((rc = h->cuda(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch"))) return rc;
+            h->launches += per_iter;
+        }
+        if (mon) {
+            unsigned long long bits[5];
+            if ((rc = h->cuda(cudaMemcpyAsync(bits, h->cdiff.p, sizeof bits, cudaMemcpyDeviceToHost, h->stream),
+                              "cudaMemcpyAsync")))
+                return rc;
+            if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+            if (cdiff_out && nrec < max_records) {
+                for (int m = 0; m < 5; m++) {
+                    double v;
+                    std::memcpy(&v, &bits[m], 8);
+                    const double init = m < 4 ? 1.0e-10 : 1.0e-20;  // constants.f90:44-45
+                    cdiff_out[nrec * 5 + m] = v >= init ? v : init;
+                }
+            }
+            nrec++;
+        }
+    }
+    if ((rc = h->cuda(cudaGetLastError(), "kernel launch"))) return rc;
+    unsigned int st = 0;
+    if ((rc = h->cuda(cudaMemcpyAsync(&st, h->status.p, 4, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync")))
+        return rc;
+    if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    h->have_run = true;
+    if (n_records) *n_records = std::min(nrec, max_records);
+    if (st & 1u) return h->fail(TNS_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
+    return TNS_OK;
+}
+
+int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double* c4, double* c5) {
+    if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_download_state: no state");
+    const size_t nc = h->ncell();
+    int rc = h->cuda(cudaMemcpyAsync(h->pinned, h->qa.p, 5 * nc * 8, cudaMemcpyDeviceToHost, h->stream),
+                     "cudaMemcpyAsync");
+    if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    double* dst[5] = {c1, c2, c3, c4, c5};
+    for (int m = 0; m < 5; m++) {
+        const double* src = h->pinned + m * nc;
+        if (h->identity) std::memcpy(dst[m], src, nc * 8);
+        else
+            for (size_t k = 0; k < nc; k++) dst[m][h->cell_of[k]] = src[k];
+    }
+    return TNS_OK;
+}
+
+int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, double* p) {
+    if (!h || !u || !v || !t || !p) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_download_primitives: no iteration has run");
+    const size_t nc = h->ncell(), ng = (size_t)h->M.nghosts(), nt = nc + ng;
+    int rc;
+    if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
+    const int np = (int)h->port_ghosts.size();
+    // stage 4 read B: recompute its primitives and ghost states from B
+    if (np) tns::launch_gport(h->P, h->M, h->qb.p, h->ports.p, np, h->gport.p, h->stream);
+    tns::launch_prim_out(h->P, h->M, h->qb.p, h->primout.p, h->stream);
+    std::vector<double> hb(4 * nt);
+    rc = h->cuda(cudaMemcpyAsync(hb.data(), h->primout.p, 4 * nt * 8, cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    double* dst[4] = {u, v, t, p};
+    for (int f = 0; f < 4; f++) {
+        const double* src = hb.data() + f * nt;
+        for (size_t k = 0; k < nc; k++) dst[f][h->cell_of[k]] = src[k];
+        for (size_t g = 0; g < ng; g++) dst[f][h->ghost_id[h->ghost_line[g]] - 1] = src[nc + g];
+    }
+    return TNS_OK;
+}
+
+int tns_debug_fetch(tns_handle* h, int which, double* out) {
+    if (!h || !out || which < 0 || which > 2) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_debug_fetch: no iteration has run");
+    const size_t nc = h->ncell();
+    const int cnt = which == 0 ? 5 : which == 1 ? 4 : 1;
+    const double* src = which == 0 ? h->d.p : which == 1 ? h->vis.p : h->dt.p;
+    std::vector<double> hb(cnt * nc);
+    if (which == 2 && !h->P.local) {
+        double dm = 0;
+        int rc = h->cuda(cudaMemcpy(&dm, h->dtmin.p, 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (rc) return rc;
+        std::fill(hb.begin(), hb.end(), dm);
+    } else {
+        int rc = h->cuda(cudaMemcpyAsync(hb.data(), src, cnt * nc * 8, cudaMemcpyDeviceToHost, h->stream),
+                         "cudaMemcpyAsync");
+        if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    }
+    for (int f = 0; f < cnt; f++)
+        for (size_t k = 0; k < nc; k++) out[f * nc + h->cell_of[k]] = hb[f * nc + k];
+    return TNS_OK;
+}
+
+int tns_set_stream(tns_handle* h, void* stream) {
+    if (!h) return TNS_ERR_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->own;
+    if (s != h->stream) {
+        cudaStreamSynchronize(h->stream);
+        h->stream = s;
+    }
+    return TNS_OK;
+}
+
+int tns_profile(tns_handle* h, int enable) {
+    if (!h) return TNS_ERR_ARG;
+    h->profile = enable != 0;
+    if (h->profile)
+        for (int k = 0; k < K_NKERNEL; k++) { h->kms[k] = 0; h->kcount[k] = 0; }
+    return TNS_OK;
+}
+
+int tns_kernel_times(tns_handle* h, int kernel, double* ms, long long* launches) {
+    if (!h || kernel < 0 || kernel >= K_NKERNEL) return TNS_ERR_ARG;
+    if (ms) *ms = h->kms[kernel];
+    if (launches) *launches = h->kcount[kernel];
+    return TNS_OK;
+}
+
+long long tns_launch_count(tns_handle* h) { return h ? h->launches : -1; }
+
+const char* tns_last_error(tns_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+void tns_destroy(tns_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    for (auto* b : {&h->x, &h->y, &h->cfldl, &h->gxc, &h->gyc, &h->ginj, &h->gport, &h->qa, &h->qb,
+                    &h->qc, &h->d, &h->vis, &h->dt, &h->dtmin, &h->partial, &h->primout})
+        b->release();
+    h->gtype.release(); h->grank.release(); h->ports.release();
+    h->counter.release(); h->status.release(); h->cdiff.release();
+    if (h->pinned) cudaFreeHost(h->pinned);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+}
+
+}  // extern "C"

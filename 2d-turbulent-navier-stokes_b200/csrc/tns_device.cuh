@@ -1,0 +1,392 @@
+// tns_device.cuh -- device-side constants, parameter block, mesh view and the per-cell
+// physics of the RK4 / JST / viscous / source / boundary hot path.
+//
+// The arithmetic restates the reference solver's Fortran (paths relative to the
+// reference project) in the same operation order; only the memory layout differs:
+// cells live in a structured (i, j) block (j fastest), ghosts in four side arrays,
+// geometry is recomputed from node coordinates instead of being stored per cell.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tns {
+
+// constants.f90:15-60
+constexpr double CMU = 0.09;
+constexpr double ALPHA_T = 0.00052;
+constexpr double BETA_T = 0.2;
+constexpr double CONST1 = 21.479;
+constexpr double CONST2 = 21.394;
+constexpr double CONST3 = 1.5;
+constexpr double C02 = 0.25;
+constexpr double C04 = 0.00390625;
+constexpr double CFLTURB = 0.5;
+constexpr double HALF = 0.5;
+constexpr double QUARTER = 0.25;
+constexpr double YAXIS_THRESH = 0.001;
+constexpr double AMU_THRESH = 0.001;
+constexpr double GTH = 35.0;
+constexpr double CONVKSC = 1.0 / 98066.5;
+
+// Scalar inputs plus every constant the Fortran folds left to right (computed once on
+// the host with the same operation order, so device values equal the reference's).
+struct Params {
+    double gama, amol, cfl, prandtl, prandtlt, p0, t0, pamb, rtred, rinit;
+    double tflame, ancomb, acomb, rhoprop, pinf, aminf, deltabl;
+    int local, npseudo, iaxis, pad_;
+    double rr, cv, cp, s0, tinf, rtol;  // turbnstwod.f90:37-42, RTOLERANCE
+    double gamrr;                        // GAMA*RR
+    double suth_amol;                    // SUTH_COEF*DSQRT(AMOL)
+    double div23;                        // 2/3
+    double fr2k;                         // DSQRT(2*DSQRT(CMU))
+    double inv1mg;                       // 1/(1-GAMA)
+    double gth08;                        // GTH**0.8
+    double rtol_rtred;                   // RTOLERANCE*RTRED
+    double bl_u;                         // 2*AMINF*DSQRT(GAMA*RR*TINF)
+    double bl_exp;                       // 1/7
+};
+
+// Ghost-side numbering: side 1 (j=-1) and 3 (j=NJ) are indexed by i, sides 2 (i=NI)
+// and 4 (i=-1) by j; the four runs are stored back to back.
+struct Mesh {
+    int ni, nj;             // cells in i and j
+    const double* x;        // node x [(ni+1)*(nj+1)], node (i,j) at i*(nj+1)+j
+    const double* y;
+    const double* cfldl;    // CFL*DL per cell
+    const int* gtype;       // BC type per ghost
+    const int* grank;       // bc.in line of each ghost (node-average order)
+    const double* gxc;      // mirrored ghost centroids (geometry.f90:114-142)
+    const double* gyc;
+    const double* ginj;     // type-6 burn-rate multiplier
+    const double* gport;    // type-6 port mass flux of the current stage
+    __host__ __device__ int ghost_index(int side, int along) const {
+        return side == 1 ? along : side == 2 ? ni + along : side == 3 ? ni + nj + along
+                                                                      : 2 * ni + nj + along;
+    }
+    __host__ __device__ int nghosts() const { return 2 * (ni + nj); }
+};
+
+__device__ __forceinline__ double dmax1(double a, double b) { return a >= b ? a : b; }
+__device__ __forceinline__ double dmin1(double a, double b) { return a <= b ? a : b; }
+
+// Fortran REAL**INTEGER by square-and-multiply.
+__device__ __forceinline__ double powi(double x, int n) {
+    double r = 1.0, b = x;
+    int m = n < 0 ? -n : n;
+    while (m) {
+        if (m & 1) r *= b;
+        m >>= 1;
+        if (m) b *= b;
+    }
+    return n < 0 ? 1.0 / r : r;
+}
+
+__device__ __forceinline__ double amu_of(const Params& P, double T) {
+    return P.suth_amol * pow(T, 0.6);
+}
+
+// Primitive variables and fluxes of one interior cell (turbnstwod.f90:204-227).
+struct Prim {
+    double u, v, t, p, rho, ri, c5, qm;
+    double f[5], g[5];
+};
+
+__device__ __forceinline__ void primitive(const Params& P, double c1, double c2, double c3,
+                                          double c4, double c5, Prim& s) {
+    const double RHO = c1;
+    s.rho = RHO;
+    s.u = c2 / RHO;
+    s.v = c3 / RHO;
+    const double E = c4 / RHO;
+    s.t = (E - 0.5 * (s.u * s.u + s.v * s.v)) / P.cv;
+    s.p = RHO * P.rr * s.t;
+    s.f[0] = c2;
+    s.f[1] = RHO * s.u * s.u + s.p;
+    s.f[2] = RHO * s.u * s.v;
+    s.f[3] = (c4 + s.p) * s.u;
+    s.g[0] = c3;
+    s.g[1] = s.f[2];
+    s.g[2] = RHO * s.v * s.v + s.p;
+    s.g[3] = (c4 + s.p) * s.v;
+    const double RT = c5 / RHO;
+    s.f[4] = RHO * RT * s.u;
+    s.g[4] = RHO * RT * s.v;
+    s.ri = RT;
+    s.c5 = c5;
+    s.qm = sqrt(s.u * s.u + s.v * s.v);
+}
+
+// Conservative + flux tail shared by BC types 2,3,4,6,7 (e.g. boundary.f90:62-70).
+__device__ __forceinline__ void ghost_tail(const Params& P, double RHO, Prim& g) {
+    g.rho = RHO;
+    const double C2 = RHO * g.u;
+    const double C3 = RHO * g.v;
+    const double E = P.cv * g.t + 0.5 * (g.u * g.u + g.v * g.v);
+    const double C4 = RHO * E;
+    g.f[0] = C2;
+    g.f[1] = RHO * g.u * g.u + g.p;
+    g.f[2] = RHO * g.u * g.v;
+    g.f[3] = (C4 + g.p) * g.u;
+    g.g[0] = C3;
+    g.g[1] = g.f[2];
+    g.g[2] = RHO * g.v * g.v + g.p;
+    g.g[3] = (C4 + g.p) * g.v;
+}
+
+// Face surface vector (geometry.f90:77-99) for face k (1..4) of a cell with nodes 1..4.
+__device__ __forceinline__ void face_vector(int iaxis, int k, const double X[4],
+                                            const double Y[4], double& sx, double& sy) {
+    const int a = k - 1, b = k & 3;  // nodes (k, k+1)
+    if (iaxis == 1) {
+        sx = (Y[b] - Y[a]) * (Y[a] + Y[b]) * HALF;
+        sy = -(X[b] - X[a]) * (Y[a] + Y[b]) * HALF;
+    } else {
+        sx = (Y[b] - Y[a]);
+        sy = -(X[b] - X[a]);
+    }
+}
+
+// Cell volume (geometry.f90:87,98,101).
+__device__ __forceinline__ double cell_volume(int iaxis, const double X[4], const double Y[4],
+                                              double ycc) {
+    double v = HALF * ((X[2] - X[0]) * (Y[3] - Y[1]) - (X[3] - X[1]) * (Y[2] - Y[0]));
+    if (iaxis == 1) v = v * ycc;
+    if (v <= 0.0) v = -v;
+    return v;
+}
+
+// Ghost state from its parent (and the parent's opposite neighbour) for BC types 2..7
+// (boundary.f90:53-327; type 6 with the port flux supplied by the caller).
+// par: parent cell, opp: parent's neighbour across the face opposite the ghost.
+// psx, psy: parent's surface vector on the ghost side; ycc_g, ycc_p: ghost / parent
+// centroid y; gport: summed port flux (type 6 only); inj: burn-rate multiplier.
+__device__ __forceinline__ void boundary_ghost(const Params& P, int type, const Prim& par,
+                                               const Prim& opp, double psx, double psy,
+                                               double ycc_g, double ycc_p, double gport,
+                                               double inj, Prim& g) {
+    double RHO, AMU, RT, C5;
+    switch (type) {
+        case 2: {  // subsonic inlet :53-71
+            g.u = fabs(par.u);
+            g.v = -par.v;
+            g.t = P.t0 - 0.5 * (g.u * g.u + g.v * g.v) / P.cp;
+            RHO = pow(P.s0 / (P.rr * g.t), P.inv1mg);
+            g.p = RHO * P.rr * g.t;
+            AMU = amu_of(P, g.t);
+            RT = AMU / RHO;
+            ghost_tail(P, RHO, g);
+            C5 = RHO * RT;
+            g.f[4] = C5 * g.u;
+            g.g[4] = C5 * g.v;
+            break;
+        }
+        case 3: {  // farfield / extrapolation :76-95
+            g.u = fabs(2.0 * par.u - opp.u);
+            g.v = 2.0 * par.v - opp.v;
+            g.t = 2.0 * par.t - opp.t;
+            g.p = 2.0 * par.p - opp.p;
+            if (P.pamb >= 0.0) g.p = P.pamb;
+            RHO = g.p / (P.rr * g.t);
+            ghost_tail(P, RHO, g);
+            C5 = par.c5;
+            g.f[4] = par.f[4];
+            g.g[4] = par.g[4];
+            break;
+        }
+        case 4: {  // symmetry :100-109
+            g.u = par.u;
+            g.v = -par.v;
+            g.t = par.t;
+            RHO = par.rho;
+            g.p = par.p;
+            ghost_tail(P, RHO, g);
+            C5 = par.c5;
+            g.f[4] = par.f[4];
+            g.g[4] = -par.g[4];
+            break;
+        }
+        case 5: {  // no-slip wall / axis :114-122
+            g.u = -par.u;
+            g.v = -par.v;
+            g.t = par.t;
+            RHO = par.rho;
+            g.p = par.p;
+            g.rho = RHO;
+            g.f[0] = -par.f[0];
+            g.f[1] = 2.0 * par.p - par.f[1];
+            g.f[2] = -par.f[2];
+            g.f[3] = -par.f[3];
+            g.g[0] = -par.g[0];
+            g.g[1] = -par.g[1];
+            g.g[2] = 2.0 * par.p - par.g[2];
+            g.g[3] = -par.g[3];
+            C5 = -par.c5;
+            g.f[4] = -par.f[4];
+            g.g[4] = -par.g[4];
+            break;
+        }
+        case 6: {  // mass injection :128-163
+            const double DNR = sqrt(psx * psx + psy * psy);
+            const double ENX = -psx / DNR, ENY = -psy / DNR;
+            const double DHYD = fabs(ycc_g + ycc_p);
+            double GP = (P.iaxis == 1) ? 2.0 * gport / (DHYD * DHYD) : gport / DHYD;
+            RHO = par.rho;
+            const double RDOT = P.acomb * pow(par.p * CONVKSC, P.ancomb) * inj;
+            double RDOTEB = RDOT;
+            double VEL = P.rhoprop / RHO * RDOTEB;
+            g.p = par.p;
+            g.u = VEL * ENX + VEL * ENX - par.u;
+            g.v = VEL * ENY + VEL * ENY - par.v;
+            g.t = P.tflame - 0.5 * (g.u * g.u + g.v * g.v) / P.cp;
+            AMU = amu_of(P, g.t);
+            const double GVAL =
+                (GP / (P.rhoprop * RDOT)) * pow(P.rhoprop * RDOT * DHYD / AMU, -0.125);
+            if (GVAL > GTH) RDOTEB = RDOTEB * (1.0 + 0.023 * (pow(GVAL, 0.8) - P.gth08));
+            VEL = P.rhoprop / RHO * RDOTEB;
+            g.u = VEL * ENX + VEL * ENX - par.u;
+            g.v = VEL * ENY + VEL * ENY - par.v;
+            g.t = P.tflame - 0.5 * (g.u * g.u + g.v * g.v) / P.cp;
+            RHO = g.p / (P.rr * g.t);
+            AMU = amu_of(P, g.t);
+            RT = AMU / RHO;
+            C5 = RHO * RT;
+            ghost_tail(P, RHO, g);
+            g.f[4] = C5 * g.u;
+            g.g[4] = C5 * g.v;
+            break;
+        }
+        default: {  // 7: boundary-layer inlet :310-327
+            g.p = P.pinf;
+            g.t = P.tinf;
+            g.v = -par.v;
+            RHO = g.p / (P.rr * g.t);
+            if (ycc_g <= P.deltabl)
+                g.u = P.bl_u * pow(ycc_g / P.deltabl, P.bl_exp) - par.u;
+            else
+                g.u = P.bl_u - par.u;
+            AMU = amu_of(P, g.t);
+            RT = AMU / RHO;
+            ghost_tail(P, RHO, g);
+            C5 = RHO * RT;
+            g.f[4] = C5 * g.u;
+            g.g[4] = C5 * g.v;
+            break;
+        }
+    }
+    g.c5 = C5;
+    g.ri = C5 / g.rho;
+    g.qm = sqrt(g.u * g.u + g.v * g.v);
+}
+
+// Turbulence / radial sources of one cell (source_terms.f90:258-320).  Neighbours
+// a,b,c,d are NC1..NC4.
+struct SrcIn {
+    double xa, xb, xc, xd, ya, yb, yc, yd;
+    double ua, ub, uc, ud, va, vb, vc, vd, ra, rb, rc, rd, qa, qb, qc, qd;
+};
+
+__device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, double RHO,
+                                             double RI, double TI, double PI, double VI,
+                                             double YCCI, double& src3, double& src5) {
+    const double DNR = (s.xa - s.xc) * (s.yb - s.yd) - (s.xb - s.xd) * (s.ya - s.yc);
+    const double DQX = ((s.qa - s.qc) * (s.yb - s.yd) - (s.qb - s.qd) * (s.ya - s.yc)) / DNR;
+    const double DRX = ((s.ra - s.rc) * (s.yb - s.yd) - (s.rb - s.rd) * (s.ya - s.yc)) / DNR;
+    const double DUX = ((s.ua - s.uc) * (s.yb - s.yd) - (s.ub - s.ud) * (s.ya - s.yc)) / DNR;
+    const double DVX = ((s.va - s.vc) * (s.yb - s.yd) - (s.vb - s.vd) * (s.ya - s.yc)) / DNR;
+    const double DQY = (-(s.qa - s.qc) * (s.xb - s.xd) + (s.qb - s.qd) * (s.xa - s.xc)) / DNR;
+    const double DRY = (-(s.ra - s.rc) * (s.xb - s.xd) + (s.rb - s.rd) * (s.xa - s.xc)) / DNR;
+    const double DUY = (-(s.ua - s.uc) * (s.xb - s.xd) + (s.ub - s.ud) * (s.xa - s.xc)) / DNR;
+    const double DVY = (-(s.va - s.vc) * (s.xb - s.xd) + (s.vb - s.vd) * (s.xa - s.xc)) / DNR;
+    const double AMU = amu_of(P, TI);
+    const double CHI = RHO * RI / (CMU * AMU);
+    const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
+    const double FR2 = tanh(sqrt(CHI)) / tanh(CHI * P.fr2k);
+    const double AMUT = FMU * RHO * RI;
+    const double PHI = DQX * DRX + DQY * DRY;
+    double DEE = 0.0;
+    if (PHI > 0.0) DEE = DRX * DRX + DRY * DRY;
+    double PK;
+    const double DIV23 = P.div23;
+    const double pw = powi(AMUT / dmax1(AMUT, AMU_THRESH * AMU), P.npseudo);
+    if (P.iaxis == 1) {
+        const double VBYY = (YCCI < YAXIS_THRESH) ? DVY : VI / YCCI;
+        const double DIVVEL = DUX + DVY + VBYY;
+        PK = AMUT / RHO *
+             (DUX * DUX + DVY * DVY + VBYY * VBYY + DUX * DUX + DVY * DVY + VBYY * VBYY +
+              (DUY + DVX) * (DUY + DVX) - DIV23 * DIVVEL * DIVVEL);
+        PK = dmax1(PK, 0.0);
+        src5 = (RHO * (CONST1 - CONST2 * FR2) * sqrt(RI * PK) - RHO * CONST3 * DEE) * pw;
+        const double TTT = (AMU + AMUT) * (VBYY + VBYY - DIV23 * DIVVEL);
+        src3 = (PI - TTT) / YCCI;
+    } else {
+        const double DIVVEL = DUX + DVY;
+        PK = AMUT / RHO *
+             (DUX * DUX + DVY * DVY + DUX * DUX + DVY * DVY + (DUY + DVX) * (DUY + DVX) -
+              DIV23 * DIVVEL * DIVVEL);
+        PK = dmax1(PK, 0.0);
+        src5 = (RHO * (CONST1 - CONST2 * FR2) * sqrt(RI * PK) - RHO * CONST3 * DEE) * pw;
+        src3 = 0.0;
+    }
+}
+
+// One face of the thin-layer viscous flux (viscous.f90:130-217): A = the cell, C = the
+// face neighbour, B, D = the face's nodes (node averages).  Adds the face's
+// contribution to vis[0..3] (face 1 assigns, later faces accumulate).
+struct FaceIn {
+    double sx, sy, xa, ya, xb, yb, xc, yc, xd, yd;
+    double ua, va, ta, ub, vb, tb, uc, vc, tc, ud, vd, td;
+    double rhoa, rhob, rhoc, rhod, ra, rb, rc, rd;
+};
+
+__device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, bool first,
+                                             double vis[4]) {
+    const double DNR = (f.xa - f.xc) * (f.yb - f.yd) - (f.xb - f.xd) * (f.ya - f.yc);
+    const double DUX = ((f.ua - f.uc) * (f.yb - f.yd) - (f.ub - f.ud) * (f.ya - f.yc)) / DNR;
+    const double DVX = ((f.va - f.vc) * (f.yb - f.yd) - (f.vb - f.vd) * (f.ya - f.yc)) / DNR;
+    const double DTX = ((f.ta - f.tc) * (f.yb - f.yd) - (f.tb - f.td) * (f.ya - f.yc)) / DNR;
+    const double DRX = ((f.ra - f.rc) * (f.yb - f.yd) - (f.rb - f.rd) * (f.ya - f.yc)) / DNR;
+    const double DUY = (-(f.ua - f.uc) * (f.xb - f.xd) + (f.ub - f.ud) * (f.xa - f.xc)) / DNR;
+    const double DVY = (-(f.va - f.vc) * (f.xb - f.xd) + (f.vb - f.vd) * (f.xa - f.xc)) / DNR;
+    const double DTY = (-(f.ta - f.tc) * (f.xb - f.xd) + (f.tb - f.td) * (f.xa - f.xc)) / DNR;
+    const double DRY = (-(f.ra - f.rc) * (f.xb - f.xd) + (f.rb - f.rd) * (f.xa - f.xc)) / DNR;
+    const double UAVG = QUARTER * (f.ua + f.ub + f.uc + f.ud);
+    const double VAVG = QUARTER * (f.va + f.vb + f.vc + f.vd);
+    const double TAVG = QUARTER * (f.ta + f.tb + f.tc + f.td);
+    const double RHOAVG = QUARTER * (f.rhoa + f.rhob + f.rhoc + f.rhod);
+    const double RAVG = QUARTER * (f.ra + f.rb + f.rc + f.rd);
+    double DIVVEL;
+    if (P.iaxis == 1) {
+        const double YAVG = HALF * (f.yb + f.yd);
+        const double VBYY = (YAVG < YAXIS_THRESH) ? DVY : VAVG / YAVG;
+        DIVVEL = DUX + DVY + VBYY;
+    } else {
+        DIVVEL = DUX + DVY;
+    }
+    const double AMU = amu_of(P, TAVG);
+    const double AK = AMU * P.cp / P.prandtl;
+    const double CHI = RHOAVG * RAVG / (AMU * CMU);
+    const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
+    const double AMUT = RHOAVG * RAVG * FMU;
+    const double AKT = AMUT * P.cp / P.prandtlt;
+    const double AMUEFF = AMU + AMUT;
+    const double AKEFF = AK + AKT;
+    const double TXX = AMUEFF * (DUX + DUX - P.div23 * DIVVEL);
+    const double TYY = AMUEFF * (DVY + DVY - P.div23 * DIVVEL);
+    const double TXY = AMUEFF * (DUY + DVX);
+    const double QXX = UAVG * TXX + VAVG * TXY + AKEFF * DTX;
+    const double QYY = UAVG * TXY + VAVG * TYY + AKEFF * DTY;
+    if (first) {
+        vis[0] = TXX * f.sx + TXY * f.sy;
+        vis[1] = TXY * f.sx + TYY * f.sy;
+        vis[2] = QXX * f.sx + QYY * f.sy;
+        vis[3] = AMUEFF * DRX * f.sx + AMUEFF * DRY * f.sy;
+    } else {
+        vis[0] = vis[0] + TXX * f.sx + TXY * f.sy;
+        vis[1] = vis[1] + TXY * f.sx + TYY * f.sy;
+        vis[2] = vis[2] + QXX * f.sx + QYY * f.sy;
+        vis[3] = vis[3] + AMUEFF * DRX * f.sx + AMUEFF * DRY * f.sy;
+    }
+}
+
+}  // namespace tns

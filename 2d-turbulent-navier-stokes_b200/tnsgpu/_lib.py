@@ -1,0 +1,84 @@
+"""ctypes binding of libtnsgpu.so (the C ABI declared in include/tnsgpu.h).
+
+The library is built in-tree (``tnsgpu.build.build_library``); there is no fallback:
+if the shared object is missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtnsgpu.so")
+
+TNS_OK = 0
+ERRORS = {-1: "TNS_ERR_ARG", -2: "TNS_ERR_MESH", -3: "TNS_ERR_UNSUPPORTED",
+          -4: "TNS_ERR_CUDA", -5: "TNS_ERR_NONFINITE", -6: "TNS_ERR_STATE"}
+
+# every symbol include/tnsgpu.h declares
+EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
+           "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
+           "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
+           "tns_last_error", "tns_destroy")
+
+
+class TnsMesh(C.Structure):
+    _fields_ = [("nods", C.c_int), ("neles", C.c_int), ("nghosts", C.c_int),
+                ("x", C.c_void_p), ("y", C.c_void_p), ("nod", C.c_void_p), ("ld_nod", C.c_int),
+                ("nc1", C.c_void_p), ("nc2", C.c_void_p), ("nc3", C.c_void_p),
+                ("nc4", C.c_void_p), ("nparent", C.c_void_p), ("nghost", C.c_void_p),
+                ("ntype", C.c_void_p), ("nside", C.c_void_p)]
+
+
+class TnsParams(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "gama", "amol", "cfl", "prandtl", "prandtlt", "p0", "t0", "pamb", "rtred", "rinit",
+        "tflame", "ancomb", "acomb", "rhoprop", "pinf", "aminf", "deltabl")] + [
+        (n, C.c_int) for n in ("local", "npseudo", "iaxis", "precision")]
+
+
+class TnsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (raises OSError when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with tnsgpu.build.build_library()")
+    L = C.CDLL(path)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_void_p
+    L.tns_create.argtypes = [C.POINTER(TnsMesh), C.POINTER(TnsParams), C.POINTER(vp)]
+    L.tns_set_injection_scale.argtypes = [vp, dp]
+    L.tns_upload_state.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.tns_run.argtypes = [vp, ip, ip, dp, ip, C.POINTER(C.c_int)]
+    L.tns_download_state.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.tns_download_primitives.argtypes = [vp, dp, dp, dp, dp]
+    L.tns_debug_fetch.argtypes = [vp, ip, dp]
+    L.tns_set_stream.argtypes = [vp, vp]
+    L.tns_profile.argtypes = [vp, ip]
+    L.tns_kernel_times.argtypes = [vp, ip, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    L.tns_launch_count.argtypes = [vp]
+    L.tns_launch_count.restype = C.c_longlong
+    L.tns_last_error.argtypes = [vp]
+    L.tns_last_error.restype = C.c_char_p
+    L.tns_destroy.argtypes = [vp]
+    L.tns_destroy.restype = None
+    for n in EXPORTS:
+        if n not in ("tns_launch_count", "tns_last_error", "tns_destroy"):
+            getattr(L, n).restype = C.c_int
+    _lib = L
+    return L
+
+
+def ptr(a: np.ndarray) -> int:
+    return a.ctypes.data

@@ -1,0 +1,126 @@
+"""Host-side mirror of the reference main program's hot loop over the C ABI.
+
+``Solver`` holds one device handle for a mesh and a flow.in; its calls map one to one
+onto the C entry points (include/tnsgpu.h) that replace the RK4 loop of
+src/solvers/turbnstwod.f90:95-168 (and the identical turbnsaxis.f90).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .formats import Flow, Mesh
+
+
+def make_params(flow: Flow, rinit: float, precision: int = 0) -> _lib.TnsParams:
+    p = _lib.TnsParams()
+    for n in ("gama", "amol", "cfl", "prandtl", "prandtlt", "p0", "t0", "pamb", "rtred",
+              "tflame", "ancomb", "acomb", "rhoprop", "pinf", "aminf", "deltabl"):
+        setattr(p, n, float(getattr(flow, n)))
+    p.rinit = float(rinit)
+    p.local, p.npseudo, p.iaxis = int(flow.local), int(flow.npseudo), int(flow.iaxis)
+    p.precision = int(precision)
+    return p
+
+
+class Solver:
+    """Device solver for one case.  Arrays follow Fortran ids (cell k at index k-1)."""
+
+    def __init__(self, mesh: Mesh, flow: Flow, rinit: float, precision: int = 0):
+        L = _lib.load()
+        self.L, self.mesh, self.flow = L, mesh, flow
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        # NOD is passed column-major (NOD(I,K) = nod[(K-1)*LD + I-1]) like Fortran holds it
+        self._a = dict(x=np.ascontiguousarray(mesh.x, np.float64),
+                       y=np.ascontiguousarray(mesh.y, np.float64),
+                       nod=i32(mesh.nod.T.reshape(-1)),
+                       nc1=i32(mesh.nc[:, 0]), nc2=i32(mesh.nc[:, 1]), nc3=i32(mesh.nc[:, 2]),
+                       nc4=i32(mesh.nc[:, 3]), nparent=i32(mesh.nparent),
+                       nghost=i32(mesh.nghost), ntype=i32(mesh.ntype), nside=i32(mesh.nside))
+        a = self._a
+        m = _lib.TnsMesh(mesh.nods, mesh.neles, mesh.nghosts, a["x"].ctypes.data,
+                         a["y"].ctypes.data, a["nod"].ctypes.data, mesh.neles,
+                         a["nc1"].ctypes.data, a["nc2"].ctypes.data, a["nc3"].ctypes.data,
+                         a["nc4"].ctypes.data, a["nparent"].ctypes.data,
+                         a["nghost"].ctypes.data, a["ntype"].ctypes.data,
+                         a["nside"].ctypes.data)
+        self._params = make_params(flow, rinit, precision)
+        h = C.c_void_p()
+        rc = L.tns_create(C.byref(m), C.byref(self._params), C.byref(h))
+        self.h = h
+        self._check(rc)
+        if mesh.inj_scale is not None:
+            self.set_injection_scale(mesh.inj_scale)
+        self.maxid = int(max(mesh.neles, int(mesh.nghost.max()) if mesh.nghosts else 0))
+
+    # -- plumbing
+    def _check(self, rc: int):
+        if rc != _lib.TNS_OK:
+            msg = self.L.tns_last_error(self.h).decode() if self.h else ""
+            raise _lib.TnsError(rc, msg)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.tns_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the C entry points
+    def set_injection_scale(self, scale: np.ndarray):
+        s = np.ascontiguousarray(scale, np.float64)
+        self._check(self.L.tns_set_injection_scale(self.h, s.ctypes.data))
+
+    def upload(self, c: np.ndarray):
+        """c: [5, NELES] conservative state C1..C5."""
+        c = np.ascontiguousarray(c, np.float64)
+        self._check(self.L.tns_upload_state(self.h, *(c[k].ctypes.data for k in range(5))))
+
+    def run(self, niter: int, monitor_every: int = 1000) -> np.ndarray:
+        maxrec = max(1, niter // monitor_every + 1) if monitor_every > 0 else 1
+        buf = np.zeros(5 * maxrec)
+        n = C.c_int(0)
+        self._check(self.L.tns_run(self.h, int(niter), int(monitor_every), buf.ctypes.data,
+                                   maxrec, C.byref(n)))
+        return buf[: 5 * n.value].reshape(-1, 5)
+
+    def download(self) -> np.ndarray:
+        c = np.zeros((5, self.mesh.neles))
+        self._check(self.L.tns_download_state(self.h, *(c[k].ctypes.data for k in range(5))))
+        return c
+
+    def primitives(self) -> np.ndarray:
+        """[4, maxid] U, V, T, P by Fortran id (cells and ghosts)."""
+        out = np.zeros((4, self.maxid))
+        self._check(self.L.tns_download_primitives(self.h, *(out[k].ctypes.data for k in range(4))))
+        return out
+
+    def debug(self, which: int) -> np.ndarray:
+        cnt = {0: 5, 1: 4, 2: 1}[which]
+        out = np.zeros((cnt, self.mesh.neles))
+        self._check(self.L.tns_debug_fetch(self.h, int(which), out.ctypes.data))
+        return out
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self._check(self.L.tns_set_stream(self.h, stream_ptr))
+
+    def profile(self, enable: bool):
+        self._check(self.L.tns_profile(self.h, 1 if enable else 0))
+
+    def kernel_times(self) -> dict:
+        out = {}
+        for k, name in enumerate(("dissipation", "stage1", "stage", "dtmin", "gport")):
+            ms, n = C.c_double(0), C.c_longlong(0)
+            self._check(self.L.tns_kernel_times(self.h, k, C.byref(ms), C.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
+    def launch_count(self) -> int:
+        return int(self.L.tns_launch_count(self.h))

@@ -1,0 +1,112 @@
+/*
+ * tnsgpu.h -- C ABI of the B200 RK4 hot path of the 2-D / axisymmetric turbulent
+ * Navier-Stokes solver (drop-in for the per-iteration calls of the reference Fortran
+ * mains src/solvers/turbnstwod.f90 and turbnsaxis.f90).
+ *
+ * The reference has no plugin API: its main program calls argument-less subroutines
+ * that share module globals.  The entry points below replace exactly that seam
+ * (turbnstwod.f90:95-168, the RK4 loop); everything before it (flow.in / grid.in /
+ * bc.in reads, geometry.f90:22-52) and after it (restart.in, POSTPROCESS) stays with
+ * the caller.  All arguments are plain pointers and sizes; arrays are the caller's
+ * Fortran arrays (1-based ids, column-major), borrowed for the duration of a call.
+ *
+ * Return codes: 0 = success, negative = error (tns_last_error() gives the text).
+ * A handle owns one CUDA stream and all device memory; handles are not thread-safe.
+ */
+#ifndef TNSGPU_H
+#define TNSGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TNS_OK 0
+#define TNS_ERR_ARG (-1)          /* null pointer / bad size */
+#define TNS_ERR_MESH (-2)         /* inconsistent grid.in / bc.in arrays */
+#define TNS_ERR_UNSUPPORTED (-3)  /* mesh is not one structured i x j block */
+#define TNS_ERR_CUDA (-4)         /* CUDA runtime error */
+#define TNS_ERR_NONFINITE (-5)    /* state became NaN / Inf */
+#define TNS_ERR_STATE (-6)        /* call out of order (e.g. no state uploaded) */
+
+/* Mesh as COMPUTE_GEOMETRY holds it after reading grid.in and bc.in
+ * (geometry.f90:25-52; solver_state.f90:113-125). */
+typedef struct tns_mesh {
+    int nods, neles, nghosts;
+    const double *x, *y;       /* X(1:NODS), Y(1:NODS) in metres (after the 0.001 scaling) */
+    const int *nod;            /* NOD(LD,4) column-major: NOD(I,K) = nod[(K-1)*ld_nod + I-1] */
+    int ld_nod;                /* leading dimension of NOD (NN in the reference) */
+    const int *nc1, *nc2, *nc3, *nc4;             /* NC1..NC4(1:NELES) */
+    const int *nparent, *nghost, *ntype, *nside;  /* bc.in columns, (1:NGHOSTS) */
+} tns_mesh;
+
+/* The 17 flow.in values that reach the hot path (turbnstwod.f90:20-23) plus RINIT
+ * (cold start or restart.in) and the inputs of BC types 6 and 7 that the reference
+ * declares but never assigns (solver_state.f90:36-42: TFLAME, ANCOMB, ACOMB, RHOPROP,
+ * PINF, AMINF, DELTABL). */
+typedef struct tns_params {
+    double gama, amol, cfl, prandtl, prandtlt, p0, t0, pamb, rtred, rinit;
+    double tflame, ancomb, acomb, rhoprop, pinf, aminf, deltabl;
+    int local, npseudo, iaxis;
+    int precision; /* 0 = FP64 (the only mode of this version) */
+} tns_params;
+
+typedef struct tns_handle tns_handle;
+
+/* Builds the device mesh: validates the arrays, detects the structured i x j block,
+ * computes DL and the ghost centroids (geometry.f90:55-149) and uploads everything.
+ * Replaces: CALL COMPUTE_GEOMETRY's consumers + the module state setup
+ * (turbnstwod.f90:32-48). */
+int tns_create(const tns_mesh *mesh, const tns_params *params, tns_handle **out);
+
+/* Burn-rate multiplier per bc.in line for type-6 ghosts (default 1).  No reference
+ * counterpart (the reference cannot express an axial variation). */
+int tns_set_injection_scale(tns_handle *h, const double *scale /* [NGHOSTS] */);
+
+/* Uploads C1..C5(1:NELES) as the state at the start of the next iteration.
+ * Replaces: the COLD <- C copy before the loop (turbnstwod.f90:87-90). */
+int tns_upload_state(tns_handle *h, const double *c1, const double *c2, const double *c3,
+                     const double *c4, const double *c5);
+
+/* Runs niter full RK4 iterations (turbnstwod.f90:95-168).  Every monitor_every-th
+ * iteration (counting from 1 within this call, as MOD(ITER,1000) does) the five CDIFF
+ * values max(init, max|COLD-C|) are appended to cdiff_out (5 doubles per record, at
+ * most max_records); *n_records receives the count.  monitor_every <= 0 disables it. */
+int tns_run(tns_handle *h, int niter, int monitor_every, double *cdiff_out, int max_records,
+            int *n_records);
+
+/* Downloads C1..C5(1:NELES) (for restart.in, turbnstwod.f90:171-195). */
+int tns_download_state(tns_handle *h, double *c1, double *c2, double *c3, double *c4,
+                       double *c5);
+
+/* U, V, T, P as the reference leaves them after its last stage (interior cells from the
+ * last stage's PRIMITIVE_VARS, ghosts from its APPLY_BOUNDARY), scattered to Fortran
+ * ids: u[id-1] for cells 1..NELES and ghosts NGHOST(k).  Arrays must hold the largest
+ * id.  Feeds POSTPROCESS (solver_state.f90:230-283). */
+int tns_download_primitives(tns_handle *h, double *u, double *v, double *t, double *p);
+
+/* Frozen terms of the last iteration, for checking: which = 0: D241..D245 (5 arrays),
+ * 1: VISU, VISV, VIST, VISR (4), 2: DT (1).  out holds count*NELES doubles, cell order
+ * 1..NELES per array. */
+int tns_debug_fetch(tns_handle *h, int which, double *out);
+
+/* Runs the next tns_run on this CUDA stream (cudaStream_t passed as void*; NULL
+ * restores the handle's own stream). */
+int tns_set_stream(tns_handle *h, void *stream);
+
+/* Per-kernel device timing of the next tns_run calls (CUDA events around every
+ * launch); tns_kernel_times returns, for kernel k, the summed milliseconds and the
+ * launch count.  Kernel ids: 0 dissipation, 1 stage 1 (viscous), 2 stages 2-4,
+ * 3 dtmin, 4 gport. */
+int tns_profile(tns_handle *h, int enable);
+int tns_kernel_times(tns_handle *h, int kernel, double *ms, long long *launches);
+
+/* Number of kernel launches issued by this handle so far. */
+long long tns_launch_count(tns_handle *h);
+
+const char *tns_last_error(tns_handle *h);
+void tns_destroy(tns_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

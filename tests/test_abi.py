@@ -1,0 +1,71 @@
+"""The C-ABI library: it loads without a GPU, exports every symbol include/tnsgpu.h
+declares, and rejects bad meshes on the host before touching CUDA."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tnsgpu import _lib, cases
+from tnsgpu.solver import make_params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "tnsgpu.h")).read()
+    return sorted(set(re.findall(r"\b(tns_[a-z_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    names = _declared()
+    assert len(names) >= 13
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(_lib.EXPORTS)
+
+
+def _create(mesh, flow=None):
+    L = _lib.load()
+    flow = flow or cases.ramp_flow()
+    i32 = lambda a: np.ascontiguousarray(a, np.int32)
+    keep = [np.ascontiguousarray(mesh.x), np.ascontiguousarray(mesh.y), i32(mesh.nod.T.reshape(-1)),
+            i32(mesh.nc[:, 0]), i32(mesh.nc[:, 1]), i32(mesh.nc[:, 2]), i32(mesh.nc[:, 3]),
+            i32(mesh.nparent), i32(mesh.nghost), i32(mesh.ntype), i32(mesh.nside)]
+    m = _lib.TnsMesh(mesh.nods, mesh.neles, mesh.nghosts, *(k.ctypes.data for k in keep[:3]),
+                     mesh.neles, *(k.ctypes.data for k in keep[3:]))
+    p = make_params(flow, 1e-6)
+    h = C.c_void_p()
+    rc = L.tns_create(C.byref(m), C.byref(p), C.byref(h))
+    msg = L.tns_last_error(h).decode() if h else ""
+    if h:
+        L.tns_destroy(h)
+    return rc, msg
+
+
+@pytest.mark.parametrize("breakage,code", [
+    ("type", -2), ("side", -2), ("parent", -2), ("nc", -2), ("unstructured", -3)])
+def test_host_validation_rejects_bad_meshes(breakage, code):
+    m = cases.ramp_mesh(6, 4)
+    if breakage == "type":
+        m.ntype[3] = 1          # no BC type 1 in boundary.f90:33-45
+    elif breakage == "side":
+        m.nside[0] = 5
+    elif breakage == "parent":
+        m.nparent[2] = m.nparent[2] + 1
+    elif breakage == "nc":
+        m.nc[5, 1] = 10_000     # neither a cell nor a ghost
+    else:
+        # swap two interior neighbours: still consistent ids, no longer an i x j block
+        m.nc[9, 1], m.nc[9, 2] = m.nc[9, 2], m.nc[9, 1]
+    rc, msg = _create(m)
+    assert rc == code, (rc, msg)
+    assert msg
+
+
+def test_valid_mesh_passes_host_checks():
+    rc, msg = _create(cases.ramp_mesh(6, 4))
+    # on a machine without a GPU the first CUDA call fails; with one it succeeds
+    assert rc in (0, -4), (rc, msg)

@@ -1,0 +1,189 @@
+"""CUDA path vs the CPU oracle through the C ABI (include/tnsgpu.h).
+
+Tolerances: FP64 everywhere; the GPU contracts a*b+c into FMA and uses CUDA's pow/tanh,
+so results are not bit-identical.  Q and the CDIFF history must agree to <= 1e-10
+relative (max-norm per variable).  Exception, documented in the oracle tests: with IAXIS=1
+and a type-5 axis, C5 is ill-conditioned in the scheme itself (a 1e-15 input change
+moves it by up to ~1e-4), so there C5 is checked against that envelope.
+"""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from tnsgpu import cases, formats
+from tnsgpu.solver import Solver
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.atleast_2d(a), np.atleast_2d(b)
+    return np.max(np.abs(a - b), axis=1) / np.maximum(np.max(np.abs(b), axis=1), 1e-300)
+
+
+def _cold(mesh, flow):
+    ri = formats.rinit_cold(flow)
+    return formats.cold_state(flow, mesh.neles, ri), ri
+
+
+def _bl_case():
+    # ramp with a type-7 boundary-layer inlet (PINF / AMINF / DELTABL as parameters)
+    m = cases.ramp_mesh(24, 12)
+    m.ntype[m.ntype == 2] = 7
+    f = cases.ramp_flow()
+    f.pinf, f.aminf, f.deltabl = 8.6e5, 0.05, 0.01
+    return m, f
+
+
+CASES = {
+    "ramp": lambda: (cases.ramp_mesh(48, 20), cases.ramp_flow()),
+    "ramp_global_dt": lambda: (cases.ramp_mesh(40, 16), formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
+    "nozzle2d_bc4": lambda: (cases.nozzle_2d_mesh(37, 19), cases.nozzle_2d_flow()),
+    "boundary_layer_bc7": _bl_case,
+    "odd_tiles": lambda: (cases.ramp_mesh(13, 45), cases.ramp_flow()),
+}
+
+
+def _state(name, mesh, flow):
+    if name.startswith("ramp") or name == "odd_tiles":
+        return cases.noisy_restart_state(flow, mesh.neles)
+    return _cold(mesh, flow)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_one_iteration_frozen_terms_and_state(name):
+    mesh, flow = CASES[name]()
+    c0, ri = _state(name, mesh, flow)
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    s.run(1, 0)
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    o.iterate(1, 0)
+    ne = mesh.neles
+    d_ref = np.stack([o.fetch(f"D24{k}")[:ne] for k in range(1, 6)])
+    v_ref = np.stack([o.fetch(k)[:ne] for k in ("VISU", "VISV", "VIST", "VISR")])
+    assert np.all(rel(s.debug(0), d_ref) < 1e-12)
+    assert np.all(rel(s.debug(1), v_ref) < 1e-12)
+    assert np.all(rel(s.debug(2), o.fetch("DT")[None, :ne]) < 1e-13)
+    assert np.all(rel(s.download(), o.state()) < 1e-12)
+    # U,V,T,P of cells and ghosts as the reference leaves them (POSTPROCESS input)
+    nn = o.nn
+    pr = s.primitives()[:, :nn]
+    ref = np.stack([o.fetch(k)[:nn] for k in ("U", "V", "T", "P")])
+    assert np.all(rel(pr, ref) < 1e-11)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_many_iterations_state_and_residual_history(name):
+    mesh, flow = CASES[name]()
+    c0, ri = _state(name, mesh, flow)
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    hist = s.run(60, monitor_every=20)
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    ref_hist = o.iterate(60, 20)
+    assert hist.shape == (3, 5)
+    assert np.all(rel(s.download(), o.state()) < TOL)
+    assert np.max(np.abs(hist - ref_hist) / np.abs(ref_hist)) < TOL
+
+
+def test_ramp_192x64_2000_iterations():
+    """The 2-D ramp case end to end: 2000 RK4 iterations from the seeded noisy restart,
+    Q and the CDIFF history (every 1000 iterations) vs the oracle."""
+    mesh, flow = cases.ramp_mesh(192, 64), cases.ramp_flow(2000)
+    c0, ri = cases.noisy_restart_state(flow, mesh.neles)
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    hist = s.run(2000, 1000)
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    ref_hist = o.iterate(2000, 1000)
+    assert np.all(rel(s.download(), o.state()) < TOL)
+    assert np.max(np.abs(hist - ref_hist) / np.abs(ref_hist)) < TOL
+
+
+def _axi_check(mesh, flow, niter):
+    c0, ri = _cold(mesh, flow)
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    s.run(niter, 0)
+    q = s.download()
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    o.iterate(niter, 0)
+    ref = o.state()
+    # the oracle's own response to a 1e-15 input perturbation
+    c1 = c0 * (1 + 1e-15 * np.random.default_rng(7).standard_normal(c0.shape))
+    o2 = Oracle(mesh, flow, ri)
+    o2.set_state(c1)
+    o2.iterate(niter, 0)
+    env = rel(o2.state(), ref)
+    err = rel(q, ref)
+    return err, env
+
+
+@pytest.mark.parametrize("kind", ["nozzle_plume", "port"])
+def test_axisymmetric_cases(kind):
+    mesh = cases.nozzle_plume_mesh(64, 24) if kind == "nozzle_plume" else cases.port_mesh(64, 24)
+    flow = cases.nozzle_plume_flow() if kind == "nozzle_plume" else cases.port_flow()
+    err, env = _axi_check(mesh, flow, 20)
+    assert np.all(err[:4] < TOL), err
+    assert err[4] < max(100 * env[4], TOL), (err, env)
+    # same geometry with the axis as a symmetry line: well conditioned, full parity
+    mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    err, env = _axi_check(mesh, flow, 20)
+    assert np.all(err < TOL), (err, env)
+
+
+def test_type6_injection_profile_and_port_flux():
+    mesh, flow = cases.port_mesh(40, 16), cases.port_flow()
+    mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    c0, ri = _cold(mesh, flow)
+    s = Solver(mesh, flow, ri)      # applies mesh.inj_scale (+-2 % per ghost)
+    s.upload(c0)
+    s.run(10, 0)
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    o.iterate(10, 0)
+    assert np.all(rel(s.download(), o.state()) < TOL)
+    nn = o.nn
+    assert np.all(rel(s.primitives()[:, :nn], np.stack([o.fetch(k)[:nn] for k in "UVTP"])) < 1e-9)
+
+
+def test_full_size_nozzle_plume_first_iterations():
+    """1024 x 384 (the benchmark mesh): two iterations against the oracle at full size."""
+    mesh, flow = cases.nozzle_plume_mesh(1024, 384), cases.nozzle_plume_flow()
+    err, env = _axi_check(mesh, flow, 2)
+    assert np.all(err[:4] < TOL), err
+    assert err[4] < max(100 * env[4], TOL), (err, env)
+
+
+def test_nonfinite_state_is_reported():
+    mesh, flow = cases.ramp_mesh(16, 8), cases.ramp_flow()
+    c0, ri = cases.noisy_restart_state(flow, mesh.neles)
+    c0[3, 17] = np.nan
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    with pytest.raises(Exception) as e:
+        s.run(2, 0)
+    assert "NONFINITE" in str(e.value)
+
+
+def test_graph_replay_equals_direct_launches():
+    """tns_run replays a captured CUDA graph; with per-kernel profiling on it launches
+    directly.  Both must give bit-identical states."""
+    mesh, flow = cases.ramp_mesh(40, 20), cases.ramp_flow()
+    c0, ri = cases.noisy_restart_state(flow, mesh.neles)
+    a = Solver(mesh, flow, ri)
+    a.upload(c0)
+    a.run(7, 0)
+    b = Solver(mesh, flow, ri)
+    b.upload(c0)
+    b.profile(True)
+    b.run(7, 0)
+    assert np.array_equal(a.download(), b.download())
+    kt = b.kernel_times()
+    assert kt["dissipation"][1] == 7 and kt["stage1"][1] == 7 and kt["stage"][1] == 21
