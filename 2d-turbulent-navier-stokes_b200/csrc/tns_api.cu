@@ -62,6 +62,8 @@ struct tns_handle {
     double* pinned = nullptr;  // 5*ncell staging
     bool have_state = false, have_run = false;
     cudaGraphExec_t graph = nullptr;
+    long long per_iter = 0;
+    unsigned int* status_host = nullptr;  // pinned
     bool profile = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     double kms[K_NKERNEL] = {0};
@@ -329,6 +331,8 @@ int alloc_state(tns_handle* h) {
         (rc = h->cuda(cudaMemset(h->dt.p, 0, nc * 8), "cudaMemset")) ||
         (rc = h->cuda(cudaMemset(h->vis.p, 0, 4 * nc * 8), "cudaMemset")))
         return rc;
+    if ((rc = h->cuda(cudaMallocHost((void**)&h->status_host, sizeof(unsigned int)), "cudaMallocHost")))
+        return rc;
     return h->cuda(cudaMallocHost((void**)&h->pinned, 5 * nc * sizeof(double)), "cudaMallocHost");
 }
 
@@ -412,19 +416,94 @@ int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const do
     if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
     const size_t nc = h->ncell();
     const double* src[5] = {c1, c2, c3, c4, c5};
-    for (int m = 0; m < 5; m++) {
-        double* dst = h->pinned + m * nc;
-        if (h->identity) std::memcpy(dst, src[m], nc * 8);
-        else
-            for (size_t k = 0; k < nc; k++) dst[k] = src[m][h->cell_of[k]];
+    int rc;
+    bool direct = h->identity;
+    for (int m = 0; m < 5 && direct; m++) {
+        cudaPointerAttributes at;
+        direct = cudaPointerGetAttributes(&at, src[m]) == cudaSuccess && at.type == cudaMemoryTypeHost;
     }
-    int rc = h->cuda(cudaMemcpyAsync(h->qa.p, h->pinned, 5 * nc * 8, cudaMemcpyHostToDevice, h->stream),
-                     "cudaMemcpyAsync");
-    if (rc) return rc;
+    cudaGetLastError();
+    if (direct) {
+        // page-locked caller arrays: one DMA per component, no staging copy
+        for (int m = 0; m < 5; m++)
+            if ((rc = h->cuda(cudaMemcpyAsync(h->qa.p + m * nc, src[m], nc * 8, cudaMemcpyHostToDevice,
+                                              h->stream), "cudaMemcpyAsync")))
+                return rc;
+    } else {
+        for (int m = 0; m < 5; m++) {
+            double* dst = h->pinned + m * nc;
+            if (h->identity) std::memcpy(dst, src[m], nc * 8);
+            else
+                for (size_t k = 0; k < nc; k++) dst[k] = src[m][h->cell_of[k]];
+        }
+        if ((rc = h->cuda(cudaMemcpyAsync(h->qa.p, h->pinned, 5 * nc * 8, cudaMemcpyHostToDevice, h->stream),
+                          "cudaMemcpyAsync")))
+            return rc;
+    }
     rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     if (rc) return rc;
     h->have_state = true;
     return TNS_OK;
+}
+
+namespace {
+
+// Captures one unmonitored iteration as a CUDA graph (once per handle).
+int ensure_graph(tns_handle* h) {
+    if (h->graph) return TNS_OK;
+    cudaGraph_t g;
+    int rc;
+    if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture")))
+        return rc;
+    const long long before = h->launches;
+    enqueue_iteration(h, false);
+    h->per_iter = h->launches - before;
+    h->launches = before;
+    if ((rc = h->cuda(cudaStreamEndCapture(h->stream, &g), "capture"))) return rc;
+    rc = h->cuda(cudaGraphInstantiate(&h->graph, g, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(g);
+    return rc;
+}
+
+int enqueue_plain(tns_handle* h, int niter) {
+    int rc;
+    if (h->profile) {
+        for (int it = 0; it < niter; it++) enqueue_iteration(h, false);
+        return TNS_OK;
+    }
+    if ((rc = ensure_graph(h))) return rc;
+    for (int it = 0; it < niter; it++) {
+        if ((rc = h->cuda(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch"))) return rc;
+        h->launches += h->per_iter;
+    }
+    return TNS_OK;
+}
+
+int check_status(tns_handle* h) {
+    int rc;
+    if ((rc = h->cuda(cudaGetLastError(), "kernel launch"))) return rc;
+    if ((rc = h->cuda(cudaMemcpyAsync(h->status_host, h->status.p, 4, cudaMemcpyDeviceToHost, h->stream),
+                      "cudaMemcpyAsync")))
+        return rc;
+    if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    if (*h->status_host & 1u) return h->fail(TNS_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
+    return TNS_OK;
+}
+
+}  // namespace
+
+int tns_enqueue(tns_handle* h, int niter) {
+    if (!h) return TNS_ERR_ARG;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_enqueue: no state uploaded");
+    if (niter <= 0) return TNS_OK;
+    const int rc = enqueue_plain(h, niter);
+    if (!rc) h->have_run = true;
+    return rc;
+}
+
+int tns_synchronize(tns_handle* h) {
+    if (!h) return TNS_ERR_ARG;
+    return check_status(h);
 }
 
 int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int max_records,
@@ -434,29 +513,18 @@ int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int 
     if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_run: no state uploaded");
     if (niter <= 0) return TNS_OK;
     int nrec = 0, rc;
-    const bool use_graph = !h->profile;
-    if (use_graph && !h->graph) {
-        cudaGraph_t g;
-        if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture")))
-            return rc;
-        const long long before = h->launches;
-        enqueue_iteration(h, false);
-        h->launches = before;
-        if ((rc = h->cuda(cudaStreamEndCapture(h->stream, &g), "capture"))) return rc;
-        rc = h->cuda(cudaGraphInstantiate(&h->graph, g, 0), "cudaGraphInstantiate");
-        cudaGraphDestroy(g);
-        if (rc) return rc;
-    }
-    const long long per_iter = 1 + (h->P.local ? 0 : 1) + 4 + 4 * (h->port_ghosts.empty() ? 0 : 1);
-    for (int it = 1; it <= niter; it++) {
-        const bool mon = monitor_every > 0 && it % monitor_every == 0;
-        if (mon || !use_graph) {
-            enqueue_iteration(h, mon);
-        } else {
-            if ((rc = h->cuda(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch"))) return rc;
-            h->launches += per_iter;
+    for (int it = 1; it <= niter;) {
+        // run unmonitored iterations up to the next monitored one as one batch
+        int next = (monitor_every > 0) ? ((it + monitor_every - 1) / monitor_every) * monitor_every
+                                       : niter + 1;
+        if (next > niter) next = niter + 1;
+        if (next > it) {
+            if ((rc = enqueue_plain(h, next - it))) return rc;
+            it = next;
+            if (it > niter) break;
         }
-        if (mon) {
+        enqueue_iteration(h, true);  // iteration `it` is monitored
+        {
             unsigned long long bits[5];
             if ((rc = h->cuda(cudaMemcpyAsync(bits, h->cdiff.p, sizeof bits, cudaMemcpyDeviceToHost, h->stream),
                               "cudaMemcpyAsync")))
@@ -472,16 +540,11 @@ int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int 
             }
             nrec++;
         }
+        it++;
     }
-    if ((rc = h->cuda(cudaGetLastError(), "kernel launch"))) return rc;
-    unsigned int st = 0;
-    if ((rc = h->cuda(cudaMemcpyAsync(&st, h->status.p, 4, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync")))
-        return rc;
-    if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     h->have_run = true;
     if (n_records) *n_records = std::min(nrec, max_records);
-    if (st & 1u) return h->fail(TNS_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
-    return TNS_OK;
+    return check_status(h);
 }
 
 int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double* c4, double* c5) {
@@ -585,6 +648,7 @@ void tns_destroy(tns_handle* h) {
     h->gtype.release(); h->grank.release(); h->ports.release();
     h->counter.release(); h->status.release(); h->cdiff.release();
     if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->status_host) cudaFreeHost(h->status_host);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->own) cudaStreamDestroy(h->own);

@@ -19,7 +19,7 @@ ERRORS = {-1: "TNS_ERR_ARG", -2: "TNS_ERR_MESH", -3: "TNS_ERR_UNSUPPORTED",
 
 # every symbol include/tnsgpu.h declares
 EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
-           "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
+           "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy")
 
@@ -61,6 +61,8 @@ def load(path: str = LIB_PATH):
     L.tns_set_injection_scale.argtypes = [vp, dp]
     L.tns_upload_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_run.argtypes = [vp, ip, ip, dp, ip, C.POINTER(C.c_int)]
+    L.tns_enqueue.argtypes = [vp, ip]
+    L.tns_synchronize.argtypes = [vp]
     L.tns_download_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_download_primitives.argtypes = [vp, dp, dp, dp, dp]
     L.tns_debug_fetch.argtypes = [vp, ip, dp]

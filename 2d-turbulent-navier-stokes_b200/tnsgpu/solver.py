@@ -91,6 +91,17 @@ class Solver:
                                    maxrec, C.byref(n)))
         return buf[: 5 * n.value].reshape(-1, 5)
 
+    def enqueue(self, niter: int):
+        """Asynchronous iterations (no residual monitor); errors surface at synchronize()."""
+        self._check(self.L.tns_enqueue(self.h, int(niter)))
+
+    def synchronize(self):
+        self._check(self.L.tns_synchronize(self.h))
+
+    def upload_ptrs(self, ptrs):
+        """Upload from five host addresses (e.g. page-locked buffers) of NELES doubles."""
+        self._check(self.L.tns_upload_state(self.h, *[int(p) for p in ptrs]))
+
     def download(self) -> np.ndarray:
         c = np.zeros((5, self.mesh.neles))
         self._check(self.L.tns_download_state(self.h, *(c[k].ctypes.data for k in range(5))))

@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Benchmark of the RK4 hot path: cell-iterations per second on B200.
+
+Workload (default): the axisymmetric nozzle + plume mesh, 1024 x 384 cells (IAXIS=1,
+LOCAL=1, CFL 0.25, cold start at M=0.01), FP64.  One step = one full RK4 iteration
+(dissipation pre-pass + 4 stages) over the whole mesh with the state resident in HBM;
+L2 is flushed (256 MiB write) between steps outside the timed events.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): every rank solves an independent replica of the mesh (the path has
+no exchange step on one GPU: "replicas only"); value = N * cells / max-over-ranks step
+time.  --impl reference times the CPU oracle (a line-faithful C restatement of the
+reference Fortran, which cannot be compiled here) on the host, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "2d-turbulent-navier-stokes_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "RK4 cell-iters/s on 1 B200, FP32 vs FP64 at equal residual; adjoint/primal time"
+UNIT = "cell-iter/s"
+# Compulsory DRAM bytes per cell for one launch of each kernel (FP64, 8 B words):
+#   dissipation: Q_old 5 + nodes 2 + CFL*DL 1 in, D 5 + DT 1 out            = 14 words
+#   stage1     : Q_old 5 + D 5 + DT 1 + nodes 2 in, VIS 4 + Q 5 out        = 22 words
+#   stage 2..4 : Q_in 5 + Q_old 5 + D 5 + VIS 4 + DT 1 + nodes 2 in, Q 5 out = 27 words
+KERNEL_BYTES_PER_CELL = {"dissipation": 112, "stage1": 176, "stage": 216}
+KERNEL_NAMES = {"dissipation": "k_dissipation", "stage1": "k_stage<1>", "stage": "k_stage<0>"}
+
+
+def _case(name):
+    from tnsgpu import cases, formats
+    if name == "nozzle_plume_1024x384":
+        m, f = cases.nozzle_plume_mesh(1024, 384), cases.nozzle_plume_flow()
+        ri = formats.rinit_cold(f)
+        return m, f, formats.cold_state(f, m.neles, ri), ri, \
+            "nozzle_plume_1024x384 (IAXIS=1, LOCAL=1, CFL 0.25, cold start M=0.01)"
+    if name == "port_4096x1536":
+        m, f = cases.port_mesh(4096, 1536), cases.port_flow()
+        ri = formats.rinit_cold(f)
+        return m, f, formats.cold_state(f, m.neles, ri), ri, \
+            "port_4096x1536 (IAXIS=1, type-6 injection, cold start)"
+    if name == "ramp_192x64":
+        m, f = cases.ramp_mesh(192, 64), cases.ramp_flow()
+        c, ri = cases.noisy_restart_state(f, m.neles)
+        return m, f, c, ri, "ramp_192x64 (IAXIS=0, seeded restart)"
+    raise SystemExit(f"unknown case {name}")
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic(case, kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        return json.load(open(p)).get(case, {}).get(kernel)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            t = [x.strip() for x in line.split(",")]
+            if len(t) >= 8:
+                rows.append(t)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def run_ours(args, rank, world, dev):
+    import numpy as np
+    import torch
+    from tnsgpu.solver import Solver
+
+    mesh, flow, c0, rinit, wname = _case(args.case)
+    s = Solver(mesh, flow, rinit)
+    # one non-default stream for the solver, the L2 flush and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    s.set_stream(stream.cuda_stream)
+    s.upload(c0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    K, W = args.steps, args.warmup
+    for _ in range(W):
+        flush.zero_()
+        s.enqueue(1)
+    s.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    clocks = Clocks(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = s.launch_count()
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record(stream)
+        s.enqueue(1)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    s.synchronize()
+    launches = s.launch_count() - l0
+    ms = sum(a.elapsed_time(b) for a, b in ev) / K
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * mesh.neles / (ms * 1e-3)
+
+    # per-kernel device times (events around each launch, L2 flushed between iterations)
+    s.profile(True)
+    P = max(3, min(K, 20))
+    for _ in range(P):
+        flush.zero_()
+        s.enqueue(1)
+    s.synchronize()
+    kt = s.kernel_times()
+    s.profile(False)
+    dom = max(("dissipation", "stage1", "stage"), key=lambda k: kt[k][0])
+    avg_ms = kt[dom][0] / max(kt[dom][1], 1)
+    peak, peak_kind = _peaks()
+    bytes_launch = KERNEL_BYTES_PER_CELL[dom] * mesh.neles
+    achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
+    traffic = _traffic(args.case, KERNEL_NAMES[dom])
+    total_kms = sum(kt[k][0] for k in kt) / P
+    kernel_split = {k: round(kt[k][0] / P * 1e3, 2) for k in kt if kt[k][1]}
+
+    # end to end through the C ABI: pinned host state -> device, one monitored
+    # iteration, residual (CDIFF) back to the host
+    host = torch.empty((5, mesh.neles), dtype=torch.float64, pin_memory=True)
+    host.copy_(torch.from_numpy(np.ascontiguousarray(c0)))
+    ptrs = [host[k].data_ptr() for k in range(5)]
+    E = max(3, min(K, 200))
+    for _ in range(2):
+        s.upload_ptrs(ptrs)
+        s.run(1, 1)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(E):
+        s.upload_ptrs(ptrs)
+        s.run(1, 1)
+    e2e_s = (time.perf_counter() - t0) / E
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * mesh.neles / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 5 * mesh.neles * 8, "d2h_bytes_per_step": 5 * 8 + 4,
+           "ms_per_step": round(e2e_s * 1e3, 4)}
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": round(ms, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wname, "cells": mesh.neles, "precision": "fp64",
+                   "step": "one RK4 iteration (dissipation pre-pass + 4 stages)",
+                   "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind,
+                     "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+                     "traffic": traffic,
+                     "iteration_bytes_per_cell": 960,
+                     "iteration_frac": value / world * 960 / (peak * 1e9)},
+        "kernel_us_per_iteration": kernel_split,
+        "device_ms_per_iteration_profiled": round(total_kms, 5),
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0):
+    """The oracle (FP64 C restatement of the reference, single thread) on this host."""
+    from oracle.pyoracle import Oracle
+    o = Oracle(mesh, flow, rinit)
+    o.set_state(c0)
+    t0 = time.perf_counter()
+    o.iterate(1, 0)
+    one = time.perf_counter() - t0
+    n = max(1, int(budget_s / max(one, 1e-6)))
+    t0 = time.perf_counter()
+    o.iterate(n, 0)
+    dt = time.perf_counter() - t0
+    return {"value": mesh.neles * n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} RK4 iterations of the same {mesh.neles}-cell mesh and start "
+                      f"state, single thread ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    mesh, flow, c0, rinit, wname = _case(args.case)
+    from oracle.pyoracle import Oracle
+    o = Oracle(mesh, flow, rinit)
+    o.set_state(c0)
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.warmup, 3))):
+        o.iterate(1, 0)
+    per = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
+    n = min(args.steps, max(1, int(150.0 / max(per, 1e-6))))
+    times = []
+    for _ in range(n):
+        t = time.perf_counter()
+        o.iterate(1, 0)
+        times.append(time.perf_counter() - t)
+    ms = 1e3 * sum(times) / n
+    value = mesh.neles / (ms * 1e-3)
+    sample = (f"{n} of {args.steps} requested steps, each one full RK4 iteration of the "
+              f"{mesh.neles}-cell mesh, single thread (the reference is serial)")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": n,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": wname, "cells": mesh.neles, "precision": "fp64",
+                   "step": "one RK4 iteration (dissipation pre-pass + 4 stages)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--case", default="nozzle_plume_1024x384")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

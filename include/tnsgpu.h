@@ -74,6 +74,15 @@ int tns_upload_state(tns_handle *h, const double *c1, const double *c2, const do
 int tns_run(tns_handle *h, int niter, int monitor_every, double *cdiff_out, int max_records,
             int *n_records);
 
+/* Asynchronous form of tns_run without the residual monitor: enqueues niter RK4
+ * iterations on the handle's stream and returns at once.  Errors of the iterations
+ * (non-finite state) are reported by the next tns_synchronize / tns_run. */
+int tns_enqueue(tns_handle *h, int niter);
+
+/* Waits for the work enqueued on the handle's stream; TNS_ERR_NONFINITE if the state
+ * became NaN / Inf since the last check. */
+int tns_synchronize(tns_handle *h);
+
 /* Downloads C1..C5(1:NELES) (for restart.in, turbnstwod.f90:171-195). */
 int tns_download_state(tns_handle *h, double *c1, double *c2, double *c3, double *c4,
                        double *c5);

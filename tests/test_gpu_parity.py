@@ -64,10 +64,10 @@ def test_one_iteration_frozen_terms_and_state(name):
     ne = mesh.neles
     d_ref = np.stack([o.fetch(f"D24{k}")[:ne] for k in range(1, 6)])
     v_ref = np.stack([o.fetch(k)[:ne] for k in ("VISU", "VISV", "VIST", "VISR")])
-    assert np.all(rel(s.debug(0), d_ref) < 1e-12)
-    assert np.all(rel(s.debug(1), v_ref) < 1e-12)
+    assert np.all(rel(s.debug(0), d_ref) < 1e-11)
+    assert np.all(rel(s.debug(1), v_ref) < 1e-11)
     assert np.all(rel(s.debug(2), o.fetch("DT")[None, :ne]) < 1e-13)
-    assert np.all(rel(s.download(), o.state()) < 1e-12)
+    assert np.all(rel(s.download(), o.state()) < 1e-11)
     # U,V,T,P of cells and ghosts as the reference leaves them (POSTPROCESS input)
     nn = o.nn
     pr = s.primitives()[:, :nn]
