@@ -23,7 +23,7 @@ using tns::Params;
 
 namespace {
 
-enum KernelId { K_DISS = 0, K_STAGE1 = 1, K_STAGE = 2, K_DTMIN = 3, K_GPORT = 4, K_NKERNEL = 5 };
+enum KernelId { K_DISS = 0, K_VISC = 1, K_STAGE = 2, K_DTMIN = 3, K_GPORT = 4, K_NKERNEL = 5 };
 
 template <class T>
 struct DevBuf {
@@ -113,6 +113,9 @@ Params make_params(const tns_params& p) {
     P.rtol_rtred = P.rtol * p.rtred;
     P.bl_u = 2.0 * p.aminf * std::sqrt(P.gamrr * P.tinf);
     P.bl_exp = 1.0 / 7.0;
+    P.inv_cv = 1.0 / P.cv;
+    P.cp_pr = P.cp / p.prandtl;
+    P.cp_prt = P.cp / p.prandtlt;
     return P;
 }
 
@@ -369,8 +372,10 @@ void enqueue_iteration(tns_handle* h, bool monitor) {
     if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
     for (int st = 0; st < 4; st++) {
         if (np) launch(h, K_GPORT, [&] { tns::launch_gport(P, M, in[st], h->ports.p, np, h->gport.p, s); });
-        launch(h, st == 0 ? K_STAGE1 : K_STAGE, [&] {
-            tns::launch_stage(P, M, st == 0, in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
+        // the frozen viscous flux of Q_old uses stage 1's boundary state (viscous.f90:29)
+        if (st == 0) launch(h, K_VISC, [&] { tns::launch_viscous(P, M, A, h->vis.p, s); });
+        launch(h, K_STAGE, [&] {
+            tns::launch_stage(P, M, in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
                               alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
                               st == 3 ? h->status.p : nullptr, s);
         });

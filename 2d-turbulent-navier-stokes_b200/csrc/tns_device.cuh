@@ -2,9 +2,10 @@
 // physics of the RK4 / JST / viscous / source / boundary hot path.
 //
 // The arithmetic restates the reference solver's Fortran (paths relative to the
-// reference project) in the same operation order; only the memory layout differs:
-// cells live in a structured (i, j) block (j fastest), ghosts in four side arrays,
-// geometry is recomputed from node coordinates instead of being stored per cell.
+// reference project) in its operation order, except where one reciprocal replaces a
+// run of divisions by the same value and T**0.6 is exp(0.6*log T) (each a few ulp);
+// the memory layout is new: cells live in a structured (i, j) block (j fastest), ghosts
+// in four side arrays, geometry is recomputed from node coordinates.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,6 +46,8 @@ struct Params {
     double rtol_rtred;                   // RTOLERANCE*RTRED
     double bl_u;                         // 2*AMINF*DSQRT(GAMA*RR*TINF)
     double bl_exp;                       // 1/7
+    double inv_cv;                       // 1/CV
+    double cp_pr, cp_prt;                // CP/PRANDTL, CP/PRANDTLT
 };
 
 // Ghost-side numbering: side 1 (j=-1) and 3 (j=NJ) are indexed by i, sides 2 (i=NI)
@@ -82,8 +85,12 @@ __device__ __forceinline__ double powi(double x, int n) {
     return n < 0 ? 1.0 / r : r;
 }
 
+// T**0.6 as exp(0.6*log(T)): within a few ulp of pow and a third cheaper on the GPU.
+__device__ __forceinline__ double pow06(double T) { return exp(0.6 * log(T)); }
+
+// Sutherland-type molecular viscosity SUTH_COEF*DSQRT(AMOL)*T**0.6 (viscous.f90:188).
 __device__ __forceinline__ double amu_of(const Params& P, double T) {
-    return P.suth_amol * pow(T, 0.6);
+    return P.suth_amol * pow06(T);
 }
 
 // Primitive variables and fluxes of one interior cell (turbnstwod.f90:204-227).
@@ -95,11 +102,12 @@ struct Prim {
 __device__ __forceinline__ void primitive(const Params& P, double c1, double c2, double c3,
                                           double c4, double c5, Prim& s) {
     const double RHO = c1;
+    const double rr = 1.0 / RHO;  // one reciprocal instead of four divisions
     s.rho = RHO;
-    s.u = c2 / RHO;
-    s.v = c3 / RHO;
-    const double E = c4 / RHO;
-    s.t = (E - 0.5 * (s.u * s.u + s.v * s.v)) / P.cv;
+    s.u = c2 * rr;
+    s.v = c3 * rr;
+    const double E = c4 * rr;
+    s.t = (E - 0.5 * (s.u * s.u + s.v * s.v)) * P.inv_cv;
     s.p = RHO * P.rr * s.t;
     s.f[0] = c2;
     s.f[1] = RHO * s.u * s.u + s.p;
@@ -109,7 +117,7 @@ __device__ __forceinline__ void primitive(const Params& P, double c1, double c2,
     s.g[1] = s.f[2];
     s.g[2] = RHO * s.v * s.v + s.p;
     s.g[3] = (c4 + s.p) * s.v;
-    const double RT = c5 / RHO;
+    const double RT = c5 * rr;
     s.f[4] = RHO * RT * s.u;
     s.g[4] = RHO * RT * s.v;
     s.ri = RT;
@@ -289,15 +297,16 @@ struct SrcIn {
 __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, double RHO,
                                              double RI, double TI, double PI, double VI,
                                              double YCCI, double& src3, double& src5) {
-    const double DNR = (s.xa - s.xc) * (s.yb - s.yd) - (s.xb - s.xd) * (s.ya - s.yc);
-    const double DQX = ((s.qa - s.qc) * (s.yb - s.yd) - (s.qb - s.qd) * (s.ya - s.yc)) / DNR;
-    const double DRX = ((s.ra - s.rc) * (s.yb - s.yd) - (s.rb - s.rd) * (s.ya - s.yc)) / DNR;
-    const double DUX = ((s.ua - s.uc) * (s.yb - s.yd) - (s.ub - s.ud) * (s.ya - s.yc)) / DNR;
-    const double DVX = ((s.va - s.vc) * (s.yb - s.yd) - (s.vb - s.vd) * (s.ya - s.yc)) / DNR;
-    const double DQY = (-(s.qa - s.qc) * (s.xb - s.xd) + (s.qb - s.qd) * (s.xa - s.xc)) / DNR;
-    const double DRY = (-(s.ra - s.rc) * (s.xb - s.xd) + (s.rb - s.rd) * (s.xa - s.xc)) / DNR;
-    const double DUY = (-(s.ua - s.uc) * (s.xb - s.xd) + (s.ub - s.ud) * (s.xa - s.xc)) / DNR;
-    const double DVY = (-(s.va - s.vc) * (s.xb - s.xd) + (s.vb - s.vd) * (s.xa - s.xc)) / DNR;
+    const double ybd = s.yb - s.yd, yac = s.ya - s.yc, xbd = s.xb - s.xd, xac = s.xa - s.xc;
+    const double iDNR = 1.0 / (xac * ybd - xbd * yac);
+    const double DQX = ((s.qa - s.qc) * ybd - (s.qb - s.qd) * yac) * iDNR;
+    const double DRX = ((s.ra - s.rc) * ybd - (s.rb - s.rd) * yac) * iDNR;
+    const double DUX = ((s.ua - s.uc) * ybd - (s.ub - s.ud) * yac) * iDNR;
+    const double DVX = ((s.va - s.vc) * ybd - (s.vb - s.vd) * yac) * iDNR;
+    const double DQY = (-(s.qa - s.qc) * xbd + (s.qb - s.qd) * xac) * iDNR;
+    const double DRY = (-(s.ra - s.rc) * xbd + (s.rb - s.rd) * xac) * iDNR;
+    const double DUY = (-(s.ua - s.uc) * xbd + (s.ub - s.ud) * xac) * iDNR;
+    const double DVY = (-(s.va - s.vc) * xbd + (s.vb - s.vd) * xac) * iDNR;
     const double AMU = amu_of(P, TI);
     const double CHI = RHO * RI / (CMU * AMU);
     const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
@@ -341,15 +350,16 @@ struct FaceIn {
 
 __device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, bool first,
                                              double vis[4]) {
-    const double DNR = (f.xa - f.xc) * (f.yb - f.yd) - (f.xb - f.xd) * (f.ya - f.yc);
-    const double DUX = ((f.ua - f.uc) * (f.yb - f.yd) - (f.ub - f.ud) * (f.ya - f.yc)) / DNR;
-    const double DVX = ((f.va - f.vc) * (f.yb - f.yd) - (f.vb - f.vd) * (f.ya - f.yc)) / DNR;
-    const double DTX = ((f.ta - f.tc) * (f.yb - f.yd) - (f.tb - f.td) * (f.ya - f.yc)) / DNR;
-    const double DRX = ((f.ra - f.rc) * (f.yb - f.yd) - (f.rb - f.rd) * (f.ya - f.yc)) / DNR;
-    const double DUY = (-(f.ua - f.uc) * (f.xb - f.xd) + (f.ub - f.ud) * (f.xa - f.xc)) / DNR;
-    const double DVY = (-(f.va - f.vc) * (f.xb - f.xd) + (f.vb - f.vd) * (f.xa - f.xc)) / DNR;
-    const double DTY = (-(f.ta - f.tc) * (f.xb - f.xd) + (f.tb - f.td) * (f.xa - f.xc)) / DNR;
-    const double DRY = (-(f.ra - f.rc) * (f.xb - f.xd) + (f.rb - f.rd) * (f.xa - f.xc)) / DNR;
+    const double ybd = f.yb - f.yd, yac = f.ya - f.yc, xbd = f.xb - f.xd, xac = f.xa - f.xc;
+    const double iDNR = 1.0 / (xac * ybd - xbd * yac);
+    const double DUX = ((f.ua - f.uc) * ybd - (f.ub - f.ud) * yac) * iDNR;
+    const double DVX = ((f.va - f.vc) * ybd - (f.vb - f.vd) * yac) * iDNR;
+    const double DTX = ((f.ta - f.tc) * ybd - (f.tb - f.td) * yac) * iDNR;
+    const double DRX = ((f.ra - f.rc) * ybd - (f.rb - f.rd) * yac) * iDNR;
+    const double DUY = (-(f.ua - f.uc) * xbd + (f.ub - f.ud) * xac) * iDNR;
+    const double DVY = (-(f.va - f.vc) * xbd + (f.vb - f.vd) * xac) * iDNR;
+    const double DTY = (-(f.ta - f.tc) * xbd + (f.tb - f.td) * xac) * iDNR;
+    const double DRY = (-(f.ra - f.rc) * xbd + (f.rb - f.rd) * xac) * iDNR;
     const double UAVG = QUARTER * (f.ua + f.ub + f.uc + f.ud);
     const double VAVG = QUARTER * (f.va + f.vb + f.vc + f.vd);
     const double TAVG = QUARTER * (f.ta + f.tb + f.tc + f.td);
@@ -364,11 +374,11 @@ __device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, b
         DIVVEL = DUX + DVY;
     }
     const double AMU = amu_of(P, TAVG);
-    const double AK = AMU * P.cp / P.prandtl;
+    const double AK = AMU * P.cp_pr;
     const double CHI = RHOAVG * RAVG / (AMU * CMU);
     const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
     const double AMUT = RHOAVG * RAVG * FMU;
-    const double AKT = AMUT * P.cp / P.prandtlt;
+    const double AKT = AMUT * P.cp_prt;
     const double AMUEFF = AMU + AMUT;
     const double AKEFF = AK + AKT;
     const double TXX = AMUEFF * (DUX + DUX - P.div23 * DIVVEL);

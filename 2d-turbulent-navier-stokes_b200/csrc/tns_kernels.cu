@@ -16,11 +16,20 @@
 
 namespace tns {
 
-constexpr int TJ = 32;  // tile extent along j (contiguous in memory)
-constexpr int TI = 8;   // tile extent along i
+#ifndef TNS_TI
+#define TNS_TI 8
+#endif
+#ifndef TNS_STAGE_MINB
+#define TNS_STAGE_MINB 3
+#endif
+#ifndef TNS_VISC_MINB
+#define TNS_VISC_MINB 1
+#endif
+constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
+constexpr int TI = TNS_TI;  // tile extent along i
 constexpr int NTHREADS = TJ * TI;
 
-// ------------------------------------------------------------------ stage kernel
+// ------------------------------------------------------------ shared helpers
 
 // Halo-1 slot grid (TI+2) x (TJ+2), node grid (TI+3) x (TJ+3) (nodes of every halo cell).
 constexpr int SW = TJ + 2;
@@ -30,58 +39,8 @@ constexpr int NNODE = (TI + 3) * NW;
 constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
 constexpr int NAVG = (TI + 1) * AW;
 
-enum Field {
-    FU, FV, FT, FP, FRHO, FRI, FC5, FQM, FF0, FF1, FF2, FF3, FF4, FG0, FG1, FG2, FG3, FG4,
-    FXC, FYC, NFIELD
-};
-enum AvgField { AU, AV, AT, ARHO, AR, NAVGF };
-
-size_t stage_smem_bytes(bool with_viscous) {
-    size_t b = sizeof(double) * ((size_t)NFIELD * NSLOT + 2 * NNODE);
-    if (with_viscous) b += sizeof(double) * (size_t)NAVGF * NAVG;
-    return b;
-}
-
-__device__ __forceinline__ void load_prim(const double* sm, int s, Prim& p) {
-    p.u = sm[FU * NSLOT + s];
-    p.v = sm[FV * NSLOT + s];
-    p.t = sm[FT * NSLOT + s];
-    p.p = sm[FP * NSLOT + s];
-    p.rho = sm[FRHO * NSLOT + s];
-    p.ri = sm[FRI * NSLOT + s];
-    p.c5 = sm[FC5 * NSLOT + s];
-    p.qm = sm[FQM * NSLOT + s];
-#pragma unroll
-    for (int m = 0; m < 5; m++) {
-        p.f[m] = sm[(FF0 + m) * NSLOT + s];
-        p.g[m] = sm[(FG0 + m) * NSLOT + s];
-    }
-}
-
-__device__ __forceinline__ void store_prim(double* sm, int s, const Prim& p) {
-    sm[FU * NSLOT + s] = p.u;
-    sm[FV * NSLOT + s] = p.v;
-    sm[FT * NSLOT + s] = p.t;
-    sm[FP * NSLOT + s] = p.p;
-    sm[FRHO * NSLOT + s] = p.rho;
-    sm[FRI * NSLOT + s] = p.ri;
-    sm[FC5 * NSLOT + s] = p.c5;
-    sm[FQM * NSLOT + s] = p.qm;
-#pragma unroll
-    for (int m = 0; m < 5; m++) {
-        sm[(FF0 + m) * NSLOT + s] = p.f[m];
-        sm[(FG0 + m) * NSLOT + s] = p.g[m];
-    }
-}
-
-// Loads the halo-1 tile of Q_in, fills primitives / fluxes / centroids of every cell
-// and the BC state of every ghost in it.  Shared by the stage kernel and the
-// primitive-output kernel.  Ends with a __syncthreads().
-__device__ void fill_tile(const Params& P, const Mesh& M, const double* __restrict__ q,
-                          size_t ncell, int i0, int j0, double* sm, double* snx,
-                          double* sny) {
+__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny) {
     const int tid = threadIdx.y * TJ + threadIdx.x;
-    // nodes (i0-1 .. i0+TI+1) x (j0-1 .. j0+TJ+1)
     for (int s = tid; s < NNODE; s += NTHREADS) {
         const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
         if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
@@ -90,52 +49,71 @@ __device__ void fill_tile(const Params& P, const Mesh& M, const double* __restri
             sny[s] = M.y[n];
         }
     }
-    __syncthreads();
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
-        const int li = s / SW, lj = s % SW;
-        const int i = i0 - 1 + li, j = j0 - 1 + lj;
-        if (i >= 0 && i < M.ni && j >= 0 && j < M.nj) {
-            const size_t c = (size_t)i * M.nj + j;
-            Prim p;
-            primitive(P, q[c], q[ncell + c], q[2 * ncell + c], q[3 * ncell + c],
-                      q[4 * ncell + c], p);
-            store_prim(sm, s, p);
-            const int n1 = li * NW + lj;  // node (i, j) in the node grid
-            sm[FXC * NSLOT + s] = (snx[n1] + snx[n1 + NW] + snx[n1 + NW + 1] + snx[n1 + 1]) * 0.25;
-            sm[FYC * NSLOT + s] = (sny[n1] + sny[n1 + NW] + sny[n1 + NW + 1] + sny[n1 + 1]) * 0.25;
-        }
-    }
-    __syncthreads();
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
-        const int li = s / SW, lj = s % SW;
-        const int i = i0 - 1 + li, j = j0 - 1 + lj;
-        const bool in_i = i >= 0 && i < M.ni, in_j = j >= 0 && j < M.nj;
-        int side = 0, along = 0, sp = 0, so = 0;
-        if (in_i && j == -1) { side = 1; along = i; sp = s + 1; so = s + 2; }
-        else if (in_j && i == M.ni) { side = 2; along = j; sp = s - SW; so = s - 2 * SW; }
-        else if (in_i && j == M.nj) { side = 3; along = i; sp = s - 1; so = s - 2; }
-        else if (in_j && i == -1) { side = 4; along = j; sp = s + SW; so = s + 2 * SW; }
-        if (!side) continue;
-        const int g = M.ghost_index(side, along);
-        Prim par, opp, gh;
-        load_prim(sm, sp, par);
-        load_prim(sm, so, opp);
-        const int type = M.gtype[g];
-        double psx = 0.0, psy = 0.0;
-        if (type == 6) {
-            const int pli = sp / SW, plj = sp % SW;
-            const int n1 = pli * NW + plj;
-            const double X[4] = {snx[n1], snx[n1 + NW], snx[n1 + NW + 1], snx[n1 + 1]};
-            const double Y[4] = {sny[n1], sny[n1 + NW], sny[n1 + NW + 1], sny[n1 + 1]};
-            face_vector(P.iaxis, side, X, Y, psx, psy);
-        }
-        boundary_ghost(P, type, par, opp, psx, psy, M.gyc[g], sm[FYC * NSLOT + sp],
-                       type == 6 ? M.gport[g] : 0.0, M.ginj[g], gh);
-        store_prim(sm, s, gh);
-        sm[FXC * NSLOT + s] = M.gxc[g];
-        sm[FYC * NSLOT + s] = M.gyc[g];
-    }
-    __syncthreads();
+}
+
+__device__ __forceinline__ void cell_prim(const Params& P, const double* __restrict__ q, size_t ncell,
+                                          size_t c, Prim& p) {
+    primitive(P, q[c], q[ncell + c], q[2 * ncell + c], q[3 * ncell + c], q[4 * ncell + c], p);
+}
+
+// Classifies halo position (i, j): 0 = cell, 1..4 = ghost on that side, -1 = unused.
+__device__ __forceinline__ int classify(const Mesh& M, int i, int j, int& along) {
+    const bool in_i = i >= 0 && i < M.ni, in_j = j >= 0 && j < M.nj;
+    if (in_i && in_j) return 0;
+    if (in_i && j == -1) { along = i; return 1; }
+    if (in_j && i == M.ni) { along = j; return 2; }
+    if (in_i && j == M.nj) { along = i; return 3; }
+    if (in_j && i == -1) { along = j; return 4; }
+    return -1;
+}
+
+// BC state of the ghost on `side` at `along`, from the parent and the parent's opposite
+// neighbour read straight from the state array (bit-identical to their PRIMITIVE_VARS).
+__device__ void ghost_state(const Params& P, const Mesh& M, const double* __restrict__ q,
+                            size_t ncell, int side, int along, Prim& gh) {
+    int ip, jp, io, jo;
+    if (side == 1) { ip = along; jp = 0; io = along; jo = 1; }
+    else if (side == 2) { ip = M.ni - 1; jp = along; io = M.ni - 2; jo = along; }
+    else if (side == 3) { ip = along; jp = M.nj - 1; io = along; jo = M.nj - 2; }
+    else { ip = 0; jp = along; io = 1; jo = along; }
+    const int g = M.ghost_index(side, along);
+    const int type = M.gtype[g];
+    Prim par, opp;
+    cell_prim(P, q, ncell, (size_t)ip * M.nj + jp, par);
+    if (type == 3) cell_prim(P, q, ncell, (size_t)io * M.nj + jo, opp);
+    else opp = par;
+    const size_t n1 = (size_t)ip * (M.nj + 1) + jp;
+    const double X[4] = {M.x[n1], M.x[n1 + M.nj + 1], M.x[n1 + M.nj + 2], M.x[n1 + 1]};
+    const double Y[4] = {M.y[n1], M.y[n1 + M.nj + 1], M.y[n1 + M.nj + 2], M.y[n1 + 1]};
+    double psx = 0.0, psy = 0.0;
+    if (type == 6) face_vector(P.iaxis, side, X, Y, psx, psy);
+    const double ycc_p = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
+    boundary_ghost(P, type, par, opp, psx, psy, M.gyc[g], ycc_p, type == 6 ? M.gport[g] : 0.0,
+                   M.ginj[g], gh);
+}
+
+// ------------------------------------------------------------------ stage kernel
+
+// Shared-memory fields of the stage tile, paired for 16-byte loads.
+struct StageSmem {
+    double2 fg[5][NSLOT];  // (F_m, G_m)
+    double2 uv[NSLOT];     // (U, V)
+    double2 xy[NSLOT];     // centroid
+    double2 rq[NSLOT];     // (C5/C1, |V|)
+    double2 tp[NSLOT];     // (T, P)
+    double rho[NSLOT];
+    double nx[NNODE], ny[NNODE];
+};
+
+size_t stage_smem_bytes() { return sizeof(StageSmem); }
+
+__device__ __forceinline__ void put_slot(StageSmem& S, int s, const Prim& p) {
+#pragma unroll
+    for (int m = 0; m < 5; m++) S.fg[m][s] = make_double2(p.f[m], p.g[m]);
+    S.uv[s] = make_double2(p.u, p.v);
+    S.rq[s] = make_double2(p.ri, p.qm);
+    S.tp[s] = make_double2(p.t, p.p);
+    S.rho[s] = p.rho;
 }
 
 struct StageArgs {
@@ -143,7 +121,7 @@ struct StageArgs {
     const double* qold;  // state at the start of the iteration [5][ncell]
     double* qout;        // stage output [5][ncell] (may alias qold: own-cell reads only)
     const double* d;     // dissipation [5][ncell]
-    double* vis;         // viscous flux [4][ncell] (written in stage 1, read otherwise)
+    const double* vis;   // viscous flux [4][ncell]
     const double* dt;    // per-cell DT (LOCAL=1)
     const double* dtmin; // DTMIN (LOCAL=0)
     double alpha;
@@ -151,192 +129,112 @@ struct StageArgs {
     unsigned int* status;       // bit 0: non-finite state
 };
 
-template <bool VISC>
-__global__ void __launch_bounds__(NTHREADS)
-k_stage(Params P, Mesh M, StageArgs A) {
-    extern __shared__ double smem[];
-    double* sm = smem;
-    double* snx = sm + NFIELD * NSLOT;
-    double* sny = snx + NNODE;
-    double* avg = sny + NNODE;
+// One RK stage (turbnstwod.f90:204-227, boundary.f90:24-48, source_terms.f90:24-104,
+// residual.f90:23-83) on a TI x TJ tile with its halo staged in shared memory.
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage(Params P, Mesh M, StageArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
-    fill_tile(P, M, A.qin, ncell, i0, j0, sm, snx, sny);
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    __syncthreads();
+    for (int s = tid; s < NSLOT; s += NTHREADS) {
+        const int li = s / SW, lj = s % SW;
+        int along = 0;
+        const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
+        if (kind < 0) continue;
+        Prim p;
+        if (kind == 0) {
+            cell_prim(P, A.qin, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
+            const int n1 = li * NW + lj;
+            S.xy[s] = make_double2((S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25,
+                                   (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25);
+        } else {
+            ghost_state(P, M, A.qin, ncell, kind, along, p);
+            const int g = M.ghost_index(kind, along);
+            S.xy[s] = make_double2(M.gxc[g], M.gyc[g]);
+        }
+        put_slot(S, s, p);
+    }
+    __syncthreads();
 
     const int tj = threadIdx.x, ti = threadIdx.y;
     const int i = i0 + ti, j = j0 + tj;
-
-    if (VISC) {
-        // nodal averages (viscous.f90:40-59,77-124) of nodes (i0..i0+TI, j0..j0+TJ)
-        const int tid = ti * TJ + tj;
-        for (int s = tid; s < NAVG; s += NTHREADS) {
-            const int la = s / AW, lb = s % AW;
-            const int a = i0 + la, b = j0 + lb;
-            if (a > M.ni || b > M.nj) continue;
-            double un = 0.0, vn = 0.0, tn = 0.0, rhon = 0.0, rn = 0.0;
-            int cnt = 0, ng = 0, gs[2], gr[2];
-            // surrounding positions in ascending cell-id order
-            const int ps[4] = {la * SW + lb, la * SW + lb + 1, (la + 1) * SW + lb,
-                               (la + 1) * SW + lb + 1};
-            const int pi[4] = {a - 1, a - 1, a, a}, pj[4] = {b - 1, b, b - 1, b};
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const bool in_i = pi[k] >= 0 && pi[k] < M.ni, in_j = pj[k] >= 0 && pj[k] < M.nj;
-                const int sl = ps[k];
-                if (in_i && in_j) {
-                    un = un + sm[FU * NSLOT + sl];
-                    vn = vn + sm[FV * NSLOT + sl];
-                    tn = tn + sm[FT * NSLOT + sl];
-                    rhon = rhon + sm[FRHO * NSLOT + sl];
-                    rn = rn + sm[FRI * NSLOT + sl];
-                    cnt++;
-                } else if (in_i || in_j) {
-                    int side, along;
-                    if (in_i) { side = pj[k] < 0 ? 1 : 3; along = pi[k]; }
-                    else { side = pi[k] < 0 ? 4 : 2; along = pj[k]; }
-                    const int g = M.ghost_index(side, along);
-                    gs[ng] = sl;
-                    gr[ng] = g;
-                    ng++;
-                }
-            }
-            if (ng == 2 && M.grank[gr[1]] < M.grank[gr[0]]) {
-                int t = gs[0]; gs[0] = gs[1]; gs[1] = t;
-                t = gr[0]; gr[0] = gr[1]; gr[1] = t;
-            }
-            for (int k = 0; k < ng; k++) {
-                const int sl = gs[k];
-                un = un + sm[FU * NSLOT + sl];
-                vn = vn + sm[FV * NSLOT + sl];
-                tn = tn + sm[FT * NSLOT + sl];
-                rhon = rhon + sm[FRHO * NSLOT + sl];
-                rn = rn + sm[FRI * NSLOT + sl];
-                const int type = M.gtype[gr[k]];
-                if (type == 4) {
-                    vn = 0.0;
-                } else if (type == 5) {
-                    un = 0.0;
-                    vn = 0.0;
-                    rn = P.rtol_rtred;
-                }
-                cnt++;
-            }
-            const double df = (double)cnt;
-            avg[AU * NAVG + s] = un / df;
-            avg[AV * NAVG + s] = vn / df;
-            avg[AT * NAVG + s] = tn / df;
-            avg[ARHO * NAVG + s] = rhon / df;
-            avg[AR * NAVG + s] = dmax1(P.rtol, rn / df);
-        }
-        __syncthreads();
-    }
-
     const bool valid = i < M.ni && j < M.nj;
     double dv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (valid) {
-    const size_t cell = (size_t)i * M.nj + j;
-    const int c = (ti + 1) * SW + (tj + 1);
-    const int nb[4] = {c - 1, c + SW, c + 1, c - SW};  // NC1..NC4
-    const int n1 = (ti + 1) * NW + (tj + 1);
-    const double X[4] = {snx[n1], snx[n1 + NW], snx[n1 + NW + 1], snx[n1 + 1]};
-    const double Y[4] = {sny[n1], sny[n1 + NW], sny[n1 + NW + 1], sny[n1 + 1]};
-    double SX[4], SY[4];
+        const size_t cell = (size_t)i * M.nj + j;
+        const int c = (ti + 1) * SW + (tj + 1);
+        const int nb[4] = {c - 1, c + SW, c + 1, c - SW};  // NC1..NC4
+        const int n1 = (ti + 1) * NW + (tj + 1);
+        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
+        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
+        double SX[4], SY[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) face_vector(P.iaxis, k + 1, X, Y, SX[k], SY[k]);
-    const double ycc = sm[FYC * NSLOT + c];
-    const double VOL = cell_volume(P.iaxis, X, Y, ycc);
+        for (int k = 0; k < 4; k++) face_vector(P.iaxis, k + 1, X, Y, SX[k], SY[k]);
+        const double2 xyc = S.xy[c];
+        const double VOL = cell_volume(P.iaxis, X, Y, xyc.y);
 
-    double vis[4];
-    if (VISC) {
-        const int a1 = ti * AW + tj;  // node (i, j) in the average grid
-        const int an[4] = {a1, a1 + AW, a1 + AW + 1, a1 + 1};
+        // inviscid residual (residual.f90:23-62)
+        double R[5];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int nc = nb[k], B = an[k], D = an[(k + 1) & 3];
-            FaceIn f;
-            f.sx = SX[k]; f.sy = SY[k];
-            f.xa = sm[FXC * NSLOT + c]; f.ya = ycc;
-            f.xb = X[k]; f.yb = Y[k];
-            f.xc = sm[FXC * NSLOT + nc]; f.yc = sm[FYC * NSLOT + nc];
-            f.xd = X[(k + 1) & 3]; f.yd = Y[(k + 1) & 3];
-            f.ua = sm[FU * NSLOT + c]; f.va = sm[FV * NSLOT + c]; f.ta = sm[FT * NSLOT + c];
-            f.ub = avg[AU * NAVG + B]; f.vb = avg[AV * NAVG + B]; f.tb = avg[AT * NAVG + B];
-            f.uc = sm[FU * NSLOT + nc]; f.vc = sm[FV * NSLOT + nc]; f.tc = sm[FT * NSLOT + nc];
-            f.ud = avg[AU * NAVG + D]; f.vd = avg[AV * NAVG + D]; f.td = avg[AT * NAVG + D];
-            f.rhoa = sm[FRHO * NSLOT + c]; f.rhob = avg[ARHO * NAVG + B];
-            f.rhoc = sm[FRHO * NSLOT + nc]; f.rhod = avg[ARHO * NAVG + D];
-            f.ra = sm[FRI * NSLOT + c]; f.rb = avg[AR * NAVG + B];
-            f.rc = sm[FRI * NSLOT + nc]; f.rd = avg[AR * NAVG + D];
-            viscous_face(P, f, k == 0, vis);
+        for (int m = 0; m < 5; m++) {
+            const double2 I = S.fg[m][c], a = S.fg[m][nb[0]], b = S.fg[m][nb[1]],
+                          e = S.fg[m][nb[2]], d = S.fg[m][nb[3]];
+            R[m] = HALF * ((I.x + a.x) * SX[0] + (I.y + a.y) * SY[0] + (I.x + b.x) * SX[1] +
+                           (I.y + b.y) * SY[1] + (I.x + e.x) * SX[2] + (I.y + e.y) * SY[2] +
+                           (I.x + d.x) * SX[3] + (I.y + d.y) * SY[3]);
+        }
+
+        // source terms (source_terms.f90:258-320)
+        {
+            SrcIn s;
+            const double2 xa = S.xy[nb[0]], xb = S.xy[nb[1]], xc = S.xy[nb[2]], xd = S.xy[nb[3]];
+            const double2 ua = S.uv[nb[0]], ub = S.uv[nb[1]], uc = S.uv[nb[2]], ud = S.uv[nb[3]];
+            const double2 ra = S.rq[nb[0]], rb = S.rq[nb[1]], rc = S.rq[nb[2]], rd = S.rq[nb[3]];
+            s.xa = xa.x; s.xb = xb.x; s.xc = xc.x; s.xd = xd.x;
+            s.ya = xa.y; s.yb = xb.y; s.yc = xc.y; s.yd = xd.y;
+            s.ua = ua.x; s.ub = ub.x; s.uc = uc.x; s.ud = ud.x;
+            s.va = ua.y; s.vb = ub.y; s.vc = uc.y; s.vd = ud.y;
+            s.ra = ra.x; s.rb = rb.x; s.rc = rc.x; s.rd = rd.x;
+            s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
+            const double2 tp = S.tp[c];
+            double src3, src5;
+            source_terms(P, s, S.rho[c], S.rq[c].x, tp.x, tp.y, S.uv[c].y, xyc.y, src3, src5);
+            R[4] = R[4] - VOL * src5;
+            if (P.iaxis == 1) R[2] = R[2] - VOL * src3;
+        }
+
+        // update (residual.f90:67-83)
+        const double DT = P.local ? A.dt[cell] : *A.dtmin;
+        const double DTBYVOL = DT / VOL;
+        const double al = A.alpha;
+        double Cn[5], Co[5], vis[4], dd[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            Co[m] = A.qold[m * ncell + cell];
+            dd[m] = A.d[m * ncell + cell];
         }
 #pragma unroll
-        for (int k = 0; k < 4; k++) A.vis[k * ncell + cell] = vis[k];
-    } else {
-#pragma unroll
         for (int k = 0; k < 4; k++) vis[k] = A.vis[k * ncell + cell];
+        Cn[0] = Co[0] - al * DTBYVOL * (R[0] - dd[0]);
+        Cn[1] = Co[1] - al * DTBYVOL * (R[1] - vis[0] - dd[1]);
+        Cn[2] = Co[2] - al * DTBYVOL * (R[2] - vis[1] - dd[2]);
+        Cn[3] = Co[3] - al * DTBYVOL * (R[3] - vis[2] - dd[3]);
+        Cn[4] = Co[4] - al * DTBYVOL * CFLTURB * (R[4] - vis[3] - dd[4]);
+        Cn[4] = Cn[0] * dmax1(P.rtol, Cn[4] / Cn[0]);
+#pragma unroll
+        for (int m = 0; m < 5; m++) A.qout[m * ncell + cell] = Cn[m];
+        if (A.status) {
+            bool bad = false;
+#pragma unroll
+            for (int m = 0; m < 5; m++) bad |= !isfinite(Cn[m]);
+            if (bad) atomicOr(A.status, 1u);
+        }
+#pragma unroll
+        for (int m = 0; m < 5; m++) dv[m] = fabs(Co[m] - Cn[m]);
     }
-
-    // inviscid residual (residual.f90:23-62)
-    double R[5];
-#pragma unroll
-    for (int m = 0; m < 5; m++) {
-        const double* F = sm + (FF0 + m) * NSLOT;
-        const double* G = sm + (FG0 + m) * NSLOT;
-        const double FI = F[c], GI = G[c];
-        R[m] = HALF * ((FI + F[nb[0]]) * SX[0] + (GI + G[nb[0]]) * SY[0] +
-                       (FI + F[nb[1]]) * SX[1] + (GI + G[nb[1]]) * SY[1] +
-                       (FI + F[nb[2]]) * SX[2] + (GI + G[nb[2]]) * SY[2] +
-                       (FI + F[nb[3]]) * SX[3] + (GI + G[nb[3]]) * SY[3]);
-    }
-
-    // source terms (source_terms.f90:258-320)
-    {
-        SrcIn s;
-        const int a = nb[0], b = nb[1], cc = nb[2], d = nb[3];
-        s.xa = sm[FXC * NSLOT + a]; s.xb = sm[FXC * NSLOT + b];
-        s.xc = sm[FXC * NSLOT + cc]; s.xd = sm[FXC * NSLOT + d];
-        s.ya = sm[FYC * NSLOT + a]; s.yb = sm[FYC * NSLOT + b];
-        s.yc = sm[FYC * NSLOT + cc]; s.yd = sm[FYC * NSLOT + d];
-        s.ua = sm[FU * NSLOT + a]; s.ub = sm[FU * NSLOT + b];
-        s.uc = sm[FU * NSLOT + cc]; s.ud = sm[FU * NSLOT + d];
-        s.va = sm[FV * NSLOT + a]; s.vb = sm[FV * NSLOT + b];
-        s.vc = sm[FV * NSLOT + cc]; s.vd = sm[FV * NSLOT + d];
-        s.ra = sm[FRI * NSLOT + a]; s.rb = sm[FRI * NSLOT + b];
-        s.rc = sm[FRI * NSLOT + cc]; s.rd = sm[FRI * NSLOT + d];
-        s.qa = sm[FQM * NSLOT + a]; s.qb = sm[FQM * NSLOT + b];
-        s.qc = sm[FQM * NSLOT + cc]; s.qd = sm[FQM * NSLOT + d];
-        double src3, src5;
-        source_terms(P, s, sm[FRHO * NSLOT + c], sm[FRI * NSLOT + c], sm[FT * NSLOT + c],
-                     sm[FP * NSLOT + c], sm[FV * NSLOT + c], ycc, src3, src5);
-        R[4] = R[4] - VOL * src5;
-        if (P.iaxis == 1) R[2] = R[2] - VOL * src3;
-    }
-
-    // update (residual.f90:67-83)
-    const double DT = P.local ? A.dt[cell] : *A.dtmin;
-    const double DTBYVOL = DT / VOL;
-    const double al = A.alpha;
-    double Cn[5], Co[5];
-#pragma unroll
-    for (int m = 0; m < 5; m++) Co[m] = A.qold[m * ncell + cell];
-    Cn[0] = Co[0] - al * DTBYVOL * (R[0] - A.d[cell]);
-    Cn[1] = Co[1] - al * DTBYVOL * (R[1] - vis[0] - A.d[ncell + cell]);
-    Cn[2] = Co[2] - al * DTBYVOL * (R[2] - vis[1] - A.d[2 * ncell + cell]);
-    Cn[3] = Co[3] - al * DTBYVOL * (R[3] - vis[2] - A.d[3 * ncell + cell]);
-    Cn[4] = Co[4] - al * DTBYVOL * CFLTURB * (R[4] - vis[3] - A.d[4 * ncell + cell]);
-    Cn[4] = Cn[0] * dmax1(P.rtol, Cn[4] / Cn[0]);
-#pragma unroll
-    for (int m = 0; m < 5; m++) A.qout[m * ncell + cell] = Cn[m];
-
-    if (A.status) {
-        bool bad = false;
-#pragma unroll
-        for (int m = 0; m < 5; m++) bad |= !isfinite(Cn[m]);
-        if (bad) atomicOr(A.status, 1u);
-    }
-#pragma unroll
-    for (int m = 0; m < 5; m++) dv[m] = fabs(Co[m] - Cn[m]);
-    }  // valid
     if (A.cdiff) {
         // max |COLD - C| per component: warp max, then one atomic per warp on the ordered
         // bit pattern (non-negative doubles order like their bits)
@@ -347,6 +245,171 @@ k_stage(Params P, Mesh M, StageArgs A) {
             if ((threadIdx.x & 31) == 0)
                 atomicMax(&A.cdiff[m], (unsigned long long)__double_as_longlong(v));
         }
+    }
+}
+
+// ---------------------------------------------------------------- viscous kernel
+
+// Faces owned by a tile: i-faces (between cells (i-1,j) and (i,j)) for i in i0..i0+TI,
+// j-faces (between (i,j-1) and (i,j)) for j in j0..j0+TJ.
+constexpr int NIF = (TI + 1) * TJ;
+constexpr int NJF = TI * (TJ + 1);
+
+struct ViscSmem {
+    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT], xc[NSLOT], yc[NSLOT];
+    double au[NAVG], av[NAVG], at[NAVG], arho[NAVG], ar[NAVG];
+    double fi[4][NIF], fj[4][NJF];
+    double nx[NNODE], ny[NNODE];
+};
+
+size_t visc_smem_bytes() { return sizeof(ViscSmem); }
+
+// One face flux (viscous.f90:130-217) in the orientation of cell A (slot sa) for its
+// face k (1..4): C = slot sc, B/D = face nodes given in node-average and node-grid
+// coordinates.
+__device__ __forceinline__ void face_flux(const Params& P, const ViscSmem& S, int sa, int sc,
+                                          int ab, int ad, int nb, int nd, double out[4]) {
+    FaceIn f;
+    f.xb = S.nx[nb]; f.yb = S.ny[nb];
+    f.xd = S.nx[nd]; f.yd = S.ny[nd];
+    if (P.iaxis == 1) {
+        f.sx = (f.yd - f.yb) * (f.yb + f.yd) * HALF;
+        f.sy = -(f.xd - f.xb) * (f.yb + f.yd) * HALF;
+    } else {
+        f.sx = (f.yd - f.yb);
+        f.sy = -(f.xd - f.xb);
+    }
+    f.xa = S.xc[sa]; f.ya = S.yc[sa];
+    f.xc = S.xc[sc]; f.yc = S.yc[sc];
+    f.ua = S.u[sa]; f.va = S.v[sa]; f.ta = S.t[sa];
+    f.uc = S.u[sc]; f.vc = S.v[sc]; f.tc = S.t[sc];
+    f.ub = S.au[ab]; f.vb = S.av[ab]; f.tb = S.at[ab];
+    f.ud = S.au[ad]; f.vd = S.av[ad]; f.td = S.at[ad];
+    f.rhoa = S.rho[sa]; f.rhoc = S.rho[sc]; f.rhob = S.arho[ab]; f.rhod = S.arho[ad];
+    f.ra = S.ri[sa]; f.rc = S.ri[sc]; f.rb = S.ar[ab]; f.rd = S.ar[ad];
+    viscous_face(P, f, true, out);
+}
+
+// Frozen viscous flux VIS of Q_old (viscous.f90:29-217): nodal averages, then each face
+// of the tile once; a cell adds its four faces in order 1..4, negating the faces that
+// were evaluated in the neighbour's orientation.
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous(Params P, Mesh M, const double* __restrict__ q,
+                                                      double* __restrict__ vis) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ViscSmem& S = *reinterpret_cast<ViscSmem*>(smem_raw);
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    __syncthreads();
+    for (int s = tid; s < NSLOT; s += NTHREADS) {
+        const int li = s / SW, lj = s % SW;
+        int along = 0;
+        const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
+        if (kind < 0) continue;
+        Prim p;
+        if (kind == 0) {
+            cell_prim(P, q, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
+            const int n1 = li * NW + lj;
+            S.xc[s] = (S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25;
+            S.yc[s] = (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25;
+        } else {
+            ghost_state(P, M, q, ncell, kind, along, p);
+            const int g = M.ghost_index(kind, along);
+            S.xc[s] = M.gxc[g];
+            S.yc[s] = M.gyc[g];
+        }
+        S.u[s] = p.u; S.v[s] = p.v; S.t[s] = p.t; S.rho[s] = p.rho; S.ri[s] = p.ri;
+    }
+    __syncthreads();
+    // nodal averages (viscous.f90:40-59,77-124) of nodes (i0..i0+TI, j0..j0+TJ)
+    for (int s = tid; s < NAVG; s += NTHREADS) {
+        const int la = s / AW, lb = s % AW;
+        const int a = i0 + la, b = j0 + lb;
+        if (a > M.ni || b > M.nj) continue;
+        double un = 0.0, vn = 0.0, tn = 0.0, rhon = 0.0, rn = 0.0;
+        int cnt = 0, ng = 0, gs[2] = {0, 0}, gr[2] = {0, 0};
+        // the four surrounding positions in ascending cell-id order
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int pi = a - 1 + (k >> 1), pj = b - 1 + (k & 1);
+            const int sl = (la + (k >> 1)) * SW + lb + (k & 1);
+            int along = 0;
+            const int kind = classify(M, pi, pj, along);
+            if (kind == 0) {
+                un = un + S.u[sl]; vn = vn + S.v[sl]; tn = tn + S.t[sl];
+                rhon = rhon + S.rho[sl]; rn = rn + S.ri[sl];
+                cnt++;
+            } else if (kind > 0) {
+                gs[ng] = sl;
+                gr[ng] = M.ghost_index(kind, along);
+                ng++;
+            }
+        }
+        if (ng == 2 && M.grank[gr[1]] < M.grank[gr[0]]) {
+            int t = gs[0]; gs[0] = gs[1]; gs[1] = t;
+            t = gr[0]; gr[0] = gr[1]; gr[1] = t;
+        }
+        for (int k = 0; k < ng; k++) {
+            const int sl = gs[k];
+            un = un + S.u[sl]; vn = vn + S.v[sl]; tn = tn + S.t[sl];
+            rhon = rhon + S.rho[sl]; rn = rn + S.ri[sl];
+            const int type = M.gtype[gr[k]];
+            if (type == 4) {
+                vn = 0.0;
+            } else if (type == 5) {
+                un = 0.0; vn = 0.0; rn = P.rtol_rtred;
+            }
+            cnt++;
+        }
+        const double idf = cnt == 4 ? 0.25 : 1.0 / (double)cnt;
+        S.au[s] = un * idf; S.av[s] = vn * idf; S.at[s] = tn * idf; S.arho[s] = rhon * idf;
+        S.ar[s] = dmax1(P.rtol, rn * idf);
+    }
+    __syncthreads();
+    // i-faces: orientation of cell (i-1, j) as its face 2, or of (0, j) as its face 4
+    for (int f = tid; f < NIF; f += NTHREADS) {
+        const int ii = f / TJ, jj = f % TJ;
+        const int i = i0 + ii, j = j0 + jj;
+        if (i > M.ni || j >= M.nj) continue;
+        double out[4];
+        const int sL = ii * SW + jj + 1, sR = sL + SW;  // cells (i-1, j), (i, j)
+        const int aLo = ii * AW + jj, aHi = aLo + 1;    // nodes (i, j), (i, j+1)
+        const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
+        if (i == 0) face_flux(P, S, sR, sL, aHi, aLo, nHi, nLo, out);  // face 4: B=N4, D=N1
+        else face_flux(P, S, sL, sR, aLo, aHi, nLo, nHi, out);          // face 2: B=N2, D=N3
+#pragma unroll
+        for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
+    }
+    // j-faces: orientation of cell (i, j-1) as its face 3, or of (i, 0) as its face 1
+    for (int f = tid; f < NJF; f += NTHREADS) {
+        const int ii = f / AW, jj = f % AW;
+        const int i = i0 + ii, j = j0 + jj;
+        if (i >= M.ni || j > M.nj) continue;
+        double out[4];
+        const int sB = (ii + 1) * SW + jj, sT = sB + 1;  // cells (i, j-1), (i, j)
+        const int aL = ii * AW + jj, aR = aL + AW;       // nodes (i, j), (i+1, j)
+        const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
+        if (j == 0) face_flux(P, S, sT, sB, aL, aR, nL, nR, out);  // face 1: B=N1, D=N2
+        else face_flux(P, S, sB, sT, aR, aL, nR, nL, out);          // face 3: B=N3, D=N4
+#pragma unroll
+        for (int k = 0; k < 4; k++) S.fj[k][f] = out[k];
+    }
+    __syncthreads();
+    const int tj = threadIdx.x, ti = threadIdx.y;
+    const int i = i0 + ti, j = j0 + tj;
+    if (i >= M.ni || j >= M.nj) return;
+    const size_t cell = (size_t)i * M.nj + j;
+    const int f1 = ti * AW + tj, f3 = f1 + 1;          // j-faces j, j+1
+    const int f4 = ti * TJ + tj, f2 = f4 + TJ;         // i-faces i, i+1
+    const double s1 = (j == 0) ? 1.0 : -1.0, s4 = (i == 0) ? 1.0 : -1.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double acc = s1 * S.fj[k][f1];
+        acc = acc + S.fi[k][f2];
+        acc = acc + S.fj[k][f3];
+        acc = acc + s4 * S.fi[k][f4];
+        vis[k * ncell + cell] = acc;
     }
 }
 
@@ -374,10 +437,11 @@ __device__ __forceinline__ double local_dt(const Params& P, double c1, double c2
                                            double c4, double cfldl) {
     // turbnstwod.f90:97-108
     const double RHO = c1;
-    const double U = c2 / RHO, V = c3 / RHO;
+    const double rr = 1.0 / RHO;
+    const double U = c2 * rr, V = c3 * rr;
     const double VEL = sqrt(U * U + V * V);
-    const double E = c4 / RHO;
-    const double T = (E - 0.5 * (U * U + V * V)) / P.cv;
+    const double E = c4 * rr;
+    const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
     return cfldl / (fabs(VEL) + sqrt(P.gamrr * T));
 }
 
@@ -411,9 +475,10 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, Diss
             }
             // P as in the DT loop (turbnstwod.f90:98-104)
             const double RHO = C[0];
-            const double U = C[1] / RHO, V = C[2] / RHO;
-            const double E = C[3] / RHO;
-            const double T = (E - 0.5 * (U * U + V * V)) / P.cv;
+            const double rr = 1.0 / RHO;
+            const double U = C[1] * rr, V = C[2] * rr;
+            const double E = C[3] * rr;
+            const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
             sd[DP * NDSLOT + s] = RHO * P.rr * T;
         }
     }
@@ -589,35 +654,27 @@ __global__ void k_gport(Params P, Mesh M, const double* __restrict__ q, const in
 // U, V, T, P of every cell and ghost computed from q (the last stage's input), the
 // arrays COMPUTE_PRIMITIVE_VARS / APPLY_BOUNDARY leave behind.  Output layout:
 // [4][ncell + nghost] with ghosts in side-array order.
-__global__ void __launch_bounds__(NTHREADS)
-k_prim_out(Params P, Mesh M, const double* __restrict__ q, double* out) {
-    extern __shared__ double smem[];
-    double* sm = smem;
-    double* snx = sm + NFIELD * NSLOT;
-    double* sny = snx + NNODE;
+__global__ void k_prim_out(Params P, Mesh M, const double* __restrict__ q, double* out) {
     const size_t ncell = (size_t)M.ni * M.nj;
-    const size_t ntot = ncell + M.nghosts();
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
-    fill_tile(P, M, q, ncell, i0, j0, sm, snx, sny);
-    const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
-        const int li = s / SW, lj = s % SW;
-        const int i = i0 - 1 + li, j = j0 - 1 + lj;
-        const bool in_i = i >= 0 && i < M.ni, in_j = j >= 0 && j < M.nj;
-        size_t o;
-        if (in_i && in_j) {
-            if (li < 1 || li > TI || lj < 1 || lj > TJ) continue;  // owned by another tile
-            o = (size_t)i * M.nj + j;
-        } else if (in_i && j == -1) o = ncell + M.ghost_index(1, i);
-        else if (in_j && i == M.ni) o = ncell + M.ghost_index(2, j);
-        else if (in_i && j == M.nj) o = ncell + M.ghost_index(3, i);
-        else if (in_j && i == -1) o = ncell + M.ghost_index(4, j);
-        else continue;
-        out[o] = sm[FU * NSLOT + s];
-        out[ntot + o] = sm[FV * NSLOT + s];
-        out[2 * ntot + o] = sm[FT * NSLOT + s];
-        out[3 * ntot + o] = sm[FP * NSLOT + s];
+    const size_t ng = M.nghosts(), ntot = ncell + ng;
+    const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k >= ntot) return;
+    Prim p;
+    if (k < ncell) {
+        cell_prim(P, q, ncell, k, p);
+    } else {
+        const int g = (int)(k - ncell);
+        int side, along;
+        if (g < M.ni) { side = 1; along = g; }
+        else if (g < M.ni + M.nj) { side = 2; along = g - M.ni; }
+        else if (g < 2 * M.ni + M.nj) { side = 3; along = g - M.ni - M.nj; }
+        else { side = 4; along = g - 2 * M.ni - M.nj; }
+        ghost_state(P, M, q, ncell, side, along, p);
     }
+    out[k] = p.u;
+    out[ntot + k] = p.v;
+    out[2 * ntot + k] = p.t;
+    out[3 * ntot + k] = p.p;
 }
 
 // ------------------------------------------------------------------ launchers
@@ -626,14 +683,11 @@ static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni +
 
 cudaError_t configure_kernels() {
     cudaError_t e;
-    e = cudaFuncSetAttribute(k_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stage_smem_bytes(true));
+    e = cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage_smem_bytes());
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stage_smem_bytes(false));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_prim_out, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stage_smem_bytes(false));
+    e = cudaFuncSetAttribute(k_viscous, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)visc_smem_bytes());
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_dissipation, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)diss_smem_bytes());
@@ -645,15 +699,16 @@ void launch_dissipation(const Params& P, const Mesh& M, const double* q, double*
     k_dissipation<<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
 }
 
-void launch_stage(const Params& P, const Mesh& M, bool viscous, const double* qin,
-                  const double* qold, double* qout, const double* d, double* vis,
-                  const double* dt, const double* dtmin, double alpha,
-                  unsigned long long* cdiff, unsigned int* status, cudaStream_t s) {
+void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis, cudaStream_t s) {
+    k_viscous<<<tile_grid(M), dim3(TJ, TI), visc_smem_bytes(), s>>>(P, M, q, vis);
+}
+
+void launch_stage(const Params& P, const Mesh& M, const double* qin, const double* qold,
+                  double* qout, const double* d, const double* vis, const double* dt,
+                  const double* dtmin, double alpha, unsigned long long* cdiff,
+                  unsigned int* status, cudaStream_t s) {
     StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status};
-    if (viscous)
-        k_stage<true><<<tile_grid(M), dim3(TJ, TI), stage_smem_bytes(true), s>>>(P, M, A);
-    else
-        k_stage<false><<<tile_grid(M), dim3(TJ, TI), stage_smem_bytes(false), s>>>(P, M, A);
+    k_stage<<<tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s>>>(P, M, A);
 }
 
 int dtmin_blocks(const Mesh& M) {
@@ -677,7 +732,8 @@ void launch_gport(const Params& P, const Mesh& M, const double* q, const int* gh
 
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,
                      cudaStream_t s) {
-    k_prim_out<<<tile_grid(M), dim3(TJ, TI), stage_smem_bytes(false), s>>>(P, M, q, out);
+    const size_t ntot = (size_t)M.ni * M.nj + M.nghosts();
+    k_prim_out<<<(unsigned)((ntot + 255) / 256), 256, 0, s>>>(P, M, q, out);
 }
 
 }  // namespace tns

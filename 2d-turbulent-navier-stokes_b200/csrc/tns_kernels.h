@@ -9,16 +9,18 @@
 namespace tns {
 
 cudaError_t configure_kernels();
-size_t stage_smem_bytes(bool with_viscous);
+size_t stage_smem_bytes();
+size_t visc_smem_bytes();
 size_t diss_smem_bytes();
 int dtmin_blocks(const Mesh& M);
 
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,
                         const double* dtmin, cudaStream_t s);
-void launch_stage(const Params& P, const Mesh& M, bool viscous, const double* qin,
-                  const double* qold, double* qout, const double* d, double* vis,
-                  const double* dt, const double* dtmin, double alpha,
-                  unsigned long long* cdiff, unsigned int* status, cudaStream_t s);
+void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis, cudaStream_t s);
+void launch_stage(const Params& P, const Mesh& M, const double* qin, const double* qold,
+                  double* qout, const double* d, const double* vis, const double* dt,
+                  const double* dtmin, double alpha, unsigned long long* cdiff,
+                  unsigned int* status, cudaStream_t s);
 void launch_dtmin(const Params& P, const Mesh& M, const double* q, double* partial,
                   unsigned int* counter, double* dtmin, cudaStream_t s);
 void launch_gport(const Params& P, const Mesh& M, const double* q, const int* ghosts, int nport,

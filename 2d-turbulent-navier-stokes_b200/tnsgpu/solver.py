@@ -127,7 +127,7 @@ class Solver:
 
     def kernel_times(self) -> dict:
         out = {}
-        for k, name in enumerate(("dissipation", "stage1", "stage", "dtmin", "gport")):
+        for k, name in enumerate(("dissipation", "viscous", "stage", "dtmin", "gport")):
             ms, n = C.c_double(0), C.c_longlong(0)
             self._check(self.L.tns_kernel_times(self.h, k, C.byref(ms), C.byref(n)))
             out[name] = (ms.value, n.value)

@@ -104,7 +104,7 @@ int tns_set_stream(tns_handle *h, void *stream);
 
 /* Per-kernel device timing of the next tns_run calls (CUDA events around every
  * launch); tns_kernel_times returns, for kernel k, the summed milliseconds and the
- * launch count.  Kernel ids: 0 dissipation, 1 stage 1 (viscous), 2 stages 2-4,
+ * launch count.  Kernel ids: 0 dissipation, 1 viscous flux, 2 RK stages (all four),
  * 3 dtmin, 4 gport. */
 int tns_profile(tns_handle *h, int enable);
 int tns_kernel_times(tns_handle *h, int kernel, double *ms, long long *launches);
