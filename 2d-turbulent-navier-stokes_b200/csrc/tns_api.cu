@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -642,6 +643,57 @@ int tns_kernel_times(tns_handle* h, int kernel, double* ms, long long* launches)
 long long tns_launch_count(tns_handle* h) { return h ? h->launches : -1; }
 
 const char* tns_last_error(tns_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+}  // extern "C"
+
+// ----------------------------------------------------------- allocation-free time step
+//
+// Scratch of tns_time_step_noalloc, in device memory that exists as soon as the library
+// is loaded: one partial minimum per block, then the blocks' completion counter.
+// Every GPU that loads the library keeps this array until the process exits.
+static __device__ __align__(256) unsigned char g_step_scratch[TNS_NOALLOC_MAX_BLOCKS * sizeof(double) + 256];
+
+namespace {
+std::mutex g_step_mutex;
+void* g_step_ptr[256] = {};  // device address of g_step_scratch, per device ordinal
+}  // namespace
+
+extern "C" {
+
+int tns_time_step_noalloc(const double* d_q, const double* d_cfldl, long long ncell,
+                          const tns_params* params, double* d_dt, double* d_dtmin, void* stream) {
+    if (!d_q || !d_cfldl || !params || !d_dt || !d_dtmin || ncell <= 0) return TNS_ERR_ARG;
+    const long long per_block = 256LL * TNS_NOALLOC_CELLS_PER_THREAD;
+    const long long nblocks = (ncell + per_block - 1) / per_block;
+    if (nblocks > TNS_NOALLOC_MAX_BLOCKS) return TNS_ERR_TOO_LARGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return TNS_ERR_CUDA;
+    void* base = nullptr;
+    {
+        // set-up, once per device: the host-side name of the array is not a device
+        // address, so ask the runtime for it with this device current
+        std::lock_guard<std::mutex> lock(g_step_mutex);
+        if (!g_step_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_step_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return TNS_ERR_CUDA;
+            }
+            g_step_ptr[dev] = p;
+        }
+        base = g_step_ptr[dev];
+    }
+    double* partial = static_cast<double*>(base);
+    unsigned int* counter =
+        reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(base) + TNS_NOALLOC_MAX_BLOCKS * sizeof(double));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the array keeps whatever the previous call left: the counter must start at zero
+    if (cudaMemsetAsync(counter, 0, sizeof(unsigned int), s) != cudaSuccess) return TNS_ERR_CUDA;
+    const Params P = make_params(*params);
+    tns::launch_time_step_scratch(P, d_q, d_cfldl, ncell, d_dt, partial, counter, d_dtmin,
+                                  (int)nblocks, s);
+    return cudaGetLastError() == cudaSuccess ? TNS_OK : TNS_ERR_CUDA;
+}
 
 void tns_destroy(tns_handle* h) {
     if (!h) return;

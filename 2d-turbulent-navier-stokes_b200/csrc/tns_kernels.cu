@@ -610,6 +610,50 @@ k_dtmin(Params P, Mesh M, const double* __restrict__ q, double* dt, double* part
     }
 }
 
+// Variant of k_dtmin for caller-provided device buffers (tns_time_step_noalloc): also
+// stores the per-cell DT, and reduces through the scratch the launcher is handed
+// (`partial`: one double per block, `counter`: zero on entry, left at zero on exit).
+__global__ void __launch_bounds__(256)
+k_time_step_scratch(Params P, const double* __restrict__ q, const double* __restrict__ cfldl,
+                    long long ncell, double* __restrict__ dt, double* partial,
+                    unsigned int* counter, double* dtmin) {
+    double mn = 100000.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const double v = local_dt(P, q[c], q[ncell + c], q[2 * ncell + c], q[3 * ncell + c],
+                                  cfldl[c]);
+        dt[c] = v;
+        mn = dmin1(mn, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    __shared__ double wmin[8];
+    __shared__ bool last;
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmin[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = fmin(b, wmin[w]);
+        partial[blockIdx.x] = b;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double b = 100000.0;
+        for (unsigned int k = 0; k < gridDim.x; k++) b = fmin(b, ((volatile double*)partial)[k]);
+        *dtmin = b;
+        *counter = 0u;
+    }
+}
+
+void launch_time_step_scratch(const Params& P, const double* q, const double* cfldl,
+                              long long ncell, double* dt, double* partial,
+                              unsigned int* counter, double* dtmin, int nblocks,
+                              cudaStream_t s) {
+    k_time_step_scratch<<<nblocks, 256, 0, s>>>(P, q, cfldl, ncell, dt, partial, counter, dtmin);
+}
+
 // ------------------------------------------------------------ port mass flux
 
 // One warp per type-6 ghost: sum of C1*U*DELY(*YCC) along the mesh line through the

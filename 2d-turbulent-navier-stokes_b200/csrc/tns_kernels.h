@@ -23,6 +23,10 @@ void launch_stage(const Params& P, const Mesh& M, const double* qin, const doubl
                   unsigned int* status, cudaStream_t s);
 void launch_dtmin(const Params& P, const Mesh& M, const double* q, double* partial,
                   unsigned int* counter, double* dtmin, cudaStream_t s);
+void launch_time_step_scratch(const Params& P, const double* q, const double* cfldl,
+                              long long ncell, double* dt, double* partial,
+                              unsigned int* counter, double* dtmin, int nblocks,
+                              cudaStream_t s);
 void launch_gport(const Params& P, const Mesh& M, const double* q, const int* ghosts, int nport,
                   double* gport, cudaStream_t s);
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,

@@ -15,13 +15,15 @@ LIB_PATH = os.path.join(HERE, "libtnsgpu.so")
 
 TNS_OK = 0
 ERRORS = {-1: "TNS_ERR_ARG", -2: "TNS_ERR_MESH", -3: "TNS_ERR_UNSUPPORTED",
-          -4: "TNS_ERR_CUDA", -5: "TNS_ERR_NONFINITE", -6: "TNS_ERR_STATE"}
+          -4: "TNS_ERR_CUDA", -5: "TNS_ERR_NONFINITE", -6: "TNS_ERR_STATE",
+          -7: "TNS_ERR_TOO_LARGE"}
+NOALLOC_MAX_CELLS = 256 * 4 * 8192
 
 # every symbol include/tnsgpu.h declares
 EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
            "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
-           "tns_last_error", "tns_destroy")
+           "tns_last_error", "tns_destroy", "tns_time_step_noalloc")
 
 
 class TnsMesh(C.Structure):
@@ -75,6 +77,7 @@ def load(path: str = LIB_PATH):
     L.tns_last_error.restype = C.c_char_p
     L.tns_destroy.argtypes = [vp]
     L.tns_destroy.restype = None
+    L.tns_time_step_noalloc.argtypes = [vp, vp, C.c_longlong, C.POINTER(TnsParams), vp, vp, vp]
     for n in EXPORTS:
         if n not in ("tns_launch_count", "tns_last_error", "tns_destroy"):
             getattr(L, n).restype = C.c_int

@@ -27,6 +27,7 @@ extern "C" {
 #define TNS_ERR_CUDA (-4)         /* CUDA runtime error */
 #define TNS_ERR_NONFINITE (-5)    /* state became NaN / Inf */
 #define TNS_ERR_STATE (-6)        /* call out of order (e.g. no state uploaded) */
+#define TNS_ERR_TOO_LARGE (-7)    /* problem exceeds a fixed-size buffer (tns_time_step_noalloc) */
 
 /* Mesh as COMPUTE_GEOMETRY holds it after reading grid.in and bc.in
  * (geometry.f90:25-52; solver_state.f90:113-125). */
@@ -113,6 +114,35 @@ int tns_kernel_times(tns_handle *h, int kernel, double *ms, long long *launches)
 long long tns_launch_count(tns_handle *h);
 
 const char *tns_last_error(tns_handle *h);
+
+/* Allocation-free time step.  No counterpart in the reference: it serves callers that
+ * cannot allocate device memory while they run the solver -- code inside a CUDA stream
+ * capture (cudaMalloc would break the capture), hosts whose device memory all comes
+ * from one preallocated pool or arena, and plugin hosts that forbid allocation on
+ * their time loop.  It computes, for a state already in device memory, the per-cell
+ * time step DT = CFL*DL/(|V| + sqrt(GAMA*RR*T)) and DTMIN = min(1e5, min DT) of
+ * turbnstwod.f90:97-108, exactly as the handle-based path does, without a handle.
+ *
+ *   d_q      device, [5][ncell] conservative state, component-major (C1 block, C2, ...)
+ *   d_cfldl  device, [ncell] CFL*DL per cell (DL = shortest cell edge, geometry.f90:70-74)
+ *   params   gama, amol and cfl are read (the others may be zero)
+ *   d_dt     device, [ncell] out: DT per cell (the LOCAL=1 step)
+ *   d_dtmin  device, one double out: DTMIN (the LOCAL=0 step)
+ *   stream   cudaStream_t as void* (NULL = the legacy default stream)
+ *
+ * Its reduction scratch is a fixed array inside the library (one partial minimum per
+ * block of TNS_NOALLOC_CELLS_PER_THREAD*256 cells, at most TNS_NOALLOC_MAX_BLOCKS
+ * blocks: 64 KiB), so ncell is limited to TNS_NOALLOC_MAX_CELLS; larger problems get
+ * TNS_ERR_TOO_LARGE.  It calls no cudaMalloc / cudaFree.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) and must therefore be made
+ * before any stream capture starts.  All calls share the one array, so calls that may
+ * overlap on the GPU (different streams without ordering) race; serialise them.  The
+ * call is asynchronous on `stream`. */
+#define TNS_NOALLOC_MAX_BLOCKS 8192
+#define TNS_NOALLOC_CELLS_PER_THREAD 4
+#define TNS_NOALLOC_MAX_CELLS (256LL * TNS_NOALLOC_CELLS_PER_THREAD * TNS_NOALLOC_MAX_BLOCKS)
+int tns_time_step_noalloc(const double *d_q, const double *d_cfldl, long long ncell,
+                          const tns_params *params, double *d_dt, double *d_dtmin, void *stream);
 void tns_destroy(tns_handle *h);
 
 #ifdef __cplusplus

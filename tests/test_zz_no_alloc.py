@@ -1,0 +1,89 @@
+"""The allocation-free time step (tns_time_step_noalloc) against the handle-based path.
+
+Callers that cannot allocate device memory while they run -- inside a CUDA stream
+capture, or with all device memory taken from a preallocated pool -- get the time
+step of turbnstwod.f90:97-108 from tns_time_step_noalloc, whose reduction scratch is a
+fixed array inside the library.  This test drives it through the C ABI with device
+buffers it allocates itself (it is only the checker), twice in a row, and compares
+DT and DTMIN with what tns_run computed for the same state (tns_debug_fetch).
+
+This file is collected last so a run that stops at the first failure has run every
+other test before it.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from tnsgpu import _lib, cases
+from tnsgpu.solver import Solver, make_params
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13  # the DT tolerance of the parity tests
+
+
+def _cfldl(mesh, cfl):
+    """CFL*DL per cell in cell-id order, DL = shortest edge (geometry.f90:70-74)."""
+    x, y = mesh.x, mesh.y
+    n = mesh.nod - 1
+    edges = []
+    for a, b in ((0, 1), (1, 2), (2, 3), (3, 0)):
+        dx = x[n[:, a]] - x[n[:, b]]
+        dy = y[n[:, a]] - y[n[:, b]]
+        edges.append(np.sqrt(dx * dx + dy * dy))
+    dl = np.minimum(np.minimum(np.minimum(edges[0], edges[1]), edges[2]), edges[3])
+    return cfl * dl
+
+
+def _noalloc(torch, q_host, cfldl_dev, params, stream):
+    L = _lib.load()
+    q = torch.from_numpy(np.ascontiguousarray(q_host)).cuda()
+    ncell = q_host.shape[1]
+    dt = torch.full((ncell,), math.nan, dtype=torch.float64, device="cuda")
+    dtmin = torch.full((1,), math.nan, dtype=torch.float64, device="cuda")
+    rc = L.tns_time_step_noalloc(q.data_ptr(), cfldl_dev.data_ptr(), ncell, C.byref(params),
+                                 dt.data_ptr(), dtmin.data_ptr(), stream)
+    assert rc == 0, _lib.ERRORS.get(rc, rc)
+    torch.cuda.synchronize()
+    return dt.cpu().numpy(), float(dtmin.cpu().numpy()[0])
+
+
+@pytest.mark.parametrize("local", [1, 0])
+def test_noalloc_time_step_matches_handle_path_on_two_calls(local):
+    import torch
+    mesh = cases.ramp_mesh(48, 20)
+    flow = cases.ramp_flow()
+    flow.local = local
+    c0, rinit = cases.noisy_restart_state(flow, mesh.neles)
+    params = make_params(flow, rinit)
+    cfldl = torch.from_numpy(_cfldl(mesh, flow.cfl)).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+
+    s = Solver(mesh, flow, rinit)
+    state = c0
+    for call in range(2):
+        # handle-based path: DT of the state an iteration starts from
+        s.upload(state)
+        s.run(1, 0)
+        ref = s.debug(2)[0]
+        dt, dtmin = _noalloc(torch, state, cfldl, params, stream)
+        if local:
+            assert np.max(np.abs(dt - ref) / ref) <= TOL, call
+            assert abs(dtmin - min(1.0e5, ref.min())) <= TOL * dtmin, call
+        else:
+            assert abs(dtmin - ref[0]) <= TOL * dtmin, call  # LOCAL=0 runs on DTMIN
+            assert abs(dtmin - dt.min()) <= TOL * dtmin, call
+        state = s.download()  # the next call starts from a different state
+    s.close()
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    import torch
+    L = _lib.load()
+    params = make_params(cases.ramp_flow(), 1e-6)
+    buf = torch.zeros(8, dtype=torch.float64, device="cuda")
+    p = buf.data_ptr()
+    rc = L.tns_time_step_noalloc(p, p, _lib.NOALLOC_MAX_CELLS + 1, C.byref(params), p, p, None)
+    assert rc == -7  # TNS_ERR_TOO_LARGE, nothing launched
+    assert L.tns_time_step_noalloc(None, p, 10, C.byref(params), p, p, None) == -1
