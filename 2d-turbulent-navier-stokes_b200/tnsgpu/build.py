@@ -11,6 +11,23 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
               "-Xcompiler", "-fPIC", "-shared"]
 
 
+MAINS = os.path.join(os.path.dirname(HERE), "mains")
+
+
+def build_mains() -> list:
+    """twodturb / axiturb: the main program with the RK4 loop on the GPU (g++, linked
+    against the in-tree libtnsgpu.so).  Both read IAXIS from flow.in; they differ only
+    in the default used when flow.in has 16 values."""
+    out = []
+    for name, iaxis in (("twodturb", 0), ("axiturb", 1)):
+        exe = os.path.join(MAINS, name)
+        subprocess.run(["g++", "-O2", "-std=c++17", f"-DTNS_DEFAULT_IAXIS={iaxis}",
+                        os.path.join(MAINS, "tnsmain.cpp"), "-o", exe, f"-L{HERE}", "-ltnsgpu",
+                        "-Wl,-rpath,$ORIGIN/../tnsgpu"], check=True)
+        out.append(exe)
+    return out
+
+
 def build_library(verbose: bool = False) -> str:
     out = os.path.join(HERE, "libtnsgpu.so")
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
