@@ -57,13 +57,22 @@ struct tns_handle {
     cudaStream_t own = nullptr, stream = nullptr;
     DevBuf<double> x, y, cfldl, gxc, gyc, ginj, gport, qa, qb, qc, d, vis, dt, dtmin, partial,
         primout;
+    // mixed FP32/FP64 path: FP64 state ping-pong (qa, qa2) and FP32 scratch
+    int precision = 0;
+    int cur = 0;  // mixed: which of qa / qa2 holds the state
+    DevBuf<double> qa2;
+    DevBuf<float> dqb, dqc, df, visf, dtf;
+    cudaGraphExec_t graph_mx[2] = {nullptr, nullptr};
+    // monitored iteration (CDIFF reduction in stage 4): FP64, mixed per parity
+    cudaGraphExec_t graph_mon = nullptr;
+    cudaGraphExec_t graph_mon_mx[2] = {nullptr, nullptr};
     DevBuf<int> gtype, grank, ports;
     DevBuf<unsigned int> counter, status;
     DevBuf<unsigned long long> cdiff;
     double* pinned = nullptr;  // 5*ncell staging
     bool have_state = false, have_run = false;
     cudaGraphExec_t graph = nullptr;
-    long long per_iter = 0;
+    long long per_iter = 0, per_iter_mon = 0;
     unsigned int* status_host = nullptr;  // pinned
     bool profile = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -85,6 +94,8 @@ struct tns_handle {
         return fail(TNS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     }
     size_t ncell() const { return (size_t)ni * nj; }
+    double* state() { return precision == 1 && cur ? qa2.p : qa.p; }
+    double* other_state() { return precision == 1 && !cur ? qa2.p : qa.p; }
 };
 
 namespace {
@@ -322,18 +333,30 @@ int upload_mesh(tns_handle* h) {
 int alloc_state(tns_handle* h) {
     const size_t nc = h->ncell();
     int rc;
-    if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qb.alloc(5 * nc), "cudaMalloc")) ||
-        (rc = h->cuda(h->qc.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->d.alloc(5 * nc), "cudaMalloc")) ||
-        (rc = h->cuda(h->vis.alloc(4 * nc), "cudaMalloc")) || (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc")) ||
-        (rc = h->cuda(h->dtmin.alloc(1), "cudaMalloc")) ||
+    if (h->precision == 1) {
+        if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qa2.alloc(5 * nc), "cudaMalloc")) ||
+            (rc = h->cuda(h->dqb.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->dqc.alloc(5 * nc), "cudaMalloc")) ||
+            (rc = h->cuda(h->df.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->visf.alloc(4 * nc), "cudaMalloc")) ||
+            (rc = h->cuda(h->dtf.alloc(nc), "cudaMalloc")))
+            return rc;
+        if ((rc = h->cuda(cudaMemset(h->dtf.p, 0, nc * 4), "cudaMemset")) ||
+            (rc = h->cuda(cudaMemset(h->visf.p, 0, 4 * nc * 4), "cudaMemset")))
+            return rc;
+    } else if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qb.alloc(5 * nc), "cudaMalloc")) ||
+               (rc = h->cuda(h->qc.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->d.alloc(5 * nc), "cudaMalloc")) ||
+               (rc = h->cuda(h->vis.alloc(4 * nc), "cudaMalloc")) || (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc"))) {
+        return rc;
+    }
+    if ((rc = h->cuda(h->dtmin.alloc(1), "cudaMalloc")) ||
         (rc = h->cuda(h->partial.alloc((size_t)tns::dtmin_blocks(h->M)), "cudaMalloc")) ||
         (rc = h->cuda(h->counter.alloc(1), "cudaMalloc")) || (rc = h->cuda(h->status.alloc(1), "cudaMalloc")) ||
         (rc = h->cuda(h->cdiff.alloc(5), "cudaMalloc")))
         return rc;
     if ((rc = h->cuda(cudaMemset(h->counter.p, 0, 4), "cudaMemset")) ||
-        (rc = h->cuda(cudaMemset(h->status.p, 0, 4), "cudaMemset")) ||
-        (rc = h->cuda(cudaMemset(h->dt.p, 0, nc * 8), "cudaMemset")) ||
-        (rc = h->cuda(cudaMemset(h->vis.p, 0, 4 * nc * 8), "cudaMemset")))
+        (rc = h->cuda(cudaMemset(h->status.p, 0, 4), "cudaMemset")))
+        return rc;
+    if (h->precision == 0 && ((rc = h->cuda(cudaMemset(h->dt.p, 0, nc * 8), "cudaMemset")) ||
+                              (rc = h->cuda(cudaMemset(h->vis.p, 0, 4 * nc * 8), "cudaMemset"))))
         return rc;
     if ((rc = h->cuda(cudaMallocHost((void**)&h->status_host, sizeof(unsigned int)), "cudaMallocHost")))
         return rc;
@@ -356,9 +379,35 @@ void launch(tns_handle* h, int kid, F&& f) {
     }
 }
 
+// One mixed-precision RK4 iteration from state buffer `in` to `out` (FP32 increments
+// dQ_B, dQ_C between the stages).  The previous state survives in `in`, so the last
+// stage's input (in + dQ_B) can be reconstructed for tns_download_primitives.
+void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) {
+    const Params& P = h->P;
+    const Mesh& M = h->M;
+    cudaStream_t s = h->stream;
+    const int np = (int)h->port_ghosts.size();
+    if (!P.local)
+        launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
+    launch(h, K_DISS, [&] { tns::launch_dissipation_mx2(P, M, A, h->df.p, h->dtf.p, h->dtmin.p, s); });
+    static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
+    const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
+    float* out[4] = {h->dqb.p, h->dqc.p, h->dqb.p, nullptr};
+    if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
+    for (int st = 0; st < 4; st++) {
+        if (np) launch(h, K_GPORT, [&] { tns::launch_gport_mx(P, M, A, in[st], h->ports.p, np, h->gport.p, s); });
+        if (st == 0) launch(h, K_VISC, [&] { tns::launch_viscous_mx(P, M, A, h->visf.p, s); });
+        launch(h, K_STAGE, [&] {
+            tns::launch_stage_mx(P, M, A, in[st], out[st], st == 3 ? Aout : nullptr, h->df.p, h->visf.p,
+                                 h->dtf.p, h->dtmin.p, alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
+                                 st == 3 ? h->status.p : nullptr, s);
+        });
+    }
+}
+
 // One RK4 iteration (turbnstwod.f90:97-168).  Buffers: A = state, B/C = stage scratch;
 // stage 4 writes A in place (each cell reads only its own COLD there).
-void enqueue_iteration(tns_handle* h, bool monitor) {
+void enqueue_iteration_f64(tns_handle* h, bool monitor) {
     const Params& P = h->P;
     const Mesh& M = h->M;
     cudaStream_t s = h->stream;
@@ -393,7 +442,9 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
     if (!mesh || !params) return TNS_ERR_ARG;
     tns_handle* h = new tns_handle();
     *out = h;
-    if (params->precision != 0) return h->fail(TNS_ERR_ARG, "precision mode %d is not available", params->precision);
+    if (params->precision != 0 && params->precision != 1)
+        return h->fail(TNS_ERR_ARG, "precision mode %d is not available (0 = FP64, 1 = mixed)", params->precision);
+    h->precision = params->precision;
     if (!(params->gama > 1.0) || !(params->amol > 0.0) || !(params->cfl > 0.0))
         return h->fail(TNS_ERR_ARG, "GAMA must exceed 1, AMOL and CFL must be positive");
     h->P = make_params(*params);
@@ -403,6 +454,7 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
     if ((rc = h->cuda(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
     h->stream = h->own;
     if ((rc = h->cuda(tns::configure_kernels(), "cudaFuncSetAttribute"))) return rc;
+    if ((rc = h->cuda(tns::configure_kernels_mx(), "cudaFuncSetAttribute"))) return rc;
     if ((rc = upload_mesh(h))) return rc;
     if ((rc = alloc_state(h))) return rc;
     cudaEventCreate(&h->ev[0]);
@@ -432,7 +484,7 @@ int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const do
     if (direct) {
         // page-locked caller arrays: one DMA per component, no staging copy
         for (int m = 0; m < 5; m++)
-            if ((rc = h->cuda(cudaMemcpyAsync(h->qa.p + m * nc, src[m], nc * 8, cudaMemcpyHostToDevice,
+            if ((rc = h->cuda(cudaMemcpyAsync(h->state() + m * nc, src[m], nc * 8, cudaMemcpyHostToDevice,
                                               h->stream), "cudaMemcpyAsync")))
                 return rc;
     } else {
@@ -442,7 +494,7 @@ int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const do
             else
                 for (size_t k = 0; k < nc; k++) dst[k] = src[m][h->cell_of[k]];
         }
-        if ((rc = h->cuda(cudaMemcpyAsync(h->qa.p, h->pinned, 5 * nc * 8, cudaMemcpyHostToDevice, h->stream),
+        if ((rc = h->cuda(cudaMemcpyAsync(h->state(), h->pinned, 5 * nc * 8, cudaMemcpyHostToDevice, h->stream),
                           "cudaMemcpyAsync")))
             return rc;
     }
@@ -454,21 +506,69 @@ int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const do
 
 namespace {
 
-// Captures one unmonitored iteration as a CUDA graph (once per handle).
-int ensure_graph(tns_handle* h) {
-    if (h->graph) return TNS_OK;
+// Enqueues one iteration of the handle's precision mode and advances the state buffer.
+void enqueue_iteration(tns_handle* h, bool monitor) {
+    if (h->precision == 1) {
+        enqueue_iteration_mx(h, monitor, h->state(), h->other_state());
+        h->cur ^= 1;
+    } else {
+        enqueue_iteration_f64(h, monitor);
+    }
+}
+
+int capture(tns_handle* h, cudaGraphExec_t* exec, bool mixed, int parity, bool monitor = false) {
     cudaGraph_t g;
     int rc;
     if ((rc = h->cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture")))
         return rc;
     const long long before = h->launches;
-    enqueue_iteration(h, false);
+    if (mixed) {
+        double* A = parity ? h->qa2.p : h->qa.p;
+        double* B = parity ? h->qa.p : h->qa2.p;
+        enqueue_iteration_mx(h, monitor, A, B);
+    } else {
+        enqueue_iteration_f64(h, monitor);
+    }
     h->per_iter = h->launches - before;
     h->launches = before;
     if ((rc = h->cuda(cudaStreamEndCapture(h->stream, &g), "capture"))) return rc;
-    rc = h->cuda(cudaGraphInstantiate(&h->graph, g, 0), "cudaGraphInstantiate");
+    rc = h->cuda(cudaGraphInstantiate(exec, g, 0), "cudaGraphInstantiate");
     cudaGraphDestroy(g);
     return rc;
+}
+
+// Captures one unmonitored iteration as a CUDA graph (once per handle; the mixed path
+// needs one per state-buffer parity).
+int ensure_graph(tns_handle* h) {
+    int rc;
+    if (h->precision == 1) {
+        for (int par = 0; par < 2; par++)
+            if (!h->graph_mx[par] && (rc = capture(h, &h->graph_mx[par], true, par))) return rc;
+        return TNS_OK;
+    }
+    if (h->graph) return TNS_OK;
+    return capture(h, &h->graph, false, 0);
+}
+
+// One monitored iteration: a captured graph (memset of the CDIFF slots + the iteration),
+// or direct launches when per-kernel profiling is on.
+int enqueue_monitored(tns_handle* h) {
+    if (h->profile) {
+        enqueue_iteration(h, true);
+        return TNS_OK;
+    }
+    int rc;
+    cudaGraphExec_t* g = h->precision == 1 ? &h->graph_mon_mx[h->cur] : &h->graph_mon;
+    if (!*g) {
+        const long long per = h->per_iter;
+        if ((rc = capture(h, g, h->precision == 1, h->cur, true))) return rc;
+        h->per_iter_mon = h->per_iter;
+        h->per_iter = per;
+    }
+    if ((rc = h->cuda(cudaGraphLaunch(*g, h->stream), "cudaGraphLaunch"))) return rc;
+    if (h->precision == 1) h->cur ^= 1;
+    h->launches += h->per_iter_mon;
+    return TNS_OK;
 }
 
 int enqueue_plain(tns_handle* h, int niter) {
@@ -479,7 +579,9 @@ int enqueue_plain(tns_handle* h, int niter) {
     }
     if ((rc = ensure_graph(h))) return rc;
     for (int it = 0; it < niter; it++) {
-        if ((rc = h->cuda(cudaGraphLaunch(h->graph, h->stream), "cudaGraphLaunch"))) return rc;
+        cudaGraphExec_t g = h->precision == 1 ? h->graph_mx[h->cur] : h->graph;
+        if ((rc = h->cuda(cudaGraphLaunch(g, h->stream), "cudaGraphLaunch"))) return rc;
+        if (h->precision == 1) h->cur ^= 1;
         h->launches += h->per_iter;
     }
     return TNS_OK;
@@ -529,7 +631,7 @@ int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int 
             it = next;
             if (it > niter) break;
         }
-        enqueue_iteration(h, true);  // iteration `it` is monitored
+        if ((rc = enqueue_monitored(h))) return rc;  // iteration `it` is monitored
         {
             unsigned long long bits[5];
             if ((rc = h->cuda(cudaMemcpyAsync(bits, h->cdiff.p, sizeof bits, cudaMemcpyDeviceToHost, h->stream),
@@ -557,7 +659,7 @@ int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double
     if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
     if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_download_state: no state");
     const size_t nc = h->ncell();
-    int rc = h->cuda(cudaMemcpyAsync(h->pinned, h->qa.p, 5 * nc * 8, cudaMemcpyDeviceToHost, h->stream),
+    int rc = h->cuda(cudaMemcpyAsync(h->pinned, h->state(), 5 * nc * 8, cudaMemcpyDeviceToHost, h->stream),
                      "cudaMemcpyAsync");
     if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     double* dst[5] = {c1, c2, c3, c4, c5};
@@ -577,9 +679,15 @@ int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, doub
     int rc;
     if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
     const int np = (int)h->port_ghosts.size();
-    // stage 4 read B: recompute its primitives and ghost states from B
-    if (np) tns::launch_gport(h->P, h->M, h->qb.p, h->ports.p, np, h->gport.p, h->stream);
-    tns::launch_prim_out(h->P, h->M, h->qb.p, h->primout.p, h->stream);
+    if (h->precision == 1) {
+        // stage 4 read (previous state + dQ_B)
+        if (np) tns::launch_gport_mx(h->P, h->M, h->other_state(), h->dqb.p, h->ports.p, np, h->gport.p, h->stream);
+        tns::launch_prim_out_mx(h->P, h->M, h->other_state(), h->dqb.p, h->primout.p, h->stream);
+    } else {
+        // stage 4 read B: recompute its primitives and ghost states from B
+        if (np) tns::launch_gport(h->P, h->M, h->qb.p, h->ports.p, np, h->gport.p, h->stream);
+        tns::launch_prim_out(h->P, h->M, h->qb.p, h->primout.p, h->stream);
+    }
     std::vector<double> hb(4 * nt);
     rc = h->cuda(cudaMemcpyAsync(hb.data(), h->primout.p, 4 * nt * 8, cudaMemcpyDeviceToHost, h->stream),
                  "cudaMemcpyAsync");
@@ -600,7 +708,14 @@ int tns_debug_fetch(tns_handle* h, int which, double* out) {
     const int cnt = which == 0 ? 5 : which == 1 ? 4 : 1;
     const double* src = which == 0 ? h->d.p : which == 1 ? h->vis.p : h->dt.p;
     std::vector<double> hb(cnt * nc);
-    if (which == 2 && !h->P.local) {
+    if (h->precision == 1 && !(which == 2 && !h->P.local)) {
+        const float* fs = which == 0 ? h->df.p : which == 1 ? h->visf.p : h->dtf.p;
+        std::vector<float> fb(cnt * nc);
+        int rc = h->cuda(cudaMemcpyAsync(fb.data(), fs, cnt * nc * 4, cudaMemcpyDeviceToHost, h->stream),
+                         "cudaMemcpyAsync");
+        if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+        for (size_t k = 0; k < hb.size(); k++) hb[k] = fb[k];
+    } else if (which == 2 && !h->P.local) {
         double dm = 0;
         int rc = h->cuda(cudaMemcpy(&dm, h->dtmin.p, 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
         if (rc) return rc;
@@ -699,6 +814,13 @@ void tns_destroy(tns_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    for (auto g : h->graph_mx)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto g : h->graph_mon_mx)
+        if (g) cudaGraphExecDestroy(g);
+    if (h->graph_mon) cudaGraphExecDestroy(h->graph_mon);
+    h->qa2.release(); h->dqb.release(); h->dqc.release(); h->df.release(); h->visf.release();
+    h->dtf.release();
     for (auto* b : {&h->x, &h->y, &h->cfldl, &h->gxc, &h->gyc, &h->ginj, &h->gport, &h->qa, &h->qb,
                     &h->qc, &h->d, &h->vis, &h->dt, &h->dtmin, &h->partial, &h->primout})
         b->release();

@@ -13,84 +13,9 @@
 // from the parent and the parent's opposite neighbour, both already in the tile.
 #include "tns_device.cuh"
 #include "tns_kernels.h"
+#include "tns_tile.cuh"
 
 namespace tns {
-
-#ifndef TNS_TI
-#define TNS_TI 8
-#endif
-#ifndef TNS_STAGE_MINB
-#define TNS_STAGE_MINB 3
-#endif
-#ifndef TNS_VISC_MINB
-#define TNS_VISC_MINB 1
-#endif
-constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
-constexpr int TI = TNS_TI;  // tile extent along i
-constexpr int NTHREADS = TJ * TI;
-
-// ------------------------------------------------------------ shared helpers
-
-// Halo-1 slot grid (TI+2) x (TJ+2), node grid (TI+3) x (TJ+3) (nodes of every halo cell).
-constexpr int SW = TJ + 2;
-constexpr int NSLOT = (TI + 2) * SW;
-constexpr int NW = TJ + 3;
-constexpr int NNODE = (TI + 3) * NW;
-constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
-constexpr int NAVG = (TI + 1) * AW;
-
-__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny) {
-    const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int s = tid; s < NNODE; s += NTHREADS) {
-        const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
-        if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
-            const size_t n = (size_t)a * (M.nj + 1) + b;
-            snx[s] = M.x[n];
-            sny[s] = M.y[n];
-        }
-    }
-}
-
-__device__ __forceinline__ void cell_prim(const Params& P, const double* __restrict__ q, size_t ncell,
-                                          size_t c, Prim& p) {
-    primitive(P, q[c], q[ncell + c], q[2 * ncell + c], q[3 * ncell + c], q[4 * ncell + c], p);
-}
-
-// Classifies halo position (i, j): 0 = cell, 1..4 = ghost on that side, -1 = unused.
-__device__ __forceinline__ int classify(const Mesh& M, int i, int j, int& along) {
-    const bool in_i = i >= 0 && i < M.ni, in_j = j >= 0 && j < M.nj;
-    if (in_i && in_j) return 0;
-    if (in_i && j == -1) { along = i; return 1; }
-    if (in_j && i == M.ni) { along = j; return 2; }
-    if (in_i && j == M.nj) { along = i; return 3; }
-    if (in_j && i == -1) { along = j; return 4; }
-    return -1;
-}
-
-// BC state of the ghost on `side` at `along`, from the parent and the parent's opposite
-// neighbour read straight from the state array (bit-identical to their PRIMITIVE_VARS).
-__device__ void ghost_state(const Params& P, const Mesh& M, const double* __restrict__ q,
-                            size_t ncell, int side, int along, Prim& gh) {
-    int ip, jp, io, jo;
-    if (side == 1) { ip = along; jp = 0; io = along; jo = 1; }
-    else if (side == 2) { ip = M.ni - 1; jp = along; io = M.ni - 2; jo = along; }
-    else if (side == 3) { ip = along; jp = M.nj - 1; io = along; jo = M.nj - 2; }
-    else { ip = 0; jp = along; io = 1; jo = along; }
-    const int g = M.ghost_index(side, along);
-    const int type = M.gtype[g];
-    Prim par, opp;
-    cell_prim(P, q, ncell, (size_t)ip * M.nj + jp, par);
-    if (type == 3) cell_prim(P, q, ncell, (size_t)io * M.nj + jo, opp);
-    else opp = par;
-    const size_t n1 = (size_t)ip * (M.nj + 1) + jp;
-    const double X[4] = {M.x[n1], M.x[n1 + M.nj + 1], M.x[n1 + M.nj + 2], M.x[n1 + 1]};
-    const double Y[4] = {M.y[n1], M.y[n1 + M.nj + 1], M.y[n1 + M.nj + 2], M.y[n1 + 1]};
-    double psx = 0.0, psy = 0.0;
-    if (type == 6) face_vector(P.iaxis, side, X, Y, psx, psy);
-    const double ycc_p = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
-    boundary_ghost(P, type, par, opp, psx, psy, M.gyc[g], ycc_p, type == 6 ? M.gport[g] : 0.0,
-                   M.ginj[g], gh);
-}
 
 // ------------------------------------------------------------------ stage kernel
 
@@ -426,10 +351,11 @@ size_t diss_smem_bytes() {
     return sizeof(double) * ((size_t)NDF * NDSLOT + (size_t)NRF * NRSLOT + 2 * NNODE);
 }
 
+template <class OutT>
 struct DissArgs {
     const double* q;     // Q_old [5][ncell]
-    double* d;           // out: D [5][ncell]
-    double* dt;          // out: DT per cell (LOCAL=1)
+    OutT* d;             // out: D [5][ncell] (FP64, or FP32 on the mixed path)
+    OutT* dt;            // out: DT per cell (LOCAL=1)
     const double* dtmin; // DTMIN (LOCAL=0)
 };
 
@@ -445,7 +371,8 @@ __device__ __forceinline__ double local_dt(const Params& P, double c1, double c2
     return cfldl / (fabs(VEL) + sqrt(P.gamrr * T));
 }
 
-__global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, DissArgs A) {
+template <class OutT>
+__global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, DissArgs<OutT> A) {
     extern __shared__ double smem[];
     double* sd = smem;                  // NDF x NDSLOT
     double* sr = sd + NDF * NDSLOT;     // NRF x NRSLOT
@@ -519,7 +446,7 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, Diss
         if (P.local) {
             DT = local_dt(P, sd[DC0 * NDSLOT + d], sd[DC1 * NDSLOT + d], sd[DC2 * NDSLOT + d],
                           sd[DC3 * NDSLOT + d], M.cfldl[c]);
-            if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) A.dt[c] = DT;
+            if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) A.dt[c] = (OutT)DT;
         } else {
             DT = *A.dtmin;
         }
@@ -570,7 +497,7 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, Diss
             D2 = D2 + a2 * (Cm[dn[k]] - CI);
             D4 = D4 + a4 * (Qm[rn[k]] - D2I);
         }
-        A.d[m * ncell + cell] = D2 - D4;
+        A.d[m * ncell + cell] = (OutT)(D2 - D4);
     }
 }
 
@@ -733,14 +660,23 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(k_viscous, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)visc_smem_bytes());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_dissipation, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_dissipation<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diss_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_dissipation<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)diss_smem_bytes());
 }
 
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,
                         const double* dtmin, cudaStream_t s) {
-    DissArgs A{q, d, dt, dtmin};
-    k_dissipation<<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
+    DissArgs<double> A{q, d, dt, dtmin};
+    k_dissipation<double><<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
+}
+
+void launch_dissipation_mx(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
+                           const double* dtmin, cudaStream_t s) {
+    DissArgs<float> A{q, d, dt, dtmin};
+    k_dissipation<float><<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
 }
 
 void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis, cudaStream_t s) {

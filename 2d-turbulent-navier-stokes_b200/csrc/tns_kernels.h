@@ -32,4 +32,20 @@ void launch_gport(const Params& P, const Mesh& M, const double* q, const int* gh
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,
                      cudaStream_t s);
 
+// mixed FP32/FP64 path (tns_kernels_mx.cu)
+cudaError_t configure_kernels_mx();
+void launch_dissipation_mx(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
+                           const double* dtmin, cudaStream_t s);
+void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
+                            const double* dtmin, cudaStream_t s);
+void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* vis, cudaStream_t s);
+void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,
+                     float* dqout, double* qout, const float* d, const float* vis, const float* dt,
+                     const double* dtmin, double alpha, unsigned long long* cdiff,
+                     unsigned int* status, cudaStream_t s);
+void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
+                     const int* ghosts, int nport, double* gport, cudaStream_t s);
+void launch_prim_out_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
+                        double* out, cudaStream_t s);
+
 }  // namespace tns

@@ -1,0 +1,707 @@
+// tns_kernels_mx.cu -- mixed FP32/FP64 kernels of one RK4 iteration.
+//
+// What stays FP64: the state Q (and every stage state COLD + dQ), primitive variables,
+// geometry (node coordinates, surface vectors, volumes, centroids), every difference of
+// nearly equal quantities (gradient stencils, node averages), the part of the flux
+// residual that cancels (a per-tile reference flux times the closed-contour sum of S),
+// the state accumulation and the residual monitor.  What is FP32: the stage increments
+// dQ, the dissipation D, the viscous flux VIS and DT as stored, the flux deviations from
+// the tile reference, and the flux / source / viscous arithmetic with its
+// transcendentals (T**0.6, tanh, sqrt).
+//
+// Storing flux deviations instead of fluxes keeps the FP32 rounding of the residual
+// proportional to the flow's variation inside a tile rather than to the pressure and
+// total-enthalpy levels, so the iteration can still converge by RTRED=1e-5 and more.
+#include "tns_device.cuh"
+#include "tns_kernels.h"
+#include "tns_tile.cuh"
+
+namespace tns {
+
+__device__ __forceinline__ float pow06f(float T) { return __expf(0.6f * __logf(T)); }
+
+// tanh for the FP32 path: the Maclaurin series x - x^3/3 + 2x^5/15 - 17x^7/315 +
+// 62x^9/2835 - 1382x^11/155925 + 21844x^13/6081075 for |x| < 1/4 (the first omitted
+// term is below 2e-12 relative there), and the identity tanh|x| = 1 - 2/(exp(2|x|)+1)
+// above, where its cancellation costs at most ~5e-7 relative.
+__device__ __forceinline__ float tanh_f32(float x) {
+    const float ax = fabsf(x);
+    if (ax < 0.25f) {
+        const float x2 = x * x;
+        return x * (1.0f + x2 * (-1.0f / 3.0f + x2 * (2.0f / 15.0f + x2 * (-17.0f / 315.0f +
+                    x2 * (62.0f / 2835.0f + x2 * (-1382.0f / 155925.0f + x2 * (21844.0f / 6081075.0f)))))));
+    }
+    const float r = 1.0f - __fdividef(2.0f, __expf(2.0f * ax) + 1.0f);
+    return copysignf(r, x);
+}
+
+// ------------------------------------------------------------------ stage kernel
+
+struct StageSmemMx {
+    float2 fg[5][NSLOT];   // (F_m - Fref_m, G_m - Gref_m)
+    double2 uv[NSLOT];     // (U, V)
+    double2 rq[NSLOT];     // (C5/C1, |V|)
+    double2 xy[NSLOT];     // centroid
+    double p[NSLOT];       // pressure (FP64: the axisymmetric radial balance cancels)
+    float2 tr[NSLOT];      // (T, RHO)
+    double fref[5], gref[5];
+    double nx[NNODE], ny[NNODE];
+};
+
+size_t stage_mx_smem_bytes() { return sizeof(StageSmemMx); }
+
+struct StageArgsMx {
+    const double* cold;   // state at the start of the iteration [5][ncell]
+    const float* dqin;    // stage input increment (null in stage 1)
+    float* dqout;         // stage output increment (stages 1-3)
+    double* qout;         // new state (stage 4) [5][ncell]
+    const float* d;       // dissipation [5][ncell]
+    const float* vis;     // viscous flux [4][ncell]
+    const float* dt;      // per-cell DT (LOCAL=1)
+    const double* dtmin;  // DTMIN (LOCAL=0)
+    float alpha;
+    unsigned long long* cdiff;
+    unsigned int* status;
+};
+
+__device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p) {
+#pragma unroll
+    for (int m = 0; m < 5; m++)
+        S.fg[m][s] = make_float2((float)(p.f[m] - S.fref[m]), (float)(p.g[m] - S.gref[m]));
+    S.uv[s] = make_double2(p.u, p.v);
+    S.rq[s] = make_double2(p.ri, p.qm);
+    S.p[s] = p.p;
+    S.tr[s] = make_float2((float)p.t, (float)p.rho);
+}
+
+#ifndef TNS_STAGE_MX_MINB
+#define TNS_STAGE_MX_MINB 4
+#endif
+#ifndef TNS_VISC_MX_MINB
+#define TNS_VISC_MX_MINB 3
+#endif
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmemMx& S = *reinterpret_cast<StageSmemMx*>(smem_raw);
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const StateMixed st{A.cold, A.dqin, ncell};
+    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    if (tid == 0) {
+        // tile reference flux: the first cell of the tile
+        Prim r;
+        cell_prim(P, st, (size_t)i0 * M.nj + j0, r);
+#pragma unroll
+        for (int m = 0; m < 5; m++) { S.fref[m] = r.f[m]; S.gref[m] = r.g[m]; }
+    }
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    __syncthreads();
+    for (int s = tid; s < NSLOT; s += NTHREADS) {
+        const int li = s / SW, lj = s % SW;
+        int along = 0;
+        const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
+        if (kind < 0) continue;
+        Prim p;
+        if (kind == 0) {
+            cell_prim(P, st, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
+            const int n1 = li * NW + lj;
+            S.xy[s] = make_double2((S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25,
+                                   (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25);
+        } else {
+            ghost_state(P, M, st, kind, along, p);
+            const int g = M.ghost_index(kind, along);
+            S.xy[s] = make_double2(M.gxc[g], M.gyc[g]);
+        }
+        put_slot_mx(S, s, p);
+    }
+    __syncthreads();
+
+    const int tj = threadIdx.x, ti = threadIdx.y;
+    const int i = i0 + ti, j = j0 + tj;
+    const bool valid = i < M.ni && j < M.nj;
+    double dv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+        const size_t cell = (size_t)i * M.nj + j;
+        const int c = (ti + 1) * SW + (tj + 1);
+        const int nb[4] = {c - 1, c + SW, c + 1, c - SW};
+        const int n1 = (ti + 1) * NW + (tj + 1);
+        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
+        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
+        double SX[4], SY[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) face_vector(P.iaxis, k + 1, X, Y, SX[k], SY[k]);
+        const double2 xyc = S.xy[c];
+        const double VOL = cell_volume(P.iaxis, X, Y, xyc.y);
+        const double sumx = SX[0] + SX[1] + SX[2] + SX[3], sumy = SY[0] + SY[1] + SY[2] + SY[3];
+        float sx[4], sy[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) { sx[k] = (float)SX[k]; sy[k] = (float)SY[k]; }
+
+        // residual: FP32 over flux deviations + FP64 reference part (residual.f90:23-62)
+        float R[5];
+        double R64[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            const float2 I = S.fg[m][c], a = S.fg[m][nb[0]], b = S.fg[m][nb[1]], e = S.fg[m][nb[2]],
+                         d = S.fg[m][nb[3]];
+            R[m] = 0.5f * ((I.x + a.x) * sx[0] + (I.y + a.y) * sy[0] + (I.x + b.x) * sx[1] +
+                           (I.y + b.y) * sy[1] + (I.x + e.x) * sx[2] + (I.y + e.y) * sy[2] +
+                           (I.x + d.x) * sx[3] + (I.y + d.y) * sy[3]);
+            R64[m] = S.fref[m] * sumx + S.gref[m] * sumy;
+        }
+
+        // source terms (source_terms.f90:258-320): FP64 stencil differences, FP32 rest
+        {
+            const int a = nb[0], b = nb[1], cc = nb[2], d = nb[3];
+            const double2 xa = S.xy[a], xb = S.xy[b], xc = S.xy[cc], xd = S.xy[d];
+            const double ybd = xb.y - xd.y, yac = xa.y - xc.y, xbd = xb.x - xd.x, xac = xa.x - xc.x;
+            const float idnr = (float)(1.0 / (xac * ybd - xbd * yac));
+            const float fybd = (float)ybd, fyac = (float)yac, fxbd = (float)xbd, fxac = (float)xac;
+            const double2 ua = S.uv[a], ub = S.uv[b], uc = S.uv[cc], ud = S.uv[d];
+            const double2 ra = S.rq[a], rb = S.rq[b], rc = S.rq[cc], rd = S.rq[d];
+            const float dqac = (float)(ra.y - rc.y), dqbd = (float)(rb.y - rd.y);
+            const float drac = (float)(ra.x - rc.x), drbd = (float)(rb.x - rd.x);
+            const float duac = (float)(ua.x - uc.x), dubd = (float)(ub.x - ud.x);
+            const float dvac = (float)(ua.y - uc.y), dvbd = (float)(ub.y - ud.y);
+            const float DQX = (dqac * fybd - dqbd * fyac) * idnr;
+            const float DRX = (drac * fybd - drbd * fyac) * idnr;
+            const float DUX = (duac * fybd - dubd * fyac) * idnr;
+            const float DVX = (dvac * fybd - dvbd * fyac) * idnr;
+            const float DQY = (-dqac * fxbd + dqbd * fxac) * idnr;
+            const float DRY = (-drac * fxbd + drbd * fxac) * idnr;
+            const float DUY = (-duac * fxbd + dubd * fxac) * idnr;
+            const float DVY = (-dvac * fxbd + dvbd * fxac) * idnr;
+            const float2 trc = S.tr[c];
+            const float RHO = trc.y, RI = (float)S.rq[c].x, T = trc.x;
+            const float AMU = (float)P.suth_amol * pow06f(T);
+            const float CHI = RHO * RI / ((float)CMU * AMU);
+            const float chi2 = CHI * CHI;
+            const float FMU = tanh_f32((float)ALPHA_T * chi2) / tanh_f32((float)BETA_T * chi2);
+            const float FR2 = tanh_f32(sqrtf(CHI)) / tanh_f32(CHI * (float)P.fr2k);
+            const float AMUT = FMU * RHO * RI;
+            const float PHI = DQX * DRX + DQY * DRY;
+            const float DEE = PHI > 0.0f ? DRX * DRX + DRY * DRY : 0.0f;
+            const float DIV23 = (float)P.div23;
+            float pw = AMUT / fmaxf(AMUT, (float)AMU_THRESH * AMU);
+            {
+                float r = 1.0f, bb = pw;
+                int mm = P.npseudo < 0 ? -P.npseudo : P.npseudo;
+                while (mm) {
+                    if (mm & 1) r *= bb;
+                    mm >>= 1;
+                    if (mm) bb *= bb;
+                }
+                pw = P.npseudo < 0 ? 1.0f / r : r;
+            }
+            float PK, src5;
+            const float volf = (float)VOL;
+            if (P.iaxis == 1) {
+                const double ycc = xyc.y;
+                const float VBYY = (ycc < YAXIS_THRESH) ? DVY : (float)(S.uv[c].y / ycc);
+                const float DIVVEL = DUX + DVY + VBYY;
+                PK = AMUT / RHO *
+                     (DUX * DUX + DVY * DVY + VBYY * VBYY + DUX * DUX + DVY * DVY + VBYY * VBYY +
+                      (DUY + DVX) * (DUY + DVX) - DIV23 * DIVVEL * DIVVEL);
+                PK = fmaxf(PK, 0.0f);
+                src5 = (RHO * ((float)CONST1 - (float)CONST2 * FR2) * sqrtf(RI * PK) -
+                        RHO * (float)CONST3 * DEE) * pw;
+                const float TTT = (AMU + AMUT) * (VBYY + VBYY - DIV23 * DIVVEL);
+                // SOURCE3 = (P - TTT)/YCC: the P part cancels the reference flux in FP64
+                R64[2] -= VOL * (S.p[c] / ycc);
+                R[2] += volf * (TTT / (float)ycc);
+            } else {
+                const float DIVVEL = DUX + DVY;
+                PK = AMUT / RHO *
+                     (DUX * DUX + DVY * DVY + DUX * DUX + DVY * DVY + (DUY + DVX) * (DUY + DVX) -
+                      DIV23 * DIVVEL * DIVVEL);
+                PK = fmaxf(PK, 0.0f);
+                src5 = (RHO * ((float)CONST1 - (float)CONST2 * FR2) * sqrtf(RI * PK) -
+                        RHO * (float)CONST3 * DEE) * pw;
+            }
+            R[4] -= volf * src5;
+        }
+#pragma unroll
+        for (int m = 0; m < 5; m++) R[m] += (float)R64[m];
+
+        // update (residual.f90:67-83) as an FP32 increment on the FP64 state
+        const float DT = P.local ? A.dt[cell] : (float)*A.dtmin;
+        const float dtv = -A.alpha * (DT / (float)VOL);
+        float inc[5];
+        inc[0] = dtv * (R[0] - A.d[cell]);
+        inc[1] = dtv * (R[1] - A.vis[cell] - A.d[ncell + cell]);
+        inc[2] = dtv * (R[2] - A.vis[ncell + cell] - A.d[2 * ncell + cell]);
+        inc[3] = dtv * (R[3] - A.vis[2 * ncell + cell] - A.d[3 * ncell + cell]);
+        inc[4] = dtv * (float)CFLTURB * (R[4] - A.vis[3 * ncell + cell] - A.d[4 * ncell + cell]);
+        double Co[5], Cn[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            Co[m] = A.cold[m * ncell + cell];
+            Cn[m] = Co[m] + (double)inc[m];
+        }
+        // nu~ floor C5 = C1*max(RTOL, C5/C1), applied only where it binds
+        if (Cn[4] < P.rtol * Cn[0]) {
+            Cn[4] = P.rtol * Cn[0];
+            inc[4] = (float)(Cn[4] - Co[4]);
+        }
+        if (A.qout) {
+#pragma unroll
+            for (int m = 0; m < 5; m++) A.qout[m * ncell + cell] = Cn[m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < 5; m++) A.dqout[m * ncell + cell] = inc[m];
+        }
+        if (A.status) {
+            bool bad = false;
+#pragma unroll
+            for (int m = 0; m < 5; m++) bad |= !isfinite(Cn[m]);
+            if (bad) atomicOr(A.status, 1u);
+        }
+#pragma unroll
+        for (int m = 0; m < 5; m++) dv[m] = fabs(Co[m] - Cn[m]);
+    }
+    if (A.cdiff) {
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            double v = dv[m];
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(&A.cdiff[m], (unsigned long long)__double_as_longlong(v));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- viscous kernel
+
+constexpr int NIFM = (TI + 1) * TJ;
+constexpr int NJFM = TI * (TJ + 1);
+
+struct ViscSmemMx {
+    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT], xc[NSLOT], yc[NSLOT];
+    double au[NAVG], av[NAVG], at[NAVG], arho[NAVG], ar[NAVG];
+    float fi[4][NIFM], fj[4][NJFM];
+    double nx[NNODE], ny[NNODE];
+};
+
+size_t visc_mx_smem_bytes() { return sizeof(ViscSmemMx); }
+
+// One face of viscous.f90:130-217: FP64 geometry and stencil differences, FP32 rest.
+__device__ __forceinline__ void face_flux_mx(const Params& P, const ViscSmemMx& S, int sa, int sc,
+                                             int ab, int ad, int nb, int nd, float out[4]) {
+    const double xb = S.nx[nb], yb = S.ny[nb], xd = S.nx[nd], yd = S.ny[nd];
+    double SXd, SYd;
+    if (P.iaxis == 1) {
+        SXd = (yd - yb) * (yb + yd) * HALF;
+        SYd = -(xd - xb) * (yb + yd) * HALF;
+    } else {
+        SXd = (yd - yb);
+        SYd = -(xd - xb);
+    }
+    const float sx = (float)SXd, sy = (float)SYd;
+    const double xa = S.xc[sa], ya = S.yc[sa], xc = S.xc[sc], yc = S.yc[sc];
+    const double ybd = yb - yd, yac = ya - yc, xbd = xb - xd, xac = xa - xc;
+    const float idnr = (float)(1.0 / (xac * ybd - xbd * yac));
+    const float fybd = (float)ybd, fyac = (float)yac, fxbd = (float)xbd, fxac = (float)xac;
+    const double ua = S.u[sa], va = S.v[sa], ta = S.t[sa], uc = S.u[sc], vc = S.v[sc], tc = S.t[sc];
+    const double ub = S.au[ab], vb = S.av[ab], tb = S.at[ab], ud = S.au[ad], vd = S.av[ad], td = S.at[ad];
+    const double ra = S.ri[sa], rc = S.ri[sc], rb = S.ar[ab], rd = S.ar[ad];
+    const float duac = (float)(ua - uc), dubd = (float)(ub - ud);
+    const float dvac = (float)(va - vc), dvbd = (float)(vb - vd);
+    const float dtac = (float)(ta - tc), dtbd = (float)(tb - td);
+    const float drac = (float)(ra - rc), drbd = (float)(rb - rd);
+    const float DUX = (duac * fybd - dubd * fyac) * idnr;
+    const float DVX = (dvac * fybd - dvbd * fyac) * idnr;
+    const float DTX = (dtac * fybd - dtbd * fyac) * idnr;
+    const float DRX = (drac * fybd - drbd * fyac) * idnr;
+    const float DUY = (-duac * fxbd + dubd * fxac) * idnr;
+    const float DVY = (-dvac * fxbd + dvbd * fxac) * idnr;
+    const float DTY = (-dtac * fxbd + dtbd * fxac) * idnr;
+    const float DRY = (-drac * fxbd + drbd * fxac) * idnr;
+    const float UAVG = (float)(QUARTER * (ua + ub + uc + ud));
+    const float VAVG = (float)(QUARTER * (va + vb + vc + vd));
+    const float TAVG = (float)(QUARTER * (ta + tb + tc + td));
+    const float RHOAVG = (float)(QUARTER * (S.rho[sa] + S.arho[ab] + S.rho[sc] + S.arho[ad]));
+    const float RAVG = (float)(QUARTER * (ra + rb + rc + rd));
+    float DIVVEL;
+    if (P.iaxis == 1) {
+        const double YAVG = HALF * (yb + yd);
+        const float VBYY = (YAVG < YAXIS_THRESH) ? DVY : (float)(QUARTER * (va + vb + vc + vd) / YAVG);
+        DIVVEL = DUX + DVY + VBYY;
+    } else {
+        DIVVEL = DUX + DVY;
+    }
+    const float AMU = (float)P.suth_amol * pow06f(TAVG);
+    const float AK = AMU * (float)P.cp_pr;
+    const float CHI = RHOAVG * RAVG / (AMU * (float)CMU);
+    const float chi2 = CHI * CHI;
+    const float FMU = tanh_f32((float)ALPHA_T * chi2) / tanh_f32((float)BETA_T * chi2);
+    const float AMUT = RHOAVG * RAVG * FMU;
+    const float AKT = AMUT * (float)P.cp_prt;
+    const float AMUEFF = AMU + AMUT;
+    const float AKEFF = AK + AKT;
+    const float DIV23 = (float)P.div23;
+    const float TXX = AMUEFF * (DUX + DUX - DIV23 * DIVVEL);
+    const float TYY = AMUEFF * (DVY + DVY - DIV23 * DIVVEL);
+    const float TXY = AMUEFF * (DUY + DVX);
+    const float QXX = UAVG * TXX + VAVG * TXY + AKEFF * DTX;
+    const float QYY = UAVG * TXY + VAVG * TYY + AKEFF * DTY;
+    out[0] = TXX * sx + TXY * sy;
+    out[1] = TXY * sx + TYY * sy;
+    out[2] = QXX * sx + QYY * sy;
+    out[3] = AMUEFF * DRX * sx + AMUEFF * DRY * sy;
+}
+
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
+                                                         float* __restrict__ vis) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ViscSmemMx& S = *reinterpret_cast<ViscSmemMx*>(smem_raw);
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    __syncthreads();
+    for (int s = tid; s < NSLOT; s += NTHREADS) {
+        const int li = s / SW, lj = s % SW;
+        int along = 0;
+        const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
+        if (kind < 0) continue;
+        Prim p;
+        if (kind == 0) {
+            cell_prim(P, q, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
+            const int n1 = li * NW + lj;
+            S.xc[s] = (S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25;
+            S.yc[s] = (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25;
+        } else {
+            ghost_state(P, M, q, ncell, kind, along, p);
+            const int g = M.ghost_index(kind, along);
+            S.xc[s] = M.gxc[g];
+            S.yc[s] = M.gyc[g];
+        }
+        S.u[s] = p.u; S.v[s] = p.v; S.t[s] = p.t; S.rho[s] = p.rho; S.ri[s] = p.ri;
+    }
+    __syncthreads();
+    for (int s = tid; s < NAVG; s += NTHREADS) {
+        const int la = s / AW, lb = s % AW;
+        const int a = i0 + la, b = j0 + lb;
+        if (a > M.ni || b > M.nj) continue;
+        double un = 0.0, vn = 0.0, tn = 0.0, rhon = 0.0, rn = 0.0;
+        int cnt = 0, ng = 0, gs[2] = {0, 0}, gr[2] = {0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int pi = a - 1 + (k >> 1), pj = b - 1 + (k & 1);
+            const int sl = (la + (k >> 1)) * SW + lb + (k & 1);
+            int along = 0;
+            const int kind = classify(M, pi, pj, along);
+            if (kind == 0) {
+                un = un + S.u[sl]; vn = vn + S.v[sl]; tn = tn + S.t[sl];
+                rhon = rhon + S.rho[sl]; rn = rn + S.ri[sl];
+                cnt++;
+            } else if (kind > 0) {
+                gs[ng] = sl;
+                gr[ng] = M.ghost_index(kind, along);
+                ng++;
+            }
+        }
+        if (ng == 2 && M.grank[gr[1]] < M.grank[gr[0]]) {
+            int t = gs[0]; gs[0] = gs[1]; gs[1] = t;
+            t = gr[0]; gr[0] = gr[1]; gr[1] = t;
+        }
+        for (int k = 0; k < ng; k++) {
+            const int sl = gs[k];
+            un = un + S.u[sl]; vn = vn + S.v[sl]; tn = tn + S.t[sl];
+            rhon = rhon + S.rho[sl]; rn = rn + S.ri[sl];
+            const int type = M.gtype[gr[k]];
+            if (type == 4) {
+                vn = 0.0;
+            } else if (type == 5) {
+                un = 0.0; vn = 0.0; rn = P.rtol_rtred;
+            }
+            cnt++;
+        }
+        const double idf = cnt == 4 ? 0.25 : 1.0 / (double)cnt;
+        S.au[s] = un * idf; S.av[s] = vn * idf; S.at[s] = tn * idf; S.arho[s] = rhon * idf;
+        S.ar[s] = dmax1(P.rtol, rn * idf);
+    }
+    __syncthreads();
+    for (int f = tid; f < NIFM; f += NTHREADS) {
+        const int ii = f / TJ, jj = f % TJ;
+        const int i = i0 + ii, j = j0 + jj;
+        if (i > M.ni || j >= M.nj) continue;
+        float out[4];
+        const int sL = ii * SW + jj + 1, sR = sL + SW;
+        const int aLo = ii * AW + jj, aHi = aLo + 1;
+        const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
+        if (i == 0) face_flux_mx(P, S, sR, sL, aHi, aLo, nHi, nLo, out);
+        else face_flux_mx(P, S, sL, sR, aLo, aHi, nLo, nHi, out);
+#pragma unroll
+        for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
+    }
+    for (int f = tid; f < NJFM; f += NTHREADS) {
+        const int ii = f / AW, jj = f % AW;
+        const int i = i0 + ii, j = j0 + jj;
+        if (i >= M.ni || j > M.nj) continue;
+        float out[4];
+        const int sB = (ii + 1) * SW + jj, sT = sB + 1;
+        const int aL = ii * AW + jj, aR = aL + AW;
+        const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
+        if (j == 0) face_flux_mx(P, S, sT, sB, aL, aR, nL, nR, out);
+        else face_flux_mx(P, S, sB, sT, aR, aL, nR, nL, out);
+#pragma unroll
+        for (int k = 0; k < 4; k++) S.fj[k][f] = out[k];
+    }
+    __syncthreads();
+    const int tj = threadIdx.x, ti = threadIdx.y;
+    const int i = i0 + ti, j = j0 + tj;
+    if (i >= M.ni || j >= M.nj) return;
+    const size_t cell = (size_t)i * M.nj + j;
+    const int f1 = ti * AW + tj, f3 = f1 + 1;
+    const int f4 = ti * TJ + tj, f2 = f4 + TJ;
+    const float s1 = (j == 0) ? 1.0f : -1.0f, s4 = (i == 0) ? 1.0f : -1.0f;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        vis[k * ncell + cell] = ((s1 * S.fj[k][f1] + S.fi[k][f2]) + S.fj[k][f3]) + s4 * S.fi[k][f4];
+}
+
+// ------------------------------------------------------------ dissipation kernel
+
+// JST dissipation (solver_state.f90:70-225) with FP64 state, pressure and every
+// difference of the state, FP32 sensors, Laplacian differences and blend.
+constexpr int DWM = TJ + 4;
+constexpr int NDSLOTM = (TI + 4) * DWM;
+constexpr int RWM = TJ + 2;
+constexpr int NRSLOTM = (TI + 2) * RWM;
+
+struct DissSmemMx {
+    double c[5][NDSLOTM];
+    double p[NDSLOTM];
+    float vbd[NRSLOTM], anu[NRSLOTM], anurt[NRSLOTM], d2q[5][NRSLOTM];
+    double nx[NNODE], ny[NNODE];
+};
+
+size_t diss_mx_smem_bytes() { return sizeof(DissSmemMx); }
+
+__device__ __forceinline__ double local_dt_mx(const Params& P, double c1, double c2, double c3,
+                                              double c4, double cfldl) {
+    const double rr = 1.0 / c1;
+    const double U = c2 * rr, V = c3 * rr;
+    const double VEL = sqrt(U * U + V * V);
+    const double E = c4 * rr;
+    const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
+    return cfldl / (fabs(VEL) + sqrt(P.gamrr * T));
+}
+
+__global__ void __launch_bounds__(NTHREADS) k_dissipation_mx(Params P, Mesh M, const double* __restrict__ q,
+                                                             float* __restrict__ dout, float* __restrict__ dtout,
+                                                             const double* __restrict__ dtmin) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DissSmemMx& S = *reinterpret_cast<DissSmemMx*>(smem_raw);
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    for (int s = tid; s < NDSLOTM; s += NTHREADS) {
+        const int i = i0 - 2 + s / DWM, j = j0 - 2 + s % DWM;
+        if (i >= 0 && i < M.ni && j >= 0 && j < M.nj) {
+            const size_t c = (size_t)i * M.nj + j;
+            double C[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++) {
+                C[m] = q[m * ncell + c];
+                S.c[m][s] = C[m];
+            }
+            const double rr = 1.0 / C[0];
+            const double U = C[1] * rr, V = C[2] * rr;
+            const double T = (C[3] * rr - 0.5 * (U * U + V * V)) * P.inv_cv;
+            S.p[s] = C[0] * P.rr * T;
+        }
+    }
+    __syncthreads();
+    for (int s = tid; s < NRSLOTM; s += NTHREADS) {
+        const int ri = s / RWM, rj = s % RWM;
+        const int i = i0 - 1 + ri, j = j0 - 1 + rj;
+        if (!(i >= 0 && i < M.ni && j >= 0 && j < M.nj)) continue;
+        const int d = (ri + 1) * DWM + (rj + 1);
+        int nbs[4] = {d - 1, d + DWM, d + 1, d - DWM};
+        if (j == 0) nbs[0] = d;
+        if (i == M.ni - 1) nbs[1] = d;
+        if (j == M.nj - 1) nbs[2] = d;
+        if (i == 0) nbs[3] = d;
+        const double PIE = S.p[d], C5I = S.c[4][d];
+        double an = 0.0, ad = 0.0, rn = 0.0, rd = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            an += fabs(S.p[nbs[k]] - PIE);
+            ad += fabs(S.p[nbs[k]] + PIE);
+            rn += fabs(S.c[4][nbs[k]] - C5I);
+            rd += fabs(S.c[4][nbs[k]] + C5I);
+        }
+        S.anu[s] = (float)an / (float)ad;
+        S.anurt[s] = (float)rn / (float)fmax(rd, 8.0 * S.c[0][d] * P.rtol);
+#pragma unroll
+        for (int m = 0; m < 5; m++)
+            S.d2q[m][s] = (float)(S.c[m][nbs[0]] + S.c[m][nbs[1]] + S.c[m][nbs[2]] + S.c[m][nbs[3]] - 4.0 * S.c[m][d]);
+        const size_t c = (size_t)i * M.nj + j;
+        double DT;
+        if (P.local) {
+            DT = local_dt_mx(P, S.c[0][d], S.c[1][d], S.c[2][d], S.c[3][d], M.cfldl[c]);
+            if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) dtout[c] = (float)DT;
+        } else {
+            DT = *dtmin;
+        }
+        const int n1 = ri * NW + rj;
+        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
+        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
+        const double ycc = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
+        S.vbd[s] = (float)(cell_volume(P.iaxis, X, Y, ycc) / DT);
+    }
+    __syncthreads();
+    const int tj = threadIdx.x, ti = threadIdx.y;
+    const int i = i0 + ti, j = j0 + tj;
+    if (i >= M.ni || j >= M.nj) return;
+    const size_t cell = (size_t)i * M.nj + j;
+    const int r = (ti + 1) * RWM + (tj + 1);
+    const int d = (ti + 2) * DWM + (tj + 2);
+    const int rn[4] = {r - 1, r + RWM, r + 1, r - RWM};
+    const int dn[4] = {d - 1, d + DWM, d + 1, d - DWM};
+    const bool has[4] = {j > 0, i < M.ni - 1, j < M.nj - 1, i > 0};
+    const float VOLBYDT = S.vbd[r];
+    float D2c[4], D4c[4], D2t[4], D4t[4];
+    const float ANUI = S.anu[r], ANURTI = S.anurt[r];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float D24N = 0.5f * (VOLBYDT + S.vbd[rn[k]]);
+        float E2N = (float)C02 * fmaxf(ANUI, S.anu[rn[k]]);
+        float E4N = fmaxf(0.0f, (float)C04 - E2N);
+        D2c[k] = E2N * D24N;
+        D4c[k] = E4N * D24N;
+        E2N = (float)C02 * fmaxf(ANURTI, S.anurt[rn[k]]);
+        E4N = fmaxf(0.0f, (float)C04 - E2N);
+        D2t[k] = E2N * D24N;
+        D4t[k] = E4N * D24N;
+    }
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        const double CI = S.c[m][d];
+        const float D2I = S.d2q[m][r];
+        float D2 = 0.0f, D4 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!has[k]) continue;
+            const float a2 = (m == 4) ? D2t[k] : D2c[k];
+            const float a4 = (m == 4) ? D4t[k] : D4c[k];
+            D2 += a2 * (float)(S.c[m][dn[k]] - CI);
+            D4 += a4 * (S.d2q[m][rn[k]] - D2I);
+        }
+        dout[m * ncell + cell] = D2 - D4;
+    }
+}
+
+// ------------------------------------------------------------ port mass flux
+
+__global__ void k_gport_mx(Params P, Mesh M, const double* __restrict__ cold,
+                           const float* __restrict__ dq, const int* ghosts, int nport,
+                           double* gport) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= nport) return;
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const StateMixed st{cold, dq, ncell};
+    const int g = ghosts[w];
+    int side, along;
+    if (g < M.ni) { side = 1; along = g; }
+    else if (g < M.ni + M.nj) { side = 2; along = g - M.ni; }
+    else if (g < 2 * M.ni + M.nj) { side = 3; along = g - M.ni - M.nj; }
+    else { side = 4; along = g - 2 * M.ni - M.nj; }
+    const int len = (side == 1 || side == 3) ? M.nj : M.ni;
+    double sum = 0.0;
+    for (int k = lane; k < len; k += 32) {
+        const int i = (side == 1 || side == 3) ? along : k;
+        const int j = (side == 1 || side == 3) ? k : along;
+        const size_t c = (size_t)i * M.nj + j;
+        const size_t n1 = (size_t)i * (M.nj + 1) + j;
+        const double y1 = M.y[n1], y2 = M.y[n1 + M.nj + 1], y3 = M.y[n1 + M.nj + 2], y4 = M.y[n1 + 1];
+        double dely;
+        if (side == 1) dely = HALF * ((y1 + y2) - (y3 + y4));
+        else if (side == 2) dely = HALF * ((y2 + y3) - (y1 + y4));
+        else if (side == 3) dely = HALF * ((y3 + y4) - (y1 + y2));
+        else dely = HALF * ((y4 + y1) - (y2 + y3));
+        const double c1 = st.c(0, c), u = st.c(1, c) / c1;
+        double term = c1 * u * dely;
+        if (P.iaxis == 1) term = term * ((y1 + y2 + y3 + y4) * 0.25);
+        sum += term;
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) gport[g] = sum;
+}
+
+// ------------------------------------------------------ primitive output
+
+__global__ void k_prim_out_mx(Params P, Mesh M, const double* __restrict__ cold,
+                              const float* __restrict__ dq, double* out) {
+    const size_t ncell = (size_t)M.ni * M.nj;
+    const size_t ng = M.nghosts(), ntot = ncell + ng;
+    const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k >= ntot) return;
+    const StateMixed st{cold, dq, ncell};
+    Prim p;
+    if (k < ncell) {
+        cell_prim(P, st, k, p);
+    } else {
+        const int g = (int)(k - ncell);
+        int side, along;
+        if (g < M.ni) { side = 1; along = g; }
+        else if (g < M.ni + M.nj) { side = 2; along = g - M.ni; }
+        else if (g < 2 * M.ni + M.nj) { side = 3; along = g - M.ni - M.nj; }
+        else { side = 4; along = g - 2 * M.ni - M.nj; }
+        ghost_state(P, M, st, side, along, p);
+    }
+    out[k] = p.u;
+    out[ntot + k] = p.v;
+    out[2 * ntot + k] = p.t;
+    out[3 * ntot + k] = p.p;
+}
+
+// ------------------------------------------------------------------ launchers
+
+static dim3 tile_grid_mx(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
+
+cudaError_t configure_kernels_mx() {
+    cudaError_t e = cudaFuncSetAttribute(k_stage_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)stage_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_dissipation_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diss_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_viscous_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)visc_mx_smem_bytes());
+}
+
+void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
+                            const double* dtmin, cudaStream_t s) {
+    k_dissipation_mx<<<tile_grid_mx(M), dim3(TJ, TI), diss_mx_smem_bytes(), s>>>(P, M, q, d, dt, dtmin);
+}
+
+void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* vis, cudaStream_t s) {
+    k_viscous_mx<<<tile_grid_mx(M), dim3(TJ, TI), visc_mx_smem_bytes(), s>>>(P, M, q, vis);
+}
+
+void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,
+                     float* dqout, double* qout, const float* d, const float* vis, const float* dt,
+                     const double* dtmin, double alpha, unsigned long long* cdiff,
+                     unsigned int* status, cudaStream_t s) {
+    StageArgsMx A{cold, dqin, dqout, qout, d, vis, dt, dtmin, (float)alpha, cdiff, status};
+    k_stage_mx<<<tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s>>>(P, M, A);
+}
+
+void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
+                     const int* ghosts, int nport, double* gport, cudaStream_t s) {
+    if (nport <= 0) return;
+    k_gport_mx<<<(nport + 7) / 8, 256, 0, s>>>(P, M, cold, dq, ghosts, nport, gport);
+}
+
+void launch_prim_out_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
+                        double* out, cudaStream_t s) {
+    const size_t ntot = (size_t)M.ni * M.nj + M.nghosts();
+    k_prim_out_mx<<<(unsigned)((ntot + 255) / 256), 256, 0, s>>>(P, M, cold, dq, out);
+}
+
+}  // namespace tns

@@ -1,0 +1,113 @@
+// tns_tile.cuh -- tile geometry and the helpers every tile kernel shares: node staging,
+// halo classification, primitive variables of a cell, and the ghost state of a halo
+// position (BC of boundary.f90:24-327 from the parent and its opposite neighbour).
+#pragma once
+
+#include "tns_device.cuh"
+
+namespace tns {
+
+#ifndef TNS_TI
+#define TNS_TI 8
+#endif
+#ifndef TNS_STAGE_MINB
+#define TNS_STAGE_MINB 3
+#endif
+#ifndef TNS_VISC_MINB
+#define TNS_VISC_MINB 1
+#endif
+constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
+constexpr int TI = TNS_TI;  // tile extent along i
+constexpr int NTHREADS = TJ * TI;
+
+
+// Halo-1 slot grid (TI+2) x (TJ+2), node grid (TI+3) x (TJ+3) (nodes of every halo cell).
+constexpr int SW = TJ + 2;
+constexpr int NSLOT = (TI + 2) * SW;
+constexpr int NW = TJ + 3;
+constexpr int NNODE = (TI + 3) * NW;
+constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
+constexpr int NAVG = (TI + 1) * AW;
+
+__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny) {
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    for (int s = tid; s < NNODE; s += NTHREADS) {
+        const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
+        if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
+            const size_t n = (size_t)a * (M.nj + 1) + b;
+            snx[s] = M.x[n];
+            sny[s] = M.y[n];
+        }
+    }
+}
+
+// How a kernel reads the conservative state of cell c: FP64 array, or FP64 COLD plus an
+// FP32 stage increment (the mixed-precision path).
+struct StateF64 {
+    const double* __restrict__ q;
+    size_t n;
+    __device__ __forceinline__ double c(int m, size_t cell) const { return q[m * n + cell]; }
+};
+struct StateMixed {
+    const double* __restrict__ cold;
+    const float* __restrict__ dq;  // null in stage 1 (state = COLD)
+    size_t n;
+    __device__ __forceinline__ double c(int m, size_t cell) const {
+        const double v = cold[m * n + cell];
+        return dq ? v + (double)dq[m * n + cell] : v;
+    }
+};
+
+template <class St>
+__device__ __forceinline__ void cell_prim(const Params& P, const St& st, size_t c, Prim& p) {
+    primitive(P, st.c(0, c), st.c(1, c), st.c(2, c), st.c(3, c), st.c(4, c), p);
+}
+
+__device__ __forceinline__ void cell_prim(const Params& P, const double* __restrict__ q, size_t ncell,
+                                          size_t c, Prim& p) {
+    cell_prim(P, StateF64{q, ncell}, c, p);
+}
+
+// Classifies halo position (i, j): 0 = cell, 1..4 = ghost on that side, -1 = unused.
+__device__ __forceinline__ int classify(const Mesh& M, int i, int j, int& along) {
+    const bool in_i = i >= 0 && i < M.ni, in_j = j >= 0 && j < M.nj;
+    if (in_i && in_j) return 0;
+    if (in_i && j == -1) { along = i; return 1; }
+    if (in_j && i == M.ni) { along = j; return 2; }
+    if (in_i && j == M.nj) { along = i; return 3; }
+    if (in_j && i == -1) { along = j; return 4; }
+    return -1;
+}
+
+// BC state of the ghost on `side` at `along`, from the parent and the parent's opposite
+// neighbour read straight from the state array (bit-identical to their PRIMITIVE_VARS).
+template <class St>
+__device__ void ghost_state(const Params& P, const Mesh& M, const St& st, int side, int along,
+                            Prim& gh) {
+    int ip, jp, io, jo;
+    if (side == 1) { ip = along; jp = 0; io = along; jo = 1; }
+    else if (side == 2) { ip = M.ni - 1; jp = along; io = M.ni - 2; jo = along; }
+    else if (side == 3) { ip = along; jp = M.nj - 1; io = along; jo = M.nj - 2; }
+    else { ip = 0; jp = along; io = 1; jo = along; }
+    const int g = M.ghost_index(side, along);
+    const int type = M.gtype[g];
+    Prim par, opp;
+    cell_prim(P, st, (size_t)ip * M.nj + jp, par);
+    if (type == 3) cell_prim(P, st, (size_t)io * M.nj + jo, opp);
+    else opp = par;
+    const size_t n1 = (size_t)ip * (M.nj + 1) + jp;
+    const double X[4] = {M.x[n1], M.x[n1 + M.nj + 1], M.x[n1 + M.nj + 2], M.x[n1 + 1]};
+    const double Y[4] = {M.y[n1], M.y[n1 + M.nj + 1], M.y[n1 + M.nj + 2], M.y[n1 + 1]};
+    double psx = 0.0, psy = 0.0;
+    if (type == 6) face_vector(P.iaxis, side, X, Y, psx, psy);
+    const double ycc_p = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
+    boundary_ghost(P, type, par, opp, psx, psy, M.gyc[g], ycc_p, type == 6 ? M.gport[g] : 0.0,
+                   M.ginj[g], gh);
+}
+
+__device__ __forceinline__ void ghost_state(const Params& P, const Mesh& M, const double* __restrict__ q,
+                                            size_t ncell, int side, int along, Prim& gh) {
+    ghost_state(P, M, StateF64{q, ncell}, side, along, gh);
+}
+
+}  // namespace tns

@@ -39,6 +39,13 @@ UNIT = "cell-iter/s"
 #                (stage 1 reads Q_in = Q_old once: 22 words; mean of the 4 = 25.75)
 KERNEL_BYTES_PER_CELL = {"dissipation": 112, "viscous": 88, "stage": 206}
 KERNEL_NAMES = {"dissipation": "k_dissipation", "viscous": "k_viscous", "stage": "k_stage"}
+# Mixed FP32/FP64 path: D, VIS, DT and the stage increments dQ are FP32 (4 B words):
+#   dissipation: Q_old 40 + nodes 16 + CFL*DL 8 in, D 20 + DT 4 out              = 88
+#   viscous    : Q_old 40 + nodes 16 in, VIS 16 out                              = 72
+#   stage      : Q_old 40 + dQ_in 20 + D 20 + VIS 16 + DT 4 + nodes 16 in,
+#                dQ_out 20 out (stage 4: Q_new 40); stage 1 reads no dQ_in        -> mean 143
+KERNEL_BYTES_PER_CELL_MX = {"dissipation": 88, "viscous": 72, "stage": 143}
+KERNEL_NAMES_MX = {"dissipation": "k_dissipation_mx", "viscous": "k_viscous_mx", "stage": "k_stage_mx"}
 
 
 def _case(name):
@@ -120,27 +127,15 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def run_ours(args, rank, world, dev):
-    import numpy as np
-    import torch
-    from tnsgpu.solver import Solver
-
-    mesh, flow, c0, rinit, wname = _case(args.case)
-    s = Solver(mesh, flow, rinit)
-    # one non-default stream for the solver, the L2 flush and the timing events
-    stream = torch.cuda.Stream(device=dev)
-    torch.cuda.set_stream(stream)
-    s.set_stream(stream.cuda_stream)
-    s.upload(c0)
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    K, W = args.steps, args.warmup
+def time_steps(s, stream, flush, K, W, world, torch):
+    """Device time per step (one RK4 iteration; L2 flushed between steps, outside the
+    events), max over ranks, plus our launches in the timed region."""
     for _ in range(W):
         flush.zero_()
         s.enqueue(1)
     s.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(K)]
-    clocks = Clocks(dev)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -153,14 +148,56 @@ def run_ours(args, rank, world, dev):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    clk = clocks.stop()
     s.synchronize()
-    launches = s.launch_count() - l0
     ms = sum(a.elapsed_time(b) for a, b in ev) / K
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        t = torch.tensor([ms], dtype=torch.float64, device=stream.device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
+    return ms, s.launch_count() - l0
+
+
+def pin_to_gpu_numa_node(dev: int):
+    """Restricts this process to the CPUs local to the GPU (NVML), so page-locked host
+    buffers live on the GPU's NUMA node and host<->device copies take the short path."""
+    try:
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        # match by UUID: CUDA_VISIBLE_DEVICES renumbers devices, NVML does not
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        cpus = {w * 64 + b for w, word in enumerate(words) for b in range(64) if word >> b & 1}
+        cpus &= os.sched_getaffinity(0)
+        if cpus:
+            os.sched_setaffinity(0, cpus)
+        return sorted(cpus)
+    except Exception:
+        return None
+
+
+def run_ours(args, rank, world, dev):
+    import numpy as np
+    import torch
+    from tnsgpu.solver import Solver
+
+    numa_cpus = pin_to_gpu_numa_node(dev)
+    mesh, flow, c0, rinit, wname = _case(args.case)
+    prec = 1 if args.precision == "mixed" else 0
+    kbytes = KERNEL_BYTES_PER_CELL_MX if prec else KERNEL_BYTES_PER_CELL
+    knames = KERNEL_NAMES_MX if prec else KERNEL_NAMES
+    s = Solver(mesh, flow, rinit, precision=prec)
+    # one non-default stream for the solver, the L2 flush and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    s.set_stream(stream.cuda_stream)
+    s.upload(c0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    K, W = args.steps, args.warmup
+    clocks = Clocks(dev)
+    ms, launches = time_steps(s, stream, flush, K, W, world, torch)
+    clk = clocks.stop()
     value = world * mesh.neles / (ms * 1e-3)
 
     # per-kernel device times (events around each launch, L2 flushed between iterations)
@@ -175,9 +212,9 @@ def run_ours(args, rank, world, dev):
     dom = max(("dissipation", "viscous", "stage"), key=lambda k: kt[k][0])
     avg_ms = kt[dom][0] / max(kt[dom][1], 1)
     peak, peak_kind = _peaks()
-    bytes_launch = KERNEL_BYTES_PER_CELL[dom] * mesh.neles
+    bytes_launch = kbytes[dom] * mesh.neles
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
-    traffic = _traffic(args.case, KERNEL_NAMES[dom])
+    traffic = _traffic(args.case, knames[dom])
     total_kms = sum(kt[k][0] for k in kt) / P
     kernel_split = {k: round(kt[k][0] / P * 1e3, 2) for k in kt if kt[k][1]}
 
@@ -204,8 +241,20 @@ def run_ours(args, rank, world, dev):
         e2e_s = float(t.item())
     e2e = {"value": world * mesh.neles / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": 5 * mesh.neles * 8, "d2h_bytes_per_step": 5 * 8 + 4,
-           "ms_per_step": round(e2e_s * 1e3, 4)}
+           "ms_per_step": round(e2e_s * 1e3, 4),
+           "host_cpus": f"{len(numa_cpus)} GPU-local" if numa_cpus else "unpinned"}
     s.close()
+
+    # the other precision on the same workload and stream, for the FP32-vs-FP64 metric
+    other = None
+    if not args.single_precision_mode:
+        s2 = Solver(mesh, flow, rinit, precision=1 - prec)
+        s2.set_stream(stream.cuda_stream)
+        s2.upload(c0)
+        ms2, _ = time_steps(s2, stream, flush, K, W, world, torch)
+        s2.close()
+        other = {"precision": "fp64" if prec else "mixed", "value": world * mesh.neles / (ms2 * 1e-3),
+                 "ms_per_step": round(ms2, 5), "mixed_over_fp64": (ms2 / ms) if prec == 0 else (ms / ms2)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -214,12 +263,13 @@ def run_ours(args, rank, world, dev):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": round(ms, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wname, "cells": mesh.neles, "precision": "fp64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if prec else "f64",
+        "data": "synthetic",
+        "config": {"workload": wname, "cells": mesh.neles, "precision": args.precision,
                    "step": "one RK4 iteration (dissipation pre-pass + 4 stages)",
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": knames[dom], "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
@@ -229,6 +279,7 @@ def run_ours(args, rank, world, dev):
         "kernel_us_per_iteration": kernel_split,
         "device_ms_per_iteration_profiled": round(total_kms, 5),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "other_precision": other,
         "cpu_baseline": cpu,
     }
     if rank == 0:
@@ -294,6 +345,10 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--case", default="nozzle_plume_1024x384")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
+                    help="arithmetic of the timed path (the other one is timed too, as other_precision)")
+    ap.add_argument("--single-precision-mode", action="store_true",
+                    help="time only --precision (no other_precision entry)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

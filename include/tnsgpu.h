@@ -48,7 +48,8 @@ typedef struct tns_params {
     double gama, amol, cfl, prandtl, prandtlt, p0, t0, pamb, rtred, rinit;
     double tflame, ancomb, acomb, rhoprop, pinf, aminf, deltabl;
     int local, npseudo, iaxis;
-    int precision; /* 0 = FP64 (the only mode of this version) */
+    int precision; /* 0 = FP64; 1 = mixed: FP64 state, geometry and differences, FP32
+                      increments, D, VIS, DT and flux / JST / viscous / source arithmetic */
 } tns_params;
 
 typedef struct tns_handle tns_handle;
