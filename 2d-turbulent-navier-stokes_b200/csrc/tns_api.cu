@@ -54,6 +54,7 @@ struct tns_handle {
     std::vector<int> port_ghosts;
     std::vector<double> hX, hY, hcfldl, hgxc, hgyc, hginj;  // host layout (device order)
     std::vector<int> hgtype, hgrank;
+    std::vector<int> node_of;   // structured node index -> 1-based node id
     cudaStream_t own = nullptr, stream = nullptr;
     DevBuf<double> x, y, cfldl, gxc, gyc, ginj, gport, qa, qb, qc, d, vis, dt, dtmin, partial,
         primout;
@@ -295,6 +296,7 @@ int build_mesh(tns_handle* h, const tns_mesh* m) {
         if (h->ghost_line[g] < 0) return h->fail(TNS_ERR_MESH, "boundary face %d has no bc.in line", g);
     h->hX.swap(X); h->hY.swap(Y); h->hcfldl.swap(cfldl); h->hgxc.swap(gxc); h->hgyc.swap(gyc);
     h->hginj.swap(ginj); h->hgtype.swap(gtype); h->hgrank.swap(grank);
+    h->node_of.swap(node_of);
     return TNS_OK;
 }
 
@@ -672,9 +674,11 @@ int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double
     return TNS_OK;
 }
 
-int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, double* p) {
-    if (!h || !u || !v || !t || !p) return TNS_ERR_ARG;
-    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_download_primitives: no iteration has run");
+}  // extern "C"
+
+namespace {
+// U, V, T, P of the last stage's input for cells and ghosts into h->primout (device).
+int fill_primitives(tns_handle* h) {
     const size_t nc = h->ncell(), ng = (size_t)h->M.nghosts(), nt = nc + ng;
     int rc;
     if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
@@ -688,6 +692,18 @@ int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, doub
         if (np) tns::launch_gport(h->P, h->M, h->qb.p, h->ports.p, np, h->gport.p, h->stream);
         tns::launch_prim_out(h->P, h->M, h->qb.p, h->primout.p, h->stream);
     }
+    return h->cuda(cudaGetLastError(), "kernel launch");
+}
+}  // namespace
+
+extern "C" {
+
+int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, double* p) {
+    if (!h || !u || !v || !t || !p) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_download_primitives: no iteration has run");
+    const size_t nc = h->ncell(), ng = (size_t)h->M.nghosts(), nt = nc + ng;
+    int rc;
+    if ((rc = fill_primitives(h))) return rc;
     std::vector<double> hb(4 * nt);
     rc = h->cuda(cudaMemcpyAsync(hb.data(), h->primout.p, 4 * nt * 8, cudaMemcpyDeviceToHost, h->stream),
                  "cudaMemcpyAsync");
@@ -699,6 +715,43 @@ int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, doub
         for (size_t g = 0; g < ng; g++) dst[f][h->ghost_id[h->ghost_line[g]] - 1] = src[nc + g];
     }
     return TNS_OK;
+}
+
+int tns_node_averages(tns_handle* h, double* pn, double* un, double* vn, double* tn) {
+    if (!h || !pn || !un || !vn || !tn) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_node_averages: no iteration has run");
+    int rc;
+    if ((rc = fill_primitives(h))) return rc;
+    const size_t nnode = (size_t)(h->ni + 1) * (h->nj + 1);
+    DevBuf<double> dn;
+    if ((rc = h->cuda(dn.alloc(4 * nnode), "cudaMalloc"))) return rc;
+    tns::launch_node_average(h->M, h->primout.p, dn.p, h->stream);
+    std::vector<double> hb(4 * nnode);
+    rc = h->cuda(cudaMemcpyAsync(hb.data(), dn.p, 4 * nnode * 8, cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    dn.release();
+    if (rc) return rc;
+    double* dst[4] = {pn, un, vn, tn};
+    for (int f = 0; f < 4; f++)
+        for (size_t k = 0; k < nnode; k++) dst[f][h->node_of[k] - 1] = hb[f * nnode + k];
+    return TNS_OK;
+}
+
+int tns_boundary_integrals(tns_handle* h, int type, int side, double out[4]) {
+    if (!h || !out || type < 0 || type > 7 || side < 0 || side > 4) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_boundary_integrals: no iteration has run");
+    int rc;
+    if ((rc = fill_primitives(h))) return rc;
+    DevBuf<double> acc;
+    if ((rc = h->cuda(acc.alloc(4), "cudaMalloc"))) return rc;
+    cudaMemsetAsync(acc.p, 0, 4 * sizeof(double), h->stream);
+    tns::launch_boundary_sums(h->P, h->M, h->primout.p, type, side, acc.p, h->stream);
+    rc = h->cuda(cudaMemcpyAsync(out, acc.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    acc.release();
+    return rc;
 }
 
 int tns_debug_fetch(tns_handle* h, int which, double* out) {

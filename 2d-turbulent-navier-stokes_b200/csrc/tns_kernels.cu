@@ -648,6 +648,92 @@ __global__ void k_prim_out(Params P, Mesh M, const double* __restrict__ q, doubl
     out[3 * ntot + k] = p.p;
 }
 
+// ---------------------------------------------------------- post-processing
+
+// POSTPROCESS node averages (solver_state.f90:237-281) of the [4][ncell+nghost] U,V,T,P
+// array k_prim_out produced: cells in ascending id order, then the ghosts of the node
+// in bc.in order, divided by their count.  Output [4][nnode] as (P, U, V, T).
+__global__ void k_node_average(Mesh M, const double* __restrict__ prim, double* __restrict__ out) {
+    const size_t ncell = (size_t)M.ni * M.nj, ntot = ncell + M.nghosts();
+    const size_t nnode = (size_t)(M.ni + 1) * (M.nj + 1);
+    const size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (n >= nnode) return;
+    const int a = (int)(n / (M.nj + 1)), b = (int)(n % (M.nj + 1));
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    int cnt = 0, ng = 0;
+    size_t gk[2] = {0, 0};
+    int gr[2] = {0, 0};
+    for (int k = 0; k < 4; k++) {
+        const int pi = a - 1 + (k >> 1), pj = b - 1 + (k & 1);
+        int along = 0;
+        const int kind = classify(M, pi, pj, along);
+        if (kind == 0) {
+            const size_t c = (size_t)pi * M.nj + pj;
+            s[0] += prim[3 * ntot + c]; s[1] += prim[c]; s[2] += prim[ntot + c]; s[3] += prim[2 * ntot + c];
+            cnt++;
+        } else if (kind > 0) {
+            const int g = M.ghost_index(kind, along);
+            gk[ng] = ncell + g;
+            gr[ng] = M.grank[g];
+            ng++;
+        }
+    }
+    if (ng == 2 && gr[1] < gr[0]) { const size_t t = gk[0]; gk[0] = gk[1]; gk[1] = t; }
+    for (int k = 0; k < ng; k++) {
+        const size_t c = gk[k];
+        s[0] += prim[3 * ntot + c]; s[1] += prim[c]; s[2] += prim[ntot + c]; s[3] += prim[2 * ntot + c];
+        cnt++;
+    }
+    const double d = (double)cnt;
+#pragma unroll
+    for (int f = 0; f < 4; f++) out[f * nnode + n] = s[f] / d;
+}
+
+// Boundary-face sums over the ghosts whose BC type / side match (0 = any), with the face
+// state (parent + ghost)/2: [0] sum P*SX, [1] sum P*SY, [2] sum RHO*(U*SX+V*SY),
+// [3] sum |S|.  One warp per 32 faces; one atomicAdd per warp and quantity.
+__global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ prim, int type,
+                                int side, double* __restrict__ out) {
+    const size_t ncell = (size_t)M.ni * M.nj, ntot = ncell + M.nghosts();
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (g < M.nghosts()) {
+        int sd, along;
+        if (g < M.ni) { sd = 1; along = g; }
+        else if (g < M.ni + M.nj) { sd = 2; along = g - M.ni; }
+        else if (g < 2 * M.ni + M.nj) { sd = 3; along = g - M.ni - M.nj; }
+        else { sd = 4; along = g - 2 * M.ni - M.nj; }
+        if ((type == 0 || M.gtype[g] == type) && (side == 0 || sd == side)) {
+            int ip, jp;
+            if (sd == 1) { ip = along; jp = 0; }
+            else if (sd == 2) { ip = M.ni - 1; jp = along; }
+            else if (sd == 3) { ip = along; jp = M.nj - 1; }
+            else { ip = 0; jp = along; }
+            const size_t cp = (size_t)ip * M.nj + jp, cg = ncell + g;
+            const size_t n1 = (size_t)ip * (M.nj + 1) + jp;
+            const double X[4] = {M.x[n1], M.x[n1 + M.nj + 1], M.x[n1 + M.nj + 2], M.x[n1 + 1]};
+            const double Y[4] = {M.y[n1], M.y[n1 + M.nj + 1], M.y[n1 + M.nj + 2], M.y[n1 + 1]};
+            double sx, sy;
+            face_vector(P.iaxis, sd, X, Y, sx, sy);
+            const double u = 0.5 * (prim[cp] + prim[cg]), vv = 0.5 * (prim[ntot + cp] + prim[ntot + cg]);
+            const double tp = prim[2 * ntot + cp], tg = prim[2 * ntot + cg];
+            const double pp = prim[3 * ntot + cp], pg = prim[3 * ntot + cg];
+            const double pf = 0.5 * (pp + pg);
+            const double rho = 0.5 * (pp / (P.rr * tp) + pg / (P.rr * tg));
+            v[0] = pf * sx;
+            v[1] = pf * sy;
+            v[2] = rho * (u * sx + vv * sy);
+            v[3] = sqrt(sx * sx + sy * sy);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x != 0.0) atomicAdd(&out[q], x);
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 
 static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
@@ -708,6 +794,16 @@ void launch_gport(const Params& P, const Mesh& M, const double* q, const int* gh
     const int threads = 256, warps_per_block = threads / 32;
     k_gport<<<(nport + warps_per_block - 1) / warps_per_block, threads, 0, s>>>(P, M, q, ghosts,
                                                                                nport, gport);
+}
+
+void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStream_t s) {
+    const size_t nnode = (size_t)(M.ni + 1) * (M.nj + 1);
+    k_node_average<<<(unsigned)((nnode + 255) / 256), 256, 0, s>>>(M, prim, out);
+}
+
+void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
+                          double* out, cudaStream_t s) {
+    k_boundary_sums<<<(M.nghosts() + 255) / 256, 256, 0, s>>>(P, M, prim, type, side, out);
 }
 
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,

@@ -32,6 +32,10 @@ void launch_gport(const Params& P, const Mesh& M, const double* q, const int* gh
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,
                      cudaStream_t s);
 
+void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStream_t s);
+void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
+                          double* out, cudaStream_t s);
+
 // mixed FP32/FP64 path (tns_kernels_mx.cu)
 cudaError_t configure_kernels_mx();
 void launch_dissipation_mx(const Params& P, const Mesh& M, const double* q, float* d, float* dt,

@@ -157,12 +157,10 @@ int main() {
     if (!bc.ok()) { std::fprintf(stderr, "cannot open %s\n", fnamebc.c_str()); return 2; }
     const int nghosts = (int)num(bc.read(1)[0]);
     std::vector<int> NPARENT(nghosts), NGHOST(nghosts), NTYPE(nghosts), NSIDE(nghosts);
-    int maxid = neles;
     for (int i = 0; i < nghosts; i++) {
         auto t = bc.read(4);
         NPARENT[i] = (int)num(t[0]); NGHOST[i] = (int)num(t[1]);
         NTYPE[i] = (int)num(t[2]); NSIDE[i] = (int)num(t[3]);
-        if (NGHOST[i] > maxid) maxid = NGHOST[i];
     }
 
     // thermodynamics and initial state (turbnstwod.f90:37-90)
@@ -271,29 +269,15 @@ int main() {
     // POSTPROCESS (solver_state.f90:230-283)
     std::printf(" Postprocessing.\n  \n");
     if (niter > 0) {
-        std::vector<double> U(maxid), V(maxid), T(maxid), PP(maxid);
-        if ((rc = tns_download_primitives(h, U.data(), V.data(), T.data(), PP.data())))
-            die(h, rc, "tns_download_primitives");
+        // node averages of P, U, V, T computed on the GPU (tns_node_averages)
         std::vector<double> s1(nods + 1, 0.0), s2(nods + 1, 0.0), s3(nods + 1, 0.0), s4(nods + 1, 0.0);
-        std::vector<int> cnt(nods + 1, 0);
-        auto add = [&](int k, int cell) {
-            cnt[k]++;
-            s1[k] += PP[cell]; s2[k] += U[cell]; s3[k] += V[cell]; s4[k] += T[cell];
-        };
-        for (int i = 0; i < neles; i++)
-            for (int j = 0; j < 4; j++) add(NOD[(size_t)j * neles + i], i);
-        for (int g = 0; g < nghosts; g++) {
-            const int np = NPARENT[g] - 1, ns = NSIDE[g], ng = NGHOST[g] - 1;
-            const int a = ns - 1, b = ns & 3;
-            add(NOD[(size_t)a * neles + np], ng);
-            add(NOD[(size_t)b * neles + np], ng);
-        }
+        if ((rc = tns_node_averages(h, s1.data() + 1, s2.data() + 1, s3.data() + 1, s4.data() + 1)))
+            die(h, rc, "tns_node_averages");
         FILE* tp = std::fopen("tec_plot.dat", "w");
         std::fprintf(tp, " VARIABLES = \"X\", \"Y\", \"U\", \"V\", \"P\", \"RHO\", \"MACH\", \"T\"\n");
         std::fprintf(tp, " ZONE F = FEPOINT, ET = QUADRILATERAL, N = %12d , E = %12d\n", nods, neles);
         for (int i = 1; i <= nods; i++) {
-            const double d = (double)cnt[i];
-            const double PNN = s1[i] / d, UNN = s2[i] / d, VNN = s3[i] / d, TNN = s4[i] / d;
+            const double PNN = s1[i], UNN = s2[i], VNN = s3[i], TNN = s4[i];
             const double AMN = std::sqrt(UNN * UNN + VNN * VNN) / std::sqrt(P.gama * RR * TNN);
             const double RON = PNN / (RR * TNN);
             std::fprintf(tp, "%s%s%s%s%s%s%s%s\n", ld(X[i]).c_str(), ld(Y[i]).c_str(), ld(UNN).c_str(),

@@ -23,7 +23,8 @@ NOALLOC_MAX_CELLS = 256 * 4 * 8192
 EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
            "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
-           "tns_last_error", "tns_destroy", "tns_time_step_noalloc")
+           "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
+           "tns_boundary_integrals")
 
 
 class TnsMesh(C.Structure):
@@ -68,6 +69,8 @@ def load(path: str = LIB_PATH):
     L.tns_download_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_download_primitives.argtypes = [vp, dp, dp, dp, dp]
     L.tns_debug_fetch.argtypes = [vp, ip, dp]
+    L.tns_node_averages.argtypes = [vp, dp, dp, dp, dp]
+    L.tns_boundary_integrals.argtypes = [vp, ip, ip, dp]
     L.tns_set_stream.argtypes = [vp, vp]
     L.tns_profile.argtypes = [vp, ip]
     L.tns_kernel_times.argtypes = [vp, ip, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]

@@ -59,7 +59,7 @@ def wall_force(mesh, prims, amol: float, iaxis: int, side: int = None, wall_type
     """Pressure force sum(p S) over the wall faces (per radian when IAXIS=1)."""
     _, _, pf, _, _ = _face_state(mesh, prims, amol)
     sx, sy, _, _ = face_vectors(mesh, iaxis)
-    sel = mesh.ntype == wall_type
+    sel = np.ones(mesh.nghosts, bool) if wall_type is None else mesh.ntype == wall_type
     if side is not None:
         sel &= mesh.nside == side
     return np.array([np.sum(pf[sel] * sx[sel]), np.sum(pf[sel] * sy[sel])])

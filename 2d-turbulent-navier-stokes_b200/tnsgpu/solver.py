@@ -113,6 +113,18 @@ class Solver:
         self._check(self.L.tns_download_primitives(self.h, *(out[k].ctypes.data for k in range(4))))
         return out
 
+    def node_averages(self) -> np.ndarray:
+        """[4, NODS] P, U, V, T node averages of POSTPROCESS (computed on the GPU)."""
+        out = np.zeros((4, self.mesh.nods))
+        self._check(self.L.tns_node_averages(self.h, *(out[k].ctypes.data for k in range(4))))
+        return out
+
+    def boundary_integrals(self, btype: int = 0, side: int = 0) -> np.ndarray:
+        """[sum P*SX, sum P*SY, sum RHO*(U*SX+V*SY), sum |S|] over matching boundary faces."""
+        out = np.zeros(4)
+        self._check(self.L.tns_boundary_integrals(self.h, int(btype), int(side), out.ctypes.data))
+        return out
+
     def debug(self, which: int) -> np.ndarray:
         cnt = {0: 5, 1: 4, 2: 1}[which]
         out = np.zeros((cnt, self.mesh.neles))

@@ -95,6 +95,20 @@ int tns_download_state(tns_handle *h, double *c1, double *c2, double *c3, double
  * id.  Feeds POSTPROCESS (solver_state.f90:230-283). */
 int tns_download_primitives(tns_handle *h, double *u, double *v, double *t, double *p);
 
+/* POSTPROCESS on the GPU (solver_state.f90:237-281): node averages of P, U, V, T of the
+ * last stage (cells in element order, then ghosts in bc.in order, divided by their
+ * count), scattered to node ids: pn[id-1], id = 1..NODS.  tec_plot.dat's P[bar], RHO and
+ * MACH follow from these (solver_state.f90:272-278). */
+int tns_node_averages(tns_handle *h, double *pn, double *un, double *vn, double *tn);
+
+/* Boundary integrals on the GPU over the faces whose bc.in line has NTYPE == type and
+ * NSIDE == side (0 = any), with the face state (parent + ghost)/2 of the last stage and
+ * the face vector S of geometry.f90:77-99 (per radian when IAXIS=1):
+ * out[0] = sum P*SX, out[1] = sum P*SY (pressure force on those faces), out[2] =
+ * sum RHO*(U*SX + V*SY) (mass flow out through them), out[3] = sum |S|.  No reference
+ * counterpart (THRUST is declared in solver_state.f90:40 but never computed). */
+int tns_boundary_integrals(tns_handle *h, int type, int side, double out[4]);
+
 /* Frozen terms of the last iteration, for checking: which = 0: D241..D245 (5 arrays),
  * 1: VISU, VISV, VIST, VISR (4), 2: DT (1).  out holds count*NELES doubles, cell order
  * 1..NELES per array. */
