@@ -1,0 +1,405 @@
+// tns_batch_api.cu -- batch runtime: many solver handles advanced together.
+//
+// A batch co-schedules cases created with tns_create (any sizes, any parameters, one
+// precision mode).  Each kernel phase of an RK4 iteration (dissipation pre-pass, frozen
+// viscous flux, four stages) is ONE launch over a table of (case, tile j, tile i)
+// entries covering every active case, so small cases share the GPU instead of each
+// paying a full set of launches on a mostly idle device.  One iteration per state parity
+// (mixed ping-pong) and monitor mode is captured as a CUDA graph; the graphs are
+// re-captured when the set of active cases changes, with the tile table compacted to
+// the active cases.  Per-case residual records drive a per-case stop criterion
+// (convergence masking) and a case whose state turns non-finite is masked off while the
+// others carry on.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tns_handle.h"
+#include "tns_tile.cuh"
+
+using tns::BatchCase;
+
+struct tns_batch {
+    std::string err;
+    std::vector<tns_handle*> cases;
+    int precision = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<BatchCase> desc;          // host copy of the device descriptors
+    std::vector<int> cur_at_desc;         // mixed: member parity the descriptors map
+    std::vector<int> active, failed;      // host masks
+    std::vector<int> active_at_capture;
+    DevBuf<BatchCase> d_desc;
+    DevBuf<int> d_active;
+    DevBuf<int4> d_tiles;
+    DevBuf<unsigned long long> d_cdiff;   // [ncases][5]
+    DevBuf<unsigned int> d_status;        // [ncases]
+    unsigned long long* h_cdiff = nullptr;  // pinned [ncases][5]
+    unsigned int* h_status = nullptr;       // pinned [ncases]
+    int ntiles = 0;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [monitor][parity]
+    long long per_iter[2] = {0, 0};
+    long long launches = 0;
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return TNS_OK;
+        return fail(TNS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+    void drop_graphs() {
+        for (auto& row : graph)
+            for (auto& g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+    }
+};
+
+namespace {
+
+// Descriptor of case k, mapping parity 0 to the member's current state buffer.
+BatchCase describe(tns_batch* b, int k) {
+    tns_handle* h = b->cases[k];
+    BatchCase c{};
+    c.P = h->P;
+    c.M = h->M;
+    c.qa = h->state();
+    c.qb = h->qb.p;
+    c.qc = h->qc.p;
+    c.d = h->d.p;
+    c.vis = h->vis.p;
+    c.dt = h->dt.p;
+    c.qa2 = h->precision == 1 ? h->other_state() : nullptr;
+    c.dqb = h->dqb.p;
+    c.dqc = h->dqc.p;
+    c.df = h->df.p;
+    c.visf = h->visf.p;
+    c.dtf = h->dtf.p;
+    c.dtmin = h->dtmin.p;
+    c.cdiff = b->d_cdiff.p + 5 * (size_t)k;
+    c.status = b->d_status.p + k;
+    return c;
+}
+
+int upload_descriptors(tns_batch* b) {
+    const int n = (int)b->cases.size();
+    b->desc.resize(n);
+    b->cur_at_desc.resize(n);
+    for (int k = 0; k < n; k++) {
+        b->desc[k] = describe(b, k);
+        b->cur_at_desc[k] = b->cases[k]->cur;
+    }
+    b->drop_graphs();
+    int rc;
+    if ((rc = b->cuda(cudaMemcpyAsync(b->d_desc.p, b->desc.data(), n * sizeof(BatchCase), cudaMemcpyHostToDevice,
+                                      b->stream), "cudaMemcpyAsync")))
+        return rc;
+    return b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
+}
+
+// Tile table of the active cases, case by case, j tiles fastest (the single-case grid
+// order).
+int upload_tiles(tns_batch* b) {
+    std::vector<int4> t;
+    const int n = (int)b->cases.size();
+    for (int k = 0; k < n; k++) {
+        if (!b->active[k]) continue;
+        const tns::Mesh& M = b->cases[k]->M;
+        const int tj = (M.nj + tns::TJ - 1) / tns::TJ, ti = (M.ni + tns::TI - 1) / tns::TI;
+        for (int y = 0; y < ti; y++)
+            for (int x = 0; x < tj; x++) t.push_back(make_int4(k, x, y, 0));
+    }
+    b->ntiles = (int)t.size();
+    int rc;
+    // the stream is idle here (masks change only between synchronised iterations)
+    if (!t.empty() && (rc = b->cuda(cudaMemcpyAsync(b->d_tiles.p, t.data(), t.size() * sizeof(int4),
+                                                    cudaMemcpyHostToDevice, b->stream), "cudaMemcpyAsync")))
+        return rc;
+    if ((rc = b->cuda(cudaMemcpyAsync(b->d_active.p, b->active.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                                      b->stream), "cudaMemcpyAsync")) ||
+        (rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize")))
+        return rc;
+    b->active_at_capture = b->active;
+    b->drop_graphs();
+    return TNS_OK;
+}
+
+// One RK4 iteration of every active case (the phases of enqueue_iteration_f64 /
+// enqueue_iteration_mx in tns_api.cu, each over the whole tile table).  The global
+// time step (LOCAL=0) and the type-6 port columns are per-case reductions, launched
+// per case that needs them.
+void enqueue_batch_iteration(tns_batch* b, int parity, bool monitor) {
+    cudaStream_t s = b->stream;
+    const bool mixed = b->precision == 1;
+    const int n = (int)b->cases.size();
+    const int nt = b->ntiles;
+    auto state = [&](int k) { return (mixed && parity) ? b->desc[k].qa2 : b->desc[k].qa; };
+    for (int k = 0; k < n; k++) {
+        if (!b->active[k]) continue;
+        tns_handle* h = b->cases[k];
+        if (!h->P.local) {
+            tns::launch_dtmin(h->P, h->M, state(k), h->partial.p, h->counter.p, h->dtmin.p, s);
+            b->launches++;
+        }
+    }
+    auto phase = [&](int kernel, int stage) {
+        if (mixed)
+            tns::launch_batch_mx(b->d_desc.p, b->d_tiles.p, b->d_active.p, nt, kernel, parity, stage,
+                                 monitor ? 1 : 0, s);
+        else
+            tns::launch_batch_f64(b->d_desc.p, b->d_tiles.p, b->d_active.p, nt, kernel, stage, monitor ? 1 : 0, s);
+        b->launches++;
+    };
+    phase(0, 0);
+    if (monitor) cudaMemsetAsync(b->d_cdiff.p, 0, 5 * (size_t)n * sizeof(unsigned long long), s);
+    for (int st = 0; st < 4; st++) {
+        for (int k = 0; k < n; k++) {
+            tns_handle* h = b->cases[k];
+            const int np = (int)h->port_ghosts.size();
+            if (!b->active[k] || !np) continue;
+            if (mixed) {
+                const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
+                tns::launch_gport_mx(h->P, h->M, state(k), in[st], h->ports.p, np, h->gport.p, s);
+            } else {
+                const double* in[4] = {b->desc[k].qa, h->qb.p, h->qc.p, h->qb.p};
+                tns::launch_gport(h->P, h->M, in[st], h->ports.p, np, h->gport.p, s);
+            }
+            b->launches++;
+        }
+        if (st == 0) phase(1, 0);
+        phase(2, st);
+    }
+}
+
+int ensure_batch_graph(tns_batch* b, int monitor, int parity) {
+    cudaGraphExec_t* g = &b->graph[monitor][parity];
+    if (*g) return TNS_OK;
+    int rc;
+    if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
+    const long long before = b->launches;
+    enqueue_batch_iteration(b, parity, monitor != 0);
+    b->per_iter[monitor] = b->launches - before;
+    b->launches = before;
+    cudaGraph_t graph;
+    if ((rc = b->cuda(cudaStreamEndCapture(b->stream, &graph), "capture"))) return rc;
+    rc = b->cuda(cudaGraphInstantiate(g, graph, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(graph);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tns_batch_create(tns_handle* const* cases, int ncases, tns_batch** out) {
+    if (!out) return TNS_ERR_ARG;
+    *out = nullptr;
+    if (!cases || ncases <= 0) return TNS_ERR_ARG;
+    tns_batch* b = new tns_batch();
+    *out = b;
+    for (int k = 0; k < ncases; k++) {
+        if (!cases[k]) return b->fail(TNS_ERR_ARG, "tns_batch_create: case %d is a null handle", k);
+        for (int j = 0; j < k; j++)
+            if (cases[j] == cases[k]) return b->fail(TNS_ERR_ARG, "tns_batch_create: case %d repeats case %d", k, j);
+        if (!cases[k]->qa.p) return b->fail(TNS_ERR_STATE, "tns_batch_create: case %d was not created", k);
+    }
+    b->cases.assign(cases, cases + ncases);
+    b->precision = cases[0]->precision;
+    for (int k = 1; k < ncases; k++)
+        if (cases[k]->precision != b->precision)
+            return b->fail(TNS_ERR_ARG, "tns_batch_create: case %d has precision %d, case 0 has %d", k,
+                           cases[k]->precision, b->precision);
+    long long ntiles = 0;
+    for (tns_handle* h : b->cases)
+        ntiles += (long long)((h->M.nj + tns::TJ - 1) / tns::TJ) * ((h->M.ni + tns::TI - 1) / tns::TI);
+    if (ntiles > 0x7fffffffLL) return b->fail(TNS_ERR_TOO_LARGE, "tns_batch_create: %lld tiles", ntiles);
+    int rc;
+    if ((rc = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = b->cuda(b->d_desc.alloc(ncases), "cudaMalloc")) || (rc = b->cuda(b->d_active.alloc(ncases), "cudaMalloc")) ||
+        (rc = b->cuda(b->d_tiles.alloc((size_t)ntiles), "cudaMalloc")) ||
+        (rc = b->cuda(b->d_cdiff.alloc(5 * (size_t)ncases), "cudaMalloc")) ||
+        (rc = b->cuda(b->d_status.alloc(ncases), "cudaMalloc")) ||
+        (rc = b->cuda(cudaMallocHost((void**)&b->h_cdiff, 5 * ncases * sizeof(unsigned long long)), "cudaMallocHost")) ||
+        (rc = b->cuda(cudaMallocHost((void**)&b->h_status, ncases * sizeof(unsigned int)), "cudaMallocHost")) ||
+        (rc = b->cuda(cudaMemset(b->d_status.p, 0, ncases * sizeof(unsigned int)), "cudaMemset")))
+        return rc;
+    b->active.assign(ncases, 1);
+    b->failed.assign(ncases, 0);
+    if ((rc = upload_descriptors(b))) return rc;
+    return upload_tiles(b);
+}
+
+int tns_batch_set_active(tns_batch* b, const int* active) {
+    if (!b || !active) return TNS_ERR_ARG;
+    const int n = (int)b->cases.size();
+    bool cleared = false;
+    for (int k = 0; k < n; k++) {
+        b->active[k] = active[k] ? 1 : 0;
+        if (active[k] && b->failed[k]) {  // re-activating a failed case clears its status word
+            b->failed[k] = 0;
+            b->h_status[k] = 0;
+            cleared = true;
+        }
+    }
+    int rc;
+    if (cleared && ((rc = b->cuda(cudaMemcpyAsync(b->d_status.p, b->h_status, n * sizeof(unsigned int),
+                                                  cudaMemcpyHostToDevice, b->stream), "cudaMemcpyAsync")) ||
+                    (rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))))
+        return rc;
+    return upload_tiles(b);
+}
+
+int tns_batch_get_active(tns_batch* b, int* active) {
+    if (!b || !active) return TNS_ERR_ARG;
+    for (size_t k = 0; k < b->cases.size(); k++) active[k] = b->active[k];
+    return TNS_OK;
+}
+
+int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio, double* cdiff_ref,
+                  double* cdiff_out, int max_records, int* n_records, int* iterations, int* case_status) {
+    if (!b) return TNS_ERR_ARG;
+    const int n = (int)b->cases.size();
+    if (n_records)
+        for (int k = 0; k < n; k++) n_records[k] = 0;
+    if (iterations)
+        for (int k = 0; k < n; k++) iterations[k] = 0;
+    if (case_status)
+        for (int k = 0; k < n; k++) case_status[k] = b->failed[k] ? TNS_ERR_NONFINITE : TNS_OK;
+    if (stop_ratio > 0.0 && monitor_every <= 0)
+        return b->fail(TNS_ERR_ARG, "tns_batch_run: a stop ratio needs monitor_every > 0");
+    int rc;
+    for (int k = 0; k < n; k++) {
+        tns_handle* h = b->cases[k];
+        if (!h->have_state) return b->fail(TNS_ERR_STATE, "tns_batch_run: case %d has no state uploaded", k);
+        // work a member has queued on its own stream finishes first
+        if ((rc = b->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    }
+    if (niter <= 0) return TNS_OK;
+    bool remap = false;
+    for (int k = 0; k < n; k++) remap |= b->cases[k]->cur != b->cur_at_desc[k];
+    if (remap && (rc = upload_descriptors(b))) return rc;
+    if (b->active != b->active_at_capture && (rc = upload_tiles(b))) return rc;
+
+    std::vector<int> ran(n, 0), nrec(n, 0);
+    std::vector<double> ref(5 * (size_t)n, 0.0);
+    const bool stop = stop_ratio > 0.0;
+    if (stop)
+        for (int k = 0; k < n; k++)
+            for (int m = 0; m < 5; m++) ref[5 * k + m] = cdiff_ref ? cdiff_ref[5 * k + m] : 0.0;
+    auto set_ref = [&](int k) {
+        for (int m = 0; m < 5; m++) if (!(ref[5 * k + m] > 0.0)) return false;
+        return true;
+    };
+    int parity = 0;
+    bool any_failed = false;
+    auto active_count = [&]() {
+        int a = 0;
+        for (int k = 0; k < n; k++) a += b->active[k];
+        return a;
+    };
+    for (int it = 1; it <= niter && active_count() > 0; it++) {
+        // the run's first iteration is monitored when it sets the stop reference
+        bool needs_ref = false;
+        if (stop)
+            for (int k = 0; k < n; k++) needs_ref |= b->active[k] && !set_ref(k);
+        const bool monitor = (monitor_every > 0 && it % monitor_every == 0) || (it == 1 && needs_ref);
+        if (b->active != b->active_at_capture && (rc = upload_tiles(b))) return rc;
+        if ((rc = ensure_batch_graph(b, monitor ? 1 : 0, parity))) return rc;
+        if ((rc = b->cuda(cudaGraphLaunch(b->graph[monitor ? 1 : 0][parity], b->stream), "cudaGraphLaunch")))
+            return rc;
+        b->launches += b->per_iter[monitor ? 1 : 0];
+        for (int k = 0; k < n; k++) ran[k] += b->active[k];
+        if (b->precision == 1) parity ^= 1;
+        if (!monitor && it != niter) continue;
+        // residual records, status words and the masks, at the monitor cadence and at the end
+        if ((rc = b->cuda(cudaMemcpyAsync(b->h_status, b->d_status.p, n * sizeof(unsigned int),
+                                          cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+        if (monitor && (rc = b->cuda(cudaMemcpyAsync(b->h_cdiff, b->d_cdiff.p, 5 * n * sizeof(unsigned long long),
+                                                     cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+        if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))) return rc;
+        for (int k = 0; k < n; k++) {
+            if (!b->active[k]) continue;
+            if (b->h_status[k] & 1u) {
+                b->failed[k] = 1;
+                b->active[k] = 0;
+                any_failed = true;
+                if (case_status) case_status[k] = TNS_ERR_NONFINITE;
+                continue;
+            }
+            if (!monitor) continue;
+            double v[5];
+            for (int m = 0; m < 5; m++) {
+                std::memcpy(&v[m], &b->h_cdiff[5 * k + m], 8);
+                const double init = m < 4 ? 1.0e-10 : 1.0e-20;  // constants.f90:44-45
+                v[m] = v[m] >= init ? v[m] : init;
+            }
+            const bool record = monitor_every > 0 && it % monitor_every == 0;
+            if (record) {
+                if (cdiff_out && nrec[k] < max_records)
+                    for (int m = 0; m < 5; m++) cdiff_out[((size_t)k * max_records + nrec[k]) * 5 + m] = v[m];
+                nrec[k]++;
+            }
+            if (!stop) continue;
+            if (!set_ref(k)) {
+                for (int m = 0; m < 5; m++) ref[5 * k + m] = v[m];
+                continue;
+            }
+            double worst = 0.0;
+            for (int m = 0; m < 5; m++) worst = std::fmax(worst, v[m] / ref[5 * k + m]);
+            if (worst <= stop_ratio) b->active[k] = 0;  // converged: masked off
+        }
+    }
+    // members continue from where the batch left them
+    for (int k = 0; k < n; k++) {
+        tns_handle* h = b->cases[k];
+        if (b->precision == 1) h->cur = b->cur_at_desc[k] ^ (ran[k] & 1);
+        if (ran[k]) h->have_run = true;
+        if (iterations) iterations[k] = ran[k];
+        if (n_records) n_records[k] = std::min(nrec[k], max_records);
+    }
+    if (b->precision == 1) {
+        // the descriptors now map parity 0 to a stale buffer for odd-iteration cases
+        for (int k = 0; k < n; k++)
+            if (b->cases[k]->cur != b->cur_at_desc[k] && (rc = upload_descriptors(b))) return rc;
+    }
+    if (stop && cdiff_ref)
+        for (int k = 0; k < n; k++)
+            for (int m = 0; m < 5; m++) cdiff_ref[5 * k + m] = ref[5 * k + m];
+    if ((rc = b->cuda(cudaGetLastError(), "kernel launch"))) return rc;
+    if (any_failed) return b->fail(TNS_ERR_NONFINITE, "a case's state became non-finite (NaN/Inf); it was masked off");
+    return TNS_OK;
+}
+
+long long tns_batch_launch_count(tns_batch* b) { return b ? b->launches : -1; }
+
+const char* tns_batch_last_error(tns_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void tns_batch_destroy(tns_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    b->drop_graphs();
+    b->d_desc.release();
+    b->d_active.release();
+    b->d_tiles.release();
+    b->d_cdiff.release();
+    b->d_status.release();
+    if (b->h_cdiff) cudaFreeHost(b->h_cdiff);
+    if (b->h_status) cudaFreeHost(b->h_status);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // extern "C"

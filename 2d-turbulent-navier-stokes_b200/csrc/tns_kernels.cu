@@ -14,6 +14,7 @@
 #include "tns_device.cuh"
 #include "tns_kernels.h"
 #include "tns_tile.cuh"
+#include "tns_batch.cuh"
 
 namespace tns {
 
@@ -56,11 +57,11 @@ struct StageArgs {
 
 // One RK stage (turbnstwod.f90:204-227, boundary.f90:24-48, source_terms.f90:24-104,
 // residual.f90:23-83) on a TI x TJ tile with its halo staged in shared memory.
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage(Params P, Mesh M, StageArgs A) {
+__device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const StageArgs& A, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     load_nodes(M, i0, j0, S.nx, S.ny);
     __syncthreads();
@@ -173,6 +174,10 @@ __global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage(Params P, Me
     }
 }
 
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage(Params P, Mesh M, StageArgs A) {
+    stage_tile(P, M, A, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------- viscous kernel
 
 // Faces owned by a tile: i-faces (between cells (i-1,j) and (i,j)) for i in i0..i0+TI,
@@ -218,12 +223,12 @@ __device__ __forceinline__ void face_flux(const Params& P, const ViscSmem& S, in
 // Frozen viscous flux VIS of Q_old (viscous.f90:29-217): nodal averages, then each face
 // of the tile once; a cell adds its four faces in order 1..4, negating the faces that
 // were evaluated in the neighbour's orientation.
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous(Params P, Mesh M, const double* __restrict__ q,
-                                                      double* __restrict__ vis) {
+__device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, const double* __restrict__ q,
+                                             double* __restrict__ vis, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ViscSmem& S = *reinterpret_cast<ViscSmem*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     load_nodes(M, i0, j0, S.nx, S.ny);
     __syncthreads();
@@ -338,6 +343,11 @@ __global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous(Params P, M
     }
 }
 
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous(Params P, Mesh M, const double* __restrict__ q,
+                                                      double* __restrict__ vis) {
+    viscous_tile(P, M, q, vis, blockIdx.x, blockIdx.y);
+}
+
 // --------------------------------------------------------- dissipation kernel
 
 constexpr int DW = TJ + 4;             // halo-2 slot grid (TI+4) x (TJ+4)
@@ -372,14 +382,15 @@ __device__ __forceinline__ double local_dt(const Params& P, double c1, double c2
 }
 
 template <class OutT>
-__global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, DissArgs<OutT> A) {
+__device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M, const DissArgs<OutT>& A,
+                                                 int bx, int by) {
     extern __shared__ double smem[];
     double* sd = smem;                  // NDF x NDSLOT
     double* sr = sd + NDF * NDSLOT;     // NRF x NRSLOT
     double* snx = sr + NRF * NRSLOT;
     double* sny = snx + NNODE;
     const size_t ncell = (size_t)M.ni * M.nj;
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
 
     for (int s = tid; s < NNODE; s += NTHREADS) {
@@ -499,6 +510,11 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, Diss
         }
         A.d[m * ncell + cell] = (OutT)(D2 - D4);
     }
+}
+
+template <class OutT>
+__global__ void __launch_bounds__(NTHREADS) k_dissipation(Params P, Mesh M, DissArgs<OutT> A) {
+    dissipation_tile<OutT>(P, M, A, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------- time step min
@@ -734,6 +750,46 @@ __global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ pri
     }
 }
 
+// ------------------------------------------------------------ batched kernels
+
+// One launch per kernel advances every active case of a batch; block b works on tile
+// tiles[b] = (case, tile j, tile i) with its case's parameters and buffers.
+__global__ void __launch_bounds__(NTHREADS) k_dissipation_batch(const BatchCase* __restrict__ cases,
+                                                                const int4* __restrict__ tiles,
+                                                                const int* __restrict__ active) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    const BatchCase& c = cases[t.x];
+    DissArgs<double> A{c.qa, c.d, c.dt, c.dtmin};
+    dissipation_tile<double>(B.P, B.M, A, t.y, t.z);
+}
+
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous_batch(const BatchCase* __restrict__ cases,
+                                                                          const int4* __restrict__ tiles,
+                                                                          const int* __restrict__ active) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    viscous_tile(B.P, B.M, cases[t.x].qa, cases[t.x].vis, t.y, t.z);
+}
+
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage_batch(const BatchCase* __restrict__ cases,
+                                                                         const int4* __restrict__ tiles,
+                                                                         const int* __restrict__ active,
+                                                                         int stage, int monitor) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    const BatchCase& c = cases[t.x];
+    const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
+    const double* in[4] = {c.qa, c.qb, c.qc, c.qb};
+    double* out[4] = {c.qb, c.qc, c.qb, c.qa};
+    StageArgs A{in[stage], c.qa, out[stage], c.d, c.vis, c.dt, c.dtmin, alpha[stage],
+                (monitor && stage == 3) ? c.cdiff : nullptr, stage == 3 ? c.status : nullptr};
+    stage_tile(B.P, B.M, A, t.y, t.z);
+}
+
 // ------------------------------------------------------------------ launchers
 
 static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
@@ -749,8 +805,28 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(k_dissipation<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)diss_smem_bytes());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_dissipation<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)diss_smem_bytes());
+    e = cudaFuncSetAttribute(k_dissipation<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diss_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_dissipation_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diss_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_viscous_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)visc_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_stage_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)stage_smem_bytes());
+}
+
+void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                      int kernel, int stage, int monitor, cudaStream_t s) {
+    const dim3 blk(TJ, TI);
+    if (kernel == 0)
+        k_dissipation_batch<<<ntiles, blk, diss_smem_bytes(), s>>>(cases, tiles, active);
+    else if (kernel == 1)
+        k_viscous_batch<<<ntiles, blk, visc_smem_bytes(), s>>>(cases, tiles, active);
+    else
+        k_stage_batch<<<ntiles, blk, stage_smem_bytes(), s>>>(cases, tiles, active, stage, monitor);
 }
 
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,

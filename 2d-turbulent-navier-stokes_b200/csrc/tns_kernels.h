@@ -5,6 +5,7 @@
 #include <stddef.h>
 
 #include "tns_device.cuh"
+#include "tns_batch.cuh"
 
 namespace tns {
 
@@ -35,6 +36,12 @@ void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* ou
 void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStream_t s);
 void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
                           double* out, cudaStream_t s);
+
+// batched multi-case kernels: kernel 0 dissipation, 1 viscous, 2 stage
+void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                      int kernel, int stage, int monitor, cudaStream_t s);
+void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                     int kernel, int parity, int stage, int monitor, cudaStream_t s);
 
 // mixed FP32/FP64 path (tns_kernels_mx.cu)
 cudaError_t configure_kernels_mx();

@@ -15,6 +15,7 @@
 #include "tns_device.cuh"
 #include "tns_kernels.h"
 #include "tns_tile.cuh"
+#include "tns_batch.cuh"
 
 namespace tns {
 
@@ -80,12 +81,14 @@ __device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p
 #ifndef TNS_VISC_MX_MINB
 #define TNS_VISC_MX_MINB 3
 #endif
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
+// One stage on tile (bx, by) of a mesh; the single-case and the batched kernels wrap it.
+__device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, const StageArgsMx& A,
+                                              int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmemMx& S = *reinterpret_cast<StageSmemMx*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
     const StateMixed st{A.cold, A.dqin, ncell};
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     if (tid == 0) {
         // tile reference flux: the first cell of the tile
@@ -270,6 +273,10 @@ __global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx(Params
     }
 }
 
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
+    stage_mx_tile(P, M, A, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------- viscous kernel
 
 constexpr int NIFM = (TI + 1) * TJ;
@@ -350,12 +357,12 @@ __device__ __forceinline__ void face_flux_mx(const Params& P, const ViscSmemMx& 
     out[3] = AMUEFF * DRX * sx + AMUEFF * DRY * sy;
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
-                                                         float* __restrict__ vis) {
+__device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, const double* __restrict__ q,
+                                                float* __restrict__ vis, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ViscSmemMx& S = *reinterpret_cast<ViscSmemMx*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     load_nodes(M, i0, j0, S.nx, S.ny);
     __syncthreads();
@@ -461,6 +468,11 @@ __global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx(Param
         vis[k * ncell + cell] = ((s1 * S.fj[k][f1] + S.fi[k][f2]) + S.fj[k][f3]) + s4 * S.fi[k][f4];
 }
 
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
+                                                         float* __restrict__ vis) {
+    viscous_mx_tile(P, M, q, vis, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------ dissipation kernel
 
 // JST dissipation (solver_state.f90:70-225) with FP64 state, pressure and every
@@ -489,13 +501,13 @@ __device__ __forceinline__ double local_dt_mx(const Params& P, double c1, double
     return cfldl / (fabs(VEL) + sqrt(P.gamrr * T));
 }
 
-__global__ void __launch_bounds__(NTHREADS) k_dissipation_mx(Params P, Mesh M, const double* __restrict__ q,
-                                                             float* __restrict__ dout, float* __restrict__ dtout,
-                                                             const double* __restrict__ dtmin) {
+__device__ __forceinline__ void dissipation_mx_tile(const Params& P, const Mesh& M, const double* __restrict__ q,
+                                                    float* __restrict__ dout, float* __restrict__ dtout,
+                                                    const double* __restrict__ dtmin, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     DissSmemMx& S = *reinterpret_cast<DissSmemMx*>(smem_raw);
     const size_t ncell = (size_t)M.ni * M.nj;
-    const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+    const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     load_nodes(M, i0, j0, S.nx, S.ny);
     for (int s = tid; s < NDSLOTM; s += NTHREADS) {
@@ -595,6 +607,12 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation_mx(Params P, Mesh M, c
     }
 }
 
+__global__ void __launch_bounds__(NTHREADS) k_dissipation_mx(Params P, Mesh M, const double* __restrict__ q,
+                                                             float* __restrict__ dout, float* __restrict__ dtout,
+                                                             const double* __restrict__ dtmin) {
+    dissipation_mx_tile(P, M, q, dout, dtout, dtmin, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------ port mass flux
 
 __global__ void k_gport_mx(Params P, Mesh M, const double* __restrict__ cold,
@@ -660,6 +678,48 @@ __global__ void k_prim_out_mx(Params P, Mesh M, const double* __restrict__ cold,
     out[3 * ntot + k] = p.p;
 }
 
+// ------------------------------------------------------------ batched kernels
+
+// Mixed-path batch: `parity` selects which of qa / qa2 holds each active case's state
+// (all active cases advance together, so they share it).
+__global__ void __launch_bounds__(NTHREADS) k_dissipation_mx_batch(const BatchCase* __restrict__ cases,
+                                                                   const int4* __restrict__ tiles,
+                                                                   const int* __restrict__ active, int parity) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    const BatchCase& c = cases[t.x];
+    dissipation_mx_tile(B.P, B.M, parity ? c.qa2 : c.qa, c.df, c.dtf, c.dtmin, t.y, t.z);
+}
+
+__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
+                                                                                const int4* __restrict__ tiles,
+                                                                                const int* __restrict__ active,
+                                                                                int parity) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    const BatchCase& c = cases[t.x];
+    viscous_mx_tile(B.P, B.M, parity ? c.qa2 : c.qa, c.visf, t.y, t.z);
+}
+
+__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx_batch(const BatchCase* __restrict__ cases,
+                                                                               const int4* __restrict__ tiles,
+                                                                               const int* __restrict__ active,
+                                                                               int parity, int stage, int monitor) {
+    __shared__ BatchBlock B;
+    const int4 t = batch_prologue(cases, tiles, active, B);
+    if (!B.active) return;
+    const BatchCase& c = cases[t.x];
+    const float alpha[4] = {0.25f, 1.0f / 3.0f, 0.5f, 1.0f};
+    const float* in[4] = {nullptr, c.dqb, c.dqc, c.dqb};
+    float* out[4] = {c.dqb, c.dqc, c.dqb, nullptr};
+    StageArgsMx A{parity ? c.qa2 : c.qa, in[stage], out[stage], stage == 3 ? (parity ? c.qa : c.qa2) : nullptr,
+                  c.df, c.visf, c.dtf, c.dtmin, alpha[stage],
+                  (monitor && stage == 3) ? c.cdiff : nullptr, stage == 3 ? c.status : nullptr};
+    stage_mx_tile(B.P, B.M, A, t.y, t.z);
+}
+
 // ------------------------------------------------------------------ launchers
 
 static dim3 tile_grid_mx(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
@@ -671,8 +731,28 @@ cudaError_t configure_kernels_mx() {
     e = cudaFuncSetAttribute(k_dissipation_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)diss_mx_smem_bytes());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_viscous_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)visc_mx_smem_bytes());
+    e = cudaFuncSetAttribute(k_viscous_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)visc_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_dissipation_mx_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diss_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_viscous_mx_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)visc_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_stage_mx_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)stage_mx_smem_bytes());
+}
+
+void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                     int kernel, int parity, int stage, int monitor, cudaStream_t s) {
+    const dim3 blk(TJ, TI);
+    if (kernel == 0)
+        k_dissipation_mx_batch<<<ntiles, blk, diss_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
+    else if (kernel == 1)
+        k_viscous_mx_batch<<<ntiles, blk, visc_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
+    else
+        k_stage_mx_batch<<<ntiles, blk, stage_mx_smem_bytes(), s>>>(cases, tiles, active, parity, stage, monitor);
 }
 
 void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, float* d, float* dt,

@@ -17,6 +17,8 @@ TNS_OK = 0
 ERRORS = {-1: "TNS_ERR_ARG", -2: "TNS_ERR_MESH", -3: "TNS_ERR_UNSUPPORTED",
           -4: "TNS_ERR_CUDA", -5: "TNS_ERR_NONFINITE", -6: "TNS_ERR_STATE",
           -7: "TNS_ERR_TOO_LARGE"}
+for _code, _name in ERRORS.items():
+    globals()[_name] = _code
 NOALLOC_MAX_CELLS = 256 * 4 * 8192
 
 # every symbol include/tnsgpu.h declares
@@ -24,7 +26,10 @@ EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run
            "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
-           "tns_boundary_integrals")
+           "tns_boundary_integrals", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
+           "tns_batch_get_active", "tns_batch_launch_count", "tns_batch_last_error", "tns_batch_destroy")
+NOT_INT = ("tns_launch_count", "tns_last_error", "tns_destroy", "tns_batch_launch_count",
+           "tns_batch_last_error", "tns_batch_destroy")
 
 
 class TnsMesh(C.Structure):
@@ -81,8 +86,18 @@ def load(path: str = LIB_PATH):
     L.tns_destroy.argtypes = [vp]
     L.tns_destroy.restype = None
     L.tns_time_step_noalloc.argtypes = [vp, vp, C.c_longlong, C.POINTER(TnsParams), vp, vp, vp]
+    L.tns_batch_create.argtypes = [vp, ip, C.POINTER(vp)]
+    L.tns_batch_run.argtypes = [vp, ip, ip, C.c_double, dp, dp, ip, vp, vp, vp]
+    L.tns_batch_set_active.argtypes = [vp, vp]
+    L.tns_batch_get_active.argtypes = [vp, vp]
+    L.tns_batch_launch_count.argtypes = [vp]
+    L.tns_batch_launch_count.restype = C.c_longlong
+    L.tns_batch_last_error.argtypes = [vp]
+    L.tns_batch_last_error.restype = C.c_char_p
+    L.tns_batch_destroy.argtypes = [vp]
+    L.tns_batch_destroy.restype = None
     for n in EXPORTS:
-        if n not in ("tns_launch_count", "tns_last_error", "tns_destroy"):
+        if n not in NOT_INT:
             getattr(L, n).restype = C.c_int
     _lib = L
     return L

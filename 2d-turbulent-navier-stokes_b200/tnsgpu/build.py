@@ -6,7 +6,7 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
-SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu")
+SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu", "tns_batch_api.cu")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

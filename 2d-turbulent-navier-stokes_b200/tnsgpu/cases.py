@@ -21,9 +21,12 @@ Cases (sizes as named in the solver's benchmark configurations):
   port        -- axisymmetric 2.0 m x 0.1 m channel with a type-6 injecting port wall.
   nozzle_2d   -- small 2-D converging-diverging channel with the BC layout of the
                  reference's example case (axis 4 / wall 5 / inlet 2 / outflow 3).
+  ramp_sweep  -- a seeded parameter sweep of ramp cases (mesh size, ramp angle, P0,
+                 T0) for the batched solver.
 """
 from __future__ import annotations
 
+import dataclasses
 import math
 from typing import Callable, Optional
 
@@ -233,6 +236,46 @@ def noisy_restart_state(f: Flow, neles: int, seed: int = 0, amp: float = 1.0e-3)
     rng = np.random.default_rng(seed)
     c[0] = c[0] * (1.0 + rng.uniform(-amp, amp, neles))
     return c, rinit
+
+
+@dataclasses.dataclass
+class SweepCase:
+    """One ramp case of a parameter sweep (a line of a batch manifest)."""
+
+    name: str
+    nx: int
+    ny: int
+    angle_deg: float
+    p0: float
+    t0: float
+    amachinit: float = 0.01
+
+    def mesh(self) -> Mesh:
+        return ramp_mesh(self.nx, self.ny, self.angle_deg)
+
+    def flow(self, niter: int = 2000) -> Flow:
+        f = ramp_flow(niter, self.p0, self.t0)
+        f.istart = 0
+        f.amachinit = self.amachinit
+        return f
+
+
+def ramp_sweep(n: int = 64, seed: int = 0, nx_range=(96, 512), ny_range=(32, 192),
+               step: int = 32, angle_range=(5.0, 15.0), p0_range=(2.0e5, 1.0e6),
+               t0_range=(250.0, 400.0), amachinit: float = 0.01):
+    """n ramp cases drawn from ``numpy.random.default_rng(seed)``: per case, in this
+    order, nx and ny uniform over the multiples of ``step`` in their ranges (inclusive),
+    then the ramp angle, P0 and T0 uniform in their ranges.  Cold start at AMACHINIT."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(rng.integers(nx_range[0] // step, nx_range[1] // step + 1)) * step
+        ny = int(rng.integers(ny_range[0] // step, ny_range[1] // step + 1)) * step
+        ang = float(rng.uniform(*angle_range))
+        p0 = float(rng.uniform(*p0_range))
+        t0 = float(rng.uniform(*t0_range))
+        out.append(SweepCase(f"ramp{k:03d}_{nx}x{ny}", nx, ny, ang, p0, t0, amachinit))
+    return out
 
 
 CASES = {

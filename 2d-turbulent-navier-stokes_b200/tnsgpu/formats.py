@@ -7,6 +7,8 @@
 * ``bc.in``    -- ``NGHOSTS`` then ``NPARENT NGHOST NTYPE NSIDE`` lines (geometry.f90:47-52).
 * ``restart.in`` -- NELES lines of C1..C5, then RTRED, NPSEUDO, RINIT, NITEROLD
   (turbnstwod.f90:73-85, 186-195).
+* batch manifest -- no reference counterpart: one line per case of a parameter sweep,
+  ``name nx ny angle_deg p0 t0 amachinit`` after a ``#`` header line.
 
 Values are written with Python's shortest round-trip ``repr`` so a write/read cycle is
 exact; the Fortran list-directed reader accepts that form.
@@ -211,3 +213,32 @@ def write_case(dirpath: str, m: Mesh, f: Flow) -> None:
     os.makedirs(dirpath, exist_ok=True)
     write_grid_bc(os.path.join(dirpath, f.fnamegrid), os.path.join(dirpath, f.fnamebc), m)
     write_flow(os.path.join(dirpath, "flow.in"), f)
+
+
+MANIFEST_FIELDS = ("name", "nx", "ny", "angle_deg", "p0", "t0", "amachinit")
+
+
+def write_manifest(path: str, sweep) -> None:
+    """Batch manifest of a sweep (objects with the MANIFEST_FIELDS attributes)."""
+    with open(path, "w") as fh:
+        fh.write("# " + " ".join(MANIFEST_FIELDS) + "\n")
+        for c in sweep:
+            fh.write(" ".join(repr(getattr(c, k)) if k != "name" else c.name for k in MANIFEST_FIELDS) + "\n")
+
+
+def read_manifest(path: str) -> list:
+    """Rows of a batch manifest as dicts of MANIFEST_FIELDS (ints for nx, ny)."""
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            line = line.strip()
+            if not line or line.startswith("#"):
+                continue
+            t = line.split()
+            if len(t) != len(MANIFEST_FIELDS):
+                raise ValueError(f"{path}: manifest line needs {len(MANIFEST_FIELDS)} values: {line!r}")
+            row = {"name": t[0], "nx": int(t[1]), "ny": int(t[2])}
+            for k, v in zip(MANIFEST_FIELDS[3:], t[3:]):
+                row[k] = float(v)
+            rows.append(row)
+    return rows

@@ -160,6 +160,40 @@ int tns_time_step_noalloc(const double *d_q, const double *d_cfldl, long long nc
                           const tns_params *params, double *d_dt, double *d_dtmin, void *stream);
 void tns_destroy(tns_handle *h);
 
+/* ---- Batch of cases (no counterpart in the reference, which solves one case per run).
+ * A batch advances several handles made by tns_create together: every kernel phase of
+ * an RK4 iteration is one launch over the tiles of all active cases.  The cases may
+ * differ in mesh size, geometry and parameters; they share one precision mode.  State
+ * moves in and out through each member's tns_upload_state / tns_download_state /
+ * tns_download_primitives, before and after tns_batch_run.  The batch borrows the
+ * handles: destroy the batch first. */
+typedef struct tns_batch tns_batch;
+
+int tns_batch_create(tns_handle *const *cases, int ncases, tns_batch **out);
+
+/* Runs up to niter RK4 iterations of every active case.  Residual records (the five
+ * CDIFF values of tns_run) are taken every monitor_every-th iteration of the call and
+ * written to cdiff_out[case][max_records][5]; n_records[case] receives each count.
+ * stop_ratio > 0 enables convergence masking: a case stops (becomes inactive) at the
+ * first record where max_k CDIFF_k / REF_k <= stop_ratio.  REF is cdiff_ref[case][5]
+ * when its entries are positive; otherwise the first iteration of the call is monitored
+ * and its CDIFF becomes REF (written back to cdiff_ref when non-NULL, so a later call
+ * can continue the criterion).  iterations[case] receives the iterations each case ran.
+ * A case whose state becomes non-finite is masked off (case_status[case] =
+ * TNS_ERR_NONFINITE) while the others continue; the call then returns TNS_ERR_NONFINITE.
+ * Any output pointer may be NULL. */
+int tns_batch_run(tns_batch *b, int niter, int monitor_every, double stop_ratio, double *cdiff_ref,
+                  double *cdiff_out, int max_records, int *n_records, int *iterations,
+                  int *case_status);
+
+/* Per-case active mask (1 = iterate).  Re-activating a case that failed clears its
+ * failure: upload a finite state to it first. */
+int tns_batch_set_active(tns_batch *b, const int *active);
+int tns_batch_get_active(tns_batch *b, int *active);
+long long tns_batch_launch_count(tns_batch *b);
+const char *tns_batch_last_error(tns_batch *b);
+void tns_batch_destroy(tns_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

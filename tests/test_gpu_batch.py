@@ -1,0 +1,178 @@
+"""Batched solver (tns_batch_*) against the same cases solved one at a time.
+
+A batch runs the single-case tile code of every kernel phase, launched once over the
+tiles of all active cases, so each member's result must equal -- bit for bit -- the
+result of that case run alone through tns_run for the same number of iterations, in
+both precision modes.  The cases mix mesh sizes (including partial tiles), 2-D and
+axisymmetric flows, the global time step (LOCAL=0) and type-6 injection ports.
+"""
+import numpy as np
+import pytest
+
+from tnsgpu import _lib, cases, formats
+from tnsgpu.batch import Batch
+from tnsgpu.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _axis_sym(mesh):
+    mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    return mesh
+
+
+def _case_list():
+    ramp_b = cases.ramp_flow(p0=5.0e5, t0=350.0)
+    glob = formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})
+    out = [
+        ("ramp48x20", cases.ramp_mesh(48, 20), cases.ramp_flow(), "noisy"),
+        ("ramp40x36_12deg", cases.ramp_mesh(40, 36, 12.0), ramp_b, "noisy"),
+        ("nozzle2d", cases.nozzle_2d_mesh(40, 18), cases.nozzle_2d_flow(), "cold"),
+        ("plume_axis_sym", _axis_sym(cases.nozzle_plume_mesh(64, 24)), cases.nozzle_plume_flow(), "cold"),
+        ("global_dt", cases.ramp_mesh(40, 16), glob, "noisy"),
+        ("port", cases.port_mesh(64, 16), cases.port_flow(), "cold"),
+    ]
+    return out
+
+
+def _start(flow, mesh, kind, seed):
+    if kind == "noisy":
+        return cases.noisy_restart_state(flow, mesh.neles, seed=seed)
+    ri = formats.rinit_cold(flow)
+    return formats.cold_state(flow, mesh.neles, ri), ri
+
+
+def _members(precision, pick=None):
+    cl = _case_list()
+    if pick is not None:
+        cl = [cl[k] for k in pick]
+    out = []
+    for k, (name, mesh, flow, kind) in enumerate(cl):
+        c0, ri = _start(flow, mesh, kind, seed=k)
+        out.append((name, mesh, flow, c0, ri))
+    return out
+
+
+def _solo(mesh, flow, c0, ri, precision, chunks, monitor=0):
+    s = Solver(mesh, flow, ri, precision=precision)
+    s.upload(c0)
+    rec = []
+    for n in chunks:
+        if n:
+            rec.append(s.run(n, monitor))
+    out = s.download(), s.primitives()
+    s.close()
+    return out, rec
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_equals_solo_runs(precision):
+    mem = _members(precision)
+    solvers = []
+    for name, mesh, flow, c0, ri in mem:
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        solvers.append(s)
+    b = Batch(solvers)
+    # odd then even iteration counts: the mixed path's state parity crosses calls
+    r1 = b.run(3, monitor_every=0)
+    r2 = b.run(4, monitor_every=2)
+    assert list(r1.iterations) == [3] * len(mem) and list(r2.iterations) == [4] * len(mem)
+    assert all(len(r) == 2 for r in r2.records)
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        (q, prim), rec = _solo(mesh, flow, c0, ri, precision, [3, 4], monitor=2)
+        np.testing.assert_array_equal(solvers[k].download(), q, err_msg=name)
+        np.testing.assert_array_equal(solvers[k].primitives(), prim, err_msg=name)
+        np.testing.assert_array_equal(r2.records[k], rec[1], err_msg=name)
+    # members keep working on their own after the batch
+    solvers[0].run(1, 0)
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+def test_masked_case_does_not_move():
+    mem = _members(1, pick=[0, 1, 2])
+    solvers = [Solver(m, f, ri, precision=1) for _, m, f, _, ri in mem]
+    for s, (_, _, _, c0, _) in zip(solvers, mem):
+        s.upload(c0)
+    b = Batch(solvers)
+    b.set_active([1, 0, 1])
+    r = b.run(5, monitor_every=0)
+    assert list(r.iterations) == [5, 0, 5]
+    np.testing.assert_array_equal(solvers[1].download(), mem[1][3])
+    b.set_active([1, 1, 1])
+    r = b.run(2, monitor_every=0)
+    assert list(r.iterations) == [2, 2, 2]
+    for k, chunks in ((0, [7]), (1, [2]), (2, [7])):
+        _, mesh, flow, c0, ri = mem[k]
+        (q, _), _ = _solo(mesh, flow, c0, ri, 1, chunks)
+        np.testing.assert_array_equal(solvers[k].download(), q)
+    b.close()
+
+
+def test_convergence_mask_stops_cases_at_their_criterion():
+    """stop_ratio masks a case off at the first record with max_k CDIFF_k/REF_k <= ratio;
+    each case's state then equals a solo run of the iterations it did."""
+    mem = _members(0, pick=[0, 2, 4])
+    solvers = [Solver(m, f, ri, precision=0) for _, m, f, _, ri in mem]
+    for s, (_, _, _, c0, _) in zip(solvers, mem):
+        s.upload(c0)
+    b = Batch(solvers)
+    # the first-iteration CDIFF of a noisy restart is large, so a loose ratio stops early
+    r = b.run(60, monitor_every=5, stop_ratio=0.5)
+    assert np.all(r.reference > 0)
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        it = int(r.iterations[k])
+        assert it % 5 == 0 or it == 60, (name, it)
+        recs = r.records[k]
+        ratios = np.max(recs / r.reference[k], axis=1)
+        if it < 60:
+            assert r.active[k] == 0
+            assert ratios[-1] <= 0.5 and np.all(ratios[:-1] > 0.5), (name, ratios)
+        else:
+            assert np.all(ratios > 0.5)
+        (q, _), _ = _solo(mesh, flow, c0, ri, 0, [it])
+        np.testing.assert_array_equal(solvers[k].download(), q, err_msg=name)
+    b.close()
+
+
+def test_non_finite_case_is_masked_and_others_continue():
+    mem = _members(1, pick=[0, 1])
+    solvers = [Solver(m, f, ri, precision=1) for _, m, f, _, ri in mem]
+    bad = mem[0][3].copy()
+    bad[0, 7] = np.nan  # a NaN density in a restart state: arithmetic only, no indexing
+    solvers[0].upload(bad)
+    solvers[1].upload(mem[1][3])
+    b = Batch(solvers)
+    with pytest.raises(_lib.TnsError) as e:
+        b.run(4, monitor_every=2)
+    assert e.value.code == _lib.TNS_ERR_NONFINITE
+    r = b.run(4, monitor_every=2, raise_on_failure=False)
+    assert r.status[0] == _lib.TNS_ERR_NONFINITE and r.status[1] == _lib.TNS_OK
+    assert list(b.active()) == [0, 1]
+    _, mesh, flow, c0, ri = mem[1]
+    (q, _), _ = _solo(mesh, flow, c0, ri, 1, [8])
+    np.testing.assert_array_equal(solvers[1].download(), q)
+    b.close()
+
+
+def test_sweep_members_match_solo():
+    """Four cases of the seeded ramp sweep (sizes up to 512 x 192), mixed precision."""
+    sw = cases.ramp_sweep(64, seed=0)
+    pick = [sw[k] for k in (0, 5, 17, 40)]
+    solvers, starts = [], []
+    for c in pick:
+        mesh, flow = c.mesh(), c.flow()
+        ri = formats.rinit_cold(flow)
+        c0 = formats.cold_state(flow, mesh.neles, ri)
+        s = Solver(mesh, flow, ri, precision=1)
+        s.upload(c0)
+        solvers.append(s)
+        starts.append((mesh, flow, c0, ri))
+    b = Batch(solvers)
+    b.run(20, monitor_every=10)
+    for s, (mesh, flow, c0, ri), c in zip(solvers, starts, pick):
+        (q, _), _ = _solo(mesh, flow, c0, ri, 1, [20])
+        np.testing.assert_array_equal(s.download(), q, err_msg=c.name)
+    b.close()
