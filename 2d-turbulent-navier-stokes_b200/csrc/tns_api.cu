@@ -284,6 +284,10 @@ int alloc_state(tns_handle* h) {
     return h->cuda(cudaMallocHost((void**)&h->pinned, 5 * nc * sizeof(double)), "cudaMallocHost");
 }
 
+}  // namespace
+
+namespace tns_rt {
+
 // Timed launch wrapper: events around the launch when profiling.
 template <class F>
 void launch(tns_handle* h, int kid, F&& f) {
@@ -300,24 +304,51 @@ void launch(tns_handle* h, int kid, F&& f) {
     }
 }
 
+// The two pre-passes of an iteration read only Q_old and write disjoint arrays: the
+// dissipation (with DTMIN before it, LOCAL=0) on the side stream, the frozen viscous flux
+// (with stage 1's port columns before it) on the main stream, joined before stage 1.
+// With per-kernel profiling both run in order on the main stream.
+template <class Diss, class Visc>
+void prepass(tns_handle* h, Diss&& diss, Visc&& visc) {
+    if (h->profile || !h->side) {
+        diss(h->stream);
+        visc(h->stream);
+        return;
+    }
+    cudaEventRecord(h->fork, h->stream);
+    cudaStreamWaitEvent(h->side, h->fork, 0);
+    diss(h->side);
+    visc(h->stream);
+    cudaEventRecord(h->join, h->side);
+    cudaStreamWaitEvent(h->stream, h->join, 0);
+}
+
 // One mixed-precision RK4 iteration from state buffer `in` to `out` (FP32 increments
 // dQ_B, dQ_C between the stages).  The previous state survives in `in`, so the last
 // stage's input (in + dQ_B) can be reconstructed for tns_download_primitives.
 void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) {
     const Params& P = h->P;
     const Mesh& M = h->M;
-    cudaStream_t s = h->stream;
     const int np = (int)h->port_ghosts.size();
-    if (!P.local)
-        launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
-    launch(h, K_DISS, [&] { tns::launch_dissipation_mx2(P, M, A, h->df.p, h->dtf.p, h->dtmin.p, s); });
     static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
     const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
     float* out[4] = {h->dqb.p, h->dqc.p, h->dqb.p, nullptr};
+    prepass(
+        h,
+        [&](cudaStream_t s) {
+            if (!P.local)
+                launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
+            launch(h, K_DISS, [&] { tns::launch_dissipation_mx2(P, M, A, h->df.p, h->dtf.p, h->dtmin.p, s); });
+        },
+        [&](cudaStream_t s) {
+            if (np) launch(h, K_GPORT, [&] { tns::launch_gport_mx(P, M, A, in[0], h->ports.p, np, h->gport.p, s); });
+            launch(h, K_VISC, [&] { tns::launch_viscous_mx(P, M, A, h->visf.p, s); });
+        });
+    cudaStream_t s = h->stream;
     if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
     for (int st = 0; st < 4; st++) {
-        if (np) launch(h, K_GPORT, [&] { tns::launch_gport_mx(P, M, A, in[st], h->ports.p, np, h->gport.p, s); });
-        if (st == 0) launch(h, K_VISC, [&] { tns::launch_viscous_mx(P, M, A, h->visf.p, s); });
+        if (np && st > 0)
+            launch(h, K_GPORT, [&] { tns::launch_gport_mx(P, M, A, in[st], h->ports.p, np, h->gport.p, s); });
         launch(h, K_STAGE, [&] {
             tns::launch_stage_mx(P, M, A, in[st], out[st], st == 3 ? Aout : nullptr, h->df.p, h->visf.p,
                                  h->dtf.p, h->dtmin.p, alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
@@ -331,20 +362,28 @@ void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) 
 void enqueue_iteration_f64(tns_handle* h, bool monitor) {
     const Params& P = h->P;
     const Mesh& M = h->M;
-    cudaStream_t s = h->stream;
     double *A = h->qa.p, *B = h->qb.p, *Cq = h->qc.p;
     const int np = (int)h->port_ghosts.size();
-    if (!P.local)
-        launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
-    launch(h, K_DISS, [&] { tns::launch_dissipation(P, M, A, h->d.p, h->dt.p, h->dtmin.p, s); });
     static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
     const double* in[4] = {A, B, Cq, B};
     double* out[4] = {B, Cq, B, A};
+    prepass(
+        h,
+        [&](cudaStream_t s) {
+            if (!P.local)
+                launch(h, K_DTMIN, [&] { tns::launch_dtmin(P, M, A, h->partial.p, h->counter.p, h->dtmin.p, s); });
+            launch(h, K_DISS, [&] { tns::launch_dissipation(P, M, A, h->d.p, h->dt.p, h->dtmin.p, s); });
+        },
+        [&](cudaStream_t s) {
+            // the frozen viscous flux of Q_old uses stage 1's boundary state (viscous.f90:29)
+            if (np) launch(h, K_GPORT, [&] { tns::launch_gport(P, M, in[0], h->ports.p, np, h->gport.p, s); });
+            launch(h, K_VISC, [&] { tns::launch_viscous(P, M, A, h->vis.p, s); });
+        });
+    cudaStream_t s = h->stream;
     if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
     for (int st = 0; st < 4; st++) {
-        if (np) launch(h, K_GPORT, [&] { tns::launch_gport(P, M, in[st], h->ports.p, np, h->gport.p, s); });
-        // the frozen viscous flux of Q_old uses stage 1's boundary state (viscous.f90:29)
-        if (st == 0) launch(h, K_VISC, [&] { tns::launch_viscous(P, M, A, h->vis.p, s); });
+        if (np && st > 0)
+            launch(h, K_GPORT, [&] { tns::launch_gport(P, M, in[st], h->ports.p, np, h->gport.p, s); });
         launch(h, K_STAGE, [&] {
             tns::launch_stage(P, M, in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
                               alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
@@ -353,7 +392,7 @@ void enqueue_iteration_f64(tns_handle* h, bool monitor) {
     }
 }
 
-}  // namespace
+}  // namespace tns_rt
 
 extern "C" {
 
@@ -380,6 +419,10 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
     if ((rc = alloc_state(h))) return rc;
     cudaEventCreate(&h->ev[0]);
     cudaEventCreate(&h->ev[1]);
+    if ((rc = h->cuda(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = h->cuda(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "cudaEventCreate")) ||
+        (rc = h->cuda(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "cudaEventCreate")))
+        return rc;
     return TNS_OK;
 }
 
@@ -802,6 +845,12 @@ void tns_destroy(tns_handle* h) {
     if (h->status_host) cudaFreeHost(h->status_host);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    if (h->side) {
+        cudaStreamSynchronize(h->side);
+        cudaStreamDestroy(h->side);
+    }
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
 }

@@ -1,50 +1,66 @@
-// tns_batch.cuh -- descriptor of one case of a batched multi-case solve.  The batched
-// kernels read their case's parameters, mesh view and buffers from an array of these,
-// indexed through a table of (case, tile i, tile j) entries: one launch advances every
-// active case.
+// tns_batch.cuh -- argument blocks of the tile kernels and the descriptor of one case
+// of a batched multi-case solve.
+//
+// A single-case launch passes its argument block by value (kernel parameter space).  A
+// batched launch finds, per block, its case in an array of BatchCase descriptors in
+// global memory, indexed through a table of (case, tile j, tile i) entries; each
+// descriptor holds every argument block the case's launches need, precomputed on the
+// host (per stage, monitor mode and, on the mixed path, state parity), so a block reads
+// one read-only block instead of assembling pointers in registers.
 #pragma once
 
 #include "tns_device.cuh"
 
 namespace tns {
 
-struct BatchCase {
-    Params P;
-    Mesh M;
-    // FP64 path: state qa (in place), stage scratch qb/qc, frozen d/vis/dt
-    double *qa, *qb, *qc, *d, *vis, *dt;
-    // mixed path: state ping-pong qa/qa2, FP32 increments and frozen terms
-    double* qa2;
-    float *dqb, *dqc, *df, *visf, *dtf;
-    const double* dtmin;
-    unsigned long long* cdiff;  // 5 slots
+struct StageArgs {
+    const double* qin;   // stage input state [5][ncell]
+    const double* qold;  // state at the start of the iteration [5][ncell]
+    double* qout;        // stage output [5][ncell] (may alias qold: own-cell reads only)
+    const double* d;     // dissipation [5][ncell]
+    const double* vis;   // viscous flux [4][ncell]
+    const double* dt;    // per-cell DT (LOCAL=1)
+    const double* dtmin; // DTMIN (LOCAL=0)
+    double alpha;
+    unsigned long long* cdiff;  // 5 slots, ordered bits of max|Q_old-Q_new| (or null)
+    unsigned int* status;       // bit 0: non-finite state
+};
+
+template <class OutT>
+struct DissArgs {
+    const double* q;     // Q_old [5][ncell]
+    OutT* d;             // out: D [5][ncell] (FP64, or FP32 on the mixed path)
+    OutT* dt;            // out: DT per cell (LOCAL=1)
+    const double* dtmin; // DTMIN (LOCAL=0)
+};
+
+struct StageArgsMx {
+    const double* cold;   // state at the start of the iteration [5][ncell]
+    const float* dqin;    // stage input increment (null in stage 1)
+    float* dqout;         // stage output increment (stages 1-3)
+    double* qout;         // new state (stage 4) [5][ncell]
+    const float* d;       // dissipation [5][ncell]
+    const float* vis;     // viscous flux [4][ncell]
+    const float* dt;      // per-cell DT (LOCAL=1)
+    const double* dtmin;  // DTMIN (LOCAL=0)
+    float alpha;
+    unsigned long long* cdiff;
     unsigned int* status;
 };
 
-// Shared-memory copy of a batched block's case: every thread reads it many times.
-struct BatchBlock {
+struct BatchCase {
     Params P;
     Mesh M;
-    int active;
+    // FP64 path
+    DissArgs<double> diss;
+    StageArgs stage[2][4];  // [monitor][stage]
+    const double* q;        // state (viscous-flux input)
+    double* vis;
+    // mixed path; parity p reads the state from qmx[p] and writes it to qmx[1-p]
+    const double* qmx[2];
+    float *df, *dtf, *visf;
+    StageArgsMx stage_mx[2][2][4];  // [parity][monitor][stage]
+    const double* dtmin;
 };
-
-__device__ __forceinline__ int4 batch_prologue(const BatchCase* __restrict__ cases,
-                                              const int4* __restrict__ tiles,
-                                              const int* __restrict__ active, BatchBlock& B) {
-    static_assert(sizeof(Params) % 4 == 0 && sizeof(Mesh) % 4 == 0, "word copy");
-    constexpr int NP = sizeof(Params) / 4, NM = sizeof(Mesh) / 4;
-    const int4 t = tiles[blockIdx.x];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const BatchCase* c = cases + t.x;
-    // one word per thread: the block's case parameters and mesh view
-    if (tid < NP)
-        reinterpret_cast<int*>(&B.P)[tid] = reinterpret_cast<const int*>(&c->P)[tid];
-    else if (tid < NP + NM)
-        reinterpret_cast<int*>(&B.M)[tid - NP] = reinterpret_cast<const int*>(&c->M)[tid - NP];
-    else if (tid == NP + NM)
-        B.active = active[t.x];
-    __syncthreads();
-    return t;
-}
 
 }  // namespace tns

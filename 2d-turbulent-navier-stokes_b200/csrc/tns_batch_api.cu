@@ -40,6 +40,14 @@ struct tns_batch {
     unsigned int* h_status = nullptr;       // pinned [ncases]
     int ntiles = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [monitor][parity]
+    // schedule: 0 = one launch per phase over the tile table of all active cases;
+    // 1 = each case's own single-case launches on one of several streams, captured as
+    // parallel branches of one graph (cases run concurrently, kernels as for tns_run)
+    int mode = 0;
+    std::vector<cudaStream_t> branch;
+    std::vector<int> branch_of;  // case -> branch stream (largest cases spread first)
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
     long long per_iter[2] = {0, 0};
     long long launches = 0;
 
@@ -68,27 +76,47 @@ struct tns_batch {
 
 namespace {
 
-// Descriptor of case k, mapping parity 0 to the member's current state buffer.
+// Descriptor of case k: every argument block of its launches (the ones
+// enqueue_iteration_f64 / enqueue_iteration_mx in tns_api.cu pass), with parity 0 of the
+// mixed ping-pong reading the member's current state buffer.
 BatchCase describe(tns_batch* b, int k) {
     tns_handle* h = b->cases[k];
     BatchCase c{};
     c.P = h->P;
     c.M = h->M;
-    c.qa = h->state();
-    c.qb = h->qb.p;
-    c.qc = h->qc.p;
-    c.d = h->d.p;
-    c.vis = h->vis.p;
-    c.dt = h->dt.p;
-    c.qa2 = h->precision == 1 ? h->other_state() : nullptr;
-    c.dqb = h->dqb.p;
-    c.dqc = h->dqc.p;
-    c.df = h->df.p;
-    c.visf = h->visf.p;
-    c.dtf = h->dtf.p;
     c.dtmin = h->dtmin.p;
-    c.cdiff = b->d_cdiff.p + 5 * (size_t)k;
-    c.status = b->d_status.p + k;
+    unsigned long long* cdiff = b->d_cdiff.p + 5 * (size_t)k;
+    unsigned int* status = b->d_status.p + k;
+    if (h->precision == 0) {
+        double *A = h->qa.p, *B = h->qb.p, *Cq = h->qc.p;
+        c.diss = tns::DissArgs<double>{A, h->d.p, h->dt.p, h->dtmin.p};
+        c.q = A;
+        c.vis = h->vis.p;
+        const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
+        const double* in[4] = {A, B, Cq, B};
+        double* out[4] = {B, Cq, B, A};
+        for (int mon = 0; mon < 2; mon++)
+            for (int st = 0; st < 4; st++)
+                c.stage[mon][st] = tns::StageArgs{in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
+                                                  alpha[st], (mon && st == 3) ? cdiff : nullptr,
+                                                  st == 3 ? status : nullptr};
+    } else {
+        double* q[2] = {h->state(), h->other_state()};
+        c.qmx[0] = q[0];
+        c.qmx[1] = q[1];
+        c.df = h->df.p;
+        c.dtf = h->dtf.p;
+        c.visf = h->visf.p;
+        const float alpha[4] = {0.25f, 1.0f / 3.0f, 0.5f, 1.0f};
+        const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
+        float* out[4] = {h->dqb.p, h->dqc.p, h->dqb.p, nullptr};
+        for (int par = 0; par < 2; par++)
+            for (int mon = 0; mon < 2; mon++)
+                for (int st = 0; st < 4; st++)
+                    c.stage_mx[par][mon][st] = tns::StageArgsMx{
+                        q[par], in[st], out[st], st == 3 ? q[1 - par] : nullptr, h->df.p, h->visf.p, h->dtf.p,
+                        h->dtmin.p, alpha[st], (mon && st == 3) ? cdiff : nullptr, st == 3 ? status : nullptr};
+    }
     return c;
 }
 
@@ -144,7 +172,7 @@ void enqueue_batch_iteration(tns_batch* b, int parity, bool monitor) {
     const bool mixed = b->precision == 1;
     const int n = (int)b->cases.size();
     const int nt = b->ntiles;
-    auto state = [&](int k) { return (mixed && parity) ? b->desc[k].qa2 : b->desc[k].qa; };
+    auto state = [&](int k) { return mixed ? b->desc[k].qmx[parity] : b->desc[k].q; };
     for (int k = 0; k < n; k++) {
         if (!b->active[k]) continue;
         tns_handle* h = b->cases[k];
@@ -172,7 +200,7 @@ void enqueue_batch_iteration(tns_batch* b, int parity, bool monitor) {
                 const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
                 tns::launch_gport_mx(h->P, h->M, state(k), in[st], h->ports.p, np, h->gport.p, s);
             } else {
-                const double* in[4] = {b->desc[k].qa, h->qb.p, h->qc.p, h->qb.p};
+                const double* in[4] = {b->desc[k].q, h->qb.p, h->qc.p, h->qb.p};
                 tns::launch_gport(h->P, h->M, in[st], h->ports.p, np, h->gport.p, s);
             }
             b->launches++;
@@ -182,13 +210,82 @@ void enqueue_batch_iteration(tns_batch* b, int parity, bool monitor) {
     }
 }
 
+// Per-case launches on branch streams (schedule 1): the single-case iteration of every
+// active case, forked from and joined back to the batch stream.
+void enqueue_branches(tns_batch* b, int parity, bool monitor) {
+    const int n = (int)b->cases.size();
+    const int nb = (int)b->branch.size();
+    cudaEventRecord(b->fork, b->stream);
+    std::vector<char> used(nb, 0);
+    for (int k = 0; k < n; k++) {
+        if (!b->active[k]) continue;
+        tns_handle* h = b->cases[k];
+        const int bi = b->branch_of[k];
+        if (!used[bi]) {
+            cudaStreamWaitEvent(b->branch[bi], b->fork, 0);
+            used[bi] = 1;
+        }
+        cudaStream_t keep = h->stream, keep_side = h->side;
+        const bool prof = h->profile;
+        const long long before = h->launches;
+        h->stream = b->branch[bi];
+        h->side = nullptr;   // the case's pre-passes in order: the batch is parallel enough
+        h->profile = false;  // no event synchronisation inside a capture
+        if (b->precision == 1)
+            tns_rt::enqueue_iteration_mx(h, monitor, const_cast<double*>(b->desc[k].qmx[parity]),
+                                         const_cast<double*>(b->desc[k].qmx[1 - parity]));
+        else
+            tns_rt::enqueue_iteration_f64(h, monitor);
+        b->launches += h->launches - before;
+        h->launches = before;
+        h->stream = keep;
+        h->side = keep_side;
+        h->profile = prof;
+    }
+    for (int bi = 0; bi < nb; bi++)
+        if (used[bi]) {
+            cudaEventRecord(b->join[bi], b->branch[bi]);
+            cudaStreamWaitEvent(b->stream, b->join[bi], 0);
+        }
+}
+
+// Status words (and, on a monitored iteration, the CDIFF slots) of every case into the
+// pinned host arrays; the caller synchronises the batch stream.
+int fetch_monitor(tns_batch* b, bool monitor) {
+    const int n = (int)b->cases.size();
+    int rc;
+    if (b->mode == 0) {
+        if ((rc = b->cuda(cudaMemcpyAsync(b->h_status, b->d_status.p, n * sizeof(unsigned int),
+                                          cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+        if (monitor && (rc = b->cuda(cudaMemcpyAsync(b->h_cdiff, b->d_cdiff.p, 5 * n * sizeof(unsigned long long),
+                                                     cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+        return TNS_OK;
+    }
+    for (int k = 0; k < n; k++) {
+        if (!b->active[k]) continue;
+        tns_handle* h = b->cases[k];
+        if ((rc = b->cuda(cudaMemcpyAsync(b->h_status + k, h->status.p, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                          b->stream), "cudaMemcpyAsync")))
+            return rc;
+        if (monitor && (rc = b->cuda(cudaMemcpyAsync(b->h_cdiff + 5 * k, h->cdiff.p, 5 * sizeof(unsigned long long),
+                                                     cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+    }
+    return TNS_OK;
+}
+
 int ensure_batch_graph(tns_batch* b, int monitor, int parity) {
     cudaGraphExec_t* g = &b->graph[monitor][parity];
     if (*g) return TNS_OK;
     int rc;
     if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
     const long long before = b->launches;
-    enqueue_batch_iteration(b, parity, monitor != 0);
+    if (b->mode == 1)
+        enqueue_branches(b, parity, monitor != 0);
+    else
+        enqueue_batch_iteration(b, parity, monitor != 0);
     b->per_iter[monitor] = b->launches - before;
     b->launches = before;
     cudaGraph_t graph;
@@ -246,10 +343,14 @@ int tns_batch_set_active(tns_batch* b, const int* active) {
     bool cleared = false;
     for (int k = 0; k < n; k++) {
         b->active[k] = active[k] ? 1 : 0;
-        if (active[k] && b->failed[k]) {  // re-activating a failed case clears its status word
+        if (active[k] && b->failed[k]) {  // re-activating a failed case clears its status words
             b->failed[k] = 0;
             b->h_status[k] = 0;
             cleared = true;
+            int rc;
+            if ((rc = b->cuda(cudaMemsetAsync(b->cases[k]->status.p, 0, sizeof(unsigned int), b->stream),
+                              "cudaMemsetAsync")))
+                return rc;
         }
     }
     int rc;
@@ -323,12 +424,7 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
         if (b->precision == 1) parity ^= 1;
         if (!monitor && it != niter) continue;
         // residual records, status words and the masks, at the monitor cadence and at the end
-        if ((rc = b->cuda(cudaMemcpyAsync(b->h_status, b->d_status.p, n * sizeof(unsigned int),
-                                          cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
-            return rc;
-        if (monitor && (rc = b->cuda(cudaMemcpyAsync(b->h_cdiff, b->d_cdiff.p, 5 * n * sizeof(unsigned long long),
-                                                     cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
-            return rc;
+        if ((rc = fetch_monitor(b, monitor))) return rc;
         if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))) return rc;
         for (int k = 0; k < n; k++) {
             if (!b->active[k]) continue;
@@ -383,6 +479,42 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
     return TNS_OK;
 }
 
+int tns_batch_set_schedule(tns_batch* b, int schedule) {
+    if (!b) return TNS_ERR_ARG;
+    if (schedule != 0 && schedule != 1) return b->fail(TNS_ERR_ARG, "schedule %d is not 0 or 1", schedule);
+    int rc;
+    if (schedule == 1 && b->branch.empty()) {
+        const int n = (int)b->cases.size();
+        const int nb = std::min<int>(n, 64);
+        // longest-first assignment of cases (by cell count) to the least-loaded branch
+        std::vector<int> order(n);
+        for (int k = 0; k < n; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int c) { return b->cases[a]->ncell() > b->cases[c]->ncell(); });
+        std::vector<double> load(nb, 0.0);
+        b->branch_of.assign(n, 0);
+        for (int k : order) {
+            const int bi = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            b->branch_of[k] = bi;
+            load[bi] += (double)b->cases[k]->ncell();
+        }
+        if ((rc = b->cuda(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
+        b->branch.resize(nb);
+        b->join.resize(nb);
+        for (int i = 0; i < nb; i++)
+            if ((rc = b->cuda(cudaStreamCreateWithFlags(&b->branch[i], cudaStreamNonBlocking), "cudaStreamCreate")) ||
+                (rc = b->cuda(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming), "cudaEventCreate")))
+                return rc;
+    }
+    if (schedule != b->mode) {
+        b->mode = schedule;
+        b->drop_graphs();
+    }
+    return TNS_OK;
+}
+
+int tns_batch_get_schedule(tns_batch* b) { return b ? b->mode : TNS_ERR_ARG; }
+
 long long tns_batch_launch_count(tns_batch* b) { return b ? b->launches : -1; }
 
 const char* tns_batch_last_error(tns_batch* b) { return b ? b->err.c_str() : "null batch"; }
@@ -398,6 +530,11 @@ void tns_batch_destroy(tns_batch* b) {
     b->d_status.release();
     if (b->h_cdiff) cudaFreeHost(b->h_cdiff);
     if (b->h_status) cudaFreeHost(b->h_status);
+    for (cudaStream_t st : b->branch)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }

@@ -53,6 +53,9 @@ struct tns_handle {
     std::vector<int> hgtype, hgrank;
     std::vector<int> node_of;   // structured node index -> 1-based node id
     cudaStream_t own = nullptr, stream = nullptr;
+    // second branch of an iteration: the dissipation pre-pass runs beside the viscous flux
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     DevBuf<double> x, y, cfldl, gxc, gyc, ginj, gport, qa, qb, qc, d, vis, dt, dtmin, partial,
         primout;
     // mixed FP32/FP64 path: FP64 state ping-pong (qa, qa2) and FP32 scratch
@@ -96,3 +99,10 @@ struct tns_handle {
     double* other_state() { return precision == 1 && !cur ? qa2.p : qa.p; }
 };
 
+
+namespace tns_rt {
+// One RK4 iteration of a handle on h->stream (tns_api.cu): FP64 in place, mixed from
+// state buffer A to Aout.  The batch runtime captures these per case.
+void enqueue_iteration_f64(tns_handle* h, bool monitor);
+void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout);
+}  // namespace tns_rt

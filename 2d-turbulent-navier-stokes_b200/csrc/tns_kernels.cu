@@ -42,19 +42,6 @@ __device__ __forceinline__ void put_slot(StageSmem& S, int s, const Prim& p) {
     S.rho[s] = p.rho;
 }
 
-struct StageArgs {
-    const double* qin;   // stage input state [5][ncell]
-    const double* qold;  // state at the start of the iteration [5][ncell]
-    double* qout;        // stage output [5][ncell] (may alias qold: own-cell reads only)
-    const double* d;     // dissipation [5][ncell]
-    const double* vis;   // viscous flux [4][ncell]
-    const double* dt;    // per-cell DT (LOCAL=1)
-    const double* dtmin; // DTMIN (LOCAL=0)
-    double alpha;
-    unsigned long long* cdiff;  // 5 slots, ordered bits of max|Q_old-Q_new| (or null)
-    unsigned int* status;       // bit 0: non-finite state
-};
-
 // One RK stage (turbnstwod.f90:204-227, boundary.f90:24-48, source_terms.f90:24-104,
 // residual.f90:23-83) on a TI x TJ tile with its halo staged in shared memory.
 __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const StageArgs& A, int bx, int by) {
@@ -174,7 +161,7 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
     }
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage(Params P, Mesh M, StageArgs A) {
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MINB)) k_stage(Params P, Mesh M, StageArgs A) {
     stage_tile(P, M, A, blockIdx.x, blockIdx.y);
 }
 
@@ -343,7 +330,7 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
     }
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous(Params P, Mesh M, const double* __restrict__ q,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MINB)) k_viscous(Params P, Mesh M, const double* __restrict__ q,
                                                       double* __restrict__ vis) {
     viscous_tile(P, M, q, vis, blockIdx.x, blockIdx.y);
 }
@@ -360,14 +347,6 @@ enum RField { RVBD, RANU, RANURT, RQ0, RQ1, RQ2, RQ3, RQ4, NRF };
 size_t diss_smem_bytes() {
     return sizeof(double) * ((size_t)NDF * NDSLOT + (size_t)NRF * NRSLOT + 2 * NNODE);
 }
-
-template <class OutT>
-struct DissArgs {
-    const double* q;     // Q_old [5][ncell]
-    OutT* d;             // out: D [5][ncell] (FP64, or FP32 on the mixed path)
-    OutT* dt;            // out: DT per cell (LOCAL=1)
-    const double* dtmin; // DTMIN (LOCAL=0)
-};
 
 __device__ __forceinline__ double local_dt(const Params& P, double c1, double c2, double c3,
                                            double c4, double cfldl) {
@@ -757,37 +736,29 @@ __global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ pri
 __global__ void __launch_bounds__(NTHREADS) k_dissipation_batch(const BatchCase* __restrict__ cases,
                                                                 const int4* __restrict__ tiles,
                                                                 const int* __restrict__ active) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;  // whole block: before any barrier
     const BatchCase& c = cases[t.x];
-    DissArgs<double> A{c.qa, c.d, c.dt, c.dtmin};
-    dissipation_tile<double>(B.P, B.M, A, t.y, t.z);
+    dissipation_tile<double>(c.P, c.M, c.diss, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MINB) k_viscous_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MINB)) k_viscous_batch(const BatchCase* __restrict__ cases,
                                                                           const int4* __restrict__ tiles,
                                                                           const int* __restrict__ active) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
-    viscous_tile(B.P, B.M, cases[t.x].qa, cases[t.x].vis, t.y, t.z);
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;
+    const BatchCase& c = cases[t.x];
+    viscous_tile(c.P, c.M, c.q, c.vis, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MINB) k_stage_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_stage_batch(const BatchCase* __restrict__ cases,
                                                                          const int4* __restrict__ tiles,
                                                                          const int* __restrict__ active,
                                                                          int stage, int monitor) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
-    const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
-    const double* in[4] = {c.qa, c.qb, c.qc, c.qb};
-    double* out[4] = {c.qb, c.qc, c.qb, c.qa};
-    StageArgs A{in[stage], c.qa, out[stage], c.d, c.vis, c.dt, c.dtmin, alpha[stage],
-                (monitor && stage == 3) ? c.cdiff : nullptr, stage == 3 ? c.status : nullptr};
-    stage_tile(B.P, B.M, A, t.y, t.z);
+    stage_tile(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
 }
 
 // ------------------------------------------------------------------ launchers

@@ -51,20 +51,6 @@ struct StageSmemMx {
 
 size_t stage_mx_smem_bytes() { return sizeof(StageSmemMx); }
 
-struct StageArgsMx {
-    const double* cold;   // state at the start of the iteration [5][ncell]
-    const float* dqin;    // stage input increment (null in stage 1)
-    float* dqout;         // stage output increment (stages 1-3)
-    double* qout;         // new state (stage 4) [5][ncell]
-    const float* d;       // dissipation [5][ncell]
-    const float* vis;     // viscous flux [4][ncell]
-    const float* dt;      // per-cell DT (LOCAL=1)
-    const double* dtmin;  // DTMIN (LOCAL=0)
-    float alpha;
-    unsigned long long* cdiff;
-    unsigned int* status;
-};
-
 __device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p) {
 #pragma unroll
     for (int m = 0; m < 5; m++)
@@ -77,6 +63,11 @@ __device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p
 
 #ifndef TNS_STAGE_MX_MINB
 #define TNS_STAGE_MX_MINB 4
+#endif
+// the batched stage kernel reads its arguments from global descriptors, which costs
+// registers: at 4 blocks/SM it spills
+#ifndef TNS_STAGE_MX_BATCH_MINB
+#define TNS_STAGE_MX_BATCH_MINB 3
 #endif
 #ifndef TNS_VISC_MX_MINB
 #define TNS_VISC_MX_MINB 3
@@ -273,7 +264,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
     }
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_MINB)) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
     stage_mx_tile(P, M, A, blockIdx.x, blockIdx.y);
 }
 
@@ -468,7 +459,7 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
         vis[k * ncell + cell] = ((s1 * S.fj[k][f1] + S.fi[k][f2]) + S.fj[k][f3]) + s4 * S.fi[k][f4];
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
                                                          float* __restrict__ vis) {
     viscous_mx_tile(P, M, q, vis, blockIdx.x, blockIdx.y);
 }
@@ -685,39 +676,30 @@ __global__ void k_prim_out_mx(Params P, Mesh M, const double* __restrict__ cold,
 __global__ void __launch_bounds__(NTHREADS) k_dissipation_mx_batch(const BatchCase* __restrict__ cases,
                                                                    const int4* __restrict__ tiles,
                                                                    const int* __restrict__ active, int parity) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;  // whole block: before any barrier
     const BatchCase& c = cases[t.x];
-    dissipation_mx_tile(B.P, B.M, parity ? c.qa2 : c.qa, c.df, c.dtf, c.dtmin, t.y, t.z);
+    dissipation_mx_tile(c.P, c.M, c.qmx[parity], c.df, c.dtf, c.dtmin, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_VISC_MX_MINB) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
                                                                                 const int4* __restrict__ tiles,
                                                                                 const int* __restrict__ active,
                                                                                 int parity) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
-    viscous_mx_tile(B.P, B.M, parity ? c.qa2 : c.qa, c.visf, t.y, t.z);
+    viscous_mx_tile(c.P, c.M, c.qmx[parity], c.visf, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_STAGE_MX_MINB) k_stage_mx_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_BATCH_MINB)) k_stage_mx_batch(const BatchCase* __restrict__ cases,
                                                                                const int4* __restrict__ tiles,
                                                                                const int* __restrict__ active,
                                                                                int parity, int stage, int monitor) {
-    __shared__ BatchBlock B;
-    const int4 t = batch_prologue(cases, tiles, active, B);
-    if (!B.active) return;
+    const int4 t = tiles[blockIdx.x];
+    if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
-    const float alpha[4] = {0.25f, 1.0f / 3.0f, 0.5f, 1.0f};
-    const float* in[4] = {nullptr, c.dqb, c.dqc, c.dqb};
-    float* out[4] = {c.dqb, c.dqc, c.dqb, nullptr};
-    StageArgsMx A{parity ? c.qa2 : c.qa, in[stage], out[stage], stage == 3 ? (parity ? c.qa : c.qa2) : nullptr,
-                  c.df, c.visf, c.dtf, c.dtmin, alpha[stage],
-                  (monitor && stage == 3) ? c.cdiff : nullptr, stage == 3 ? c.status : nullptr};
-    stage_mx_tile(B.P, B.M, A, t.y, t.z);
+    stage_mx_tile(c.P, c.M, c.stage_mx[parity][monitor][stage], t.y, t.z);
 }
 
 // ------------------------------------------------------------------ launchers

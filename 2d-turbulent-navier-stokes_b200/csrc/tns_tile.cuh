@@ -13,9 +13,15 @@ namespace tns {
 #ifndef TNS_STAGE_MINB
 #define TNS_STAGE_MINB 3
 #endif
+#ifndef TNS_STAGE_BATCH_MINB
+#define TNS_STAGE_BATCH_MINB 2
+#endif
 #ifndef TNS_VISC_MINB
 #define TNS_VISC_MINB 1
 #endif
+// Resident blocks per SM of a kernel tuned at TI = 8, for the compiled TI: the same
+// threads per SM at every tile height.
+#define TNS_PER_SM(n) ((n) * 8 / TNS_TI > 0 ? (n) * 8 / TNS_TI : 1)
 constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
 constexpr int TI = TNS_TI;  // tile extent along i
 constexpr int NTHREADS = TJ * TI;

@@ -12,6 +12,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtnsgpu.so")
+# tile-height variants of the same library (TI rows of 32 cells per tile); the default
+# build is TI = 8
+TILE_VARIANTS = {8: LIB_PATH, 4: os.path.join(HERE, "libtnsgpu_ti4.so"),
+                 16: os.path.join(HERE, "libtnsgpu_ti16.so")}
+
+
+def variant_path(ti: int) -> str:
+    if ti not in TILE_VARIANTS:
+        raise ValueError(f"no tile variant TI={ti}; built: {sorted(TILE_VARIANTS)}")
+    return TILE_VARIANTS[ti]
 
 TNS_OK = 0
 ERRORS = {-1: "TNS_ERR_ARG", -2: "TNS_ERR_MESH", -3: "TNS_ERR_UNSUPPORTED",
@@ -27,7 +37,8 @@ EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
            "tns_boundary_integrals", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
-           "tns_batch_get_active", "tns_batch_launch_count", "tns_batch_last_error", "tns_batch_destroy")
+           "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule",
+           "tns_batch_launch_count", "tns_batch_last_error", "tns_batch_destroy")
 NOT_INT = ("tns_launch_count", "tns_last_error", "tns_destroy", "tns_batch_launch_count",
            "tns_batch_last_error", "tns_batch_destroy")
 
@@ -53,14 +64,14 @@ class TnsError(RuntimeError):
         self.code = code
 
 
-_lib = None
+_libs = {}
 
 
-def load(path: str = LIB_PATH):
-    """Load the library (raises OSError when it is missing)."""
-    global _lib
-    if _lib is not None:
-        return _lib
+def load(path: str = None):
+    """Load the library (raises OSError when it is missing); one instance per path."""
+    path = os.path.abspath(path or LIB_PATH)
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise OSError(f"{path} is missing: build it with tnsgpu.build.build_library()")
     L = C.CDLL(path)
@@ -90,6 +101,8 @@ def load(path: str = LIB_PATH):
     L.tns_batch_run.argtypes = [vp, ip, ip, C.c_double, dp, dp, ip, vp, vp, vp]
     L.tns_batch_set_active.argtypes = [vp, vp]
     L.tns_batch_get_active.argtypes = [vp, vp]
+    L.tns_batch_set_schedule.argtypes = [vp, ip]
+    L.tns_batch_get_schedule.argtypes = [vp]
     L.tns_batch_launch_count.argtypes = [vp]
     L.tns_batch_launch_count.restype = C.c_longlong
     L.tns_batch_last_error.argtypes = [vp]
@@ -99,7 +112,7 @@ def load(path: str = LIB_PATH):
     for n in EXPORTS:
         if n not in NOT_INT:
             getattr(L, n).restype = C.c_int
-    _lib = L
+    _libs[path] = L
     return L
 
 

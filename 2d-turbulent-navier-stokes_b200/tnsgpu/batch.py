@@ -28,9 +28,13 @@ class BatchResult:
 
 
 class Batch:
-    def __init__(self, solvers: Sequence[Solver]):
-        self.L = _lib.load()
+    def __init__(self, solvers: Sequence[Solver], schedule: int = 0):
         self.solvers = list(solvers)  # keeps the member handles alive
+        if not self.solvers:
+            raise ValueError("a batch needs at least one case")
+        self.L = self.solvers[0].L
+        if any(s.L is not self.L for s in self.solvers):
+            raise ValueError("batch members must come from one library build")
         arr = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
         self._arr = arr
         b = C.c_void_p()
@@ -38,6 +42,8 @@ class Batch:
         self.b = b
         self._check(rc)
         self.reference = np.zeros((len(self.solvers), 5))
+        if schedule:
+            self.schedule = schedule
 
     def _check(self, rc: int):
         if rc != _lib.TNS_OK:
@@ -68,6 +74,16 @@ class Batch:
             self._check(rc)
         return BatchResult(iters, [out[k, : nrec[k]] for k in range(n)], status, ref.copy(),
                            self.active())
+
+    @property
+    def schedule(self) -> int:
+        """0: one launch per phase over all cases' tiles; 1: per-case launches on
+        parallel graph branches."""
+        return int(self.L.tns_batch_get_schedule(self.b))
+
+    @schedule.setter
+    def schedule(self, value: int):
+        self._check(self.L.tns_batch_set_schedule(self.b, int(value)))
 
     def set_active(self, mask: Sequence[int]):
         m = np.ascontiguousarray(np.asarray(mask, np.int32))

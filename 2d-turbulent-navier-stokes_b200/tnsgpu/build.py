@@ -28,11 +28,23 @@ def build_mains() -> list:
     return out
 
 
-def build_library(verbose: bool = False) -> str:
-    out = os.path.join(HERE, "libtnsgpu.so")
+def _lib_cmd(out: str, ti: int, verbose: bool):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = ["nvcc", *NVCC_FLAGS, *srcs, "-o", out]
+    cmd = ["nvcc", *NVCC_FLAGS, f"-DTNS_TI={ti}", *srcs, "-o", out]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
-    return out
+    return cmd
+
+
+def build_library(verbose: bool = False, variants: bool = True) -> str:
+    """libtnsgpu.so (tile height TI = 8) and, with ``variants``, the TI = 4 and TI = 16
+    builds the autotuner chooses among (compiled concurrently)."""
+    from ._lib import TILE_VARIANTS
+    jobs = [(TILE_VARIANTS[8], 8)]
+    if variants:
+        jobs += [(TILE_VARIANTS[t], t) for t in sorted(TILE_VARIANTS) if t != 8]
+    procs = [(out, subprocess.Popen(_lib_cmd(out, ti, verbose))) for out, ti in jobs]
+    failed = [out for out, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, f"nvcc for {failed}")
+    return TILE_VARIANTS[8]

@@ -29,8 +29,11 @@ def make_params(flow: Flow, rinit: float, precision: int = 0) -> _lib.TnsParams:
 class Solver:
     """Device solver for one case.  Arrays follow Fortran ids (cell k at index k-1)."""
 
-    def __init__(self, mesh: Mesh, flow: Flow, rinit: float, precision: int = 0):
-        L = _lib.load()
+    def __init__(self, mesh: Mesh, flow: Flow, rinit: float, precision: int = 0,
+                 lib: Optional[str] = None):
+        """lib: path of the library build to use (a tile-height variant,
+        ``_lib.variant_path``); default the TI = 8 build."""
+        L = _lib.load(lib)
         self.L, self.mesh, self.flow = L, mesh, flow
         i32 = lambda a: np.ascontiguousarray(a, np.int32)
         # NOD is passed column-major (NOD(I,K) = nod[(K-1)*LD + I-1]) like Fortran holds it

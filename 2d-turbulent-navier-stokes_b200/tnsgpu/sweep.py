@@ -6,11 +6,16 @@ mixed FP32/FP64 mode, until its residual ratio max_k CDIFF_k / CDIFF_k(iteration
 reaches ``stop_ratio`` at a record (every ``monitor`` iterations) or ``niter``
 iterations pass -- once as one batch (tns_batch_run: every kernel phase is one launch
 over the tiles of all active cases, converged cases masked off) and once case by case
-through tns_run with the same criterion.  Reports both wall times (device work
-synchronised, state uploads excluded), the iterations each case ran, and whether
-every batched final state equals its sequential counterpart bit for bit.
+through tns_run with the same criterion.  Before the batched run the autotuner picks
+the tile height and the batch schedule by timing a few iterations of the sweep itself
+(its time is reported apart); the sequential solves use the default build.  Reports
+both wall times (device work synchronised, state uploads excluded), the iterations each
+case ran, and how far every batched final state is from its sequential counterpart
+(bit-identical in FP64; FP32 rounding of the per-tile reference flux in the mixed mode
+when the tuned tile height differs from the default).
 
   python -m tnsgpu.sweep [--cases 64] [--niter 5000] [--stop-ratio 1e-5] [--monitor 1000]
+                         [--precision mixed|fp64] [--no-tune]
 """
 from __future__ import annotations
 
@@ -20,17 +25,17 @@ import time
 
 import numpy as np
 
-from . import cases, formats
+from . import autotune, cases, formats
 from .batch import Batch
 from .solver import Solver
 
 
-def _solvers(sweep, precision):
+def _solvers(sweep, precision, lib=None):
     out = []
     for c in sweep:
         mesh, flow = c.mesh(), c.flow()
         ri = formats.rinit_cold(flow)
-        s = Solver(mesh, flow, ri, precision=precision)
+        s = Solver(mesh, flow, ri, precision=precision, lib=lib)
         s.upload(formats.cold_state(flow, mesh.neles, ri))
         out.append(s)
     return out
@@ -54,8 +59,8 @@ def run_sequential(solvers, niter, monitor, stop_ratio):
     return time.perf_counter() - t0, iters
 
 
-def run_batched(solvers, niter, monitor, stop_ratio):
-    b = Batch(solvers)
+def run_batched(solvers, niter, monitor, stop_ratio, schedule=0):
+    b = Batch(solvers, schedule=schedule)
     t0 = time.perf_counter()
     r = b.run(niter, monitor, stop_ratio)
     dt = time.perf_counter() - t0
@@ -64,7 +69,7 @@ def run_batched(solvers, niter, monitor, stop_ratio):
     return dt, [int(v) for v in r.iterations], launches
 
 
-def compare(ncases=64, niter=5000, stop_ratio=1.0e-5, monitor=1000, seed=0, precision=1):
+def compare(ncases=64, niter=5000, stop_ratio=1.0e-5, monitor=1000, seed=0, precision=1, tune=True):
     sweep = cases.ramp_sweep(ncases, seed=seed)
     cells = np.array([c.nx * c.ny for c in sweep])
     # warm-up: library load, kernel attributes, a graph capture on a small batch
@@ -74,24 +79,36 @@ def compare(ncases=64, niter=5000, stop_ratio=1.0e-5, monitor=1000, seed=0, prec
         s.run(2, 0)
         s.close()
 
+    t0 = time.perf_counter()
+    if tune:
+        choice = autotune.tune_batch(lambda lib: _solvers(sweep, precision, lib))
+    else:
+        choice = {"ti": 8, "schedule": 0, "lib": None, "trials": []}
+    t_tune = time.perf_counter() - t0
+
     seq = _solvers(sweep, precision)
     t_seq, it_seq = run_sequential(seq, niter, monitor, stop_ratio)
     q_seq = [s.download() for s in seq]
     for s in seq:
         s.close()
 
-    bat = _solvers(sweep, precision)
-    t_bat, it_bat, launches = run_batched(bat, niter, monitor, stop_ratio)
-    same = [bool(np.array_equal(s.download(), q)) for s, q in zip(bat, q_seq)]
+    bat = _solvers(sweep, precision, choice["lib"])
+    t_bat, it_bat, launches = run_batched(bat, niter, monitor, stop_ratio, choice["schedule"])
+    q_bat = [s.download() for s in bat]
     for s in bat:
         s.close()
+    same = all(np.array_equal(a, b) for a, b in zip(q_bat, q_seq))
+    rel = max(float(np.max(np.max(np.abs(a - b), axis=1) / np.max(np.abs(b), axis=1)))
+              for a, b in zip(q_bat, q_seq))
     work = float(np.sum(cells * np.array(it_bat)))
     return {
         "cases": ncases, "seed": seed, "precision": "mixed" if precision else "fp64",
         "cells_total": int(cells.sum()), "niter": niter, "monitor": monitor, "stop_ratio": stop_ratio,
+        "tuned": {"ti": choice["ti"], "schedule": choice["schedule"], "tuning_s": t_tune,
+                  "trials": [{k: v for k, v in t.items()} for t in choice["trials"]]},
         "batched_s": t_bat, "sequential_s": t_seq, "speedup": t_seq / t_bat,
         "batched_cell_iter_per_s": work / t_bat, "sequential_cell_iter_per_s": work / t_seq,
-        "iterations_equal": it_bat == it_seq, "states_bitwise_equal": all(same),
+        "iterations_equal": it_bat == it_seq, "states_bitwise_equal": same, "state_rel_diff_max": rel,
         "converged_cases": int(sum(i < niter for i in it_bat)),
         "iterations_min_max": [min(it_bat), max(it_bat)], "batch_launches": launches,
     }
@@ -105,9 +122,10 @@ def main():
     ap.add_argument("--monitor", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--no-tune", action="store_true", help="default tile height and schedule 0")
     a = ap.parse_args()
     print(json.dumps(compare(a.cases, a.niter, a.stop_ratio, a.monitor, a.seed,
-                             1 if a.precision == "mixed" else 0)))
+                             1 if a.precision == "mixed" else 0, not a.no_tune)))
 
 
 if __name__ == "__main__":

@@ -189,6 +189,13 @@ int tns_batch_run(tns_batch *b, int niter, int monitor_every, double stop_ratio,
 /* Per-case active mask (1 = iterate).  Re-activating a case that failed clears its
  * failure: upload a finite state to it first. */
 int tns_batch_set_active(tns_batch *b, const int *active);
+
+/* How a batch iteration is scheduled: 0 (default) = one launch per kernel phase over
+ * the tiles of all active cases; 1 = every case's own tns_run launches, the cases on
+ * parallel branches of one CUDA graph so they run concurrently.  Results are identical;
+ * which is faster depends on the case mix (tnsgpu.autotune measures both). */
+int tns_batch_set_schedule(tns_batch *b, int schedule);
+int tns_batch_get_schedule(tns_batch *b);
 int tns_batch_get_active(tns_batch *b, int *active);
 long long tns_batch_launch_count(tns_batch *b);
 const char *tns_batch_last_error(tns_batch *b);

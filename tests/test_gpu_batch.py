@@ -65,15 +65,17 @@ def _solo(mesh, flow, c0, ri, precision, chunks, monitor=0):
     return out, rec
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_batch_equals_solo_runs(precision):
+def test_batch_equals_solo_runs(precision, schedule):
     mem = _members(precision)
     solvers = []
     for name, mesh, flow, c0, ri in mem:
         s = Solver(mesh, flow, ri, precision=precision)
         s.upload(c0)
         solvers.append(s)
-    b = Batch(solvers)
+    b = Batch(solvers, schedule=schedule)
+    assert b.schedule == schedule
     # odd then even iteration counts: the mixed path's state parity crosses calls
     r1 = b.run(3, monitor_every=0)
     r2 = b.run(4, monitor_every=2)
@@ -137,14 +139,15 @@ def test_convergence_mask_stops_cases_at_their_criterion():
     b.close()
 
 
-def test_non_finite_case_is_masked_and_others_continue():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_non_finite_case_is_masked_and_others_continue(schedule):
     mem = _members(1, pick=[0, 1])
     solvers = [Solver(m, f, ri, precision=1) for _, m, f, _, ri in mem]
     bad = mem[0][3].copy()
     bad[0, 7] = np.nan  # a NaN density in a restart state: arithmetic only, no indexing
     solvers[0].upload(bad)
     solvers[1].upload(mem[1][3])
-    b = Batch(solvers)
+    b = Batch(solvers, schedule=schedule)
     with pytest.raises(_lib.TnsError) as e:
         b.run(4, monitor_every=2)
     assert e.value.code == _lib.TNS_ERR_NONFINITE
@@ -154,6 +157,11 @@ def test_non_finite_case_is_masked_and_others_continue():
     _, mesh, flow, c0, ri = mem[1]
     (q, _), _ = _solo(mesh, flow, c0, ri, 1, [8])
     np.testing.assert_array_equal(solvers[1].download(), q)
+    # a finite state uploaded again and the case re-activated: it runs and stays finite
+    solvers[0].upload(mem[0][3])
+    b.set_active([1, 1])
+    r = b.run(2, monitor_every=1)
+    assert list(r.status) == [0, 0] and list(r.iterations) == [2, 2]
     b.close()
 
 
@@ -176,3 +184,45 @@ def test_sweep_members_match_solo():
         (q, _), _ = _solo(mesh, flow, c0, ri, 1, [20])
         np.testing.assert_array_equal(s.download(), q, err_msg=c.name)
     b.close()
+
+
+@pytest.mark.parametrize("ti", [4, 16])
+def test_tile_height_variants(ti):
+    """The TI = 4 and TI = 16 builds: FP64 bit-identical to TI = 8 (same per-cell
+    arithmetic), mixed within the mixed path's own FP32 tolerance (its per-tile
+    reference flux moves with the tiling)."""
+    from tnsgpu import autotune
+    assert ti in autotune.available_tile_heights()
+    for precision in (0, 1):
+        # the port case's C5 is ill-conditioned in the mixed mode (its FP32 envelope is
+        # wider than these tolerances); it is checked in FP64 only
+        for name, mesh, flow, c0, ri in _members(precision, pick=[0, 3, 5] if precision == 0 else [0, 1, 3]):
+            s = Solver(mesh, flow, ri, precision=precision, lib=_lib.variant_path(ti))
+            s.upload(c0)
+            s.run(5, 0)
+            q = s.download()
+            s.close()
+            (q8, _), _ = _solo(mesh, flow, c0, ri, precision, [5])
+            if precision == 0:
+                np.testing.assert_array_equal(q, q8, err_msg=f"{name} TI={ti}")
+            else:
+                rel = np.max(np.abs(q - q8), axis=1) / np.max(np.abs(q8), axis=1)
+                assert np.all(rel < np.array([2e-6, 1e-4, 1e-4, 2e-6, 5e-5])), (name, ti, rel)
+
+
+def test_autotune_batch_picks_a_timed_configuration():
+    from tnsgpu import autotune
+    mem = _members(1, pick=[0, 1, 2])
+
+    def make(lib):
+        out = []
+        for _, mesh, flow, c0, ri in mem:
+            s = Solver(mesh, flow, ri, precision=1, lib=lib)
+            s.upload(c0)
+            out.append(s)
+        return out
+
+    r = autotune.tune_batch(make, iters=3, warmup=1)
+    assert r["ti"] in (4, 8, 16) and r["schedule"] in (0, 1)
+    timed = [t for t in r["trials"] if "s_per_iter" in t]
+    assert len(timed) == 6 and r["s_per_iter"] == min(t["s_per_iter"] for t in timed)
