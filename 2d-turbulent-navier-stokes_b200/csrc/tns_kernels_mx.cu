@@ -355,9 +355,9 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
-    load_nodes(M, i0, j0, S.nx, S.ny);
+    load_nodes(M, i0, j0, S.nx, S.ny, VNT);
     __syncthreads();
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
+    for (int s = tid; s < NSLOT; s += VNT) {
         const int li = s / SW, lj = s % SW;
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
@@ -377,7 +377,7 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
         S.u[s] = p.u; S.v[s] = p.v; S.t[s] = p.t; S.rho[s] = p.rho; S.ri[s] = p.ri;
     }
     __syncthreads();
-    for (int s = tid; s < NAVG; s += NTHREADS) {
+    for (int s = tid; s < NAVG; s += VNT) {
         const int la = s / AW, lb = s % AW;
         const int a = i0 + la, b = j0 + lb;
         if (a > M.ni || b > M.nj) continue;
@@ -420,36 +420,52 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
         S.ar[s] = dmax1(P.rtol, rn * idf);
     }
     __syncthreads();
-    for (int f = tid; f < NIFM; f += NTHREADS) {
-        const int ii = f / TJ, jj = f % TJ;
-        const int i = i0 + ii, j = j0 + jj;
-        if (i > M.ni || j >= M.nj) continue;
+    // all faces of the tile in one loop (i-faces first): at most three faces per thread,
+    // one inlined copy of the face flux
+    for (int f = tid; f < NIFM + NJFM; f += VNT) {
+        int sa, sc, ab, ad, nb, nd;
+        if (f < NIFM) {
+            // i-face: orientation of cell (i-1, j) as its face 2, or of (0, j) as its face 4
+            const int ii = f / TJ, jj = f % TJ;
+            const int i = i0 + ii, j = j0 + jj;
+            if (i > M.ni || j >= M.nj) continue;
+            const int sL = ii * SW + jj + 1, sR = sL + SW;  // cells (i-1, j), (i, j)
+            const int aLo = ii * AW + jj, aHi = aLo + 1;    // nodes (i, j), (i, j+1)
+            const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
+            if (i == 0) {  // face 4: B=N4, D=N1
+                sa = sR; sc = sL; ab = aHi; ad = aLo; nb = nHi; nd = nLo;
+            } else {  // face 2: B=N2, D=N3
+                sa = sL; sc = sR; ab = aLo; ad = aHi; nb = nLo; nd = nHi;
+            }
+        } else {
+            // j-face: orientation of cell (i, j-1) as its face 3, or of (i, 0) as its face 1
+            const int g = f - NIFM;
+            const int ii = g / AW, jj = g % AW;
+            const int i = i0 + ii, j = j0 + jj;
+            if (i >= M.ni || j > M.nj) continue;
+            const int sB = (ii + 1) * SW + jj, sT = sB + 1;  // cells (i, j-1), (i, j)
+            const int aL = ii * AW + jj, aR = aL + AW;       // nodes (i, j), (i+1, j)
+            const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
+            if (j == 0) {  // face 1: B=N1, D=N2
+                sa = sT; sc = sB; ab = aL; ad = aR; nb = nL; nd = nR;
+            } else {  // face 3: B=N3, D=N4
+                sa = sB; sc = sT; ab = aR; ad = aL; nb = nR; nd = nL;
+            }
+        }
         float out[4];
-        const int sL = ii * SW + jj + 1, sR = sL + SW;
-        const int aLo = ii * AW + jj, aHi = aLo + 1;
-        const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
-        if (i == 0) face_flux_mx(P, S, sR, sL, aHi, aLo, nHi, nLo, out);
-        else face_flux_mx(P, S, sL, sR, aLo, aHi, nLo, nHi, out);
+        face_flux_mx(P, S, sa, sc, ab, ad, nb, nd, out);
+        if (f < NIFM) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
-    }
-    for (int f = tid; f < NJFM; f += NTHREADS) {
-        const int ii = f / AW, jj = f % AW;
-        const int i = i0 + ii, j = j0 + jj;
-        if (i >= M.ni || j > M.nj) continue;
-        float out[4];
-        const int sB = (ii + 1) * SW + jj, sT = sB + 1;
-        const int aL = ii * AW + jj, aR = aL + AW;
-        const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
-        if (j == 0) face_flux_mx(P, S, sT, sB, aL, aR, nL, nR, out);
-        else face_flux_mx(P, S, sB, sT, aR, aL, nR, nL, out);
+            for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
+        } else {
 #pragma unroll
-        for (int k = 0; k < 4; k++) S.fj[k][f] = out[k];
+            for (int k = 0; k < 4; k++) S.fj[k][f - NIFM] = out[k];
+        }
     }
     __syncthreads();
     const int tj = threadIdx.x, ti = threadIdx.y;
     const int i = i0 + ti, j = j0 + tj;
-    if (i >= M.ni || j >= M.nj) return;
+    if (ti >= TI || i >= M.ni || j >= M.nj) return;
     const size_t cell = (size_t)i * M.nj + j;
     const int f1 = ti * AW + tj, f3 = f1 + 1;
     const int f4 = ti * TJ + tj, f2 = f4 + TJ;
@@ -459,7 +475,7 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
         vis[k * ncell + cell] = ((s1 * S.fj[k][f1] + S.fi[k][f2]) + S.fj[k][f3]) + s4 * S.fi[k][f4];
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
+__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx(Params P, Mesh M, const double* __restrict__ q,
                                                          float* __restrict__ vis) {
     viscous_mx_tile(P, M, q, vis, blockIdx.x, blockIdx.y);
 }
@@ -682,7 +698,7 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation_mx_batch(const BatchCa
     dissipation_mx_tile(c.P, c.M, c.qmx[parity], c.df, c.dtf, c.dtmin, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
                                                                                 const int4* __restrict__ tiles,
                                                                                 const int* __restrict__ active,
                                                                                 int parity) {
@@ -732,7 +748,7 @@ void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* activ
     if (kernel == 0)
         k_dissipation_mx_batch<<<ntiles, blk, diss_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
     else if (kernel == 1)
-        k_viscous_mx_batch<<<ntiles, blk, visc_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
+        k_viscous_mx_batch<<<ntiles, dim3(TJ, VROWS), visc_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
     else
         k_stage_mx_batch<<<ntiles, blk, stage_mx_smem_bytes(), s>>>(cases, tiles, active, parity, stage, monitor);
 }
@@ -743,7 +759,7 @@ void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, flo
 }
 
 void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* vis, cudaStream_t s) {
-    k_viscous_mx<<<tile_grid_mx(M), dim3(TJ, TI), visc_mx_smem_bytes(), s>>>(P, M, q, vis);
+    k_viscous_mx<<<tile_grid_mx(M), dim3(TJ, VROWS), visc_mx_smem_bytes(), s>>>(P, M, q, vis);
 }
 
 void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,

@@ -25,6 +25,13 @@ namespace tns {
 constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
 constexpr int TI = TNS_TI;  // tile extent along i
 constexpr int NTHREADS = TJ * TI;
+// The viscous kernels may run one extra row of threads: a tile has (TI+1)*TJ + TI*(TJ+1)
+// faces, which TI+1 rows of threads cover in two rounds.
+#ifndef TNS_VISC_EXTRA_ROW
+#define TNS_VISC_EXTRA_ROW 0
+#endif
+constexpr int VROWS = TI + TNS_VISC_EXTRA_ROW;
+constexpr int VNT = TJ * VROWS;
 
 
 // Halo-1 slot grid (TI+2) x (TJ+2), node grid (TI+3) x (TJ+3) (nodes of every halo cell).
@@ -35,9 +42,10 @@ constexpr int NNODE = (TI + 3) * NW;
 constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
 constexpr int NAVG = (TI + 1) * AW;
 
-__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny) {
+__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny,
+                                           int nthreads = NTHREADS) {
     const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int s = tid; s < NNODE; s += NTHREADS) {
+    for (int s = tid; s < NNODE; s += nthreads) {
         const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
         if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
             const size_t n = (size_t)a * (M.nj + 1) + b;
