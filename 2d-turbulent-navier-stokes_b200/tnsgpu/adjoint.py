@@ -1,0 +1,933 @@
+"""Discrete adjoint (reverse-mode sensitivities) of the RK4 / JST / viscous scheme.
+
+The reference has no adjoint.  This module gives gradients of an objective J(Q_N) of
+the state after N RK4 iterations with respect to inflow parameters (P0, T0), the
+cold-start Mach number AMACHINIT and mesh-node coordinates (wall shape):
+
+* ``Scheme`` restates one RK4 iteration of the solver (turbnstwod.f90:95-146 with
+  DISSIPATION solver_state.f90:70-225, COMPUTE_PRIMITIVE_VARS turbnstwod.f90:204-227,
+  APPLY_BOUNDARY boundary.f90:24-122 for BC types 2-5, COMPUTE_VISCOUS
+  viscous.f90:29-217, COMPUTE_SOURCE_TERMS source_terms.f90:24-104, COMPUTE_RESIDUAL and
+  UPDATE_SOLUTION residual.f90:23-83) in FP64 PyTorch tensor arithmetic on the
+  structured i x j block, so torch.autograd differentiates it exactly.  Geometry (face
+  vectors, volumes, centroids, DL, mirrored ghost centroids; geometry.f90:55-149) is
+  computed from the node coordinates inside the graph, so node displacements are
+  differentiable parameters.
+* ``transient_gradient`` runs the primal on the GPU through the C ABI (FP64 path),
+  keeping the state after every iteration as a checkpoint, and then sweeps backwards:
+  for n = N-1 .. 0 it recomputes iteration n from checkpoint Q_n inside autograd and
+  pulls the adjoint state back through it (one iteration of recomputation per step:
+  RK-stage intermediates are rebuilt, never stored).  ``TransientObjective`` wraps the
+  same as a ``torch.autograd.Function``.
+* ``fixed_point_adjoint`` iterates lambda <- dJ/dQ + lambda dG/dQ at a frozen state, the
+  adjoint of a converged steady solution.
+
+Scope: IAXIS 0 and 1, BC types 2, 3, 4 and 5 (the types of the ramp and nozzle cases),
+any LOCAL and NPSEUDO.  Type 6 (injection port) and 7 (boundary-layer inflow) raise
+NotImplementedError.  Objective helpers evaluate on the final state Q_N with its ghost
+cells from APPLY_BOUNDARY: the wall pressure force and the mass-weighted total-pressure
+loss between two sides.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from .formats import Flow, Mesh
+
+# constants.f90:12-60
+RUNIV = 8314.0
+CMU = 0.09
+ALPHA_T = 0.00052
+BETA_T = 0.2
+CONST1 = 21.479
+CONST2 = 21.394
+CONST3 = 1.5
+SUTH = 0.00000011848
+C02 = 0.25
+C04 = 0.00390625
+CFLTURB = 0.5
+YAXIS_THRESH = 0.001
+AMU_THRESH = 0.001
+ALPHA_RK = (0.25, 1.0 / 3.0, 0.5, 1.0)
+
+
+def dmax(a, b):
+    """DMAX1: a >= b ? a : b (gradient to the selected argument)."""
+    return torch.where(a >= b, a, b)
+
+
+def dmin(a, b):
+    return torch.where(a <= b, a, b)
+
+
+def _safe_sqrt(x):
+    """sqrt with a zero gradient where x == 0 (PK clamped to 0 by DMAX1)."""
+    pos = x > 0
+    return torch.where(pos, torch.sqrt(torch.where(pos, x, torch.ones_like(x))), torch.zeros_like(x))
+
+
+def _pad(a):
+    """(ni, nj) -> (ni+2, nj+2) with the ring holding copies of the adjacent cell."""
+    return torch.nn.functional.pad(a[None, None], (1, 1, 1, 1), mode="replicate")[0, 0]
+
+
+@dataclasses.dataclass
+class Params:
+    """Flow parameters as tensors (P0, T0, AMACHINIT may carry gradients)."""
+    p0: torch.Tensor
+    t0: torch.Tensor
+    amachinit: torch.Tensor
+    flow: Flow
+
+    @property
+    def rr(self):
+        return RUNIV / self.flow.amol
+
+    @property
+    def cv(self):
+        return self.rr / (self.flow.gama - 1.0)
+
+    @property
+    def cp(self):
+        return self.cv * self.flow.gama
+
+    def s0(self):
+        rho0 = self.p0 / (self.rr * self.t0)
+        return self.p0 / rho0 ** self.flow.gama
+
+    def cold(self):
+        """Isentropic cold start (turbnstwod.f90:53-71): (RHO, U, E, RINIT)."""
+        g = self.flow.gama
+        dyn = 1.0 + (g - 1.0) * 0.5 * self.amachinit ** 2
+        tinit = self.t0 / dyn
+        pinit = self.p0 / dyn ** (g / (g - 1.0))
+        uinit = self.amachinit * torch.sqrt(g * self.rr * tinit)
+        einit = self.cv * tinit + 0.5 * uinit ** 2
+        rhoinit = pinit / (self.rr * tinit)
+        amu = SUTH * math.sqrt(self.flow.amol) * tinit ** 0.6
+        return rhoinit, uinit, einit, amu / rhoinit
+
+
+class Scheme:
+    """One RK4 iteration of the solver as differentiable FP64 tensor arithmetic.
+
+    ``mesh`` must be one structured block numbered as ``cases.structured_mesh`` numbers
+    it (cell (i, j) id i*NJ+j+1, node (i, j) id i*(NJ+1)+j+1, faces 1..4 = j-, i+, j+,
+    i-).  State tensors are [5, NI, NJ]; node coordinates [NI+1, NJ+1].
+    """
+
+    def __init__(self, mesh: Mesh, flow: Flow, device="cpu", rinit: Optional[float] = None):
+        if mesh.shape is None:
+            raise ValueError("the adjoint needs a structured block (Mesh.shape)")
+        ni, nj = mesh.shape
+        self.ni, self.nj, self.flow, self.device = ni, nj, flow, torch.device(device)
+        ii, jj = np.meshgrid(np.arange(ni), np.arange(nj), indexing="ij")
+        expect = np.stack([ii * (nj + 1) + jj + 1, (ii + 1) * (nj + 1) + jj + 1,
+                           (ii + 1) * (nj + 1) + jj + 2, ii * (nj + 1) + jj + 2], -1).reshape(-1, 4)
+        if not np.array_equal(mesh.nod, expect):
+            raise ValueError("mesh is not in structured (i, j) numbering")
+        if np.any((mesh.ntype < 2) | (mesh.ntype > 5)):
+            bad = sorted(set(mesh.ntype.tolist()) - {2, 3, 4, 5})
+            raise NotImplementedError(f"BC types {bad}: the adjoint covers types 2-5")
+        if flow.iaxis not in (0, 1):
+            raise ValueError("IAXIS must be 0 or 1")
+        self.fixed_rinit = rinit
+        self.mesh_template = mesh
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.x0 = torch.tensor(mesh.x.reshape(ni + 1, nj + 1), **f64)
+        self.y0 = torch.tensor(mesh.y.reshape(ni + 1, nj + 1), **f64)
+        # BC type of each ghost, per side, along the side
+        types = {1: np.zeros(ni, np.int64), 2: np.zeros(nj, np.int64), 3: np.zeros(ni, np.int64),
+                 4: np.zeros(nj, np.int64)}
+        par = mesh.nparent - 1
+        pi, pj = par // nj, par % nj
+        for k in range(mesh.nghosts):
+            s = int(mesh.nside[k])
+            types[s][pi[k] if s in (1, 3) else pj[k]] = mesh.ntype[k]
+        self.types = {s: torch.tensor(v, device=dev) for s, v in types.items()}
+        # every ghost of the ring at once: parent / opposite cell (flat interior index),
+        # flat index in the padded field, BC type; sides 1, 3 along i, then 4, 2 along j
+        ai, aj = np.arange(ni), np.arange(nj)
+        par_i = np.concatenate([ai, ai, np.zeros(nj, int), np.full(nj, ni - 1)])
+        par_j = np.concatenate([np.zeros(ni, int), np.full(ni, nj - 1), aj, aj])
+        opp_i = np.concatenate([ai, ai, np.ones(nj, int), np.full(nj, ni - 2)])
+        opp_j = np.concatenate([np.ones(ni, int), np.full(ni, nj - 2), aj, aj])
+        g_i = np.concatenate([ai + 1, ai + 1, np.zeros(nj, int), np.full(nj, ni + 1)])
+        g_j = np.concatenate([np.zeros(ni, int), np.full(ni, nj + 1), aj + 1, aj + 1])
+        it = lambda a: torch.tensor(a, dtype=torch.int64, device=dev)
+        self.g_par = it(par_i * nj + par_j)
+        self.g_opp = it(opp_i * nj + opp_j)
+        self.g_pad = it(g_i * (nj + 2) + g_j)
+        self.g_type = torch.cat([self.types[1], self.types[3], self.types[4], self.types[2]])
+        self.types_present = sorted(set(int(t) for t in np.unique(mesh.ntype)))
+        self._node_average_matrices(mesh)
+
+    # ------------------------------------------------------------------ set-up
+    def _node_average_matrices(self, mesh: Mesh):
+        """NODAL_AVERAGE (viscous.f90:40-124) as sparse maps from the cell values and
+        the ghost values (ghosts in bc.in order) to the nodes.  The Fortran visits the
+        elements in id order, then the ghosts in bc.in order; a type-4 ghost zeroes VN,
+        a type-5 ghost zeroes UN, VN and sets RN = RTOLERANCE*RTRED, after which later
+        contributions add to the reset value; every visit counts.  Per node and
+        component the average is therefore (base + sum of the contributions after the
+        last reset) / count, which these matrices encode."""
+        ni, nj = self.ni, self.nj
+        nn = (ni + 1) * (nj + 1)
+        neles, ng = mesh.neles, mesh.nghosts
+        # contribution lists per node: (kind, index) with kind 0 = cell, 1 = ghost line
+        contrib = [[] for _ in range(nn)]
+        for c in range(neles):
+            for k in range(4):
+                contrib[mesh.nod[c, k] - 1].append((0, c))
+        resets = {"u": [-1] * nn, "v": [-1] * nn, "r": [-1] * nn}
+        for g in range(ng):
+            p = mesh.nparent[g] - 1
+            s = mesh.nside[g]
+            n1 = mesh.nod[p, s - 1] - 1
+            n2 = mesh.nod[p, s % 4] - 1
+            for n in (n1, n2):
+                contrib[n].append((1, g))
+                pos = len(contrib[n]) - 1
+                if mesh.ntype[g] == 4:
+                    resets["v"][n] = pos
+                elif mesh.ntype[g] == 5:
+                    resets["u"][n] = resets["v"][n] = resets["r"][n] = pos
+        # ghost line -> flat index into the padded (ni+2, nj+2) ghost ring
+        par = mesh.nparent - 1
+        pi, pj = par // nj, par % nj
+        side = mesh.nside
+        gi = np.where(side == 2, pi + 2, np.where(side == 4, pi, pi + 1))
+        gj = np.where(side == 1, pj, np.where(side == 3, pj + 2, pj + 1))
+        gflat = gi * (nj + 2) + gj
+        cflat = lambda c: ((c // nj) + 1) * (nj + 2) + (c % nj) + 1  # cell -> padded flat
+        npad = (ni + 2) * (nj + 2)
+        self.count = torch.tensor([len(c) for c in contrib], dtype=torch.float64, device=self.device)
+        self.wall_r_base = torch.zeros(nn, dtype=torch.float64, device=self.device)
+        mats = {}
+        for comp in ("u", "v", "t", "rho", "r"):
+            rows, cols = [], []
+            last = resets.get(comp, [-1] * nn)
+            for n in range(nn):
+                for pos, (kind, idx) in enumerate(contrib[n]):
+                    if pos <= last[n]:
+                        continue
+                    rows.append(n)
+                    cols.append(cflat(idx) if kind == 0 else gflat[idx])
+            mats[comp] = (torch.tensor(rows, dtype=torch.int64, device=self.device),
+                          torch.tensor(cols, dtype=torch.int64, device=self.device))
+        self.navg = mats
+        self.r_reset = torch.tensor([1.0 if resets["r"][n] >= 0 else 0.0 for n in range(nn)],
+                                    dtype=torch.float64, device=self.device)
+
+    # ------------------------------------------------------------------ pieces
+    def params(self, p0=None, t0=None, amachinit=None) -> Params:
+        f = self.flow
+        t = lambda v, d: torch.as_tensor(d if v is None else v, dtype=torch.float64, device=self.device)
+        return Params(t(p0, f.p0), t(t0, f.t0), t(amachinit, f.amachinit), f)
+
+    def rtol(self, prm: Params):
+        rinit = self.fixed_rinit if self.fixed_rinit is not None else prm.cold()[3]
+        return rinit * self.flow.rtred
+
+    def cold_state(self, prm: Params):
+        rho, u, e, rinit = prm.cold()
+        if self.fixed_rinit is not None:
+            rinit = self.fixed_rinit
+        one = torch.ones((self.ni, self.nj), dtype=torch.float64, device=self.device)
+        return torch.stack([rho * one, rho * u * one, 0.0 * one, rho * e * one, rho * rinit * one])
+
+    def geometry(self, x, y) -> Dict[str, torch.Tensor]:
+        """COMPUTE_GEOMETRY (geometry.f90:55-149) from node coordinates [NI+1, NJ+1]."""
+        X1, X2, X3, X4 = x[:-1, :-1], x[1:, :-1], x[1:, 1:], x[:-1, 1:]
+        Y1, Y2, Y3, Y4 = y[:-1, :-1], y[1:, :-1], y[1:, 1:], y[:-1, 1:]
+        xcc = (X1 + X2 + X3 + X4) * 0.25
+        ycc = (Y1 + Y2 + Y3 + Y4) * 0.25
+        L = lambda xa, ya, xb, yb: torch.sqrt((xa - xb) * (xa - xb) + (ya - yb) * (ya - yb))
+        dl = dmin(dmin(dmin(L(X1, Y1, X2, Y2), L(X2, Y2, X3, Y3)), L(X3, Y3, X4, Y4)), L(X4, Y4, X1, Y1))
+        pts = [(X1, Y1), (X2, Y2), (X3, Y3), (X4, Y4)]
+        sx, sy = [], []
+        for k in range(4):
+            (xa, ya), (xb, yb) = pts[k], pts[(k + 1) % 4]
+            if self.flow.iaxis == 1:
+                sx.append((yb - ya) * (ya + yb) * 0.5)
+                sy.append(-(xb - xa) * (ya + yb) * 0.5)
+            else:
+                sx.append(yb - ya)
+                sy.append(-(xb - xa))
+        vol = 0.5 * ((X3 - X1) * (Y4 - Y2) - (X4 - X2) * (Y3 - Y1))
+        if self.flow.iaxis == 1:
+            vol = vol * ycc
+        vol = torch.abs(vol)
+        # mirrored ghost centroids: 2 * face midpoint - parent centroid
+        xg, yg = _pad(xcc), _pad(ycc)
+        xg = xg.clone()
+        yg = yg.clone()
+        xg[1:-1, 0] = 2.0 * (0.5 * (X1[:, 0] + X2[:, 0])) - xcc[:, 0]
+        yg[1:-1, 0] = 2.0 * (0.5 * (Y1[:, 0] + Y2[:, 0])) - ycc[:, 0]
+        xg[-1, 1:-1] = 2.0 * (0.5 * (X2[-1, :] + X3[-1, :])) - xcc[-1, :]
+        yg[-1, 1:-1] = 2.0 * (0.5 * (Y2[-1, :] + Y3[-1, :])) - ycc[-1, :]
+        xg[1:-1, -1] = 2.0 * (0.5 * (X3[:, -1] + X4[:, -1])) - xcc[:, -1]
+        yg[1:-1, -1] = 2.0 * (0.5 * (Y3[:, -1] + Y4[:, -1])) - ycc[:, -1]
+        xg[0, 1:-1] = 2.0 * (0.5 * (X4[0, :] + X1[0, :])) - xcc[0, :]
+        yg[0, 1:-1] = 2.0 * (0.5 * (Y4[0, :] + Y1[0, :])) - ycc[0, :]
+        return dict(x=x, y=y, xc=xg, yc=yg, dl=dl, vol=vol, sx=sx, sy=sy)
+
+    def amu(self, t):
+        return SUTH * math.sqrt(self.flow.amol) * t ** 0.6
+
+    def primitive(self, C, prm: Params):
+        """COMPUTE_PRIMITIVE_VARS (turbnstwod.f90:204-227) on the cells."""
+        rho = C[0]
+        u = C[1] / rho
+        v = C[2] / rho
+        e = C[3] / rho
+        t = (e - 0.5 * (u * u + v * v)) / prm.cv
+        p = rho * prm.rr * t
+        rt = C[4] / rho
+        f = [C[1], rho * u * u + p, rho * u * v, (C[3] + p) * u, rho * rt * u]
+        g = [C[2], None, rho * v * v + p, (C[3] + p) * v, rho * rt * v]
+        g[1] = f[2]
+        return dict(u=u, v=v, t=t, p=p, c=[C[m] for m in range(5)], f=f, g=g)
+
+    def _ghosts(self, pr, opp, prm: Params):
+        """APPLY_BOUNDARY (boundary.f90:53-122) for every ghost of the ring at once:
+        parent values ``pr`` and the values of the cell opposite the boundary face
+        ``opp`` (1-D over the ghosts).  Each BC type present in the mesh is evaluated on
+        the whole ring and selected by the ghost's type."""
+        flow = self.flow
+        rr, cv, cp, g = prm.rr, prm.cv, prm.cp, flow.gama
+
+        def fluxes(rho, u, v, t, p):
+            c1, c2 = rho * u, rho * v
+            c3 = rho * (cv * t + 0.5 * (u * u + v * v))
+            f3 = rho * u * v
+            return [rho, c1, c2, c3], [c1, rho * u * u + p, f3, (c3 + p) * u], \
+                   [c2, f3, rho * v * v + p, (c3 + p) * v]
+
+        sel = {}
+        if 2 in self.types_present:  # subsonic inlet at P0, T0 (isentropic)
+            u2 = torch.abs(pr["u"])
+            v2 = -pr["v"]
+            t2 = prm.t0 - 0.5 * (u2 * u2 + v2 * v2) / cp
+            rho2 = (prm.s0() / (rr * t2)) ** (1.0 / (1.0 - g))
+            p2 = rho2 * rr * t2
+            c2, f2, gg2 = fluxes(rho2, u2, v2, t2, p2)
+            c5 = rho2 * (self.amu(t2) / rho2)
+            sel[2] = dict(u=u2, v=v2, t=t2, p=p2, c=c2 + [c5], f=f2 + [c5 * u2], g=gg2 + [c5 * v2])
+        if 3 in self.types_present:  # extrapolation (PAMB >= 0 fixes P)
+            u3 = torch.abs(2.0 * pr["u"] - opp["u"])
+            v3 = 2.0 * pr["v"] - opp["v"]
+            t3 = 2.0 * pr["t"] - opp["t"]
+            p3 = 2.0 * pr["p"] - opp["p"]
+            if flow.pamb >= 0.0:
+                p3 = torch.full_like(p3, flow.pamb)
+            rho3 = p3 / (rr * t3)
+            c3, f3, g3 = fluxes(rho3, u3, v3, t3, p3)
+            sel[3] = dict(u=u3, v=v3, t=t3, p=p3, c=c3 + [pr["c"][4]], f=f3 + [pr["f"][4]],
+                          g=g3 + [pr["g"][4]])
+        if 4 in self.types_present:  # symmetry
+            c4, f4, g4 = fluxes(pr["c"][0], pr["u"], -pr["v"], pr["t"], pr["p"])
+            sel[4] = dict(u=pr["u"], v=-pr["v"], t=pr["t"], p=pr["p"], c=c4 + [pr["c"][4]],
+                          f=f4 + [pr["f"][4]], g=g4 + [-pr["g"][4]])
+        if 5 in self.types_present:  # no-slip wall
+            u5, v5, rho5 = -pr["u"], -pr["v"], pr["c"][0]
+            e5 = cv * pr["t"] + 0.5 * (u5 * u5 + v5 * v5)
+            P = pr["p"]
+            sel[5] = dict(u=u5, v=v5, t=pr["t"], p=P,
+                          c=[rho5, rho5 * u5, rho5 * v5, rho5 * e5, -pr["c"][4]],
+                          f=[-pr["f"][0], 2.0 * P - pr["f"][1], -pr["f"][2], -pr["f"][3], -pr["f"][4]],
+                          g=[-pr["g"][0], -pr["g"][1], 2.0 * P - pr["g"][2], -pr["g"][3], -pr["g"][4]])
+        order = list(sel)
+
+        def pick(get):
+            r = get(sel[order[0]])
+            for ty in order[1:]:
+                r = torch.where(self.g_type == ty, get(sel[ty]), r)
+            return r
+
+        out = {k: pick(lambda T, k=k: T[k]) for k in ("u", "v", "t", "p")}
+        for k in ("c", "f", "g"):
+            out[k] = [pick(lambda T, k=k, m=m: T[k][m]) for m in range(5)]
+        return out
+
+    def boundary(self, pr, prm: Params):
+        """Padded [NI+2, NJ+2] primitive fields: cells plus the ghosts of APPLY_BOUNDARY."""
+        keys = ("u", "v", "t", "p")
+        gat = lambda a, idx: a.reshape(-1).index_select(0, idx)
+        prs = {k: gat(pr[k], self.g_par) for k in keys}
+        ops = {k: gat(pr[k], self.g_opp) for k in keys}
+        for k in ("c", "f", "g"):
+            prs[k] = [gat(a, self.g_par) for a in pr[k]]
+        gh = self._ghosts(prs, ops, prm)
+        npad = (self.ni + 2) * (self.nj + 2)
+
+        def assemble(interior, ghost):
+            ring = torch.zeros(npad, dtype=interior.dtype, device=interior.device).index_copy(0, self.g_pad, ghost)
+            return torch.nn.functional.pad(interior[None, None], (1, 1, 1, 1))[0, 0] + \
+                ring.reshape(self.ni + 2, self.nj + 2)
+
+        full = {k: assemble(pr[k], gh[k]) for k in keys}
+        for k in ("c", "f", "g"):
+            full[k] = [assemble(pr[k][m], gh[k][m]) for m in range(5)]
+        return full
+
+    @staticmethod
+    def _nb(a):
+        """The four neighbours NC1..NC4 (j-1, i+1, j+1, i-1) of every cell of a padded field."""
+        return a[1:-1, :-2], a[2:, 1:-1], a[1:-1, 2:], a[:-2, 1:-1]
+
+    def time_step(self, C, geo, prm: Params):
+        """turbnstwod.f90:97-114."""
+        rho = C[0]
+        u, v = C[1] / rho, C[2] / rho
+        vel = torch.sqrt(u * u + v * v)
+        t = (C[3] / rho - 0.5 * (u * u + v * v)) / prm.cv
+        p = rho * prm.rr * t
+        dt = self.flow.cfl * geo["dl"] / (torch.abs(vel) + torch.sqrt(self.flow.gama * prm.rr * t))
+        if self.flow.local == 0:
+            dt = torch.full_like(dt, 1.0) * torch.min(dmin(torch.full_like(dt, 100000.0), dt))
+        return dt, p
+
+    def dissipation(self, C, p, dt, geo, rtol):
+        """DISSIPATION (solver_state.f90:70-225); ghosts hold copies of their parent."""
+        P = _pad(p)
+        Pn = self._nb(P)
+        anu = (torch.abs(Pn[0] - p) + torch.abs(Pn[1] - p) + torch.abs(Pn[2] - p) + torch.abs(Pn[3] - p)) / \
+              (torch.abs(Pn[0] + p) + torch.abs(Pn[1] + p) + torch.abs(Pn[2] + p) + torch.abs(Pn[3] + p))
+        C5 = _pad(C[4])
+        c5n = self._nb(C5)
+        c5 = C[4]
+        anurt = (torch.abs(c5n[0] - c5) + torch.abs(c5n[1] - c5) + torch.abs(c5n[2] - c5) +
+                 torch.abs(c5n[3] - c5)) / dmax(torch.abs(c5n[0] + c5) + torch.abs(c5n[1] + c5) +
+                                                torch.abs(c5n[2] + c5) + torch.abs(c5n[3] + c5),
+                                                8.0 * C[0] * rtol)
+        Cp = [_pad(C[m]) for m in range(5)]
+        d2q = []
+        for m in range(5):
+            n = self._nb(Cp[m])
+            d2q.append(n[0] + n[1] + n[2] + n[3] - 4.0 * C[m])
+        vbd = geo["vol"] / dt
+        VBD = _pad(vbd)
+        vbdn = self._nb(VBD)
+        sens = [_pad(anu), _pad(anurt)]
+        out = []
+        for m in range(5):
+            S = sens[1] if m == 4 else sens[0]
+            si = S[1:-1, 1:-1]
+            sn = self._nb(S)
+            cn = self._nb(Cp[m])
+            dn = self._nb(_pad(d2q[m]))
+            D2 = D4 = None
+            for k in range(4):
+                e2 = C02 * dmax(si, sn[k])
+                e4 = dmax(torch.zeros_like(e2), C04 - e2)
+                d24 = 0.5 * (vbd + vbdn[k])
+                t2 = e2 * d24 * (cn[k] - C[m])
+                t4 = e4 * d24 * (dn[k] - d2q[m])
+                D2 = t2 if D2 is None else D2 + t2
+                D4 = t4 if D4 is None else D4 + t4
+            out.append(D2 - D4)
+        return out
+
+    def viscous(self, full, geo, prm: Params, rtol):
+        """COMPUTE_VISCOUS (viscous.f90:29-217) from the padded primitives of stage 1."""
+        flow = self.flow
+        ni, nj = self.ni, self.nj
+        rho = full["c"][0]
+        r = full["c"][4] / rho
+        vals = {"u": full["u"], "v": full["v"], "t": full["t"], "rho": rho, "r": r}
+        nodes = {}
+        for k, a in vals.items():
+            rows, cols = self.navg[k]
+            s = torch.zeros(self.count.shape[0], dtype=a.dtype, device=a.device).index_add(
+                0, rows, a.reshape(-1).index_select(0, cols))
+            if k == "r":
+                s = s + self.r_reset * (rtol * flow.rtred)
+            nodes[k] = (s / self.count).reshape(ni + 1, nj + 1)
+        nodes["r"] = dmax(torch.zeros_like(nodes["r"]) + rtol, nodes["r"])
+        x, y = geo["x"], geo["y"]
+        corner = [(slice(None, -1), slice(None, -1)), (slice(1, None), slice(None, -1)),
+                  (slice(1, None), slice(1, None)), (slice(None, -1), slice(1, None))]
+        A = {k: a[1:-1, 1:-1] for k, a in vals.items()}
+        xa, ya = geo["xc"][1:-1, 1:-1], geo["yc"][1:-1, 1:-1]
+        nbs = {k: self._nb(a) for k, a in vals.items()}
+        xcn, ycn = self._nb(geo["xc"]), self._nb(geo["yc"])
+        amu_c = SUTH * math.sqrt(flow.amol)
+        vis = None
+        for face in range(4):
+            b, d = corner[face], corner[(face + 1) % 4]
+            XB, YB, XD, YD = x[b], y[b], x[d], y[d]
+            B = {k: nodes[k][b] for k in nodes}
+            D = {k: nodes[k][d] for k in nodes}
+            Cc = {k: nbs[k][face] for k in nbs}
+            XC, YC = xcn[face], ycn[face]
+            dnr = (xa - XC) * (YB - YD) - (XB - XD) * (ya - YC)
+            gx = lambda k: ((A[k] - Cc[k]) * (YB - YD) - (B[k] - D[k]) * (ya - YC)) / dnr
+            gy = lambda k: (-(A[k] - Cc[k]) * (XB - XD) + (B[k] - D[k]) * (xa - XC)) / dnr
+            DUX, DVX, DTX, DRX = gx("u"), gx("v"), gx("t"), gx("r")
+            DUY, DVY, DTY, DRY = gy("u"), gy("v"), gy("t"), gy("r")
+            avg = lambda k: 0.25 * (A[k] + B[k] + Cc[k] + D[k])
+            UAVG, VAVG, TAVG, RHOAVG, RAVG = avg("u"), avg("v"), avg("t"), avg("rho"), avg("r")
+            if flow.iaxis == 1:
+                YAVG = 0.5 * (YB + YD)
+                VBYY = torch.where(YAVG < YAXIS_THRESH, DVY, VAVG / YAVG)
+                DIVVEL = DUX + DVY + VBYY
+            else:
+                DIVVEL = DUX + DVY
+            AMU = amu_c * TAVG ** 0.6
+            AK = AMU * prm.cp / flow.prandtl
+            CHI = RHOAVG * RAVG / (AMU * CMU)
+            FMU = torch.tanh(ALPHA_T * CHI * CHI) / torch.tanh(BETA_T * CHI * CHI)
+            AMUT = RHOAVG * RAVG * FMU
+            AKT = AMUT * prm.cp / flow.prandtlt
+            AMUEFF = AMU + AMUT
+            AKEFF = AK + AKT
+            div23 = 2.0 / 3.0
+            TXX = AMUEFF * (DUX + DUX - div23 * DIVVEL)
+            TYY = AMUEFF * (DVY + DVY - div23 * DIVVEL)
+            TXY = AMUEFF * (DUY + DVX)
+            QXX = UAVG * TXX + VAVG * TXY + AKEFF * DTX
+            QYY = UAVG * TXY + VAVG * TYY + AKEFF * DTY
+            SX, SY = geo["sx"][face], geo["sy"][face]
+            f = [TXX * SX + TXY * SY, TXY * SX + TYY * SY, QXX * SX + QYY * SY,
+                 AMUEFF * DRX * SX + AMUEFF * DRY * SY]
+            vis = f if vis is None else [vis[k] + f[k] for k in range(4)]
+        return vis
+
+    def source(self, full, geo, prm: Params):
+        """COMPUTE_SOURCE_TERMS (source_terms.f90:24-104): (SOURCE3, SOURCE5)."""
+        flow = self.flow
+        u, v = full["u"], full["v"]
+        r = full["c"][4] / full["c"][0]
+        q = torch.sqrt(u * u + v * v)
+        X, Y = self._nb(geo["xc"]), self._nb(geo["yc"])
+        U, V, R, Q = self._nb(u), self._nb(v), self._nb(r), self._nb(q)
+        XA, XB, XC, XD = X
+        YA, YB, YC, YD = Y
+        dnr = (XA - XC) * (YB - YD) - (XB - XD) * (YA - YC)
+        gx = lambda F: ((F[0] - F[2]) * (YB - YD) - (F[1] - F[3]) * (YA - YC)) / dnr
+        gy = lambda F: (-(F[0] - F[2]) * (XB - XD) + (F[1] - F[3]) * (XA - XC)) / dnr
+        DQX, DRX, DUX, DVX = gx(Q), gx(R), gx(U), gx(V)
+        DQY, DRY, DUY, DVY = gy(Q), gy(R), gy(U), gy(V)
+        rho = full["c"][0][1:-1, 1:-1]
+        ri = full["c"][4][1:-1, 1:-1] / rho
+        amu = self.amu(full["t"][1:-1, 1:-1])
+        chi = rho * ri / (CMU * amu)
+        fmu = torch.tanh(ALPHA_T * chi * chi) / torch.tanh(BETA_T * chi * chi)
+        fr2 = torch.tanh(torch.sqrt(chi)) / torch.tanh(chi * math.sqrt(2.0 * math.sqrt(CMU)))
+        amut = fmu * rho * ri
+        phi = DQX * DRX + DQY * DRY
+        dee = torch.where(phi > 0.0, DRX * DRX + DRY * DRY, torch.zeros_like(phi))
+        div23 = 2.0 / 3.0
+        ycc = geo["yc"][1:-1, 1:-1]
+        if flow.iaxis == 1:
+            vbyy = torch.where(ycc < YAXIS_THRESH, DVY, full["v"][1:-1, 1:-1] / ycc)
+            divvel = DUX + DVY + vbyy
+            pk = amut / rho * (DUX * DUX + DVY * DVY + vbyy * vbyy + DUX * DUX + DVY * DVY +
+                               vbyy * vbyy + (DUY + DVX) * (DUY + DVX) - div23 * divvel * divvel)
+        else:
+            divvel = DUX + DVY
+            pk = amut / rho * (DUX * DUX + DVY * DVY + DUX * DUX + DVY * DVY +
+                               (DUY + DVX) * (DUY + DVX) - div23 * divvel * divvel)
+        pk = dmax(pk, torch.zeros_like(pk))
+        ratio = amut / dmax(amut, AMU_THRESH * amu)
+        pw = ratio ** flow.npseudo if flow.npseudo >= 0 else 1.0 / ratio ** (-flow.npseudo)
+        s5 = (rho * (CONST1 - CONST2 * fr2) * _safe_sqrt(ri * pk) - rho * CONST3 * dee) * pw
+        s3 = None
+        if flow.iaxis == 1:
+            ttt = (amu + amut) * (vbyy + vbyy - div23 * divvel)
+            s3 = (full["p"][1:-1, 1:-1] - ttt) / ycc
+        return s3, s5
+
+    def residual(self, full, geo, s3, s5):
+        """COMPUTE_RESIDUAL (residual.f90:23-62)."""
+        R = []
+        sx, sy = geo["sx"], geo["sy"]
+        for m in range(5):
+            F, G = full["f"][m], full["g"][m]
+            FI, GI = F[1:-1, 1:-1], G[1:-1, 1:-1]
+            Fn, Gn = self._nb(F), self._nb(G)
+            acc = (FI + Fn[0]) * sx[0] + (GI + Gn[0]) * sy[0]
+            for k in range(1, 4):
+                acc = acc + (FI + Fn[k]) * sx[k] + (GI + Gn[k]) * sy[k]
+            R.append(0.5 * acc)
+        R[4] = R[4] - geo["vol"] * s5
+        if self.flow.iaxis == 1:
+            R[2] = R[2] - geo["vol"] * s3
+        return R
+
+    def iteration(self, Cold, geo, prm: Params):
+        """One RK4 iteration (turbnstwod.f90:97-146): Q_old [5, NI, NJ] -> Q_new."""
+        rtol = self.rtol(prm)
+        dt, p = self.time_step(Cold, geo, prm)
+        D = self.dissipation(Cold, p, dt, geo, rtol)
+        C = Cold
+        vis = None
+        for st in range(4):
+            full = self.boundary(self.primitive(C, prm), prm)
+            if st == 0:
+                vis = self.viscous(full, geo, prm, rtol)
+            s3, s5 = self.source(full, geo, prm)
+            R = self.residual(full, geo, s3, s5)
+            dtv = ALPHA_RK[st] * (dt / geo["vol"])
+            n0 = Cold[0] - dtv * (R[0] - D[0])
+            n1 = Cold[1] - dtv * (R[1] - vis[0] - D[1])
+            n2 = Cold[2] - dtv * (R[2] - vis[1] - D[2])
+            n3 = Cold[3] - dtv * (R[3] - vis[2] - D[3])
+            n4 = Cold[4] - dtv * CFLTURB * (R[4] - vis[3] - D[4])
+            n4 = n0 * dmax(torch.zeros_like(n0) + rtol, n4 / n0)
+            C = torch.stack([n0, n1, n2, n3, n4])
+        return C
+
+    # ------------------------------------------------------------------ objectives
+    def face_state(self, C, prm: Params, side: int):
+        """Face values (parent + ghost)/2 on one side of the final state: U, V, P, RHO, T
+        (RHO = P/(RR*T) on both sides of the face) and the face vector S."""
+        full = self.boundary(self.primitive(C, prm), prm)
+        idx = {1: ((slice(1, -1), 1), (slice(1, -1), 0)), 3: ((slice(1, -1), -2), (slice(1, -1), -1)),
+               4: ((1, slice(1, -1)), (0, slice(1, -1))), 2: ((-2, slice(1, -1)), (-1, slice(1, -1)))}[side]
+        pa, gh = idx
+        avg = lambda a: 0.5 * (a[pa] + a[gh])
+        rho = full["p"] / (prm.rr * full["t"])
+        return {"u": avg(full["u"]), "v": avg(full["v"]), "p": avg(full["p"]), "rho": avg(rho),
+                "t": avg(full["t"])}
+
+    def side_vectors(self, geo, side: int):
+        face = side - 1
+        sl = {1: (slice(None), 0), 3: (slice(None), -1), 4: (0, slice(None)), 2: (-1, slice(None))}[side]
+        return geo["sx"][face][sl], geo["sy"][face][sl]
+
+    def wall_force(self, C, geo, prm: Params, side: int = 1):
+        """Pressure force sum(p_f S) over the faces of ``side`` (per radian when IAXIS=1)."""
+        fs = self.face_state(C, prm, side)
+        sx, sy = self.side_vectors(geo, side)
+        return torch.stack([torch.sum(fs["p"] * sx), torch.sum(fs["p"] * sy)])
+
+    def total_pressure_loss(self, C, geo, prm: Params, inlet: int = 4, outlet: int = 2):
+        """1 - mass-weighted outlet P0 / mass-weighted inlet P0."""
+        g = self.flow.gama
+
+        def mean(side):
+            fs = self.face_state(C, prm, side)
+            sx, sy = self.side_vectors(geo, side)
+            m2 = (fs["u"] ** 2 + fs["v"] ** 2) / (g * prm.rr * fs["t"])
+            p0 = fs["p"] * (1.0 + 0.5 * (g - 1.0) * m2) ** (g / (g - 1.0))
+            md = torch.abs(fs["rho"] * (fs["u"] * sx + fs["v"] * sy))
+            return torch.sum(p0 * md) / torch.sum(md)
+
+        return 1.0 - mean(outlet) / mean(inlet)
+
+
+# ---------------------------------------------------------------------- parameters
+
+@dataclasses.dataclass
+class DesignSpace:
+    """Parameters of a gradient: P0, T0, AMACHINIT and displacements of chosen nodes.
+
+    ``node_ids`` are 0-based flat node indices (i*(NJ+1)+j); ``node_shape`` [n, NI+1,
+    NJ+1] gives how each displacement moves every node's y (for a wall node blended to
+    zero at the opposite boundary, the generator's (1 - f_j) column)."""
+    scheme: Scheme
+    node_shape: Optional[torch.Tensor] = None  # [n, NI+1, NJ+1]
+
+    def coords(self, dy: Optional[torch.Tensor]):
+        s = self.scheme
+        if dy is None or self.node_shape is None:
+            return s.x0, s.y0
+        return s.x0, s.y0 + torch.einsum("k,kij->ij", dy, self.node_shape)
+
+
+def ramp_wall_shape(scheme: Scheme, wall_nodes: Sequence[int], blend: np.ndarray) -> torch.Tensor:
+    """Unit displacement fields for ramp-wall nodes i in ``wall_nodes``: node (i, j)
+    moves by blend[j] (``cases.ramp_mesh`` blends a wall displacement linearly to zero
+    at the top: 1 - f_j)."""
+    ni, nj = scheme.ni, scheme.nj
+    out = torch.zeros((len(wall_nodes), ni + 1, nj + 1), dtype=torch.float64, device=scheme.device)
+    for k, i in enumerate(wall_nodes):
+        out[k, i, :] = torch.as_tensor(blend, dtype=torch.float64, device=scheme.device)
+    return out
+
+
+# ---------------------------------------------------------------------- gradients
+
+def _objective_value(scheme, objective, C, geo, prm):
+    return objective(scheme, C, geo, prm)
+
+
+def primal_gpu(mesh: Mesh, flow: Flow, c0: np.ndarray, rinit: float, niter: int, lib=None):
+    """The primal on the GPU through the C ABI (FP64): states Q_0 .. Q_N as [N+1, 5, NELES]."""
+    from .solver import Solver
+    s = Solver(mesh, flow, rinit, precision=0, lib=lib)
+    try:
+        s.upload(c0)
+        states = [np.array(c0)]
+        for _ in range(niter):
+            s.run(1, 0)
+            states.append(s.download())
+        return np.stack(states)
+    finally:
+        s.close()
+
+
+class GraphedStep:
+    """The reverse step of one iteration -- recompute Q_{n+1} = G(Q_n, p) and pull
+    lambda back: (lambda dG/dQ_n, lambda dG/dp) -- captured once as a CUDA graph with
+    static input tensors and replayed for every n.  The step is a few thousand small
+    kernels; replaying them from a graph removes the per-kernel launch cost of eager
+    execution.  Results equal the eager step up to the summation order of index_add."""
+
+    def __init__(self, scheme: Scheme, space: DesignSpace, params: List[torch.Tensor], dy_index: Optional[int]):
+        self.scheme, self.space, self.dy_index = scheme, space, dy_index
+        ni, nj = scheme.ni, scheme.nj
+        z = dict(dtype=torch.float64, device=scheme.device)
+        side = torch.cuda.Stream(device=scheme.device)
+        side.wait_stream(torch.cuda.current_stream(scheme.device))
+        with torch.cuda.stream(side):
+            # leaves of its own, first used on the warm-up stream: autograd then never
+            # synchronises with the stream the caller's leaves were first used on
+            self.params = [p.detach().clone().requires_grad_(True) for p in params]
+            self.Q = torch.zeros((5, ni, nj), **z).requires_grad_(True)
+            self.lam = torch.zeros((5, ni, nj), **z)
+            with torch.no_grad():  # a finite state for the warm-up steps
+                self.Q.copy_(scheme.cold_state(self._prm()))
+            for _ in range(2):
+                self._step()
+        torch.cuda.current_stream(scheme.device).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.out = self._step()
+
+    def _prm(self):
+        p = self.params
+        return Params(p[0], p[1], p[2], self.scheme.flow)
+
+    def _step(self):
+        dy = self.params[self.dy_index] if self.dy_index is not None else None
+        x, y = self.space.coords(dy)
+        geo = self.scheme.geometry(x, y)
+        Qn1 = self.scheme.iteration(self.Q, geo, self._prm())
+        # lambda . G as a scalar: its gradient is the vector-Jacobian product, and the
+        # seed of the backward pass is then created inside the capture
+        g = torch.autograd.grad(torch.sum(Qn1 * self.lam), [self.Q] + self.params, allow_unused=True)
+        return [v if v is not None else torch.zeros_like(p) for v, p in zip(g, [self.Q] + self.params)]
+
+    def __call__(self, Qn: torch.Tensor, lam: torch.Tensor):
+        with torch.no_grad():
+            self.Q.copy_(Qn)
+            self.lam.copy_(lam)
+        self.graph.replay()
+        return [t.clone() for t in self.out]
+
+
+def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, amachinit=None,
+                       dy: Optional[torch.Tensor] = None, space: Optional[DesignSpace] = None,
+                       niter: int = 100, states: Optional[np.ndarray] = None, primal: str = "gpu",
+                       lib=None, graph: Optional[bool] = None) -> dict:
+    """dJ/d(P0, T0, AMACHINIT, dy) of J = objective(scheme, Q_N, geo, prm), Q_0 the cold
+    start, Q_N after ``niter`` RK4 iterations.
+
+    The primal runs on the GPU FP64 path (``primal="gpu"``) or in the restatement
+    (``"torch"``); ``states`` may pass precomputed checkpoints [N+1, 5, NELES].  The
+    backward sweep recomputes each iteration from its checkpoint inside autograd; on a
+    CUDA device that step is captured once as a CUDA graph (``graph``, default on)."""
+    dev = scheme.device
+    leaf = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev,
+                                     requires_grad=True)
+    P0, T0, AM = leaf(p0, scheme.flow.p0), leaf(t0, scheme.flow.t0), leaf(amachinit, scheme.flow.amachinit)
+    if dy is not None:
+        dy = dy.detach().clone().to(dev).requires_grad_(True)
+    space = space or DesignSpace(scheme)
+    ni, nj = scheme.ni, scheme.nj
+
+    def setup():
+        prm = Params(P0, T0, AM, scheme.flow)
+        x, y = space.coords(dy)
+        return prm, scheme.geometry(x, y)
+
+    with torch.no_grad():
+        prm, geo = setup()
+        c0 = scheme.cold_state(prm)
+    if states is None:
+        if primal == "gpu":
+            mesh_now = _mesh_with_coords(scheme, space, dy)
+            f = dataclasses.replace(scheme.flow, p0=float(P0.detach()), t0=float(T0.detach()),
+                                    amachinit=float(AM.detach()))
+            rinit = float(scheme.rtol(prm).detach() / scheme.flow.rtred)
+            states = primal_gpu(mesh_now, f, c0.reshape(5, -1).cpu().numpy(), rinit, niter, lib)
+        else:
+            with torch.no_grad():
+                c, states = c0, [c0.reshape(5, -1).cpu().numpy()]
+                for _ in range(niter):
+                    c = scheme.iteration(c, geo, prm)
+                    states.append(c.reshape(5, -1).cpu().numpy())
+                states = np.stack(states)
+    ck = lambda n: torch.tensor(states[n].reshape(5, ni, nj), dtype=torch.float64, device=dev)
+
+    params = [P0, T0, AM] + ([dy] if dy is not None else [])
+    grads = [torch.zeros_like(p) for p in params]
+
+    def accumulate(g):
+        for k, v in enumerate(g):
+            if v is not None:
+                grads[k] = grads[k] + v
+
+    # dJ/dQ_N and the direct dependence of J on the parameters
+    QN = ck(niter).requires_grad_(True)
+    prm, geo = setup()
+    J = objective(scheme, QN, geo, prm)
+    g = torch.autograd.grad(J, [QN] + params, allow_unused=True)
+    lam = g[0]
+    accumulate(g[1:])
+    # reverse sweep over the iterations
+    if graph is None:
+        graph = scheme.device.type == "cuda"
+    step = GraphedStep(scheme, space, params, 3 if dy is not None else None) if graph and niter > 0 else None
+    for n in range(niter - 1, -1, -1):
+        if step is not None:
+            g = step(ck(n), lam)
+        else:
+            Qn = ck(n).requires_grad_(True)
+            prm, geo = setup()
+            Qn1 = scheme.iteration(Qn, geo, prm)
+            g = torch.autograd.grad(Qn1, [Qn] + params, grad_outputs=lam, allow_unused=True)
+        lam = g[0]
+        accumulate(g[1:])
+    del step
+    # the cold start Q_0(P0, T0, AMACHINIT)
+    prm, geo = setup()
+    Q0 = scheme.cold_state(prm)
+    g = torch.autograd.grad(Q0, params, grad_outputs=lam, allow_unused=True)
+    accumulate(g)
+    out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
+           "dJ_damachinit": float(grads[2]), "lambda0": lam.detach(), "states": states}
+    if dy is not None:
+        out["dJ_ddy"] = grads[3].detach().cpu().numpy()
+    return out
+
+
+def _mesh_with_coords(scheme: Scheme, space: DesignSpace, dy) -> Mesh:
+    """A formats.Mesh for the C ABI with the displaced node coordinates."""
+    from . import cases
+    x, y = space.coords(dy.detach() if dy is not None else None)
+    m = scheme.mesh_template
+    return dataclasses.replace(m, x=x.detach().cpu().numpy().ravel().copy(),
+                               y=y.detach().cpu().numpy().ravel().copy(), x_mm=None, y_mm=None)
+
+
+def objective_gpu(scheme: Scheme, objective: Callable, p0=None, t0=None, amachinit=None, dy=None,
+                  space: Optional[DesignSpace] = None, niter: int = 100, lib=None) -> float:
+    """J after ``niter`` iterations of the GPU FP64 primal from the cold start, for the
+    given parameters (the evaluation central differences use)."""
+    from .solver import Solver
+    dev = scheme.device
+    t = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev)
+    prm = Params(t(p0, scheme.flow.p0), t(t0, scheme.flow.t0), t(amachinit, scheme.flow.amachinit),
+                 scheme.flow)
+    space = space or DesignSpace(scheme)
+    with torch.no_grad():
+        dyt = None if dy is None else torch.as_tensor(dy, dtype=torch.float64, device=dev)
+        c0 = scheme.cold_state(prm).reshape(5, -1).cpu().numpy()
+        mesh_now = _mesh_with_coords(scheme, space, dyt)
+        f = dataclasses.replace(scheme.flow, p0=float(prm.p0), t0=float(prm.t0),
+                                amachinit=float(prm.amachinit))
+        s = Solver(mesh_now, f, float(scheme.rtol(prm).detach() / scheme.flow.rtred), precision=0, lib=lib)
+        try:
+            s.upload(c0)
+            if niter:
+                s.run(niter, 0)
+            q = s.download()
+        finally:
+            s.close()
+        x, y = space.coords(dyt)
+        geo = scheme.geometry(x, y)
+        C = torch.tensor(q.reshape(5, scheme.ni, scheme.nj), dtype=torch.float64, device=dev)
+        return float(objective(scheme, C, geo, prm))
+
+
+def fixed_point_adjoint(scheme: Scheme, objective: Callable, Qstar: torch.Tensor, niter: int = 200,
+                        p0=None, t0=None, amachinit=None, dy=None, space=None) -> dict:
+    """Adjoint of a steady state Q* = G(Q*, p): iterates lambda <- dJ/dQ + lambda dG/dQ
+    (the RK4 iteration's transposed Jacobian at Q*) and returns dJ/dp = dJ/dp|direct +
+    lambda dG/dp, with the adjoint residual history |lambda_{k+1} - lambda_k|_max.
+    Meaningful when Q* is a converged state of the primal."""
+    dev = scheme.device
+    leaf = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev,
+                                     requires_grad=True)
+    P0, T0, AM = leaf(p0, scheme.flow.p0), leaf(t0, scheme.flow.t0), leaf(amachinit, scheme.flow.amachinit)
+    if dy is not None:
+        dy = dy.detach().clone().to(dev).requires_grad_(True)
+    space = space or DesignSpace(scheme)
+    params = [P0, T0, AM] + ([dy] if dy is not None else [])
+    prm = Params(P0, T0, AM, scheme.flow)
+    x, y = space.coords(dy)
+    geo = scheme.geometry(x, y)
+    Q = Qstar.detach().clone().requires_grad_(True)
+    J = objective(scheme, Q, geo, prm)
+    gJ = torch.autograd.grad(J, [Q] + params, allow_unused=True, retain_graph=True)
+    djdq = gJ[0]
+    G = scheme.iteration(Q, geo, prm)
+    lam = djdq.clone()
+    hist = []
+    for _ in range(niter):
+        (vj,) = torch.autograd.grad(G, [Q], grad_outputs=lam, retain_graph=True)
+        new = djdq + vj
+        hist.append(float(torch.max(torch.abs(new - lam))))
+        lam = new
+    gp = torch.autograd.grad(G, params, grad_outputs=lam, allow_unused=True)
+    grads = []
+    for k, p in enumerate(params):
+        v = torch.zeros_like(p)
+        if gJ[k + 1] is not None:
+            v = v + gJ[k + 1]
+        if gp[k] is not None:
+            v = v + gp[k]
+        grads.append(v)
+    out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
+           "dJ_damachinit": float(grads[2]), "residual_history": hist, "lambda": lam.detach()}
+    if dy is not None:
+        out["dJ_ddy"] = grads[3].detach().cpu().numpy()
+    return out
+
+
+class TransientObjective(torch.autograd.Function):
+    """J(theta) with theta = [P0, T0, AMACHINIT, dy...]: forward runs the GPU primal
+    (FP64, C ABI) from the cold start for ``niter`` iterations and evaluates the
+    objective; backward is the checkpointed adjoint sweep of ``transient_gradient``."""
+
+    @staticmethod
+    def forward(ctx, theta, scheme, objective, space, niter):
+        th = theta.detach().to(torch.float64).cpu()
+        dy = th[3:] if th.numel() > 3 else None
+        with torch.enable_grad():  # forward of a Function runs with grad mode off
+            r = transient_gradient(scheme, objective, float(th[0]), float(th[1]), float(th[2]), dy=dy,
+                                   space=space, niter=niter)
+        g = [r["dJ_dp0"], r["dJ_dt0"], r["dJ_damachinit"]]
+        if dy is not None:
+            g += list(r["dJ_ddy"])
+        ctx.save_for_backward(torch.tensor(g, dtype=theta.dtype, device=theta.device))
+        return torch.tensor(r["J"], dtype=theta.dtype, device=theta.device)
+
+    @staticmethod
+    def backward(ctx, gout):
+        (g,) = ctx.saved_tensors
+        return gout * g, None, None, None, None
+
+
+# objectives --------------------------------------------------------------------
+
+def wall_force_y(scheme, C, geo, prm, side=1):
+    return scheme.wall_force(C, geo, prm, side)[1]
+
+
+def wall_force_x(scheme, C, geo, prm, side=1):
+    return scheme.wall_force(C, geo, prm, side)[0]
+
+
+def total_pressure_loss(scheme, C, geo, prm):
+    return scheme.total_pressure_loss(C, geo, prm)
