@@ -40,9 +40,15 @@ struct tns_batch {
     unsigned int* h_status = nullptr;       // pinned [ncases]
     int ntiles = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [monitor][parity]
+    // schedule 2: BLOCK unmonitored iterations in one graph per starting parity; each
+    // case's chain runs ahead on its stream with no join between the iterations
+    static constexpr int BLOCK = 8;
+    cudaGraphExec_t block[2] = {nullptr, nullptr};
+    long long per_block = 0;
     // schedule: 0 = one launch per phase over the tile table of all active cases;
     // 1 = each case's own single-case launches on one of several streams, captured as
-    // parallel branches of one graph (cases run concurrently, kernels as for tns_run)
+    // parallel branches of one graph (cases run concurrently, kernels as for tns_run);
+    // 2 = as 1, with BLOCK unmonitored iterations per graph
     int mode = 0;
     std::vector<cudaStream_t> branch;
     std::vector<int> branch_of;  // case -> branch stream (largest cases spread first)
@@ -71,6 +77,11 @@ struct tns_batch {
                     cudaGraphExecDestroy(g);
                     g = nullptr;
                 }
+        for (auto& g : block)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
     }
 };
 
@@ -210,9 +221,10 @@ void enqueue_batch_iteration(tns_batch* b, int parity, bool monitor) {
     }
 }
 
-// Per-case launches on branch streams (schedule 1): the single-case iteration of every
-// active case, forked from and joined back to the batch stream.
-void enqueue_branches(tns_batch* b, int parity, bool monitor) {
+// Per-case launches on branch streams (schedule 1): ``iters`` single-case iterations of
+// every active case (state parity alternating from ``parity``), forked from and joined
+// back to the batch stream.
+void enqueue_branches(tns_batch* b, int parity, bool monitor, int iters = 1) {
     const int n = (int)b->cases.size();
     const int nb = (int)b->branch.size();
     cudaEventRecord(b->fork, b->stream);
@@ -231,11 +243,14 @@ void enqueue_branches(tns_batch* b, int parity, bool monitor) {
         h->stream = b->branch[bi];
         h->side = nullptr;   // the case's pre-passes in order: the batch is parallel enough
         h->profile = false;  // no event synchronisation inside a capture
-        if (b->precision == 1)
-            tns_rt::enqueue_iteration_mx(h, monitor, const_cast<double*>(b->desc[k].qmx[parity]),
-                                         const_cast<double*>(b->desc[k].qmx[1 - parity]));
-        else
-            tns_rt::enqueue_iteration_f64(h, monitor);
+        for (int i = 0; i < iters; i++) {
+            const int par = parity ^ (i & 1);
+            if (b->precision == 1)
+                tns_rt::enqueue_iteration_mx(h, monitor, const_cast<double*>(b->desc[k].qmx[par]),
+                                             const_cast<double*>(b->desc[k].qmx[1 - par]));
+            else
+                tns_rt::enqueue_iteration_f64(h, monitor);
+        }
         b->launches += h->launches - before;
         h->launches = before;
         h->stream = keep;
@@ -254,7 +269,7 @@ void enqueue_branches(tns_batch* b, int parity, bool monitor) {
 int fetch_monitor(tns_batch* b, bool monitor) {
     const int n = (int)b->cases.size();
     int rc;
-    if (b->mode == 0) {
+    if (b->mode == 0) {  // the tile-table kernels write the batch's own status and CDIFF slots
         if ((rc = b->cuda(cudaMemcpyAsync(b->h_status, b->d_status.p, n * sizeof(unsigned int),
                                           cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
             return rc;
@@ -276,13 +291,29 @@ int fetch_monitor(tns_batch* b, bool monitor) {
     return TNS_OK;
 }
 
+int ensure_block_graph(tns_batch* b, int parity) {
+    cudaGraphExec_t* g = &b->block[parity];
+    if (*g) return TNS_OK;
+    int rc;
+    if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
+    const long long before = b->launches;
+    enqueue_branches(b, parity, false, tns_batch::BLOCK);
+    b->per_block = b->launches - before;
+    b->launches = before;
+    cudaGraph_t graph;
+    if ((rc = b->cuda(cudaStreamEndCapture(b->stream, &graph), "capture"))) return rc;
+    rc = b->cuda(cudaGraphInstantiate(g, graph, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(graph);
+    return rc;
+}
+
 int ensure_batch_graph(tns_batch* b, int monitor, int parity) {
     cudaGraphExec_t* g = &b->graph[monitor][parity];
     if (*g) return TNS_OK;
     int rc;
     if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
     const long long before = b->launches;
-    if (b->mode == 1)
+    if (b->mode >= 1)
         enqueue_branches(b, parity, monitor != 0);
     else
         enqueue_batch_iteration(b, parity, monitor != 0);
@@ -387,9 +418,21 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
         if ((rc = b->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     }
     if (niter <= 0) return TNS_OK;
-    bool remap = false;
-    for (int k = 0; k < n; k++) remap |= b->cases[k]->cur != b->cur_at_desc[k];
-    if (remap && (rc = upload_descriptors(b))) return rc;
+    // mixed ping-pong: when every member's state sits in the other buffer than the
+    // descriptors' parity 0 (an odd number of iterations since), start at parity 1; a
+    // mixed picture needs new descriptors (and graphs)
+    int parity = 0;
+    if (b->precision == 1) {
+        const int f0 = b->cases[0]->cur ^ b->cur_at_desc[0];
+        bool same = true;
+        for (int k = 1; k < n; k++) same &= (b->cases[k]->cur ^ b->cur_at_desc[k]) == f0;
+        if (same) {
+            parity = f0;
+        } else if ((rc = upload_descriptors(b))) {
+            return rc;
+        }
+    }
+    const int parity0 = parity;
     if (b->active != b->active_at_capture && (rc = upload_tiles(b))) return rc;
 
     std::vector<int> ran(n, 0), nrec(n, 0);
@@ -402,27 +445,44 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
         for (int m = 0; m < 5; m++) if (!(ref[5 * k + m] > 0.0)) return false;
         return true;
     };
-    int parity = 0;
     bool any_failed = false;
     auto active_count = [&]() {
         int a = 0;
         for (int k = 0; k < n; k++) a += b->active[k];
         return a;
     };
-    for (int it = 1; it <= niter && active_count() > 0; it++) {
+    for (int it = 1; it <= niter && active_count() > 0;) {
         // the run's first iteration is monitored when it sets the stop reference
         bool needs_ref = false;
         if (stop)
             for (int k = 0; k < n; k++) needs_ref |= b->active[k] && !set_ref(k);
-        const bool monitor = (monitor_every > 0 && it % monitor_every == 0) || (it == 1 && needs_ref);
+        auto monitored = [&](int j) {
+            return (monitor_every > 0 && j % monitor_every == 0) || (j == 1 && needs_ref);
+        };
+        const bool monitor = monitored(it);
         if (b->active != b->active_at_capture && (rc = upload_tiles(b))) return rc;
-        if ((rc = ensure_batch_graph(b, monitor ? 1 : 0, parity))) return rc;
-        if ((rc = b->cuda(cudaGraphLaunch(b->graph[monitor ? 1 : 0][parity], b->stream), "cudaGraphLaunch")))
-            return rc;
-        b->launches += b->per_iter[monitor ? 1 : 0];
-        for (int k = 0; k < n; k++) ran[k] += b->active[k];
-        if (b->precision == 1) parity ^= 1;
-        if (!monitor && it != niter) continue;
+        // schedule 1: a block of unmonitored iterations in one graph where one fits
+        int step = 1;
+        if (b->mode == 2 && it + tns_batch::BLOCK - 1 <= niter) {
+            step = tns_batch::BLOCK;
+            for (int j = it; j < it + tns_batch::BLOCK; j++)
+                if (monitored(j)) step = 1;
+        }
+        if (step > 1) {
+            if ((rc = ensure_block_graph(b, parity))) return rc;
+            if ((rc = b->cuda(cudaGraphLaunch(b->block[parity], b->stream), "cudaGraphLaunch"))) return rc;
+            b->launches += b->per_block;
+        } else {
+            if ((rc = ensure_batch_graph(b, monitor ? 1 : 0, parity))) return rc;
+            if ((rc = b->cuda(cudaGraphLaunch(b->graph[monitor ? 1 : 0][parity], b->stream), "cudaGraphLaunch")))
+                return rc;
+            b->launches += b->per_iter[monitor ? 1 : 0];
+        }
+        for (int k = 0; k < n; k++) ran[k] += step * b->active[k];
+        if (b->precision == 1) parity ^= (step & 1);
+        it += step;
+        const int last = it - 1;  // the iteration the check below follows
+        if (!monitor && last != niter) continue;
         // residual records, status words and the masks, at the monitor cadence and at the end
         if ((rc = fetch_monitor(b, monitor))) return rc;
         if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))) return rc;
@@ -442,7 +502,7 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
                 const double init = m < 4 ? 1.0e-10 : 1.0e-20;  // constants.f90:44-45
                 v[m] = v[m] >= init ? v[m] : init;
             }
-            const bool record = monitor_every > 0 && it % monitor_every == 0;
+            const bool record = monitor_every > 0 && last % monitor_every == 0;
             if (record) {
                 if (cdiff_out && nrec[k] < max_records)
                     for (int m = 0; m < 5; m++) cdiff_out[((size_t)k * max_records + nrec[k]) * 5 + m] = v[m];
@@ -461,15 +521,10 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
     // members continue from where the batch left them
     for (int k = 0; k < n; k++) {
         tns_handle* h = b->cases[k];
-        if (b->precision == 1) h->cur = b->cur_at_desc[k] ^ (ran[k] & 1);
+        if (b->precision == 1) h->cur = b->cur_at_desc[k] ^ parity0 ^ (ran[k] & 1);
         if (ran[k]) h->have_run = true;
         if (iterations) iterations[k] = ran[k];
         if (n_records) n_records[k] = std::min(nrec[k], max_records);
-    }
-    if (b->precision == 1) {
-        // the descriptors now map parity 0 to a stale buffer for odd-iteration cases
-        for (int k = 0; k < n; k++)
-            if (b->cases[k]->cur != b->cur_at_desc[k] && (rc = upload_descriptors(b))) return rc;
     }
     if (stop && cdiff_ref)
         for (int k = 0; k < n; k++)
@@ -481,9 +536,9 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
 
 int tns_batch_set_schedule(tns_batch* b, int schedule) {
     if (!b) return TNS_ERR_ARG;
-    if (schedule != 0 && schedule != 1) return b->fail(TNS_ERR_ARG, "schedule %d is not 0 or 1", schedule);
+    if (schedule < 0 || schedule > 2) return b->fail(TNS_ERR_ARG, "schedule %d is not 0, 1 or 2", schedule);
     int rc;
-    if (schedule == 1 && b->branch.empty()) {
+    if (schedule >= 1 && b->branch.empty()) {
         const int n = (int)b->cases.size();
         const int nb = std::min<int>(n, 64);
         // longest-first assignment of cases (by cell count) to the least-loaded branch

@@ -3,8 +3,9 @@
 The tile kernels are compiled for three tile heights -- TI = 4, 8 or 16 rows of 32
 cells per thread block (``libtnsgpu_ti4.so``, ``libtnsgpu.so``, ``libtnsgpu_ti16.so``;
 each build keeps the threads resident per SM of the TI = 8 tuning).  A batch can also
-run either schedule (0: one launch per kernel phase over the tiles of all cases; 1: the
-cases' own launches on parallel branches of one CUDA graph).  ``tune_batch`` and
+run any of three schedules (0: one launch per kernel phase over the tiles of all cases;
+1: the cases' own launches on parallel branches of one CUDA graph; 2: as 1 with 8
+iterations per graph).  ``tune_batch`` and
 ``tune_case`` time a few iterations of the caller's cases under every combination and
 return the fastest.
 
@@ -43,11 +44,13 @@ def _time_batch(solvers: Sequence[Solver], schedule: int, iters: int, warmup: in
         b.close()
 
 
-def tune_batch(make_solvers: Callable[[str], List[Solver]], iters: int = 40, warmup: int = 5,
-               tile_heights: Iterable[int] = TILE_HEIGHTS, schedules: Sequence[int] = (0, 1),
+def tune_batch(make_solvers: Callable[[str], List[Solver]], iters: int = 40, warmup: int = 16,
+               tile_heights: Iterable[int] = TILE_HEIGHTS, schedules: Sequence[int] = (0, 1, 2),
                cache: Optional[str] = None, key: Optional[str] = None) -> dict:
     """make_solvers(lib_path) builds the batch's cases (state uploaded) from that library
-    build.  Times ``iters`` iterations after ``warmup`` for every (tile height, schedule)
+    build.  Times ``iters`` iterations after ``warmup`` (enough to capture every graph a
+    schedule uses, including schedule 2's 8-iteration block) for every (tile height,
+    schedule)
     and returns {"ti", "schedule", "lib", "s_per_iter", "trials"}.  With ``cache`` (a
     JSON file) and ``key``, a stored choice is returned without timing."""
     if cache and key and os.path.exists(cache):

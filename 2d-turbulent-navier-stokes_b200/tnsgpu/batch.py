@@ -78,7 +78,7 @@ class Batch:
     @property
     def schedule(self) -> int:
         """0: one launch per phase over all cases' tiles; 1: per-case launches on
-        parallel graph branches."""
+        parallel graph branches; 2: as 1 with 8 iterations per graph."""
         return int(self.L.tns_batch_get_schedule(self.b))
 
     @schedule.setter

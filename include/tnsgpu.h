@@ -192,8 +192,10 @@ int tns_batch_set_active(tns_batch *b, const int *active);
 
 /* How a batch iteration is scheduled: 0 (default) = one launch per kernel phase over
  * the tiles of all active cases; 1 = every case's own tns_run launches, the cases on
- * parallel branches of one CUDA graph so they run concurrently.  Results are identical;
- * which is faster depends on the case mix (tnsgpu.autotune measures both). */
+ * parallel branches of one CUDA graph so they run concurrently; 2 = as 1, with 8
+ * unmonitored iterations per graph so each case runs ahead without a join between
+ * iterations.  Results are identical; which is fastest depends on the case mix
+ * (tnsgpu.autotune measures them). */
 int tns_batch_set_schedule(tns_batch *b, int schedule);
 int tns_batch_get_schedule(tns_batch *b);
 int tns_batch_get_active(tns_batch *b, int *active);

@@ -223,6 +223,30 @@ def test_autotune_batch_picks_a_timed_configuration():
         return out
 
     r = autotune.tune_batch(make, iters=3, warmup=1)
-    assert r["ti"] in (4, 8, 16) and r["schedule"] in (0, 1)
+    assert r["ti"] in (4, 8, 16) and r["schedule"] in (0, 1, 2)
     timed = [t for t in r["trials"] if "s_per_iter" in t]
-    assert len(timed) == 6 and r["s_per_iter"] == min(t["s_per_iter"] for t in timed)
+    assert len(timed) == 9 and r["s_per_iter"] == min(t["s_per_iter"] for t in timed)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_schedule2_iteration_blocks_and_parity_offset(precision):
+    """Schedule 2 runs blocks of 8 unmonitored iterations per graph between monitor
+    points, and after an odd-length call starts the next at the other state parity
+    instead of re-capturing: states and records still equal solo runs bit for bit."""
+    mem = _members(precision, pick=[0, 1, 3])
+    solvers = [Solver(m, f, ri, precision=precision) for _, m, f, _, ri in mem]
+    for s, (_, _, _, c0, _) in zip(solvers, mem):
+        s.upload(c0)
+    b = Batch(solvers, schedule=2)
+    b.run(3, monitor_every=0)
+    r = b.run(21, monitor_every=10)
+    assert list(r.iterations) == [21] * 3 and all(len(x) == 2 for x in r.records)
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        s.run(3, 0)
+        rec = s.run(21, 10)
+        np.testing.assert_array_equal(solvers[k].download(), s.download(), err_msg=name)
+        np.testing.assert_array_equal(r.records[k], rec, err_msg=name)
+        s.close()
+    b.close()
