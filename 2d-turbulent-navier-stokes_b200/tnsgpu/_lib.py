@@ -11,7 +11,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libtnsgpu.so")
+# TNSGPU_LIB names another build of the library to load by default
+LIB_PATH = os.environ.get("TNSGPU_LIB") or os.path.join(HERE, "libtnsgpu.so")
 # tile-height variants of the same library (TI rows of 32 cells per tile); the default
 # build is TI = 8
 TILE_VARIANTS = {8: LIB_PATH, 4: os.path.join(HERE, "libtnsgpu_ti4.so"),

@@ -7,8 +7,12 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
 SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu", "tns_batch_api.cu")
-NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
+# the mixed-precision kernels: FP32 division and square root to 2 ulp and FP32
+# denormals flushed (their FP32 parts are deviations and sources whose error budget is
+# FP32-level anyway; the FP64 parts are unaffected by these flags)
+FILE_FLAGS = {"tns_kernels_mx.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 
 
 MAINS = os.path.join(os.path.dirname(HERE), "mains")
@@ -28,12 +32,18 @@ def build_mains() -> list:
     return out
 
 
-def _lib_cmd(out: str, ti: int, verbose: bool):
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = ["nvcc", *NVCC_FLAGS, f"-DTNS_TI={ti}", *srcs, "-o", out]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    return cmd
+def _obj_cmds(out: str, ti: int, verbose: bool):
+    """One nvcc per source (with its own flags) into objects beside ``out``."""
+    objs, cmds = [], []
+    for src in SOURCES:
+        obj = f"{out}.{os.path.splitext(src)[0]}.o"
+        cmd = ["nvcc", *NVCC_FLAGS, *FILE_FLAGS.get(src, []), f"-DTNS_TI={ti}", "-c",
+               os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        objs.append(obj)
+        cmds.append(cmd)
+    return objs, cmds
 
 
 def build_library(verbose: bool = False, variants: bool = True) -> str:
@@ -43,8 +53,13 @@ def build_library(verbose: bool = False, variants: bool = True) -> str:
     jobs = [(TILE_VARIANTS[8], 8)]
     if variants:
         jobs += [(TILE_VARIANTS[t], t) for t in sorted(TILE_VARIANTS) if t != 8]
-    procs = [(out, subprocess.Popen(_lib_cmd(out, ti, verbose))) for out, ti in jobs]
-    failed = [out for out, p in procs if p.wait() != 0]
+    plan = [(out, *_obj_cmds(out, ti, verbose)) for out, ti in jobs]
+    procs = [(cmd[-1], subprocess.Popen(cmd)) for _, _, cmds in plan for cmd in cmds]
+    failed = [obj for obj, p in procs if p.wait() != 0]
     if failed:
         raise subprocess.CalledProcessError(1, f"nvcc for {failed}")
+    for out, objs, _ in plan:
+        subprocess.run(["nvcc", *ARCH, "-shared", *objs, "-o", out], check=True)
+        for o in objs:
+            os.remove(o)
     return TILE_VARIANTS[8]

@@ -15,7 +15,7 @@ case ran, and how far every batched final state is from its sequential counterpa
 when the tuned tile height differs from the default).
 
   python -m tnsgpu.sweep [--cases 64] [--niter 5000] [--stop-ratio 1e-5] [--monitor 1000]
-                         [--precision mixed|fp64] [--no-tune]
+                         [--precision mixed|fp64] [--no-tune] [--manifest batch.in]
 """
 from __future__ import annotations
 
@@ -69,8 +69,15 @@ def run_batched(solvers, niter, monitor, stop_ratio, schedule=0):
     return dt, [int(v) for v in r.iterations], launches
 
 
-def compare(ncases=64, niter=5000, stop_ratio=1.0e-5, monitor=1000, seed=0, precision=1, tune=True):
-    sweep = cases.ramp_sweep(ncases, seed=seed)
+def compare(ncases=64, niter=5000, stop_ratio=1.0e-5, monitor=1000, seed=0, precision=1, tune=True,
+            manifest=None):
+    """``manifest``: a batch manifest file (formats.read_manifest) instead of the seeded
+    sweep."""
+    if manifest:
+        sweep = [cases.SweepCase(**row) for row in formats.read_manifest(manifest)]
+        ncases = len(sweep)
+    else:
+        sweep = cases.ramp_sweep(ncases, seed=seed)
     cells = np.array([c.nx * c.ny for c in sweep])
     # warm-up: library load, kernel attributes, a graph capture on a small batch
     warm = _solvers(sweep[:2], precision)
@@ -123,9 +130,10 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--no-tune", action="store_true", help="default tile height and schedule 0")
+    ap.add_argument("--manifest", help="batch manifest of ramp cases (name nx ny angle_deg p0 t0 amachinit)")
     a = ap.parse_args()
     print(json.dumps(compare(a.cases, a.niter, a.stop_ratio, a.monitor, a.seed,
-                             1 if a.precision == "mixed" else 0, not a.no_tune)))
+                             1 if a.precision == "mixed" else 0, not a.no_tune, a.manifest)))
 
 
 if __name__ == "__main__":
