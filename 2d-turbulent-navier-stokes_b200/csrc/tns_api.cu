@@ -772,6 +772,23 @@ int tns_kernel_times(tns_handle* h, int kernel, double* ms, long long* launches)
 
 long long tns_launch_count(tns_handle* h) { return h ? h->launches : -1; }
 
+int tns_debug_math(int fn, long long n, const double* a, const double* b, double* out) {
+    if ((fn != 0 && fn != 1) || n < 0 || (n > 0 && (!a || !out || (fn == 1 && !b)))) return TNS_ERR_ARG;
+    if (n == 0) return TNS_OK;
+    double* d = nullptr;
+    const size_t bytes = (size_t)n * sizeof(double);
+    if (cudaMalloc((void**)&d, 3 * bytes) != cudaSuccess) return TNS_ERR_CUDA;
+    cudaError_t e = cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && fn == 1) e = cudaMemcpy(d + n, b, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        tns::launch_debug_math(fn, n, d, d + n, d + 2 * n, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? TNS_OK : TNS_ERR_CUDA;
+}
+
 const char* tns_last_error(tns_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
 }  // extern "C"

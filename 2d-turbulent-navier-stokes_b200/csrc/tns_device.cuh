@@ -85,8 +85,29 @@ __device__ __forceinline__ double powi(double x, int n) {
     return n < 0 ? 1.0 / r : r;
 }
 
-// T**0.6 as exp(0.6*log(T)): within a few ulp of pow and a third cheaper on the GPU.
-__device__ __forceinline__ double pow06(double T) { return exp(0.6 * log(T)); }
+// T**0.6 for T > 0, y = T^(3/5): a single-precision estimate exp2(0.6 log2 T) (about
+// 1e-7 relative) refined by two Newton steps on f(y) = y^5 - T^3,
+//   y <- y - f(y)/f'(y) = 0.8 y + 0.2 T^3 / y^4,
+// whose error squares per step (e' ~ 2 e^2): 2e-14 after one, FP64 rounding after two.
+// Within a few ulp of pow, at less than half the instructions of exp(0.6 log T).
+__device__ __forceinline__ double pow06(double T) {
+    double y = (double)exp2f(0.6f * __log2f((float)T));
+    const double t3 = T * T * T;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const double y2 = y * y;
+        y = 0.8 * y + 0.2 * t3 / (y2 * y2);
+    }
+    return y;
+}
+
+// tanh(a) / tanh(b) for a, b >= 0, from tanh(x) = E / (E + 2) with E = expm1(2x):
+// Ea (Eb + 2) / (Eb (Ea + 2)), one division instead of three.  Arguments are capped at
+// 20, where tanh is 1 to double precision, so E stays finite.
+__device__ __forceinline__ double tanh_ratio(double a, double b) {
+    const double ea = expm1(2.0 * fmin(a, 20.0)), eb = expm1(2.0 * fmin(b, 20.0));
+    return (ea * (eb + 2.0)) / (eb * (ea + 2.0));
+}
 
 // Sutherland-type molecular viscosity SUTH_COEF*DSQRT(AMOL)*T**0.6 (viscous.f90:188).
 __device__ __forceinline__ double amu_of(const Params& P, double T) {
@@ -309,8 +330,8 @@ __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, do
     const double DVY = (-(s.va - s.vc) * xbd + (s.vb - s.vd) * xac) * iDNR;
     const double AMU = amu_of(P, TI);
     const double CHI = RHO * RI / (CMU * AMU);
-    const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
-    const double FR2 = tanh(sqrt(CHI)) / tanh(CHI * P.fr2k);
+    const double FMU = tanh_ratio(ALPHA_T * CHI * CHI, BETA_T * CHI * CHI);
+    const double FR2 = tanh_ratio(sqrt(CHI), CHI * P.fr2k);
     const double AMUT = FMU * RHO * RI;
     const double PHI = DQX * DRX + DQY * DRY;
     double DEE = 0.0;
@@ -376,7 +397,7 @@ __device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, b
     const double AMU = amu_of(P, TAVG);
     const double AK = AMU * P.cp_pr;
     const double CHI = RHOAVG * RAVG / (AMU * CMU);
-    const double FMU = tanh(ALPHA_T * CHI * CHI) / tanh(BETA_T * CHI * CHI);
+    const double FMU = tanh_ratio(ALPHA_T * CHI * CHI, BETA_T * CHI * CHI);
     const double AMUT = RHOAVG * RAVG * FMU;
     const double AKT = AMUT * P.cp_prt;
     const double AMUEFF = AMU + AMUT;

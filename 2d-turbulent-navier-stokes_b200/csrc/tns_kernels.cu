@@ -775,6 +775,22 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_
     stage_tile(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
 }
 
+// ---------------------------------------------------------------- math check
+
+// Evaluates one of the FP64 helpers the kernels use, elementwise, for testing their
+// accuracy: fn 0 = pow06(a), 1 = tanh_ratio(a, b).
+__global__ void k_debug_math(int fn, long long n, const double* __restrict__ a, const double* __restrict__ b,
+                             double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = fn == 0 ? pow06(a[i]) : tanh_ratio(a[i], b[i]);
+}
+
+void launch_debug_math(int fn, long long n, const double* a, const double* b, double* out, cudaStream_t s) {
+    const long long blocks = (n + 255) / 256;
+    if (blocks > 0) k_debug_math<<<(unsigned)blocks, 256, 0, s>>>(fn, n, a, b, out);
+}
+
 // ------------------------------------------------------------------ launchers
 
 static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }

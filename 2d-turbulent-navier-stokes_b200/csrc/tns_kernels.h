@@ -37,6 +37,9 @@ void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStr
 void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
                           double* out, cudaStream_t s);
 
+// accuracy check of the FP64 helpers (fn 0 = pow06, 1 = tanh_ratio)
+void launch_debug_math(int fn, long long n, const double* a, const double* b, double* out, cudaStream_t s);
+
 // batched multi-case kernels: kernel 0 dissipation, 1 viscous, 2 stage
 void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
                       int kernel, int stage, int monitor, cudaStream_t s);

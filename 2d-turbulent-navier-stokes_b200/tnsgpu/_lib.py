@@ -39,7 +39,7 @@ EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
            "tns_boundary_integrals", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
            "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule",
-           "tns_batch_launch_count", "tns_batch_last_error", "tns_batch_destroy")
+           "tns_batch_launch_count", "tns_debug_math", "tns_batch_last_error", "tns_batch_destroy")
 NOT_INT = ("tns_launch_count", "tns_last_error", "tns_destroy", "tns_batch_launch_count",
            "tns_batch_last_error", "tns_batch_destroy")
 
@@ -103,6 +103,7 @@ def load(path: str = None):
     L.tns_batch_set_active.argtypes = [vp, vp]
     L.tns_batch_get_active.argtypes = [vp, vp]
     L.tns_batch_set_schedule.argtypes = [vp, ip]
+    L.tns_debug_math.argtypes = [ip, C.c_longlong, dp, dp, dp]
     L.tns_batch_get_schedule.argtypes = [vp]
     L.tns_batch_launch_count.argtypes = [vp]
     L.tns_batch_launch_count.restype = C.c_longlong

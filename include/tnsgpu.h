@@ -114,6 +114,12 @@ int tns_boundary_integrals(tns_handle *h, int type, int side, double out[4]);
  * 1..NELES per array. */
 int tns_debug_fetch(tns_handle *h, int which, double *out);
 
+/* Accuracy check of the FP64 helpers the kernels use in place of library calls,
+ * elementwise on n host values: fn 0 = T**0.6 (viscosity law, viscous.f90:188),
+ * fn 1 = tanh(a)/tanh(b) (damping ratios, viscous.f90:191, source_terms.f90:64-67).
+ * For tests; allocates and frees its own device memory. */
+int tns_debug_math(int fn, long long n, const double *a, const double *b, double *out);
+
 /* Runs the next tns_run on this CUDA stream (cudaStream_t passed as void*; NULL
  * restores the handle's own stream). */
 int tns_set_stream(tns_handle *h, void *stream);

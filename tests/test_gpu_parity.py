@@ -187,3 +187,23 @@ def test_graph_replay_equals_direct_launches():
     assert np.array_equal(a.download(), b.download())
     kt = b.kernel_times()
     assert kt["dissipation"][1] == 7 and kt["viscous"][1] == 7 and kt["stage"][1] == 28
+
+
+def test_fp64_math_helpers_match_libm():
+    """The kernels compute T**0.6 by two Newton steps from a single-precision estimate
+    and tanh(a)/tanh(b) through expm1; both agree with numpy's pow / tanh to a few ulp
+    over the temperatures and damping arguments the solver meets."""
+    from tnsgpu import _lib
+    L = _lib.load()
+    t = np.concatenate([np.logspace(0, 4, 20000), np.random.default_rng(0).uniform(100, 4000, 20000)])
+    out = np.zeros_like(t)
+    assert L.tns_debug_math(0, t.size, t.ctypes.data, None, out.ctypes.data) == 0
+    ref = t ** 0.6
+    assert np.max(np.abs(out - ref) / ref) < 8 * np.finfo(float).eps
+    rng = np.random.default_rng(1)
+    a = np.concatenate([10 ** rng.uniform(-12, 2, 20000), rng.uniform(0, 30, 20000)])
+    b = np.concatenate([10 ** rng.uniform(-12, 2, 20000), rng.uniform(0, 30, 20000)])
+    out = np.zeros_like(a)
+    assert L.tns_debug_math(1, a.size, a.ctypes.data, b.ctypes.data, out.ctypes.data) == 0
+    ref = np.tanh(a) / np.tanh(b)
+    assert np.max(np.abs(out - ref) / np.abs(ref)) < 16 * np.finfo(float).eps
