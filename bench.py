@@ -127,6 +127,21 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(x: float, world: int, torch, device) -> float:
+    """The largest of every rank's x (a time: the slowest replica sets the pace)."""
+    if world <= 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(cells: int, seconds: float, world: int) -> float:
+    """Whole-job cell-iterations per second of ``world`` replicas that each advance
+    ``cells`` cells by one iteration in ``seconds`` (the max over ranks)."""
+    return world * cells / seconds
+
+
 def time_steps(s, stream, flush, K, W, world, torch):
     """Device time per step (one RK4 iteration; L2 flushed between steps, outside the
     events), max over ranks, plus our launches in the timed region."""
@@ -149,11 +164,7 @@ def time_steps(s, stream, flush, K, W, world, torch):
     if world > 1:
         torch.distributed.barrier()
     s.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev) / K
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=stream.device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / K, world, torch, stream.device)
     return ms, s.launch_count() - l0
 
 
@@ -198,7 +209,7 @@ def run_ours(args, rank, world, dev):
     clocks = Clocks(dev)
     ms, launches = time_steps(s, stream, flush, K, W, world, torch)
     clk = clocks.stop()
-    value = world * mesh.neles / (ms * 1e-3)
+    value = replica_rate(mesh.neles, ms * 1e-3, world)
 
     # per-kernel device times (events around each launch, L2 flushed between iterations)
     s.profile(True)
@@ -234,12 +245,8 @@ def run_ours(args, rank, world, dev):
     for _ in range(E):
         s.upload_ptrs(ptrs)
         s.run(1, 1)
-    e2e_s = (time.perf_counter() - t0) / E
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * mesh.neles / e2e_s, "unit": UNIT,
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / E, world, torch, dev)
+    e2e = {"value": replica_rate(mesh.neles, e2e_s, world), "unit": UNIT,
            "h2d_bytes_per_step": 5 * mesh.neles * 8, "d2h_bytes_per_step": 5 * 8 + 4,
            "ms_per_step": round(e2e_s * 1e3, 4),
            "host_cpus": f"{len(numa_cpus)} GPU-local" if numa_cpus else "unpinned"}
@@ -253,7 +260,7 @@ def run_ours(args, rank, world, dev):
         s2.upload(c0)
         ms2, _ = time_steps(s2, stream, flush, K, W, world, torch)
         s2.close()
-        other = {"precision": "fp64" if prec else "mixed", "value": world * mesh.neles / (ms2 * 1e-3),
+        other = {"precision": "fp64" if prec else "mixed", "value": replica_rate(mesh.neles, ms2 * 1e-3, world),
                  "ms_per_step": round(ms2, 5), "mixed_over_fp64": (ms2 / ms) if prec == 0 else (ms / ms2)}
 
     cpu = None
@@ -323,7 +330,7 @@ def run_reference(args):
     sample = (f"{n} of {args.steps} requested steps, each one full RK4 iteration of the "
               f"{mesh.neles}-cell mesh, single thread (the reference is serial)")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": n,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
