@@ -72,8 +72,17 @@ def _safe_sqrt(x):
 
 
 def _pad(a):
-    """(ni, nj) -> (ni+2, nj+2) with the ring holding copies of the adjacent cell."""
-    return torch.nn.functional.pad(a[None, None], (1, 1, 1, 1), mode="replicate")[0, 0]
+    """([k,] ni, nj) -> ([k,] ni+2, nj+2) with the ring holding copies of the adjacent
+    cell."""
+    if a.dim() == 2:
+        return torch.nn.functional.pad(a[None, None], (1, 1, 1, 1), mode="replicate")[0, 0]
+    return torch.nn.functional.pad(a[None], (1, 1, 1, 1), mode="replicate")[0]
+
+
+# rows of the stacked primitive field set (COMPUTE_PRIMITIVE_VARS and the ghosts)
+U_, V_, T_, P_ = 0, 1, 2, 3
+C_, F_, G_ = 4, 9, 14     # C1..C5, F1..F5, G1..G5
+NW_ = 19
 
 
 @dataclasses.dataclass
@@ -166,6 +175,7 @@ class Scheme:
         self.g_pad = it(g_i * (nj + 2) + g_j)
         self.g_type = torch.cat([self.types[1], self.types[3], self.types[4], self.types[2]])
         self.types_present = sorted(set(int(t) for t in np.unique(mesh.ntype)))
+        self.sensor_of = torch.tensor([0, 0, 0, 0, 1], dtype=torch.int64, device=dev)
         self._node_average_matrices(mesh)
 
     # ------------------------------------------------------------------ set-up
@@ -282,7 +292,8 @@ class Scheme:
         return SUTH * math.sqrt(self.flow.amol) * t ** 0.6
 
     def primitive(self, C, prm: Params):
-        """COMPUTE_PRIMITIVE_VARS (turbnstwod.f90:204-227) on the cells."""
+        """COMPUTE_PRIMITIVE_VARS (turbnstwod.f90:204-227) on the cells, as one stacked
+        field set [19, NI, NJ]: U, V, T, P, C1..C5, F1..F5, G1..G5."""
         rho = C[0]
         u = C[1] / rho
         v = C[2] / rho
@@ -290,97 +301,74 @@ class Scheme:
         t = (e - 0.5 * (u * u + v * v)) / prm.cv
         p = rho * prm.rr * t
         rt = C[4] / rho
-        f = [C[1], rho * u * u + p, rho * u * v, (C[3] + p) * u, rho * rt * u]
-        g = [C[2], None, rho * v * v + p, (C[3] + p) * v, rho * rt * v]
-        g[1] = f[2]
-        return dict(u=u, v=v, t=t, p=p, c=[C[m] for m in range(5)], f=f, g=g)
+        f2 = rho * u * v
+        return torch.stack([u, v, t, p, C[0], C[1], C[2], C[3], C[4],
+                            C[1], rho * u * u + p, f2, (C[3] + p) * u, rho * rt * u,
+                            C[2], f2, rho * v * v + p, (C[3] + p) * v, rho * rt * v])
 
     def _ghosts(self, pr, opp, prm: Params):
         """APPLY_BOUNDARY (boundary.f90:53-122) for every ghost of the ring at once:
-        parent values ``pr`` and the values of the cell opposite the boundary face
-        ``opp`` (1-D over the ghosts).  Each BC type present in the mesh is evaluated on
-        the whole ring and selected by the ghost's type."""
+        parent field set ``pr`` [19, NG] and U, V, T, P of the cell opposite the
+        boundary face ``opp`` [4, NG].  Each BC type present in the mesh is evaluated
+        on the whole ring and selected by the ghost's type."""
         flow = self.flow
         rr, cv, cp, g = prm.rr, prm.cv, prm.cp, flow.gama
 
-        def fluxes(rho, u, v, t, p):
+        def state(rho, u, v, t, p, c5, f5, g5):
             c1, c2 = rho * u, rho * v
             c3 = rho * (cv * t + 0.5 * (u * u + v * v))
             f3 = rho * u * v
-            return [rho, c1, c2, c3], [c1, rho * u * u + p, f3, (c3 + p) * u], \
-                   [c2, f3, rho * v * v + p, (c3 + p) * v]
+            return torch.stack([u, v, t, p, rho, c1, c2, c3, c5,
+                                c1, rho * u * u + p, f3, (c3 + p) * u, f5,
+                                c2, f3, rho * v * v + p, (c3 + p) * v, g5])
 
         sel = {}
         if 2 in self.types_present:  # subsonic inlet at P0, T0 (isentropic)
-            u2 = torch.abs(pr["u"])
-            v2 = -pr["v"]
+            u2 = torch.abs(pr[U_])
+            v2 = -pr[V_]
             t2 = prm.t0 - 0.5 * (u2 * u2 + v2 * v2) / cp
             rho2 = (prm.s0() / (rr * t2)) ** (1.0 / (1.0 - g))
             p2 = rho2 * rr * t2
-            c2, f2, gg2 = fluxes(rho2, u2, v2, t2, p2)
             c5 = rho2 * (self.amu(t2) / rho2)
-            sel[2] = dict(u=u2, v=v2, t=t2, p=p2, c=c2 + [c5], f=f2 + [c5 * u2], g=gg2 + [c5 * v2])
+            sel[2] = state(rho2, u2, v2, t2, p2, c5, c5 * u2, c5 * v2)
         if 3 in self.types_present:  # extrapolation (PAMB >= 0 fixes P)
-            u3 = torch.abs(2.0 * pr["u"] - opp["u"])
-            v3 = 2.0 * pr["v"] - opp["v"]
-            t3 = 2.0 * pr["t"] - opp["t"]
-            p3 = 2.0 * pr["p"] - opp["p"]
+            u3 = torch.abs(2.0 * pr[U_] - opp[0])
+            v3 = 2.0 * pr[V_] - opp[1]
+            t3 = 2.0 * pr[T_] - opp[2]
+            p3 = 2.0 * pr[P_] - opp[3]
             if flow.pamb >= 0.0:
                 p3 = torch.full_like(p3, flow.pamb)
-            rho3 = p3 / (rr * t3)
-            c3, f3, g3 = fluxes(rho3, u3, v3, t3, p3)
-            sel[3] = dict(u=u3, v=v3, t=t3, p=p3, c=c3 + [pr["c"][4]], f=f3 + [pr["f"][4]],
-                          g=g3 + [pr["g"][4]])
+            sel[3] = state(p3 / (rr * t3), u3, v3, t3, p3, pr[C_ + 4], pr[F_ + 4], pr[G_ + 4])
         if 4 in self.types_present:  # symmetry
-            c4, f4, g4 = fluxes(pr["c"][0], pr["u"], -pr["v"], pr["t"], pr["p"])
-            sel[4] = dict(u=pr["u"], v=-pr["v"], t=pr["t"], p=pr["p"], c=c4 + [pr["c"][4]],
-                          f=f4 + [pr["f"][4]], g=g4 + [-pr["g"][4]])
+            sel[4] = state(pr[C_], pr[U_], -pr[V_], pr[T_], pr[P_], pr[C_ + 4], pr[F_ + 4], -pr[G_ + 4])
         if 5 in self.types_present:  # no-slip wall
-            u5, v5, rho5 = -pr["u"], -pr["v"], pr["c"][0]
-            e5 = cv * pr["t"] + 0.5 * (u5 * u5 + v5 * v5)
-            P = pr["p"]
-            sel[5] = dict(u=u5, v=v5, t=pr["t"], p=P,
-                          c=[rho5, rho5 * u5, rho5 * v5, rho5 * e5, -pr["c"][4]],
-                          f=[-pr["f"][0], 2.0 * P - pr["f"][1], -pr["f"][2], -pr["f"][3], -pr["f"][4]],
-                          g=[-pr["g"][0], -pr["g"][1], 2.0 * P - pr["g"][2], -pr["g"][3], -pr["g"][4]])
+            u5, v5, rho5 = -pr[U_], -pr[V_], pr[C_]
+            e5 = cv * pr[T_] + 0.5 * (u5 * u5 + v5 * v5)
+            P = pr[P_]
+            sel[5] = torch.stack([u5, v5, pr[T_], P, rho5, rho5 * u5, rho5 * v5, rho5 * e5, -pr[C_ + 4],
+                                  -pr[F_], 2.0 * P - pr[F_ + 1], -pr[F_ + 2], -pr[F_ + 3], -pr[F_ + 4],
+                                  -pr[G_], -pr[G_ + 1], 2.0 * P - pr[G_ + 2], -pr[G_ + 3], -pr[G_ + 4]])
         order = list(sel)
-
-        def pick(get):
-            r = get(sel[order[0]])
-            for ty in order[1:]:
-                r = torch.where(self.g_type == ty, get(sel[ty]), r)
-            return r
-
-        out = {k: pick(lambda T, k=k: T[k]) for k in ("u", "v", "t", "p")}
-        for k in ("c", "f", "g"):
-            out[k] = [pick(lambda T, k=k, m=m: T[k][m]) for m in range(5)]
+        out = sel[order[0]]
+        for ty in order[1:]:
+            out = torch.where(self.g_type == ty, sel[ty], out)
         return out
 
-    def boundary(self, pr, prm: Params):
-        """Padded [NI+2, NJ+2] primitive fields: cells plus the ghosts of APPLY_BOUNDARY."""
-        keys = ("u", "v", "t", "p")
-        gat = lambda a, idx: a.reshape(-1).index_select(0, idx)
-        prs = {k: gat(pr[k], self.g_par) for k in keys}
-        ops = {k: gat(pr[k], self.g_opp) for k in keys}
-        for k in ("c", "f", "g"):
-            prs[k] = [gat(a, self.g_par) for a in pr[k]]
-        gh = self._ghosts(prs, ops, prm)
+    def boundary(self, W, prm: Params):
+        """Padded field set [19, NI+2, NJ+2]: cells plus the ghosts of APPLY_BOUNDARY."""
+        flat = W.reshape(NW_, -1)
+        pr = flat.index_select(1, self.g_par)
+        opp = flat[:4].index_select(1, self.g_opp)
+        gh = self._ghosts(pr, opp, prm)
         npad = (self.ni + 2) * (self.nj + 2)
-
-        def assemble(interior, ghost):
-            ring = torch.zeros(npad, dtype=interior.dtype, device=interior.device).index_copy(0, self.g_pad, ghost)
-            return torch.nn.functional.pad(interior[None, None], (1, 1, 1, 1))[0, 0] + \
-                ring.reshape(self.ni + 2, self.nj + 2)
-
-        full = {k: assemble(pr[k], gh[k]) for k in keys}
-        for k in ("c", "f", "g"):
-            full[k] = [assemble(pr[k][m], gh[k][m]) for m in range(5)]
-        return full
+        ring = torch.zeros((NW_, npad), dtype=W.dtype, device=W.device).index_copy(1, self.g_pad, gh)
+        return torch.nn.functional.pad(W, (1, 1, 1, 1)) + ring.reshape(NW_, self.ni + 2, self.nj + 2)
 
     @staticmethod
     def _nb(a):
-        """The four neighbours NC1..NC4 (j-1, i+1, j+1, i-1) of every cell of a padded field."""
-        return a[1:-1, :-2], a[2:, 1:-1], a[1:-1, 2:], a[:-2, 1:-1]
+        """The four neighbours NC1..NC4 (j-1, i+1, j+1, i-1) of every cell of a padded field
+        (or stack of fields)."""
+        return a[..., 1:-1, :-2], a[..., 2:, 1:-1], a[..., 1:-1, 2:], a[..., :-2, 1:-1]
 
     def time_step(self, C, geo, prm: Params):
         """turbnstwod.f90:97-114."""
@@ -395,85 +383,78 @@ class Scheme:
         return dt, p
 
     def dissipation(self, C, p, dt, geo, rtol):
-        """DISSIPATION (solver_state.f90:70-225); ghosts hold copies of their parent."""
-        P = _pad(p)
-        Pn = self._nb(P)
+        """DISSIPATION (solver_state.f90:70-225); ghosts hold copies of their parent.
+        Returns D [5, NI, NJ]."""
+        Pn = self._nb(_pad(p))
         anu = (torch.abs(Pn[0] - p) + torch.abs(Pn[1] - p) + torch.abs(Pn[2] - p) + torch.abs(Pn[3] - p)) / \
               (torch.abs(Pn[0] + p) + torch.abs(Pn[1] + p) + torch.abs(Pn[2] + p) + torch.abs(Pn[3] + p))
-        C5 = _pad(C[4])
-        c5n = self._nb(C5)
+        Cp = _pad(C)
+        Cn = self._nb(Cp)
         c5 = C[4]
+        c5n = [x[4] for x in Cn]
         anurt = (torch.abs(c5n[0] - c5) + torch.abs(c5n[1] - c5) + torch.abs(c5n[2] - c5) +
                  torch.abs(c5n[3] - c5)) / dmax(torch.abs(c5n[0] + c5) + torch.abs(c5n[1] + c5) +
                                                 torch.abs(c5n[2] + c5) + torch.abs(c5n[3] + c5),
                                                 8.0 * C[0] * rtol)
-        Cp = [_pad(C[m]) for m in range(5)]
-        d2q = []
-        for m in range(5):
-            n = self._nb(Cp[m])
-            d2q.append(n[0] + n[1] + n[2] + n[3] - 4.0 * C[m])
+        d2q = Cn[0] + Cn[1] + Cn[2] + Cn[3] - 4.0 * C
+        dn = self._nb(_pad(d2q))
         vbd = geo["vol"] / dt
-        VBD = _pad(vbd)
-        vbdn = self._nb(VBD)
-        sens = [_pad(anu), _pad(anurt)]
-        out = []
-        for m in range(5):
-            S = sens[1] if m == 4 else sens[0]
-            si = S[1:-1, 1:-1]
-            sn = self._nb(S)
-            cn = self._nb(Cp[m])
-            dn = self._nb(_pad(d2q[m]))
-            D2 = D4 = None
-            for k in range(4):
-                e2 = C02 * dmax(si, sn[k])
-                e4 = dmax(torch.zeros_like(e2), C04 - e2)
-                d24 = 0.5 * (vbd + vbdn[k])
-                t2 = e2 * d24 * (cn[k] - C[m])
-                t4 = e4 * d24 * (dn[k] - d2q[m])
-                D2 = t2 if D2 is None else D2 + t2
-                D4 = t4 if D4 is None else D4 + t4
-            out.append(D2 - D4)
-        return out
+        vbdn = self._nb(_pad(vbd))
+        S = _pad(torch.stack([anu, anurt]))
+        si = S[:, 1:-1, 1:-1]
+        sn = self._nb(S)
+        comp = self.sensor_of  # sensor of each equation: ANU for 1-4, ANURT for 5
+        D2 = D4 = None
+        for k in range(4):
+            e2 = C02 * dmax(si, sn[k])
+            e4 = dmax(torch.zeros_like(e2), C04 - e2)
+            d24 = 0.5 * (vbd + vbdn[k])
+            t2 = (e2 * d24).index_select(0, comp) * (Cn[k] - C)
+            t4 = (e4 * d24).index_select(0, comp) * (dn[k] - d2q)
+            D2 = t2 if D2 is None else D2 + t2
+            D4 = t4 if D4 is None else D4 + t4
+        return D2 - D4
 
     def viscous(self, full, geo, prm: Params, rtol):
-        """COMPUTE_VISCOUS (viscous.f90:29-217) from the padded primitives of stage 1."""
+        """COMPUTE_VISCOUS (viscous.f90:29-217) from the padded field set of stage 1.
+        Returns VIS [4, NI, NJ]."""
         flow = self.flow
         ni, nj = self.ni, self.nj
-        rho = full["c"][0]
-        r = full["c"][4] / rho
-        vals = {"u": full["u"], "v": full["v"], "t": full["t"], "rho": rho, "r": r}
-        nodes = {}
-        for k, a in vals.items():
-            rows, cols = self.navg[k]
-            s = torch.zeros(self.count.shape[0], dtype=a.dtype, device=a.device).index_add(
-                0, rows, a.reshape(-1).index_select(0, cols))
-            if k == "r":
-                s = s + self.r_reset * (rtol * flow.rtred)
-            nodes[k] = (s / self.count).reshape(ni + 1, nj + 1)
-        nodes["r"] = dmax(torch.zeros_like(nodes["r"]) + rtol, nodes["r"])
+        rho = full[C_]
+        vals = torch.stack([full[U_], full[V_], full[T_], rho, full[C_ + 4] / rho])  # u v t rho r
+        flat = vals.reshape(5, -1)
+        nodes = []
+        for k, name in enumerate(("u", "v", "t", "rho", "r")):
+            rows, cols = self.navg[name]
+            sacc = torch.zeros(self.count.shape[0], dtype=vals.dtype, device=vals.device).index_add(
+                0, rows, flat[k].index_select(0, cols))
+            if name == "r":
+                sacc = sacc + self.r_reset * (rtol * flow.rtred)
+            nodes.append(sacc / self.count)
+        nodes = torch.stack(nodes).reshape(5, ni + 1, nj + 1)
+        nodes = torch.cat([nodes[:4], dmax(torch.zeros_like(nodes[4:]) + rtol, nodes[4:])])
         x, y = geo["x"], geo["y"]
         corner = [(slice(None, -1), slice(None, -1)), (slice(1, None), slice(None, -1)),
                   (slice(1, None), slice(1, None)), (slice(None, -1), slice(1, None))]
-        A = {k: a[1:-1, 1:-1] for k, a in vals.items()}
+        A = vals[:, 1:-1, 1:-1]
         xa, ya = geo["xc"][1:-1, 1:-1], geo["yc"][1:-1, 1:-1]
-        nbs = {k: self._nb(a) for k, a in vals.items()}
+        nbs = self._nb(vals)
         xcn, ycn = self._nb(geo["xc"]), self._nb(geo["yc"])
         amu_c = SUTH * math.sqrt(flow.amol)
         vis = None
         for face in range(4):
             b, d = corner[face], corner[(face + 1) % 4]
             XB, YB, XD, YD = x[b], y[b], x[d], y[d]
-            B = {k: nodes[k][b] for k in nodes}
-            D = {k: nodes[k][d] for k in nodes}
-            Cc = {k: nbs[k][face] for k in nbs}
+            B, D = nodes[(slice(None),) + b], nodes[(slice(None),) + d]
+            Cc = nbs[face]
             XC, YC = xcn[face], ycn[face]
             dnr = (xa - XC) * (YB - YD) - (XB - XD) * (ya - YC)
-            gx = lambda k: ((A[k] - Cc[k]) * (YB - YD) - (B[k] - D[k]) * (ya - YC)) / dnr
-            gy = lambda k: (-(A[k] - Cc[k]) * (XB - XD) + (B[k] - D[k]) * (xa - XC)) / dnr
-            DUX, DVX, DTX, DRX = gx("u"), gx("v"), gx("t"), gx("r")
-            DUY, DVY, DTY, DRY = gy("u"), gy("v"), gy("t"), gy("r")
-            avg = lambda k: 0.25 * (A[k] + B[k] + Cc[k] + D[k])
-            UAVG, VAVG, TAVG, RHOAVG, RAVG = avg("u"), avg("v"), avg("t"), avg("rho"), avg("r")
+            GX = ((A - Cc) * (YB - YD) - (B - D) * (ya - YC)) / dnr
+            GY = (-(A - Cc) * (XB - XD) + (B - D) * (xa - XC)) / dnr
+            DUX, DVX, DTX, DRX = GX[0], GX[1], GX[2], GX[4]
+            DUY, DVY, DTY, DRY = GY[0], GY[1], GY[2], GY[4]
+            AV = 0.25 * (A + B + Cc + D)
+            UAVG, VAVG, TAVG, RHOAVG, RAVG = AV[0], AV[1], AV[2], AV[3], AV[4]
             if flow.iaxis == 1:
                 YAVG = 0.5 * (YB + YD)
                 VBYY = torch.where(YAVG < YAXIS_THRESH, DVY, VAVG / YAVG)
@@ -495,29 +476,30 @@ class Scheme:
             QXX = UAVG * TXX + VAVG * TXY + AKEFF * DTX
             QYY = UAVG * TXY + VAVG * TYY + AKEFF * DTY
             SX, SY = geo["sx"][face], geo["sy"][face]
-            f = [TXX * SX + TXY * SY, TXY * SX + TYY * SY, QXX * SX + QYY * SY,
-                 AMUEFF * DRX * SX + AMUEFF * DRY * SY]
-            vis = f if vis is None else [vis[k] + f[k] for k in range(4)]
+            f = torch.stack([TXX * SX + TXY * SY, TXY * SX + TYY * SY, QXX * SX + QYY * SY,
+                             AMUEFF * DRX * SX + AMUEFF * DRY * SY])
+            vis = f if vis is None else vis + f
         return vis
 
     def source(self, full, geo, prm: Params):
         """COMPUTE_SOURCE_TERMS (source_terms.f90:24-104): (SOURCE3, SOURCE5)."""
         flow = self.flow
-        u, v = full["u"], full["v"]
-        r = full["c"][4] / full["c"][0]
+        u, v = full[U_], full[V_]
+        r = full[C_ + 4] / full[C_]
         q = torch.sqrt(u * u + v * v)
+        stk = torch.stack([q, r, u, v])
+        F = self._nb(stk)  # A, B, C, D = NC1..NC4
         X, Y = self._nb(geo["xc"]), self._nb(geo["yc"])
-        U, V, R, Q = self._nb(u), self._nb(v), self._nb(r), self._nb(q)
         XA, XB, XC, XD = X
         YA, YB, YC, YD = Y
         dnr = (XA - XC) * (YB - YD) - (XB - XD) * (YA - YC)
-        gx = lambda F: ((F[0] - F[2]) * (YB - YD) - (F[1] - F[3]) * (YA - YC)) / dnr
-        gy = lambda F: (-(F[0] - F[2]) * (XB - XD) + (F[1] - F[3]) * (XA - XC)) / dnr
-        DQX, DRX, DUX, DVX = gx(Q), gx(R), gx(U), gx(V)
-        DQY, DRY, DUY, DVY = gy(Q), gy(R), gy(U), gy(V)
-        rho = full["c"][0][1:-1, 1:-1]
-        ri = full["c"][4][1:-1, 1:-1] / rho
-        amu = self.amu(full["t"][1:-1, 1:-1])
+        GX = ((F[0] - F[2]) * (YB - YD) - (F[1] - F[3]) * (YA - YC)) / dnr
+        GY = (-(F[0] - F[2]) * (XB - XD) + (F[1] - F[3]) * (XA - XC)) / dnr
+        DQX, DRX, DUX, DVX = GX[0], GX[1], GX[2], GX[3]
+        DQY, DRY, DUY, DVY = GY[0], GY[1], GY[2], GY[3]
+        rho = full[C_][1:-1, 1:-1]
+        ri = full[C_ + 4][1:-1, 1:-1] / rho
+        amu = self.amu(full[T_][1:-1, 1:-1])
         chi = rho * ri / (CMU * amu)
         fmu = torch.tanh(ALPHA_T * chi * chi) / torch.tanh(BETA_T * chi * chi)
         fr2 = torch.tanh(torch.sqrt(chi)) / torch.tanh(chi * math.sqrt(2.0 * math.sqrt(CMU)))
@@ -527,7 +509,7 @@ class Scheme:
         div23 = 2.0 / 3.0
         ycc = geo["yc"][1:-1, 1:-1]
         if flow.iaxis == 1:
-            vbyy = torch.where(ycc < YAXIS_THRESH, DVY, full["v"][1:-1, 1:-1] / ycc)
+            vbyy = torch.where(ycc < YAXIS_THRESH, DVY, full[V_][1:-1, 1:-1] / ycc)
             divvel = DUX + DVY + vbyy
             pk = amut / rho * (DUX * DUX + DVY * DVY + vbyy * vbyy + DUX * DUX + DVY * DVY +
                                vbyy * vbyy + (DUY + DVX) * (DUY + DVX) - div23 * divvel * divvel)
@@ -542,25 +524,21 @@ class Scheme:
         s3 = None
         if flow.iaxis == 1:
             ttt = (amu + amut) * (vbyy + vbyy - div23 * divvel)
-            s3 = (full["p"][1:-1, 1:-1] - ttt) / ycc
+            s3 = (full[P_][1:-1, 1:-1] - ttt) / ycc
         return s3, s5
 
     def residual(self, full, geo, s3, s5):
-        """COMPUTE_RESIDUAL (residual.f90:23-62)."""
-        R = []
+        """COMPUTE_RESIDUAL (residual.f90:23-62): R [5, NI, NJ]."""
         sx, sy = geo["sx"], geo["sy"]
-        for m in range(5):
-            F, G = full["f"][m], full["g"][m]
-            FI, GI = F[1:-1, 1:-1], G[1:-1, 1:-1]
-            Fn, Gn = self._nb(F), self._nb(G)
-            acc = (FI + Fn[0]) * sx[0] + (GI + Gn[0]) * sy[0]
-            for k in range(1, 4):
-                acc = acc + (FI + Fn[k]) * sx[k] + (GI + Gn[k]) * sy[k]
-            R.append(0.5 * acc)
-        R[4] = R[4] - geo["vol"] * s5
-        if self.flow.iaxis == 1:
-            R[2] = R[2] - geo["vol"] * s3
-        return R
+        F, G = full[F_:F_ + 5], full[G_:G_ + 5]
+        FI, GI = F[:, 1:-1, 1:-1], G[:, 1:-1, 1:-1]
+        Fn, Gn = self._nb(F), self._nb(G)
+        acc = (FI + Fn[0]) * sx[0] + (GI + Gn[0]) * sy[0]
+        for k in range(1, 4):
+            acc = acc + (FI + Fn[k]) * sx[k] + (GI + Gn[k]) * sy[k]
+        R = 0.5 * acc
+        r2 = R[2] - geo["vol"] * s3 if self.flow.iaxis == 1 else R[2]
+        return torch.stack([R[0], R[1], r2, R[3], R[4] - geo["vol"] * s5])
 
     def iteration(self, Cold, geo, prm: Params):
         """One RK4 iteration (turbnstwod.f90:97-146): Q_old [5, NI, NJ] -> Q_new."""
@@ -569,20 +547,21 @@ class Scheme:
         D = self.dissipation(Cold, p, dt, geo, rtol)
         C = Cold
         vis = None
+        dtbyvol = dt / geo["vol"]
         for st in range(4):
             full = self.boundary(self.primitive(C, prm), prm)
             if st == 0:
                 vis = self.viscous(full, geo, prm, rtol)
+                # the viscous terms of equations 2..5, none in the continuity equation
+                vis5 = torch.cat([torch.zeros_like(vis[:1]), vis])
             s3, s5 = self.source(full, geo, prm)
             R = self.residual(full, geo, s3, s5)
-            dtv = ALPHA_RK[st] * (dt / geo["vol"])
-            n0 = Cold[0] - dtv * (R[0] - D[0])
-            n1 = Cold[1] - dtv * (R[1] - vis[0] - D[1])
-            n2 = Cold[2] - dtv * (R[2] - vis[1] - D[2])
-            n3 = Cold[3] - dtv * (R[3] - vis[2] - D[3])
+            dtv = ALPHA_RK[st] * dtbyvol
+            N = Cold - dtv * (R - vis5 - D)
             n4 = Cold[4] - dtv * CFLTURB * (R[4] - vis[3] - D[4])
+            n0 = N[0]
             n4 = n0 * dmax(torch.zeros_like(n0) + rtol, n4 / n0)
-            C = torch.stack([n0, n1, n2, n3, n4])
+            C = torch.cat([N[:4], n4[None]])
         return C
 
     # ------------------------------------------------------------------ objectives
@@ -594,9 +573,9 @@ class Scheme:
                4: ((1, slice(1, -1)), (0, slice(1, -1))), 2: ((-2, slice(1, -1)), (-1, slice(1, -1)))}[side]
         pa, gh = idx
         avg = lambda a: 0.5 * (a[pa] + a[gh])
-        rho = full["p"] / (prm.rr * full["t"])
-        return {"u": avg(full["u"]), "v": avg(full["v"]), "p": avg(full["p"]), "rho": avg(rho),
-                "t": avg(full["t"])}
+        rho = full[P_] / (prm.rr * full[T_])
+        return {"u": avg(full[U_]), "v": avg(full[V_]), "p": avg(full[P_]), "rho": avg(rho),
+                "t": avg(full[T_])}
 
     def side_vectors(self, geo, side: int):
         face = side - 1
