@@ -592,13 +592,14 @@ void launch_time_step_scratch(const Params& P, const double* q, const double* cf
 
 // ------------------------------------------------------------ port mass flux
 
-// One warp per type-6 ghost: sum of C1*U*DELY(*YCC) along the mesh line through the
-// parent, across to the opposite boundary (the repaired GPORT walk).
+// One block per type-6 ghost: sum of C1*U*DELY(*YCC) along the mesh line through the
+// parent, across to the opposite boundary (the repaired GPORT walk); its threads stride
+// the line, then a warp and block reduction in fixed order.
 __global__ void k_gport(Params P, Mesh M, const double* __restrict__ q, const int* ghosts,
                         int nport, double* gport) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int w = blockIdx.x;  // one block per port ghost
     const int lane = threadIdx.x & 31;
-    if (w >= nport) return;
+    if (w >= nport) return;  // whole block
     const size_t ncell = (size_t)M.ni * M.nj;
     const int g = ghosts[w];
     int side, along;
@@ -608,7 +609,7 @@ __global__ void k_gport(Params P, Mesh M, const double* __restrict__ q, const in
     else { side = 4; along = g - 2 * M.ni - M.nj; }
     const int len = (side == 1 || side == 3) ? M.nj : M.ni;
     double sum = 0.0;
-    for (int k = lane; k < len; k += 32) {
+    for (int k = threadIdx.x; k < len; k += GP_THREADS) {
         const int i = (side == 1 || side == 3) ? along : k;
         const int j = (side == 1 || side == 3) ? k : along;
         const size_t c = (size_t)i * M.nj + j;
@@ -626,7 +627,15 @@ __global__ void k_gport(Params P, Mesh M, const double* __restrict__ q, const in
         sum += term;
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0) gport[g] = sum;
+    __shared__ double part[GP_THREADS / 32];
+    if (lane == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = part[0];
+#pragma unroll
+        for (int k = 1; k < GP_THREADS / 32; k++) t += part[k];
+        gport[g] = t;
+    }
 }
 
 // ------------------------------------------------------ primitive output
@@ -868,9 +877,7 @@ void launch_dtmin(const Params& P, const Mesh& M, const double* q, double* parti
 void launch_gport(const Params& P, const Mesh& M, const double* q, const int* ghosts, int nport,
                   double* gport, cudaStream_t s) {
     if (nport <= 0) return;
-    const int threads = 256, warps_per_block = threads / 32;
-    k_gport<<<(nport + warps_per_block - 1) / warps_per_block, threads, 0, s>>>(P, M, q, ghosts,
-                                                                               nport, gport);
+    k_gport<<<nport, GP_THREADS, 0, s>>>(P, M, q, ghosts, nport, gport);
 }
 
 void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStream_t s) {

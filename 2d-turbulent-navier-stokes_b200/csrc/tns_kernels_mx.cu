@@ -625,9 +625,9 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation_mx(Params P, Mesh M, c
 __global__ void k_gport_mx(Params P, Mesh M, const double* __restrict__ cold,
                            const float* __restrict__ dq, const int* ghosts, int nport,
                            double* gport) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int w = blockIdx.x;  // one block per port ghost
     const int lane = threadIdx.x & 31;
-    if (w >= nport) return;
+    if (w >= nport) return;  // whole block
     const size_t ncell = (size_t)M.ni * M.nj;
     const StateMixed st{cold, dq, ncell};
     const int g = ghosts[w];
@@ -638,7 +638,7 @@ __global__ void k_gport_mx(Params P, Mesh M, const double* __restrict__ cold,
     else { side = 4; along = g - 2 * M.ni - M.nj; }
     const int len = (side == 1 || side == 3) ? M.nj : M.ni;
     double sum = 0.0;
-    for (int k = lane; k < len; k += 32) {
+    for (int k = threadIdx.x; k < len; k += GP_THREADS) {
         const int i = (side == 1 || side == 3) ? along : k;
         const int j = (side == 1 || side == 3) ? k : along;
         const size_t c = (size_t)i * M.nj + j;
@@ -655,7 +655,15 @@ __global__ void k_gport_mx(Params P, Mesh M, const double* __restrict__ cold,
         sum += term;
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0) gport[g] = sum;
+    __shared__ double part[GP_THREADS / 32];
+    if (lane == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = part[0];
+#pragma unroll
+        for (int k = 1; k < GP_THREADS / 32; k++) t += part[k];
+        gport[g] = t;
+    }
 }
 
 // ------------------------------------------------------ primitive output
@@ -773,7 +781,7 @@ void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const f
 void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
                      const int* ghosts, int nport, double* gport, cudaStream_t s) {
     if (nport <= 0) return;
-    k_gport_mx<<<(nport + 7) / 8, 256, 0, s>>>(P, M, cold, dq, ghosts, nport, gport);
+    k_gport_mx<<<nport, GP_THREADS, 0, s>>>(P, M, cold, dq, ghosts, nport, gport);
 }
 
 void launch_prim_out_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,

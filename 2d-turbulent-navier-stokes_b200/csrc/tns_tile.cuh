@@ -23,6 +23,7 @@ namespace tns {
 // threads per SM at every tile height.
 #define TNS_PER_SM(n) ((n) * 8 / TNS_TI > 0 ? (n) * 8 / TNS_TI : 1)
 constexpr int TJ = 32;      // tile extent along j (contiguous in memory)
+constexpr int GP_THREADS = 128;  // threads per port line of the type-6 port-flux kernels
 constexpr int TI = TNS_TI;  // tile extent along i
 constexpr int NTHREADS = TJ * TI;
 // The viscous kernels may run one extra row of threads: a tile has (TI+1)*TJ + TI*(TJ+1)

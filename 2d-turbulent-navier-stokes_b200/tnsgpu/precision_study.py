@@ -27,10 +27,15 @@ CASES = {
     "nozzle_plume_1024x384": lambda: (cases.nozzle_plume_mesh(1024, 384), cases.nozzle_plume_flow()),
     "nozzle_plume_256x96": lambda: (cases.nozzle_plume_mesh(256, 96), cases.nozzle_plume_flow()),
     "ramp_192x64": lambda: (cases.ramp_mesh(192, 64), cases.ramp_flow()),
+    "port_4096x1536": lambda: (cases.port_mesh(4096, 1536), cases.port_flow()),
+    "port_1024x384": lambda: (cases.port_mesh(1024, 384), cases.port_flow()),
 }
+# the wall whose pressure and force are reported: BC type and side (the port channel's
+# injecting wall is type 6; the other cases' upper wall is type 5)
+WALL = {"port_4096x1536": (6, 3), "port_1024x384": (6, 3)}
 
 
-def run(mesh, flow, c0, rinit, precision, iters, monitor=1000):
+def run(mesh, flow, c0, rinit, precision, iters, monitor=1000, wall=(5, 3)):
     s = Solver(mesh, flow, rinit, precision=precision)
     s.upload(c0)
     first = s.run(1, 1)[0]
@@ -53,8 +58,9 @@ def run(mesh, flow, c0, rinit, precision, iters, monitor=1000):
     if status == "ok":
         prims = s.primitives()
         out.update(state=s.download(),
-                   wall_p=objectives.wall_pressure(mesh, prims, flow.amol, side=3)[1],
-                   force=objectives.wall_force(mesh, prims, flow.amol, flow.iaxis, side=3),
+                   wall_p=objectives.wall_pressure(mesh, prims, flow.amol, side=wall[1], wall_type=wall[0])[1],
+                   force=objectives.wall_force(mesh, prims, flow.amol, flow.iaxis, side=wall[1],
+                                               wall_type=wall[0]),
                    mdot=objectives.outlet_mass_flow(mesh, prims, flow.amol, flow.iaxis, side=2))
     s.close()
     return out
@@ -75,10 +81,11 @@ def compare(case="nozzle_plume_1024x384", iters=20000, seed=0):
     rinit = formats.rinit_cold(flow)
     c0 = formats.cold_state(flow, mesh.neles, rinit)
     c1 = c0 * (1.0 + 1e-15 * np.random.default_rng(seed).standard_normal(c0.shape))
-    f64 = run(mesh, flow, c0, rinit, 0, iters)
-    f64p = run(mesh, flow, c1, rinit, 0, iters)
-    mx = run(mesh, flow, c0, rinit, 1, iters)
-    out = {"case": case, "cells": mesh.neles, "iterations": iters,
+    wall = WALL.get(case, (5, 3))
+    f64 = run(mesh, flow, c0, rinit, 0, iters, wall=wall)
+    f64p = run(mesh, flow, c1, rinit, 0, iters, wall=wall)
+    mx = run(mesh, flow, c0, rinit, 1, iters, wall=wall)
+    out = {"case": case, "cells": mesh.neles, "iterations": iters, "wall": {"type": wall[0], "side": wall[1]},
            "fp64": {k: f64[k] for k in ("status", "iterations", "cell_iter_per_s")},
            "mixed": {k: mx[k] for k in ("status", "iterations", "cell_iter_per_s")},
            "fp64_final_residual_ratio": f64["history"][-1][1] if f64["history"] else None,
