@@ -50,7 +50,9 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
+    pdl_trigger();
     load_nodes(M, i0, j0, S.nx, S.ny);
+    pdl_wait();
     __syncthreads();
     for (int s = tid; s < NSLOT; s += NTHREADS) {
         const int li = s / SW, lj = s % SW;
@@ -217,7 +219,9 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
+    pdl_trigger();
     load_nodes(M, i0, j0, S.nx, S.ny, VNT);
+    pdl_wait();
     __syncthreads();
     for (int s = tid; s < NSLOT; s += VNT) {
         const int li = s / SW, lj = s % SW;
@@ -386,6 +390,7 @@ __device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M,
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
 
+    pdl_trigger();
     for (int s = tid; s < NNODE; s += NTHREADS) {
         const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
         if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
@@ -394,6 +399,7 @@ __device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M,
             sny[s] = M.y[n];
         }
     }
+    pdl_wait();
     for (int s = tid; s < NDSLOT; s += NTHREADS) {
         const int i = i0 - 2 + s / DW, j = j0 - 2 + s % DW;
         if (i >= 0 && i < M.ni && j >= 0 && j < M.nj) {
@@ -842,17 +848,17 @@ void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* acti
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,
                         const double* dtmin, cudaStream_t s) {
     DissArgs<double> A{q, d, dt, dtmin};
-    k_dissipation<double><<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
+    launch_tile(k_dissipation<double>, tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s, P, M, A);
 }
 
 void launch_dissipation_mx(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
                            const double* dtmin, cudaStream_t s) {
     DissArgs<float> A{q, d, dt, dtmin};
-    k_dissipation<float><<<tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s>>>(P, M, A);
+    launch_tile(k_dissipation<float>, tile_grid(M), dim3(TJ, TI), diss_smem_bytes(), s, P, M, A);
 }
 
 void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis, cudaStream_t s) {
-    k_viscous<<<tile_grid(M), dim3(TJ, VROWS), visc_smem_bytes(), s>>>(P, M, q, vis);
+    launch_tile(k_viscous, tile_grid(M), dim3(TJ, VROWS), visc_smem_bytes(), s, P, M, q, vis);
 }
 
 void launch_stage(const Params& P, const Mesh& M, const double* qin, const double* qold,
@@ -860,7 +866,7 @@ void launch_stage(const Params& P, const Mesh& M, const double* qin, const doubl
                   const double* dtmin, double alpha, unsigned long long* cdiff,
                   unsigned int* status, cudaStream_t s) {
     StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status};
-    k_stage<<<tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s>>>(P, M, A);
+    launch_tile(k_stage, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s, P, M, A);
 }
 
 int dtmin_blocks(const Mesh& M) {

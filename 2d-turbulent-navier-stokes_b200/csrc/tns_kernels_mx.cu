@@ -81,6 +81,9 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
     const StateMixed st{A.cold, A.dqin, ncell};
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
+    pdl_trigger();
+    load_nodes(M, i0, j0, S.nx, S.ny);
+    pdl_wait();
     if (tid == 0) {
         // tile reference flux: the first cell of the tile
         Prim r;
@@ -88,7 +91,6 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
 #pragma unroll
         for (int m = 0; m < 5; m++) { S.fref[m] = r.f[m]; S.gref[m] = r.g[m]; }
     }
-    load_nodes(M, i0, j0, S.nx, S.ny);
     __syncthreads();
     for (int s = tid; s < NSLOT; s += NTHREADS) {
         const int li = s / SW, lj = s % SW;
@@ -355,7 +357,9 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
+    pdl_trigger();
     load_nodes(M, i0, j0, S.nx, S.ny, VNT);
+    pdl_wait();
     __syncthreads();
     for (int s = tid; s < NSLOT; s += VNT) {
         const int li = s / SW, lj = s % SW;
@@ -516,7 +520,9 @@ __device__ __forceinline__ void dissipation_mx_tile(const Params& P, const Mesh&
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
+    pdl_trigger();
     load_nodes(M, i0, j0, S.nx, S.ny);
+    pdl_wait();
     for (int s = tid; s < NDSLOTM; s += NTHREADS) {
         const int i = i0 - 2 + s / DWM, j = j0 - 2 + s % DWM;
         if (i >= 0 && i < M.ni && j >= 0 && j < M.nj) {
@@ -763,11 +769,11 @@ void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* activ
 
 void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, float* d, float* dt,
                             const double* dtmin, cudaStream_t s) {
-    k_dissipation_mx<<<tile_grid_mx(M), dim3(TJ, TI), diss_mx_smem_bytes(), s>>>(P, M, q, d, dt, dtmin);
+    launch_tile(k_dissipation_mx, tile_grid_mx(M), dim3(TJ, TI), diss_mx_smem_bytes(), s, P, M, q, d, dt, dtmin);
 }
 
 void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* vis, cudaStream_t s) {
-    k_viscous_mx<<<tile_grid_mx(M), dim3(TJ, VROWS), visc_mx_smem_bytes(), s>>>(P, M, q, vis);
+    launch_tile(k_viscous_mx, tile_grid_mx(M), dim3(TJ, VROWS), visc_mx_smem_bytes(), s, P, M, q, vis);
 }
 
 void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,
@@ -775,7 +781,7 @@ void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const f
                      const double* dtmin, double alpha, unsigned long long* cdiff,
                      unsigned int* status, cudaStream_t s) {
     StageArgsMx A{cold, dqin, dqout, qout, d, vis, dt, dtmin, (float)alpha, cdiff, status};
-    k_stage_mx<<<tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s>>>(P, M, A);
+    launch_tile(k_stage_mx, tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s, P, M, A);
 }
 
 void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,

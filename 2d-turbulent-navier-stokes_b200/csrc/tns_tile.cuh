@@ -3,6 +3,8 @@
 // position (BC of boundary.f90:24-327 from the parent and its opposite neighbour).
 #pragma once
 
+#include <utility>
+
 #include "tns_device.cuh"
 
 namespace tns {
@@ -54,6 +56,47 @@ __device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double
             sny[s] = M.y[n];
         }
     }
+}
+
+// Programmatic dependent launch: a tile kernel lets the next kernel in the stream start
+// as soon as all its blocks are running (pdl_trigger), and waits for the previous one
+// to finish, with its memory visible, before it touches data that kernel produced
+// (pdl_wait).  The node coordinates, which nothing writes, load before the wait.  Both
+// are no-ops when the kernel was not launched with the attribute.
+#ifndef TNS_PDL
+#define TNS_PDL 1
+#endif
+__device__ __forceinline__ void pdl_trigger() {
+#if TNS_PDL
+    asm volatile("griddepcontrol.launch_dependents;");
+#endif
+}
+__device__ __forceinline__ void pdl_wait() {
+#if TNS_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+// Launch of a tile kernel that may overlap its predecessor's tail (see pdl_wait).
+template <class... Exp, class... Act>
+inline cudaError_t launch_tile(void (*kernel)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                               Act&&... args) {
+#if TNS_PDL
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...);
+#else
+    kernel<<<grid, block, smem, s>>>(std::forward<Act>(args)...);
+    return cudaGetLastError();
+#endif
 }
 
 // How a kernel reads the conservative state of cell c: FP64 array, or FP64 COLD plus an
