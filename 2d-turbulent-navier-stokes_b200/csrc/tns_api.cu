@@ -183,6 +183,15 @@ int build_mesh(tns_handle* h, const tns_mesh* m) {
             const size_t n1 = (size_t)i * (nj + 1) + j;
             const double X1 = X[n1], X2 = X[n1 + nj + 1], X3 = X[n1 + nj + 2], X4 = X[n1 + 1];
             const double Y1 = Y[n1], Y2 = Y[n1 + nj + 1], Y3 = Y[n1 + nj + 2], Y4 = Y[n1 + 1];
+            // a cell the scheme would divide by: non-finite corners or zero volume
+            // (geometry.f90:75-103 takes |VOL| and would carry a zero into DT/VOL)
+            if (!(std::isfinite(X1) && std::isfinite(X2) && std::isfinite(X3) && std::isfinite(X4) &&
+                  std::isfinite(Y1) && std::isfinite(Y2) && std::isfinite(Y3) && std::isfinite(Y4)))
+                return h->fail(TNS_ERR_MESH, "cell %d has a non-finite node coordinate", c + 1);
+            double vol = 0.5 * ((X3 - X1) * (Y4 - Y2) - (X4 - X2) * (Y3 - Y1));
+            if (h->P.iaxis == 1) vol = vol * ((Y1 + Y2 + Y3 + Y4) * 0.25);
+            if (vol == 0.0)
+                return h->fail(TNS_ERR_MESH, "cell %d has zero volume (collapsed or on the axis)", c + 1);
             // geometry.f90:70-74
             const double DL12 = std::sqrt((X1 - X2) * (X1 - X2) + (Y1 - Y2) * (Y1 - Y2));
             const double DL23 = std::sqrt((X2 - X3) * (X2 - X3) + (Y2 - Y3) * (Y2 - Y3));

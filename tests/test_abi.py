@@ -46,7 +46,8 @@ def _create(mesh, flow=None):
 
 
 @pytest.mark.parametrize("breakage,code", [
-    ("type", -2), ("side", -2), ("parent", -2), ("nc", -2), ("unstructured", -3)])
+    ("type", -2), ("side", -2), ("parent", -2), ("nc", -2), ("unstructured", -3),
+    ("collapsed", -2), ("nan_coordinate", -2)])
 def test_host_validation_rejects_bad_meshes(breakage, code):
     m = cases.ramp_mesh(6, 4)
     if breakage == "type":
@@ -57,6 +58,16 @@ def test_host_validation_rejects_bad_meshes(breakage, code):
         m.nparent[2] = m.nparent[2] + 1
     elif breakage == "nc":
         m.nc[5, 1] = 10_000     # neither a cell nor a ghost
+    elif breakage == "collapsed":
+        # cell (2, 1): move its nodes N2, N3 onto N1, N4 -> zero area (DT/VOL would divide by 0)
+        n = m.nod[2 * 4 + 1] - 1
+        m.x = m.x.copy()
+        m.y = m.y.copy()
+        m.x[n[1]], m.y[n[1]] = m.x[n[0]], m.y[n[0]]
+        m.x[n[2]], m.y[n[2]] = m.x[n[3]], m.y[n[3]]
+    elif breakage == "nan_coordinate":
+        m.y = m.y.copy()
+        m.y[7] = float("nan")   # e.g. a corrupted grid.in value
     else:
         # swap two interior neighbours: still consistent ids, no longer an i x j block
         m.nc[9, 1], m.nc[9, 2] = m.nc[9, 2], m.nc[9, 1]

@@ -35,6 +35,46 @@ def test_main_reports_missing_flow_in(tmp_path):
     assert r.returncode == 2 and "flow.in" in r.stderr
 
 
+def test_main_reports_truncated_grid_in(tmp_path):
+    m, f = cases.ramp_mesh(6, 4), cases.ramp_flow(10)
+    f.istart = 0
+    formats.write_case(str(tmp_path), m, f)
+    g = tmp_path / "grid.in"
+    lines = g.read_text().splitlines()
+    g.write_text("\n".join(lines[: len(lines) // 2]) + "\n")  # cut in the middle
+    r = _run("twodturb", tmp_path)
+    assert r.returncode == 2 and "grid.in" in r.stderr and "end of file" in r.stderr
+
+
+def test_main_rejects_collapsed_cell_before_touching_cuda(tmp_path):
+    m, f = cases.ramp_mesh(6, 4), cases.ramp_flow(10)
+    f.istart = 0
+    n = m.nod[9] - 1  # cell 10: N2, N3 moved onto N1, N4
+    m.x_mm = m.x_mm.copy()
+    m.y_mm = m.y_mm.copy()
+    m.x_mm[n[1]], m.y_mm[n[1]] = m.x_mm[n[0]], m.y_mm[n[0]]
+    m.x_mm[n[2]], m.y_mm[n[2]] = m.x_mm[n[3]], m.y_mm[n[3]]
+    m.x, m.y = m.x_mm * 0.001, m.y_mm * 0.001
+    formats.write_case(str(tmp_path), m, f)
+    r = _run("twodturb", tmp_path)
+    assert r.returncode == 1
+    assert "tns_create failed (-2)" in r.stderr and "zero volume" in r.stderr
+
+
+@pytest.mark.gpu
+def test_main_reports_nan_in_restart(tmp_path):
+    """A NaN in restart.in turns the state non-finite; the main stops with the error
+    instead of writing NaN restart files."""
+    mesh, flow = cases.ramp_mesh(24, 10), cases.ramp_flow(2000)
+    c0, rinit = cases.noisy_restart_state(flow, mesh.neles)
+    c0[0, 17] = float("nan")
+    formats.write_case(str(tmp_path), mesh, flow)
+    formats.write_restart(str(tmp_path / "restart.in"), c0, flow.rtred, flow.npseudo, rinit, 0)
+    r = _run("twodturb", tmp_path)
+    assert r.returncode == 1
+    assert "(-5)" in r.stderr
+
+
 def _fortran_e(v, d=6):
     """Ew.d of a positive value, as the reference's FORMAT(... E12.6 ...) prints it."""
     if v == 0:
