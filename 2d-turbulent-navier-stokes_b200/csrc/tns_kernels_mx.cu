@@ -266,8 +266,13 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
     }
 }
 
+// Specialised on the residual monitor, so the CDIFF reduction is compiled only where it
+// runs.  (A local copy of Params to fix IAXIS costs this kernel registers and spills.)
+template <int MONITOR>
 __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_MINB)) k_stage_mx(Params P, Mesh M, StageArgsMx A) {
-    stage_mx_tile(P, M, A, blockIdx.x, blockIdx.y);
+    StageArgsMx Ac = A;
+    if (!MONITOR) Ac.cdiff = nullptr;
+    stage_mx_tile(P, M, Ac, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- viscous kernel
@@ -737,7 +742,10 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_BATCH_MINB))
 static dim3 tile_grid_mx(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
 
 cudaError_t configure_kernels_mx() {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_stage_mx<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)stage_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_stage_mx<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)stage_mx_smem_bytes());
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_dissipation_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -781,7 +789,8 @@ void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const f
                      const double* dtmin, double alpha, unsigned long long* cdiff,
                      unsigned int* status, cudaStream_t s) {
     StageArgsMx A{cold, dqin, dqout, qout, d, vis, dt, dtmin, (float)alpha, cdiff, status};
-    launch_tile(k_stage_mx, tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s, P, M, A);
+    launch_tile(cdiff ? k_stage_mx<1> : k_stage_mx<0>, tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s,
+                P, M, A);
 }
 
 void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
