@@ -163,8 +163,13 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
     }
 }
 
+// Specialised on the residual monitor, so the CDIFF reduction is compiled only where it
+// runs.
+template <int MONITOR>
 __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MINB)) k_stage(Params P, Mesh M, StageArgs A) {
-    stage_tile(P, M, A, blockIdx.x, blockIdx.y);
+    StageArgs Ac = A;
+    if (!MONITOR) Ac.cdiff = nullptr;
+    stage_tile(P, M, Ac, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- viscous kernel
@@ -812,7 +817,10 @@ static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni +
 
 cudaError_t configure_kernels() {
     cudaError_t e;
-    e = cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stage_smem_bytes());
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_viscous, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -866,7 +874,7 @@ void launch_stage(const Params& P, const Mesh& M, const double* qin, const doubl
                   const double* dtmin, double alpha, unsigned long long* cdiff,
                   unsigned int* status, cudaStream_t s) {
     StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status};
-    launch_tile(k_stage, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s, P, M, A);
+    launch_tile(cdiff ? k_stage<1> : k_stage<0>, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s, P, M, A);
 }
 
 int dtmin_blocks(const Mesh& M) {
