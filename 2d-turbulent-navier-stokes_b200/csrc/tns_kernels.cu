@@ -368,7 +368,7 @@ enum DField { DC0, DC1, DC2, DC3, DC4, DP, NDF };
 enum RField { RVBD, RANU, RANURT, RQ0, RQ1, RQ2, RQ3, RQ4, NRF };
 
 size_t diss_smem_bytes() {
-    return sizeof(double) * ((size_t)NDF * NDSLOT + (size_t)NRF * NRSLOT + 2 * NNODE);
+    return sizeof(double) * ((size_t)NDF * NDSLOT + (size_t)NRF * NRSLOT);
 }
 
 __device__ __forceinline__ double local_dt(const Params& P, double c1, double c2, double c3,
@@ -389,21 +389,11 @@ __device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M,
     extern __shared__ double smem[];
     double* sd = smem;                  // NDF x NDSLOT
     double* sr = sd + NDF * NDSLOT;     // NRF x NRSLOT
-    double* snx = sr + NRF * NRSLOT;
-    double* sny = snx + NNODE;
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
 
     pdl_trigger();
-    for (int s = tid; s < NNODE; s += NTHREADS) {
-        const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
-        if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
-            const size_t n = (size_t)a * (M.nj + 1) + b;
-            snx[s] = M.x[n];
-            sny[s] = M.y[n];
-        }
-    }
     pdl_wait();
     for (int s = tid; s < NDSLOT; s += NTHREADS) {
         const int i = i0 - 2 + s / DW, j = j0 - 2 + s % DW;
@@ -465,9 +455,10 @@ __device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M,
         } else {
             DT = *A.dtmin;
         }
-        const int n1 = ri * NW + rj;
-        const double X[4] = {snx[n1], snx[n1 + NW], snx[n1 + NW + 1], snx[n1 + 1]};
-        const double Y[4] = {sny[n1], sny[n1 + NW], sny[n1 + NW + 1], sny[n1 + 1]};
+        // the cell's corners straight from the node arrays (read once per ring cell)
+        const size_t g1 = (size_t)i * (M.nj + 1) + j, g2 = g1 + M.nj + 1;
+        const double X[4] = {M.x[g1], M.x[g2], M.x[g2 + 1], M.x[g1 + 1]};
+        const double Y[4] = {M.y[g1], M.y[g2], M.y[g2 + 1], M.y[g1 + 1]};
         const double ycc = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
         sr[RVBD * NRSLOT + s] = cell_volume(P.iaxis, X, Y, ycc) / DT;
     }
@@ -776,7 +767,7 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation_batch(const BatchCase*
     dissipation_tile<double>(c.P, c.M, c.diss, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_MINB)) k_viscous_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_BATCH_MINB)) k_viscous_batch(const BatchCase* __restrict__ cases,
                                                                           const int4* __restrict__ tiles,
                                                                           const int* __restrict__ active) {
     const int4 t = tiles[blockIdx.x];

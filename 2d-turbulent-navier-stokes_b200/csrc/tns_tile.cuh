@@ -19,7 +19,10 @@ namespace tns {
 #define TNS_STAGE_BATCH_MINB 2
 #endif
 #ifndef TNS_VISC_MINB
-#define TNS_VISC_MINB 1
+#define TNS_VISC_MINB 3  // 80 registers: 3 blocks/SM beat 2 blocks without the cap
+#endif
+#ifndef TNS_VISC_BATCH_MINB
+#define TNS_VISC_BATCH_MINB 1  // descriptor-fed arguments spill at 3 blocks/SM
 #endif
 // Resident blocks per SM of a kernel tuned at TI = 8, for the compiled TI: the same
 // threads per SM at every tile height.
