@@ -70,7 +70,10 @@ __device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p
 #define TNS_STAGE_MX_BATCH_MINB 3
 #endif
 #ifndef TNS_VISC_MX_MINB
-#define TNS_VISC_MX_MINB 3
+#define TNS_VISC_MX_MINB 4  // 64 registers with small spills beat 80 registers at 3 blocks/SM
+#endif
+#ifndef TNS_VISC_MX_BATCH_MINB
+#define TNS_VISC_MX_BATCH_MINB 3
 #endif
 // One stage on tile (bx, by) of a mesh; the single-case and the batched kernels wrap it.
 __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, const StageArgsMx& A,
@@ -717,7 +720,7 @@ __global__ void __launch_bounds__(NTHREADS) k_dissipation_mx_batch(const BatchCa
     dissipation_mx_tile(c.P, c.M, c.qmx[parity], c.df, c.dtf, c.dtmin, t.y, t.z);
 }
 
-__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_MX_MINB)) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
+__global__ void __launch_bounds__(VNT, TNS_PER_SM(TNS_VISC_MX_BATCH_MINB)) k_viscous_mx_batch(const BatchCase* __restrict__ cases,
                                                                                 const int4* __restrict__ tiles,
                                                                                 const int* __restrict__ active,
                                                                                 int parity) {
