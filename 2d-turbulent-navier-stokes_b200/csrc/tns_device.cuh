@@ -11,6 +11,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Host-and-device helpers: the discrete adjoint calls the same arithmetic from its
+// point functions, which also compile for the host.
+#define TNS_HD __host__ __device__ __forceinline__
+
 namespace tns {
 
 // constants.f90:15-60
@@ -70,11 +74,11 @@ struct Mesh {
     __host__ __device__ int nghosts() const { return 2 * (ni + nj); }
 };
 
-__device__ __forceinline__ double dmax1(double a, double b) { return a >= b ? a : b; }
-__device__ __forceinline__ double dmin1(double a, double b) { return a <= b ? a : b; }
+TNS_HD double dmax1(double a, double b) { return a >= b ? a : b; }
+TNS_HD double dmin1(double a, double b) { return a <= b ? a : b; }
 
 // Fortran REAL**INTEGER by square-and-multiply.
-__device__ __forceinline__ double powi(double x, int n) {
+TNS_HD double powi(double x, int n) {
     double r = 1.0, b = x;
     int m = n < 0 ? -n : n;
     while (m) {
@@ -90,8 +94,12 @@ __device__ __forceinline__ double powi(double x, int n) {
 //   y <- y - f(y)/f'(y) = 0.8 y + 0.2 T^3 / y^4,
 // whose error squares per step (e' ~ 2 e^2): 2e-14 after one, FP64 rounding after two.
 // Within a few ulp of pow, at less than half the instructions of exp(0.6 log T).
-__device__ __forceinline__ double pow06(double T) {
+TNS_HD double pow06(double T) {
+#ifdef __CUDA_ARCH__
     double y = (double)exp2f(0.6f * __log2f((float)T));
+#else
+    double y = (double)exp2f(0.6f * log2f((float)T));
+#endif
     const double t3 = T * T * T;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
@@ -104,13 +112,13 @@ __device__ __forceinline__ double pow06(double T) {
 // tanh(a) / tanh(b) for a, b >= 0, from tanh(x) = E / (E + 2) with E = expm1(2x):
 // Ea (Eb + 2) / (Eb (Ea + 2)), one division instead of three.  Arguments are capped at
 // 20, where tanh is 1 to double precision, so E stays finite.
-__device__ __forceinline__ double tanh_ratio(double a, double b) {
+TNS_HD double tanh_ratio(double a, double b) {
     const double ea = expm1(2.0 * fmin(a, 20.0)), eb = expm1(2.0 * fmin(b, 20.0));
     return (ea * (eb + 2.0)) / (eb * (ea + 2.0));
 }
 
 // Sutherland-type molecular viscosity SUTH_COEF*DSQRT(AMOL)*T**0.6 (viscous.f90:188).
-__device__ __forceinline__ double amu_of(const Params& P, double T) {
+TNS_HD double amu_of(const Params& P, double T) {
     return P.suth_amol * pow06(T);
 }
 
@@ -120,7 +128,7 @@ struct Prim {
     double f[5], g[5];
 };
 
-__device__ __forceinline__ void primitive(const Params& P, double c1, double c2, double c3,
+TNS_HD void primitive(const Params& P, double c1, double c2, double c3,
                                           double c4, double c5, Prim& s) {
     const double RHO = c1;
     const double rr = 1.0 / RHO;  // one reciprocal instead of four divisions
@@ -147,7 +155,7 @@ __device__ __forceinline__ void primitive(const Params& P, double c1, double c2,
 }
 
 // Conservative + flux tail shared by BC types 2,3,4,6,7 (e.g. boundary.f90:62-70).
-__device__ __forceinline__ void ghost_tail(const Params& P, double RHO, Prim& g) {
+TNS_HD void ghost_tail(const Params& P, double RHO, Prim& g) {
     g.rho = RHO;
     const double C2 = RHO * g.u;
     const double C3 = RHO * g.v;
@@ -164,7 +172,7 @@ __device__ __forceinline__ void ghost_tail(const Params& P, double RHO, Prim& g)
 }
 
 // Face surface vector (geometry.f90:77-99) for face k (1..4) of a cell with nodes 1..4.
-__device__ __forceinline__ void face_vector(int iaxis, int k, const double X[4],
+TNS_HD void face_vector(int iaxis, int k, const double X[4],
                                             const double Y[4], double& sx, double& sy) {
     const int a = k - 1, b = k & 3;  // nodes (k, k+1)
     if (iaxis == 1) {
@@ -177,7 +185,7 @@ __device__ __forceinline__ void face_vector(int iaxis, int k, const double X[4],
 }
 
 // Cell volume (geometry.f90:87,98,101).
-__device__ __forceinline__ double cell_volume(int iaxis, const double X[4], const double Y[4],
+TNS_HD double cell_volume(int iaxis, const double X[4], const double Y[4],
                                               double ycc) {
     double v = HALF * ((X[2] - X[0]) * (Y[3] - Y[1]) - (X[3] - X[1]) * (Y[2] - Y[0]));
     if (iaxis == 1) v = v * ycc;
@@ -190,7 +198,7 @@ __device__ __forceinline__ double cell_volume(int iaxis, const double X[4], cons
 // par: parent cell, opp: parent's neighbour across the face opposite the ghost.
 // psx, psy: parent's surface vector on the ghost side; ycc_g, ycc_p: ghost / parent
 // centroid y; gport: summed port flux (type 6 only); inj: burn-rate multiplier.
-__device__ __forceinline__ void boundary_ghost(const Params& P, int type, const Prim& par,
+TNS_HD void boundary_ghost(const Params& P, int type, const Prim& par,
                                                const Prim& opp, double psx, double psy,
                                                double ycc_g, double ycc_p, double gport,
                                                double inj, Prim& g) {

@@ -457,7 +457,10 @@ class Scheme:
             UAVG, VAVG, TAVG, RHOAVG, RAVG = AV[0], AV[1], AV[2], AV[3], AV[4]
             if flow.iaxis == 1:
                 YAVG = 0.5 * (YB + YD)
-                VBYY = torch.where(YAVG < YAXIS_THRESH, DVY, VAVG / YAVG)
+                near = YAVG < YAXIS_THRESH
+                # the unselected branch divides by YAVG = 0 on axis faces: keep its
+                # gradient finite (torch.where passes 0 * inf = NaN otherwise)
+                VBYY = torch.where(near, DVY, VAVG / torch.where(near, torch.ones_like(YAVG), YAVG))
                 DIVVEL = DUX + DVY + VBYY
             else:
                 DIVVEL = DUX + DVY
@@ -509,7 +512,8 @@ class Scheme:
         div23 = 2.0 / 3.0
         ycc = geo["yc"][1:-1, 1:-1]
         if flow.iaxis == 1:
-            vbyy = torch.where(ycc < YAXIS_THRESH, DVY, full[V_][1:-1, 1:-1] / ycc)
+            near = ycc < YAXIS_THRESH
+            vbyy = torch.where(near, DVY, full[V_][1:-1, 1:-1] / torch.where(near, torch.ones_like(ycc), ycc))
             divvel = DUX + DVY + vbyy
             pk = amut / rho * (DUX * DUX + DVY * DVY + vbyy * vbyy + DUX * DUX + DVY * DVY +
                                vbyy * vbyy + (DUY + DVX) * (DUY + DVX) - div23 * divvel * divvel)
