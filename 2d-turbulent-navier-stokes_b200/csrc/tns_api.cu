@@ -826,6 +826,7 @@ int tns_time_step_noalloc(const double* d_q, const double* d_cfldl, long long nc
 void tns_destroy(tns_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    tns_rt::adjoint_release(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     for (auto g : h->graph_mx)
         if (g) cudaGraphExecDestroy(g);

@@ -39,6 +39,8 @@ struct DevBuf {
 
 using namespace tns_rt;
 
+struct tns_adjoint_state;  // tns_adjoint.cu
+
 struct tns_handle {
     std::string err;
     Params P{};
@@ -80,6 +82,7 @@ struct tns_handle {
     double kms[K_NKERNEL] = {0};
     long long kcount[K_NKERNEL] = {0};
     long long launches = 0;
+    tns_adjoint_state* adj = nullptr;  // discrete adjoint buffers (tns_adjoint_enable)
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -105,4 +108,6 @@ namespace tns_rt {
 // state buffer A to Aout.  The batch runtime captures these per case.
 void enqueue_iteration_f64(tns_handle* h, bool monitor);
 void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout);
+// Frees the adjoint buffers of a handle (tns_adjoint.cu).
+void adjoint_release(tns_handle* h);
 }  // namespace tns_rt

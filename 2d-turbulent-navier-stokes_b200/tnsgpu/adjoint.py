@@ -711,14 +711,29 @@ class GraphedStep:
 def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, amachinit=None,
                        dy: Optional[torch.Tensor] = None, space: Optional[DesignSpace] = None,
                        niter: int = 100, states: Optional[np.ndarray] = None, primal: str = "gpu",
-                       lib=None, graph: Optional[bool] = None) -> dict:
+                       lib=None, graph: Optional[bool] = None, engine: Optional[str] = None) -> dict:
     """dJ/d(P0, T0, AMACHINIT, dy) of J = objective(scheme, Q_N, geo, prm), Q_0 the cold
     start, Q_N after ``niter`` RK4 iterations.
 
-    The primal runs on the GPU FP64 path (``primal="gpu"``) or in the restatement
-    (``"torch"``); ``states`` may pass precomputed checkpoints [N+1, 5, NELES].  The
-    backward sweep recomputes each iteration from its checkpoint inside autograd; on a
-    CUDA device that step is captured once as a CUDA graph (``graph``, default on)."""
+    ``engine="cuda"`` (the default on a CUDA device): the primal runs on the GPU FP64
+    path keeping a device checkpoint per iteration, and every reverse step is the
+    hand-written CUDA adjoint of the C ABI (tns_adjoint_step), which also accumulates the
+    sensitivities to geometry, RTOLERANCE, S0 and T0; one torch backward through
+    COMPUTE_GEOMETRY and the parameter formulas maps those to the gradient.  ``states``
+    (optional) are checkpoints [N+1, 5, NI, NJ]; the result's "states" is the device
+    tensor of checkpoints.
+
+    ``engine="torch"`` (the default on the CPU): the primal runs on the GPU FP64 path
+    (``primal="gpu"``) or in the restatement (``"torch"``); ``states`` may pass
+    precomputed checkpoints [N+1, 5, NELES].  The backward sweep recomputes each
+    iteration from its checkpoint inside autograd; on a CUDA device that step is
+    captured once as a CUDA graph (``graph``, default on)."""
+    if engine is None:
+        engine = "cuda" if scheme.device.type == "cuda" else "torch"
+    if engine == "cuda":
+        return _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib)
+    if engine != "torch":
+        raise ValueError(f"engine {engine!r}: 'cuda' or 'torch'")
     dev = scheme.device
     leaf = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev,
                                      requires_grad=True)
@@ -834,11 +849,19 @@ def objective_gpu(scheme: Scheme, objective: Callable, p0=None, t0=None, amachin
 
 
 def fixed_point_adjoint(scheme: Scheme, objective: Callable, Qstar: torch.Tensor, niter: int = 200,
-                        p0=None, t0=None, amachinit=None, dy=None, space=None) -> dict:
+                        p0=None, t0=None, amachinit=None, dy=None, space=None, engine: Optional[str] = None,
+                        lib=None) -> dict:
     """Adjoint of a steady state Q* = G(Q*, p): iterates lambda <- dJ/dQ + lambda dG/dQ
     (the RK4 iteration's transposed Jacobian at Q*) and returns dJ/dp = dJ/dp|direct +
     lambda dG/dp, with the adjoint residual history |lambda_{k+1} - lambda_k|_max.
-    Meaningful when Q* is a converged state of the primal."""
+    Meaningful when Q* is a converged state of the primal.  ``engine`` as in
+    ``transient_gradient`` (the CUDA engine applies tns_adjoint_step at Q*)."""
+    if engine is None:
+        engine = "cuda" if scheme.device.type == "cuda" else "torch"
+    if engine == "cuda":
+        return _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib)
+    if engine != "torch":
+        raise ValueError(f"engine {engine!r}: 'cuda' or 'torch'")
     dev = scheme.device
     leaf = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev,
                                      requires_grad=True)
@@ -873,6 +896,192 @@ def fixed_point_adjoint(scheme: Scheme, objective: Callable, Qstar: torch.Tensor
         grads.append(v)
     out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
            "dJ_damachinit": float(grads[2]), "residual_history": hist, "lambda": lam.detach()}
+    if dy is not None:
+        out["dJ_ddy"] = grads[3].detach().cpu().numpy()
+    return out
+
+
+# ---------------------------------------------------------------------- CUDA engine
+
+SENS_ORDER = ("sx", "sy", "vol", "dl", "xc", "yc", "x", "y", "rtolc", "rtoln", "t0", "s0")
+
+
+def split_sensitivities(sens: np.ndarray, ni: int, nj: int, device) -> Dict[str, torch.Tensor]:
+    """The accumulated sensitivities of tns_adjoint_sensitivities as the entries of
+    ``Scheme.geometry`` (sx, sy lists of 4; vol, dl [NI, NJ]; xc, yc [NI+2, NJ+2]; x, y
+    [NI+1, NJ+1]) and the scalars rtol, t0, s0."""
+    n, npad, nnode = ni * nj, (ni + 2) * (nj + 2), (ni + 1) * (nj + 1)
+    size = {"sx": 4 * n, "sy": 4 * n, "vol": n, "dl": n, "xc": npad, "yc": npad, "x": nnode, "y": nnode,
+            "rtolc": n, "rtoln": nnode, "t0": n, "s0": n}
+    t = torch.tensor(sens, dtype=torch.float64, device=device)
+    raw, o = {}, 0
+    for k in SENS_ORDER:
+        raw[k] = t[o:o + size[k]]
+        o += size[k]
+    return {"sx": [raw["sx"][k * n:(k + 1) * n].reshape(ni, nj) for k in range(4)],
+            "sy": [raw["sy"][k * n:(k + 1) * n].reshape(ni, nj) for k in range(4)],
+            "vol": raw["vol"].reshape(ni, nj), "dl": raw["dl"].reshape(ni, nj),
+            "xc": raw["xc"].reshape(ni + 2, nj + 2), "yc": raw["yc"].reshape(ni + 2, nj + 2),
+            "x": raw["x"].reshape(ni + 1, nj + 1), "y": raw["y"].reshape(ni + 1, nj + 1),
+            "rtol": raw["rtolc"].sum() + raw["rtoln"].sum(), "t0": raw["t0"].sum(), "s0": raw["s0"].sum()}
+
+
+class DeviceAdjoint:
+    """The hand-written CUDA discrete adjoint of one case (C ABI tns_adjoint_*): an FP64
+    handle for the mesh at the design point, on torch's current CUDA stream.  ``primal``
+    records device checkpoints Q_0..Q_N; ``step`` pulls lambda back through one iteration
+    in place; ``sensitivities`` returns (and clears) the accumulated lambda dG/dp."""
+
+    def __init__(self, scheme: Scheme, space: DesignSpace, prm: Params, dy, lib=None):
+        from .solver import Solver
+        self.scheme = scheme
+        with torch.no_grad():
+            mesh_now = _mesh_with_coords(scheme, space, dy)
+            f = dataclasses.replace(scheme.flow, p0=float(prm.p0), t0=float(prm.t0),
+                                    amachinit=float(prm.amachinit))
+            rinit = float(scheme.rtol(prm) / scheme.flow.rtred)
+        self.solver = Solver(mesh_now, f, rinit, precision=0, lib=lib)
+        self.solver.set_stream(torch.cuda.current_stream(scheme.device).cuda_stream)
+        self.solver._check(self.solver.L.tns_adjoint_enable(self.solver.h))
+
+    def primal(self, c0: torch.Tensor, niter: int) -> torch.Tensor:
+        """Checkpoints [niter+1, 5, NI, NJ] on the device from Q_0 = c0."""
+        states = torch.empty((niter + 1,) + tuple(c0.shape), dtype=torch.float64, device=self.scheme.device)
+        states[0].copy_(c0)
+        self.solver.state_from_device(states[0].data_ptr())
+        for n in range(niter):
+            self.solver.enqueue(1)
+            self.solver.state_to_device(states[n + 1].data_ptr())
+        self.solver.synchronize()
+        return states
+
+    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool):
+        if not (q.is_contiguous() and lam.is_contiguous() and lam.dtype == torch.float64
+                and q.dtype == torch.float64):
+            raise ValueError("q and lambda must be contiguous float64 device tensors")
+        self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities)
+
+    def sensitivities(self) -> Dict[str, torch.Tensor]:
+        s = self.solver.adjoint_sensitivities(reset=True)
+        return split_sensitivities(s, self.scheme.ni, self.scheme.nj, self.scheme.device)
+
+    def close(self):
+        self.solver.close()
+
+
+def _parameter_gradient(scheme: Scheme, space: DesignSpace, params: List[torch.Tensor], dy,
+                        sens: Dict[str, torch.Tensor], lam0: Optional[torch.Tensor]) -> List[torch.Tensor]:
+    """lambda dG/dp summed over the reverse steps (``sens``) plus lambda_0 dQ_0/dp, mapped
+    to the parameters by one backward through COMPUTE_GEOMETRY, RTOLERANCE(P0, T0,
+    AMACHINIT), S0(P0, T0) and the cold start."""
+    prm = Params(params[0], params[1], params[2], scheme.flow)
+    x, y = space.coords(dy)
+    geo = scheme.geometry(x, y)
+    outs, gos = [], []
+
+    def add(t, g):
+        if isinstance(t, torch.Tensor) and t.requires_grad:
+            outs.append(t)
+            gos.append(g)
+
+    for k in ("x", "y", "xc", "yc", "dl", "vol"):
+        add(geo[k], sens[k])
+    for k in range(4):
+        add(geo["sx"][k], sens["sx"][k])
+        add(geo["sy"][k], sens["sy"][k])
+    add(scheme.rtol(prm), sens["rtol"])
+    add(prm.s0(), sens["s0"])
+    add(prm.t0, sens["t0"])
+    if lam0 is not None:
+        add(scheme.cold_state(prm), lam0)
+    g = torch.autograd.grad(outs, params, grad_outputs=gos, allow_unused=True)
+    return [v if v is not None else torch.zeros_like(p) for v, p in zip(g, params)]
+
+
+def _leaves(scheme, p0, t0, amachinit, dy):
+    dev = scheme.device
+    leaf = lambda v, d: torch.tensor(float(d if v is None else v), dtype=torch.float64, device=dev,
+                                     requires_grad=True)
+    P0, T0, AM = leaf(p0, scheme.flow.p0), leaf(t0, scheme.flow.t0), leaf(amachinit, scheme.flow.amachinit)
+    if dy is not None:
+        dy = dy.detach().clone().to(dev).requires_grad_(True)
+    return [P0, T0, AM] + ([dy] if dy is not None else []), dy
+
+
+def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib) -> dict:
+    if scheme.device.type != "cuda":
+        raise ValueError("engine='cuda' needs a Scheme on a CUDA device")
+    params, dy = _leaves(scheme, p0, t0, amachinit, dy)
+    space = space or DesignSpace(scheme)
+    ni, nj = scheme.ni, scheme.nj
+    prm = Params(params[0], params[1], params[2], scheme.flow)
+    with torch.no_grad():
+        c0 = scheme.cold_state(prm).contiguous()
+    dev_adj = DeviceAdjoint(scheme, space, prm, dy, lib)
+    try:
+        if states is None:
+            st = dev_adj.primal(c0, niter)
+        elif isinstance(states, torch.Tensor):
+            st = states.to(scheme.device, torch.float64).reshape(niter + 1, 5, ni, nj).contiguous()
+        else:
+            st = torch.tensor(np.asarray(states).reshape(niter + 1, 5, ni, nj), device=scheme.device)
+        # dJ/dQ_N and the direct dependence of J on the parameters
+        QN = st[niter].clone().requires_grad_(True)
+        x, y = space.coords(dy)
+        J = objective(scheme, QN, scheme.geometry(x, y), prm)
+        g = torch.autograd.grad(J, [QN] + params, allow_unused=True)
+        grads = [v.detach() if v is not None else torch.zeros_like(p) for v, p in zip(g[1:], params)]
+        lam = g[0].detach().contiguous()
+        for n in range(niter - 1, -1, -1):
+            dev_adj.step(st[n], lam, True)
+        sens = dev_adj.sensitivities()
+    finally:
+        dev_adj.close()
+    gp = _parameter_gradient(scheme, space, params, dy, sens, lam)
+    grads = [a + b for a, b in zip(grads, gp)]
+    out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
+           "dJ_damachinit": float(grads[2]), "lambda0": lam, "states": st}
+    if dy is not None:
+        out["dJ_ddy"] = grads[3].detach().cpu().numpy()
+    return out
+
+
+def _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib) -> dict:
+    if scheme.device.type != "cuda":
+        raise ValueError("engine='cuda' needs a Scheme on a CUDA device")
+    params, dy = _leaves(scheme, p0, t0, amachinit, dy)
+    space = space or DesignSpace(scheme)
+    prm = Params(params[0], params[1], params[2], scheme.flow)
+    Q = Qstar.detach().to(scheme.device, torch.float64).contiguous().requires_grad_(True)
+    x, y = space.coords(dy)
+    J = objective(scheme, Q, scheme.geometry(x, y), prm)
+    gJ = torch.autograd.grad(J, [Q] + params, allow_unused=True)
+    djdq = gJ[0].detach().contiguous()
+    q = Q.detach()
+    dev_adj = DeviceAdjoint(scheme, space, prm, dy, lib)
+    hist = []
+    try:
+        lam = djdq.clone()
+        for _ in range(niter):
+            vj = lam.clone()
+            dev_adj.step(q, vj, False)
+            new = djdq + vj
+            hist.append(float(torch.max(torch.abs(new - lam))))
+            lam = new
+        last = lam.clone()
+        dev_adj.step(q, last, True)  # lambda dG/dp at Q*
+        sens = dev_adj.sensitivities()
+    finally:
+        dev_adj.close()
+    gp = _parameter_gradient(scheme, space, params, dy, sens, None)
+    grads = []
+    for k, p in enumerate(params):
+        v = gp[k]
+        if gJ[k + 1] is not None:
+            v = v + gJ[k + 1]
+        grads.append(v)
+    out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
+           "dJ_damachinit": float(grads[2]), "residual_history": hist, "lambda": lam}
     if dy is not None:
         out["dJ_ddy"] = grads[3].detach().cpu().numpy()
     return out

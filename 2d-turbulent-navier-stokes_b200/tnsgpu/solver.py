@@ -134,6 +134,30 @@ class Solver:
         self._check(self.L.tns_debug_fetch(self.h, int(which), out.ctypes.data))
         return out
 
+    # -- device-resident state and the discrete adjoint (FP64 handles, (i, j) numbering)
+    def state_to_device(self, ptr: int):
+        """Copies the state to device memory at ``ptr`` ([5][NELES] doubles), async."""
+        self._check(self.L.tns_copy_state_device(self.h, C.c_void_p(int(ptr)), 0))
+
+    def state_from_device(self, ptr: int):
+        """Loads the state from device memory at ``ptr`` ([5][NELES] doubles), async."""
+        self._check(self.L.tns_copy_state_device(self.h, C.c_void_p(int(ptr)), 1))
+
+    def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities: bool = False):
+        """lambda <- lambda dG/dQ_n for the iteration from Q_n (both device pointers);
+        with ``sensitivities`` also accumulates lambda dG/dp (tns_adjoint_step)."""
+        self._check(self.L.tns_adjoint_step(self.h, C.c_void_p(int(q_ptr)), C.c_void_p(int(lam_ptr)),
+                                            1 if sensitivities else 0))
+
+    def adjoint_sensitivities(self, reset: bool = True) -> np.ndarray:
+        n = int(self.L.tns_adjoint_sensitivity_size(self.h))
+        out = np.zeros(n)
+        self._check(self.L.tns_adjoint_sensitivities(self.h, out.ctypes.data, n, 1 if reset else 0))
+        return out
+
+    def adjoint_launch_count(self) -> int:
+        return int(self.L.tns_adjoint_launch_count(self.h))
+
     def set_stream(self, stream_ptr: Optional[int]):
         self._check(self.L.tns_set_stream(self.h, stream_ptr))
 

@@ -166,6 +166,36 @@ int tns_time_step_noalloc(const double *d_q, const double *d_cfldl, long long nc
                           const tns_params *params, double *d_dt, double *d_dtmin, void *stream);
 void tns_destroy(tns_handle *h);
 
+/* ---- Discrete adjoint of one FP64 RK4 iteration (no counterpart in the reference,
+ * which has no adjoint).  For the iteration map Q_{n+1} = G(Q_n) of
+ * turbnstwod.f90:95-146 -- DT, DISSIPATION, and four stages of PRIMITIVE_VARS,
+ * APPLY_BOUNDARY (types 2-5), VISCOUS (stage 1), SOURCE_TERMS, RESIDUAL, UPDATE --
+ * tns_adjoint_step replaces lambda = dJ/dQ_{n+1} by lambda dG/dQ_n, recomputing the
+ * iteration from the checkpoint Q_n on the device.  Non-smooth points (DMAX1 / DMIN1,
+ * |x|, the C5 clip, the sensor maxima) take the branch the forward took.  With
+ * TNS_ADJ_SENSITIVITIES it also accumulates lambda dG/dp, summed over calls, for:
+ *   SX(4), SY(4) per cell (face vectors), VOL, DL per cell, the centroids of the cells
+ *   and ghosts on the (NI+2) x (NJ+2) halo grid (x then y), the node coordinates (x then
+ *   y), RTOLERANCE (per cell, per node: sum them), T0 and S0 of the type-2 inlet (per
+ *   cell: sum them)
+ * in that order (tns_adjoint_sensitivity_size values), which a caller maps to node
+ * displacements and flow parameters with the derivatives of COMPUTE_GEOMETRY and of its
+ * parameter formulas.  Requirements: an FP64 handle, cells numbered in (i, j) order
+ * (faces 1..4 = j-, i+, j+, i-), at least 3 x 3 cells, BC types 2-5.  Device arrays are
+ * [5][NELES] component-major in that order; calls are asynchronous on the handle's
+ * stream (tns_set_stream). */
+#define TNS_ADJ_SENSITIVITIES 1
+int tns_adjoint_enable(tns_handle *h);
+int tns_adjoint_step(tns_handle *h, const double *d_q, double *d_lam, int flags);
+long long tns_adjoint_sensitivity_size(tns_handle *h);
+/* Copies the accumulated sensitivities to host memory `out` (count values, which must
+ * equal tns_adjoint_sensitivity_size) and, with reset != 0, zeroes them. */
+int tns_adjoint_sensitivities(tns_handle *h, double *out, long long count, int reset);
+long long tns_adjoint_launch_count(tns_handle *h);
+/* Device-to-device copy of the FP64 state: direction 0 copies it to d_buf, 1 loads it
+ * from d_buf ([5][NELES], (i, j) numbering).  For checkpointing on the device. */
+int tns_copy_state_device(tns_handle *h, double *d_buf, int direction);
+
 /* ---- Batch of cases (no counterpart in the reference, which solves one case per run).
  * A batch advances several handles made by tns_create together: every kernel phase of
  * an RK4 iteration is one launch over the tiles of all active cases.  The cases may

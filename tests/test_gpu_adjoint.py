@@ -1,6 +1,7 @@
 """Discrete adjoint on the GPU: the differentiable restatement (torch FP64 on cuda)
-against the CUDA FP64 path, and gradients whose primal runs through the C ABI against
-central finite differences of that same GPU path."""
+against the CUDA FP64 path; the hand-written CUDA adjoint (tns_adjoint_step, the
+default engine on a GPU) against autograd of the restatement, step by step and over a
+transient; and its gradients against central finite differences of the GPU FP64 path."""
 import numpy as np
 import pytest
 import torch
@@ -86,12 +87,118 @@ def test_graphed_reverse_step_equals_eager():
     mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
     dy = torch.zeros(1, dtype=torch.float64)
     a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
-                                   graph=True)
+                                   graph=True, engine="torch")
     b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
-                                   states=a["states"], graph=False)
+                                   states=a["states"], graph=False, engine="torch")
     for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
         assert abs(a[k] - b[k]) <= 1e-12 * abs(b[k]), (k, a[k], b[k])
     assert abs(a["dJ_ddy"][0] - b["dJ_ddy"][0]) <= 1e-12 * abs(b["dJ_ddy"][0])
     # index_add sums node averages with atomics: compare the adjoint state in max norm
     err = torch.max(torch.abs(a["lambda0"] - b["lambda0"])) / torch.max(torch.abs(b["lambda0"]))
     assert float(err) < 1e-12, float(err)
+
+
+def _axis_sym(mesh):
+    mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    return mesh
+
+
+STEP_CASES = {
+    "ramp": lambda: (cases.ramp_mesh(64, 24), cases.ramp_flow()),
+    "plume_axis": lambda: (_axis_sym(cases.nozzle_plume_mesh(64, 24)), cases.nozzle_plume_flow()),
+    "plume_wall_axis": lambda: (cases.nozzle_plume_mesh(48, 20), cases.nozzle_plume_flow()),
+    "global_dt": lambda: (cases.ramp_mesh(40, 16),
+                          formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
+}
+
+
+@pytest.mark.parametrize("name", sorted(STEP_CASES))
+def test_cuda_adjoint_step_matches_autograd(name):
+    """One reverse step of the CUDA adjoint against torch.autograd of the restatement on
+    a developed state; the parameter sensitivities through the gradient they give."""
+    mesh, flow = STEP_CASES[name]()
+    rinit = formats.rinit_cold(flow)
+    sch = adjoint.Scheme(mesh, flow, device="cuda", rinit=rinit)
+    space = adjoint.DesignSpace(sch)
+    c0 = formats.cold_state(flow, mesh.neles, rinit)
+    rng = np.random.default_rng(3)
+    c0 = c0 * (1 + 2e-2 * rng.uniform(-1, 1, c0.shape))
+    c0[2] = 0.05 * c0[1] * rng.uniform(-1, 1, mesh.neles)
+    prm0, geo0 = sch.params(), sch.geometry(sch.x0, sch.y0)
+    C = torch.tensor(c0.reshape(5, *mesh.shape), device="cuda")
+    with torch.no_grad():
+        for _ in range(30):
+            C = sch.iteration(C, geo0, prm0)
+    lam = torch.tensor(rng.normal(size=(5,) + mesh.shape), device="cuda")
+    params, _ = adjoint._leaves(sch, None, None, None, None)
+    prm = adjoint.Params(params[0], params[1], params[2], flow)
+    Q = C.clone().requires_grad_(True)
+    G = sch.iteration(Q, sch.geometry(sch.x0, sch.y0), prm)
+    ref = torch.autograd.grad(G, [Q] + params, grad_outputs=lam, allow_unused=True)
+    dev = adjoint.DeviceAdjoint(sch, space, prm, None)
+    try:
+        got = lam.clone().contiguous()
+        dev.step(C.contiguous(), got, True)
+        sens = dev.sensitivities()
+        launches = dev.solver.adjoint_launch_count()
+    finally:
+        dev.close()
+    assert launches > 20
+    err = torch.amax(torch.abs(got - ref[0]), dim=(1, 2)) / torch.amax(torch.abs(ref[0]), dim=(1, 2))
+    assert float(err.max()) < 1e-10, err
+    gp = adjoint._parameter_gradient(sch, space, params, None, sens, None)
+    for k in range(3):
+        r = float(ref[k + 1]) if ref[k + 1] is not None else 0.0
+        assert abs(float(gp[k]) - r) <= 1e-9 * max(abs(r), 1e-300), (k, float(gp[k]), r)
+
+
+def test_cuda_engine_transient_gradient_matches_torch_engine():
+    mesh, flow, sch, space = _ramp(64, 24, wall=(40, 46, 52))
+    dy = torch.tensor([1e-5, -2e-5, 5e-6], dtype=torch.float64)
+    N = 30
+    a = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=dy, space=space, niter=N,
+                                   engine="cuda")
+    b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=dy, space=space, niter=N,
+                                   engine="torch", states=a["states"].reshape(N + 1, 5, -1).cpu().numpy())
+    assert abs(a["J"] - b["J"]) <= 1e-13 * abs(b["J"])
+    for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
+        assert abs(a[k] - b[k]) <= 1e-9 * abs(b[k]), (k, a[k], b[k])
+    assert np.allclose(a["dJ_ddy"], b["dJ_ddy"], rtol=1e-9, atol=1e-9 * np.max(np.abs(b["dJ_ddy"])))
+    err = torch.max(torch.abs(a["lambda0"] - b["lambda0"])) / torch.max(torch.abs(b["lambda0"]))
+    assert float(err) < 1e-10, float(err)
+
+
+def test_cuda_fixed_point_adjoint_matches_torch_engine():
+    mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
+    s = Solver(mesh, flow, float(sch.rtol(sch.params()) / flow.rtred), precision=0)
+    s.upload(sch.cold_state(sch.params()).reshape(5, -1).cpu().numpy())
+    s.run(200, 0)
+    qstar = torch.tensor(s.download().reshape(5, *mesh.shape), device="cuda")
+    s.close()
+    dy = torch.zeros(1, dtype=torch.float64)
+    a = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space,
+                                    engine="cuda")
+    b = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space,
+                                    engine="torch")
+    assert np.allclose(a["residual_history"], b["residual_history"], rtol=1e-8)
+    for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
+        assert abs(a[k] - b[k]) <= 1e-9 * abs(b[k]), (k, a[k], b[k])
+    assert abs(a["dJ_ddy"][0] - b["dJ_ddy"][0]) <= 1e-9 * abs(b["dJ_ddy"][0])
+
+
+def test_cuda_adjoint_step_is_deterministic():
+    mesh, flow, sch, space = _ramp(64, 24)
+    prm = sch.params()
+    dev = adjoint.DeviceAdjoint(sch, space, prm, None)
+    try:
+        st = dev.primal(sch.cold_state(prm).contiguous(), 12)
+        lam0 = torch.tensor(np.random.default_rng(5).normal(size=(5,) + mesh.shape), device="cuda")
+        outs = []
+        for _ in range(2):
+            lam = lam0.clone()
+            for n in range(11, -1, -1):
+                dev.step(st[n], lam, True)
+            outs.append((lam, dev.sensitivities()["vol"]))
+    finally:
+        dev.close()
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
