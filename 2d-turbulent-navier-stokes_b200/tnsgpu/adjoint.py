@@ -928,9 +928,13 @@ def split_sensitivities(sens: np.ndarray, ni: int, nj: int, device) -> Dict[str,
 
 class DeviceAdjoint:
     """The hand-written CUDA discrete adjoint of one case (C ABI tns_adjoint_*): an FP64
-    handle for the mesh at the design point, on torch's current CUDA stream.  ``primal``
-    records device checkpoints Q_0..Q_N; ``step`` pulls lambda back through one iteration
-    in place; ``sensitivities`` returns (and clears) the accumulated lambda dG/dp."""
+    handle for the mesh at the design point.  ``primal`` records device checkpoints
+    Q_0..Q_N; ``step`` pulls lambda back through one iteration in place;
+    ``sensitivities`` returns (and clears) the accumulated lambda dG/dp.
+
+    The handle runs on a stream of its own (``stream``; the graph-captured step cannot
+    run on the legacy default stream), ordered after torch's current stream on entry to
+    each call and before it on exit, so callers use the tensors as usual."""
 
     def __init__(self, scheme: Scheme, space: DesignSpace, prm: Params, dy, lib=None):
         from .solver import Solver
@@ -941,25 +945,36 @@ class DeviceAdjoint:
                                     amachinit=float(prm.amachinit))
             rinit = float(scheme.rtol(prm) / scheme.flow.rtred)
         self.solver = Solver(mesh_now, f, rinit, precision=0, lib=lib)
-        self.solver.set_stream(torch.cuda.current_stream(scheme.device).cuda_stream)
+        self.stream = torch.cuda.Stream(device=scheme.device)
+        self.solver.set_stream(self.stream.cuda_stream)
         self.solver._check(self.solver.L.tns_adjoint_enable(self.solver.h))
+
+    def _enter(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.scheme.device))
+
+    def _leave(self):
+        torch.cuda.current_stream(self.scheme.device).wait_stream(self.stream)
 
     def primal(self, c0: torch.Tensor, niter: int) -> torch.Tensor:
         """Checkpoints [niter+1, 5, NI, NJ] on the device from Q_0 = c0."""
         states = torch.empty((niter + 1,) + tuple(c0.shape), dtype=torch.float64, device=self.scheme.device)
         states[0].copy_(c0)
+        self._enter()
         self.solver.state_from_device(states[0].data_ptr())
         for n in range(niter):
             self.solver.enqueue(1)
             self.solver.state_to_device(states[n + 1].data_ptr())
         self.solver.synchronize()
+        self._leave()
         return states
 
     def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool):
         if not (q.is_contiguous() and lam.is_contiguous() and lam.dtype == torch.float64
                 and q.dtype == torch.float64):
             raise ValueError("q and lambda must be contiguous float64 device tensors")
+        self._enter()
         self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities)
+        self._leave()
 
     def sensitivities(self) -> Dict[str, torch.Tensor]:
         s = self.solver.adjoint_sensitivities(reset=True)

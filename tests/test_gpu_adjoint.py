@@ -156,13 +156,16 @@ def test_cuda_engine_transient_gradient_matches_torch_engine():
     mesh, flow, sch, space = _ramp(64, 24, wall=(40, 46, 52))
     dy = torch.tensor([1e-5, -2e-5, 5e-6], dtype=torch.float64)
     N = 30
-    a = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=dy, space=space, niter=N,
+    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
                                    engine="cuda")
-    b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=dy, space=space, niter=N,
+    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
                                    engine="torch", states=a["states"].reshape(N + 1, 5, -1).cpu().numpy())
     assert abs(a["J"] - b["J"]) <= 1e-13 * abs(b["J"])
-    for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
-        assert abs(a[k] - b[k]) <= 1e-9 * abs(b[k]), (k, a[k], b[k])
+    # tolerance on each derivative: 1e-9 of itself or of its natural scale |J| / |p|
+    # (a derivative that nearly cancels is compared at the scale of its terms)
+    for k, p in (("dJ_dp0", flow.p0), ("dJ_dt0", flow.t0), ("dJ_damachinit", flow.amachinit)):
+        tol = 1e-9 * max(abs(b[k]), abs(b["J"]) / p)
+        assert abs(a[k] - b[k]) <= tol, (k, a[k], b[k])
     assert np.allclose(a["dJ_ddy"], b["dJ_ddy"], rtol=1e-9, atol=1e-9 * np.max(np.abs(b["dJ_ddy"])))
     err = torch.max(torch.abs(a["lambda0"] - b["lambda0"])) / torch.max(torch.abs(b["lambda0"]))
     assert float(err) < 1e-10, float(err)
@@ -181,8 +184,9 @@ def test_cuda_fixed_point_adjoint_matches_torch_engine():
     b = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space,
                                     engine="torch")
     assert np.allclose(a["residual_history"], b["residual_history"], rtol=1e-8)
-    for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
-        assert abs(a[k] - b[k]) <= 1e-9 * abs(b[k]), (k, a[k], b[k])
+    for k, p in (("dJ_dp0", flow.p0), ("dJ_dt0", flow.t0), ("dJ_damachinit", flow.amachinit)):
+        tol = 1e-9 * max(abs(b[k]), abs(b["J"]) / p)
+        assert abs(a[k] - b[k]) <= tol, (k, a[k], b[k])
     assert abs(a["dJ_ddy"][0] - b["dJ_ddy"][0]) <= 1e-9 * abs(b["dJ_ddy"][0])
 
 
