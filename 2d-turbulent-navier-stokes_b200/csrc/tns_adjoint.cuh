@@ -9,6 +9,7 @@
 //
 //   stage update + clip        residual.f90:67-83        (s1_point)
 //   central flux residual      residual.f90:23-62        (s1_point, s3_point)
+//   ghost back-propagation     boundary.f90:53-122       (s3g_point)
 //   source terms               source_terms.f90:24-104   (src_forward / src_reverse)
 //   primitive variables        turbnstwod.f90:204-227    (prim_adj)
 //   ghost states 2..5          boundary.f90:53-122       (ghost_adj)
@@ -193,9 +194,10 @@ TNS_HD void s0_point(const AdjArgs& a, long long ps) {
 // Reverse of COMPUTE_PRIMITIVE_VARS (turbnstwod.f90:204-227) for one cell: the adjoint
 // of its field-set rows wb -> the adjoint of its conservative state qb (added).
 TNS_HD void prim_adj(const Params& P, const double q[5], const double wb[NWROW], double qb[5]) {
-    const double rho = q[0], u = q[1] / rho, v = q[2] / rho, e = q[3] / rho;
-    const double t = (e - 0.5 * (u * u + v * v)) / P.cv;
-    const double p = rho * P.rr * t, rt = q[4] / rho;
+    const double irho = 1.0 / q[0];
+    const double rho = q[0], u = q[1] * irho, v = q[2] * irho, e = q[3] * irho;
+    const double t = (e - 0.5 * (u * u + v * v)) * P.inv_cv;
+    const double p = rho * P.rr * t, rt = q[4] * irho;
     double b[5];
     for (int m = 0; m < 5; m++) b[m] = wb[WC1 + m];
     b[1] += wb[WF + 0];
@@ -209,17 +211,14 @@ TNS_HD void prim_adj(const Params& P, const double q[5], const double wb[NWROW],
     const double rtb = wb[WF + 4] * rho * u + wb[WG + 4] * rho * v;
     rhob += pb * P.rr * t;
     const double tb = wb[WT] + pb * rho * P.rr;
-    const double eb = tb / P.cv;
-    ub -= tb * u / P.cv;
-    vb -= tb * v / P.cv;
-    b[4] += rtb / rho;
-    rhob -= rtb * rt / rho;
-    b[3] += eb / rho;
-    rhob -= eb * e / rho;
-    b[1] += ub / rho;
-    rhob -= ub * u / rho;
-    b[2] += vb / rho;
-    rhob -= vb * v / rho;
+    const double eb = tb * P.inv_cv;
+    ub -= eb * u;
+    vb -= eb * v;
+    b[4] += rtb * irho;
+    b[3] += eb * irho;
+    b[1] += ub * irho;
+    b[2] += vb * irho;
+    rhob -= (rtb * rt + eb * e + ub * u + vb * v) * irho;
     b[0] += rhob;
     for (int m = 0; m < 5; m++) qb[m] += b[m];
 }
@@ -329,9 +328,10 @@ TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const d
 struct SrcWork {
     double dnr, yBD, yAC, xBD, xAC;
     double da[4], db[4];  // q r u v: A-C and B-D differences
+    double ic1[4];        // 1 / C1 of the neighbours
     double GX[4], GY[4];  // DQX DRX DUX DVX / DQY DRY DUY DVY
     double rho, ri, amu, chi, ta, tb, fmu, sc, t1, t2, fr2, amut, dee, vbyy, divvel, sum, aor, pk, ratio, pw,
-        x, sq, A5, s3, s5, ycc, den, T;
+        x, sq, A5, s3, s5, ycc, den, T, idnr, irho, ia, itb, it2, iycc;
     bool pos, near, pkpos, selm;
 };
 
@@ -342,7 +342,8 @@ TNS_HD void src_forward(const Params& P, const double nb[4][4], const double nx[
     double f[4][4];  // q r u v per neighbour
     for (int k = 0; k < 4; k++) {
         f[0][k] = sqrt(nb[k][0] * nb[k][0] + nb[k][1] * nb[k][1]);
-        f[1][k] = nb[k][3] / nb[k][2];
+        s.ic1[k] = 1.0 / nb[k][2];
+        f[1][k] = nb[k][3] * s.ic1[k];
         f[2][k] = nb[k][0];
         f[3][k] = nb[k][1];
     }
@@ -351,36 +352,42 @@ TNS_HD void src_forward(const Params& P, const double nb[4][4], const double nx[
     s.xBD = nx[1] - nx[3];
     s.xAC = nx[0] - nx[2];
     s.dnr = s.xAC * s.yBD - s.xBD * s.yAC;
+    s.idnr = 1.0 / s.dnr;
     for (int q = 0; q < 4; q++) {
         s.da[q] = f[q][0] - f[q][2];
         s.db[q] = f[q][1] - f[q][3];
-        s.GX[q] = (s.da[q] * s.yBD - s.db[q] * s.yAC) / s.dnr;
-        s.GY[q] = (-s.da[q] * s.xBD + s.db[q] * s.xAC) / s.dnr;
+        s.GX[q] = (s.da[q] * s.yBD - s.db[q] * s.yAC) * s.idnr;
+        s.GY[q] = (-s.da[q] * s.xBD + s.db[q] * s.xAC) * s.idnr;
     }
     const double DQX = s.GX[0], DRX = s.GX[1], DUX = s.GX[2], DVX = s.GX[3];
     const double DQY = s.GY[0], DRY = s.GY[1], DUY = s.GY[2], DVY = s.GY[3];
     s.rho = rho;
     s.T = T;
-    s.ri = c5 / rho;
+    s.irho = 1.0 / rho;
+    s.ri = c5 * s.irho;
     s.amu = amu_of(P, T);
-    s.chi = rho * s.ri / (CMU * s.amu);
+    s.ia = 1.0 / (CMU * s.amu);
+    s.chi = rho * s.ri * s.ia;
     const double X2 = s.chi * s.chi;
     s.ta = tanh(ALPHA_T * X2);
     s.tb = tanh(BETA_T * X2);
-    s.fmu = s.ta / s.tb;
+    s.itb = 1.0 / s.tb;
+    s.fmu = s.ta * s.itb;
     s.sc = sqrt(s.chi);
     s.t1 = tanh(s.sc);
     s.t2 = tanh(s.chi * P.fr2k);
-    s.fr2 = s.t1 / s.t2;
+    s.it2 = 1.0 / s.t2;
+    s.fr2 = s.t1 * s.it2;
     s.amut = s.fmu * rho * s.ri;
     const double phi = DQX * DRX + DQY * DRY;
     s.pos = phi > 0.0;
     s.dee = s.pos ? DRX * DRX + DRY * DRY : 0.0;
     s.ycc = ycc;
+    s.iycc = 1.0 / ycc;
     s.near = ycc < YAXIS_THRESH;
     const double sxy = DUY + DVX;
     if (P.iaxis == 1) {
-        s.vbyy = s.near ? DVY : Vc / ycc;
+        s.vbyy = s.near ? DVY : Vc * s.iycc;
         s.divvel = DUX + DVY + s.vbyy;
         s.sum = DUX * DUX + DVY * DVY + s.vbyy * s.vbyy + DUX * DUX + DVY * DVY + s.vbyy * s.vbyy + sxy * sxy -
                 P.div23 * s.divvel * s.divvel;
@@ -389,14 +396,14 @@ TNS_HD void src_forward(const Params& P, const double nb[4][4], const double nx[
         s.divvel = DUX + DVY;
         s.sum = DUX * DUX + DVY * DVY + DUX * DUX + DVY * DVY + sxy * sxy - P.div23 * s.divvel * s.divvel;
     }
-    s.aor = s.amut / rho;
+    s.aor = s.amut * s.irho;
     const double pk0 = s.aor * s.sum;
     s.pkpos = pk0 >= 0.0;
     s.pk = s.pkpos ? pk0 : 0.0;
     const double thr = AMU_THRESH * s.amu;
     s.selm = s.amut >= thr;
     s.den = s.selm ? s.amut : thr;
-    s.ratio = s.amut / s.den;
+    s.ratio = s.selm ? 1.0 : s.amut / s.den;  // x / x = 1 exactly
     s.pw = powi(s.ratio, P.npseudo);
     s.x = s.ri * s.pk;
     s.sq = s.x > 0.0 ? sqrt(s.x) : 0.0;
@@ -405,7 +412,7 @@ TNS_HD void src_forward(const Params& P, const double nb[4][4], const double nx[
     s.s3 = 0.0;
     if (P.iaxis == 1) {
         const double ttt = (s.amu + s.amut) * (s.vbyy + s.vbyy - P.div23 * s.divvel);
-        s.s3 = (Pc - ttt) / ycc;
+        s.s3 = (Pc - ttt) * s.iycc;
     }
 }
 
@@ -430,9 +437,9 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
     rib += xb * s.pk;
     const double pkb = xb * s.ri;
     if (P.iaxis == 1) {
-        b.p = s3b / s.ycc;
-        const double tttb = -s3b / s.ycc;
-        b.ycc -= s3b * s.s3 / s.ycc;
+        b.p = s3b * s.iycc;
+        const double tttb = -b.p;
+        b.ycc -= s3b * s.s3 * s.iycc;
         const double fac = s.vbyy + s.vbyy - P.div23 * s.divvel;
         amub += tttb * fac;
         amutb += tttb * fac;
@@ -441,8 +448,8 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
     }
     const double pk0b = s.pkpos ? pkb : 0.0;
     const double aorb = pk0b * s.sum, sumb = pk0b * s.aor;
-    amutb += aorb / s.rho;
-    rhob -= aorb * s.aor / s.rho;
+    amutb += aorb * s.irho;
+    rhob -= aorb * s.aor * s.irho;
     const double DUX = s.GX[2], DVX = s.GX[3], DRX = s.GX[1], DUY = s.GY[2], DVY = s.GY[3], DRY = s.GY[1];
     const double sxy = DUY + DVX;
     GXb[2] += sumb * 4.0 * DUX;
@@ -458,8 +465,8 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
         if (s.near) {
             GYb[3] += vbyyb;
         } else {
-            b.v = vbyyb / s.ycc;
-            b.ycc -= vbyyb * s.vbyy / s.ycc;
+            b.v = vbyyb * s.iycc;
+            b.ycc -= vbyyb * s.vbyy * s.iycc;
         }
     }
     if (s.pos) {
@@ -478,14 +485,14 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
     const double fmub = amutb * s.rho * s.ri;
     rhob += amutb * s.fmu * s.ri;
     rib += amutb * s.fmu * s.rho;
-    chib += fmub * (ALPHA_T * (1.0 - s.ta * s.ta) - s.fmu * BETA_T * (1.0 - s.tb * s.tb)) / s.tb * 2.0 * s.chi;
-    chib += fr2b * (((1.0 - s.t1 * s.t1) * 0.5 / s.sc) / s.t2 - s.fr2 * (1.0 - s.t2 * s.t2) * P.fr2k / s.t2);
-    rhob += chib * s.ri / (CMU * s.amu);
-    rib += chib * s.rho / (CMU * s.amu);
-    amub -= chib * s.chi / s.amu;
+    chib += fmub * (ALPHA_T * (1.0 - s.ta * s.ta) - s.fmu * BETA_T * (1.0 - s.tb * s.tb)) * s.itb * 2.0 * s.chi;
+    chib += fr2b * ((1.0 - s.t1 * s.t1) * 0.5 / s.sc - s.fr2 * (1.0 - s.t2 * s.t2) * P.fr2k) * s.it2;
+    rhob += chib * s.ri * s.ia;
+    rib += chib * s.rho * s.ia;
+    amub -= chib * s.chi * s.ia * CMU;
     b.t = amub * 0.6 * s.amu / s.T;  // AMU = SUTH sqrt(AMOL) T**0.6
-    b.c5 = rib / s.rho;
-    rhob -= rib * s.ri / s.rho;
+    b.c5 = rib * s.irho;
+    rhob -= rib * s.ri * s.irho;
     b.c1 = rhob;
     // gradients of q r u v (q only enters the switch PHI > 0: no derivative)
     double dnrb = 0.0, xACb = 0.0, xBDb = 0.0, yACb = 0.0, yBDb = 0.0;
@@ -495,17 +502,17 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
     for (int q = 1; q < 4; q++) {
         const double gx = GXb[q], gy = GYb[q];
         if (gx == 0.0 && gy == 0.0) continue;
-        const double dab = (gx * s.yBD - gy * s.xBD) / s.dnr;
-        const double dbb = (-gx * s.yAC + gy * s.xAC) / s.dnr;
+        const double dab = (gx * s.yBD - gy * s.xBD) * s.idnr;
+        const double dbb = (-gx * s.yAC + gy * s.xAC) * s.idnr;
         fb[q][0] += dab;
         fb[q][2] -= dab;
         fb[q][1] += dbb;
         fb[q][3] -= dbb;
-        yBDb += gx * s.da[q] / s.dnr;
-        yACb -= gx * s.db[q] / s.dnr;
-        xBDb -= gy * s.da[q] / s.dnr;
-        xACb += gy * s.db[q] / s.dnr;
-        dnrb -= (gx * s.GX[q] + gy * s.GY[q]) / s.dnr;
+        yBDb += gx * s.da[q] * s.idnr;
+        yACb -= gx * s.db[q] * s.idnr;
+        xBDb -= gy * s.da[q] * s.idnr;
+        xACb += gy * s.db[q] * s.idnr;
+        dnrb -= (gx * s.GX[q] + gy * s.GY[q]) * s.idnr;
     }
     xACb += dnrb * s.yBD;
     yBDb += dnrb * s.xAC;
@@ -514,11 +521,11 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
     b.nx[0] = xACb; b.nx[2] = -xACb; b.nx[1] = xBDb; b.nx[3] = -xBDb;
     b.ny[0] = yACb; b.ny[2] = -yACb; b.ny[1] = yBDb; b.ny[3] = -yBDb;
     for (int k = 0; k < 4; k++) {
-        const double r = nb[k][3] / nb[k][2];
+        const double r = nb[k][3] * s.ic1[k];
         b.nb[k][0] = fb[2][k];
         b.nb[k][1] = fb[3][k];
-        b.nb[k][3] = fb[1][k] / nb[k][2];
-        b.nb[k][2] = -fb[1][k] * r / nb[k][2];
+        b.nb[k][3] = fb[1][k] * s.ic1[k];
+        b.nb[k][2] = -fb[1][k] * r * s.ic1[k];
     }
     (void)Vc;
 }
@@ -602,8 +609,9 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
         }
     }
     const double dtbyvolb = a.alpha * dtvb;
-    const double dtb = dtbyvolb / g.vol;
-    double volb = -dtbyvolb * DT / (g.vol * g.vol);
+    const double ivol = 1.0 / g.vol;
+    const double dtb = dtbyvolb * ivol;
+    double volb = -dtb * DT * ivol;
     if (a.first) a.dtbar[cell] = dtb;
     else a.dtbar[cell] += dtb;
     // source reverse: R5 -= VOL*SOURCE5, R3 -= VOL*SOURCE3
@@ -666,8 +674,10 @@ TNS_HD void load_rows(const AdjArgs& a, long long ps, double r[NWROW]) {
     for (int q = 0; q < NWROW; q++) r[q] = wv(a, q, ps);
 }
 
-// Gathers the adjoint of one cell's field-set rows (flux, sources, viscous, ghosts it is
-// parent or opposite cell of) and pulls it back to the cell's conservative state.
+// Gathers the adjoint of one cell's field-set rows from the residual (flux), the
+// sources (its own and its neighbours') and, in stage 1, the viscous flux, and pulls it
+// back to the cell's conservative state: the adjoint of the stage input (stages 2-4) or
+// a part of the adjoint of Q_n (stage 1).  Ghost contributions follow in s3g_point.
 TNS_HD void s3_point(const AdjArgs& a, long long cell) {
     const int i = (int)(cell / a.nj), j = (int)(cell % a.nj);
     CellGeo g;
@@ -711,13 +721,60 @@ TNS_HD void s3_point(const AdjArgs& a, long long cell) {
         wb[WC1] += a.wvisc[3 * a.npad + ps];
         wb[WC5] += a.wvisc[4 * a.npad + ps];
     }
-    double pw[NWROW], gw[NWROW], ow[NWROW], gb[NWROW], dummy[NWROW];
+    double q[5], qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int m = 0; m < 5; m++) q[m] = a.qin[m * a.ncell + cell];
+    prim_adj(a.P, q, wb, qb);
+    for (int m = 0; m < 5; m++) {
+        if (a.stage1) a.lam_old[m * a.ncell + cell] += qb[m];
+        else a.lam_out[m * a.ncell + cell] = qb[m];
+    }
+    if (a.geo) {
+        a.xcbar[ps] += xcb;
+        a.ycbar[ps] += ycb;
+    }
+}
+
+// Cells within two of the boundary, the ones a ghost can have as parent or opposite cell:
+// rows {0, 1, NI-2, NI-1} at every j, then columns {0, 1, NJ-2, NJ-1} of rows 2..NI-3.
+TNS_HD long long band_count(const AdjArgs& a) {
+    const long long nr = a.ni >= 4 ? 4 : a.ni, nc = a.nj >= 4 ? 4 : a.nj;
+    return nr * a.nj + (a.ni >= 5 ? (long long)(a.ni - 4) * nc : 0);
+}
+
+TNS_HD void band_cell(const AdjArgs& a, long long idx, int& i, int& j) {
+    const int nr = a.ni >= 4 ? 4 : a.ni, nc = a.nj >= 4 ? 4 : a.nj;
+    if (idx < (long long)nr * a.nj) {
+        const int r = (int)(idx / a.nj);
+        i = a.ni >= 4 ? (r < 2 ? r : a.ni - 4 + r) : r;
+        j = (int)(idx % a.nj);
+    } else {
+        const long long t = idx - (long long)nr * a.nj;
+        const int c = (int)(t % nc);
+        i = 2 + (int)(t / nc);
+        j = a.nj >= 4 ? (c < 2 ? c : a.nj - 4 + c) : c;
+    }
+}
+
+// The ghost part of the stage gather for one boundary-band cell: the adjoint of each
+// ghost whose parent this cell is (all types) or whose opposite cell it is (type 3),
+// pulled back through APPLY_BOUNDARY and this cell's primitives, added to the output of
+// s3_point (prim_adj is linear in the row adjoint).
+TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
+    int i, j;
+    band_cell(a, idx, i, j);
+    const long long cell = cell_of(a, i, j), ps = padi(a, i, j);
+    double wb[NWROW], pw[NWROW], gw[NWROW], ow[NWROW], gb[NWROW];
+    for (int r = 0; r < NWROW; r++) wb[r] = 0.0;
     double t0b = 0.0, s0b = 0.0;
+    bool any = false;
+    CellGeo g;
+    cell_geo(a, i, j, g);
     load_rows(a, ps, pw);
     for (int k = 0; k < 4; k++) {
         // the ghost on this cell's face k
         const int gi = i + di_of(k), gj = j + dj_of(k);
         if (is_cell(a, gi, gj)) continue;
+        any = true;
         int along = 0;
         const int side = ghost_side(a, gi, gj, along);
         const int type = a.M.gtype[a.M.ghost_index(side, along)];
@@ -726,6 +783,7 @@ TNS_HD void s3_point(const AdjArgs& a, long long cell) {
         load_rows(a, gps, gw);
         if (type == 3) load_rows(a, padi(a, i - di_of(k), j - dj_of(k)), ow);
         else load_rows(a, ps, ow);
+        double dummy[NWROW];
         for (int r = 0; r < NWROW; r++) dummy[r] = 0.0;
         ghost_adj(a.P, type, gw, pw, ow, gb, wb, dummy, t0b, s0b);
         if (a.geo) {
@@ -741,6 +799,7 @@ TNS_HD void s3_point(const AdjArgs& a, long long cell) {
         int along = 0;
         const int side = ghost_side(a, gi, gj, along);
         if (a.M.gtype[a.M.ghost_index(side, along)] != 3) continue;
+        any = true;
         const long long pc = cell_of(a, pi, pj), pps = padi(a, pi, pj), gps = padi(a, gi, gj);
         CellGeo pg;
         cell_geo(a, pi, pj, pg);
@@ -756,16 +815,15 @@ TNS_HD void s3_point(const AdjArgs& a, long long cell) {
         wb[WT] += obar[WT];
         wb[WP] += obar[WP];
     }
+    if (!any) return;
     double q[5], qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int m = 0; m < 5; m++) q[m] = a.qin[m * a.ncell + cell];
     prim_adj(a.P, q, wb, qb);
     for (int m = 0; m < 5; m++) {
         if (a.stage1) a.lam_old[m * a.ncell + cell] += qb[m];
-        else a.lam_out[m * a.ncell + cell] = qb[m];
+        else a.lam_out[m * a.ncell + cell] += qb[m];
     }
     if (a.geo) {
-        a.xcbar[ps] += xcb;
-        a.ycbar[ps] += ycb;
         a.t0bar[cell] += t0b;
         a.s0bar[cell] += s0b;
     }
@@ -846,15 +904,15 @@ TNS_HD void v0_point(const AdjArgs& a, long long node) {
 // the flux it adds to VISU, VISV, VIST, VISR).  out: NVF values (see VF_*).
 TNS_HD void visc_face_adj(const Params& P, const FaceIn& f, const double w[4], double* out, long long stride) {
     const double ybd = f.yb - f.yd, yac = f.ya - f.yc, xbd = f.xb - f.xd, xac = f.xa - f.xc;
-    const double dnr = xac * ybd - xbd * yac;
+    const double dnr = xac * ybd - xbd * yac, idnr = 1.0 / dnr;
     const double A[5] = {f.ua, f.va, f.ta, f.rhoa, f.ra}, B[5] = {f.ub, f.vb, f.tb, f.rhob, f.rb};
     const double C[5] = {f.uc, f.vc, f.tc, f.rhoc, f.rc}, D[5] = {f.ud, f.vd, f.td, f.rhod, f.rd};
     double da[5], db[5], GX[5], GY[5];
     for (int q = 0; q < 5; q++) {
         da[q] = A[q] - C[q];
         db[q] = B[q] - D[q];
-        GX[q] = (da[q] * ybd - db[q] * yac) / dnr;
-        GY[q] = (-da[q] * xbd + db[q] * xac) / dnr;
+        GX[q] = (da[q] * ybd - db[q] * yac) * idnr;
+        GY[q] = (-da[q] * xbd + db[q] * xac) * idnr;
     }
     double AV[5];
     for (int q = 0; q < 5; q++) AV[q] = 0.25 * (A[q] + B[q] + C[q] + D[q]);
@@ -873,10 +931,11 @@ TNS_HD void visc_face_adj(const Params& P, const FaceIn& f, const double w[4], d
     }
     const double AMU = amu_of(P, TAVG);
     const double AK = AMU * P.cp_pr;
-    const double CHI = RHOAVG * RAVG / (AMU * CMU);
+    const double iac = 1.0 / (AMU * CMU);
+    const double CHI = RHOAVG * RAVG * iac;
     const double X2 = CHI * CHI;
-    const double ta = tanh(ALPHA_T * X2), tb = tanh(BETA_T * X2);
-    const double FMU = ta / tb;
+    const double ta = tanh(ALPHA_T * X2), tb = tanh(BETA_T * X2), itb = 1.0 / tb;
+    const double FMU = ta * itb;
     const double AMUT = RHOAVG * RAVG * FMU;
     const double AKT = AMUT * P.cp_prt;
     const double AMUEFF = AMU + AMUT, AKEFF = AK + AKT;
@@ -926,10 +985,10 @@ TNS_HD void visc_face_adj(const Params& P, const FaceIn& f, const double w[4], d
     AVb[3] += AMUTb * RAVG * FMU;
     AVb[4] += AMUTb * RHOAVG * FMU;
     const double FMUb = AMUTb * RHOAVG * RAVG;
-    const double CHIb = FMUb * (ALPHA_T * (1.0 - ta * ta) - FMU * BETA_T * (1.0 - tb * tb)) / tb * 2.0 * CHI;
-    AVb[3] += CHIb * RAVG / (AMU * CMU);
-    AVb[4] += CHIb * RHOAVG / (AMU * CMU);
-    AMUb -= CHIb * CHI / AMU;
+    const double CHIb = FMUb * (ALPHA_T * (1.0 - ta * ta) - FMU * BETA_T * (1.0 - tb * tb)) * itb * 2.0 * CHI;
+    AVb[3] += CHIb * RAVG * iac;
+    AVb[4] += CHIb * RHOAVG * iac;
+    AMUb -= CHIb * CHI * iac * CMU;
     AVb[2] += AMUb * 0.6 * AMU / TAVG;
     double Ab[5], Bb[5], Cb[5], Db[5];
     for (int q = 0; q < 5; q++) Ab[q] = Bb[q] = Cb[q] = Db[q] = 0.25 * AVb[q];
@@ -937,17 +996,17 @@ TNS_HD void visc_face_adj(const Params& P, const FaceIn& f, const double w[4], d
     for (int q = 0; q < 5; q++) {
         const double gx = GXb[q], gy = GYb[q];
         if (gx == 0.0 && gy == 0.0) continue;
-        const double dab = (gx * ybd - gy * xbd) / dnr;
-        const double dbb = (-gx * yac + gy * xac) / dnr;
+        const double dab = (gx * ybd - gy * xbd) * idnr;
+        const double dbb = (-gx * yac + gy * xac) * idnr;
         Ab[q] += dab;
         Cb[q] -= dab;
         Bb[q] += dbb;
         Db[q] -= dbb;
-        ybdb += gx * da[q] / dnr;
-        yacb -= gx * db[q] / dnr;
-        xbdb -= gy * da[q] / dnr;
-        xacb += gy * db[q] / dnr;
-        dnrb -= (gx * GX[q] + gy * GY[q]) / dnr;
+        ybdb += gx * da[q] * idnr;
+        yacb -= gx * db[q] * idnr;
+        xbdb -= gy * da[q] * idnr;
+        xacb += gy * db[q] * idnr;
+        dnrb -= (gx * GX[q] + gy * GY[q]) * idnr;
     }
     xacb += dnrb * ybd;
     ybdb += dnrb * xac;

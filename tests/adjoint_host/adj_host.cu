@@ -98,6 +98,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
             for (long long p = 0; p < a.npad; p++) v3_point(a, p);
         }
         for (long long c = 0; c < n; c++) s3_point(a, c);
+        for (long long c = 0; c < band_count(a); c++) s3g_point(a, c);
     }
     for (long long c = 0; c < n; c++) d0_point(a, c);
     for (long long c = 0; c < n; c++) d1_point(a, c);
