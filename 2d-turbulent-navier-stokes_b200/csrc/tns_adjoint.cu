@@ -89,8 +89,9 @@ struct tns_adjoint_state {
         wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens;
     DevBuf<int> ninfo;
     long long nsens = 0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // without / with sensitivities
-    long long per_step[2] = {0, 0};
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // [frozen][sensitivities]
+    long long per_step[4] = {0, 0, 0, 0};
+    bool have_forward = false;  // the buffers hold the forward values of the last state
     long long launches = 0;
 };
 
@@ -153,24 +154,28 @@ long long sens_size(long long n, long long npad, long long nnode) {
 }
 
 // One reverse step, enqueued on stream st: recompute from q0, reverse into lamold, copy
-// the result to lam.  Returns the number of kernels launched.
-long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, cudaStream_t st) {
+// the result to lam.  With `frozen` the forward values of the previous step's state are
+// reused: no recompute, no field sets, node averages or dissipation pre-pass.  Returns
+// the number of kernels launched.
+long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen, cudaStream_t st) {
     const Params& P = h->P;
     const Mesh& M = h->M;
     long long nl = 0;
     static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
-    // forward recompute with the solver's kernels
-    if (!P.local) {
-        tns::launch_dtmin(P, M, s->q0.p, h->partial.p, h->counter.p, s->dtmin.p, st);
-        nl++;
-    }
-    tns::launch_dissipation(P, M, s->q0.p, s->d.p, s->dt.p, s->dtmin.p, st);
-    tns::launch_viscous(P, M, s->q0.p, s->vis.p, st);
     double* qs[4] = {s->q0.p, s->q1.p, s->q2.p, s->q3.p};
-    for (int k = 0; k < 3; k++)
-        tns::launch_stage(P, M, qs[k], s->q0.p, qs[k + 1], s->d.p, s->vis.p, s->dt.p, s->dtmin.p, alpha[k],
-                          nullptr, nullptr, st);
-    nl += 5;
+    if (!frozen) {
+        // forward recompute with the solver's kernels
+        if (!P.local) {
+            tns::launch_dtmin(P, M, s->q0.p, h->partial.p, h->counter.p, s->dtmin.p, st);
+            nl++;
+        }
+        tns::launch_dissipation(P, M, s->q0.p, s->d.p, s->dt.p, s->dtmin.p, st);
+        tns::launch_viscous(P, M, s->q0.p, s->vis.p, st);
+        for (int k = 0; k < 3; k++)
+            tns::launch_stage(P, M, qs[k], s->q0.p, qs[k + 1], s->d.p, s->vis.p, s->dt.p, s->dtmin.p, alpha[k],
+                              nullptr, nullptr, st);
+        nl += 5;
+    }
     // reverse
     AdjArgs a = base_args(h, s, geo);
     double* lam_stage[5] = {nullptr, s->lamA.p, s->lamB.p, s->lamA.p, s->lam.p};
@@ -181,24 +186,34 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, cudaStream_
         a.stage1 = k == 0;
         a.lam_in = lam_stage[k + 1];
         a.lam_out = lam_stage[k];
-        launch_points(k_adj_fields, a, a.npad, st);
+        a.w = s->w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
+        if (!frozen) {
+            launch_points(k_adj_fields, a, a.npad, st);
+            nl++;
+        }
         launch_points(k_adj_stage, a, a.ncell, st);
-        nl += 2;
+        nl++;
         if (k == 0) {
-            launch_points(k_adj_nodes, a, a.nnode, st);
+            if (!frozen) {
+                launch_points(k_adj_nodes, a, a.nnode, st);
+                nl++;
+            }
             launch_points(k_adj_faces, a, a.nif + a.njf, st);
             launch_points(k_adj_node_bar, a, a.nnode, st);
             launch_points(k_adj_slot_bar, a, a.npad, st);
-            nl += 4;
+            nl += 3;
         }
         launch_points(k_adj_gather, a, a.ncell, st);
         launch_points(k_adj_gather_ghosts, a, band_count(a), st);
         nl += 2;
     }
-    launch_points(k_adj_diss_pre, a, a.ncell, st);
+    if (!frozen) {
+        launch_points(k_adj_diss_pre, a, a.ncell, st);
+        nl++;
+    }
     launch_points(k_adj_diss_faces, a, a.ncell, st);
     launch_points(k_adj_diss_gather, a, a.ncell, st);
-    nl += 3;
+    nl += 2;
     if (!P.local) {
         cudaMemsetAsync(s->dtsum.p, 0, sizeof(double), st);
         k_adj_dtsum<<<148, ADJ_THREADS, 0, st>>>(s->dtbar.p, a.ncell, s->dtsum.p);
@@ -254,7 +269,7 @@ int tns_adjoint_enable(tns_handle* h) {
         long long count;
     } reqs[] = {{&s->q0, 5 * n}, {&s->q1, 5 * n}, {&s->q2, 5 * n}, {&s->q3, 5 * n}, {&s->d, 5 * n},
                 {&s->vis, 4 * n}, {&s->dt, n}, {&s->dtmin, 1}, {&s->lam, 5 * n}, {&s->lamA, 5 * n},
-                {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->w, NWROW * npad}, {&s->gbar, 5 * npad},
+                {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->w, 4 * NWROW * npad}, {&s->gbar, 5 * npad},
                 {&s->srcn, 16 * n}, {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad},
                 {&s->dbar, 5 * n}, {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dpre, NDPRE * n},
                 {&s->dout, NDOUT * n}, {&s->navg, NNA * nnode}, {&s->nbar, 5 * nnode}, {&s->vfi, NVF * nif},
@@ -282,27 +297,33 @@ int tns_adjoint_step(tns_handle* h, const double* d_q, double* d_lam, int flags)
     if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
     tns_adjoint_state* s = h->adj;
     const int geo = flags & TNS_ADJ_SENSITIVITIES ? 1 : 0;
+    const int frozen = flags & TNS_ADJ_FROZEN ? 1 : 0;
+    if (frozen && !s->have_forward)
+        return h->fail(TNS_ERR_STATE, "tns_adjoint_step: TNS_ADJ_FROZEN before any step without it");
     const size_t bytes = sizeof(double) * 5 * (size_t)h->ni * h->nj;
     cudaStream_t st = h->stream;
-    if ((rc = h->cuda(cudaMemcpyAsync(s->q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: state in")) ||
+    if ((!frozen &&
+         (rc = h->cuda(cudaMemcpyAsync(s->q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: state in"))) ||
         (rc = h->cuda(cudaMemcpyAsync(s->lam.p, d_lam, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: lambda in")))
         return rc;
+    const int gi = frozen * 2 + geo;
     if (h->profile) {
-        s->launches += enqueue_step(h, s, geo, st);
+        s->launches += enqueue_step(h, s, geo, frozen, st);
     } else {
-        if (!s->graph[geo]) {
+        if (!s->graph[gi]) {
             cudaGraph_t g;
             if ((rc = h->cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "adjoint capture")))
                 return rc;
-            s->per_step[geo] = enqueue_step(h, s, geo, st);
+            s->per_step[gi] = enqueue_step(h, s, geo, frozen, st);
             if ((rc = h->cuda(cudaStreamEndCapture(st, &g), "adjoint capture"))) return rc;
-            rc = h->cuda(cudaGraphInstantiate(&s->graph[geo], g, 0), "adjoint graph instantiate");
+            rc = h->cuda(cudaGraphInstantiate(&s->graph[gi], g, 0), "adjoint graph instantiate");
             cudaGraphDestroy(g);
             if (rc) return rc;
         }
-        if ((rc = h->cuda(cudaGraphLaunch(s->graph[geo], st), "adjoint graph launch"))) return rc;
-        s->launches += s->per_step[geo];
+        if ((rc = h->cuda(cudaGraphLaunch(s->graph[gi], st), "adjoint graph launch"))) return rc;
+        s->launches += s->per_step[gi];
     }
+    s->have_forward = true;
     if ((rc = h->cuda(cudaMemcpyAsync(d_lam, s->lam.p, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: lambda out")))
         return rc;
     return h->cuda(cudaGetLastError(), "tns_adjoint_step");

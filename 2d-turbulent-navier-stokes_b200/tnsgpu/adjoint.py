@@ -968,12 +968,13 @@ class DeviceAdjoint:
         self._leave()
         return states
 
-    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool):
+    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool, frozen: bool = False):
+        """``frozen``: q is the previous step's state (its forward values are reused)."""
         if not (q.is_contiguous() and lam.is_contiguous() and lam.dtype == torch.float64
                 and q.dtype == torch.float64):
             raise ValueError("q and lambda must be contiguous float64 device tensors")
         self._enter()
-        self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities)
+        self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities, frozen)
         self._leave()
 
     def sensitivities(self) -> Dict[str, torch.Tensor]:
@@ -1077,14 +1078,14 @@ def _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, sp
     hist = []
     try:
         lam = djdq.clone()
-        for _ in range(niter):
+        for it in range(niter):
             vj = lam.clone()
-            dev_adj.step(q, vj, False)
+            dev_adj.step(q, vj, False, frozen=it > 0)  # Q* is fixed: forward values reused
             new = djdq + vj
             hist.append(float(torch.max(torch.abs(new - lam))))
             lam = new
         last = lam.clone()
-        dev_adj.step(q, last, True)  # lambda dG/dp at Q*
+        dev_adj.step(q, last, True, frozen=niter > 0)  # lambda dG/dp at Q*
         sens = dev_adj.sensitivities()
     finally:
         dev_adj.close()

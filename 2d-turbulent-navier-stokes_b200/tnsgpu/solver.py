@@ -143,11 +143,12 @@ class Solver:
         """Loads the state from device memory at ``ptr`` ([5][NELES] doubles), async."""
         self._check(self.L.tns_copy_state_device(self.h, C.c_void_p(int(ptr)), 1))
 
-    def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities: bool = False):
+    def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities: bool = False, frozen: bool = False):
         """lambda <- lambda dG/dQ_n for the iteration from Q_n (both device pointers);
-        with ``sensitivities`` also accumulates lambda dG/dp (tns_adjoint_step)."""
-        self._check(self.L.tns_adjoint_step(self.h, C.c_void_p(int(q_ptr)), C.c_void_p(int(lam_ptr)),
-                                            1 if sensitivities else 0))
+        with ``sensitivities`` also accumulates lambda dG/dp; with ``frozen`` Q_n is the
+        previous call's state and its forward values are reused (tns_adjoint_step)."""
+        flags = (1 if sensitivities else 0) | (2 if frozen else 0)
+        self._check(self.L.tns_adjoint_step(self.h, C.c_void_p(int(q_ptr)), C.c_void_p(int(lam_ptr)), flags))
 
     def adjoint_sensitivities(self, reset: bool = True) -> np.ndarray:
         n = int(self.L.tns_adjoint_sensitivity_size(self.h))

@@ -185,6 +185,10 @@ void tns_destroy(tns_handle *h);
  * [5][NELES] component-major in that order; calls are asynchronous on the handle's
  * stream (tns_set_stream). */
 #define TNS_ADJ_SENSITIVITIES 1
+/* TNS_ADJ_FROZEN: Q_n is the state of the previous call (d_q is not read); the forward
+ * values kept from that call are reused, which skips the recomputed iteration and every
+ * state-only pass -- the fixed-point adjoint at a converged state. */
+#define TNS_ADJ_FROZEN 2
 int tns_adjoint_enable(tns_handle *h);
 int tns_adjoint_step(tns_handle *h, const double *d_q, double *d_lam, int flags);
 long long tns_adjoint_sensitivity_size(tns_handle *h);

@@ -206,3 +206,25 @@ def test_cuda_adjoint_step_is_deterministic():
     finally:
         dev.close()
     assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
+def test_frozen_adjoint_steps_equal_full_steps():
+    """TNS_ADJ_FROZEN reuses the forward values of the previous call's state: bitwise the
+    same lambda and sensitivities as full steps at that state."""
+    mesh, flow, sch, space = _ramp(64, 24)
+    prm = sch.params()
+    dev = adjoint.DeviceAdjoint(sch, space, prm, None)
+    try:
+        q = dev.primal(sch.cold_state(prm).contiguous(), 40)[40].contiguous()
+        lam0 = torch.tensor(np.random.default_rng(9).normal(size=(5,) + mesh.shape), device="cuda")
+        runs = []
+        for frozen in (False, True):
+            lam = lam0.clone()
+            dev.step(q, lam, False)
+            for _ in range(3):
+                dev.step(q, lam, False, frozen=frozen)
+            dev.step(q, lam, True, frozen=frozen)
+            runs.append((lam, dev.sensitivities()["sx"][1]))
+    finally:
+        dev.close()
+    assert torch.equal(runs[0][0], runs[1][0]) and torch.equal(runs[0][1], runs[1][1])
