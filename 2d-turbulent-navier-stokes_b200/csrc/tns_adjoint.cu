@@ -57,6 +57,7 @@ TNS_ADJ_KERNEL(k_adj_diss_pre, d0_point, 1)
 TNS_ADJ_KERNEL(k_adj_diss_faces, d1_point, 1)
 TNS_ADJ_KERNEL(k_adj_diss_gather, d2_point, 1)
 TNS_ADJ_KERNEL(k_adj_dtmin, dtmin_point, 1)
+TNS_ADJ_KERNEL(k_adj_final, final_point, 1)
 
 // LOCAL = 0: sum of the per-cell dt adjoints (block sums, one atomic per block).
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_dtsum(const double* __restrict__ v, long long n,
@@ -85,8 +86,12 @@ void launch_points(K kernel, const AdjArgs& a, long long n, cudaStream_t s) {
 
 // Device buffers and graphs of the adjoint of one handle.
 struct tns_adjoint_state {
-    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, lam, lamA, lamB, lamold, w, gbar, srcn, srcg, wself,
-        wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens;
+    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, lam, lamA, lamB, lamold, lamg, lamd, w, gbar, srcn, srcg,
+        wself, wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens;
+    // branches of a step: the ghost gather beside the interior gather, the dissipation
+    // reverse beside the viscous reverse
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev = nullptr;
     DevBuf<int> ninfo;
     long long nsens = 0;
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // [frozen][sensitivities]
@@ -115,6 +120,8 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.dtmin = s->dtmin.p;
     a.w = s->w.p;
     a.lam_old = s->lamold.p;
+    a.lamg = s->lamg.p;
+    a.lamd = s->lamd.p;
     a.gbar = s->gbar.p;
     a.srcn = s->srcn.p;
     a.srcg = s->srcg.p;
@@ -178,6 +185,14 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
     }
     // reverse
     AdjArgs a = base_args(h, s, geo);
+    auto fork = [&](cudaStream_t to) {
+        cudaEventRecord(s->ev, st);
+        cudaStreamWaitEvent(to, s->ev, 0);
+    };
+    auto join = [&](cudaStream_t from) {
+        cudaEventRecord(s->ev, from);
+        cudaStreamWaitEvent(st, s->ev, 0);
+    };
     double* lam_stage[5] = {nullptr, s->lamA.p, s->lamB.p, s->lamA.p, s->lam.p};
     for (int k = 3; k >= 0; k--) {
         a.qin = qs[k];
@@ -194,6 +209,22 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
         launch_points(k_adj_stage, a, a.ncell, st);
         nl++;
         if (k == 0) {
+            // dissipation / time-step reverse on a branch (it needs only D_bar, DT_bar)
+            fork(s->side[0]);
+            if (!frozen) {
+                launch_points(k_adj_diss_pre, a, a.ncell, s->side[0]);
+                nl++;
+            }
+            launch_points(k_adj_diss_faces, a, a.ncell, s->side[0]);
+            launch_points(k_adj_diss_gather, a, a.ncell, s->side[0]);
+            nl += 2;
+            if (!P.local) {
+                cudaMemsetAsync(s->dtsum.p, 0, sizeof(double), s->side[0]);
+                k_adj_dtsum<<<148, ADJ_THREADS, 0, s->side[0]>>>(s->dtbar.p, a.ncell, s->dtsum.p);
+                launch_points(k_adj_dtmin, a, a.ncell, s->side[0]);
+                nl += 2;
+            }
+            // viscous reverse on the main stream
             if (!frozen) {
                 launch_points(k_adj_nodes, a, a.nnode, st);
                 nl++;
@@ -203,24 +234,16 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
             launch_points(k_adj_slot_bar, a, a.npad, st);
             nl += 3;
         }
+        fork(s->side[1]);
+        launch_points(k_adj_gather_ghosts, a, band_count(a), s->side[1]);
         launch_points(k_adj_gather, a, a.ncell, st);
-        launch_points(k_adj_gather_ghosts, a, band_count(a), st);
         nl += 2;
+        join(s->side[1]);
     }
-    if (!frozen) {
-        launch_points(k_adj_diss_pre, a, a.ncell, st);
-        nl++;
-    }
-    launch_points(k_adj_diss_faces, a, a.ncell, st);
-    launch_points(k_adj_diss_gather, a, a.ncell, st);
-    nl += 2;
-    if (!P.local) {
-        cudaMemsetAsync(s->dtsum.p, 0, sizeof(double), st);
-        k_adj_dtsum<<<148, ADJ_THREADS, 0, st>>>(s->dtbar.p, a.ncell, s->dtsum.p);
-        launch_points(k_adj_dtmin, a, a.ncell, st);
-        nl += 2;
-    }
-    cudaMemcpyAsync(s->lam.p, s->lamold.p, sizeof(double) * 5 * a.ncell, cudaMemcpyDeviceToDevice, st);
+    join(s->side[0]);
+    a.lam_out = s->lam.p;
+    launch_points(k_adj_final, a, a.ncell, st);
+    nl++;
     return nl;
 }
 
@@ -241,8 +264,14 @@ void adjoint_release(tns_handle* h) {
     if (!s) return;
     for (auto& g : s->graph)
         if (g) cudaGraphExecDestroy(g);
+    for (auto& x : s->side)
+        if (x) {
+            cudaStreamSynchronize(x);
+            cudaStreamDestroy(x);
+        }
+    if (s->ev) cudaEventDestroy(s->ev);
     for (auto* b : {&s->q0, &s->q1, &s->q2, &s->q3, &s->d, &s->vis, &s->dt, &s->dtmin, &s->lam, &s->lamA, &s->lamB,
-                    &s->lamold, &s->w, &s->gbar, &s->srcn, &s->srcg, &s->wself, &s->wvisc, &s->dbar, &s->visbar,
+                    &s->lamold, &s->lamg, &s->lamd, &s->w, &s->gbar, &s->srcn, &s->srcg, &s->wself, &s->wvisc, &s->dbar, &s->visbar,
                     &s->dtbar, &s->dpre, &s->dout, &s->navg, &s->nbar, &s->vfi, &s->vfj, &s->dtsum, &s->sens})
         b->release();
     s->ninfo.release();
@@ -269,7 +298,8 @@ int tns_adjoint_enable(tns_handle* h) {
         long long count;
     } reqs[] = {{&s->q0, 5 * n}, {&s->q1, 5 * n}, {&s->q2, 5 * n}, {&s->q3, 5 * n}, {&s->d, 5 * n},
                 {&s->vis, 4 * n}, {&s->dt, n}, {&s->dtmin, 1}, {&s->lam, 5 * n}, {&s->lamA, 5 * n},
-                {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->w, 4 * NWROW * npad}, {&s->gbar, 5 * npad},
+                {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->lamg, 5 * n}, {&s->lamd, 5 * n},
+                {&s->w, 4 * NWROW * npad}, {&s->gbar, 5 * npad},
                 {&s->srcn, 16 * n}, {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad},
                 {&s->dbar, 5 * n}, {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dpre, NDPRE * n},
                 {&s->dout, NDOUT * n}, {&s->navg, NNA * nnode}, {&s->nbar, 5 * nnode}, {&s->vfi, NVF * nif},
@@ -280,7 +310,10 @@ int tns_adjoint_enable(tns_handle* h) {
             return rc;
         }
     }
-    if ((rc = h->cuda(s->ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)"))) {
+    if ((rc = h->cuda(s->ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)")) ||
+        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[0], cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[1], cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = h->cuda(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate"))) {
         tns_rt::adjoint_release(h);
         return rc;
     }

@@ -66,7 +66,9 @@ struct AdjArgs {
     // adjoint state
     const double* lam_in;  // adjoint of the stage output [5][ncell]
     double* lam_out;       // adjoint of the stage input (stages 2-4) [5][ncell]
-    double* lam_old;       // adjoint of Q_n [5][ncell]
+    double* lam_old;       // adjoint of Q_n, residual / source / viscous parts [5][ncell]
+    double* lamg;          // ghost part of the last stage gather, boundary band [5][ncell]
+    double* lamd;          // dissipation and time-step part of the adjoint of Q_n [5][ncell]
     double* gbar;          // adjoint of the residual [5][npad], ghost ring zero
     double* srcn;          // source adjoint to neighbour k: u v C1 C5 [4][4][ncell]
     double* srcg;          // source adjoint to neighbour k's centroid x y [4][2][ncell]
@@ -104,6 +106,10 @@ TNS_HD bool is_cell(const AdjArgs& a, int i, int j) { return i >= 0 && i < a.ni 
 TNS_HD long long cell_of(const AdjArgs& a, int i, int j) { return (long long)i * a.nj + j; }
 TNS_HD double wv(const AdjArgs& a, int row, long long ps) { return a.w[row * a.npad + ps]; }
 TNS_HD double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+// Within two cells of the boundary (a ghost's parent or opposite cell).
+TNS_HD bool in_band(const AdjArgs& a, int i, int j) {
+    return i < 2 || i >= a.ni - 2 || j < 2 || j >= a.nj - 2;
+}
 
 // Ghost side (1..4) of ring position (i, j), or 0 for a cell / corner.
 TNS_HD int ghost_side(const AdjArgs& a, int i, int j, int& along) {
@@ -578,6 +584,7 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
         vv[m] = m ? a.vis[(m - 1) * a.ncell + cell] : 0.0;
         res[m] = R[m] - vv[m] - dd[m];
         lb[m] = a.lam_in[m * a.ncell + cell];
+        if (!a.first && in_band(a, i, j)) lb[m] += a.lamg[m * a.ncell + cell];
         lh[m] = lb[m];
     }
     const double n0 = qo[0] - dtv * res[0];
@@ -757,8 +764,9 @@ TNS_HD void band_cell(const AdjArgs& a, long long idx, int& i, int& j) {
 
 // The ghost part of the stage gather for one boundary-band cell: the adjoint of each
 // ghost whose parent this cell is (all types) or whose opposite cell it is (type 3),
-// pulled back through APPLY_BOUNDARY and this cell's primitives, added to the output of
-// s3_point (prim_adj is linear in the row adjoint).
+// pulled back through APPLY_BOUNDARY and this cell's primitives into lamg (prim_adj is
+// linear in the row adjoint, so this part adds to s3_point's; it runs beside it, and the
+// next stage -- or final_point -- adds it).
 TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
     int i, j;
     band_cell(a, idx, i, j);
@@ -815,14 +823,13 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         wb[WT] += obar[WT];
         wb[WP] += obar[WP];
     }
-    if (!any) return;
-    double q[5], qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int m = 0; m < 5; m++) q[m] = a.qin[m * a.ncell + cell];
-    prim_adj(a.P, q, wb, qb);
-    for (int m = 0; m < 5; m++) {
-        if (a.stage1) a.lam_old[m * a.ncell + cell] += qb[m];
-        else a.lam_out[m * a.ncell + cell] += qb[m];
+    double qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (any) {
+        double q[5];
+        for (int m = 0; m < 5; m++) q[m] = a.qin[m * a.ncell + cell];
+        prim_adj(a.P, q, wb, qb);
     }
+    for (int m = 0; m < 5; m++) a.lamg[m * a.ncell + cell] = qb[m];
     if (a.geo) {
         a.t0bar[cell] += t0b;
         a.s0bar[cell] += s0b;
@@ -1393,7 +1400,7 @@ TNS_HD void d2_point(const AdjArgs& a, long long cell) {
     double dlb = 0.0;
     ts_adj(P, q, a.M.cfldl[cell], pb, P.local ? dtb : 0.0, qb, dlb);
     if (!P.local) a.dtbar[cell] = dtb;
-    for (int m = 0; m < 5; m++) a.lam_old[m * n + cell] += qb[m];
+    for (int m = 0; m < 5; m++) a.lamd[m * n + cell] = qb[m];
     if (a.geo) {
         a.volbar[cell] += volb;
         a.dlbar[cell] += dlb;
@@ -1415,8 +1422,21 @@ TNS_HD void dtmin_point(const AdjArgs& a, long long cell) {
     if (!(dtl == *a.dtmin) || dtl >= 100000.0) return;
     double qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, dlb = 0.0;
     ts_adj(P, q, a.M.cfldl[cell], 0.0, *a.dtsum, qb, dlb);
-    for (int m = 0; m < 5; m++) a.lam_old[m * n + cell] += qb[m];
+    for (int m = 0; m < 5; m++) a.lamd[m * n + cell] += qb[m];
     if (a.geo) a.dlbar[cell] += dlb;
+}
+
+
+// The adjoint of Q_n: residual / source / viscous part, dissipation / time-step part and
+// the ghost part of stage 1's gather.
+TNS_HD void final_point(const AdjArgs& a, long long cell) {
+    const int i = (int)(cell / a.nj), j = (int)(cell % a.nj);
+    const bool band = in_band(a, i, j);
+    for (int m = 0; m < 5; m++) {
+        double v = a.lam_old[m * a.ncell + cell] + a.lamd[m * a.ncell + cell];
+        if (band) v += a.lamg[m * a.ncell + cell];
+        a.lam_out[m * a.ncell + cell] = v;
+    }
 }
 
 }  // namespace adj

@@ -36,7 +36,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.nif = (long long)(ni + 1) * nj;
     a.njf = (long long)ni * (nj + 1);
     const long long n = a.ncell;
-    std::vector<double> w(NWROW * a.npad), lamA(5 * n), lamB(5 * n), lamold(5 * n), gbar(5 * a.npad, 0.0),
+    std::vector<double> w(NWROW * a.npad), lamA(5 * n), lamB(5 * n), lamold(5 * n), lamg(5 * n), lamd(5 * n),
+        gbar(5 * a.npad, 0.0),
         srcn(16 * n), srcg(8 * n), wself(5 * n), wvisc(5 * a.npad, 0.0), dbar(5 * n), visbar(4 * n), dtbar(n),
         dpre(NDPRE * n), dout(NDOUT * n), navg(NNA * a.nnode), nbar(5 * a.nnode), vfi(NVF * a.nif),
         vfj(NVF * a.njf);
@@ -49,6 +50,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.dtmin = &dtmin;
     a.w = w.data();
     a.lam_old = lamold.data();
+    a.lamg = lamg.data();
+    a.lamd = lamd.data();
     a.gbar = gbar.data();
     a.srcn = srcn.data();
     a.srcg = srcg.data();
@@ -107,6 +110,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
         for (long long c = 0; c < n; c++) dts += dtbar[c];
         for (long long c = 0; c < n; c++) dtmin_point(a, c);
     }
-    std::memcpy(lam, lamold.data(), sizeof(double) * 5 * n);
+    a.lam_out = lam;
+    for (long long c = 0; c < n; c++) final_point(a, c);
     return 0;
 }
