@@ -263,6 +263,10 @@ def run_ours(args, rank, world, dev):
         other = {"precision": "fp64" if prec else "mixed", "value": replica_rate(mesh.neles, ms2 * 1e-3, world),
                  "ms_per_step": round(ms2, 5), "mixed_over_fp64": (ms2 / ms) if prec == 0 else (ms / ms2)}
 
+    adj = None
+    if world == 1 and not args.no_adjoint:
+        adj = adjoint_timing(torch, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0)
@@ -287,10 +291,68 @@ def run_ours(args, rank, world, dev):
         "device_ms_per_iteration_profiled": round(total_kms, 5),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         "other_precision": other,
+        "adjoint": adj,
         "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def adjoint_timing(torch, dev, K=50):
+    """adjoint/primal time on the discrete-adjoint workload (compression ramp 512 x 192,
+    IAXIS=0, LOCAL=1, cold start): one primal RK4 iteration (captured graph) against one
+    reverse step of the CUDA adjoint (tns_adjoint_step) -- with recomputation and the
+    parameter sensitivities, as a transient gradient takes it, and frozen at a fixed
+    state, as the fixed-point adjoint takes it.  CUDA events on the adjoint's stream,
+    K steps each after 5 warm-up steps; L2 not flushed on either side (the 512 x 192
+    working set is L2-resident for both)."""
+    from tnsgpu import adjoint, cases
+    mesh, flow = cases.ramp_mesh(512, 192), cases.ramp_flow()
+    flow.istart = 0
+    sch = adjoint.Scheme(mesh, flow, device=f"cuda:{dev}")
+    prm = sch.params()
+    da = adjoint.DeviceAdjoint(sch, adjoint.DesignSpace(sch), prm, None)
+    try:
+        st = da.primal(sch.cold_state(prm).contiguous(), K + 5)
+        S, s = da.stream, da.solver
+        ev = lambda: torch.cuda.Event(enable_timing=True)
+
+        def timed(fn):
+            torch.cuda.synchronize()
+            a, b = ev(), ev()
+            a.record(S)
+            for n in range(K):
+                fn(n)
+            b.record(S)
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) * 1e3 / K
+
+        s.state_from_device(st[0].data_ptr())
+        for _ in range(5):
+            s.enqueue(1)
+        primal_us = timed(lambda n: s.enqueue(1))
+        lam = torch.randn_like(st[0])
+        for n in range(5):
+            s.adjoint_step(st[n].data_ptr(), lam.data_ptr(), True)
+        launches0 = s.adjoint_launch_count()
+        step_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), True))
+        per_step = (s.adjoint_launch_count() - launches0) // K
+        q = st[K].contiguous()
+        s.adjoint_step(q.data_ptr(), lam.data_ptr(), False)
+        for _ in range(5):
+            s.adjoint_step(q.data_ptr(), lam.data_ptr(), False, True)
+        frozen_us = timed(lambda n: s.adjoint_step(q.data_ptr(), lam.data_ptr(), False, True))
+        da.sensitivities()
+    finally:
+        da.close()
+    return {"workload": "ramp_512x192 (IAXIS=0, LOCAL=1, cold start)", "steps": K,
+            "primal_iteration_us": round(primal_us, 2),
+            "transient_step_us": round(step_us, 2),
+            "fixed_point_step_us": round(frozen_us, 2),
+            "transient_step_over_primal": round(step_us / primal_us, 3),
+            "fixed_point_step_over_primal": round(frozen_us / primal_us, 3),
+            "transient_gradient_over_primal": round((primal_us + step_us) / primal_us, 3),
+            "kernels_per_transient_step": int(per_step)}
 
 
 def cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0):
@@ -352,6 +414,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--case", default="nozzle_plume_1024x384")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/primal timing")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
                     help="arithmetic of the timed path (the other one is timed too, as other_precision)")
     ap.add_argument("--single-precision-mode", action="store_true",
