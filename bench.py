@@ -298,13 +298,13 @@ def run_ours(args, rank, world, dev):
         print(json.dumps(line), flush=True)
 
 
-def adjoint_timing(torch, dev, K=50):
+def adjoint_timing(torch, dev, K=50, W=5):
     """adjoint/primal time on the discrete-adjoint workload (compression ramp 512 x 192,
     IAXIS=0, LOCAL=1, cold start): one primal RK4 iteration (captured graph) against one
     reverse step of the CUDA adjoint (tns_adjoint_step) -- with recomputation and the
     parameter sensitivities, as a transient gradient takes it, and frozen at a fixed
     state, as the fixed-point adjoint takes it.  CUDA events on the adjoint's stream,
-    K steps each after 5 warm-up steps; L2 not flushed on either side (the 512 x 192
+    K steps each after W warm-up steps; L2 not flushed on either side (the 512 x 192
     working set is L2-resident for both)."""
     from tnsgpu import adjoint, cases
     mesh, flow = cases.ramp_mesh(512, 192), cases.ramp_flow()
@@ -313,7 +313,7 @@ def adjoint_timing(torch, dev, K=50):
     prm = sch.params()
     da = adjoint.DeviceAdjoint(sch, adjoint.DesignSpace(sch), prm, None)
     try:
-        st = da.primal(sch.cold_state(prm).contiguous(), K + 5)
+        st = da.primal(sch.cold_state(prm).contiguous(), K + W)
         S, s = da.stream, da.solver
         ev = lambda: torch.cuda.Event(enable_timing=True)
 
@@ -328,18 +328,18 @@ def adjoint_timing(torch, dev, K=50):
             return a.elapsed_time(b) * 1e3 / K
 
         s.state_from_device(st[0].data_ptr())
-        for _ in range(5):
+        for _ in range(W):
             s.enqueue(1)
         primal_us = timed(lambda n: s.enqueue(1))
         lam = torch.randn_like(st[0])
-        for n in range(5):
+        for n in range(W):
             s.adjoint_step(st[n].data_ptr(), lam.data_ptr(), True)
         launches0 = s.adjoint_launch_count()
         step_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), True))
         per_step = (s.adjoint_launch_count() - launches0) // K
         q = st[K].contiguous()
         s.adjoint_step(q.data_ptr(), lam.data_ptr(), False)
-        for _ in range(5):
+        for _ in range(W):
             s.adjoint_step(q.data_ptr(), lam.data_ptr(), False, True)
         frozen_us = timed(lambda n: s.adjoint_step(q.data_ptr(), lam.data_ptr(), False, True))
         da.sensitivities()
@@ -415,6 +415,8 @@ def main():
     ap.add_argument("--case", default="nozzle_plume_1024x384")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/primal timing")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="print only the adjoint/primal timing (K = --steps, W = --warmup), for profiling")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
                     help="arithmetic of the timed path (the other one is timed too, as other_precision)")
     ap.add_argument("--single-precision-mode", action="store_true",
@@ -435,6 +437,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local))
     try:
+        if args.adjoint_only:
+            if rank == 0:
+                print(json.dumps({"adjoint": adjoint_timing(torch, local, args.steps, args.warmup)}), flush=True)
+            return
         run_ours(args, rank, world, local)
     finally:
         if world > 1:
