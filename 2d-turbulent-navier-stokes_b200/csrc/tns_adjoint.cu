@@ -58,6 +58,7 @@ TNS_ADJ_KERNEL(k_adj_diss_faces, d1_point, 1)
 TNS_ADJ_KERNEL(k_adj_diss_gather, d2_point, 1)
 TNS_ADJ_KERNEL(k_adj_dtmin, dtmin_point, 1)
 TNS_ADJ_KERNEL(k_adj_final, final_point, 1)
+TNS_ADJ_KERNEL(k_adj_centroids, centroid_point, 1)
 
 // LOCAL = 0: sum of the per-cell dt adjoints (block sums, one atomic per block).
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_dtsum(const double* __restrict__ v, long long n,
@@ -87,7 +88,7 @@ void launch_points(K kernel, const AdjArgs& a, long long n, cudaStream_t s) {
 // Device buffers and graphs of the adjoint of one handle.
 struct tns_adjoint_state {
     DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, lam, lamA, lamB, lamold, lamg, lamd, w, gbar, srcn, srcg,
-        wself, wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens;
+        wself, wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens, xcs, ycs;
     // branches of a step: the ghost gather beside the interior gather, the dissipation
     // reverse beside the viscous reverse
     cudaStream_t side[2] = {nullptr, nullptr};
@@ -119,6 +120,8 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.dt = s->dt.p;
     a.dtmin = s->dtmin.p;
     a.w = s->w.p;
+    a.xcs = s->xcs.p;
+    a.ycs = s->ycs.p;
     a.lam_old = s->lamold.p;
     a.lamg = s->lamg.p;
     a.lamd = s->lamd.p;
@@ -272,7 +275,8 @@ void adjoint_release(tns_handle* h) {
     if (s->ev) cudaEventDestroy(s->ev);
     for (auto* b : {&s->q0, &s->q1, &s->q2, &s->q3, &s->d, &s->vis, &s->dt, &s->dtmin, &s->lam, &s->lamA, &s->lamB,
                     &s->lamold, &s->lamg, &s->lamd, &s->w, &s->gbar, &s->srcn, &s->srcg, &s->wself, &s->wvisc, &s->dbar, &s->visbar,
-                    &s->dtbar, &s->dpre, &s->dout, &s->navg, &s->nbar, &s->vfi, &s->vfj, &s->dtsum, &s->sens})
+                    &s->dtbar, &s->dpre, &s->dout, &s->navg, &s->nbar, &s->vfi, &s->vfj, &s->dtsum, &s->sens, &s->xcs,
+                    &s->ycs})
         b->release();
     s->ninfo.release();
     delete s;
@@ -303,7 +307,7 @@ int tns_adjoint_enable(tns_handle* h) {
                 {&s->srcn, 16 * n}, {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad},
                 {&s->dbar, 5 * n}, {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dpre, NDPRE * n},
                 {&s->dout, NDOUT * n}, {&s->navg, NNA * nnode}, {&s->nbar, 5 * nnode}, {&s->vfi, NVF * nif},
-                {&s->vfj, NVF * njf}, {&s->dtsum, 1}, {&s->sens, s->nsens}};
+                {&s->vfj, NVF * njf}, {&s->dtsum, 1}, {&s->sens, s->nsens}, {&s->xcs, npad}, {&s->ycs, npad}};
     for (auto& r : reqs) {
         if ((rc = h->cuda(r.b->alloc((size_t)r.count), "cudaMalloc (adjoint)"))) {
             tns_rt::adjoint_release(h);
@@ -321,6 +325,8 @@ int tns_adjoint_enable(tns_handle* h) {
     cudaMemsetAsync(s->gbar.p, 0, sizeof(double) * 5 * npad, h->stream);
     cudaMemsetAsync(s->wvisc.p, 0, sizeof(double) * 5 * npad, h->stream);
     cudaMemsetAsync(s->sens.p, 0, sizeof(double) * s->nsens, h->stream);
+    const AdjArgs a = base_args(h, s, 0);
+    launch_points(k_adj_centroids, a, npad, h->stream);
     return h->cuda(cudaStreamSynchronize(h->stream), "tns_adjoint_enable");
 }
 

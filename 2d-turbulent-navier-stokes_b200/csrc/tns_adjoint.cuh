@@ -63,6 +63,8 @@ struct AdjArgs {
     const double* dtmin;  // global time step [1] (LOCAL = 0)
     double alpha;
     double* w;            // field set of the stage input [NWROW][npad]
+    double* xcs;          // centroids of the cells and ghosts on the halo grid [npad]
+    double* ycs;          //   (fixed geometry: filled once by centroid_point)
     // adjoint state
     const double* lam_in;  // adjoint of the stage output [5][ncell]
     double* lam_out;       // adjoint of the stage input (stages 2-4) [5][ncell]
@@ -136,8 +138,8 @@ TNS_HD void cell_geo(const AdjArgs& a, int i, int j, CellGeo& g) {
     g.vol = cell_volume(a.P.iaxis, g.X, g.Y, g.yc);
 }
 
-// Centroid of a cell or of a ghost (mirrored, geometry.f90:114-142).
-TNS_HD void slot_centroid(const AdjArgs& a, int i, int j, double& xc, double& yc) {
+// Centroid of a cell or of a ghost (mirrored, geometry.f90:114-142), from the nodes.
+TNS_HD void slot_centroid_nodes(const AdjArgs& a, int i, int j, double& xc, double& yc) {
     if (is_cell(a, i, j)) {
         const long long nw = a.nj + 1, n1 = (long long)i * nw + j;
         xc = (a.M.x[n1] + a.M.x[n1 + nw] + a.M.x[n1 + nw + 1] + a.M.x[n1 + 1]) * 0.25;
@@ -149,6 +151,23 @@ TNS_HD void slot_centroid(const AdjArgs& a, int i, int j, double& xc, double& yc
         xc = a.M.gxc[g];
         yc = a.M.gyc[g];
     }
+}
+
+// Fills the halo-grid centroid table (corners zero); run once per handle.
+TNS_HD void centroid_point(const AdjArgs& a, long long ps) {
+    const int i = (int)(ps / (a.nj + 2)) - 1, j = (int)(ps % (a.nj + 2)) - 1;
+    int along = 0;
+    double xc = 0.0, yc = 0.0;
+    if (is_cell(a, i, j) || ghost_side(a, i, j, along)) slot_centroid_nodes(a, i, j, xc, yc);
+    a.xcs[ps] = xc;
+    a.ycs[ps] = yc;
+}
+
+// Centroid of a cell or ghost from the table.
+TNS_HD void slot_centroid(const AdjArgs& a, int i, int j, double& xc, double& yc) {
+    const long long ps = padi(a, i, j);
+    xc = a.xcs[ps];
+    yc = a.ycs[ps];
 }
 
 // ------------------------------------------------------------------ forward field set

@@ -40,7 +40,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
         gbar(5 * a.npad, 0.0),
         srcn(16 * n), srcg(8 * n), wself(5 * n), wvisc(5 * a.npad, 0.0), dbar(5 * n), visbar(4 * n), dtbar(n),
         dpre(NDPRE * n), dout(NDOUT * n), navg(NNA * a.nnode), nbar(5 * a.nnode), vfi(NVF * a.nif),
-        vfj(NVF * a.njf);
+        vfj(NVF * a.njf), xcs(a.npad), ycs(a.npad);
     std::vector<int> ninfo(a.nnode);
     double dts = 0.0;
     a.qold = q0;
@@ -49,6 +49,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.dt = DT;
     a.dtmin = &dtmin;
     a.w = w.data();
+    a.xcs = xcs.data();
+    a.ycs = ycs.data();
     a.lam_old = lamold.data();
     a.lamg = lamg.data();
     a.lamd = lamd.data();
@@ -82,6 +84,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.rtoln = sp; sp += a.nnode;
     a.t0bar = sp; sp += n;
     a.s0bar = sp;
+    for (long long p = 0; p < a.npad; p++) centroid_point(a, p);
     const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
     const double* qs[4] = {q0, q1, q2, q3};
     double* lam_stage[5] = {nullptr, lamA.data(), lamB.data(), lamA.data(), lam};  // adjoint of Q_k
