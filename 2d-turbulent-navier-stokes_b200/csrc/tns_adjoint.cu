@@ -59,6 +59,7 @@ TNS_ADJ_KERNEL(k_adj_diss_gather, d2_point, 1)
 TNS_ADJ_KERNEL(k_adj_dtmin, dtmin_point, 1)
 TNS_ADJ_KERNEL(k_adj_final, final_point, 1)
 TNS_ADJ_KERNEL(k_adj_centroids, centroid_point, 1)
+TNS_ADJ_KERNEL(k_adj_geo, geo_point, 1)
 
 // LOCAL = 0: sum of the per-cell dt adjoints (block sums, one atomic per block).
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_dtsum(const double* __restrict__ v, long long n,
@@ -91,7 +92,7 @@ struct tns_adjoint_state {
         wself, wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens, xcs, ycs;
     // branches of a step: the ghost gather beside the interior gather, the dissipation
     // reverse beside the viscous reverse
-    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev = nullptr;
     DevBuf<int> ninfo;
     long long nsens = 0;
@@ -126,6 +127,8 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.lamg = s->lamg.p;
     a.lamd = s->lamd.p;
     a.gbar = s->gbar.p;
+    a.gbar4 = s->gbar.p;
+    a.w4 = s->w.p;
     a.srcn = s->srcn.p;
     a.srcg = s->srcg.p;
     a.wself = s->wself.p;
@@ -205,6 +208,7 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
         a.lam_in = lam_stage[k + 1];
         a.lam_out = lam_stage[k];
         a.w = s->w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
+        a.gbar = s->gbar.p + (size_t)k * 5 * a.npad;  // one residual adjoint per stage
         if (!frozen) {
             launch_points(k_adj_fields, a, a.npad, st);
             nl++;
@@ -233,6 +237,12 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
                 nl++;
             }
             launch_points(k_adj_faces, a, a.nif + a.njf, st);
+            if (geo) {
+                // face-vector sensitivities of the whole step on their own branch
+                fork(s->side[2]);
+                launch_points(k_adj_geo, a, a.ncell, s->side[2]);
+                nl++;
+            }
             launch_points(k_adj_node_bar, a, a.nnode, st);
             launch_points(k_adj_slot_bar, a, a.npad, st);
             nl += 3;
@@ -244,6 +254,7 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
         join(s->side[1]);
     }
     join(s->side[0]);
+    if (geo) join(s->side[2]);
     a.lam_out = s->lam.p;
     launch_points(k_adj_final, a, a.ncell, st);
     nl++;
@@ -303,7 +314,7 @@ int tns_adjoint_enable(tns_handle* h) {
     } reqs[] = {{&s->q0, 5 * n}, {&s->q1, 5 * n}, {&s->q2, 5 * n}, {&s->q3, 5 * n}, {&s->d, 5 * n},
                 {&s->vis, 4 * n}, {&s->dt, n}, {&s->dtmin, 1}, {&s->lam, 5 * n}, {&s->lamA, 5 * n},
                 {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->lamg, 5 * n}, {&s->lamd, 5 * n},
-                {&s->w, 4 * NWROW * npad}, {&s->gbar, 5 * npad},
+                {&s->w, 4 * NWROW * npad}, {&s->gbar, 4 * 5 * npad},
                 {&s->srcn, 16 * n}, {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad},
                 {&s->dbar, 5 * n}, {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dpre, NDPRE * n},
                 {&s->dout, NDOUT * n}, {&s->navg, NNA * nnode}, {&s->nbar, 5 * nnode}, {&s->vfi, NVF * nif},
@@ -317,12 +328,13 @@ int tns_adjoint_enable(tns_handle* h) {
     if ((rc = h->cuda(s->ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)")) ||
         (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[0], cudaStreamNonBlocking), "cudaStreamCreate")) ||
         (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[1], cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[2], cudaStreamNonBlocking), "cudaStreamCreate")) ||
         (rc = h->cuda(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate"))) {
         tns_rt::adjoint_release(h);
         return rc;
     }
     // the ghost ring of the residual adjoint stays zero; the sensitivities start at zero
-    cudaMemsetAsync(s->gbar.p, 0, sizeof(double) * 5 * npad, h->stream);
+    cudaMemsetAsync(s->gbar.p, 0, sizeof(double) * 4 * 5 * npad, h->stream);
     cudaMemsetAsync(s->wvisc.p, 0, sizeof(double) * 5 * npad, h->stream);
     cudaMemsetAsync(s->sens.p, 0, sizeof(double) * s->nsens, h->stream);
     const AdjArgs a = base_args(h, s, 0);

@@ -71,7 +71,9 @@ struct AdjArgs {
     double* lam_old;       // adjoint of Q_n, residual / source / viscous parts [5][ncell]
     double* lamg;          // ghost part of the last stage gather, boundary band [5][ncell]
     double* lamd;          // dissipation and time-step part of the adjoint of Q_n [5][ncell]
-    double* gbar;          // adjoint of the residual [5][npad], ghost ring zero
+    double* gbar;          // adjoint of the residual of this stage [5][npad], ghost ring zero
+    double* gbar4;         // the four stages' residual adjoints [4][5][npad] (stage k at k)
+    double* w4;            // the four stages' field sets [4][NWROW][npad]
     double* srcn;          // source adjoint to neighbour k: u v C1 C5 [4][4][ncell]
     double* srcg;          // source adjoint to neighbour k's centroid x y [4][2][ncell]
     double* wself;         // source adjoint to the cell itself: T P V C1 C5 [5][ncell]
@@ -657,16 +659,7 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
         a.srcg[(k * 2 + 0) * a.ncell + cell] = b.nx[k];
         a.srcg[(k * 2 + 1) * a.ncell + cell] = b.ny[k];
     }
-    if (a.geo) {
-        for (int k = 0; k < 4; k++) {
-            double sxb = 0.0, syb = 0.0;
-            for (int m = 0; m < 5; m++) {
-                sxb += 0.5 * gb[m] * (wv(a, WF + m, ps) + wv(a, WF + m, pn[k]));
-                syb += 0.5 * gb[m] * (wv(a, WG + m, ps) + wv(a, WG + m, pn[k]));
-            }
-            a.sxbar[k * a.ncell + cell] += sxb;
-            a.sybar[k * a.ncell + cell] += syb;
-        }
+    if (a.geo) {  // (the face-vector part of the residual reverse: geo_point)
         a.volbar[cell] += volb;
         a.ycbar[ps] += b.ycc;
         a.rtolc[cell] += rtolb;
@@ -1149,8 +1142,7 @@ TNS_HD void v2_point(const AdjArgs& a, long long node) {
 }
 
 // Viscous adjoint of one halo slot (cell or ghost): its face parts and its share of the
-// node averages at its corners, as adjoints of its U, V, T, C1, C5 rows.  For cells, also
-// the face-vector sensitivities of its four faces.
+// node averages at its corners, as adjoints of its U, V, T, C1, C5 rows.
 TNS_HD void v3_point(const AdjArgs& a, long long ps) {
     const int pi = (int)(ps / (a.nj + 2)) - 1, pj = (int)(ps % (a.nj + 2)) - 1;
     int along = 0;
@@ -1194,23 +1186,6 @@ TNS_HD void v3_point(const AdjArgs& a, long long ps) {
     if (a.geo) {
         a.xcbar[ps] += xb;
         a.ycbar[ps] += yb;
-        if (cell) {
-            const long long c = cell_of(a, pi, pj);
-            // faces 1..4 of the cell: j-face (i, j), i-face (i+1, j), j-face (i, j+1), i-face (i, j)
-            const double* fb[4] = {a.vfj + ((long long)pi * (a.nj + 1) + pj), a.vfi + ((long long)(pi + 1) * a.nj + pj),
-                                   a.vfj + ((long long)pi * (a.nj + 1) + pj + 1), a.vfi + ((long long)pi * a.nj + pj)};
-            const long long st[4] = {a.njf, a.nif, a.njf, a.nif};
-            for (int k = 0; k < 4; k++) {
-                double sxb = 0.0, syb = 0.0;
-                for (int q = 0; q < 4; q++) {
-                    const double vb = a.visbar[q * a.ncell + c];
-                    sxb += vb * fb[k][(VF_CX + q) * st[k]];
-                    syb += vb * fb[k][(VF_CY + q) * st[k]];
-                }
-                a.sxbar[k * a.ncell + c] += sxb;
-                a.sybar[k * a.ncell + c] += syb;
-            }
-        }
     }
 }
 
@@ -1445,6 +1420,43 @@ TNS_HD void dtmin_point(const AdjArgs& a, long long cell) {
     if (a.geo) a.dlbar[cell] += dlb;
 }
 
+
+// Face-vector sensitivities of one cell for the step: the residual's (stages 1-4,
+// SX_k_bar += 1/2 sum_m R_m_bar (F_m + F_m of neighbour k), likewise G and SY) and the
+// viscous flux's (VIS_bar of the cell times dF/dSX, dF/dSY of each face, which both
+// sides of a face share).  Runs once per step, beside the rest of the stage-1 reverse.
+TNS_HD void geo_point(const AdjArgs& a, long long cell) {
+    const int i = (int)(cell / a.nj), j = (int)(cell % a.nj);
+    const long long ps = padi(a, i, j);
+    double sxb[4] = {0.0, 0.0, 0.0, 0.0}, syb[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int st = 0; st < 4; st++) {
+        const double* gb = a.gbar4 + (size_t)st * 5 * a.npad;
+        const double* w = a.w4 + (size_t)st * NWROW * a.npad;
+        for (int m = 0; m < 5; m++) {
+            const double g = 0.5 * gb[m * a.npad + ps];
+            const double F = w[(WF + m) * a.npad + ps], G = w[(WG + m) * a.npad + ps];
+            for (int k = 0; k < 4; k++) {
+                const long long pn = padi(a, i + di_of(k), j + dj_of(k));
+                sxb[k] += g * (F + w[(WF + m) * a.npad + pn]);
+                syb[k] += g * (G + w[(WG + m) * a.npad + pn]);
+            }
+        }
+    }
+    // faces 1..4 of the cell: j-face (i, j), i-face (i+1, j), j-face (i, j+1), i-face (i, j)
+    const double* fb[4] = {a.vfj + ((long long)i * (a.nj + 1) + j), a.vfi + ((long long)(i + 1) * a.nj + j),
+                           a.vfj + ((long long)i * (a.nj + 1) + j + 1), a.vfi + ((long long)i * a.nj + j)};
+    const long long stv[4] = {a.njf, a.nif, a.njf, a.nif};
+    for (int k = 0; k < 4; k++)
+        for (int q = 0; q < 4; q++) {
+            const double vb = a.visbar[q * a.ncell + cell];
+            sxb[k] += vb * fb[k][(VF_CX + q) * stv[k]];
+            syb[k] += vb * fb[k][(VF_CY + q) * stv[k]];
+        }
+    for (int k = 0; k < 4; k++) {
+        a.sxbar[k * a.ncell + cell] += sxb[k];
+        a.sybar[k * a.ncell + cell] += syb[k];
+    }
+}
 
 // The adjoint of Q_n: residual / source / viscous part, dissipation / time-step part and
 // the ghost part of stage 1's gather.

@@ -36,8 +36,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.nif = (long long)(ni + 1) * nj;
     a.njf = (long long)ni * (nj + 1);
     const long long n = a.ncell;
-    std::vector<double> w(NWROW * a.npad), lamA(5 * n), lamB(5 * n), lamold(5 * n), lamg(5 * n), lamd(5 * n),
-        gbar(5 * a.npad, 0.0),
+    std::vector<double> w(4 * NWROW * a.npad), lamA(5 * n), lamB(5 * n), lamold(5 * n), lamg(5 * n), lamd(5 * n),
+        gbar(4 * 5 * a.npad, 0.0),
         srcn(16 * n), srcg(8 * n), wself(5 * n), wvisc(5 * a.npad, 0.0), dbar(5 * n), visbar(4 * n), dtbar(n),
         dpre(NDPRE * n), dout(NDOUT * n), navg(NNA * a.nnode), nbar(5 * a.nnode), vfi(NVF * a.nif),
         vfj(NVF * a.njf), xcs(a.npad), ycs(a.npad);
@@ -54,7 +54,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.lam_old = lamold.data();
     a.lamg = lamg.data();
     a.lamd = lamd.data();
-    a.gbar = gbar.data();
+    a.gbar4 = gbar.data();
+    a.w4 = w.data();
     a.srcn = srcn.data();
     a.srcg = srcg.data();
     a.wself = wself.data();
@@ -95,6 +96,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
         a.stage1 = st == 0;
         a.lam_in = lam_stage[st + 1];
         a.lam_out = lam_stage[st];
+        a.w = w.data() + (size_t)st * NWROW * a.npad;
+        a.gbar = gbar.data() + (size_t)st * 5 * a.npad;
         for (long long p = 0; p < a.npad; p++) s0_point(a, p);
         for (long long c = 0; c < n; c++) s1_point(a, c);
         if (st == 0) {
@@ -102,6 +105,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
             for (long long f = 0; f < a.nif + a.njf; f++) v1_point(a, f);
             for (long long k = 0; k < a.nnode; k++) v2_point(a, k);
             for (long long p = 0; p < a.npad; p++) v3_point(a, p);
+            if (geo)
+                for (long long c = 0; c < n; c++) geo_point(a, c);
         }
         for (long long c = 0; c < n; c++) s3_point(a, c);
         for (long long c = 0; c < band_count(a); c++) s3g_point(a, c);
