@@ -86,26 +86,42 @@ void launch_points(K kernel, const AdjArgs& a, long long n, cudaStream_t s) {
 
 }  // namespace
 
+// The forward values of one state (checkpoint): stage inputs, D, VIS, DT, the four
+// stages' field sets, node averages and the dissipation pre-pass.  Two sets, so that
+// the next checkpoint's forward values are computed while this one's reverse runs.
+struct AdjForward {
+    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, w, navg, dpre;
+    DevBuf<int> ninfo;
+};
+
 // Device buffers and graphs of the adjoint of one handle.
 struct tns_adjoint_state {
-    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, lam, lamA, lamB, lamold, lamg, lamd, w, gbar, srcn, srcg,
-        wself, wvisc, dbar, visbar, dtbar, dpre, dout, navg, nbar, vfi, vfj, dtsum, sens, xcs, ycs;
-    // branches of a step: the ghost gather beside the interior gather, the dissipation
-    // reverse beside the viscous reverse
-    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t ev = nullptr;
-    DevBuf<int> ninfo;
+    AdjForward set[2];
+    int cur = 0;                         // the set of the last step's state
+    bool have_forward = false;           // set[cur] holds forward values
+    int pre_set = -1;                    // a set prefetched by the last step ...
+    const double* pre_ptr = nullptr;     // ... for the state at this device address
+    DevBuf<double> lam, lamA, lamB, lamold, lamg, lamd, gbar, srcn, srcg, wself, wvisc, dbar, visbar, dtbar, dout,
+        nbar, vfi, vfj, dtsum, sens, xcs, ycs;
     long long nsens = 0;
-    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};  // [frozen][sensitivities]
-    long long per_step[4] = {0, 0, 0, 0};
-    bool have_forward = false;  // the buffers hold the forward values of the last state
+    // branches of a step: dissipation reverse, ghost gather, face-vector sensitivities,
+    // forward values of the next checkpoint
+    cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
+    // the reverse runs on high-priority streams (main + side 0-2), the prefetch branch on
+    // the lowest priority, so that the reverse -- the critical path -- keeps its SMs
+    cudaStream_t hp = nullptr;
+    cudaEvent_t ev = nullptr;
+    // [set][mode: bit 0 forward first, bit 1 prefetch the other set][sensitivities]
+    cudaGraphExec_t graph[2][4][2] = {};
+    long long per_step[2][4][2] = {};
     long long launches = 0;
 };
 
 namespace {
 
-AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
+AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int set, int geo) {
     AdjArgs a{};
+    const AdjForward& f = s->set[set];
     a.P = h->P;
     a.M = h->M;
     a.ni = h->ni;
@@ -115,12 +131,16 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.nnode = (long long)(h->ni + 1) * (h->nj + 1);
     a.nif = (long long)(h->ni + 1) * h->nj;
     a.njf = (long long)h->ni * (h->nj + 1);
-    a.qold = s->q0.p;
-    a.d = s->d.p;
-    a.vis = s->vis.p;
-    a.dt = s->dt.p;
-    a.dtmin = s->dtmin.p;
-    a.w = s->w.p;
+    a.qold = f.q0.p;
+    a.d = f.d.p;
+    a.vis = f.vis.p;
+    a.dt = f.dt.p;
+    a.dtmin = f.dtmin.p;
+    a.w = f.w.p;
+    a.w4 = f.w.p;
+    a.navg = f.navg.p;
+    a.ninfo = f.ninfo.p;
+    a.dpre = f.dpre.p;
     a.xcs = s->xcs.p;
     a.ycs = s->ycs.p;
     a.lam_old = s->lamold.p;
@@ -128,7 +148,6 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.lamd = s->lamd.p;
     a.gbar = s->gbar.p;
     a.gbar4 = s->gbar.p;
-    a.w4 = s->w.p;
     a.srcn = s->srcn.p;
     a.srcg = s->srcg.p;
     a.wself = s->wself.p;
@@ -136,10 +155,7 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int geo) {
     a.dbar = s->dbar.p;
     a.visbar = s->visbar.p;
     a.dtbar = s->dtbar.p;
-    a.dpre = s->dpre.p;
     a.dout = s->dout.p;
-    a.navg = s->navg.p;
-    a.ninfo = s->ninfo.p;
     a.nbar = s->nbar.p;
     a.vfi = s->vfi.p;
     a.vfj = s->vfj.p;
@@ -166,31 +182,46 @@ long long sens_size(long long n, long long npad, long long nnode) {
     return 8 * n + 2 * n + 2 * npad + 2 * nnode + n + nnode + 2 * n;
 }
 
-// One reverse step, enqueued on stream st: recompute from q0, reverse into lamold, copy
-// the result to lam.  With `frozen` the forward values of the previous step's state are
-// reused: no recompute, no field sets, node averages or dissipation pre-pass.  Returns
-// the number of kernels launched.
-long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen, cudaStream_t st) {
+const double kAlpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
+
+// Forward values of the state in set `set` (its q0), on stream st: the iteration with the
+// solver's kernels (stages 1-3 keep their outputs), then every pass of the reverse that
+// depends on the state alone.  Returns the number of kernels launched.
+long long enqueue_forward(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
     const Params& P = h->P;
     const Mesh& M = h->M;
+    AdjForward& f = s->set[set];
     long long nl = 0;
-    static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
-    double* qs[4] = {s->q0.p, s->q1.p, s->q2.p, s->q3.p};
-    if (!frozen) {
-        // forward recompute with the solver's kernels
-        if (!P.local) {
-            tns::launch_dtmin(P, M, s->q0.p, h->partial.p, h->counter.p, s->dtmin.p, st);
-            nl++;
-        }
-        tns::launch_dissipation(P, M, s->q0.p, s->d.p, s->dt.p, s->dtmin.p, st);
-        tns::launch_viscous(P, M, s->q0.p, s->vis.p, st);
-        for (int k = 0; k < 3; k++)
-            tns::launch_stage(P, M, qs[k], s->q0.p, qs[k + 1], s->d.p, s->vis.p, s->dt.p, s->dtmin.p, alpha[k],
-                              nullptr, nullptr, st);
-        nl += 5;
+    if (!P.local) {
+        tns::launch_dtmin(P, M, f.q0.p, h->partial.p, h->counter.p, f.dtmin.p, st);
+        nl++;
     }
-    // reverse
-    AdjArgs a = base_args(h, s, geo);
+    tns::launch_dissipation(P, M, f.q0.p, f.d.p, f.dt.p, f.dtmin.p, st);
+    tns::launch_viscous(P, M, f.q0.p, f.vis.p, st);
+    double* qs[4] = {f.q0.p, f.q1.p, f.q2.p, f.q3.p};
+    for (int k = 0; k < 3; k++)
+        tns::launch_stage(P, M, qs[k], f.q0.p, qs[k + 1], f.d.p, f.vis.p, f.dt.p, f.dtmin.p, kAlpha[k], nullptr,
+                          nullptr, st);
+    nl += 5;
+    AdjArgs a = base_args(h, s, set, 0);
+    for (int k = 0; k < 4; k++) {
+        a.qin = qs[k];
+        a.w = f.w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
+        launch_points(k_adj_fields, a, a.npad, st);
+    }
+    a.w = f.w.p;
+    launch_points(k_adj_nodes, a, a.nnode, st);
+    launch_points(k_adj_diss_pre, a, a.ncell, st);
+    return nl + 6;
+}
+
+// The reverse of the iteration whose forward values are in set `set`: lambda (s->lam)
+// -> lambda dG/dQ_n, written back to s->lam.
+long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo, cudaStream_t st) {
+    const Params& P = h->P;
+    AdjForward& f = s->set[set];
+    long long nl = 0;
+    AdjArgs a = base_args(h, s, set, geo);
     auto fork = [&](cudaStream_t to) {
         cudaEventRecord(s->ev, st);
         cudaStreamWaitEvent(to, s->ev, 0);
@@ -199,29 +230,22 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
         cudaEventRecord(s->ev, from);
         cudaStreamWaitEvent(st, s->ev, 0);
     };
+    double* qs[4] = {f.q0.p, f.q1.p, f.q2.p, f.q3.p};
     double* lam_stage[5] = {nullptr, s->lamA.p, s->lamB.p, s->lamA.p, s->lam.p};
     for (int k = 3; k >= 0; k--) {
         a.qin = qs[k];
-        a.alpha = alpha[k];
+        a.alpha = kAlpha[k];
         a.first = k == 3;
         a.stage1 = k == 0;
         a.lam_in = lam_stage[k + 1];
         a.lam_out = lam_stage[k];
-        a.w = s->w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
+        a.w = f.w.p + (size_t)k * NWROW * a.npad;     // this stage's field set
         a.gbar = s->gbar.p + (size_t)k * 5 * a.npad;  // one residual adjoint per stage
-        if (!frozen) {
-            launch_points(k_adj_fields, a, a.npad, st);
-            nl++;
-        }
         launch_points(k_adj_stage, a, a.ncell, st);
         nl++;
         if (k == 0) {
             // dissipation / time-step reverse on a branch (it needs only D_bar, DT_bar)
             fork(s->side[0]);
-            if (!frozen) {
-                launch_points(k_adj_diss_pre, a, a.ncell, s->side[0]);
-                nl++;
-            }
             launch_points(k_adj_diss_faces, a, a.ncell, s->side[0]);
             launch_points(k_adj_diss_gather, a, a.ncell, s->side[0]);
             nl += 2;
@@ -232,10 +256,6 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
                 nl += 2;
             }
             // viscous reverse on the main stream
-            if (!frozen) {
-                launch_points(k_adj_nodes, a, a.nnode, st);
-                nl++;
-            }
             launch_points(k_adj_faces, a, a.nif + a.njf, st);
             if (geo) {
                 // face-vector sensitivities of the whole step on their own branch
@@ -257,7 +277,29 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int geo, int frozen,
     if (geo) join(s->side[2]);
     a.lam_out = s->lam.p;
     launch_points(k_adj_final, a, a.ncell, st);
-    nl++;
+    return nl + 1;
+}
+
+// One step: [forward of set X], the reverse of set X, and (mode bit 1) the forward of
+// the other set on a branch beside the reverse.
+long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int set, int mode, int geo, cudaStream_t user) {
+    long long nl = 0;
+    cudaStream_t st = s->hp;
+    cudaEventRecord(s->ev, user);
+    cudaStreamWaitEvent(st, s->ev, 0);
+    if (mode & 1) nl += enqueue_forward(h, s, set, st);
+    if (mode & 2) {
+        cudaEventRecord(s->ev, st);
+        cudaStreamWaitEvent(s->side[3], s->ev, 0);
+        nl += enqueue_forward(h, s, set ^ 1, s->side[3]);
+    }
+    nl += enqueue_reverse(h, s, set, geo, st);
+    if (mode & 2) {
+        cudaEventRecord(s->ev, s->side[3]);
+        cudaStreamWaitEvent(st, s->ev, 0);
+    }
+    cudaEventRecord(s->ev, st);
+    cudaStreamWaitEvent(user, s->ev, 0);
     return nl;
 }
 
@@ -276,20 +318,29 @@ namespace tns_rt {
 void adjoint_release(tns_handle* h) {
     tns_adjoint_state* s = h->adj;
     if (!s) return;
-    for (auto& g : s->graph)
-        if (g) cudaGraphExecDestroy(g);
+    for (auto& a : s->graph)
+        for (auto& b : a)
+            for (auto& g : b)
+                if (g) cudaGraphExecDestroy(g);
     for (auto& x : s->side)
         if (x) {
             cudaStreamSynchronize(x);
             cudaStreamDestroy(x);
         }
+    if (s->hp) {
+        cudaStreamSynchronize(s->hp);
+        cudaStreamDestroy(s->hp);
+    }
     if (s->ev) cudaEventDestroy(s->ev);
-    for (auto* b : {&s->q0, &s->q1, &s->q2, &s->q3, &s->d, &s->vis, &s->dt, &s->dtmin, &s->lam, &s->lamA, &s->lamB,
-                    &s->lamold, &s->lamg, &s->lamd, &s->w, &s->gbar, &s->srcn, &s->srcg, &s->wself, &s->wvisc, &s->dbar, &s->visbar,
-                    &s->dtbar, &s->dpre, &s->dout, &s->navg, &s->nbar, &s->vfi, &s->vfj, &s->dtsum, &s->sens, &s->xcs,
-                    &s->ycs})
+    for (auto& f : s->set) {
+        for (auto* b : {&f.q0, &f.q1, &f.q2, &f.q3, &f.d, &f.vis, &f.dt, &f.dtmin, &f.w, &f.navg, &f.dpre})
+            b->release();
+        f.ninfo.release();
+    }
+    for (auto* b : {&s->lam, &s->lamA, &s->lamB, &s->lamold, &s->lamg, &s->lamd, &s->gbar, &s->srcn, &s->srcg,
+                    &s->wself, &s->wvisc, &s->dbar, &s->visbar, &s->dtbar, &s->dout, &s->nbar, &s->vfi, &s->vfj,
+                    &s->dtsum, &s->sens, &s->xcs, &s->ycs})
         b->release();
-    s->ninfo.release();
     delete s;
     h->adj = nullptr;
 }
@@ -311,39 +362,50 @@ int tns_adjoint_enable(tns_handle* h) {
     struct Req {
         DevBuf<double>* b;
         long long count;
-    } reqs[] = {{&s->q0, 5 * n}, {&s->q1, 5 * n}, {&s->q2, 5 * n}, {&s->q3, 5 * n}, {&s->d, 5 * n},
-                {&s->vis, 4 * n}, {&s->dt, n}, {&s->dtmin, 1}, {&s->lam, 5 * n}, {&s->lamA, 5 * n},
-                {&s->lamB, 5 * n}, {&s->lamold, 5 * n}, {&s->lamg, 5 * n}, {&s->lamd, 5 * n},
-                {&s->w, 4 * NWROW * npad}, {&s->gbar, 4 * 5 * npad},
-                {&s->srcn, 16 * n}, {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad},
-                {&s->dbar, 5 * n}, {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dpre, NDPRE * n},
-                {&s->dout, NDOUT * n}, {&s->navg, NNA * nnode}, {&s->nbar, 5 * nnode}, {&s->vfi, NVF * nif},
-                {&s->vfj, NVF * njf}, {&s->dtsum, 1}, {&s->sens, s->nsens}, {&s->xcs, npad}, {&s->ycs, npad}};
+    };
+    std::vector<Req> reqs = {{&s->lam, 5 * n}, {&s->lamA, 5 * n}, {&s->lamB, 5 * n}, {&s->lamold, 5 * n},
+                             {&s->lamg, 5 * n}, {&s->lamd, 5 * n}, {&s->gbar, 4 * 5 * npad}, {&s->srcn, 16 * n},
+                             {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad}, {&s->dbar, 5 * n},
+                             {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dout, NDOUT * n}, {&s->nbar, 5 * nnode},
+                             {&s->vfi, NVF * nif}, {&s->vfj, NVF * njf}, {&s->dtsum, 1}, {&s->sens, s->nsens},
+                             {&s->xcs, npad}, {&s->ycs, npad}};
+    for (auto& f : s->set)
+        for (Req r : std::vector<Req>{{&f.q0, 5 * n}, {&f.q1, 5 * n}, {&f.q2, 5 * n}, {&f.q3, 5 * n},
+                                      {&f.d, 5 * n}, {&f.vis, 4 * n}, {&f.dt, n}, {&f.dtmin, 1},
+                                      {&f.w, 4 * NWROW * npad}, {&f.navg, NNA * nnode}, {&f.dpre, NDPRE * n}})
+            reqs.push_back(r);
     for (auto& r : reqs) {
         if ((rc = h->cuda(r.b->alloc((size_t)r.count), "cudaMalloc (adjoint)"))) {
             tns_rt::adjoint_release(h);
             return rc;
         }
     }
-    if ((rc = h->cuda(s->ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)")) ||
-        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[0], cudaStreamNonBlocking), "cudaStreamCreate")) ||
-        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[1], cudaStreamNonBlocking), "cudaStreamCreate")) ||
-        (rc = h->cuda(cudaStreamCreateWithFlags(&s->side[2], cudaStreamNonBlocking), "cudaStreamCreate")) ||
-        (rc = h->cuda(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate"))) {
+    rc = 0;
+    for (auto& f : s->set)
+        if (!rc) rc = h->cuda(f.ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)");
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    for (int k = 0; k < 4; k++)
+        if (!rc)
+            rc = h->cuda(cudaStreamCreateWithPriority(&s->side[k], cudaStreamNonBlocking, k == 3 ? prio_low : prio_high),
+                         "cudaStreamCreate");
+    if (!rc) rc = h->cuda(cudaStreamCreateWithPriority(&s->hp, cudaStreamNonBlocking, prio_high), "cudaStreamCreate");
+    if (!rc) rc = h->cuda(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
+    if (rc) {
         tns_rt::adjoint_release(h);
         return rc;
     }
-    // the ghost ring of the residual adjoint stays zero; the sensitivities start at zero
+    // the ghost ring of the residual adjoints stays zero; the sensitivities start at zero
     cudaMemsetAsync(s->gbar.p, 0, sizeof(double) * 4 * 5 * npad, h->stream);
     cudaMemsetAsync(s->wvisc.p, 0, sizeof(double) * 5 * npad, h->stream);
     cudaMemsetAsync(s->sens.p, 0, sizeof(double) * s->nsens, h->stream);
-    const AdjArgs a = base_args(h, s, 0);
+    const AdjArgs a = base_args(h, s, 0, 0);
     launch_points(k_adj_centroids, a, npad, h->stream);
     return h->cuda(cudaStreamSynchronize(h->stream), "tns_adjoint_enable");
 }
 
-int tns_adjoint_step(tns_handle* h, const double* d_q, double* d_lam, int flags) {
-    if (!h || !d_q || !d_lam) return TNS_ERR_ARG;
+int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_next, double* d_lam, int flags) {
+    if (!h || !d_lam || (!d_q && !(flags & TNS_ADJ_FROZEN))) return TNS_ERR_ARG;
     int rc;
     if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
     tns_adjoint_state* s = h->adj;
@@ -351,33 +413,59 @@ int tns_adjoint_step(tns_handle* h, const double* d_q, double* d_lam, int flags)
     const int frozen = flags & TNS_ADJ_FROZEN ? 1 : 0;
     if (frozen && !s->have_forward)
         return h->fail(TNS_ERR_STATE, "tns_adjoint_step: TNS_ADJ_FROZEN before any step without it");
+    if (frozen && d_q_next)
+        return h->fail(TNS_ERR_ARG, "tns_adjoint_step: TNS_ADJ_FROZEN takes no next state");
     const size_t bytes = sizeof(double) * 5 * (size_t)h->ni * h->nj;
     cudaStream_t st = h->stream;
-    if ((!frozen &&
-         (rc = h->cuda(cudaMemcpyAsync(s->q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: state in"))) ||
-        (rc = h->cuda(cudaMemcpyAsync(s->lam.p, d_lam, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: lambda in")))
+    int set = s->cur, mode = 0;
+    if (!frozen) {
+        if (s->pre_set >= 0 && s->pre_ptr == d_q) {
+            set = s->pre_set;  // prefetched by the previous step
+        } else {
+            set = s->cur;
+            mode |= 1;
+            if ((rc = h->cuda(cudaMemcpyAsync(s->set[set].q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st),
+                              "adjoint: state in")))
+                return rc;
+        }
+    }
+    if (d_q_next) {
+        mode |= 2;
+        if ((rc = h->cuda(cudaMemcpyAsync(s->set[set ^ 1].q0.p, d_q_next, bytes, cudaMemcpyDeviceToDevice, st),
+                          "adjoint: next state in")))
+            return rc;
+    }
+    if ((rc = h->cuda(cudaMemcpyAsync(s->lam.p, d_lam, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: lambda in")))
         return rc;
-    const int gi = frozen * 2 + geo;
     if (h->profile) {
-        s->launches += enqueue_step(h, s, geo, frozen, st);
+        s->launches += enqueue_step(h, s, set, mode, geo, st);
     } else {
-        if (!s->graph[gi]) {
+        cudaGraphExec_t& ge = s->graph[set][mode][geo];
+        if (!ge) {
             cudaGraph_t g;
             if ((rc = h->cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "adjoint capture")))
                 return rc;
-            s->per_step[gi] = enqueue_step(h, s, geo, frozen, st);
+            s->per_step[set][mode][geo] = enqueue_step(h, s, set, mode, geo, st);
             if ((rc = h->cuda(cudaStreamEndCapture(st, &g), "adjoint capture"))) return rc;
-            rc = h->cuda(cudaGraphInstantiate(&s->graph[gi], g, 0), "adjoint graph instantiate");
+            rc = h->cuda(cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority),
+                         "adjoint graph instantiate");
             cudaGraphDestroy(g);
             if (rc) return rc;
         }
-        if ((rc = h->cuda(cudaGraphLaunch(s->graph[gi], st), "adjoint graph launch"))) return rc;
-        s->launches += s->per_step[gi];
+        if ((rc = h->cuda(cudaGraphLaunch(ge, st), "adjoint graph launch"))) return rc;
+        s->launches += s->per_step[set][mode][geo];
     }
+    s->cur = set;
     s->have_forward = true;
+    s->pre_set = d_q_next ? (set ^ 1) : -1;
+    s->pre_ptr = d_q_next;
     if ((rc = h->cuda(cudaMemcpyAsync(d_lam, s->lam.p, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: lambda out")))
         return rc;
     return h->cuda(cudaGetLastError(), "tns_adjoint_step");
+}
+
+int tns_adjoint_step(tns_handle* h, const double* d_q, double* d_lam, int flags) {
+    return tns_adjoint_step_next(h, d_q, nullptr, d_lam, flags);
 }
 
 long long tns_adjoint_sensitivity_size(tns_handle* h) {

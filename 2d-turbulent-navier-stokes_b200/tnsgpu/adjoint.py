@@ -968,13 +968,17 @@ class DeviceAdjoint:
         self._leave()
         return states
 
-    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool, frozen: bool = False):
-        """``frozen``: q is the previous step's state (its forward values are reused)."""
-        if not (q.is_contiguous() and lam.is_contiguous() and lam.dtype == torch.float64
-                and q.dtype == torch.float64):
-            raise ValueError("q and lambda must be contiguous float64 device tensors")
+    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool, frozen: bool = False,
+             q_next: Optional[torch.Tensor] = None):
+        """``frozen``: q is the previous step's state (its forward values are reused).
+        ``q_next``: the state of the next step, whose forward values are computed beside
+        this reverse (it must stay unchanged until that step)."""
+        for t in (q, lam) + ((q_next,) if q_next is not None else ()):
+            if not (t.is_contiguous() and t.dtype == torch.float64):
+                raise ValueError("q, q_next and lambda must be contiguous float64 device tensors")
         self._enter()
-        self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities, frozen)
+        self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities, frozen,
+                                 q_next.data_ptr() if q_next is not None else None)
         self._leave()
 
     def sensitivities(self) -> Dict[str, torch.Tensor]:

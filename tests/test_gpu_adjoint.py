@@ -191,6 +191,8 @@ def test_cuda_fixed_point_adjoint_matches_torch_engine():
 
 
 def test_cuda_adjoint_step_is_deterministic():
+    """Repeated sweeps, and a sweep whose next checkpoint's forward values are computed
+    beside each reverse (tns_adjoint_step_next), give bitwise the same results."""
     mesh, flow, sch, space = _ramp(64, 24)
     prm = sch.params()
     dev = adjoint.DeviceAdjoint(sch, space, prm, None)
@@ -198,14 +200,16 @@ def test_cuda_adjoint_step_is_deterministic():
         st = dev.primal(sch.cold_state(prm).contiguous(), 12)
         lam0 = torch.tensor(np.random.default_rng(5).normal(size=(5,) + mesh.shape), device="cuda")
         outs = []
-        for _ in range(2):
+        for pipelined in (False, False, True):
             lam = lam0.clone()
             for n in range(11, -1, -1):
-                dev.step(st[n], lam, True)
-            outs.append((lam, dev.sensitivities()["vol"]))
+                dev.step(st[n], lam, True, q_next=st[n - 1] if pipelined and n > 0 else None)
+            s = dev.sensitivities()
+            outs.append((lam, s["vol"], s["sx"][2]))
     finally:
         dev.close()
-    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    for o in outs[1:]:
+        assert all(torch.equal(a, b) for a, b in zip(outs[0], o))
 
 
 def test_frozen_adjoint_steps_equal_full_steps():
