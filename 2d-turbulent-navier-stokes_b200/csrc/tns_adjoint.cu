@@ -35,6 +35,10 @@ constexpr int ADJ_THREADS = TNS_ADJ_THREADS;
         if (i < n) fn(a, i);                                                             \
     }
 
+// Stream priorities for the reverse (high) and the prefetch branch (low).
+#ifndef TNS_ADJ_PRIORITY
+#define TNS_ADJ_PRIORITY 1
+#endif
 #ifndef TNS_ADJ_STAGE_MINB
 #define TNS_ADJ_STAGE_MINB 3
 #endif
@@ -385,6 +389,9 @@ int tns_adjoint_enable(tns_handle* h) {
         if (!rc) rc = h->cuda(f.ninfo.alloc((size_t)nnode), "cudaMalloc (adjoint)");
     int prio_low = 0, prio_high = 0;
     cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+#if !TNS_ADJ_PRIORITY
+    prio_high = prio_low;
+#endif
     for (int k = 0; k < 4; k++)
         if (!rc)
             rc = h->cuda(cudaStreamCreateWithPriority(&s->side[k], cudaStreamNonBlocking, k == 3 ? prio_low : prio_high),
@@ -447,7 +454,7 @@ int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_ne
                 return rc;
             s->per_step[set][mode][geo] = enqueue_step(h, s, set, mode, geo, st);
             if ((rc = h->cuda(cudaStreamEndCapture(st, &g), "adjoint capture"))) return rc;
-            rc = h->cuda(cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority),
+            rc = h->cuda(cudaGraphInstantiateWithFlags(&ge, g, TNS_ADJ_PRIORITY ? cudaGraphInstantiateFlagUseNodePriority : 0),
                          "adjoint graph instantiate");
             cudaGraphDestroy(g);
             if (rc) return rc;
