@@ -312,7 +312,8 @@ int check_mesh(tns_handle* h) {
     if (!h->identity) return h->fail(TNS_ERR_ARG, "the adjoint needs cells numbered in (i, j) order");
     if (h->ni < 3 || h->nj < 3) return h->fail(TNS_ERR_ARG, "the adjoint needs at least 3 x 3 cells");
     for (int t : h->hgtype)
-        if (t < 2 || t > 5) return h->fail(TNS_ERR_ARG, "BC type %d: the adjoint covers types 2-5", t);
+        if (t < 2 || t > 7 || t == 6)
+            return h->fail(TNS_ERR_ARG, "BC type %d: the adjoint covers types 2-5 and 7", t);
     return TNS_OK;
 }
 

@@ -1,4 +1,4 @@
-// tns_adjoint.cuh -- discrete adjoint of one RK4 iteration (BC types 2-5, FP64).
+// tns_adjoint.cuh -- discrete adjoint of one RK4 iteration (BC types 2-5 and 7, FP64).
 //
 // Given lambda_{n+1} = dJ/dQ_{n+1}, the reverse step returns lambda_n = lambda_{n+1}
 // dG/dQ_n for the iteration map Q_{n+1} = G(Q_n) of turbnstwod.f90:95-146, and (on
@@ -12,7 +12,7 @@
 //   ghost back-propagation     boundary.f90:53-122       (s3g_point)
 //   source terms               source_terms.f90:24-104   (src_forward / src_reverse)
 //   primitive variables        turbnstwod.f90:204-227    (prim_adj)
-//   ghost states 2..5          boundary.f90:53-122       (ghost_adj)
+//   ghost states 2..5, 7       boundary.f90:53-122,310-327 (ghost_adj)
 //   viscous flux               viscous.f90:29-217        (v0..v3_point, visc_face_adj)
 //   JST dissipation            solver_state.f90:70-225   (d0..d2_point)
 //   time step (LOCAL 0/1)      turbnstwod.f90:97-114     (ts_adj, dtmin_point)
@@ -194,7 +194,8 @@ TNS_HD void s0_point(const AdjArgs& a, long long ps) {
             const int k = side - 1;
             const int pi = i - di_of(k), pj = j - dj_of(k);
             const long long pc = cell_of(a, pi, pj), oc = cell_of(a, pi - di_of(k), pj - dj_of(k));
-            const int type = a.M.gtype[a.M.ghost_index(side, along)];
+            const int gidx = a.M.ghost_index(side, along);
+            const int type = a.M.gtype[gidx];
             Prim par, opp;
             primitive(a.P, a.qin[pc], a.qin[a.ncell + pc], a.qin[2 * a.ncell + pc], a.qin[3 * a.ncell + pc],
                       a.qin[4 * a.ncell + pc], par);
@@ -203,7 +204,7 @@ TNS_HD void s0_point(const AdjArgs& a, long long ps) {
                           a.qin[4 * a.ncell + oc], opp);
             else
                 opp = par;
-            boundary_ghost(a.P, type, par, opp, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, p);
+            boundary_ghost(a.P, type, par, opp, 0.0, 0.0, a.M.gyc[gidx], 0.0, 0.0, 1.0, p);
             row[WC1] = p.rho;
             row[WC5] = p.c5;
         }
@@ -275,13 +276,15 @@ TNS_HD void tail_adj(const Params& P, double rho, double u, double v, double t, 
     vb += c3b * rho;
 }
 
-// Reverse of APPLY_BOUNDARY for one ghost of type 2..5 (boundary.f90:53-122).  gw, pw,
-// ow: field-set rows of the ghost, its parent and the parent's opposite neighbour; gb:
-// the ghost's row adjoint.  Adds to the parent's rows (pb), the opposite cell's U V T P
-// (ob) and, for the type-2 inlet, to the adjoints of T0 and S0.
+// Reverse of APPLY_BOUNDARY for one ghost of type 2..5 or 7 (boundary.f90:53-122,
+// 310-327).  gw, pw, ow: field-set rows of the ghost, its parent and the parent's opposite
+// neighbour; gb: the ghost's row adjoint; ycg: the ghost's mirrored centroid y.  Adds to
+// the parent's rows (pb), the opposite cell's U V T P (ob), the adjoints of T0 and S0
+// (type-2 inlet; type 7 through TINF and the profile velocity, both set by T0) and of
+// the ghost's centroid y (type 7).
 TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const double pw[NWROW],
                       const double ow[NWROW], const double gb[NWROW], double pb[NWROW], double ob[NWROW],
-                      double& t0b, double& s0b) {
+                      double& t0b, double& s0b, double ycg, double& ygb) {
     if (type == 5) {
         pb[WU] -= gb[WU];
         pb[WV] -= gb[WV];
@@ -325,6 +328,25 @@ TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const d
         const double xb = ub * sgn(2.0 * pw[WU] - ow[WU]);
         pb[WU] += 2.0 * xb;
         ob[WU] -= xb;
+    } else if (type == 7) {  // boundary-layer inlet: P = PINF, T = TINF, U from the 1/7 profile
+        const double c5 = gw[WC5];
+        const double c5b = gb[WC5] + gb[WF + 4] * u + gb[WG + 4] * v;
+        ub += gb[WF + 4] * c5;
+        vb += gb[WG + 4] * c5;
+        const double amu = amu_of(P, t);
+        tb += c5b * 0.6 * amu / t;  // C5 = RHO * (AMU(T) / RHO)
+        tb -= rhob * rho / t;       // RHO = PINF / (RR T)
+        // U = BL_U (YCC/DELTABL)**(1/7) - U_parent (BL_U - U_parent above the layer)
+        double blub = ub;
+        if (ycg <= P.deltabl) {
+            const double r = ycg / P.deltabl, f = pow(r, P.bl_exp);
+            blub = ub * f;
+            if (r > 0.0) ygb += ub * P.bl_u * P.bl_exp * f / r / P.deltabl;
+        }
+        pb[WU] -= ub;
+        pb[WV] -= vb;
+        // TINF = T0 / (1 + (GAMA-1)/2 AMINF^2) and BL_U = 2 AMINF sqrt(GAMA RR TINF)
+        t0b += tb * P.tinf / P.t0 + blub * P.bl_u / (2.0 * P.t0);
     } else {  // type 2: subsonic inlet at P0, T0
         const double c5 = gw[WC5];
         double c5b = gb[WC5] + gb[WF + 4] * u + gb[WG + 4] * v;
@@ -805,10 +827,11 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         else load_rows(a, ps, ow);
         double dummy[NWROW];
         for (int r = 0; r < NWROW; r++) dummy[r] = 0.0;
-        ghost_adj(a.P, type, gw, pw, ow, gb, wb, dummy, t0b, s0b);
+        double ygb = 0.0;
+        ghost_adj(a.P, type, gw, pw, ow, gb, wb, dummy, t0b, s0b, a.M.gyc[a.M.ghost_index(side, along)], ygb);
         if (a.geo) {
             a.xcbar[gps] += a.srcg[(k * 2 + 0) * a.ncell + cell];
-            a.ycbar[gps] += a.srcg[(k * 2 + 1) * a.ncell + cell];
+            a.ycbar[gps] += a.srcg[(k * 2 + 1) * a.ncell + cell] + ygb;
         }
     }
     for (int k = 0; k < 4; k++) {
@@ -828,8 +851,8 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         load_rows(a, pps, par);
         load_rows(a, gps, gw);
         for (int r = 0; r < NWROW; r++) pbd[r] = obar[r] = 0.0;
-        double t0d = 0.0, s0d = 0.0;
-        ghost_adj(a.P, 3, gw, par, pw, gb, pbd, obar, t0d, s0d);
+        double t0d = 0.0, s0d = 0.0, ygd = 0.0;
+        ghost_adj(a.P, 3, gw, par, pw, gb, pbd, obar, t0d, s0d, 0.0, ygd);
         wb[WU] += obar[WU];
         wb[WV] += obar[WV];
         wb[WT] += obar[WT];

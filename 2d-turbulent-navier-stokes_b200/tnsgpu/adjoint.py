@@ -22,8 +22,8 @@ cold-start Mach number AMACHINIT and mesh-node coordinates (wall shape):
 * ``fixed_point_adjoint`` iterates lambda <- dJ/dQ + lambda dG/dQ at a frozen state, the
   adjoint of a converged steady solution.
 
-Scope: IAXIS 0 and 1, BC types 2, 3, 4 and 5 (the types of the ramp and nozzle cases),
-any LOCAL and NPSEUDO.  Type 6 (injection port) and 7 (boundary-layer inflow) raise
+Scope: IAXIS 0 and 1, BC types 2, 3, 4, 5 and 7 (boundary-layer inflow), any LOCAL and
+NPSEUDO.  Type 6 (injection port, whose ghosts sum the port column) raises
 NotImplementedError.  Objective helpers evaluate on the final state Q_N with its ghost
 cells from APPLY_BOUNDARY: the wall pressure force and the mass-weighted total-pressure
 loss between two sides.
@@ -140,9 +140,9 @@ class Scheme:
                            (ii + 1) * (nj + 1) + jj + 2, ii * (nj + 1) + jj + 2], -1).reshape(-1, 4)
         if not np.array_equal(mesh.nod, expect):
             raise ValueError("mesh is not in structured (i, j) numbering")
-        if np.any((mesh.ntype < 2) | (mesh.ntype > 5)):
-            bad = sorted(set(mesh.ntype.tolist()) - {2, 3, 4, 5})
-            raise NotImplementedError(f"BC types {bad}: the adjoint covers types 2-5")
+        if np.any((mesh.ntype < 2) | (mesh.ntype > 7) | (mesh.ntype == 6)):
+            bad = sorted(set(mesh.ntype.tolist()) - {2, 3, 4, 5, 7})
+            raise NotImplementedError(f"BC types {bad}: the adjoint covers types 2-5 and 7")
         if flow.iaxis not in (0, 1):
             raise ValueError("IAXIS must be 0 or 1")
         self.fixed_rinit = rinit
@@ -306,11 +306,12 @@ class Scheme:
                             C[1], rho * u * u + p, f2, (C[3] + p) * u, rho * rt * u,
                             C[2], f2, rho * v * v + p, (C[3] + p) * v, rho * rt * v])
 
-    def _ghosts(self, pr, opp, prm: Params):
-        """APPLY_BOUNDARY (boundary.f90:53-122) for every ghost of the ring at once:
-        parent field set ``pr`` [19, NG] and U, V, T, P of the cell opposite the
-        boundary face ``opp`` [4, NG].  Each BC type present in the mesh is evaluated
-        on the whole ring and selected by the ghost's type."""
+    def _ghosts(self, pr, opp, prm: Params, ycg=None):
+        """APPLY_BOUNDARY (boundary.f90:53-122, 310-327) for every ghost of the ring at
+        once: parent field set ``pr`` [19, NG] and U, V, T, P of the cell opposite the
+        boundary face ``opp`` [4, NG]; ``ycg`` [NG] the ghosts' mirrored centroid y
+        (type 7).  Each BC type present in the mesh is evaluated on the whole ring and
+        selected by the ghost's type."""
         flow = self.flow
         rr, cv, cp, g = prm.rr, prm.cv, prm.cp, flow.gama
 
@@ -348,18 +349,38 @@ class Scheme:
             sel[5] = torch.stack([u5, v5, pr[T_], P, rho5, rho5 * u5, rho5 * v5, rho5 * e5, -pr[C_ + 4],
                                   -pr[F_], 2.0 * P - pr[F_ + 1], -pr[F_ + 2], -pr[F_ + 3], -pr[F_ + 4],
                                   -pr[G_], -pr[G_ + 1], 2.0 * P - pr[G_ + 2], -pr[G_ + 3], -pr[G_ + 4]])
+        if 7 in self.types_present:  # boundary-layer inlet, 1/7-power profile (boundary.f90:310-327)
+            tinf = prm.t0 / (1.0 + 0.5 * (g - 1.0) * flow.aminf ** 2)
+            blu = 2.0 * flow.aminf * torch.sqrt(g * rr * tinf)
+            inside = ycg <= flow.deltabl
+            # the profile is evaluated on the whole ring: keep the other ghosts (mirrored
+            # below a wall, y < 0) out of the power so that no NaN gradient leaks
+            ratio = torch.where(inside & (ycg > 0), ycg, torch.full_like(ycg, flow.deltabl)) / flow.deltabl
+            u7 = torch.where(inside, blu * ratio ** (1.0 / 7.0), blu * torch.ones_like(ycg)) - pr[U_]
+            v7 = -pr[V_]
+            t7 = tinf * torch.ones_like(ycg)
+            p7 = torch.full_like(ycg, flow.pinf)
+            rho7 = p7 / (rr * t7)
+            c5 = rho7 * (self.amu(t7) / rho7)
+            sel[7] = state(rho7, u7, v7, t7, p7, c5, c5 * u7, c5 * v7)
         order = list(sel)
         out = sel[order[0]]
         for ty in order[1:]:
             out = torch.where(self.g_type == ty, sel[ty], out)
         return out
 
-    def boundary(self, W, prm: Params):
-        """Padded field set [19, NI+2, NJ+2]: cells plus the ghosts of APPLY_BOUNDARY."""
+    def boundary(self, W, prm: Params, geo=None):
+        """Padded field set [19, NI+2, NJ+2]: cells plus the ghosts of APPLY_BOUNDARY
+        (type 7 reads the ghosts' centroids from ``geo``)."""
         flat = W.reshape(NW_, -1)
         pr = flat.index_select(1, self.g_par)
         opp = flat[:4].index_select(1, self.g_opp)
-        gh = self._ghosts(pr, opp, prm)
+        ycg = None
+        if 7 in self.types_present:
+            if geo is None:
+                raise ValueError("BC type 7 needs the geometry")
+            ycg = geo["yc"].reshape(-1).index_select(0, self.g_pad)
+        gh = self._ghosts(pr, opp, prm, ycg)
         npad = (self.ni + 2) * (self.nj + 2)
         ring = torch.zeros((NW_, npad), dtype=W.dtype, device=W.device).index_copy(1, self.g_pad, gh)
         return torch.nn.functional.pad(W, (1, 1, 1, 1)) + ring.reshape(NW_, self.ni + 2, self.nj + 2)
@@ -553,7 +574,7 @@ class Scheme:
         vis = None
         dtbyvol = dt / geo["vol"]
         for st in range(4):
-            full = self.boundary(self.primitive(C, prm), prm)
+            full = self.boundary(self.primitive(C, prm), prm, geo)
             if st == 0:
                 vis = self.viscous(full, geo, prm, rtol)
                 # the viscous terms of equations 2..5, none in the continuity equation
@@ -569,10 +590,10 @@ class Scheme:
         return C
 
     # ------------------------------------------------------------------ objectives
-    def face_state(self, C, prm: Params, side: int):
+    def face_state(self, C, prm: Params, side: int, geo=None):
         """Face values (parent + ghost)/2 on one side of the final state: U, V, P, RHO, T
         (RHO = P/(RR*T) on both sides of the face) and the face vector S."""
-        full = self.boundary(self.primitive(C, prm), prm)
+        full = self.boundary(self.primitive(C, prm), prm, geo)
         idx = {1: ((slice(1, -1), 1), (slice(1, -1), 0)), 3: ((slice(1, -1), -2), (slice(1, -1), -1)),
                4: ((1, slice(1, -1)), (0, slice(1, -1))), 2: ((-2, slice(1, -1)), (-1, slice(1, -1)))}[side]
         pa, gh = idx
@@ -588,7 +609,7 @@ class Scheme:
 
     def wall_force(self, C, geo, prm: Params, side: int = 1):
         """Pressure force sum(p_f S) over the faces of ``side`` (per radian when IAXIS=1)."""
-        fs = self.face_state(C, prm, side)
+        fs = self.face_state(C, prm, side, geo)
         sx, sy = self.side_vectors(geo, side)
         return torch.stack([torch.sum(fs["p"] * sx), torch.sum(fs["p"] * sy)])
 
@@ -597,7 +618,7 @@ class Scheme:
         g = self.flow.gama
 
         def mean(side):
-            fs = self.face_state(C, prm, side)
+            fs = self.face_state(C, prm, side, geo)
             sx, sy = self.side_vectors(geo, side)
             m2 = (fs["u"] ** 2 + fs["v"] ** 2) / (g * prm.rr * fs["t"])
             p0 = fs["p"] * (1.0 + 0.5 * (g - 1.0) * m2) ** (g / (g - 1.0))

@@ -23,7 +23,15 @@ CASES = {
     "plume_axis": lambda: (_axis_sym(cases.nozzle_plume_mesh(32, 12)), cases.nozzle_plume_flow()),
     "global_dt": lambda: (cases.ramp_mesh(20, 10),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
+    "bl_inlet": lambda: _bl_inlet(24, 12),
 }
+
+
+def _bl_inlet(nx, ny):
+    """The ramp with its inlet as a type-7 boundary-layer inflow (M 0.3, 0.1 m layer)."""
+    mesh, flow = cases.ramp_mesh(nx, ny), cases.ramp_flow()
+    mesh.ntype[mesh.ntype == 2] = 7
+    return mesh, formats.Flow(**{**flow.__dict__, "pinf": 8.5e5, "aminf": 0.3, "deltabl": 0.1})
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

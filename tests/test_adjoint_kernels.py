@@ -33,7 +33,14 @@ CASES = {
     "plume_wall_axis": lambda: (cases.nozzle_plume_mesh(28, 10), cases.nozzle_plume_flow()),
     "global_dt": lambda: (cases.ramp_mesh(20, 10),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
+    "bl_inlet": lambda: _bl_inlet(24, 12),
 }
+
+
+def _bl_inlet(nx, ny):
+    mesh, flow = cases.ramp_mesh(nx, ny), cases.ramp_flow()
+    mesh.ntype[mesh.ntype == 2] = 7
+    return mesh, formats.Flow(**{**flow.__dict__, "pinf": 8.5e5, "aminf": 0.3, "deltabl": 0.1})
 
 
 @pytest.fixture(scope="session")
@@ -55,7 +62,7 @@ def _stages(sch, Cold, geo, prm, rtol):
     Cs, Cc, vis = [Cold], Cold, None
     dtbyvol = dt / geo["vol"]
     for st in range(4):
-        full = sch.boundary(sch.primitive(Cc, prm), prm)
+        full = sch.boundary(sch.primitive(Cc, prm), prm, geo)
         if st == 0:
             vis = sch.viscous(full, geo, prm, rtol)
             vis5 = torch.cat([torch.zeros_like(vis[:1]), vis])

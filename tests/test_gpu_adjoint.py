@@ -109,7 +109,15 @@ STEP_CASES = {
     "plume_wall_axis": lambda: (cases.nozzle_plume_mesh(48, 20), cases.nozzle_plume_flow()),
     "global_dt": lambda: (cases.ramp_mesh(40, 16),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
+    "bl_inlet": lambda: _bl_inlet(48, 20),
 }
+
+
+def _bl_inlet(nx, ny):
+    """The ramp with its inlet as a type-7 boundary-layer inflow (M 0.3, 0.1 m layer)."""
+    mesh, flow = cases.ramp_mesh(nx, ny), cases.ramp_flow()
+    mesh.ntype[mesh.ntype == 2] = 7
+    return mesh, formats.Flow(**{**flow.__dict__, "pinf": 8.5e5, "aminf": 0.3, "deltabl": 0.1})
 
 
 @pytest.mark.parametrize("name", sorted(STEP_CASES))
