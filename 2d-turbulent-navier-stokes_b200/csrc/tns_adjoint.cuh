@@ -586,6 +586,13 @@ TNS_HD void src_reverse(const Params& P, const SrcWork& s, const double nb[4][4]
 // the forward, and writes the residual adjoint (gbar), the source adjoints for the
 // neighbours (srcn, srcg) and the cell (wself); accumulates the adjoints of Q_n, D, VIS
 // and DT.
+// TNS_ADJ_SRC_RECOMPUTE: the stage reverse evaluates the source terms twice (values for
+// the residual, then intermediates for the reverse) instead of keeping them live across
+// the update: spill-free at 166 registers, 414 vs 425 us per 512 x 192 transient step.
+#ifndef TNS_ADJ_SRC_RECOMPUTE
+#define TNS_ADJ_SRC_RECOMPUTE 1
+#endif
+
 TNS_HD void s1_point(const AdjArgs& a, long long cell) {
     const int i = (int)(cell / a.nj), j = (int)(cell % a.nj);
     const Params& P = a.P;
@@ -613,10 +620,22 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
         slot_centroid(a, i + di_of(k), j + dj_of(k), nx[k], ny[k]);
     }
     const double Vc = wv(a, WV, ps);
+    double src5, src3;
+#if TNS_ADJ_SRC_RECOMPUTE
+    {
+        SrcWork s0;  // only SOURCE3/5 here; the reverse recomputes the intermediates
+        src_forward(P, nb, nx, ny, wv(a, WC1, ps), wv(a, WC5, ps), wv(a, WT, ps), wv(a, WP, ps), Vc, g.yc, s0);
+        src5 = s0.s5;
+        src3 = s0.s3;
+    }
+#else
     SrcWork s;
     src_forward(P, nb, nx, ny, wv(a, WC1, ps), wv(a, WC5, ps), wv(a, WT, ps), wv(a, WP, ps), Vc, g.yc, s);
-    R[4] = R[4] - g.vol * s.s5;
-    if (P.iaxis == 1) R[2] = R[2] - g.vol * s.s3;
+    src5 = s.s5;
+    src3 = s.s3;
+#endif
+    R[4] = R[4] - g.vol * src5;
+    if (P.iaxis == 1) R[2] = R[2] - g.vol * src3;
     // update and clip
     const double DT = P.local ? a.dt[cell] : *a.dtmin;
     const double dtv = a.alpha * (DT / g.vol);
@@ -667,8 +686,19 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
     // source reverse: R5 -= VOL*SOURCE5, R3 -= VOL*SOURCE3
     const double s5b = -g.vol * gb[4];
     const double s3b = P.iaxis == 1 ? -g.vol * gb[2] : 0.0;
-    volb -= s.s5 * gb[4];
-    if (P.iaxis == 1) volb -= s.s3 * gb[2];
+    volb -= src5 * gb[4];
+    if (P.iaxis == 1) volb -= src3 * gb[2];
+#if TNS_ADJ_SRC_RECOMPUTE
+    for (int k = 0; k < 4; k++) {
+        nb[k][0] = wv(a, WU, pn[k]);
+        nb[k][1] = wv(a, WV, pn[k]);
+        nb[k][2] = wv(a, WC1, pn[k]);
+        nb[k][3] = wv(a, WC5, pn[k]);
+        slot_centroid(a, i + di_of(k), j + dj_of(k), nx[k], ny[k]);
+    }
+    SrcWork s;
+    src_forward(P, nb, nx, ny, wv(a, WC1, ps), wv(a, WC5, ps), wv(a, WT, ps), wv(a, WP, ps), Vc, g.yc, s);
+#endif
     SrcBar b;
     src_reverse(P, s, nb, Vc, s3b, s5b, b);
     a.wself[0 * a.ncell + cell] = b.t;
