@@ -871,16 +871,18 @@ def objective_gpu(scheme: Scheme, objective: Callable, p0=None, t0=None, amachin
 
 def fixed_point_adjoint(scheme: Scheme, objective: Callable, Qstar: torch.Tensor, niter: int = 200,
                         p0=None, t0=None, amachinit=None, dy=None, space=None, engine: Optional[str] = None,
-                        lib=None) -> dict:
+                        lib=None, history_every: int = 1) -> dict:
     """Adjoint of a steady state Q* = G(Q*, p): iterates lambda <- dJ/dQ + lambda dG/dQ
     (the RK4 iteration's transposed Jacobian at Q*) and returns dJ/dp = dJ/dp|direct +
     lambda dG/dp, with the adjoint residual history |lambda_{k+1} - lambda_k|_max.
     Meaningful when Q* is a converged state of the primal.  ``engine`` as in
-    ``transient_gradient`` (the CUDA engine applies tns_adjoint_step at Q*)."""
+    ``transient_gradient`` (the CUDA engine applies tns_adjoint_step at Q*, and records
+    the residual every ``history_every`` sweeps)."""
     if engine is None:
         engine = "cuda" if scheme.device.type == "cuda" else "torch"
     if engine == "cuda":
-        return _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib)
+        return _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib,
+                                 history_every)
     if engine != "torch":
         raise ValueError(f"engine {engine!r}: 'cuda' or 'torch'")
     dev = scheme.device
@@ -1087,7 +1089,8 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
     return out
 
 
-def _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib) -> dict:
+def _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, space, lib,
+                      history_every=1) -> dict:
     if scheme.device.type != "cuda":
         raise ValueError("engine='cuda' needs a Scheme on a CUDA device")
     params, dy = _leaves(scheme, p0, t0, amachinit, dy)
@@ -1107,7 +1110,8 @@ def _fixed_point_cuda(scheme, objective, Qstar, niter, p0, t0, amachinit, dy, sp
             vj = lam.clone()
             dev_adj.step(q, vj, False, frozen=it > 0)  # Q* is fixed: forward values reused
             new = djdq + vj
-            hist.append(float(torch.max(torch.abs(new - lam))))
+            if (it + 1) % history_every == 0 or it == niter - 1:
+                hist.append(float(torch.max(torch.abs(new - lam))))
             lam = new
         last = lam.clone()
         dev_adj.step(q, last, True, frozen=niter > 0)  # lambda dG/dp at Q*
