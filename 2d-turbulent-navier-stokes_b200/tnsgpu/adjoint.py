@@ -644,7 +644,7 @@ class DesignSpace:
         s = self.scheme
         if dy is None or self.node_shape is None:
             return s.x0, s.y0
-        return s.x0, s.y0 + torch.einsum("k,kij->ij", dy, self.node_shape)
+        return s.x0, s.y0 + torch.einsum("k,kij->ij", dy.to(self.node_shape.device), self.node_shape)
 
 
 def ramp_wall_shape(scheme: Scheme, wall_nodes: Sequence[int], blend: np.ndarray) -> torch.Tensor:

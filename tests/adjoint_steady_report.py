@@ -85,6 +85,7 @@ def main():
     t0 = time.perf_counter()
     q, n, ratio, first = converge(Solver, mesh, flow, rinit, c0, a.tol, a.max_primal)
     out["primal"] = {"iterations": n, "residual_ratio": ratio, "seconds": time.perf_counter() - t0}
+    print(json.dumps({"primal": out["primal"]}), file=sys.stderr, flush=True)
     qstar = torch.tensor(q.reshape(5, nx, ny), device="cuda")
     dy = torch.zeros(1, dtype=torch.float64)
     t0 = time.perf_counter()
@@ -93,6 +94,8 @@ def main():
     torch.cuda.synchronize()
     out["fixed_point"] = {"iterations": a.adjoint_iters, "seconds": time.perf_counter() - t0,
                           "residual_every_50k": fp["residual_history"]}
+    print(json.dumps({"fixed_point": out["fixed_point"], "grads": {"p0": fp["dJ_dp0"], "dy": float(fp["dJ_ddy"][0])}}),
+          file=sys.stderr, flush=True)
     grads = {"p0": fp["dJ_dp0"], "t0": fp["dJ_dt0"], "dy": float(fp["dJ_ddy"][0])}
 
     def J_at(which, value):
@@ -101,7 +104,7 @@ def main():
             f = dataclasses.replace(flow, p0=value)
         elif which == "t0":
             f = dataclasses.replace(flow, t0=value)
-        d = torch.tensor([value if which == "dy" else 0.0], dtype=torch.float64)
+        d = torch.tensor([value if which == "dy" else 0.0], dtype=torch.float64, device="cuda")
         if which == "dy":
             m = adjoint._mesh_with_coords(sch, space, d)
         p = sch.params(f.p0, f.t0)
@@ -121,6 +124,7 @@ def main():
     for which, base, h in (("p0", flow.p0, 1e-6 * flow.p0), ("dy", 0.0, 3e-7)):
         v = (J_at(which, base + h) - J_at(which, base - h)) / (2 * h)
         fd[which] = {"adjoint": grads[which], "fd": v, "rel_diff": abs(grads[which] - v) / max(abs(v), 1e-300)}
+        print(json.dumps({which: fd[which]}), file=sys.stderr, flush=True)
     fd["t0"] = {"adjoint": grads["t0"]}
     out["finite_differences"] = fd
     out["fd_seconds"] = time.perf_counter() - t0
