@@ -64,6 +64,8 @@ TNS_ADJ_KERNEL(k_adj_dtmin, dtmin_point, 1)
 TNS_ADJ_KERNEL(k_adj_final, final_point, 1)
 TNS_ADJ_KERNEL(k_adj_centroids, centroid_point, 1)
 TNS_ADJ_KERNEL(k_adj_geo, geo_point, 1)
+TNS_ADJ_KERNEL(k_adj_port, port_point, 1)
+TNS_ADJ_KERNEL(k_adj_port_nodes, port_node_point, 1)
 
 // LOCAL = 0: sum of the per-cell dt adjoints (block sums, one atomic per block).
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_dtsum(const double* __restrict__ v, long long n,
@@ -94,7 +96,7 @@ void launch_points(K kernel, const AdjArgs& a, long long n, cudaStream_t s) {
 // stages' field sets, node averages and the dissipation pre-pass.  Two sets, so that
 // the next checkpoint's forward values are computed while this one's reverse runs.
 struct AdjForward {
-    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, w, navg, dpre;
+    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, w, navg, dpre, gport;  // gport: [4][nghost]
     DevBuf<int> ninfo;
 };
 
@@ -106,7 +108,7 @@ struct tns_adjoint_state {
     int pre_set = -1;                    // a set prefetched by the last step ...
     const double* pre_ptr = nullptr;     // ... for the state at this device address
     DevBuf<double> lam, lamA, lamB, lamold, lamg, lamd, gbar, srcn, srcg, wself, wvisc, dbar, visbar, dtbar, dout,
-        nbar, vfi, vfj, dtsum, sens, xcs, ycs;
+        nbar, vfi, vfj, dtsum, sens, xcs, ycs, gportb, portacc;  // gportb [4][nghost], portacc [3][nghost]
     long long nsens = 0;
     // branches of a step: dissipation reverse, ghost gather, face-vector sensitivities,
     // forward values of the next checkpoint
@@ -145,6 +147,14 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int set, int geo) {
     a.navg = f.navg.p;
     a.ninfo = f.ninfo.p;
     a.dpre = f.dpre.p;
+    a.gport = f.gport.p;
+    a.qst[0] = f.q0.p;
+    a.qst[1] = f.q1.p;
+    a.qst[2] = f.q2.p;
+    a.qst[3] = f.q3.p;
+    a.gportb = s->gportb.p;
+    a.gportb4 = s->gportb.p;
+    a.portacc = s->portacc.p;
     a.xcs = s->xcs.p;
     a.ycs = s->ycs.p;
     a.lam_old = s->lamold.p;
@@ -200,20 +210,37 @@ long long enqueue_forward(tns_handle* h, tns_adjoint_state* s, int set, cudaStre
         tns::launch_dtmin(P, M, f.q0.p, h->partial.p, h->counter.p, f.dtmin.p, st);
         nl++;
     }
-    tns::launch_dissipation(P, M, f.q0.p, f.d.p, f.dt.p, f.dtmin.p, st);
-    tns::launch_viscous(P, M, f.q0.p, f.vis.p, st);
+    // the type-6 ghosts read the port mass flux of each stage's input (one slice per stage)
+    const int np = (int)h->port_ghosts.size();
+    const size_t ng = (size_t)M.nghosts();
+    Mesh Ms[4] = {M, M, M, M};
     double* qs[4] = {f.q0.p, f.q1.p, f.q2.p, f.q3.p};
-    for (int k = 0; k < 3; k++)
-        tns::launch_stage(P, M, qs[k], f.q0.p, qs[k + 1], f.d.p, f.vis.p, f.dt.p, f.dtmin.p, kAlpha[k], nullptr,
+    for (int k = 0; k < 4; k++) Ms[k].gport = f.gport.p + k * ng;
+    auto gport = [&](int k) {
+        if (np) {
+            tns::launch_gport(P, Ms[k], qs[k], h->ports.p, np, f.gport.p + k * ng, st);
+            nl++;
+        }
+    };
+    tns::launch_dissipation(P, M, f.q0.p, f.d.p, f.dt.p, f.dtmin.p, st);
+    gport(0);
+    tns::launch_viscous(P, Ms[0], f.q0.p, f.vis.p, st);
+    for (int k = 0; k < 3; k++) {
+        if (k) gport(k);
+        tns::launch_stage(P, Ms[k], qs[k], f.q0.p, qs[k + 1], f.d.p, f.vis.p, f.dt.p, f.dtmin.p, kAlpha[k], nullptr,
                           nullptr, st);
+    }
+    gport(3);
     nl += 5;
     AdjArgs a = base_args(h, s, set, 0);
     for (int k = 0; k < 4; k++) {
         a.qin = qs[k];
+        a.gport = f.gport.p + k * ng;
         a.w = f.w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
         launch_points(k_adj_fields, a, a.npad, st);
     }
     a.w = f.w.p;
+    a.gport = f.gport.p;
     launch_points(k_adj_nodes, a, a.nnode, st);
     launch_points(k_adj_diss_pre, a, a.ncell, st);
     return nl + 6;
@@ -245,6 +272,8 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
         a.lam_out = lam_stage[k];
         a.w = f.w.p + (size_t)k * NWROW * a.npad;     // this stage's field set
         a.gbar = s->gbar.p + (size_t)k * 5 * a.npad;  // one residual adjoint per stage
+        a.gport = f.gport.p + (size_t)k * a.M.nghosts();
+        a.gportb = s->gportb.p + (size_t)k * a.M.nghosts();
         launch_points(k_adj_stage, a, a.ncell, st);
         nl++;
         if (k == 0) {
@@ -261,12 +290,6 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
             }
             // viscous reverse on the main stream
             launch_points(k_adj_faces, a, a.nif + a.njf, st);
-            if (geo) {
-                // face-vector sensitivities of the whole step on their own branch
-                fork(s->side[2]);
-                launch_points(k_adj_geo, a, a.ncell, s->side[2]);
-                nl++;
-            }
             launch_points(k_adj_node_bar, a, a.nnode, st);
             launch_points(k_adj_slot_bar, a, a.npad, st);
             nl += 3;
@@ -276,6 +299,21 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
         launch_points(k_adj_gather, a, a.ncell, st);
         nl += 2;
         join(s->side[1]);
+        if (!h->port_ghosts.empty()) {
+            // the port mass flux's adjoint down each port line
+            launch_points(k_adj_port, a, a.ncell, st);
+            nl++;
+        }
+    }
+    if (geo) {
+        // face-vector (and port) sensitivities of the whole step on their own branch
+        fork(s->side[2]);
+        launch_points(k_adj_geo, a, a.ncell, s->side[2]);
+        nl++;
+        if (!h->port_ghosts.empty()) {
+            launch_points(k_adj_port_nodes, a, a.nnode, s->side[2]);
+            nl++;
+        }
     }
     join(s->side[0]);
     if (geo) join(s->side[2]);
@@ -312,8 +350,7 @@ int check_mesh(tns_handle* h) {
     if (!h->identity) return h->fail(TNS_ERR_ARG, "the adjoint needs cells numbered in (i, j) order");
     if (h->ni < 3 || h->nj < 3) return h->fail(TNS_ERR_ARG, "the adjoint needs at least 3 x 3 cells");
     for (int t : h->hgtype)
-        if (t < 2 || t > 7 || t == 6)
-            return h->fail(TNS_ERR_ARG, "BC type %d: the adjoint covers types 2-5 and 7", t);
+        if (t < 2 || t > 7) return h->fail(TNS_ERR_ARG, "BC type %d: the adjoint covers types 2-7", t);
     return TNS_OK;
 }
 
@@ -338,13 +375,13 @@ void adjoint_release(tns_handle* h) {
     }
     if (s->ev) cudaEventDestroy(s->ev);
     for (auto& f : s->set) {
-        for (auto* b : {&f.q0, &f.q1, &f.q2, &f.q3, &f.d, &f.vis, &f.dt, &f.dtmin, &f.w, &f.navg, &f.dpre})
+        for (auto* b : {&f.q0, &f.q1, &f.q2, &f.q3, &f.d, &f.vis, &f.dt, &f.dtmin, &f.w, &f.navg, &f.dpre, &f.gport})
             b->release();
         f.ninfo.release();
     }
     for (auto* b : {&s->lam, &s->lamA, &s->lamB, &s->lamold, &s->lamg, &s->lamd, &s->gbar, &s->srcn, &s->srcg,
                     &s->wself, &s->wvisc, &s->dbar, &s->visbar, &s->dtbar, &s->dout, &s->nbar, &s->vfi, &s->vfj,
-                    &s->dtsum, &s->sens, &s->xcs, &s->ycs})
+                    &s->dtsum, &s->sens, &s->xcs, &s->ycs, &s->gportb, &s->portacc})
         b->release();
     delete s;
     h->adj = nullptr;
@@ -373,11 +410,13 @@ int tns_adjoint_enable(tns_handle* h) {
                              {&s->srcg, 8 * n}, {&s->wself, 5 * n}, {&s->wvisc, 5 * npad}, {&s->dbar, 5 * n},
                              {&s->visbar, 4 * n}, {&s->dtbar, n}, {&s->dout, NDOUT * n}, {&s->nbar, 5 * nnode},
                              {&s->vfi, NVF * nif}, {&s->vfj, NVF * njf}, {&s->dtsum, 1}, {&s->sens, s->nsens},
-                             {&s->xcs, npad}, {&s->ycs, npad}};
+                             {&s->xcs, npad}, {&s->ycs, npad}, {&s->gportb, 4 * (2 * (h->ni + h->nj))},
+                             {&s->portacc, 3 * (2 * (h->ni + h->nj))}};
     for (auto& f : s->set)
         for (Req r : std::vector<Req>{{&f.q0, 5 * n}, {&f.q1, 5 * n}, {&f.q2, 5 * n}, {&f.q3, 5 * n},
                                       {&f.d, 5 * n}, {&f.vis, 4 * n}, {&f.dt, n}, {&f.dtmin, 1},
-                                      {&f.w, 4 * NWROW * npad}, {&f.navg, NNA * nnode}, {&f.dpre, NDPRE * n}})
+                                      {&f.w, 4 * NWROW * npad}, {&f.navg, NNA * nnode}, {&f.dpre, NDPRE * n},
+                                      {&f.gport, 4 * (2 * (h->ni + h->nj))}})
             reqs.push_back(r);
     for (auto& r : reqs) {
         if ((rc = h->cuda(r.b->alloc((size_t)r.count), "cudaMalloc (adjoint)"))) {
@@ -407,6 +446,9 @@ int tns_adjoint_enable(tns_handle* h) {
     cudaMemsetAsync(s->gbar.p, 0, sizeof(double) * 4 * 5 * npad, h->stream);
     cudaMemsetAsync(s->wvisc.p, 0, sizeof(double) * 5 * npad, h->stream);
     cudaMemsetAsync(s->sens.p, 0, sizeof(double) * s->nsens, h->stream);
+    cudaMemsetAsync(s->portacc.p, 0, sizeof(double) * s->portacc.n, h->stream);
+    cudaMemsetAsync(s->gportb.p, 0, sizeof(double) * s->gportb.n, h->stream);
+    for (auto& f : s->set) cudaMemsetAsync(f.gport.p, 0, sizeof(double) * f.gport.n, h->stream);
     const AdjArgs a = base_args(h, s, 0, 0);
     launch_points(k_adj_centroids, a, npad, h->stream);
     return h->cuda(cudaStreamSynchronize(h->stream), "tns_adjoint_enable");

@@ -1,4 +1,4 @@
-// tns_adjoint.cuh -- discrete adjoint of one RK4 iteration (BC types 2-5 and 7, FP64).
+// tns_adjoint.cuh -- discrete adjoint of one RK4 iteration (BC types 2-7, FP64).
 //
 // Given lambda_{n+1} = dJ/dQ_{n+1}, the reverse step returns lambda_n = lambda_{n+1}
 // dG/dQ_n for the iteration map Q_{n+1} = G(Q_n) of turbnstwod.f90:95-146, and (on
@@ -12,7 +12,9 @@
 //   ghost back-propagation     boundary.f90:53-122       (s3g_point)
 //   source terms               source_terms.f90:24-104   (src_forward / src_reverse)
 //   primitive variables        turbnstwod.f90:204-227    (prim_adj)
-//   ghost states 2..5, 7       boundary.f90:53-122,310-327 (ghost_adj)
+//   ghost states 2..7          boundary.f90:53-327       (ghost_adj)
+//   port mass flux GPORT       boundary.f90:168-305      (gport_point, port_point,
+//                                                         port_node_point)
 //   viscous flux               viscous.f90:29-217        (v0..v3_point, visc_face_adj)
 //   JST dissipation            solver_state.f90:70-225   (d0..d2_point)
 //   time step (LOCAL 0/1)      turbnstwod.f90:97-114     (ts_adj, dtmin_point)
@@ -91,6 +93,12 @@ struct AdjArgs {
     double* vfi;           // i-face adjoints [NVF][nif]
     double* vfj;           // j-face adjoints [NVF][njf]
     double* dtsum;         // LOCAL = 0: sum of the dt adjoints [1]
+    // type-6 port ghosts
+    const double* gport;   // port mass flux of this stage's input [nghost]
+    double* gportb;        // its adjoint [nghost] (this stage)
+    const double* gportb4; // the four stages' [4][nghost]
+    const double* qst[4];  // the four stage inputs (column terms of GPORT)
+    double* portacc;       // parent face vector x, y and centroid y adjoints per ghost [3][nghost]
     // parameter sensitivities (accumulated when geo != 0)
     int geo;
     double *sxbar, *sybar;   // [4][ncell] face vectors
@@ -204,7 +212,16 @@ TNS_HD void s0_point(const AdjArgs& a, long long ps) {
                           a.qin[4 * a.ncell + oc], opp);
             else
                 opp = par;
-            boundary_ghost(a.P, type, par, opp, 0.0, 0.0, a.M.gyc[gidx], 0.0, 0.0, 1.0, p);
+            double psx = 0.0, psy = 0.0, ycp = 0.0, gp = 0.0;
+            if (type == 6) {
+                CellGeo pg;
+                cell_geo(a, pi, pj, pg);
+                psx = pg.sx[k];
+                psy = pg.sy[k];
+                ycp = pg.yc;
+                gp = a.gport[gidx];
+            }
+            boundary_ghost(a.P, type, par, opp, psx, psy, a.M.gyc[gidx], ycp, gp, a.M.ginj[gidx], p);
             row[WC1] = p.rho;
             row[WC5] = p.c5;
         }
@@ -276,15 +293,24 @@ TNS_HD void tail_adj(const Params& P, double rho, double u, double v, double t, 
     vb += c3b * rho;
 }
 
-// Reverse of APPLY_BOUNDARY for one ghost of type 2..5 or 7 (boundary.f90:53-122,
-// 310-327).  gw, pw, ow: field-set rows of the ghost, its parent and the parent's opposite
-// neighbour; gb: the ghost's row adjoint; ycg: the ghost's mirrored centroid y.  Adds to
-// the parent's rows (pb), the opposite cell's U V T P (ob), the adjoints of T0 and S0
-// (type-2 inlet; type 7 through TINF and the profile velocity, both set by T0) and of
-// the ghost's centroid y (type 7).
+// Geometry and port inputs of one ghost: its mirrored centroid y, the parent's centroid
+// y and face vector on the ghost's side, the port mass flux and burn-rate multiplier.
+struct GhostGeo {
+    double ycg, ycp, psx, psy, gport, inj;
+};
+struct GhostGeoBar {
+    double ycg, ycp, psx, psy, gport;
+};
+
+// Reverse of APPLY_BOUNDARY for one ghost of type 2..7 (boundary.f90:53-327).  gw, pw,
+// ow: field-set rows of the ghost, its parent and the parent's opposite neighbour; gb:
+// the ghost's row adjoint; gg: its geometry and port inputs.  Adds to the parent's rows
+// (pb), the opposite cell's U V T P (ob), the adjoints of T0 and S0 (type-2 inlet; type
+// 7 through TINF and the profile velocity, both set by T0) and of the geometry and port
+// inputs (gbar: types 6 and 7).
 TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const double pw[NWROW],
                       const double ow[NWROW], const double gb[NWROW], double pb[NWROW], double ob[NWROW],
-                      double& t0b, double& s0b, double ycg, double& ygb) {
+                      double& t0b, double& s0b, const GhostGeo& gg, GhostGeoBar& gbar) {
     if (type == 5) {
         pb[WU] -= gb[WU];
         pb[WV] -= gb[WV];
@@ -328,6 +354,74 @@ TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const d
         const double xb = ub * sgn(2.0 * pw[WU] - ow[WU]);
         pb[WU] += 2.0 * xb;
         ob[WU] -= xb;
+    } else if (type == 6) {  // mass injection (boundary.f90:128-163)
+        // forward, as boundary_ghost evaluates it
+        const double DNR = sqrt(gg.psx * gg.psx + gg.psy * gg.psy);
+        const double ENX = -gg.psx / DNR, ENY = -gg.psy / DNR;
+        const double hs = gg.ycg + gg.ycp;
+        const double DHYD = fabs(hs);
+        const double GP = (P.iaxis == 1) ? 2.0 * gg.gport / (DHYD * DHYD) : gg.gport / DHYD;
+        const double RHO0 = pw[WC1], PP = pw[WP];
+        const double RDOT = P.acomb * pow(PP * CONVKSC, P.ancomb) * gg.inj;
+        const double VEL1 = P.rhoprop / RHO0 * RDOT;
+        const double u1 = VEL1 * ENX + VEL1 * ENX - pw[WU], v1 = VEL1 * ENY + VEL1 * ENY - pw[WV];
+        const double t1 = P.tflame - 0.5 * (u1 * u1 + v1 * v1) / P.cp;
+        const double AMU1 = amu_of(P, t1);
+        const double A = GP / (P.rhoprop * RDOT), B = P.rhoprop * RDOT * DHYD / AMU1;
+        const double Bp = pow(B, -0.125);
+        const double GVAL = A * Bp;
+        const bool ero = GVAL > GTH;
+        const double fac = ero ? 1.0 + 0.023 * (pow(GVAL, 0.8) - P.gth08) : 1.0;
+        const double RDOTEB = RDOT * fac;
+        const double VEL2 = P.rhoprop / RHO0 * RDOTEB;
+        // reverse: final state (RHO = P / (RR T), C5 = RHO * (AMU(T) / RHO))
+        const double c5 = gw[WC5];
+        const double c5b = gb[WC5] + gb[WF + 4] * u + gb[WG + 4] * v;
+        ub += gb[WF + 4] * c5;
+        vb += gb[WG + 4] * c5;
+        tb += c5b * 0.6 * amu_of(P, t) / t;
+        ppb += rhob / (P.rr * t);
+        tb -= rhob * rho / t;
+        // T = TFLAME - (U^2 + V^2) / (2 CP)
+        ub -= tb * u / P.cp;
+        vb -= tb * v / P.cp;
+        // U = 2 VEL2 ENX - U_parent
+        double ENXb = 2.0 * ub * VEL2, ENYb = 2.0 * vb * VEL2;
+        const double VEL2b = 2.0 * (ub * ENX + vb * ENY);
+        pb[WU] -= ub;
+        pb[WV] -= vb;
+        double RHO0b = -VEL2b * VEL2 / RHO0;
+        const double RDOTEBb = VEL2b * P.rhoprop / RHO0;
+        double RDOTb = RDOTEBb * fac, GVALb = 0.0;
+        if (ero) GVALb = RDOTEBb * RDOT * 0.023 * 0.8 * pow(GVAL, -0.2);
+        // GVAL = (GP / (RHOPROP RDOT)) * (RHOPROP RDOT DHYD / AMU1)**(-1/8)
+        const double Ab = GVALb * Bp, Bb = GVALb * A * (-0.125) * Bp / B;
+        const double GPb = Ab / (P.rhoprop * RDOT);
+        RDOTb += -Ab * A / RDOT + Bb * B / RDOT;
+        double DHYDb = Bb * B / DHYD;
+        const double AMU1b = -Bb * B / AMU1;
+        const double t1b = AMU1b * 0.6 * AMU1 / t1;
+        const double u1b = -t1b * u1 / P.cp, v1b = -t1b * v1 / P.cp;
+        ENXb += 2.0 * u1b * VEL1;
+        ENYb += 2.0 * v1b * VEL1;
+        const double VEL1b = 2.0 * (u1b * ENX + v1b * ENY);
+        pb[WU] -= u1b;
+        pb[WV] -= v1b;
+        RHO0b -= VEL1b * VEL1 / RHO0;
+        RDOTb += VEL1b * P.rhoprop / RHO0;
+        // RDOT = ACOMB (P CONVKSC)**ANCOMB INJ; P = P_parent; RHO0 = RHO_parent
+        if (P.ancomb != 0.0) ppb += RDOTb * RDOT * P.ancomb / PP;
+        pb[WP] += ppb;
+        pb[WC1] += RHO0b;
+        // GP = GPORT / DHYD (2 GPORT / DHYD^2 for IAXIS=1), DHYD = |YCC_ghost + YCC_parent|
+        gbar.gport += GPb * ((P.iaxis == 1) ? 2.0 / (DHYD * DHYD) : 1.0 / DHYD);
+        DHYDb -= GPb * GP * ((P.iaxis == 1) ? 2.0 : 1.0) / DHYD;
+        gbar.ycg += DHYDb * sgn(hs);
+        gbar.ycp += DHYDb * sgn(hs);
+        // EN = -PS / |PS|
+        const double DNRb = -(ENXb * ENX + ENYb * ENY) / DNR;
+        gbar.psx += -ENXb / DNR + DNRb * gg.psx / DNR;
+        gbar.psy += -ENYb / DNR + DNRb * gg.psy / DNR;
     } else if (type == 7) {  // boundary-layer inlet: P = PINF, T = TINF, U from the 1/7 profile
         const double c5 = gw[WC5];
         const double c5b = gb[WC5] + gb[WF + 4] * u + gb[WG + 4] * v;
@@ -338,10 +432,10 @@ TNS_HD void ghost_adj(const Params& P, int type, const double gw[NWROW], const d
         tb -= rhob * rho / t;       // RHO = PINF / (RR T)
         // U = BL_U (YCC/DELTABL)**(1/7) - U_parent (BL_U - U_parent above the layer)
         double blub = ub;
-        if (ycg <= P.deltabl) {
-            const double r = ycg / P.deltabl, f = pow(r, P.bl_exp);
+        if (gg.ycg <= P.deltabl) {
+            const double r = gg.ycg / P.deltabl, f = pow(r, P.bl_exp);
             blub = ub * f;
-            if (r > 0.0) ygb += ub * P.bl_u * P.bl_exp * f / r / P.deltabl;
+            if (r > 0.0) gbar.ycg += ub * P.bl_u * P.bl_exp * f / r / P.deltabl;
         }
         pb[WU] -= ub;
         pb[WV] -= vb;
@@ -857,11 +951,19 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         else load_rows(a, ps, ow);
         double dummy[NWROW];
         for (int r = 0; r < NWROW; r++) dummy[r] = 0.0;
-        double ygb = 0.0;
-        ghost_adj(a.P, type, gw, pw, ow, gb, wb, dummy, t0b, s0b, a.M.gyc[a.M.ghost_index(side, along)], ygb);
+        const int gidx = a.M.ghost_index(side, along);
+        GhostGeo gg{a.M.gyc[gidx], g.yc, g.sx[k], g.sy[k], type == 6 ? a.gport[gidx] : 0.0, a.M.ginj[gidx]};
+        GhostGeoBar gbr{0.0, 0.0, 0.0, 0.0, 0.0};
+        ghost_adj(a.P, type, gw, pw, ow, gb, wb, dummy, t0b, s0b, gg, gbr);
+        if (type == 6) a.gportb[gidx] = gbr.gport;
         if (a.geo) {
             a.xcbar[gps] += a.srcg[(k * 2 + 0) * a.ncell + cell];
-            a.ycbar[gps] += a.srcg[(k * 2 + 1) * a.ncell + cell] + ygb;
+            a.ycbar[gps] += a.srcg[(k * 2 + 1) * a.ncell + cell] + gbr.ycg;
+            if (type == 6) {  // parent face vector and centroid: added by geo_point
+                a.portacc[0 * a.M.nghosts() + gidx] += gbr.psx;
+                a.portacc[1 * a.M.nghosts() + gidx] += gbr.psy;
+                a.portacc[2 * a.M.nghosts() + gidx] += gbr.ycp;
+            }
         }
     }
     for (int k = 0; k < 4; k++) {
@@ -881,8 +983,10 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         load_rows(a, pps, par);
         load_rows(a, gps, gw);
         for (int r = 0; r < NWROW; r++) pbd[r] = obar[r] = 0.0;
-        double t0d = 0.0, s0d = 0.0, ygd = 0.0;
-        ghost_adj(a.P, 3, gw, par, pw, gb, pbd, obar, t0d, s0d, 0.0, ygd);
+        double t0d = 0.0, s0d = 0.0;
+        const GhostGeo gg{0.0, 0.0, 0.0, 0.0, 0.0, 1.0};
+        GhostGeoBar gbd{0.0, 0.0, 0.0, 0.0, 0.0};
+        ghost_adj(a.P, 3, gw, par, pw, gb, pbd, obar, t0d, s0d, gg, gbd);
         wb[WU] += obar[WU];
         wb[WV] += obar[WV];
         wb[WT] += obar[WT];
@@ -1505,10 +1609,133 @@ TNS_HD void geo_point(const AdjArgs& a, long long cell) {
             sxb[k] += vb * fb[k][(VF_CX + q) * stv[k]];
             syb[k] += vb * fb[k][(VF_CY + q) * stv[k]];
         }
+    // a type-6 ghost on one of the cell's faces: its face-vector and centroid adjoints
+    // gathered over the step's stages (then cleared for the next step)
+    double ycb = 0.0;
+    for (int k = 0; k < 4; k++) {
+        const int gi = i + di_of(k), gj = j + dj_of(k);
+        if (is_cell(a, gi, gj)) continue;
+        int along = 0;
+        const int side = ghost_side(a, gi, gj, along);
+        const int g = a.M.ghost_index(side, along);
+        if (a.M.gtype[g] != 6) continue;
+        const int ng = a.M.nghosts();
+        sxb[k] += a.portacc[0 * ng + g];
+        syb[k] += a.portacc[1 * ng + g];
+        ycb += a.portacc[2 * ng + g];
+        a.portacc[0 * ng + g] = a.portacc[1 * ng + g] = a.portacc[2 * ng + g] = 0.0;
+    }
+    if (ycb != 0.0) a.ycbar[ps] += ycb;
     for (int k = 0; k < 4; k++) {
         a.sxbar[k * a.ncell + cell] += sxb[k];
         a.sybar[k * a.ncell + cell] += syb[k];
     }
+}
+
+// The port ghost of `side` whose line (the cells from the port wall across to the
+// opposite side) holds cell (i, j), or -1.
+TNS_HD int port_of(const AdjArgs& a, int side, int i, int j) {
+    const int along = (side == 1 || side == 3) ? i : j;
+    const int g = a.M.ghost_index(side, along);
+    return a.M.gtype[g] == 6 ? g : -1;
+}
+
+// DELY of the GPORT sum (boundary.f90:230-305 walk) for a cell with node y y[4] seen from
+// `side`, and its derivative with respect to each node y.
+TNS_HD double port_dely(int side, const double y[4], double d[4]) {
+    const double sgn4[4][4] = {{0.5, 0.5, -0.5, -0.5}, {-0.5, 0.5, 0.5, -0.5}, {-0.5, -0.5, 0.5, 0.5},
+                               {0.5, -0.5, -0.5, 0.5}};
+    for (int n = 0; n < 4; n++) d[n] = sgn4[side - 1][n];
+    if (side == 1) return 0.5 * ((y[0] + y[1]) - (y[2] + y[3]));
+    if (side == 2) return 0.5 * ((y[1] + y[2]) - (y[0] + y[3]));
+    if (side == 3) return 0.5 * ((y[2] + y[3]) - (y[0] + y[1]));
+    return 0.5 * ((y[3] + y[0]) - (y[1] + y[2]));
+}
+
+TNS_HD void cell_y(const AdjArgs& a, int i, int j, double y[4]) {
+    const long long nw = a.nj + 1, n1 = (long long)i * nw + j;
+    y[0] = a.M.y[n1];
+    y[1] = a.M.y[n1 + nw];
+    y[2] = a.M.y[n1 + nw + 1];
+    y[3] = a.M.y[n1 + 1];
+}
+
+// GPORT of one port ghost: the sum over its line of C1 * U * DELY (* YCC for IAXIS=1)
+// (serial; the solver's k_gport sums the same terms in a block reduction).
+TNS_HD void gport_point(const AdjArgs& a, long long g, const double* q, double* out) {
+    int side, along;
+    const int ni = a.ni, nj = a.nj;
+    if (g < ni) { side = 1; along = (int)g; }
+    else if (g < ni + nj) { side = 2; along = (int)g - ni; }
+    else if (g < 2 * ni + nj) { side = 3; along = (int)g - ni - nj; }
+    else { side = 4; along = (int)g - 2 * ni - nj; }
+    if (a.M.gtype[g] != 6) return;
+    const int len = (side == 1 || side == 3) ? nj : ni;
+    double sum = 0.0;
+    for (int k = 0; k < len; k++) {
+        const int i = (side == 1 || side == 3) ? along : k, j = (side == 1 || side == 3) ? k : along;
+        const long long c = cell_of(a, i, j);
+        double y[4], d[4];
+        cell_y(a, i, j, y);
+        const double c1 = q[c], u = q[a.ncell + c] / c1;
+        double term = c1 * u * port_dely(side, y, d);
+        if (a.P.iaxis == 1) term = term * ((y[0] + y[1] + y[2] + y[3]) * 0.25);
+        sum += term;
+    }
+    out[g] = sum;
+}
+
+// Reverse of GPORT for one cell of the stage input: the port ghosts whose lines hold the
+// cell pass their adjoint to its C2 (C1 * (C2 / C1) * DELY [* YCC]; the C1 dependence
+// cancels).
+TNS_HD void port_point(const AdjArgs& a, long long cell) {
+    const int i = (int)(cell / a.nj), j = (int)(cell % a.nj);
+    double y[4], d[4], add = 0.0;
+    bool any = false;
+    for (int side = 1; side <= 4; side++) {
+        const int g = port_of(a, side, i, j);
+        if (g < 0) continue;
+        if (!any) cell_y(a, i, j, y);
+        any = true;
+        double f = port_dely(side, y, d);
+        if (a.P.iaxis == 1) f *= (y[0] + y[1] + y[2] + y[3]) * 0.25;
+        add += a.gportb[g] * f;
+    }
+    if (!any) return;
+    if (a.stage1) a.lam_old[a.ncell + cell] += add;
+    else a.lam_out[a.ncell + cell] += add;
+}
+
+// Node-y sensitivities of GPORT over the step's four stages, gathered per node from its
+// (up to four) cells.
+TNS_HD void port_node_point(const AdjArgs& a, long long node) {
+    const int na = (int)(node / (a.nj + 1)), nb = (int)(node % (a.nj + 1));
+    const int ng = a.M.nghosts();
+    double yb = 0.0;
+    for (int c4 = 0; c4 < 4; c4++) {
+        const int i = na - 1 + (c4 >> 1), j = nb - 1 + (c4 & 1);
+        if (!is_cell(a, i, j)) continue;
+        const int nn = ((na - i) << 1) | (nb - j);  // 0 (i,j) 2 (i+1,j) 3 (i+1,j+1) 1 (i,j+1)
+        const int corner = nn == 0 ? 0 : (nn == 2 ? 1 : (nn == 3 ? 2 : 3));
+        double y[4], d[4];
+        cell_y(a, i, j, y);
+        const double ycc = (y[0] + y[1] + y[2] + y[3]) * 0.25;
+        const long long c = cell_of(a, i, j);
+        for (int side = 1; side <= 4; side++) {
+            const int g = port_of(a, side, i, j);
+            if (g < 0) continue;
+            const double dely = port_dely(side, y, d);
+            for (int st = 0; st < 4; st++) {
+                const double* q = a.qst[st];
+                const double c1 = q[c];
+                const double mom = c1 * (q[a.ncell + c] / c1);
+                const double gb = a.gportb4[st * ng + g];
+                if (a.P.iaxis == 1) yb += gb * mom * (d[corner] * ycc + dely * 0.25);
+                else yb += gb * mom * d[corner];
+            }
+        }
+    }
+    a.ynbar[node] += yb;
 }
 
 // The adjoint of Q_n: residual / source / viscous part, dissipation / time-step part and

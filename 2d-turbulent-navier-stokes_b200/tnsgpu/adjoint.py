@@ -140,9 +140,9 @@ class Scheme:
                            (ii + 1) * (nj + 1) + jj + 2, ii * (nj + 1) + jj + 2], -1).reshape(-1, 4)
         if not np.array_equal(mesh.nod, expect):
             raise ValueError("mesh is not in structured (i, j) numbering")
-        if np.any((mesh.ntype < 2) | (mesh.ntype > 7) | (mesh.ntype == 6)):
-            bad = sorted(set(mesh.ntype.tolist()) - {2, 3, 4, 5, 7})
-            raise NotImplementedError(f"BC types {bad}: the adjoint covers types 2-5 and 7")
+        if np.any((mesh.ntype < 2) | (mesh.ntype > 7)):
+            bad = sorted(set(mesh.ntype.tolist()) - {2, 3, 4, 5, 6, 7})
+            raise NotImplementedError(f"BC types {bad}: the adjoint covers types 2-7")
         if flow.iaxis not in (0, 1):
             raise ValueError("IAXIS must be 0 or 1")
         self.fixed_rinit = rinit
@@ -174,6 +174,14 @@ class Scheme:
         self.g_opp = it(opp_i * nj + opp_j)
         self.g_pad = it(g_i * (nj + 2) + g_j)
         self.g_type = torch.cat([self.types[1], self.types[3], self.types[4], self.types[2]])
+        # type-6 burn-rate multiplier per ring ghost (bc.in order -> ring order)
+        inj = np.ones(2 * (ni + nj))
+        if mesh.inj_scale is not None:
+            ring_off = {1: 0, 3: ni, 4: 2 * ni, 2: 2 * ni + nj}
+            for k in range(mesh.nghosts):
+                sd = int(mesh.nside[k])
+                inj[ring_off[sd] + (pi[k] if sd in (1, 3) else pj[k])] = mesh.inj_scale[k]
+        self.g_inj = torch.tensor(inj, dtype=torch.float64, device=dev)
         self.types_present = sorted(set(int(t) for t in np.unique(mesh.ntype)))
         self.sensor_of = torch.tensor([0, 0, 0, 0, 1], dtype=torch.int64, device=dev)
         self._node_average_matrices(mesh)
@@ -306,12 +314,14 @@ class Scheme:
                             C[1], rho * u * u + p, f2, (C[3] + p) * u, rho * rt * u,
                             C[2], f2, rho * v * v + p, (C[3] + p) * v, rho * rt * v])
 
-    def _ghosts(self, pr, opp, prm: Params, ycg=None):
+    def _ghosts(self, pr, opp, prm: Params, ycg=None, port=None):
         """APPLY_BOUNDARY (boundary.f90:53-122, 310-327) for every ghost of the ring at
         once: parent field set ``pr`` [19, NG] and U, V, T, P of the cell opposite the
         boundary face ``opp`` [4, NG]; ``ycg`` [NG] the ghosts' mirrored centroid y
-        (type 7).  Each BC type present in the mesh is evaluated on the whole ring and
-        selected by the ghost's type."""
+        (types 6, 7); ``port`` the type-6 inputs per ring ghost (port mass flux, the
+        parent's face vector on the ghost side, the parent's centroid y).  Each BC type
+        present in the mesh is evaluated on the whole ring and selected by the ghost's
+        type."""
         flow = self.flow
         rr, cv, cp, g = prm.rr, prm.cv, prm.cp, flow.gama
 
@@ -349,6 +359,35 @@ class Scheme:
             sel[5] = torch.stack([u5, v5, pr[T_], P, rho5, rho5 * u5, rho5 * v5, rho5 * e5, -pr[C_ + 4],
                                   -pr[F_], 2.0 * P - pr[F_ + 1], -pr[F_ + 2], -pr[F_ + 3], -pr[F_ + 4],
                                   -pr[G_], -pr[G_ + 1], 2.0 * P - pr[G_ + 2], -pr[G_ + 3], -pr[G_ + 4]])
+        if 6 in self.types_present:  # mass injection (boundary.f90:128-163)
+            gport, psx, psy, ycp = port
+            six = self.g_type == 6
+            # the other ghosts of the ring get harmless inputs (on an axis the face vector
+            # and DHYD are 0): no NaN may reach the gradient through the unselected branch
+            psx = torch.where(six, psx, torch.ones_like(psx))
+            psy = torch.where(six, psy, torch.zeros_like(psy))
+            gport = torch.where(six, gport, torch.zeros_like(gport))
+            dnr = torch.sqrt(psx * psx + psy * psy)
+            enx, eny = -psx / dnr, -psy / dnr
+            dhyd = torch.abs(torch.where(six, ycg + ycp, torch.ones_like(ycg)))
+            gp = 2.0 * gport / (dhyd * dhyd) if flow.iaxis == 1 else gport / dhyd
+            rho0, p6 = pr[C_], pr[P_]
+            rdot = flow.acomb * (p6 * (1.0 / 98066.5)) ** flow.ancomb * self.g_inj
+            vel = flow.rhoprop / rho0 * rdot
+            u1 = vel * enx + vel * enx - pr[U_]
+            v1 = vel * eny + vel * eny - pr[V_]
+            t1 = flow.tflame - 0.5 * (u1 * u1 + v1 * v1) / cp
+            gval = (gp / (flow.rhoprop * rdot)) * (flow.rhoprop * rdot * dhyd / self.amu(t1)) ** (-0.125)
+            ero = gval > 35.0  # GTH
+            gsafe = torch.where(ero, gval, torch.full_like(gval, 35.0))
+            rdoteb = torch.where(ero, rdot * (1.0 + 0.023 * (gsafe ** 0.8 - 35.0 ** 0.8)), rdot)
+            vel = flow.rhoprop / rho0 * rdoteb
+            u6 = vel * enx + vel * enx - pr[U_]
+            v6 = vel * eny + vel * eny - pr[V_]
+            t6 = flow.tflame - 0.5 * (u6 * u6 + v6 * v6) / cp
+            rho6 = p6 / (rr * t6)
+            c5 = rho6 * (self.amu(t6) / rho6)
+            sel[6] = state(rho6, u6, v6, t6, p6, c5, c5 * u6, c5 * v6)
         if 7 in self.types_present:  # boundary-layer inlet, 1/7-power profile (boundary.f90:310-327)
             tinf = prm.t0 / (1.0 + 0.5 * (g - 1.0) * flow.aminf ** 2)
             blu = 2.0 * flow.aminf * torch.sqrt(g * rr * tinf)
@@ -375,15 +414,39 @@ class Scheme:
         flat = W.reshape(NW_, -1)
         pr = flat.index_select(1, self.g_par)
         opp = flat[:4].index_select(1, self.g_opp)
-        ycg = None
-        if 7 in self.types_present:
+        ycg = port = None
+        if 6 in self.types_present or 7 in self.types_present:
             if geo is None:
-                raise ValueError("BC type 7 needs the geometry")
+                raise ValueError("BC types 6 and 7 need the geometry")
             ycg = geo["yc"].reshape(-1).index_select(0, self.g_pad)
-        gh = self._ghosts(pr, opp, prm, ycg)
+        if 6 in self.types_present:
+            port = self._port_inputs(W, geo)
+        gh = self._ghosts(pr, opp, prm, ycg, port)
         npad = (self.ni + 2) * (self.nj + 2)
         ring = torch.zeros((NW_, npad), dtype=W.dtype, device=W.device).index_copy(1, self.g_pad, gh)
         return torch.nn.functional.pad(W, (1, 1, 1, 1)) + ring.reshape(NW_, self.ni + 2, self.nj + 2)
+
+    def _port_inputs(self, W, geo):
+        """Type-6 inputs per ring ghost: the port mass flux GPORT, the sum over the
+        cells of the ghost's line (the parent's column across to the opposite side) of
+        C1 * U * DELY (* YCC for IAXIS=1), DELY the cell's extent normal to the ghost's
+        side from its node y; and the parent's face vector and centroid y."""
+        y = geo["y"]
+        Y1, Y2, Y3, Y4 = y[:-1, :-1], y[1:, :-1], y[1:, 1:], y[:-1, 1:]
+        c1 = W[C_]
+        term = c1 * (W[C_ + 1] / c1)
+        if self.flow.iaxis == 1:
+            term = term * ((Y1 + Y2 + Y3 + Y4) * 0.25)
+        g1 = torch.sum(term * (0.5 * ((Y1 + Y2) - (Y3 + Y4))), dim=1)
+        g3 = torch.sum(term * (0.5 * ((Y3 + Y4) - (Y1 + Y2))), dim=1)
+        g4 = torch.sum(term * (0.5 * ((Y4 + Y1) - (Y2 + Y3))), dim=0)
+        g2 = torch.sum(term * (0.5 * ((Y2 + Y3) - (Y1 + Y4))), dim=0)
+        gport = torch.cat([g1, g3, g4, g2])
+        sx, sy = geo["sx"], geo["sy"]
+        psx = torch.cat([sx[0][:, 0], sx[2][:, -1], sx[3][0, :], sx[1][-1, :]])
+        psy = torch.cat([sy[0][:, 0], sy[2][:, -1], sy[3][0, :], sy[1][-1, :]])
+        ycp = geo["yc"][1:-1, 1:-1].reshape(-1).index_select(0, self.g_par)
+        return gport, psx, psy, ycp
 
     @staticmethod
     def _nb(a):

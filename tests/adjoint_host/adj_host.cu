@@ -14,7 +14,7 @@ using namespace tns::adj;
 
 extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double* x, const double* y,
                              const double* cfldl, const int* gtype, const int* grank, const double* gxc,
-                             const double* gyc, const double* q0, const double* q1, const double* q2,
+                             const double* gyc, const double* ginj, const double* q0, const double* q1, const double* q2,
                              const double* q3, const double* D, const double* VIS, const double* DT,
                              double dtmin, double* lam, int geo, double* sens) {
     AdjArgs a{};
@@ -28,6 +28,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.M.grank = grank;
     a.M.gxc = gxc;
     a.M.gyc = gyc;
+    a.M.ginj = ginj;
     a.ni = ni;
     a.nj = nj;
     a.ncell = (long long)ni * nj;
@@ -41,6 +42,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
         srcn(16 * n), srcg(8 * n), wself(5 * n), wvisc(5 * a.npad, 0.0), dbar(5 * n), visbar(4 * n), dtbar(n),
         dpre(NDPRE * n), dout(NDOUT * n), navg(NNA * a.nnode), nbar(5 * a.nnode), vfi(NVF * a.nif),
         vfj(NVF * a.njf), xcs(a.npad), ycs(a.npad);
+    const long long ng = 2LL * (ni + nj);
+    std::vector<double> gport(4 * ng, 0.0), gportb(4 * ng, 0.0), portacc(3 * ng, 0.0);
     std::vector<int> ninfo(a.nnode);
     double dts = 0.0;
     a.qold = q0;
@@ -72,6 +75,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.vfj = vfj.data();
     a.dtsum = &dts;
     a.geo = geo;
+    a.gportb4 = gportb.data();
+    a.portacc = portacc.data();
     double* sp = sens;
     a.sxbar = sp; sp += 4 * n;
     a.sybar = sp; sp += 4 * n;
@@ -88,6 +93,10 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     for (long long p = 0; p < a.npad; p++) centroid_point(a, p);
     const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
     const double* qs[4] = {q0, q1, q2, q3};
+    for (int k = 0; k < 4; k++) {
+        a.qst[k] = qs[k];
+        for (long long g = 0; g < ng; g++) gport_point(a, g, qs[k], gport.data() + k * ng);
+    }
     double* lam_stage[5] = {nullptr, lamA.data(), lamB.data(), lamA.data(), lam};  // adjoint of Q_k
     for (int st = 3; st >= 0; st--) {
         a.qin = qs[st];
@@ -98,6 +107,8 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
         a.lam_out = lam_stage[st];
         a.w = w.data() + (size_t)st * NWROW * a.npad;
         a.gbar = gbar.data() + (size_t)st * 5 * a.npad;
+        a.gport = gport.data() + st * ng;
+        a.gportb = gportb.data() + st * ng;
         for (long long p = 0; p < a.npad; p++) s0_point(a, p);
         for (long long c = 0; c < n; c++) s1_point(a, c);
         if (st == 0) {
@@ -105,11 +116,14 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
             for (long long f = 0; f < a.nif + a.njf; f++) v1_point(a, f);
             for (long long k = 0; k < a.nnode; k++) v2_point(a, k);
             for (long long p = 0; p < a.npad; p++) v3_point(a, p);
-            if (geo)
-                for (long long c = 0; c < n; c++) geo_point(a, c);
         }
         for (long long c = 0; c < n; c++) s3_point(a, c);
         for (long long c = 0; c < band_count(a); c++) s3g_point(a, c);
+        for (long long c = 0; c < n; c++) port_point(a, c);
+    }
+    if (geo) {
+        for (long long c = 0; c < n; c++) geo_point(a, c);
+        for (long long k = 0; k < a.nnode; k++) port_node_point(a, k);
     }
     for (long long c = 0; c < n; c++) d0_point(a, c);
     for (long long c = 0; c < n; c++) d1_point(a, c);

@@ -24,6 +24,12 @@ CASES = {
     "global_dt": lambda: (cases.ramp_mesh(20, 10),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
     "bl_inlet": lambda: _bl_inlet(24, 12),
+    "port": lambda: (cases.port_mesh(16, 8), cases.port_flow()),
+    "port_burn_law": lambda: (cases.port_mesh(16, 8, seed=3),
+                              formats.Flow(**{**cases.port_flow().__dict__, "ancomb": 0.3})),
+    # a burn rate small enough for the erosive branch (GVAL > GTH) at every port ghost
+    "port_erosive": lambda: (cases.port_mesh(16, 8, seed=4),
+                             formats.Flow(**{**cases.port_flow().__dict__, "ancomb": 0.3, "acomb": 1.0e-6})),
 }
 
 
@@ -55,7 +61,8 @@ def test_restatement_matches_oracle(name):
 
 
 def test_unsupported_boundary_types_are_refused():
-    mesh, flow = cases.port_mesh(16, 8), cases.port_flow()
+    mesh, flow = cases.ramp_mesh(16, 8), cases.ramp_flow()
+    mesh.ntype[0] = 9
     with pytest.raises(NotImplementedError):
         adjoint.Scheme(mesh, flow)
 

@@ -34,6 +34,12 @@ CASES = {
     "global_dt": lambda: (cases.ramp_mesh(20, 10),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
     "bl_inlet": lambda: _bl_inlet(24, 12),
+    "port": lambda: (cases.port_mesh(16, 8), cases.port_flow()),
+    "port_burn_law": lambda: (cases.port_mesh(16, 8, seed=3),
+                              formats.Flow(**{**cases.port_flow().__dict__, "ancomb": 0.3})),
+    # a burn rate small enough for the erosive branch (GVAL > GTH) at every port ghost
+    "port_erosive": lambda: (cases.port_mesh(16, 8, seed=4),
+                             formats.Flow(**{**cases.port_flow().__dict__, "ancomb": 0.3, "acomb": 1.0e-6})),
 }
 
 
@@ -95,7 +101,12 @@ def _ghost_layout(mesh, sch, geo):
     xg, yg = geo["xc"].detach().numpy(), geo["yc"].detach().numpy()
     gx = np.concatenate([xg[1:-1, 0], xg[-1, 1:-1], xg[1:-1, -1], xg[0, 1:-1]])
     gy = np.concatenate([yg[1:-1, 0], yg[-1, 1:-1], yg[1:-1, -1], yg[0, 1:-1]])
-    return gtype, grank, np.ascontiguousarray(gx), np.ascontiguousarray(gy)
+    ginj = np.ones(ng)
+    if mesh.inj_scale is not None:
+        for L in range(mesh.nghosts):
+            s = int(mesh.nside[L])
+            ginj[off[s] + (pi[L] if s in (1, 3) else pj[L])] = mesh.inj_scale[L]
+    return gtype, grank, np.ascontiguousarray(gx), np.ascontiguousarray(gy), ginj
 
 
 def _state(mesh, flow, sch, rinit, seed):
@@ -138,7 +149,7 @@ def _run(harness, name, seed=0):
     grads = [g if g is not None else torch.zeros_like(l) for g, l in zip(grads, leaves)]
     # the harness
     f = lambda t: np.ascontiguousarray(t.detach().numpy().reshape(-1), np.float64)
-    gtype, grank, gx, gy = _ghost_layout(mesh, sch, geo0)
+    gtype, grank, gx, gy, ginj = _ghost_layout(mesh, sch, geo0)
     x, y = f(sch.x0), f(sch.y0)
     cfldl = f(flow.cfl * geo0["dl"])
     q = [f(c) for c in Cs[:4]]
@@ -150,7 +161,7 @@ def _run(harness, name, seed=0):
     prms = make_params(flow, rinit, 0)
     P = lambda a: a.ctypes.data_as(C.c_void_p)
     rc = harness.adj_host_step(C.byref(prms), ni, nj, P(x), P(y), P(cfldl), P(gtype), P(grank), P(gx), P(gy),
-                               P(q[0]), P(q[1]), P(q[2]), P(q[3]), P(Dn), P(Vn), P(DTn), C.c_double(dtmin),
+                               P(ginj), P(q[0]), P(q[1]), P(q[2]), P(q[3]), P(Dn), P(Vn), P(DTn), C.c_double(dtmin),
                                P(lam_io), 1, P(sens))
     assert rc == 0
     return sch, grads, lam_io, sens

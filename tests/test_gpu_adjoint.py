@@ -110,6 +110,9 @@ STEP_CASES = {
     "global_dt": lambda: (cases.ramp_mesh(40, 16),
                           formats.Flow(**{**cases.ramp_flow().__dict__, "local": 0})),
     "bl_inlet": lambda: _bl_inlet(48, 20),
+    "port": lambda: (cases.port_mesh(48, 16), cases.port_flow()),
+    "port_erosive": lambda: (cases.port_mesh(48, 16, seed=4),
+                             formats.Flow(**{**cases.port_flow().__dict__, "ancomb": 0.3, "acomb": 1.0e-6})),
 }
 
 
