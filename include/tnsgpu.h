@@ -169,7 +169,7 @@ void tns_destroy(tns_handle *h);
 /* ---- Discrete adjoint of one FP64 RK4 iteration (no counterpart in the reference,
  * which has no adjoint).  For the iteration map Q_{n+1} = G(Q_n) of
  * turbnstwod.f90:95-146 -- DT, DISSIPATION, and four stages of PRIMITIVE_VARS,
- * APPLY_BOUNDARY (types 2-5, 7), VISCOUS (stage 1), SOURCE_TERMS, RESIDUAL, UPDATE --
+ * APPLY_BOUNDARY (types 2-7, with the type-6 port mass flux), VISCOUS (stage 1), SOURCE_TERMS, RESIDUAL, UPDATE --
  * tns_adjoint_step replaces lambda = dJ/dQ_{n+1} by lambda dG/dQ_n, recomputing the
  * iteration from the checkpoint Q_n on the device.  Non-smooth points (DMAX1 / DMIN1,
  * |x|, the C5 clip, the sensor maxima) take the branch the forward took.  With
@@ -181,7 +181,8 @@ void tns_destroy(tns_handle *h);
  * in that order (tns_adjoint_sensitivity_size values), which a caller maps to node
  * displacements and flow parameters with the derivatives of COMPUTE_GEOMETRY and of its
  * parameter formulas.  Requirements: an FP64 handle, cells numbered in (i, j) order
- * (faces 1..4 = j-, i+, j+, i-), at least 3 x 3 cells, BC types 2-5 and 7.  Device arrays are
+ * (faces 1..4 = j-, i+, j+, i-), at least 3 x 3 cells.  The type-6 port ghosts' node-y
+ * sensitivities (through the port mass flux) are part of the node-coordinate block.  Device arrays are
  * [5][NELES] component-major in that order; calls are asynchronous on the handle's
  * stream (tns_set_stream). */
 #define TNS_ADJ_SENSITIVITIES 1
