@@ -6,7 +6,7 @@ cold-start Mach number AMACHINIT and mesh-node coordinates (wall shape):
 
 * ``Scheme`` restates one RK4 iteration of the solver (turbnstwod.f90:95-146 with
   DISSIPATION solver_state.f90:70-225, COMPUTE_PRIMITIVE_VARS turbnstwod.f90:204-227,
-  APPLY_BOUNDARY boundary.f90:24-122 for BC types 2-5, COMPUTE_VISCOUS
+  APPLY_BOUNDARY boundary.f90:24-327 for BC types 2-7, COMPUTE_VISCOUS
   viscous.f90:29-217, COMPUTE_SOURCE_TERMS source_terms.f90:24-104, COMPUTE_RESIDUAL and
   UPDATE_SOLUTION residual.f90:23-83) in FP64 PyTorch tensor arithmetic on the
   structured i x j block, so torch.autograd differentiates it exactly.  Geometry (face
