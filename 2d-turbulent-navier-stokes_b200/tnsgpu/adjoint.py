@@ -795,7 +795,8 @@ class GraphedStep:
 def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, amachinit=None,
                        dy: Optional[torch.Tensor] = None, space: Optional[DesignSpace] = None,
                        niter: int = 100, states: Optional[np.ndarray] = None, primal: str = "gpu",
-                       lib=None, graph: Optional[bool] = None, engine: Optional[str] = None) -> dict:
+                       lib=None, graph: Optional[bool] = None, engine: Optional[str] = None,
+                       max_states: Optional[int] = None) -> dict:
     """dJ/d(P0, T0, AMACHINIT, dy) of J = objective(scheme, Q_N, geo, prm), Q_0 the cold
     start, Q_N after ``niter`` RK4 iterations.
 
@@ -805,7 +806,10 @@ def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, am
     sensitivities to geometry, RTOLERANCE, S0 and T0; one torch backward through
     COMPUTE_GEOMETRY and the parameter formulas maps those to the gradient.  ``states``
     (optional) are checkpoints [N+1, 5, NI, NJ]; the result's "states" is the device
-    tensor of checkpoints.
+    tensor of checkpoints.  ``max_states`` bounds the device states held at once: the
+    sweep then keeps snapshots at recursive bisection points and recomputes each
+    segment's states from its snapshot (O(N log2(N / max_states)) extra primal
+    iterations, the same gradient bit for bit; "states" is then None).
 
     ``engine="torch"`` (the default on the CPU): the primal runs on the GPU FP64 path
     (``primal="gpu"``) or in the restatement (``"torch"``); ``states`` may pass
@@ -815,7 +819,8 @@ def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, am
     if engine is None:
         engine = "cuda" if scheme.device.type == "cuda" else "torch"
     if engine == "cuda":
-        return _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib)
+        return _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib,
+                                        max_states)
     if engine != "torch":
         raise ValueError(f"engine {engine!r}: 'cuda' or 'torch'")
     dev = scheme.device
@@ -1114,7 +1119,74 @@ def _leaves(scheme, p0, t0, amachinit, dy):
     return [P0, T0, AM] + ([dy] if dy is not None else []), dy
 
 
-def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib) -> dict:
+class _Checkpoints:
+    """Bounded device memory for the reverse sweep: ``cap`` state slots.  ``sweep(lo,
+    hi, slot)`` runs the reverse steps hi-1 .. lo from the state at iteration lo (held in
+    ``slot``).  If the segment's states fit in the free slots, they are recomputed and
+    stored, then reversed; with one free slot left, each state is recomputed from the
+    snapshot in turn; otherwise the state at the midpoint is recomputed into a slot, the
+    upper half is swept, the slot is released and the lower half is swept (recursive
+    bisection, a revolve-style schedule)."""
+
+    def __init__(self, dev_adj: "DeviceAdjoint", cap: int, shape, device):
+        if cap < 2:
+            raise ValueError("max_states must be at least 2")
+        self.dev, self.cap = dev_adj, cap
+        self.pool = torch.empty((cap,) + tuple(shape), dtype=torch.float64, device=device)
+        self.free = list(range(cap - 1, -1, -1))
+        self.recomputed = 0
+
+    def take(self) -> int:
+        return self.free.pop()
+
+    def give(self, k: int):
+        self.free.append(k)
+
+    def advance(self, src: int, n: int, dst: int):
+        """Slot dst <- the state n primal iterations after the one in slot src."""
+        s = self.dev.solver
+        self.dev._enter()
+        s.state_from_device(self.pool[src].data_ptr())
+        if n:
+            s.enqueue(n)
+        s.state_to_device(self.pool[dst].data_ptr())
+        self.dev._leave()
+        self.recomputed += n
+
+    def sweep(self, lo: int, hi: int, slot: int, lam: torch.Tensor, sens: bool):
+        n = hi - lo
+        if n <= 0:
+            return
+        if n - 1 <= len(self.free):
+            slots = [slot]
+            for _ in range(n - 1):
+                k = self.take()
+                self.advance(slots[-1], 1, k)
+                slots.append(k)
+            for m in range(n - 1, -1, -1):
+                self.dev.step(self.pool[slots[m]], lam, sens)
+            for k in slots[1:]:
+                self.give(k)
+            return
+        if len(self.free) == 1:
+            # one slot left: each state of the segment recomputed from the snapshot
+            k = self.take()
+            for m in range(hi - 1, lo, -1):
+                self.advance(slot, m - lo, k)
+                self.dev.step(self.pool[k], lam, sens)
+            self.give(k)
+            self.dev.step(self.pool[slot], lam, sens)
+            return
+        mid = lo + n // 2
+        k = self.take()
+        self.advance(slot, mid - lo, k)
+        self.sweep(mid, hi, k, lam, sens)
+        self.give(k)
+        self.sweep(lo, mid, slot, lam, sens)
+
+
+def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib,
+                             max_states=None) -> dict:
     if scheme.device.type != "cuda":
         raise ValueError("engine='cuda' needs a Scheme on a CUDA device")
     params, dy = _leaves(scheme, p0, t0, amachinit, dy)
@@ -1124,6 +1196,33 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
     with torch.no_grad():
         c0 = scheme.cold_state(prm).contiguous()
     dev_adj = DeviceAdjoint(scheme, space, prm, dy, lib)
+    if states is None and max_states is not None and max_states < niter + 1:
+        try:
+            cp = _Checkpoints(dev_adj, max_states, c0.shape, scheme.device)
+            root = cp.take()
+            cp.pool[root].copy_(c0)
+            top = cp.take()
+            cp.advance(root, niter, top)  # Q_N (the primal itself)
+            QN = cp.pool[top].clone().requires_grad_(True)
+            cp.give(top)
+            x, y = space.coords(dy)
+            J = objective(scheme, QN, scheme.geometry(x, y), prm)
+            g = torch.autograd.grad(J, [QN] + params, allow_unused=True)
+            grads = [v.detach() if v is not None else torch.zeros_like(p) for v, p in zip(g[1:], params)]
+            lam = g[0].detach().contiguous()
+            cp.recomputed = 0
+            cp.sweep(0, niter, root, lam, True)
+            sens = dev_adj.sensitivities()
+        finally:
+            dev_adj.close()
+        gp = _parameter_gradient(scheme, space, params, dy, sens, lam)
+        grads = [a + b for a, b in zip(grads, gp)]
+        out = {"J": float(J.detach()), "dJ_dp0": float(grads[0]), "dJ_dt0": float(grads[1]),
+               "dJ_damachinit": float(grads[2]), "lambda0": lam, "states": None,
+               "recomputed_iterations": cp.recomputed}
+        if dy is not None:
+            out["dJ_ddy"] = grads[3].detach().cpu().numpy()
+        return out
     try:
         if states is None:
             st = dev_adj.primal(c0, niter)

@@ -243,3 +243,20 @@ def test_frozen_adjoint_steps_equal_full_steps():
     finally:
         dev.close()
     assert torch.equal(runs[0][0], runs[1][0]) and torch.equal(runs[0][1], runs[1][1])
+
+
+def test_bounded_memory_sweep_equals_stored_states():
+    """max_states: snapshots at bisection points, segments recomputed from them (the
+    primal is deterministic, so the gradient is the same bit for bit)."""
+    mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
+    dy = torch.tensor([2e-5], dtype=torch.float64)
+    N = 30
+    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, engine="cuda")
+    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, engine="cuda",
+                                   max_states=4)
+    assert b["states"] is None and b["recomputed_iterations"] > N
+    assert a["J"] == b["J"]
+    for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
+        assert a[k] == b[k], (k, a[k], b[k])
+    assert np.array_equal(a["dJ_ddy"], b["dJ_ddy"])
+    assert torch.equal(a["lambda0"], b["lambda0"])
