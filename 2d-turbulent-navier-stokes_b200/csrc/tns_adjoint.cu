@@ -117,9 +117,10 @@ struct tns_adjoint_state {
     // the lowest priority, so that the reverse -- the critical path -- keeps its SMs
     cudaStream_t hp = nullptr;
     cudaEvent_t ev = nullptr;
-    // [set][mode: bit 0 forward first, bit 1 prefetch the other set][sensitivities]
-    cudaGraphExec_t graph[2][4][2] = {};
-    long long per_step[2][4][2] = {};
+    // [set][mode: bit 0 forward first, bit 1 prefetch the other set][sensitivities: none,
+    // scalars, all]
+    cudaGraphExec_t graph[2][4][3] = {};
+    long long per_step[2][4][3] = {};
     long long launches = 0;
 };
 
@@ -174,7 +175,8 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int set, int geo) {
     a.vfi = s->vfi.p;
     a.vfj = s->vfj.p;
     a.dtsum = s->dtsum.p;
-    a.geo = geo;
+    a.sens = geo >= 1;  // geo: 0 none, 1 scalars (RTOLERANCE, T0, S0), 2 everything
+    a.geo = geo >= 2;
     double* sp = s->sens.p;
     const long long n = a.ncell;
     a.sxbar = sp; sp += 4 * n;
@@ -305,7 +307,7 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
             nl++;
         }
     }
-    if (geo) {
+    if (geo >= 2) {
         // face-vector (and port) sensitivities of the whole step on their own branch
         fork(s->side[2]);
         launch_points(k_adj_geo, a, a.ncell, s->side[2]);
@@ -316,7 +318,7 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
         }
     }
     join(s->side[0]);
-    if (geo) join(s->side[2]);
+    if (geo >= 2) join(s->side[2]);
     a.lam_out = s->lam.p;
     launch_points(k_adj_final, a, a.ncell, st);
     return nl + 1;
@@ -459,7 +461,7 @@ int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_ne
     int rc;
     if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
     tns_adjoint_state* s = h->adj;
-    const int geo = flags & TNS_ADJ_SENSITIVITIES ? 1 : 0;
+    const int geo = (flags & TNS_ADJ_SENSITIVITIES) ? 2 : ((flags & TNS_ADJ_SCALARS) ? 1 : 0);
     const int frozen = flags & TNS_ADJ_FROZEN ? 1 : 0;
     if (frozen && !s->have_forward)
         return h->fail(TNS_ERR_STATE, "tns_adjoint_step: TNS_ADJ_FROZEN before any step without it");

@@ -99,8 +99,9 @@ struct AdjArgs {
     const double* gportb4; // the four stages' [4][nghost]
     const double* qst[4];  // the four stage inputs (column terms of GPORT)
     double* portacc;       // parent face vector x, y and centroid y adjoints per ghost [3][nghost]
-    // parameter sensitivities (accumulated when geo != 0)
-    int geo;
+    // parameter sensitivities: sens != 0 accumulates RTOLERANCE, T0 and S0; geo != 0 (which
+    // implies sens) also every geometric quantity
+    int sens, geo;
     double *sxbar, *sybar;   // [4][ncell] face vectors
     double *volbar, *dlbar;  // [ncell]
     double *xcbar, *ycbar;   // [npad] centroids (ghost ring: mirrored centroids)
@@ -805,10 +806,10 @@ TNS_HD void s1_point(const AdjArgs& a, long long cell) {
         a.srcg[(k * 2 + 0) * a.ncell + cell] = b.nx[k];
         a.srcg[(k * 2 + 1) * a.ncell + cell] = b.ny[k];
     }
+    if (a.sens) a.rtolc[cell] += rtolb;
     if (a.geo) {  // (the face-vector part of the residual reverse: geo_point)
         a.volbar[cell] += volb;
         a.ycbar[ps] += b.ycc;
-        a.rtolc[cell] += rtolb;
     }
 }
 
@@ -999,7 +1000,7 @@ TNS_HD void s3g_point(const AdjArgs& a, long long idx) {
         prim_adj(a.P, q, wb, qb);
     }
     for (int m = 0; m < 5; m++) a.lamg[m * a.ncell + cell] = qb[m];
-    if (a.geo) {
+    if (a.sens) {
         a.t0bar[cell] += t0b;
         a.s0bar[cell] += s0b;
     }
@@ -1291,10 +1292,10 @@ TNS_HD void v2_point(const AdjArgs& a, long long node) {
         a.nbar[c * a.nnode + node] = s[c];
     }
     if ((info >> NI_RESET) & 1) rtolb += s[4] * a.P.rtred;
+    if (a.sens) a.rtoln[node] += rtolb;
     if (a.geo) {
         a.xnbar[node] += xb;
         a.ynbar[node] += yb;
-        a.rtoln[node] += rtolb;
     }
 }
 
@@ -1552,10 +1553,10 @@ TNS_HD void d2_point(const AdjArgs& a, long long cell) {
     ts_adj(P, q, a.M.cfldl[cell], pb, P.local ? dtb : 0.0, qb, dlb);
     if (!P.local) a.dtbar[cell] = dtb;
     for (int m = 0; m < 5; m++) a.lamd[m * n + cell] = qb[m];
+    if (a.sens) a.rtolc[cell] += rtolb;
     if (a.geo) {
         a.volbar[cell] += volb;
         a.dlbar[cell] += dlb;
-        a.rtolc[cell] += rtolb;
     }
 }
 

@@ -1059,9 +1059,10 @@ class DeviceAdjoint:
         self._leave()
         return states
 
-    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities: bool, frozen: bool = False,
+    def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities, frozen: bool = False,
              q_next: Optional[torch.Tensor] = None):
-        """``frozen``: q is the previous step's state (its forward values are reused).
+        """``sensitivities``: True (all), "scalars" (RTOLERANCE, T0, S0) or False.
+        ``frozen``: q is the previous step's state (its forward values are reused).
         ``q_next``: the state of the next step, whose forward values are computed beside
         this reverse (it must stay unchanged until that step)."""
         for t in (q, lam) + ((q_next,) if q_next is not None else ()):
@@ -1211,7 +1212,7 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
             grads = [v.detach() if v is not None else torch.zeros_like(p) for v, p in zip(g[1:], params)]
             lam = g[0].detach().contiguous()
             cp.recomputed = 0
-            cp.sweep(0, niter, root, lam, True)
+            cp.sweep(0, niter, root, lam, True if dy is not None else "scalars")
             sens = dev_adj.sensitivities()
         finally:
             dev_adj.close()
@@ -1237,8 +1238,10 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
         g = torch.autograd.grad(J, [QN] + params, allow_unused=True)
         grads = [v.detach() if v is not None else torch.zeros_like(p) for v, p in zip(g[1:], params)]
         lam = g[0].detach().contiguous()
+        # without node displacements only the scalar sensitivities are needed
+        mode = True if dy is not None else "scalars"
         for n in range(niter - 1, -1, -1):
-            dev_adj.step(st[n], lam, True)
+            dev_adj.step(st[n], lam, mode)
         sens = dev_adj.sensitivities()
     finally:
         dev_adj.close()

@@ -143,14 +143,15 @@ class Solver:
         """Loads the state from device memory at ``ptr`` ([5][NELES] doubles), async."""
         self._check(self.L.tns_copy_state_device(self.h, C.c_void_p(int(ptr)), 1))
 
-    def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities: bool = False, frozen: bool = False,
+    def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities=False, frozen: bool = False,
                      q_next_ptr: Optional[int] = None):
         """lambda <- lambda dG/dQ_n for the iteration from Q_n (both device pointers);
-        with ``sensitivities`` also accumulates lambda dG/dp; with ``frozen`` Q_n is the
-        previous call's state and its forward values are reused; ``q_next_ptr`` (the
-        next call's Q_n) has its forward values computed beside this reverse
-        (tns_adjoint_step_next)."""
-        flags = (1 if sensitivities else 0) | (2 if frozen else 0)
+        with ``sensitivities`` also accumulates lambda dG/dp (True: all of them;
+        "scalars": RTOLERANCE, T0 and S0 only); with ``frozen`` Q_n is the previous
+        call's state and its forward values are reused; ``q_next_ptr`` (the next call's
+        Q_n) has its forward values computed beside this reverse (tns_adjoint_step_next)."""
+        sens = 4 if sensitivities == "scalars" else (1 if sensitivities else 0)
+        flags = sens | (2 if frozen else 0)
         nxt = C.c_void_p(int(q_next_ptr)) if q_next_ptr else None
         self._check(self.L.tns_adjoint_step_next(self.h, C.c_void_p(int(q_ptr)) if q_ptr else None, nxt,
                                                  C.c_void_p(int(lam_ptr)), flags))

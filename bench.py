@@ -337,6 +337,10 @@ def adjoint_timing(torch, dev, K=50, W=5):
         launches0 = s.adjoint_launch_count()
         step_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), True))
         per_step = (s.adjoint_launch_count() - launches0) // K
+        # the same sweep for flow-parameter gradients only (no geometric sensitivities)
+        for n in range(W):
+            s.adjoint_step(st[n].data_ptr(), lam.data_ptr(), "scalars")
+        scalars_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), "scalars"))
         q = st[K].contiguous()
         s.adjoint_step(q.data_ptr(), lam.data_ptr(), False)
         for _ in range(W):
@@ -350,6 +354,7 @@ def adjoint_timing(torch, dev, K=50, W=5):
             "transient_step_us": round(step_us, 2),
             "fixed_point_step_us": round(frozen_us, 2),
             "transient_step_over_primal": round(step_us / primal_us, 3),
+            "transient_step_flow_parameters_us": round(scalars_us, 2),
             "fixed_point_step_over_primal": round(frozen_us / primal_us, 3),
             "transient_gradient_over_primal": round((primal_us + step_us) / primal_us, 3),
             "kernels_per_transient_step": int(per_step)}

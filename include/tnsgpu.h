@@ -190,6 +190,10 @@ void tns_destroy(tns_handle *h);
  * values kept from that call are reused, which skips the recomputed iteration and every
  * state-only pass -- the fixed-point adjoint at a converged state. */
 #define TNS_ADJ_FROZEN 2
+/* TNS_ADJ_SCALARS: accumulate only the RTOLERANCE, T0 and S0 sensitivities (enough for
+ * gradients with respect to P0, T0 and AMACHINIT); the geometric blocks stay untouched.
+ * TNS_ADJ_SENSITIVITIES (everything) takes precedence. */
+#define TNS_ADJ_SCALARS 4
 int tns_adjoint_enable(tns_handle *h);
 int tns_adjoint_step(tns_handle *h, const double *d_q, double *d_lam, int flags);
 /* The same step, with the forward values of the next checkpoint d_q_next (the state the

@@ -74,6 +74,7 @@ extern "C" int adj_host_step(const tns_params* prm, int ni, int nj, const double
     a.vfi = vfi.data();
     a.vfj = vfj.data();
     a.dtsum = &dts;
+    a.sens = geo;
     a.geo = geo;
     a.gportb4 = gportb.data();
     a.portacc = portacc.data();

@@ -260,3 +260,15 @@ def test_bounded_memory_sweep_equals_stored_states():
         assert a[k] == b[k], (k, a[k], b[k])
     assert np.array_equal(a["dJ_ddy"], b["dJ_ddy"])
     assert torch.equal(a["lambda0"], b["lambda0"])
+
+
+def test_scalar_sensitivities_equal_full_ones():
+    """Without node displacements the sweep accumulates only the RTOLERANCE, T0 and S0
+    sensitivities (TNS_ADJ_SCALARS): the P0, T0, AMACHINIT gradient is unchanged."""
+    mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
+    N = 20
+    a = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=torch.zeros(1, dtype=torch.float64),
+                                   space=space, niter=N, engine="cuda")
+    b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, niter=N, engine="cuda")
+    for k in ("J", "dJ_dp0", "dJ_dt0", "dJ_damachinit"):
+        assert a[k] == b[k], (k, a[k], b[k])
