@@ -272,3 +272,34 @@ def test_scalar_sensitivities_equal_full_ones():
     b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, niter=N, engine="cuda")
     for k in ("J", "dJ_dp0", "dJ_dt0", "dJ_damachinit"):
         assert a[k] == b[k], (k, a[k], b[k])
+
+
+def test_adjoint_abi_errors_leave_the_handle_usable():
+    """Refusals are return codes with a message: a mixed-precision handle, a frozen step
+    before any full step, a sensitivity buffer of the wrong size."""
+    import ctypes as C
+    from tnsgpu import _lib
+    mesh, flow = cases.ramp_mesh(32, 12), cases.ramp_flow()
+    rinit = formats.rinit_cold(flow)
+    mx = Solver(mesh, flow, rinit, precision=1)
+    try:
+        assert mx.L.tns_adjoint_enable(mx.h) == _lib.TNS_ERR_ARG
+        assert b"FP64" in mx.L.tns_last_error(mx.h)
+    finally:
+        mx.close()
+    s = Solver(mesh, flow, rinit, precision=0)
+    try:
+        q = torch.tensor(formats.cold_state(flow, mesh.neles, rinit), device="cuda").contiguous()
+        lam = torch.ones_like(q)
+        torch.cuda.synchronize()
+        rc = s.L.tns_adjoint_step(s.h, C.c_void_p(q.data_ptr()), C.c_void_p(lam.data_ptr()), 2)
+        assert rc == _lib.TNS_ERR_STATE, rc
+        n = int(s.L.tns_adjoint_sensitivity_size(s.h))
+        buf = np.zeros(n + 1)
+        assert s.L.tns_adjoint_sensitivities(s.h, buf.ctypes.data, n + 1, 0) == _lib.TNS_ERR_ARG
+        s.adjoint_step(q.data_ptr(), lam.data_ptr(), True)
+        s.synchronize()
+        assert torch.isfinite(lam).all()
+        assert np.isfinite(s.adjoint_sensitivities()).all()
+    finally:
+        s.close()
