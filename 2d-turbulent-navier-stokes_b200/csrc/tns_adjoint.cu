@@ -1,16 +1,18 @@
 // tns_adjoint.cu -- the discrete adjoint of one FP64 RK4 iteration on the device.
 //
 // tns_adjoint_step(h, Q_n, lambda) recomputes the iteration from the checkpoint Q_n with
-// the solver's own FP64 kernels (dissipation + DT, viscous flux, stages 1-3, keeping every
-// stage input), then runs the hand-derived reverse of tns_adjoint.cuh: stages 4..1 (field
-// set, residual / update / source reverse, gather into the stage input), the viscous flux
-// reverse inside stage 1 (node averages, faces, nodes, slots), and the dissipation / time
-// step reverse.  The whole step -- recompute and reverse, 25 to 30 kernels -- is one CUDA
-// graph per handle (one with and one without the parameter sensitivities), replayed on
-// the handle's stream for every checkpoint.
+// the solver's own FP64 kernels (dissipation + DT, viscous flux, the port mass flux,
+// stages 1-3, keeping every stage input) and the state-only passes of the reverse (field
+// sets, node averages, dissipation pre-pass), then runs the hand-derived reverse of
+// tns_adjoint.cuh: stages 4..1 (residual / update / source reverse, gather into the
+// stage input, ghosts, port lines), the viscous flux reverse inside stage 1 (faces,
+// nodes, slots), and the dissipation / time-step reverse.  A step -- about 30 kernels,
+// with three short branches beside the main reverse -- is one CUDA graph per (forward
+// set, mode, sensitivity level), captured on first use and replayed on the handle's
+// stream for every checkpoint.  TNS_ADJ_FROZEN replays only the reverse (fixed-point
+// adjoint); tns_adjoint_step_next adds the next checkpoint's forward values on a branch.
 #include <cuda_runtime.h>
 
-#include <cstring>
 #include <vector>
 
 #include "tns_adjoint.cuh"
