@@ -98,9 +98,26 @@ void launch_points(K kernel, const AdjArgs& a, long long n, cudaStream_t s) {
 // stages' field sets, node averages and the dissipation pre-pass.  Two sets, so that
 // the next checkpoint's forward values are computed while this one's reverse runs.
 struct AdjForward {
-    DevBuf<double> q0, q1, q2, q3, d, vis, dt, dtmin, w, navg, dpre, gport;  // gport: [4][nghost]
+    DevBuf<double> q0, rec, w, navg, dpre;
     DevBuf<int> ninfo;
+    // one record (tns_adjoint_record): stage inputs 1-3, D, VIS, DT, DTMIN and the four
+    // stages' port mass flux, carved from `rec` in this order
+    double *q1 = nullptr, *q2 = nullptr, *q3 = nullptr, *d = nullptr, *vis = nullptr, *dt = nullptr,
+           *dtmin = nullptr, *gport = nullptr;
+    void carve(long long n) {
+        double* p = rec.p;
+        q1 = p; p += 5 * n;
+        q2 = p; p += 5 * n;
+        q3 = p; p += 5 * n;
+        d = p; p += 5 * n;
+        vis = p; p += 4 * n;
+        dt = p; p += n;
+        dtmin = p; p += 1;
+        gport = p;
+    }
 };
+
+long long record_size(long long n, long long ng) { return 25 * n + 1 + 4 * ng; }
 
 // Device buffers and graphs of the adjoint of one handle.
 struct tns_adjoint_state {
@@ -119,10 +136,10 @@ struct tns_adjoint_state {
     // the lowest priority, so that the reverse -- the critical path -- keeps its SMs
     cudaStream_t hp = nullptr;
     cudaEvent_t ev = nullptr;
-    // [set][mode: bit 0 forward first, bit 1 prefetch the other set][sensitivities: none,
-    // scalars, all]
-    cudaGraphExec_t graph[2][4][3] = {};
-    long long per_step[2][4][3] = {};
+    // [set][mode: bit 0 forward first, bit 1 prefetch the other set, bit 2 state-only
+    // passes first (recorded forward values)][sensitivities: none, scalars, all]
+    cudaGraphExec_t graph[2][8][3] = {};
+    long long per_step[2][8][3] = {};
     long long launches = 0;
 };
 
@@ -141,20 +158,20 @@ AdjArgs base_args(tns_handle* h, tns_adjoint_state* s, int set, int geo) {
     a.nif = (long long)(h->ni + 1) * h->nj;
     a.njf = (long long)h->ni * (h->nj + 1);
     a.qold = f.q0.p;
-    a.d = f.d.p;
-    a.vis = f.vis.p;
-    a.dt = f.dt.p;
-    a.dtmin = f.dtmin.p;
+    a.d = f.d;
+    a.vis = f.vis;
+    a.dt = f.dt;
+    a.dtmin = f.dtmin;
     a.w = f.w.p;
     a.w4 = f.w.p;
     a.navg = f.navg.p;
     a.ninfo = f.ninfo.p;
     a.dpre = f.dpre.p;
-    a.gport = f.gport.p;
+    a.gport = f.gport;
     a.qst[0] = f.q0.p;
-    a.qst[1] = f.q1.p;
-    a.qst[2] = f.q2.p;
-    a.qst[3] = f.q3.p;
+    a.qst[1] = f.q1;
+    a.qst[2] = f.q2;
+    a.qst[3] = f.q3;
     a.gportb = s->gportb.p;
     a.gportb4 = s->gportb.p;
     a.portacc = s->portacc.p;
@@ -205,49 +222,62 @@ const double kAlpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
 // Forward values of the state in set `set` (its q0), on stream st: the iteration with the
 // solver's kernels (stages 1-3 keep their outputs), then every pass of the reverse that
 // depends on the state alone.  Returns the number of kernels launched.
-long long enqueue_forward(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
+long long enqueue_forward_primal(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
     const Params& P = h->P;
     const Mesh& M = h->M;
     AdjForward& f = s->set[set];
     long long nl = 0;
     if (!P.local) {
-        tns::launch_dtmin(P, M, f.q0.p, h->partial.p, h->counter.p, f.dtmin.p, st);
+        tns::launch_dtmin(P, M, f.q0.p, h->partial.p, h->counter.p, f.dtmin, st);
         nl++;
     }
     // the type-6 ghosts read the port mass flux of each stage's input (one slice per stage)
     const int np = (int)h->port_ghosts.size();
     const size_t ng = (size_t)M.nghosts();
     Mesh Ms[4] = {M, M, M, M};
-    double* qs[4] = {f.q0.p, f.q1.p, f.q2.p, f.q3.p};
-    for (int k = 0; k < 4; k++) Ms[k].gport = f.gport.p + k * ng;
+    double* qs[4] = {f.q0.p, f.q1, f.q2, f.q3};
+    for (int k = 0; k < 4; k++) Ms[k].gport = f.gport + k * ng;
     auto gport = [&](int k) {
         if (np) {
-            tns::launch_gport(P, Ms[k], qs[k], h->ports.p, np, f.gport.p + k * ng, st);
+            tns::launch_gport(P, Ms[k], qs[k], h->ports.p, np, f.gport + k * ng, st);
             nl++;
         }
     };
-    tns::launch_dissipation(P, M, f.q0.p, f.d.p, f.dt.p, f.dtmin.p, st);
+    tns::launch_dissipation(P, M, f.q0.p, f.d, f.dt, f.dtmin, st);
     gport(0);
-    tns::launch_viscous(P, Ms[0], f.q0.p, f.vis.p, st);
+    tns::launch_viscous(P, Ms[0], f.q0.p, f.vis, st);
     for (int k = 0; k < 3; k++) {
         if (k) gport(k);
-        tns::launch_stage(P, Ms[k], qs[k], f.q0.p, qs[k + 1], f.d.p, f.vis.p, f.dt.p, f.dtmin.p, kAlpha[k], nullptr,
+        tns::launch_stage(P, Ms[k], qs[k], f.q0.p, qs[k + 1], f.d, f.vis, f.dt, f.dtmin, kAlpha[k], nullptr,
                           nullptr, st);
     }
     gport(3);
-    nl += 5;
+    return nl + 5;
+}
+
+// The passes of the reverse that depend on the state alone: the four stages' field sets,
+// the node averages and the dissipation pre-pass.
+long long enqueue_forward_state(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
+    AdjForward& f = s->set[set];
+    const size_t ng = (size_t)h->M.nghosts();
+    double* qs[4] = {f.q0.p, f.q1, f.q2, f.q3};
     AdjArgs a = base_args(h, s, set, 0);
     for (int k = 0; k < 4; k++) {
         a.qin = qs[k];
-        a.gport = f.gport.p + k * ng;
+        a.gport = f.gport + k * ng;
         a.w = f.w.p + (size_t)k * NWROW * a.npad;  // one field set per stage
         launch_points(k_adj_fields, a, a.npad, st);
     }
     a.w = f.w.p;
-    a.gport = f.gport.p;
+    a.gport = f.gport;
     launch_points(k_adj_nodes, a, a.nnode, st);
     launch_points(k_adj_diss_pre, a, a.ncell, st);
-    return nl + 6;
+    return 6;
+}
+
+long long enqueue_forward(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
+    const long long nl = enqueue_forward_primal(h, s, set, st);
+    return nl + enqueue_forward_state(h, s, set, st);
 }
 
 // The reverse of the iteration whose forward values are in set `set`: lambda (s->lam)
@@ -265,7 +295,7 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
         cudaEventRecord(s->ev, from);
         cudaStreamWaitEvent(st, s->ev, 0);
     };
-    double* qs[4] = {f.q0.p, f.q1.p, f.q2.p, f.q3.p};
+    double* qs[4] = {f.q0.p, f.q1, f.q2, f.q3};
     double* lam_stage[5] = {nullptr, s->lamA.p, s->lamB.p, s->lamA.p, s->lam.p};
     for (int k = 3; k >= 0; k--) {
         a.qin = qs[k];
@@ -276,7 +306,7 @@ long long enqueue_reverse(tns_handle* h, tns_adjoint_state* s, int set, int geo,
         a.lam_out = lam_stage[k];
         a.w = f.w.p + (size_t)k * NWROW * a.npad;     // this stage's field set
         a.gbar = s->gbar.p + (size_t)k * 5 * a.npad;  // one residual adjoint per stage
-        a.gport = f.gport.p + (size_t)k * a.M.nghosts();
+        a.gport = f.gport + (size_t)k * a.M.nghosts();
         a.gportb = s->gportb.p + (size_t)k * a.M.nghosts();
         launch_points(k_adj_stage, a, a.ncell, st);
         nl++;
@@ -334,6 +364,7 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int set, int mode, i
     cudaEventRecord(s->ev, user);
     cudaStreamWaitEvent(st, s->ev, 0);
     if (mode & 1) nl += enqueue_forward(h, s, set, st);
+    else if (mode & 4) nl += enqueue_forward_state(h, s, set, st);
     if (mode & 2) {
         cudaEventRecord(s->ev, st);
         cudaStreamWaitEvent(s->side[3], s->ev, 0);
@@ -379,7 +410,7 @@ void adjoint_release(tns_handle* h) {
     }
     if (s->ev) cudaEventDestroy(s->ev);
     for (auto& f : s->set) {
-        for (auto* b : {&f.q0, &f.q1, &f.q2, &f.q3, &f.d, &f.vis, &f.dt, &f.dtmin, &f.w, &f.navg, &f.dpre, &f.gport})
+        for (auto* b : {&f.q0, &f.rec, &f.w, &f.navg, &f.dpre})
             b->release();
         f.ninfo.release();
     }
@@ -417,10 +448,8 @@ int tns_adjoint_enable(tns_handle* h) {
                              {&s->xcs, npad}, {&s->ycs, npad}, {&s->gportb, 4 * (2 * (h->ni + h->nj))},
                              {&s->portacc, 3 * (2 * (h->ni + h->nj))}};
     for (auto& f : s->set)
-        for (Req r : std::vector<Req>{{&f.q0, 5 * n}, {&f.q1, 5 * n}, {&f.q2, 5 * n}, {&f.q3, 5 * n},
-                                      {&f.d, 5 * n}, {&f.vis, 4 * n}, {&f.dt, n}, {&f.dtmin, 1},
-                                      {&f.w, 4 * NWROW * npad}, {&f.navg, NNA * nnode}, {&f.dpre, NDPRE * n},
-                                      {&f.gport, 4 * (2 * (h->ni + h->nj))}})
+        for (Req r : std::vector<Req>{{&f.q0, 5 * n}, {&f.rec, record_size(n, 2 * (h->ni + h->nj))},
+                                      {&f.w, 4 * NWROW * npad}, {&f.navg, NNA * nnode}, {&f.dpre, NDPRE * n}})
             reqs.push_back(r);
     for (auto& r : reqs) {
         if ((rc = h->cuda(r.b->alloc((size_t)r.count), "cudaMalloc (adjoint)"))) {
@@ -452,13 +481,17 @@ int tns_adjoint_enable(tns_handle* h) {
     cudaMemsetAsync(s->sens.p, 0, sizeof(double) * s->nsens, h->stream);
     cudaMemsetAsync(s->portacc.p, 0, sizeof(double) * s->portacc.n, h->stream);
     cudaMemsetAsync(s->gportb.p, 0, sizeof(double) * s->gportb.n, h->stream);
-    for (auto& f : s->set) cudaMemsetAsync(f.gport.p, 0, sizeof(double) * f.gport.n, h->stream);
+    for (auto& f : s->set) {
+        f.carve(n);
+        cudaMemsetAsync(f.rec.p, 0, sizeof(double) * f.rec.n, h->stream);
+    }
     const AdjArgs a = base_args(h, s, 0, 0);
     launch_points(k_adj_centroids, a, npad, h->stream);
     return h->cuda(cudaStreamSynchronize(h->stream), "tns_adjoint_enable");
 }
 
-int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_next, double* d_lam, int flags) {
+static int adjoint_step_impl(tns_handle* h, const double* d_q, const double* d_q_next, const double* d_rec,
+                             double* d_lam, int flags) {
     if (!h || !d_lam || (!d_q && !(flags & TNS_ADJ_FROZEN))) return TNS_ERR_ARG;
     int rc;
     if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
@@ -472,7 +505,18 @@ int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_ne
     const size_t bytes = sizeof(double) * 5 * (size_t)h->ni * h->nj;
     cudaStream_t st = h->stream;
     int set = s->cur, mode = 0;
-    if (!frozen) {
+    if (d_rec && (frozen || d_q_next))
+        return h->fail(TNS_ERR_ARG, "tns_adjoint_step_recorded: no TNS_ADJ_FROZEN, no next state");
+    if (d_rec) {
+        // forward values from the record: only the state-only passes run
+        set = s->cur;
+        mode = 4;
+        AdjForward& f = s->set[set];
+        if ((rc = h->cuda(cudaMemcpyAsync(f.q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "adjoint: state in")) ||
+            (rc = h->cuda(cudaMemcpyAsync(f.rec.p, d_rec, sizeof(double) * f.rec.n, cudaMemcpyDeviceToDevice, st),
+                          "adjoint: record in")))
+            return rc;
+    } else if (!frozen) {
         if (s->pre_set >= 0 && s->pre_ptr == d_q) {
             set = s->pre_set;  // prefetched by the previous step
         } else {
@@ -518,8 +562,47 @@ int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_ne
     return h->cuda(cudaGetLastError(), "tns_adjoint_step");
 }
 
+int tns_adjoint_step_next(tns_handle* h, const double* d_q, const double* d_q_next, double* d_lam, int flags) {
+    return adjoint_step_impl(h, d_q, d_q_next, nullptr, d_lam, flags);
+}
+
 int tns_adjoint_step(tns_handle* h, const double* d_q, double* d_lam, int flags) {
-    return tns_adjoint_step_next(h, d_q, nullptr, d_lam, flags);
+    return adjoint_step_impl(h, d_q, nullptr, nullptr, d_lam, flags);
+}
+
+int tns_adjoint_step_recorded(tns_handle* h, const double* d_q, const double* d_rec, double* d_lam, int flags) {
+    if (!d_rec) return TNS_ERR_ARG;
+    return adjoint_step_impl(h, d_q, nullptr, d_rec, d_lam, flags);
+}
+
+long long tns_adjoint_record_size(tns_handle* h) {
+    if (!h) return -1;
+    return record_size((long long)h->ni * h->nj, 2LL * (h->ni + h->nj));
+}
+
+int tns_adjoint_record(tns_handle* h, const double* d_q, double* d_q_next, double* d_rec) {
+    if (!h || !d_q || !d_q_next || !d_rec) return TNS_ERR_ARG;
+    int rc;
+    if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
+    tns_adjoint_state* s = h->adj;
+    const int set = s->cur;
+    AdjForward& f = s->set[set];
+    const size_t bytes = sizeof(double) * 5 * (size_t)h->ni * h->nj;
+    cudaStream_t st = h->stream;
+    if ((rc = h->cuda(cudaMemcpyAsync(f.q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "record: state in")))
+        return rc;
+    // the iteration with the solver's kernels: stages 1-3 into the set, stage 4 to d_q_next
+    s->launches += enqueue_forward_primal(h, s, set, st);
+    Mesh M3 = h->M;
+    M3.gport = f.gport + 3 * (size_t)h->M.nghosts();
+    tns::launch_stage(h->P, M3, f.q3, f.q0.p, d_q_next, f.d, f.vis, f.dt, f.dtmin, kAlpha[3], nullptr, nullptr, st);
+    s->launches++;
+    s->have_forward = false;  // the set lacks the state-only passes
+    s->pre_set = -1;
+    if ((rc = h->cuda(cudaMemcpyAsync(d_rec, f.rec.p, sizeof(double) * f.rec.n, cudaMemcpyDeviceToDevice, st),
+                      "record: out")))
+        return rc;
+    return h->cuda(cudaGetLastError(), "tns_adjoint_record");
 }
 
 long long tns_adjoint_sensitivity_size(tns_handle* h) {

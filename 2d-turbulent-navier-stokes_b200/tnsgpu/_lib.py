@@ -41,9 +41,10 @@ EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run
            "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule",
            "tns_batch_launch_count", "tns_debug_math", "tns_batch_last_error", "tns_batch_destroy",
            "tns_adjoint_enable", "tns_adjoint_step", "tns_adjoint_step_next", "tns_adjoint_sensitivity_size",
+           "tns_adjoint_record_size", "tns_adjoint_record", "tns_adjoint_step_recorded",
            "tns_adjoint_sensitivities", "tns_adjoint_launch_count", "tns_copy_state_device")
 NOT_INT = ("tns_launch_count", "tns_last_error", "tns_destroy", "tns_batch_launch_count",
-           "tns_batch_last_error", "tns_batch_destroy", "tns_adjoint_sensitivity_size",
+           "tns_batch_last_error", "tns_batch_destroy", "tns_adjoint_sensitivity_size", "tns_adjoint_record_size",
            "tns_adjoint_launch_count")
 
 
@@ -117,6 +118,10 @@ def load(path: str = None):
     L.tns_adjoint_enable.argtypes = [vp]
     L.tns_adjoint_step.argtypes = [vp, vp, vp, ip]
     L.tns_adjoint_step_next.argtypes = [vp, vp, vp, vp, ip]
+    L.tns_adjoint_step_recorded.argtypes = [vp, vp, vp, vp, ip]
+    L.tns_adjoint_record.argtypes = [vp, vp, vp, vp]
+    L.tns_adjoint_record_size.argtypes = [vp]
+    L.tns_adjoint_record_size.restype = C.c_longlong
     L.tns_adjoint_sensitivity_size.argtypes = [vp]
     L.tns_adjoint_sensitivity_size.restype = C.c_longlong
     L.tns_adjoint_sensitivities.argtypes = [vp, vp, C.c_longlong, ip]

@@ -796,7 +796,7 @@ def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, am
                        dy: Optional[torch.Tensor] = None, space: Optional[DesignSpace] = None,
                        niter: int = 100, states: Optional[np.ndarray] = None, primal: str = "gpu",
                        lib=None, graph: Optional[bool] = None, engine: Optional[str] = None,
-                       max_states: Optional[int] = None) -> dict:
+                       max_states: Optional[int] = None, record: Optional[bool] = None) -> dict:
     """dJ/d(P0, T0, AMACHINIT, dy) of J = objective(scheme, Q_N, geo, prm), Q_0 the cold
     start, Q_N after ``niter`` RK4 iterations.
 
@@ -809,7 +809,10 @@ def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, am
     tensor of checkpoints.  ``max_states`` bounds the device states held at once: the
     sweep then keeps snapshots at recursive bisection points and recomputes each
     segment's states from its snapshot (O(N log2(N / max_states)) extra primal
-    iterations, the same gradient bit for bit; "states" is then None).
+    iterations, the same gradient bit for bit; "states" is then None).  ``record`` keeps
+    every iteration's forward values from the primal (tns_adjoint_record, about 25
+    doubles a cell an iteration) so that the reverse steps need not recompute them;
+    default: when they fit in half the free device memory.
 
     ``engine="torch"`` (the default on the CPU): the primal runs on the GPU FP64 path
     (``primal="gpu"``) or in the restatement (``"torch"``); ``states`` may pass
@@ -820,7 +823,7 @@ def transient_gradient(scheme: Scheme, objective: Callable, p0=None, t0=None, am
         engine = "cuda" if scheme.device.type == "cuda" else "torch"
     if engine == "cuda":
         return _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib,
-                                        max_states)
+                                        max_states, record)
     if engine != "torch":
         raise ValueError(f"engine {engine!r}: 'cuda' or 'torch'")
     dev = scheme.device
@@ -1059,18 +1062,34 @@ class DeviceAdjoint:
         self._leave()
         return states
 
+    def primal_recorded(self, c0: torch.Tensor, niter: int):
+        """Checkpoints [niter+1, 5, NI, NJ] and the iterations' forward values
+        [niter, record size] (tns_adjoint_record), from Q_0 = c0."""
+        states = torch.empty((niter + 1,) + tuple(c0.shape), dtype=torch.float64, device=self.scheme.device)
+        recs = torch.empty((niter, self.solver.adjoint_record_size()), dtype=torch.float64,
+                           device=self.scheme.device)
+        states[0].copy_(c0)
+        self._enter()
+        for n in range(niter):
+            self.solver.adjoint_record(states[n].data_ptr(), states[n + 1].data_ptr(), recs[n].data_ptr())
+        self.solver.synchronize()
+        self._leave()
+        return states, recs
+
     def step(self, q: torch.Tensor, lam: torch.Tensor, sensitivities, frozen: bool = False,
-             q_next: Optional[torch.Tensor] = None):
+             q_next: Optional[torch.Tensor] = None, rec: Optional[torch.Tensor] = None):
         """``sensitivities``: True (all), "scalars" (RTOLERANCE, T0, S0) or False.
         ``frozen``: q is the previous step's state (its forward values are reused).
         ``q_next``: the state of the next step, whose forward values are computed beside
-        this reverse (it must stay unchanged until that step)."""
-        for t in (q, lam) + ((q_next,) if q_next is not None else ()):
+        this reverse (it must stay unchanged until that step).  ``rec``: the iteration's
+        recorded forward values (``primal_recorded``), used instead of recomputing."""
+        for t in (q, lam) + tuple(x for x in (q_next, rec) if x is not None):
             if not (t.is_contiguous() and t.dtype == torch.float64):
-                raise ValueError("q, q_next and lambda must be contiguous float64 device tensors")
+                raise ValueError("q, q_next, rec and lambda must be contiguous float64 device tensors")
         self._enter()
         self.solver.adjoint_step(q.data_ptr(), lam.data_ptr(), sensitivities, frozen,
-                                 q_next.data_ptr() if q_next is not None else None)
+                                 q_next.data_ptr() if q_next is not None else None,
+                                 rec.data_ptr() if rec is not None else None)
         self._leave()
 
     def sensitivities(self) -> Dict[str, torch.Tensor]:
@@ -1187,7 +1206,7 @@ class _Checkpoints:
 
 
 def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, niter, states, lib,
-                             max_states=None) -> dict:
+                             max_states=None, record=None) -> dict:
     if scheme.device.type != "cuda":
         raise ValueError("engine='cuda' needs a Scheme on a CUDA device")
     params, dy = _leaves(scheme, p0, t0, amachinit, dy)
@@ -1224,8 +1243,15 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
         if dy is not None:
             out["dJ_ddy"] = grads[3].detach().cpu().numpy()
         return out
+    recs = None
     try:
-        if states is None:
+        if states is None and record is not False:
+            need = niter * dev_adj.solver.adjoint_record_size() * 8
+            if record or need < 0.5 * torch.cuda.mem_get_info(scheme.device)[0]:
+                st, recs = dev_adj.primal_recorded(c0, niter)
+        if recs is not None:
+            pass
+        elif states is None:
             st = dev_adj.primal(c0, niter)
         elif isinstance(states, torch.Tensor):
             st = states.to(scheme.device, torch.float64).reshape(niter + 1, 5, ni, nj).contiguous()
@@ -1241,7 +1267,7 @@ def _transient_gradient_cuda(scheme, objective, p0, t0, amachinit, dy, space, ni
         # without node displacements only the scalar sensitivities are needed
         mode = True if dy is not None else "scalars"
         for n in range(niter - 1, -1, -1):
-            dev_adj.step(st[n], lam, mode)
+            dev_adj.step(st[n], lam, mode, rec=recs[n] if recs is not None else None)
         sens = dev_adj.sensitivities()
     finally:
         dev_adj.close()

@@ -143,8 +143,17 @@ class Solver:
         """Loads the state from device memory at ``ptr`` ([5][NELES] doubles), async."""
         self._check(self.L.tns_copy_state_device(self.h, C.c_void_p(int(ptr)), 1))
 
+    def adjoint_record_size(self) -> int:
+        return int(self.L.tns_adjoint_record_size(self.h))
+
+    def adjoint_record(self, q_ptr: int, q_next_ptr: int, rec_ptr: int):
+        """One iteration from Q_n (device) to Q_{n+1}, keeping its forward values in the
+        record at rec_ptr (tns_adjoint_record)."""
+        self._check(self.L.tns_adjoint_record(self.h, C.c_void_p(int(q_ptr)), C.c_void_p(int(q_next_ptr)),
+                                              C.c_void_p(int(rec_ptr))))
+
     def adjoint_step(self, q_ptr: int, lam_ptr: int, sensitivities=False, frozen: bool = False,
-                     q_next_ptr: Optional[int] = None):
+                     q_next_ptr: Optional[int] = None, rec_ptr: Optional[int] = None):
         """lambda <- lambda dG/dQ_n for the iteration from Q_n (both device pointers);
         with ``sensitivities`` also accumulates lambda dG/dp (True: all of them;
         "scalars": RTOLERANCE, T0 and S0 only); with ``frozen`` Q_n is the previous
@@ -152,6 +161,10 @@ class Solver:
         Q_n) has its forward values computed beside this reverse (tns_adjoint_step_next)."""
         sens = 4 if sensitivities == "scalars" else (1 if sensitivities else 0)
         flags = sens | (2 if frozen else 0)
+        if rec_ptr:
+            self._check(self.L.tns_adjoint_step_recorded(self.h, C.c_void_p(int(q_ptr)), C.c_void_p(int(rec_ptr)),
+                                                         C.c_void_p(int(lam_ptr)), flags))
+            return
         nxt = C.c_void_p(int(q_next_ptr)) if q_next_ptr else None
         self._check(self.L.tns_adjoint_step_next(self.h, C.c_void_p(int(q_ptr)) if q_ptr else None, nxt,
                                                  C.c_void_p(int(lam_ptr)), flags))

@@ -301,8 +301,10 @@ def run_ours(args, rank, world, dev):
 def adjoint_timing(torch, dev, K=50, W=5):
     """adjoint/primal time on the discrete-adjoint workload (compression ramp 512 x 192,
     IAXIS=0, LOCAL=1, cold start): one primal RK4 iteration (captured graph) against one
-    reverse step of the CUDA adjoint (tns_adjoint_step) -- with recomputation and the
-    parameter sensitivities, as a transient gradient takes it, and frozen at a fixed
+    reverse step of the CUDA adjoint -- with the parameter sensitivities and the
+    iteration's forward values recorded by the primal (tns_adjoint_record /
+    tns_adjoint_step_recorded), as a transient gradient takes it, or recomputed
+    (tns_adjoint_step), and frozen at a fixed
     state, as the fixed-point adjoint takes it.  CUDA events on the adjoint's stream,
     K steps each after W warm-up steps; L2 not flushed on either side (the 512 x 192
     working set is L2-resident for both)."""
@@ -334,13 +336,26 @@ def adjoint_timing(torch, dev, K=50, W=5):
         lam = torch.randn_like(st[0])
         for n in range(W):
             s.adjoint_step(st[n].data_ptr(), lam.data_ptr(), True)
+        recompute_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), True))
+        # the sweep as transient_gradient runs it: a primal that records each iteration's
+        # forward values (tns_adjoint_record), then reverse steps that read them
+        rs = s.adjoint_record_size()
+        recs = torch.empty((K, rs), dtype=torch.float64, device=st.device)
+        st2 = torch.empty_like(st[:K + 1])
+        st2[0].copy_(st[0])
+        s.adjoint_record(st2[0].data_ptr(), st2[1].data_ptr(), recs[0].data_ptr())
+        record_us = timed(lambda n: s.adjoint_record(st2[n].data_ptr(), st2[n + 1].data_ptr(), recs[n].data_ptr()))
+        for n in range(min(W, K)):
+            s.adjoint_step(st2[n].data_ptr(), lam.data_ptr(), True, rec_ptr=recs[n].data_ptr())
         launches0 = s.adjoint_launch_count()
-        step_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), True))
+        step_us = timed(lambda n: s.adjoint_step(st2[K - 1 - n].data_ptr(), lam.data_ptr(), True,
+                                                 rec_ptr=recs[K - 1 - n].data_ptr()))
         per_step = (s.adjoint_launch_count() - launches0) // K
         # the same sweep for flow-parameter gradients only (no geometric sensitivities)
-        for n in range(W):
-            s.adjoint_step(st[n].data_ptr(), lam.data_ptr(), "scalars")
-        scalars_us = timed(lambda n: s.adjoint_step(st[K - 1 - n].data_ptr(), lam.data_ptr(), "scalars"))
+        for n in range(min(W, K)):
+            s.adjoint_step(st2[n].data_ptr(), lam.data_ptr(), "scalars", rec_ptr=recs[n].data_ptr())
+        scalars_us = timed(lambda n: s.adjoint_step(st2[K - 1 - n].data_ptr(), lam.data_ptr(), "scalars",
+                                                    rec_ptr=recs[K - 1 - n].data_ptr()))
         q = st[K].contiguous()
         s.adjoint_step(q.data_ptr(), lam.data_ptr(), False)
         for _ in range(W):
@@ -351,12 +366,14 @@ def adjoint_timing(torch, dev, K=50, W=5):
         da.close()
     return {"workload": "ramp_512x192 (IAXIS=0, LOCAL=1, cold start)", "steps": K,
             "primal_iteration_us": round(primal_us, 2),
+            "primal_record_iteration_us": round(record_us, 2),
             "transient_step_us": round(step_us, 2),
+            "transient_step_recompute_us": round(recompute_us, 2),
             "fixed_point_step_us": round(frozen_us, 2),
             "transient_step_over_primal": round(step_us / primal_us, 3),
             "transient_step_flow_parameters_us": round(scalars_us, 2),
             "fixed_point_step_over_primal": round(frozen_us / primal_us, 3),
-            "transient_gradient_over_primal": round((primal_us + step_us) / primal_us, 3),
+            "transient_gradient_over_primal": round((record_us + step_us) / primal_us, 3),
             "kernels_per_transient_step": int(per_step)}
 
 

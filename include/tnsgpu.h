@@ -203,6 +203,15 @@ int tns_adjoint_step(tns_handle *h, const double *d_q, double *d_lam, int flags)
  * NULL.  Results are bitwise those of tns_adjoint_step; on a B200 at 98k cells the
  * overlapped step measured slower (439 us) than recomputing in sequence (410 us). */
 int tns_adjoint_step_next(tns_handle *h, const double *d_q, const double *d_q_next, double *d_lam, int flags);
+/* Recorded forward values, for transient sweeps with memory to spare: tns_adjoint_record
+ * runs one iteration from d_q (the solver's kernels, the same result as tns_enqueue),
+ * writes Q_{n+1} to d_q_next and the iteration's forward values -- stage inputs 1-3, D,
+ * VIS, DT, DTMIN, the port mass flux of each stage -- to d_rec
+ * (tns_adjoint_record_size doubles).  tns_adjoint_step_recorded(h, Q_n, rec_n, ...)
+ * then skips the recomputation (same results as tns_adjoint_step). */
+long long tns_adjoint_record_size(tns_handle *h);
+int tns_adjoint_record(tns_handle *h, const double *d_q, double *d_q_next, double *d_rec);
+int tns_adjoint_step_recorded(tns_handle *h, const double *d_q, const double *d_rec, double *d_lam, int flags);
 long long tns_adjoint_sensitivity_size(tns_handle *h);
 /* Copies the accumulated sensitivities to host memory `out` (count values, which must
  * equal tns_adjoint_sensitivity_size) and, with reset != 0, zeroes them. */

@@ -303,3 +303,18 @@ def test_adjoint_abi_errors_leave_the_handle_usable():
         assert np.isfinite(s.adjoint_sensitivities()).all()
     finally:
         s.close()
+
+
+def test_recorded_forward_values_equal_recomputed():
+    """tns_adjoint_record's primal equals tns_enqueue's bit for bit, and reverse steps
+    reading the records equal recomputing ones."""
+    mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
+    dy = torch.tensor([1e-5], dtype=torch.float64)
+    N = 25
+    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, record=True)
+    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, record=False)
+    assert torch.equal(a["states"], b["states"])
+    for k in ("J", "dJ_dp0", "dJ_dt0", "dJ_damachinit"):
+        assert a[k] == b[k], (k, a[k], b[k])
+    assert np.array_equal(a["dJ_ddy"], b["dJ_ddy"])
+    assert torch.equal(a["lambda0"], b["lambda0"])
