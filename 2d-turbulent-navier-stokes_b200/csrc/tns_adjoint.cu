@@ -222,10 +222,11 @@ const double kAlpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
 // Forward values of the state in set `set` (its q0), on stream st: the iteration with the
 // solver's kernels (stages 1-3 keep their outputs), then every pass of the reverse that
 // depends on the state alone.  Returns the number of kernels launched.
-long long enqueue_forward_primal(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st) {
+long long enqueue_forward_primal(tns_handle* h, tns_adjoint_state* s, int set, cudaStream_t st,
+                                 const AdjForward* into = nullptr) {
     const Params& P = h->P;
     const Mesh& M = h->M;
-    AdjForward& f = s->set[set];
+    const AdjForward& f = into ? *into : s->set[set];
     long long nl = 0;
     if (!P.local) {
         tns::launch_dtmin(P, M, f.q0.p, h->partial.p, h->counter.p, f.dtmin, st);
@@ -586,22 +587,21 @@ int tns_adjoint_record(tns_handle* h, const double* d_q, double* d_q_next, doubl
     if (!h->adj && (rc = tns_adjoint_enable(h))) return rc;
     tns_adjoint_state* s = h->adj;
     const int set = s->cur;
-    AdjForward& f = s->set[set];
-    const size_t bytes = sizeof(double) * 5 * (size_t)h->ni * h->nj;
     cudaStream_t st = h->stream;
-    if ((rc = h->cuda(cudaMemcpyAsync(f.q0.p, d_q, bytes, cudaMemcpyDeviceToDevice, st), "record: state in")))
-        return rc;
-    // the iteration with the solver's kernels: stages 1-3 into the set, stage 4 to d_q_next
-    s->launches += enqueue_forward_primal(h, s, set, st);
+    // the iteration with the solver's kernels, reading d_q and writing its forward values
+    // straight into the record (stages 1-3, D, VIS, DT, DTMIN, port flux) and Q_{n+1}
+    // into d_q_next
+    AdjForward r;
+    r.q0.p = const_cast<double*>(d_q);
+    r.rec.p = d_rec;
+    r.carve((long long)h->ni * h->nj);
+    s->launches += enqueue_forward_primal(h, s, set, st, &r);
     Mesh M3 = h->M;
-    M3.gport = f.gport + 3 * (size_t)h->M.nghosts();
-    tns::launch_stage(h->P, M3, f.q3, f.q0.p, d_q_next, f.d, f.vis, f.dt, f.dtmin, kAlpha[3], nullptr, nullptr, st);
+    M3.gport = r.gport + 3 * (size_t)h->M.nghosts();
+    tns::launch_stage(h->P, M3, r.q3, r.q0.p, d_q_next, r.d, r.vis, r.dt, r.dtmin, kAlpha[3], nullptr, nullptr, st);
     s->launches++;
-    s->have_forward = false;  // the set lacks the state-only passes
-    s->pre_set = -1;
-    if ((rc = h->cuda(cudaMemcpyAsync(d_rec, f.rec.p, sizeof(double) * f.rec.n, cudaMemcpyDeviceToDevice, st),
-                      "record: out")))
-        return rc;
+    r.q0.p = nullptr;  // borrowed: not released by the DevBuf
+    r.rec.p = nullptr;
     return h->cuda(cudaGetLastError(), "tns_adjoint_record");
 }
 
