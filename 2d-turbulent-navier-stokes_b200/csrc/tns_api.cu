@@ -604,10 +604,25 @@ int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double
     if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
     if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_download_state: no state");
     const size_t nc = h->ncell();
-    int rc = h->cuda(cudaMemcpyAsync(h->pinned, h->state(), 5 * nc * 8, cudaMemcpyDeviceToHost, h->stream),
-                     "cudaMemcpyAsync");
-    if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     double* dst[5] = {c1, c2, c3, c4, c5};
+    bool direct = h->identity;
+    for (int m = 0; m < 5 && direct; m++) {
+        cudaPointerAttributes at;
+        direct = cudaPointerGetAttributes(&at, dst[m]) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    }
+    cudaGetLastError();
+    int rc;
+    if (direct) {
+        // page-locked caller arrays: one DMA per component, no staging copy
+        for (int m = 0; m < 5; m++)
+            if ((rc = h->cuda(cudaMemcpyAsync(dst[m], h->state() + m * nc, nc * 8, cudaMemcpyDeviceToHost,
+                                              h->stream), "cudaMemcpyAsync")))
+                return rc;
+        return h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    }
+    rc = h->cuda(cudaMemcpyAsync(h->pinned, h->state(), 5 * nc * 8, cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    if (rc || (rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     for (int m = 0; m < 5; m++) {
         const double* src = h->pinned + m * nc;
         if (h->identity) std::memcpy(dst[m], src, nc * 8);

@@ -105,6 +105,10 @@ class Solver:
         """Upload from five host addresses (e.g. page-locked buffers) of NELES doubles."""
         self._check(self.L.tns_upload_state(self.h, *[int(p) for p in ptrs]))
 
+    def download_ptrs(self, ptrs):
+        """Download into five host addresses (e.g. page-locked buffers) of NELES doubles."""
+        self._check(self.L.tns_download_state(self.h, *[int(p) for p in ptrs]))
+
     def download(self) -> np.ndarray:
         c = np.zeros((5, self.mesh.neles))
         self._check(self.L.tns_download_state(self.h, *(c[k].ctypes.data for k in range(5))))

@@ -67,6 +67,14 @@ def _case(name):
     raise SystemExit(f"unknown case {name}")
 
 
+def workload_config(wname, cells, precision, world):
+    """The config object both arms print for the same workload."""
+    return {"workload": wname, "cells": cells, "precision": precision,
+            "step": "one RK4 iteration (dissipation pre-pass + 4 stages)",
+            "l2": "flushed between steps (256 MiB write outside the timed events)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -230,14 +238,17 @@ def run_ours(args, rank, world, dev):
     kernel_split = {k: round(kt[k][0] / P * 1e3, 2) for k in kt if kt[k][1]}
 
     # end to end through the C ABI: pinned host state -> device, one monitored
-    # iteration, residual (CDIFF) back to the host
+    # iteration, the new state and the residual (CDIFF) back to the host
     host = torch.empty((5, mesh.neles), dtype=torch.float64, pin_memory=True)
     host.copy_(torch.from_numpy(np.ascontiguousarray(c0)))
+    back = torch.empty((5, mesh.neles), dtype=torch.float64, pin_memory=True)
     ptrs = [host[k].data_ptr() for k in range(5)]
+    bptrs = [back[k].data_ptr() for k in range(5)]
     E = max(3, min(K, 200))
     for _ in range(2):
         s.upload_ptrs(ptrs)
         s.run(1, 1)
+        s.download_ptrs(bptrs)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -245,10 +256,14 @@ def run_ours(args, rank, world, dev):
     for _ in range(E):
         s.upload_ptrs(ptrs)
         s.run(1, 1)
+        s.download_ptrs(bptrs)
     e2e_s = max_over_ranks((time.perf_counter() - t0) / E, world, torch, dev)
     e2e = {"value": replica_rate(mesh.neles, e2e_s, world), "unit": UNIT,
-           "h2d_bytes_per_step": 5 * mesh.neles * 8, "d2h_bytes_per_step": 5 * 8 + 4,
+           "h2d_bytes_per_step": 5 * mesh.neles * 8,
+           "d2h_bytes_per_step": 5 * mesh.neles * 8 + 5 * 8 + 4,
            "ms_per_step": round(e2e_s * 1e3, 4),
+           "step": "upload Q from pinned host, one monitored RK4 iteration, download Q, "
+                   "CDIFF record and status word",
            "host_cpus": f"{len(numa_cpus)} GPU-local" if numa_cpus else "unpinned"}
     s.close()
 
@@ -276,10 +291,7 @@ def run_ours(args, rank, world, dev):
         "warmup": W, "ms_per_step": round(ms, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if prec else "f64",
         "data": "synthetic",
-        "config": {"workload": wname, "cells": mesh.neles, "precision": args.precision,
-                   "step": "one RK4 iteration (dissipation pre-pass + 4 stages)",
-                   "l2": "flushed between steps (256 MiB write outside the timed events)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": workload_config(wname, mesh.neles, args.precision, world),
         "roofline": {"bound": "hbm", "kernel": knames[dom], "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
@@ -380,7 +392,7 @@ def adjoint_timing(torch, dev, K=50, W=5):
 def cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0):
     """The oracle (FP64 C restatement of the reference, single thread) on this host."""
     from oracle.pyoracle import Oracle
-    o = Oracle(mesh, flow, rinit)
+    o = Oracle(mesh, flow, rinit, native=True)
     o.set_state(c0)
     t0 = time.perf_counter()
     o.iterate(1, 0)
@@ -391,13 +403,14 @@ def cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0):
     dt = time.perf_counter() - t0
     return {"value": mesh.neles * n / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{n} RK4 iterations of the same {mesh.neles}-cell mesh and start "
-                      f"state, single thread ({dt:.1f} s)"}
+                      f"state, single thread ({dt:.1f} s), gcc -O3 -march=native "
+                      f"-ffp-contract=off built on this host"}
 
 
 def run_reference(args):
     mesh, flow, c0, rinit, wname = _case(args.case)
     from oracle.pyoracle import Oracle
-    o = Oracle(mesh, flow, rinit)
+    o = Oracle(mesh, flow, rinit, native=True)
     o.set_state(c0)
     t0 = time.perf_counter()
     for _ in range(max(1, min(args.warmup, 3))):
@@ -412,14 +425,14 @@ def run_reference(args):
     ms = 1e3 * sum(times) / n
     value = mesh.neles / (ms * 1e-3)
     sample = (f"{n} of {args.steps} requested steps, each one full RK4 iteration of the "
-              f"{mesh.neles}-cell mesh, single thread (the reference is serial)")
+              f"{mesh.neles}-cell mesh, single thread (the reference is serial), gcc -O3 "
+              f"-march=native -ffp-contract=off built on this host")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": wname, "cells": mesh.neles, "precision": "fp64",
-                   "step": "one RK4 iteration (dissipation pre-pass + 4 stages)"},
+        "config": workload_config(wname, mesh.neles, args.precision, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,

@@ -137,11 +137,12 @@ long long tns_launch_count(tns_handle *h);
 const char *tns_last_error(tns_handle *h);
 
 /* Allocation-free time step.  No counterpart in the reference: it serves callers that
- * cannot allocate device memory while they run the solver -- code inside a CUDA stream
- * capture (cudaMalloc would break the capture), hosts whose device memory all comes
- * from one preallocated pool or arena, and plugin hosts that forbid allocation on
- * their time loop.  It computes, for a state already in device memory, the per-cell
- * time step DT = CFL*DL/(|V| + sqrt(GAMA*RR*T)) and DTMIN = min(1e5, min DT) of
+ * cannot allocate device memory while they run the solver -- hosts whose device memory
+ * all comes from one preallocated pool or arena (an allocation outside it fails or
+ * breaks their accounting), and plugin hosts that forbid allocation on their time loop
+ * (cudaMalloc synchronises the device and may stall other work).  It computes, for a
+ * state already in device memory, the per-cell time step
+ * DT = CFL*DL/(|V| + sqrt(GAMA*RR*T)) and DTMIN = min(1e5, min DT) of
  * turbnstwod.f90:97-108, exactly as the handle-based path does, without a handle.
  *
  *   d_q      device, [5][ncell] conservative state, component-major (C1 block, C2, ...)
@@ -155,10 +156,12 @@ const char *tns_last_error(tns_handle *h);
  * block of TNS_NOALLOC_CELLS_PER_THREAD*256 cells, at most TNS_NOALLOC_MAX_BLOCKS
  * blocks: 64 KiB), so ncell is limited to TNS_NOALLOC_MAX_CELLS; larger problems get
  * TNS_ERR_TOO_LARGE.  It calls no cudaMalloc / cudaFree.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress) and must therefore be made
- * before any stream capture starts.  All calls share the one array, so calls that may
- * overlap on the GPU (different streams without ordering) race; serialise them.  The
- * call is asynchronous on `stream`. */
+ * looks up the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture starts.  The address is kept until the process exits; after
+ * cudaDeviceReset on that device it no longer names the array, so do not call this entry
+ * point on a device that has been reset.  All calls share the one array, so calls that
+ * may overlap on the GPU (different streams without ordering) race; serialise them.
+ * The call is asynchronous on `stream`. */
 #define TNS_NOALLOC_MAX_BLOCKS 8192
 #define TNS_NOALLOC_CELLS_PER_THREAD 4
 #define TNS_NOALLOC_MAX_CELLS (256LL * TNS_NOALLOC_CELLS_PER_THREAD * TNS_NOALLOC_MAX_BLOCKS)

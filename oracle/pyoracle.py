@@ -11,7 +11,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libtnsoracle.so")
-_lib = None
+_NATIVE_PATH = os.path.join(_HERE, "_build", "libtnsoracle_native.so")
+_libs = {}
 
 
 class OraParams(C.Structure):
@@ -26,12 +27,21 @@ def build() -> str:
     return _LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+def build_native() -> str:
+    """The -march=native copy, compiled on this machine (for the CPU timings only)."""
+    subprocess.run(["make", "-s", "-B", "-C", _HERE, "native"], check=True)
+    return _NATIVE_PATH
+
+
+def lib(native: bool = False):
+    """The oracle library: the portable build, or with ``native`` the -march=native
+    copy, rebuilt on first use in this process so it targets the CPU it runs on."""
+    if native not in _libs:
+        if native:
+            build_native()
+        elif not os.path.exists(_LIB_PATH):
             build()
-        L = C.CDLL(_LIB_PATH)
+        L = C.CDLL(_NATIVE_PATH if native else _LIB_PATH)
         dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
         L.ora_create.restype = C.c_void_p
@@ -52,8 +62,8 @@ def lib():
             getattr(L, n).argtypes = [C.c_void_p]
         L.ora_update.argtypes = [C.c_void_p, C.c_double]
         L.ora_postprocess.argtypes = [C.c_void_p, dp, dp, dp, dp]
-        _lib = L
-    return _lib
+        _libs[native] = L
+    return _libs[native]
 
 
 def params_from_flow(f, rinit: float) -> OraParams:
@@ -69,8 +79,9 @@ def params_from_flow(f, rinit: float) -> OraParams:
 class Oracle:
     """One oracle solver instance over a Mesh (formats.Mesh) and Flow."""
 
-    def __init__(self, mesh, flow, rinit: float):
-        L = lib()
+    def __init__(self, mesh, flow, rinit: float, native: bool = False):
+        self._native = native
+        L = lib(native)
         self.mesh, self.flow = mesh, flow
         self._p = params_from_flow(flow, rinit)
         self._inj = None
@@ -89,38 +100,38 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().ora_destroy(self.h)
+            lib(self._native).ora_destroy(self.h)
             self.h = None
 
     def set_state(self, c: np.ndarray):
-        lib().ora_set_state(self.h, np.ascontiguousarray(c, np.float64).reshape(-1))
+        lib(self._native).ora_set_state(self.h, np.ascontiguousarray(c, np.float64).reshape(-1))
 
     def cold_start(self):
-        lib().ora_cold_start(self.h, float(self.flow.amachinit))
+        lib(self._native).ora_cold_start(self.h, float(self.flow.amachinit))
 
     def state(self) -> np.ndarray:
         out = np.zeros(5 * self.mesh.neles)
-        lib().ora_get_state(self.h, out)
+        lib(self._native).ora_get_state(self.h, out)
         return out.reshape(5, self.mesh.neles)
 
     def iterate(self, niter: int, monitor_every: int = 1000):
         maxrec = max(1, niter // max(monitor_every, 1) + 1)
         buf = np.zeros(5 * maxrec)
-        n = lib().ora_iterate(self.h, int(niter), int(monitor_every), buf.ctypes.data, maxrec)
+        n = lib(self._native).ora_iterate(self.h, int(niter), int(monitor_every), buf.ctypes.data, maxrec)
         return buf[: 5 * min(n, maxrec)].reshape(-1, 5)
 
     def fetch(self, name: str) -> np.ndarray:
         out = np.zeros(max(self.nn, self.mesh.nods) + 1)
-        n = lib().ora_fetch(self.h, name.encode(), out, out.shape[0])
+        n = lib(self._native).ora_fetch(self.h, name.encode(), out, out.shape[0])
         if n < 0:
             raise KeyError(name)
         return out[:n].copy()
 
     def call(self, routine: str, *args):
-        getattr(lib(), "ora_" + routine)(self.h, *args)
+        getattr(lib(self._native), "ora_" + routine)(self.h, *args)
 
     def postprocess(self):
         n = self.mesh.nods
         pn, un, vn, tn = (np.zeros(n) for _ in range(4))
-        lib().ora_postprocess(self.h, pn, un, vn, tn)
+        lib(self._native).ora_postprocess(self.h, pn, un, vn, tn)
         return pn, un, vn, tn

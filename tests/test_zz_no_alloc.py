@@ -1,11 +1,14 @@
 """The allocation-free time step (tns_time_step_noalloc) against the handle-based path.
 
-Callers that cannot allocate device memory while they run -- inside a CUDA stream
-capture, or with all device memory taken from a preallocated pool -- get the time
-step of turbnstwod.f90:97-108 from tns_time_step_noalloc, whose reduction scratch is a
-fixed array inside the library.  This test drives it through the C ABI with device
-buffers it allocates itself (it is only the checker), twice in a row, and compares
-DT and DTMIN with what tns_run computed for the same state (tns_debug_fetch).
+Callers that cannot allocate device memory while they run -- hosts whose device memory
+all comes from one preallocated pool, or plugin hosts that forbid allocation on their
+time loop -- get the time step of turbnstwod.f90:97-108 from tns_time_step_noalloc,
+whose reduction scratch is a fixed array inside the library.  This test drives it
+through the C ABI with device buffers it allocates itself (it is only the checker),
+twice in a row, and compares DT and DTMIN with what tns_run computed for the same
+state (tns_debug_fetch).  The meshes span one reduction block (960 cells), several
+(16 384 cells: 16 partial minima, the last block's reduction through the shared array,
+the completion counter left at zero for the next call) and many (393 216 cells).
 
 This file is collected last so a run that stops at the first failure has run every
 other test before it.
@@ -49,10 +52,11 @@ def _noalloc(torch, q_host, cfldl_dev, params, stream):
     return dt.cpu().numpy(), float(dtmin.cpu().numpy()[0])
 
 
+@pytest.mark.parametrize("shape", [(48, 20), (256, 64), (1024, 384)])
 @pytest.mark.parametrize("local", [1, 0])
-def test_noalloc_time_step_matches_handle_path_on_two_calls(local):
+def test_noalloc_time_step_matches_handle_path_on_two_calls(local, shape):
     import torch
-    mesh = cases.ramp_mesh(48, 20)
+    mesh = cases.ramp_mesh(*shape)
     flow = cases.ramp_flow()
     flow.local = local
     c0, rinit = cases.noisy_restart_state(flow, mesh.neles)
