@@ -250,7 +250,7 @@ long long enqueue_forward_primal(tns_handle* h, tns_adjoint_state* s, int set, c
     for (int k = 0; k < 3; k++) {
         if (k) gport(k);
         tns::launch_stage(P, Ms[k], qs[k], f.q0.p, qs[k + 1], f.d, f.vis, f.dt, f.dtmin, kAlpha[k], nullptr,
-                          nullptr, st);
+                          nullptr, h->status.p, st);
     }
     gport(3);
     return nl + 5;
@@ -598,7 +598,8 @@ int tns_adjoint_record(tns_handle* h, const double* d_q, double* d_q_next, doubl
     s->launches += enqueue_forward_primal(h, s, set, st, &r);
     Mesh M3 = h->M;
     M3.gport = r.gport + 3 * (size_t)h->M.nghosts();
-    tns::launch_stage(h->P, M3, r.q3, r.q0.p, d_q_next, r.d, r.vis, r.dt, r.dtmin, kAlpha[3], nullptr, nullptr, st);
+    tns::launch_stage(h->P, M3, r.q3, r.q0.p, d_q_next, r.d, r.vis, r.dt, r.dtmin, kAlpha[3], nullptr, nullptr,
+                      h->status.p, st);
     s->launches++;
     r.q0.p = nullptr;  // borrowed: not released by the DevBuf
     r.rec.p = nullptr;

@@ -18,6 +18,7 @@
 
 #include "tns_handle.h"
 #include "tns_params.h"
+#include "tns_tile.cuh"
 
 using tns::make_params;
 
@@ -200,6 +201,115 @@ int build_mesh(tns_handle* h, const tns_mesh* m) {
     return TNS_OK;
 }
 
+// Static geometry of the tile kernels, from the device-order node and ghost-centroid
+// arrays with the reference's formulas (geometry.f90:55-149; the gradients of
+// source_terms.f90:24-60 and viscous.f90:130-180): VOL per cell, the stage tiles' static
+// blocks (tns_tile.cuh) and the viscous face rows (tns_device.cuh FaceGeo).
+void build_geometry(tns_handle* h) {
+    using namespace tns;
+    const int ni = h->ni, nj = h->nj, iaxis = h->P.iaxis;
+    const std::vector<double>&X = h->hX, &Y = h->hY;
+    auto node = [&](int a, int b, double& x, double& y) {
+        const size_t n = (size_t)a * (nj + 1) + b;
+        x = X[n];
+        y = Y[n];
+    };
+    // centroid of halo position (i, j): a cell from its corners, a ghost mirrored
+    auto centroid = [&](int i, int j, double& x, double& y) {
+        if (i >= 0 && i < ni && j >= 0 && j < nj) {
+            const size_t n1 = (size_t)i * (nj + 1) + j;
+            x = (X[n1] + X[n1 + nj + 1] + X[n1 + nj + 2] + X[n1 + 1]) * 0.25;
+            y = (Y[n1] + Y[n1 + nj + 1] + Y[n1 + nj + 2] + Y[n1 + 1]) * 0.25;
+            return;
+        }
+        const int g = j == -1 ? h->M.ghost_index(1, i) : i == ni ? h->M.ghost_index(2, j)
+                    : j == nj ? h->M.ghost_index(3, i) : h->M.ghost_index(4, j);
+        x = h->hgxc[g];
+        y = h->hgyc[g];
+    };
+    // coefficients of the difference gradient over points a, b, c, d
+    auto grad = [](double xa, double ya, double xb, double yb, double xc, double yc, double xd,
+                   double yd, double* out, size_t stride) {
+        const double ybd = yb - yd, yac = ya - yc, xbd = xb - xd, xac = xa - xc;
+        const double iDNR = 1.0 / (xac * ybd - xbd * yac);
+        out[0] = ybd * iDNR;
+        out[stride] = -yac * iDNR;
+        out[2 * stride] = -xbd * iDNR;
+        out[3 * stride] = xac * iDNR;
+    };
+    const size_t nc = (size_t)ni * nj;
+    h->hcvol.assign(nc, 0.0);
+    const int ntj = (nj + TJ - 1) / TJ, nti = (ni + TI - 1) / TI;
+    h->hstile.assign((size_t)ntj * nti * STILE, 0.0);
+    for (int i = 0; i < ni; i++)
+        for (int j = 0; j < nj; j++) {
+            const size_t k = (size_t)i * nj + j;
+            double* blk = &h->hstile[((size_t)(i / TI) * ntj + j / TJ) * STILE];
+            const int ti = i % TI, tj = j % TJ, gc = 2 * SNN + ti * TJ + tj;
+            double xa, ya, xb, yb, xc, yc, xd, yd;
+            centroid(i, j - 1, xa, ya);  // NC1..NC4
+            centroid(i + 1, j, xb, yb);
+            centroid(i, j + 1, xc, yc);
+            centroid(i - 1, j, xd, yd);
+            grad(xa, ya, xb, yb, xc, yc, xd, yd, blk + gc + ST_GA * TI * TJ, (size_t)TI * TJ);
+            const size_t n1 = (size_t)i * (nj + 1) + j;
+            const double Xc[4] = {X[n1], X[n1 + nj + 1], X[n1 + nj + 2], X[n1 + 1]};
+            const double Yc[4] = {Y[n1], Y[n1 + nj + 1], Y[n1 + nj + 2], Y[n1 + 1]};
+            const double ycc = (Yc[0] + Yc[1] + Yc[2] + Yc[3]) * 0.25;
+            const double vol = cell_volume(iaxis, Xc, Yc, ycc);
+            h->hcvol[k] = vol;
+            blk[gc + ST_RVOL * TI * TJ] = 1.0 / vol;
+            blk[gc + ST_RYCC * TI * TJ] = 1.0 / ycc;
+        }
+    for (int a = 0; a <= ni; a++)  // nodes of each tile's cells; shared rows go to both tiles
+        for (int b = 0; b <= nj; b++)
+            for (int bi = std::max(0, (a - 1) / TI); bi <= std::min(nti - 1, a / TI); bi++)
+                for (int bj = std::max(0, (b - 1) / TJ); bj <= std::min(ntj - 1, b / TJ); bj++) {
+                    const int la = a - bi * TI, lb = b - bj * TJ;
+                    if (la < 0 || la > TI || lb < 0 || lb > TJ) continue;
+                    double* blk = &h->hstile[((size_t)bi * ntj + bj) * STILE];
+                    node(a, b, blk[la * SNW + lb], blk[SNN + la * SNW + lb]);
+                }
+    // one face: A = the evaluating cell, C = the neighbour, B, D = the face's nodes
+    auto face = [&](std::vector<double>& fg, size_t nf, size_t f, int ia, int ja, int ic, int jc,
+                    int ib, int jb, int id, int jd) {
+        double xa, ya, xc, yc, xb, yb, xd, yd;
+        centroid(ia, ja, xa, ya);
+        centroid(ic, jc, xc, yc);
+        node(ib, jb, xb, yb);
+        node(id, jd, xd, yd);
+        if (iaxis == 1) {
+            fg[FG_SX * nf + f] = (yd - yb) * (yb + yd) * HALF;
+            fg[FG_SY * nf + f] = -(xd - xb) * (yb + yd) * HALF;
+        } else {
+            fg[FG_SX * nf + f] = (yd - yb);
+            fg[FG_SY * nf + f] = -(xd - xb);
+        }
+        grad(xa, ya, xb, yb, xc, yc, xd, yd, &fg[FG_GA * nf + f], nf);
+        const double yavg = HALF * (yb + yd);
+        fg[FG_RYAVG * nf + f] = (iaxis == 1 && !(yavg < YAXIS_THRESH)) ? 1.0 / yavg : 0.0;
+    };
+    const size_t nfi = (size_t)(ni + 1) * nj, nfj = (size_t)ni * (nj + 1);
+    h->hfgi.assign((size_t)FG_N * nfi, 0.0);
+    h->hfgj.assign((size_t)FG_N * nfj, 0.0);
+    for (int i = 0; i <= ni; i++)
+        for (int j = 0; j < nj; j++) {
+            const size_t f = (size_t)i * nj + j;
+            if (i == 0)  // face 4 of cell (0, j): B = node (0, j+1), D = node (0, j)
+                face(h->hfgi, nfi, f, 0, j, -1, j, 0, j + 1, 0, j);
+            else  // face 2 of cell (i-1, j): B = node (i, j), D = node (i, j+1)
+                face(h->hfgi, nfi, f, i - 1, j, i, j, i, j, i, j + 1);
+        }
+    for (int i = 0; i < ni; i++)
+        for (int j = 0; j <= nj; j++) {
+            const size_t f = (size_t)i * (nj + 1) + j;
+            if (j == 0)  // face 1 of cell (i, 0): B = node (i, 0), D = node (i+1, 0)
+                face(h->hfgj, nfj, f, i, 0, i, -1, i, 0, i + 1, 0);
+            else  // face 3 of cell (i, j-1): B = node (i+1, j), D = node (i, j)
+                face(h->hfgj, nfj, f, i, j - 1, i, j, i + 1, j, i, j);
+        }
+}
+
 // Device copy of the layout built by build_mesh.
 int upload_mesh(tns_handle* h) {
     const size_t nnode = h->hX.size(), ncell = h->hcfldl.size(), ngs = h->hgxc.size();
@@ -225,10 +335,29 @@ int upload_mesh(tns_handle* h) {
         (rc = up(h->ports.p, h->port_ghosts.data(), h->port_ghosts.size() * 4)))
         return rc;
     if ((rc = h->cuda(cudaMemset(h->gport.p, 0, ngs * 8), "cudaMemset"))) return rc;
+    build_geometry(h);
+    if ((rc = h->cuda(h->cvol.alloc(h->hcvol.size()), "cudaMalloc")) ||
+        (rc = h->cuda(h->stile.alloc(h->hstile.size()), "cudaMalloc")) ||
+        (rc = h->cuda(h->fgi.alloc(h->hfgi.size()), "cudaMalloc")) ||
+        (rc = h->cuda(h->fgj.alloc(h->hfgj.size()), "cudaMalloc")) ||
+        (rc = up(h->cvol.p, h->hcvol.data(), h->hcvol.size() * 8)) ||
+        (rc = up(h->stile.p, h->hstile.data(), h->hstile.size() * 8)) ||
+        (rc = up(h->fgi.p, h->hfgi.data(), h->hfgi.size() * 8)) ||
+        (rc = up(h->fgj.p, h->hfgj.data(), h->hfgj.size() * 8)))
+        return rc;
+    // the host copies are not read again
+    std::vector<double>().swap(h->hcvol);
+    std::vector<double>().swap(h->hstile);
+    std::vector<double>().swap(h->hfgi);
+    std::vector<double>().swap(h->hfgj);
     Mesh& M = h->M;
     M.ni = h->ni; M.nj = h->nj; M.x = h->x.p; M.y = h->y.p; M.cfldl = h->cfldl.p; M.gtype = h->gtype.p;
     M.grank = h->grank.p; M.gxc = h->gxc.p; M.gyc = h->gyc.p; M.ginj = h->ginj.p;
     M.gport = h->gport.p;
+    M.cvol = h->cvol.p;
+    M.stile = h->stile.p;
+    M.fgi = h->fgi.p;
+    M.fgj = h->fgj.p;
     return TNS_OK;
 }
 
@@ -368,7 +497,7 @@ void enqueue_iteration_f64(tns_handle* h, bool monitor) {
         launch(h, K_STAGE, [&] {
             tns::launch_stage(P, M, in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
                               alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
-                              st == 3 ? h->status.p : nullptr, s);
+                              st == 3 ? h->status.p : nullptr, h->status.p, s);
         });
     }
 }
@@ -540,6 +669,8 @@ int check_status(tns_handle* h) {
         return rc;
     if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
     if (*h->status_host & 1u) return h->fail(TNS_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
+    if (*h->status_host & 2u)
+        return h->fail(TNS_ERR_CUDA, "a stage tile's static-data copy did not complete in its bounded wait");
     return TNS_OK;
 }
 
@@ -851,7 +982,8 @@ void tns_destroy(tns_handle* h) {
     h->qa2.release(); h->dqb.release(); h->dqc.release(); h->df.release(); h->visf.release();
     h->dtf.release();
     for (auto* b : {&h->x, &h->y, &h->cfldl, &h->gxc, &h->gyc, &h->ginj, &h->gport, &h->qa, &h->qb,
-                    &h->qc, &h->d, &h->vis, &h->dt, &h->dtmin, &h->partial, &h->primout})
+                    &h->qc, &h->d, &h->vis, &h->dt, &h->dtmin, &h->partial, &h->primout, &h->cvol,
+                    &h->stile, &h->fgi, &h->fgj})
         b->release();
     h->gtype.release(); h->grank.release(); h->ports.release();
     h->counter.release(); h->status.release(); h->cdiff.release();

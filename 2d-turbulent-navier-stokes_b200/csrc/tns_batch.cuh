@@ -23,7 +23,8 @@ struct StageArgs {
     const double* dtmin; // DTMIN (LOCAL=0)
     double alpha;
     unsigned long long* cdiff;  // 5 slots, ordered bits of max|Q_old-Q_new| (or null)
-    unsigned int* status;       // bit 0: non-finite state
+    unsigned int* status;       // bit 0: non-finite state (checked where non-null)
+    unsigned int* error;        // bit 1: a tile's static-block copy did not complete
 };
 
 template <class OutT>

@@ -110,7 +110,7 @@ BatchCase describe(tns_batch* b, int k) {
             for (int st = 0; st < 4; st++)
                 c.stage[mon][st] = tns::StageArgs{in[st], A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p,
                                                   alpha[st], (mon && st == 3) ? cdiff : nullptr,
-                                                  st == 3 ? status : nullptr};
+                                                  st == 3 ? status : nullptr, status};
     } else {
         double* q[2] = {h->state(), h->other_state()};
         c.qmx[0] = q[0];
@@ -488,11 +488,12 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
         if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))) return rc;
         for (int k = 0; k < n; k++) {
             if (!b->active[k]) continue;
-            if (b->h_status[k] & 1u) {
+            if (b->h_status[k] & 3u) {
+                // bit 0: non-finite state; bit 1: a tile's static-data copy did not complete
                 b->failed[k] = 1;
                 b->active[k] = 0;
                 any_failed = true;
-                if (case_status) case_status[k] = TNS_ERR_NONFINITE;
+                if (case_status) case_status[k] = (b->h_status[k] & 1u) ? TNS_ERR_NONFINITE : TNS_ERR_CUDA;
                 continue;
             }
             if (!monitor) continue;

@@ -3,9 +3,11 @@
 //
 // The arithmetic restates the reference solver's Fortran (paths relative to the
 // reference project) in its operation order, except where one reciprocal replaces a
-// run of divisions by the same value and T**0.6 is exp(0.6*log T) (each a few ulp);
-// the memory layout is new: cells live in a structured (i, j) block (j fastest), ghosts
-// in four side arrays, geometry is recomputed from node coordinates.
+// run of divisions by the same value, T**0.6 is computed by a division-free Newton
+// refinement, and stored gradient coefficients fold a division by a static determinant
+// (each a few ulp).  The memory layout is new: cells live in a structured (i, j) block
+// (j fastest), ghosts in four side arrays; face vectors come from the node coordinates
+// in each tile, the static gradient coefficients and volumes from per-mesh arrays.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -54,6 +56,17 @@ struct Params {
     double cp_pr, cp_prt;                // CP/PRANDTL, CP/PRANDTLT
 };
 
+// Static per-face geometry of the viscous flux (viscous.f90:130-217), [FG_N][nfaces]
+// for the i-faces (index i*NJ + j, between cells (i-1, j) and (i, j), i = 0..NI) and the
+// j-faces (index i*(NJ+1) + j, between (i, j-1) and (i, j), j = 0..NJ), each in the
+// orientation of the cell that evaluates it (that of cell (i-1, j) as its face 2, or of
+// (0, j) as its face 4; that of (i, j-1) as its face 3, or of (i, 0) as its face 1):
+//   FG_SX, FG_SY  face vector; FG_GA..FG_GD diamond-gradient coefficients (A = the cell,
+//   C = the neighbour, B, D = the face's nodes: dF/dx = (F_A - F_C) GA + (F_B - F_D) GB,
+//   dF/dy = (F_A - F_C) GC + (F_B - F_D) GD); FG_RYAVG 1/YAVG of the axisymmetric v/y
+//   term, or 0 where YAVG is below the axis threshold (then dv/dy).
+enum FaceGeo { FG_SX, FG_SY, FG_GA, FG_GB, FG_GC, FG_GD, FG_RYAVG, FG_N };
+
 // Ghost-side numbering: side 1 (j=-1) and 3 (j=NJ) are indexed by i, sides 2 (i=NI)
 // and 4 (i=-1) by j; the four runs are stored back to back.
 struct Mesh {
@@ -67,6 +80,10 @@ struct Mesh {
     const double* gyc;
     const double* ginj;     // type-6 burn-rate multiplier
     const double* gport;    // type-6 port mass flux of the current stage
+    const double* cvol;     // VOL per cell (geometry.f90:87,98,101)
+    const double* stile;    // static data of the stage tiles, one block per tile (tns_tile.cuh)
+    const double* fgi;      // [FG_N][(ni+1)*nj] static i-face geometry
+    const double* fgj;      // [FG_N][ni*(nj+1)] static j-face geometry
     __host__ __device__ int ghost_index(int side, int along) const {
         return side == 1 ? along : side == 2 ? ni + along : side == 3 ? ni + nj + along
                                                                       : 2 * ni + nj + along;
@@ -89,24 +106,26 @@ TNS_HD double powi(double x, int n) {
     return n < 0 ? 1.0 / r : r;
 }
 
-// T**0.6 for T > 0, y = T^(3/5): a single-precision estimate exp2(0.6 log2 T) (about
-// 1e-7 relative) refined by two Newton steps on f(y) = y^5 - T^3,
-//   y <- y - f(y)/f'(y) = 0.8 y + 0.2 T^3 / y^4,
-// whose error squares per step (e' ~ 2 e^2): 2e-14 after one, FP64 rounding after two.
-// Within a few ulp of pow, at less than half the instructions of exp(0.6 log T).
+// T**0.6 for T > 0, as T * w with w = T^(-2/5) = (T^2)^(-1/5): a single-precision
+// estimate exp2(-0.4 log2 T) (about 1e-7 relative) refined by two Newton steps for the
+// inverse fifth root of a = T^2, which need no division:
+//   w <- w + w (1 - a w^5) / 5,
+// whose error goes as e' ~ 3 e^2: 3e-14 after one step, FP64 rounding after two.
+// Within a few ulp of pow.
 TNS_HD double pow06(double T) {
 #ifdef __CUDA_ARCH__
-    double y = (double)exp2f(0.6f * __log2f((float)T));
+    double w = (double)exp2f(-0.4f * __log2f((float)T));
 #else
-    double y = (double)exp2f(0.6f * log2f((float)T));
+    double w = (double)exp2f(-0.4f * log2f((float)T));
 #endif
-    const double t3 = T * T * T;
+    const double a = T * T;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-        const double y2 = y * y;
-        y = 0.8 * y + 0.2 * t3 / (y2 * y2);
+        const double w2 = w * w;
+        const double t = 1.0 - a * (w2 * w2 * w);
+        w = w + 0.2 * w * t;
     }
-    return y;
+    return T * w;
 }
 
 // tanh(a) / tanh(b) for a, b >= 0, from tanh(x) = E / (E + 2) with E = expm1(2x):
@@ -316,26 +335,27 @@ TNS_HD void boundary_ghost(const Params& P, int type, const Prim& par,
     g.qm = sqrt(g.u * g.u + g.v * g.v);
 }
 
-// Turbulence / radial sources of one cell (source_terms.f90:258-320).  Neighbours
-// a,b,c,d are NC1..NC4.
+// Turbulence / radial sources of one cell (source_terms.f90:24-104).  Neighbours
+// a,b,c,d are NC1..NC4; ga..gd are the cell's stored coefficients of the centroid-
+// difference gradient (source_terms.f90:24-60): dF/dx = (F_a - F_c) ga + (F_b - F_d) gb,
+// dF/dy = (F_a - F_c) gc + (F_b - F_d) gd, i.e. ga = (y_b - y_d)/DNR, gb = -(y_a - y_c)/DNR,
+// gc = -(x_b - x_d)/DNR, gd = (x_a - x_c)/DNR with DNR = (x_a - x_c)(y_b - y_d) -
+// (x_b - x_d)(y_a - y_c) over the four neighbour centroids; RYCC is 1/YCC.
 struct SrcIn {
-    double xa, xb, xc, xd, ya, yb, yc, yd;
+    double ga, gb, gc, gd;
     double ua, ub, uc, ud, va, vb, vc, vd, ra, rb, rc, rd, qa, qb, qc, qd;
 };
 
 __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, double RHO,
                                              double RI, double TI, double PI, double VI,
-                                             double YCCI, double& src3, double& src5) {
-    const double ybd = s.yb - s.yd, yac = s.ya - s.yc, xbd = s.xb - s.xd, xac = s.xa - s.xc;
-    const double iDNR = 1.0 / (xac * ybd - xbd * yac);
-    const double DQX = ((s.qa - s.qc) * ybd - (s.qb - s.qd) * yac) * iDNR;
-    const double DRX = ((s.ra - s.rc) * ybd - (s.rb - s.rd) * yac) * iDNR;
-    const double DUX = ((s.ua - s.uc) * ybd - (s.ub - s.ud) * yac) * iDNR;
-    const double DVX = ((s.va - s.vc) * ybd - (s.vb - s.vd) * yac) * iDNR;
-    const double DQY = (-(s.qa - s.qc) * xbd + (s.qb - s.qd) * xac) * iDNR;
-    const double DRY = (-(s.ra - s.rc) * xbd + (s.rb - s.rd) * xac) * iDNR;
-    const double DUY = (-(s.ua - s.uc) * xbd + (s.ub - s.ud) * xac) * iDNR;
-    const double DVY = (-(s.va - s.vc) * xbd + (s.vb - s.vd) * xac) * iDNR;
+                                             double YCCI, double RYCC, double& src3,
+                                             double& src5) {
+    const double dqac = s.qa - s.qc, dqbd = s.qb - s.qd, drac = s.ra - s.rc, drbd = s.rb - s.rd;
+    const double duac = s.ua - s.uc, dubd = s.ub - s.ud, dvac = s.va - s.vc, dvbd = s.vb - s.vd;
+    const double DQX = dqac * s.ga + dqbd * s.gb, DQY = dqac * s.gc + dqbd * s.gd;
+    const double DRX = drac * s.ga + drbd * s.gb, DRY = drac * s.gc + drbd * s.gd;
+    const double DUX = duac * s.ga + dubd * s.gb, DUY = duac * s.gc + dubd * s.gd;
+    const double DVX = dvac * s.ga + dvbd * s.gb, DVY = dvac * s.gc + dvbd * s.gd;
     const double AMU = amu_of(P, TI);
     const double CHI = RHO * RI / (CMU * AMU);
     const double FMU = tanh_ratio(ALPHA_T * CHI * CHI, BETA_T * CHI * CHI);
@@ -346,9 +366,11 @@ __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, do
     if (PHI > 0.0) DEE = DRX * DRX + DRY * DRY;
     double PK;
     const double DIV23 = P.div23;
-    const double pw = powi(AMUT / dmax1(AMUT, AMU_THRESH * AMU), P.npseudo);
+    // (AMUT / DMAX1(AMUT, AMU_THRESH*AMU))**NPSEUDO: exactly 1 when AMUT is the larger
+    const double thr = AMU_THRESH * AMU;
+    const double pw = AMUT >= thr ? 1.0 : powi(AMUT / thr, P.npseudo);
     if (P.iaxis == 1) {
-        const double VBYY = (YCCI < YAXIS_THRESH) ? DVY : VI / YCCI;
+        const double VBYY = (YCCI < YAXIS_THRESH) ? DVY : VI * RYCC;
         const double DIVVEL = DUX + DVY + VBYY;
         PK = AMUT / RHO *
              (DUX * DUX + DVY * DVY + VBYY * VBYY + DUX * DUX + DVY * DVY + VBYY * VBYY +
@@ -356,7 +378,7 @@ __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, do
         PK = dmax1(PK, 0.0);
         src5 = (RHO * (CONST1 - CONST2 * FR2) * sqrt(RI * PK) - RHO * CONST3 * DEE) * pw;
         const double TTT = (AMU + AMUT) * (VBYY + VBYY - DIV23 * DIVVEL);
-        src3 = (PI - TTT) / YCCI;
+        src3 = (PI - TTT) * RYCC;
     } else {
         const double DIVVEL = DUX + DVY;
         PK = AMUT / RHO *
@@ -369,26 +391,30 @@ __device__ __forceinline__ void source_terms(const Params& P, const SrcIn& s, do
 }
 
 // One face of the thin-layer viscous flux (viscous.f90:130-217): A = the cell, C = the
-// face neighbour, B, D = the face's nodes (node averages).  Adds the face's
-// contribution to vis[0..3] (face 1 assigns, later faces accumulate).
+// face neighbour, B, D = the face's nodes (node averages).  FaceIn holds the coordinates
+// (the discrete adjoint's face reverse reads them).
 struct FaceIn {
     double sx, sy, xa, ya, xb, yb, xc, yc, xd, yd;
     double ua, va, ta, ub, vb, tb, uc, vc, tc, ud, vd, td;
     double rhoa, rhob, rhoc, rhod, ra, rb, rc, rd;
 };
 
-__device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, bool first,
-                                             double vis[4]) {
-    const double ybd = f.yb - f.yd, yac = f.ya - f.yc, xbd = f.xb - f.xd, xac = f.xa - f.xc;
-    const double iDNR = 1.0 / (xac * ybd - xbd * yac);
-    const double DUX = ((f.ua - f.uc) * ybd - (f.ub - f.ud) * yac) * iDNR;
-    const double DVX = ((f.va - f.vc) * ybd - (f.vb - f.vd) * yac) * iDNR;
-    const double DTX = ((f.ta - f.tc) * ybd - (f.tb - f.td) * yac) * iDNR;
-    const double DRX = ((f.ra - f.rc) * ybd - (f.rb - f.rd) * yac) * iDNR;
-    const double DUY = (-(f.ua - f.uc) * xbd + (f.ub - f.ud) * xac) * iDNR;
-    const double DVY = (-(f.va - f.vc) * xbd + (f.vb - f.vd) * xac) * iDNR;
-    const double DTY = (-(f.ta - f.tc) * xbd + (f.tb - f.td) * xac) * iDNR;
-    const double DRY = (-(f.ra - f.rc) * xbd + (f.rb - f.rd) * xac) * iDNR;
+// One face from its stored geometry (FG_*): the flux of viscous.f90:130-217 with the
+// diamond gradient from the coefficients.  Assigns vis[0..3].
+struct FaceVals {
+    double ua, va, ta, ub, vb, tb, uc, vc, tc, ud, vd, td;
+    double rhoa, rhob, rhoc, rhod, ra, rb, rc, rd;
+};
+
+__device__ __forceinline__ void viscous_face(const Params& P, const FaceVals& f, double sx,
+                                             double sy, double ga, double gb, double gc,
+                                             double gd, double ryavg, double vis[4]) {
+    const double duac = f.ua - f.uc, dubd = f.ub - f.ud, dvac = f.va - f.vc, dvbd = f.vb - f.vd;
+    const double dtac = f.ta - f.tc, dtbd = f.tb - f.td, drac = f.ra - f.rc, drbd = f.rb - f.rd;
+    const double DUX = duac * ga + dubd * gb, DUY = duac * gc + dubd * gd;
+    const double DVX = dvac * ga + dvbd * gb, DVY = dvac * gc + dvbd * gd;
+    const double DTX = dtac * ga + dtbd * gb, DTY = dtac * gc + dtbd * gd;
+    const double DRX = drac * ga + drbd * gb, DRY = drac * gc + drbd * gd;
     const double UAVG = QUARTER * (f.ua + f.ub + f.uc + f.ud);
     const double VAVG = QUARTER * (f.va + f.vb + f.vc + f.vd);
     const double TAVG = QUARTER * (f.ta + f.tb + f.tc + f.td);
@@ -396,8 +422,7 @@ __device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, b
     const double RAVG = QUARTER * (f.ra + f.rb + f.rc + f.rd);
     double DIVVEL;
     if (P.iaxis == 1) {
-        const double YAVG = HALF * (f.yb + f.yd);
-        const double VBYY = (YAVG < YAXIS_THRESH) ? DVY : VAVG / YAVG;
+        const double VBYY = (ryavg == 0.0) ? DVY : VAVG * ryavg;
         DIVVEL = DUX + DVY + VBYY;
     } else {
         DIVVEL = DUX + DVY;
@@ -415,17 +440,10 @@ __device__ __forceinline__ void viscous_face(const Params& P, const FaceIn& f, b
     const double TXY = AMUEFF * (DUY + DVX);
     const double QXX = UAVG * TXX + VAVG * TXY + AKEFF * DTX;
     const double QYY = UAVG * TXY + VAVG * TYY + AKEFF * DTY;
-    if (first) {
-        vis[0] = TXX * f.sx + TXY * f.sy;
-        vis[1] = TXY * f.sx + TYY * f.sy;
-        vis[2] = QXX * f.sx + QYY * f.sy;
-        vis[3] = AMUEFF * DRX * f.sx + AMUEFF * DRY * f.sy;
-    } else {
-        vis[0] = vis[0] + TXX * f.sx + TXY * f.sy;
-        vis[1] = vis[1] + TXY * f.sx + TYY * f.sy;
-        vis[2] = vis[2] + QXX * f.sx + QYY * f.sy;
-        vis[3] = vis[3] + AMUEFF * DRX * f.sx + AMUEFF * DRY * f.sy;
-    }
+    vis[0] = TXX * sx + TXY * sy;
+    vis[1] = TXY * sx + TYY * sy;
+    vis[2] = QXX * sx + QYY * sy;
+    vis[3] = AMUEFF * DRX * sx + AMUEFF * DRY * sy;
 }
 
 }  // namespace tns

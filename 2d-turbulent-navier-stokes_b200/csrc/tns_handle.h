@@ -52,6 +52,7 @@ struct tns_handle {
     std::vector<int> ghost_id;    // bc.in line -> Fortran ghost id
     std::vector<int> port_ghosts;
     std::vector<double> hX, hY, hcfldl, hgxc, hgyc, hginj;  // host layout (device order)
+    std::vector<double> hcvol, hstile, hfgi, hfgj;  // static geometry (VOL, stage tiles, faces)
     std::vector<int> hgtype, hgrank;
     std::vector<int> node_of;   // structured node index -> 1-based node id
     cudaStream_t own = nullptr, stream = nullptr;
@@ -59,7 +60,7 @@ struct tns_handle {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     DevBuf<double> x, y, cfldl, gxc, gyc, ginj, gport, qa, qb, qc, d, vis, dt, dtmin, partial,
-        primout;
+        primout, cvol, stile, fgi, fgj;
     // mixed FP32/FP64 path: FP64 state ping-pong (qa, qa2) and FP32 scratch
     int precision = 0;
     int cur = 0;  // mixed: which of qa / qa2 holds the state

@@ -20,15 +20,16 @@ namespace tns {
 
 // ------------------------------------------------------------------ stage kernel
 
-// Shared-memory fields of the stage tile, paired for 16-byte loads.
+// Shared-memory fields of the stage tile, paired for 16-byte loads; the tile's static
+// block (nodes, gradient coefficients, 1/VOL, 1/YCC) arrives by one bulk copy.
 struct StageSmem {
+    double st[STILE];      // static block (tns_tile.cuh)
     double2 fg[5][NSLOT];  // (F_m, G_m)
     double2 uv[NSLOT];     // (U, V)
-    double2 xy[NSLOT];     // centroid
     double2 rq[NSLOT];     // (C5/C1, |V|)
     double2 tp[NSLOT];     // (T, P)
     double rho[NSLOT];
-    double nx[NNODE], ny[NNODE];
+    unsigned long long bar;  // completion of the static block's copy
 };
 
 size_t stage_smem_bytes() { return sizeof(StageSmem); }
@@ -51,7 +52,12 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     pdl_trigger();
-    load_nodes(M, i0, j0, S.nx, S.ny);
+    // the static block is written by nothing: its copy overlaps the previous kernel's tail
+    if (tid == 0) {
+        bulk_barrier_init(&S.bar);
+        const size_t tile = (size_t)by * ((M.nj + TJ - 1) / TJ) + bx;
+        bulk_copy_start(S.st, M.stile + tile * STILE, STILE * sizeof(double), &S.bar);
+    }
     pdl_wait();
     __syncthreads();
     for (int s = tid; s < NSLOT; s += NTHREADS) {
@@ -60,19 +66,20 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
         Prim p;
-        if (kind == 0) {
+        if (kind == 0)
             cell_prim(P, A.qin, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-            const int n1 = li * NW + lj;
-            S.xy[s] = make_double2((S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25,
-                                   (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25);
-        } else {
+        else
             ghost_state(P, M, A.qin, ncell, kind, along, p);
-            const int g = M.ghost_index(kind, along);
-            S.xy[s] = make_double2(M.gxc[g], M.gyc[g]);
-        }
         put_slot(S, s, p);
     }
     __syncthreads();
+    if (!bulk_wait(&S.bar)) {
+        // the copy did not complete: report it, give it one more bounded wait (it writes
+        // this block's shared memory) and leave the tile
+        if (tid == 0) atomicOr(A.error, 2u);
+        bulk_wait(&S.bar);
+        return;
+    }
 
     const int tj = threadIdx.x, ti = threadIdx.y;
     const int i = i0 + ti, j = j0 + tj;
@@ -82,16 +89,36 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
         const size_t cell = (size_t)i * M.nj + j;
         const int c = (ti + 1) * SW + (tj + 1);
         const int nb[4] = {c - 1, c + SW, c + 1, c - SW};  // NC1..NC4
-        const int n1 = (ti + 1) * NW + (tj + 1);
-        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
-        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
+        const int n1 = ti * SNW + tj;  // node 1 of the cell in the static block
+        const int gc = 2 * SNN + ti * TJ + tj;
+        const double* X0 = S.st;
+        const double* Y0 = S.st + SNN;
+
+        // source terms first (source_terms.f90:24-104): only src3 / src5 stay live into
+        // the residual
+        double src3, src5;
+        {
+            SrcIn s;
+            s.ga = S.st[gc + ST_GA * NTHREADS]; s.gb = S.st[gc + ST_GB * NTHREADS];
+            s.gc = S.st[gc + ST_GC * NTHREADS]; s.gd = S.st[gc + ST_GD * NTHREADS];
+            const double2 ua = S.uv[nb[0]], ub = S.uv[nb[1]], uc = S.uv[nb[2]], ud = S.uv[nb[3]];
+            const double2 ra = S.rq[nb[0]], rb = S.rq[nb[1]], rc = S.rq[nb[2]], rd = S.rq[nb[3]];
+            s.ua = ua.x; s.ub = ub.x; s.uc = uc.x; s.ud = ud.x;
+            s.va = ua.y; s.vb = ub.y; s.vc = uc.y; s.vd = ud.y;
+            s.ra = ra.x; s.rb = rb.x; s.rc = rc.x; s.rd = rd.x;
+            s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
+            const double2 tp = S.tp[c];
+            const double YCCI = (Y0[n1] + Y0[n1 + SNW] + Y0[n1 + SNW + 1] + Y0[n1 + 1]) * 0.25;
+            source_terms(P, s, S.rho[c], S.rq[c].x, tp.x, tp.y, S.uv[c].y, YCCI,
+                         S.st[gc + ST_RYCC * NTHREADS], src3, src5);
+        }
+
+        // inviscid residual (residual.f90:23-62) with the sources (residual.f90:57-61)
+        const double X[4] = {X0[n1], X0[n1 + SNW], X0[n1 + SNW + 1], X0[n1 + 1]};
+        const double Y[4] = {Y0[n1], Y0[n1 + SNW], Y0[n1 + SNW + 1], Y0[n1 + 1]};
         double SX[4], SY[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) face_vector(P.iaxis, k + 1, X, Y, SX[k], SY[k]);
-        const double2 xyc = S.xy[c];
-        const double VOL = cell_volume(P.iaxis, X, Y, xyc.y);
-
-        // inviscid residual (residual.f90:23-62)
         double R[5];
 #pragma unroll
         for (int m = 0; m < 5; m++) {
@@ -101,29 +128,13 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
                            (I.y + b.y) * SY[1] + (I.x + e.x) * SX[2] + (I.y + e.y) * SY[2] +
                            (I.x + d.x) * SX[3] + (I.y + d.y) * SY[3]);
         }
-
-        // source terms (source_terms.f90:258-320)
-        {
-            SrcIn s;
-            const double2 xa = S.xy[nb[0]], xb = S.xy[nb[1]], xc = S.xy[nb[2]], xd = S.xy[nb[3]];
-            const double2 ua = S.uv[nb[0]], ub = S.uv[nb[1]], uc = S.uv[nb[2]], ud = S.uv[nb[3]];
-            const double2 ra = S.rq[nb[0]], rb = S.rq[nb[1]], rc = S.rq[nb[2]], rd = S.rq[nb[3]];
-            s.xa = xa.x; s.xb = xb.x; s.xc = xc.x; s.xd = xd.x;
-            s.ya = xa.y; s.yb = xb.y; s.yc = xc.y; s.yd = xd.y;
-            s.ua = ua.x; s.ub = ub.x; s.uc = uc.x; s.ud = ud.x;
-            s.va = ua.y; s.vb = ub.y; s.vc = uc.y; s.vd = ud.y;
-            s.ra = ra.x; s.rb = rb.x; s.rc = rc.x; s.rd = rd.x;
-            s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
-            const double2 tp = S.tp[c];
-            double src3, src5;
-            source_terms(P, s, S.rho[c], S.rq[c].x, tp.x, tp.y, S.uv[c].y, xyc.y, src3, src5);
-            R[4] = R[4] - VOL * src5;
-            if (P.iaxis == 1) R[2] = R[2] - VOL * src3;
-        }
+        const double VOL = M.cvol[cell];
+        R[4] = R[4] - VOL * src5;
+        if (P.iaxis == 1) R[2] = R[2] - VOL * src3;
 
         // update (residual.f90:67-83)
         const double DT = P.local ? A.dt[cell] : *A.dtmin;
-        const double DTBYVOL = DT / VOL;
+        const double DTBYVOL = DT * S.st[gc + ST_RVOL * NTHREADS];
         const double al = A.alpha;
         double Cn[5], Co[5], vis[4], dd[5];
 #pragma unroll
@@ -180,38 +191,28 @@ constexpr int NIF = (TI + 1) * TJ;
 constexpr int NJF = TI * (TJ + 1);
 
 struct ViscSmem {
-    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT], xc[NSLOT], yc[NSLOT];
+    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT];
     double au[NAVG], av[NAVG], at[NAVG], arho[NAVG], ar[NAVG];
     double fi[4][NIF], fj[4][NJF];
-    double nx[NNODE], ny[NNODE];
 };
 
 size_t visc_smem_bytes() { return sizeof(ViscSmem); }
 
-// One face flux (viscous.f90:130-217) in the orientation of cell A (slot sa) for its
-// face k (1..4): C = slot sc, B/D = face nodes given in node-average and node-grid
-// coordinates.
+// One face flux (viscous.f90:130-217) in the orientation of cell A (slot sa): C = slot
+// sc, B/D = the face's nodes in node-average coordinates, geometry from the face's
+// stored row fg[k * nf] (FG_*).
 __device__ __forceinline__ void face_flux(const Params& P, const ViscSmem& S, int sa, int sc,
-                                          int ab, int ad, int nb, int nd, double out[4]) {
-    FaceIn f;
-    f.xb = S.nx[nb]; f.yb = S.ny[nb];
-    f.xd = S.nx[nd]; f.yd = S.ny[nd];
-    if (P.iaxis == 1) {
-        f.sx = (f.yd - f.yb) * (f.yb + f.yd) * HALF;
-        f.sy = -(f.xd - f.xb) * (f.yb + f.yd) * HALF;
-    } else {
-        f.sx = (f.yd - f.yb);
-        f.sy = -(f.xd - f.xb);
-    }
-    f.xa = S.xc[sa]; f.ya = S.yc[sa];
-    f.xc = S.xc[sc]; f.yc = S.yc[sc];
+                                          int ab, int ad, const double* __restrict__ fg,
+                                          size_t nf, double out[4]) {
+    FaceVals f;
     f.ua = S.u[sa]; f.va = S.v[sa]; f.ta = S.t[sa];
     f.uc = S.u[sc]; f.vc = S.v[sc]; f.tc = S.t[sc];
     f.ub = S.au[ab]; f.vb = S.av[ab]; f.tb = S.at[ab];
     f.ud = S.au[ad]; f.vd = S.av[ad]; f.td = S.at[ad];
     f.rhoa = S.rho[sa]; f.rhoc = S.rho[sc]; f.rhob = S.arho[ab]; f.rhod = S.arho[ad];
     f.ra = S.ri[sa]; f.rc = S.ri[sc]; f.rb = S.ar[ab]; f.rd = S.ar[ad];
-    viscous_face(P, f, true, out);
+    viscous_face(P, f, fg[FG_SX * nf], fg[FG_SY * nf], fg[FG_GA * nf], fg[FG_GB * nf],
+                 fg[FG_GC * nf], fg[FG_GD * nf], P.iaxis == 1 ? fg[FG_RYAVG * nf] : 0.0, out);
 }
 
 // Frozen viscous flux VIS of Q_old (viscous.f90:29-217): nodal averages, then each face
@@ -225,26 +226,17 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     pdl_trigger();
-    load_nodes(M, i0, j0, S.nx, S.ny, VNT);
     pdl_wait();
-    __syncthreads();
     for (int s = tid; s < NSLOT; s += VNT) {
         const int li = s / SW, lj = s % SW;
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
         Prim p;
-        if (kind == 0) {
+        if (kind == 0)
             cell_prim(P, q, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-            const int n1 = li * NW + lj;
-            S.xc[s] = (S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25;
-            S.yc[s] = (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25;
-        } else {
+        else
             ghost_state(P, M, q, ncell, kind, along, p);
-            const int g = M.ghost_index(kind, along);
-            S.xc[s] = M.gxc[g];
-            S.yc[s] = M.gyc[g];
-        }
         S.u[s] = p.u; S.v[s] = p.v; S.t[s] = p.t; S.rho[s] = p.rho; S.ri[s] = p.ri;
     }
     __syncthreads();
@@ -295,8 +287,11 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
     __syncthreads();
     // all faces of the tile in one loop (i-faces first): at most three faces per thread,
     // one inlined copy of the face flux
+    const size_t nfi = (size_t)(M.ni + 1) * M.nj, nfj = (size_t)M.ni * (M.nj + 1);
     for (int f = tid; f < NIF + NJF; f += VNT) {
-        int sa, sc, ab, ad, nb, nd;
+        int sa, sc, ab, ad;
+        const double* fg;
+        size_t nf;
         if (f < NIF) {
             // i-face: orientation of cell (i-1, j) as its face 2, or of (0, j) as its face 4
             const int ii = f / TJ, jj = f % TJ;
@@ -304,12 +299,13 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
             if (i > M.ni || j >= M.nj) continue;
             const int sL = ii * SW + jj + 1, sR = sL + SW;  // cells (i-1, j), (i, j)
             const int aLo = ii * AW + jj, aHi = aLo + 1;    // nodes (i, j), (i, j+1)
-            const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
             if (i == 0) {  // face 4: B=N4, D=N1
-                sa = sR; sc = sL; ab = aHi; ad = aLo; nb = nHi; nd = nLo;
+                sa = sR; sc = sL; ab = aHi; ad = aLo;
             } else {  // face 2: B=N2, D=N3
-                sa = sL; sc = sR; ab = aLo; ad = aHi; nb = nLo; nd = nHi;
+                sa = sL; sc = sR; ab = aLo; ad = aHi;
             }
+            fg = M.fgi + ((size_t)i * M.nj + j);
+            nf = nfi;
         } else {
             // j-face: orientation of cell (i, j-1) as its face 3, or of (i, 0) as its face 1
             const int g = f - NIF;
@@ -318,15 +314,16 @@ __device__ __forceinline__ void viscous_tile(const Params& P, const Mesh& M, con
             if (i >= M.ni || j > M.nj) continue;
             const int sB = (ii + 1) * SW + jj, sT = sB + 1;  // cells (i, j-1), (i, j)
             const int aL = ii * AW + jj, aR = aL + AW;       // nodes (i, j), (i+1, j)
-            const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
             if (j == 0) {  // face 1: B=N1, D=N2
-                sa = sT; sc = sB; ab = aL; ad = aR; nb = nL; nd = nR;
+                sa = sT; sc = sB; ab = aL; ad = aR;
             } else {  // face 3: B=N3, D=N4
-                sa = sB; sc = sT; ab = aR; ad = aL; nb = nR; nd = nL;
+                sa = sB; sc = sT; ab = aR; ad = aL;
             }
+            fg = M.fgj + ((size_t)i * (M.nj + 1) + j);
+            nf = nfj;
         }
         double out[4];
-        face_flux(P, S, sa, sc, ab, ad, nb, nd, out);
+        face_flux(P, S, sa, sc, ab, ad, fg, nf, out);
         if (f < NIF) {
 #pragma unroll
             for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
@@ -455,12 +452,7 @@ __device__ __forceinline__ void dissipation_tile(const Params& P, const Mesh& M,
         } else {
             DT = *A.dtmin;
         }
-        // the cell's corners straight from the node arrays (read once per ring cell)
-        const size_t g1 = (size_t)i * (M.nj + 1) + j, g2 = g1 + M.nj + 1;
-        const double X[4] = {M.x[g1], M.x[g2], M.x[g2 + 1], M.x[g1 + 1]};
-        const double Y[4] = {M.y[g1], M.y[g2], M.y[g2 + 1], M.y[g1 + 1]};
-        const double ycc = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
-        sr[RVBD * NRSLOT + s] = cell_volume(P.iaxis, X, Y, ycc) / DT;
+        sr[RVBD * NRSLOT + s] = M.cvol[c] / DT;
     }
     __syncthreads();
 
@@ -863,8 +855,8 @@ void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis
 void launch_stage(const Params& P, const Mesh& M, const double* qin, const double* qold,
                   double* qout, const double* d, const double* vis, const double* dt,
                   const double* dtmin, double alpha, unsigned long long* cdiff,
-                  unsigned int* status, cudaStream_t s) {
-    StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status};
+                  unsigned int* status, unsigned int* error, cudaStream_t s) {
+    StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status, error};
     launch_tile(cdiff ? k_stage<1> : k_stage<0>, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s, P, M, A);
 }
 

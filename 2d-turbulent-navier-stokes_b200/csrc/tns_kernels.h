@@ -18,10 +18,11 @@ int dtmin_blocks(const Mesh& M);
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,
                         const double* dtmin, cudaStream_t s);
 void launch_viscous(const Params& P, const Mesh& M, const double* q, double* vis, cudaStream_t s);
+// error: bit 1 is set when a tile's static-block copy did not complete (must not be null)
 void launch_stage(const Params& P, const Mesh& M, const double* qin, const double* qold,
                   double* qout, const double* d, const double* vis, const double* dt,
                   const double* dtmin, double alpha, unsigned long long* cdiff,
-                  unsigned int* status, cudaStream_t s);
+                  unsigned int* status, unsigned int* error, cudaStream_t s);
 void launch_dtmin(const Params& P, const Mesh& M, const double* q, double* partial,
                   unsigned int* counter, double* dtmin, cudaStream_t s);
 void launch_time_step_scratch(const Params& P, const double* q, const double* cfldl,

@@ -48,6 +48,17 @@ constexpr int NNODE = (TI + 3) * NW;
 constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
 constexpr int NAVG = (TI + 1) * AW;
 
+// Static block of one stage tile (tile (bx, by) at M.stile + (by * ntiles_j + bx) * STILE),
+// built on the host: the nodes of the tile's cells, (i0..i0+TI) x (j0..j0+TJ), x then y
+// (index la * SNW + lb), then per cell (index ti * TJ + tj) the source-gradient
+// coefficients GA..GD, 1/VOL and 1/YCC (see source_terms).  Positions outside the mesh
+// hold zeros.  A multiple of 16 bytes, so a tile's block is one bulk copy.
+constexpr int SNW = TJ + 1;
+constexpr int SNN = (TI + 1) * SNW;
+enum StageTileField { ST_GA, ST_GB, ST_GC, ST_GD, ST_RVOL, ST_RYCC, ST_NF };
+constexpr int STILE = 2 * SNN + ST_NF * TI * TJ;
+static_assert(STILE % 2 == 0, "a stage tile block must be a multiple of 16 bytes");
+
 __device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny,
                                            int nthreads = NTHREADS) {
     const int tid = threadIdx.y * TJ + threadIdx.x;
@@ -78,6 +89,39 @@ __device__ __forceinline__ void pdl_wait() {
 #if TNS_PDL
     asm volatile("griddepcontrol.wait;" ::: "memory");
 #endif
+}
+
+// One-shot bulk copy global -> shared through the TMA engine, completed on an mbarrier
+// (cp.async.bulk with mbarrier::complete_tx).  Both addresses 16-byte aligned, bytes a
+// multiple of 16.  bulk_copy_start: one thread, after it initialised the barrier
+// (bulk_barrier_init); the block's other threads may wait on it after a __syncthreads.
+__device__ __forceinline__ void bulk_barrier_init(unsigned long long* bar) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_copy_start(void* dst, const void* src, unsigned bytes,
+                                                unsigned long long* bar) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
+}
+// Waits for phase 0 of the barrier with a bounded number of polls; false if the copy did
+// not complete in that many (the caller reports it and skips the tile).
+__device__ __forceinline__ bool bulk_wait(unsigned long long* bar, int max_polls = 1 << 20) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    for (int k = 0; k < max_polls; k++) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(b) : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 // Launch of a tile kernel that may overlap its predecessor's tail (see pdl_wait).
