@@ -4,7 +4,8 @@ Tolerances: FP64 everywhere; the GPU contracts a*b+c into FMA and uses CUDA's po
 so results are not bit-identical.  Q and the CDIFF history must agree to <= 1e-10
 relative (max-norm per variable).  Exception, documented in the oracle tests: with IAXIS=1
 and a type-5 axis, C5 is ill-conditioned in the scheme itself (a 1e-15 input change
-moves it by up to ~1e-4), so there C5 is checked against that envelope.
+moves it by up to ~1e-4), so there C5 is held to ENV_FACTOR times the oracle's own
+response to a 1e-15 relative perturbation of the initial state (measured ratios 0.5-2.2).
 """
 import numpy as np
 import pytest
@@ -15,6 +16,7 @@ from tnsgpu.solver import Solver
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
+ENV_FACTOR = 10.0
 
 
 def rel(a, b):
@@ -140,7 +142,7 @@ def test_axisymmetric_cases(kind):
     flow = cases.nozzle_plume_flow() if kind == "nozzle_plume" else cases.port_flow()
     err, env = _axi_check(mesh, flow, 20, kind)
     assert np.all(err[:4] < TOL), err
-    assert err[4] < max(100 * env[4], TOL), (err, env)
+    assert err[4] < max(ENV_FACTOR * env[4], TOL), (err, env)
     # same geometry with the axis as a symmetry line: well conditioned, full parity
     mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
     err, env = _axi_check(mesh, flow, 20, kind + " (type-4 axis)")
@@ -168,7 +170,7 @@ def test_full_size_nozzle_plume_200_iterations():
     mesh, flow = cases.nozzle_plume_mesh(1024, 384), cases.nozzle_plume_flow()
     err, env = _axi_check(mesh, flow, 200, "nozzle_plume")
     assert np.all(err[:4] < TOL), err
-    assert err[4] < max(100 * env[4], TOL), (err, env)
+    assert err[4] < max(ENV_FACTOR * env[4], TOL), (err, env)
 
 
 def test_full_size_port_channel_first_iterations():
@@ -177,7 +179,7 @@ def test_full_size_port_channel_first_iterations():
     mesh, flow = cases.port_mesh(4096, 1536), cases.port_flow()
     err, env = _axi_check(mesh, flow, 2, "port")
     assert np.all(err[:4] < TOL), err
-    assert err[4] < max(100 * env[4], TOL), (err, env)
+    assert err[4] < max(ENV_FACTOR * env[4], TOL), (err, env)
 
 
 def test_nonfinite_state_is_reported():
