@@ -113,7 +113,7 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
                          S.st[gc + ST_RYCC * NTHREADS], src3, src5);
         }
 
-        // inviscid residual (residual.f90:23-62) with the sources (residual.f90:57-61)
+        // inviscid residual (residual.f90:23-62) with the sources (residual.f90:54,58)
         const double X[4] = {X0[n1], X0[n1 + SNW], X0[n1 + SNW + 1], X0[n1 + 1]};
         const double Y[4] = {Y0[n1], Y0[n1 + SNW], Y0[n1 + SNW + 1], Y0[n1 + 1]};
         double SX[4], SY[4];

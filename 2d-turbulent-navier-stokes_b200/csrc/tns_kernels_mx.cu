@@ -149,7 +149,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             R64[m] = S.fref[m] * sumx + S.gref[m] * sumy;
         }
 
-        // source terms (source_terms.f90:258-320): FP64 stencil differences, FP32 rest
+        // source terms (source_terms.f90:24-104): FP64 stencil differences, FP32 rest
         {
             const int a = nb[0], b = nb[1], cc = nb[2], d = nb[3];
             const double2 xa = S.xy[a], xb = S.xy[b], xc = S.xy[cc], xd = S.xy[d];

@@ -4,7 +4,7 @@ flow and total-pressure loss.
 The reference computes none of these (THRUST is declared, solver_state.f90:40, and
 never used).  They are defined here on the solver's own discretisation: a boundary
 face carries the average of its parent cell and its ghost (the states the flux
-residual uses on that face, residual.f90:187-207), and the face's surface vector S is
+residual uses on that face, residual.f90:33-54), and the face's surface vector S is
 geometry.f90:77-99's, so axisymmetric forces and fluxes are per radian.
 
 All functions take a formats.Mesh and the [4, maxid] U, V, T, P array of

@@ -1,8 +1,9 @@
-"""Full-size adjoint check on the 512 x 192 ramp (run by hand on a GPU machine; not
-collected by pytest):
+"""Full-size adjoint check on the 512 x 192 ramp -- TEST INFRASTRUCTURE: it checks the
+product's CUDA adjoint against central finite differences of the GPU FP64 path and of
+the oracle, and prints the figures; run by hand on a GPU machine:
 
-  python tests/adjoint_report.py [--primal-iters 5000] [--transient-iters 500]
-                                 [--fixed-point-iters 200] [--oracle-fd]
+  python oracle/adjoint_report.py [--primal-iters 5000] [--transient-iters 500]
+                                  [--fixed-point-iters 200] [--oracle-fd]
 
 Geometry and BCs as the 192 x 64 ramp case, at 512 x 192 cells.  Parameters: P0, T0,
 AMACHINIT and the displacements of the 64 ramp-wall nodes i = 260, 264, ..., 512 (every
@@ -13,8 +14,8 @@ AMACHINIT and the displacements of the 64 ramp-wall nodes i = 260, 264, ..., 512
    (CDIFF at the end over CDIFF of iteration 1), then the fixed-point adjoint at that
    state (adjoint residual history).
 2. The transient gradient of J(Q_N), N = ``--transient-iters``, from the cold start:
-   primal on the GPU through the C ABI with a checkpoint per iteration, reverse sweep in
-   the differentiable restatement.  Two objectives: the wall pressure force (y) and the
+   primal on the GPU through the C ABI with a checkpoint (or a record of the forward
+   values) per iteration, reverse sweep of CUDA adjoint steps (tnsgpu.adjoint).  Two objectives: the wall pressure force (y) and the
    total-pressure loss between the inlet (side 4) and the outlet (side 2).
 3. Central finite differences (relative step 1e-6 and 2e-6; node displacement 3e-7 m
    and 6e-7 m) of both objectives for 4 parameters -- P0, T0, AMACHINIT and wall node
@@ -130,7 +131,7 @@ def main():
     for obj in objectives:
         t0 = time.perf_counter()
         r = adjoint.transient_gradient(sch, getattr(adjoint, obj), dy=dy.to(sch.device), space=space,
-                                       niter=N, primal="gpu")
+                                       niter=N)
         total = time.perf_counter() - t0
         grads[obj] = r
         out[obj] = {"J": r["J"], "dJ_dp0": r["dJ_dp0"], "dJ_dt0": r["dJ_dt0"],

@@ -1,9 +1,10 @@
-"""Fixed-point (steady-state) adjoint on a case that converges (run by hand on a GPU
-machine; not collected by pytest):
+"""Fixed-point (steady-state) adjoint on a case that converges -- TEST INFRASTRUCTURE:
+it checks the product's CUDA fixed-point adjoint against central finite differences of
+the converged objective and prints the figures; run by hand on a GPU machine:
 
-  python tests/adjoint_steady_report.py [--nx 64] [--ny 24] [--cfl 0.5] [--tol 1e-6]
-                                        [--adjoint-iters 600000] [--fd-iters 700000]
-                                        [--max-primal 2000000]
+  python oracle/adjoint_steady_report.py [--nx 64] [--ny 24] [--cfl 0.5] [--tol 1e-6]
+                                         [--adjoint-iters 600000] [--fd-iters 700000]
+                                         [--max-primal 2000000]
 
 The compression ramp (BCs as the 192 x 64 ramp case) at NX x NY cells and CFL 0.5, the
 one configuration of the ramp family whose explicit iteration converges.
@@ -90,7 +91,7 @@ def main():
     dy = torch.zeros(1, dtype=torch.float64)
     t0 = time.perf_counter()
     fp = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=a.adjoint_iters, dy=dy, space=space,
-                                     engine="cuda", history_every=50000)
+                                     history_every=50000)
     torch.cuda.synchronize()
     out["fixed_point"] = {"iterations": a.adjoint_iters, "seconds": time.perf_counter() - t0,
                           "residual_every_50k": fp["residual_history"]}

@@ -1,5 +1,5 @@
-"""Discrete adjoint (tnsgpu.adjoint): the differentiable restatement of one RK4 iteration
-against the oracle, the checkpointed reverse sweep against plain autograd, the gradients
+"""Discrete adjoint: the differentiable restatement of one RK4 iteration
+(oracle/adjoint_restatement.py, the CUDA adjoint's checker) against the oracle, the checkpointed reverse sweep against plain autograd, the gradients
 against central finite differences of the oracle, and the fixed-point adjoint against
 the truncated Neumann series it sums.  CPU only (torch FP64 on the host)."""
 import dataclasses
@@ -8,6 +8,8 @@ import numpy as np
 import pytest
 import torch
 
+from oracle.adjoint_restatement import (RestatedScheme, fixed_point_adjoint_torch,
+                                        transient_gradient_torch)
 from oracle.pyoracle import Oracle
 from tnsgpu import adjoint, cases, formats
 
@@ -46,7 +48,7 @@ def test_restatement_matches_oracle(name):
     rinit = formats.rinit_cold(flow)
     c0 = formats.cold_state(flow, mesh.neles, rinit)
     c0[0] *= 1 + 1e-3 * np.random.default_rng(1).uniform(-1, 1, mesh.neles)
-    sch = adjoint.Scheme(mesh, flow, rinit=rinit)
+    sch = RestatedScheme(mesh, flow, rinit=rinit)
     prm, geo = sch.params(), sch.geometry(sch.x0, sch.y0)
     o = Oracle(mesh, flow, rinit)
     o.set_state(c0)
@@ -70,7 +72,7 @@ def test_unsupported_boundary_types_are_refused():
 def _ramp_space(nx=24, ny=12, wall=(14, 18)):
     mesh, flow = cases.ramp_mesh(nx, ny), cases.ramp_flow()
     flow.istart = 0
-    sch = adjoint.Scheme(mesh, flow)
+    sch = RestatedScheme(mesh, flow)
     blend = 1.0 - cases.stretch_one_sided(ny, cases.beta_for_first_cell(ny, 0.3, 1e-5))
     space = adjoint.DesignSpace(sch, adjoint.ramp_wall_shape(sch, list(wall), blend))
     return mesh, flow, sch, space
@@ -79,8 +81,8 @@ def _ramp_space(nx=24, ny=12, wall=(14, 18)):
 def test_checkpointed_sweep_equals_autograd_through_all_iterations():
     mesh, flow, sch, space = _ramp_space(12, 8, wall=(8,))
     N = 6
-    r = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=torch.zeros(1, dtype=torch.float64),
-                                   space=space, niter=N, primal="torch")
+    r = transient_gradient_torch(sch, adjoint.wall_force_y, dy=torch.zeros(1, dtype=torch.float64),
+                                 space=space, niter=N, primal="torch")
     th = [torch.tensor(v, dtype=torch.float64, requires_grad=True) for v in (flow.p0, flow.t0, flow.amachinit)]
     dy = torch.zeros(1, dtype=torch.float64, requires_grad=True)
     prm = adjoint.Params(th[0], th[1], th[2], flow)
@@ -128,7 +130,7 @@ def test_gradient_matches_central_differences_of_the_oracle(objective):
     N = 20
     obj = getattr(adjoint, objective)
     dy0 = torch.zeros(2, dtype=torch.float64)
-    r = adjoint.transient_gradient(sch, obj, dy=dy0, space=space, niter=N, primal="torch")
+    r = transient_gradient_torch(sch, obj, dy=dy0, space=space, niter=N, primal="torch")
     got = {"p0": r["dJ_dp0"], "t0": r["dJ_dt0"], "am": r["dJ_damachinit"],
            "dy0": r["dJ_ddy"][0], "dy1": r["dJ_ddy"][1]}
     base = {"p0": flow.p0, "t0": flow.t0, "am": flow.amachinit, "dy0": 1.0, "dy1": 1.0}
@@ -152,7 +154,7 @@ def test_fixed_point_adjoint_sums_the_neumann_series():
         for _ in range(3):
             Q = sch.iteration(Q, geo, prm)
     K = 4
-    r = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, Q, niter=K)
+    r = fixed_point_adjoint_torch(sch, adjoint.wall_force_y, Q, niter=K)
     n = Q.numel()
     A = torch.autograd.functional.jacobian(lambda q: sch.iteration(q.reshape(Q.shape), geo, prm).reshape(-1),
                                            Q.reshape(-1))

@@ -2,7 +2,7 @@
 
 The adjoint point functions are compiled for the host (tests/adjoint_host/adj_host.cu)
 and run in the order the CUDA kernels run them.  For one RK4 iteration Q_{n+1} = G(Q_n)
-of the differentiable restatement (tnsgpu.adjoint.Scheme) and a random lambda, they must
+of the differentiable restatement (oracle/adjoint_restatement.py) and a random lambda, they must
 reproduce lambda dG/dQ_n and the sensitivities to every geometric quantity the iteration
 reads (face vectors, volumes, DL, cell / ghost centroids, node coordinates), RTOLERANCE,
 S0 and T0 -- the gradients autograd returns for those quantities made leaves."""
@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 import torch
 
+from oracle.adjoint_restatement import RestatedScheme
 from tnsgpu import adjoint, cases, formats
 from tnsgpu.solver import make_params
 
@@ -62,7 +63,7 @@ def harness(tmp_path_factory):
 
 
 def _stages(sch, Cold, geo, prm, rtol):
-    """Scheme.iteration, keeping the stage states, D, VIS and DT."""
+    """RestatedScheme.iteration, keeping the stage states, D, VIS and DT."""
     dt, p = sch.time_step(Cold, geo, prm)
     D = sch.dissipation(Cold, p, dt, geo, rtol)
     Cs, Cc, vis = [Cold], Cold, None
@@ -126,7 +127,7 @@ def _state(mesh, flow, sch, rinit, seed):
 def _run(harness, name, seed=0):
     mesh, flow = CASES[name]()
     rinit = formats.rinit_cold(flow)
-    sch = adjoint.Scheme(mesh, flow, rinit=rinit)
+    sch = RestatedScheme(mesh, flow, rinit=rinit)
     ni, nj = sch.ni, sch.nj
     Cn = _state(mesh, flow, sch, rinit, seed).requires_grad_(True)
     prm = sch.params()

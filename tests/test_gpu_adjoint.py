@@ -1,11 +1,14 @@
-"""Discrete adjoint on the GPU: the differentiable restatement (torch FP64 on cuda)
-against the CUDA FP64 path; the hand-written CUDA adjoint (tns_adjoint_step, the
-default engine on a GPU) against autograd of the restatement, step by step and over a
-transient; and its gradients against central finite differences of the GPU FP64 path."""
+"""Discrete adjoint on the GPU: the differentiable restatement (oracle/adjoint_restatement,
+torch FP64 on cuda) against the CUDA FP64 path; the hand-written CUDA adjoint
+(tns_adjoint_step, the product's engine) against autograd of the restatement, step by
+step and over a transient; and its gradients against central finite differences of the
+GPU FP64 path."""
 import numpy as np
 import pytest
 import torch
 
+from oracle.adjoint_restatement import (RestatedScheme, fixed_point_adjoint_torch,
+                                        transient_gradient_torch)
 from tnsgpu import adjoint, cases, formats
 from tnsgpu.solver import Solver
 
@@ -15,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def _ramp(nx=64, ny=24, wall=(40, 52)):
     mesh, flow = cases.ramp_mesh(nx, ny), cases.ramp_flow()
     flow.istart = 0
-    sch = adjoint.Scheme(mesh, flow, device="cuda")
+    sch = RestatedScheme(mesh, flow, device="cuda")
     blend = 1.0 - cases.stretch_one_sided(ny, cases.beta_for_first_cell(ny, 0.3, 1e-5))
     space = adjoint.DesignSpace(sch, adjoint.ramp_wall_shape(sch, list(wall), blend))
     return mesh, flow, sch, space
@@ -24,7 +27,7 @@ def _ramp(nx=64, ny=24, wall=(40, 52)):
 def test_restatement_on_cuda_matches_the_cuda_fp64_path():
     mesh, flow = cases.ramp_mesh(64, 24), cases.ramp_flow()
     c0, rinit = cases.noisy_restart_state(flow, mesh.neles)
-    sch = adjoint.Scheme(mesh, flow, device="cuda", rinit=rinit)
+    sch = RestatedScheme(mesh, flow, device="cuda", rinit=rinit)
     prm, geo = sch.params(), sch.geometry(sch.x0, sch.y0)
     s = Solver(mesh, flow, rinit, precision=0)
     s.upload(c0)
@@ -46,7 +49,7 @@ def test_gpu_primal_gradient_matches_gpu_finite_differences():
     mesh, flow, sch, space = _ramp()
     N = 40
     dy0 = torch.zeros(2, dtype=torch.float64)
-    r = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy0, space=space, niter=N, primal="gpu")
+    r = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy0, space=space, niter=N)
     got = {"p0": r["dJ_dp0"], "t0": r["dJ_dt0"], "am": r["dJ_damachinit"], "dy0": r["dJ_ddy"][0]}
     base = {"p0": flow.p0, "t0": flow.t0, "am": flow.amachinit, "dy0": 1.0}
     eps = np.finfo(np.float64).eps
@@ -77,7 +80,7 @@ def test_autograd_function_backward_is_the_adjoint():
     J = adjoint.TransientObjective.apply(theta, sch, adjoint.wall_force_y, space, 10)
     J.backward()
     r = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=torch.zeros(1, dtype=torch.float64),
-                                   space=space, niter=10, primal="gpu")
+                                   space=space, niter=10)
     ref = torch.tensor([r["dJ_dp0"], r["dJ_dt0"], r["dJ_damachinit"], r["dJ_ddy"][0]], dtype=torch.float64)
     assert torch.allclose(theta.grad, ref, rtol=1e-12, atol=0.0)
     assert abs(float(J) - r["J"]) <= 1e-12 * abs(r["J"])
@@ -86,10 +89,10 @@ def test_autograd_function_backward_is_the_adjoint():
 def test_graphed_reverse_step_equals_eager():
     mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
     dy = torch.zeros(1, dtype=torch.float64)
-    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
-                                   graph=True, engine="torch")
-    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
-                                   states=a["states"], graph=False, engine="torch")
+    a = transient_gradient_torch(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
+                                 graph=True)
+    b = transient_gradient_torch(sch, adjoint.wall_force_y, dy=dy, space=space, niter=8, primal="gpu",
+                                 states=a["states"], graph=False)
     for k in ("dJ_dp0", "dJ_dt0", "dJ_damachinit"):
         assert abs(a[k] - b[k]) <= 1e-12 * abs(b[k]), (k, a[k], b[k])
     assert abs(a["dJ_ddy"][0] - b["dJ_ddy"][0]) <= 1e-12 * abs(b["dJ_ddy"][0])
@@ -129,7 +132,7 @@ def test_cuda_adjoint_step_matches_autograd(name):
     a developed state; the parameter sensitivities through the gradient they give."""
     mesh, flow = STEP_CASES[name]()
     rinit = formats.rinit_cold(flow)
-    sch = adjoint.Scheme(mesh, flow, device="cuda", rinit=rinit)
+    sch = RestatedScheme(mesh, flow, device="cuda", rinit=rinit)
     space = adjoint.DesignSpace(sch)
     c0 = formats.cold_state(flow, mesh.neles, rinit)
     rng = np.random.default_rng(3)
@@ -167,10 +170,9 @@ def test_cuda_engine_transient_gradient_matches_torch_engine():
     mesh, flow, sch, space = _ramp(64, 24, wall=(40, 46, 52))
     dy = torch.tensor([1e-5, -2e-5, 5e-6], dtype=torch.float64)
     N = 30
-    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
-                                   engine="cuda")
-    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
-                                   engine="torch", states=a["states"].reshape(N + 1, 5, -1).cpu().numpy())
+    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N)
+    b = transient_gradient_torch(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
+                                 states=a["states"].reshape(N + 1, 5, -1).cpu().numpy())
     assert abs(a["J"] - b["J"]) <= 1e-13 * abs(b["J"])
     # tolerance on each derivative: 1e-9 of itself or of its natural scale |J| / |p|
     # (a derivative that nearly cancels is compared at the scale of its terms)
@@ -190,10 +192,8 @@ def test_cuda_fixed_point_adjoint_matches_torch_engine():
     qstar = torch.tensor(s.download().reshape(5, *mesh.shape), device="cuda")
     s.close()
     dy = torch.zeros(1, dtype=torch.float64)
-    a = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space,
-                                    engine="cuda")
-    b = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space,
-                                    engine="torch")
+    a = adjoint.fixed_point_adjoint(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space)
+    b = fixed_point_adjoint_torch(sch, adjoint.wall_force_y, qstar, niter=20, dy=dy, space=space)
     assert np.allclose(a["residual_history"], b["residual_history"], rtol=1e-8)
     for k, p in (("dJ_dp0", flow.p0), ("dJ_dt0", flow.t0), ("dJ_damachinit", flow.amachinit)):
         tol = 1e-9 * max(abs(b[k]), abs(b["J"]) / p)
@@ -251,8 +251,8 @@ def test_bounded_memory_sweep_equals_stored_states():
     mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
     dy = torch.tensor([2e-5], dtype=torch.float64)
     N = 30
-    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, engine="cuda")
-    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N, engine="cuda",
+    a = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N)
+    b = adjoint.transient_gradient(sch, adjoint.wall_force_y, dy=dy, space=space, niter=N,
                                    max_states=4)
     assert b["states"] is None and b["recomputed_iterations"] > N
     assert a["J"] == b["J"]
@@ -268,8 +268,8 @@ def test_scalar_sensitivities_equal_full_ones():
     mesh, flow, sch, space = _ramp(48, 16, wall=(30,))
     N = 20
     a = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, dy=torch.zeros(1, dtype=torch.float64),
-                                   space=space, niter=N, engine="cuda")
-    b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, niter=N, engine="cuda")
+                                   space=space, niter=N)
+    b = adjoint.transient_gradient(sch, adjoint.total_pressure_loss, niter=N)
     for k in ("J", "dJ_dp0", "dJ_dt0", "dJ_damachinit"):
         assert a[k] == b[k], (k, a[k], b[k])
 

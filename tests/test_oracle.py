@@ -156,7 +156,7 @@ def test_oracle_matches_literal_dt_and_dissipation():
 def test_axis_wall_sensitivity_is_a_property_of_the_scheme():
     """With IAXIS=1 and the axis as a type-5 wall, a 1e-15 relative input change moves C5
     by orders of magnitude more after one iteration (the PHI>0 switch of DEE,
-    source_terms.f90:290-291, acting on roundoff-level radial velocity); with the axis as
+    source_terms.f90:71-72, acting on roundoff-level radial velocity); with the axis as
     type 4 it does not.  GPU parity tests for such cases are compared against this envelope."""
     f = cases.port_flow()
     for axis_type, big in ((5, True), (4, False)):
