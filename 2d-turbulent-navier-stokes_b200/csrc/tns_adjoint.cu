@@ -382,6 +382,7 @@ long long enqueue_step(tns_handle* h, tns_adjoint_state* s, int set, int mode, i
 }
 
 int check_mesh(tns_handle* h) {
+    if (h->unstructured) return h->fail(TNS_ERR_UNSUPPORTED, "the adjoint needs one structured i x j block");
     if (h->precision != 0) return h->fail(TNS_ERR_ARG, "the adjoint runs on FP64 handles (precision 0)");
     if (!h->identity) return h->fail(TNS_ERR_ARG, "the adjoint needs cells numbered in (i, j) order");
     if (h->ni < 3 || h->nj < 3) return h->fail(TNS_ERR_ARG, "the adjoint needs at least 3 x 3 cells");

@@ -19,6 +19,7 @@
 #include "tns_handle.h"
 #include "tns_params.h"
 #include "tns_tile.cuh"
+#include "tns_umesh.h"
 
 using tns::make_params;
 
@@ -470,6 +471,10 @@ void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) 
 // One RK4 iteration (turbnstwod.f90:97-168).  Buffers: A = state, B/C = stage scratch;
 // stage 4 writes A in place (each cell reads only its own COLD there).
 void enqueue_iteration_f64(tns_handle* h, bool monitor) {
+    if (h->unstructured) {
+        enqueue_iteration_u(h, monitor);
+        return;
+    }
     const Params& P = h->P;
     const Mesh& M = h->M;
     double *A = h->qa.p, *B = h->qb.p, *Cq = h->qc.p;
@@ -519,13 +524,21 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
         return h->fail(TNS_ERR_ARG, "GAMA must exceed 1, AMOL and CFL must be positive");
     h->P = make_params(*params);
     int rc;
-    // host-side validation and layout first: mesh errors are reported without a GPU
-    if ((rc = build_mesh(h, mesh))) return rc;
+    // host-side validation and layout first: mesh errors are reported without a GPU.  A
+    // mesh that is not one structured block takes the general (gather) layout, FP64 only.
+    rc = build_mesh(h, mesh);
+    if (rc == TNS_ERR_UNSUPPORTED) {
+        const std::string why = h->err;
+        if (h->precision != 0)
+            return h->fail(TNS_ERR_UNSUPPORTED, "mixed precision needs one structured i x j block (%s)", why.c_str());
+        rc = tns_rt::umesh_build(h, mesh);
+    }
+    if (rc) return rc;
     if ((rc = h->cuda(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
     h->stream = h->own;
     if ((rc = h->cuda(tns::configure_kernels(), "cudaFuncSetAttribute"))) return rc;
     if ((rc = h->cuda(tns::configure_kernels_mx(), "cudaFuncSetAttribute"))) return rc;
-    if ((rc = upload_mesh(h))) return rc;
+    if ((rc = h->unstructured ? tns_rt::umesh_upload(h) : upload_mesh(h))) return rc;
     if ((rc = alloc_state(h))) return rc;
     cudaEventCreate(&h->ev[0]);
     cudaEventCreate(&h->ev[1]);
@@ -538,6 +551,7 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
 
 int tns_set_injection_scale(tns_handle* h, const double* scale) {
     if (!h || !scale) return TNS_ERR_ARG;
+    if (h->unstructured) return tns_rt::umesh_set_injection(h, scale);
     std::vector<double> g((size_t)h->M.nghosts(), 1.0);
     for (size_t k = 0; k < g.size(); k++) g[k] = scale[h->ghost_line[k]];
     return h->cuda(cudaMemcpy(h->ginj.p, g.data(), g.size() * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
@@ -768,6 +782,7 @@ int tns_download_state(tns_handle* h, double* c1, double* c2, double* c3, double
 namespace {
 // U, V, T, P of the last stage's input for cells and ghosts into h->primout (device).
 int fill_primitives(tns_handle* h) {
+    if (h->unstructured) return tns_rt::umesh_primitives(h);
     const size_t nc = h->ncell(), ng = (size_t)h->M.nghosts(), nt = nc + ng;
     int rc;
     if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
@@ -790,7 +805,7 @@ extern "C" {
 int tns_download_primitives(tns_handle* h, double* u, double* v, double* t, double* p) {
     if (!h || !u || !v || !t || !p) return TNS_ERR_ARG;
     if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_download_primitives: no iteration has run");
-    const size_t nc = h->ncell(), ng = (size_t)h->M.nghosts(), nt = nc + ng;
+    const size_t nc = h->ncell(), ng = h->unstructured ? (size_t)h->nghosts : (size_t)h->M.nghosts(), nt = nc + ng;
     int rc;
     if ((rc = fill_primitives(h))) return rc;
     std::vector<double> hb(4 * nt);
@@ -810,11 +825,21 @@ int tns_node_averages(tns_handle* h, double* pn, double* un, double* vn, double*
     if (!h || !pn || !un || !vn || !tn) return TNS_ERR_ARG;
     if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_node_averages: no iteration has run");
     int rc;
-    if ((rc = fill_primitives(h))) return rc;
-    const size_t nnode = (size_t)(h->ni + 1) * (h->nj + 1);
+    const size_t nnode = h->unstructured ? (size_t)h->nods : (size_t)(h->ni + 1) * (h->nj + 1);
     DevBuf<double> dn;
     if ((rc = h->cuda(dn.alloc(4 * nnode), "cudaMalloc"))) return rc;
-    tns::launch_node_average(h->M, h->primout.p, dn.p, h->stream);
+    if (h->unstructured) {
+        if ((rc = tns_rt::umesh_node_averages(h, dn.p))) {
+            dn.release();
+            return rc;
+        }
+    } else {
+        if ((rc = fill_primitives(h))) {
+            dn.release();
+            return rc;
+        }
+        tns::launch_node_average(h->M, h->primout.p, dn.p, h->stream);
+    }
     std::vector<double> hb(4 * nnode);
     rc = h->cuda(cudaMemcpyAsync(hb.data(), dn.p, 4 * nnode * 8, cudaMemcpyDeviceToHost, h->stream),
                  "cudaMemcpyAsync");
@@ -831,11 +856,18 @@ int tns_boundary_integrals(tns_handle* h, int type, int side, double out[4]) {
     if (!h || !out || type < 0 || type > 7 || side < 0 || side > 4) return TNS_ERR_ARG;
     if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_boundary_integrals: no iteration has run");
     int rc;
-    if ((rc = fill_primitives(h))) return rc;
     DevBuf<double> acc;
     if ((rc = h->cuda(acc.alloc(4), "cudaMalloc"))) return rc;
     cudaMemsetAsync(acc.p, 0, 4 * sizeof(double), h->stream);
-    tns::launch_boundary_sums(h->P, h->M, h->primout.p, type, side, acc.p, h->stream);
+    if (h->unstructured) {
+        rc = tns_rt::umesh_boundary_sums(h, type, side, acc.p);
+    } else if (!(rc = fill_primitives(h))) {
+        tns::launch_boundary_sums(h->P, h->M, h->primout.p, type, side, acc.p, h->stream);
+    }
+    if (rc) {
+        acc.release();
+        return rc;
+    }
     rc = h->cuda(cudaMemcpyAsync(out, acc.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
                  "cudaMemcpyAsync");
     if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
@@ -973,6 +1005,7 @@ void tns_destroy(tns_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     tns_rt::adjoint_release(h);
+    tns_rt::umesh_release(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     for (auto g : h->graph_mx)
         if (g) cudaGraphExecDestroy(g);

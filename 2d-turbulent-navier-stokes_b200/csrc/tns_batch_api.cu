@@ -341,6 +341,8 @@ int tns_batch_create(tns_handle* const* cases, int ncases, tns_batch** out) {
         for (int j = 0; j < k; j++)
             if (cases[j] == cases[k]) return b->fail(TNS_ERR_ARG, "tns_batch_create: case %d repeats case %d", k, j);
         if (!cases[k]->qa.p) return b->fail(TNS_ERR_STATE, "tns_batch_create: case %d was not created", k);
+        if (cases[k]->unstructured)
+            return b->fail(TNS_ERR_UNSUPPORTED, "tns_batch_create: case %d is not one structured i x j block", k);
     }
     b->cases.assign(cases, cases + ncases);
     b->precision = cases[0]->precision;

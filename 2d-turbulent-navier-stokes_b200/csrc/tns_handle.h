@@ -40,6 +40,7 @@ struct DevBuf {
 using namespace tns_rt;
 
 struct tns_adjoint_state;  // tns_adjoint.cu
+struct tns_umesh_state;    // tns_unstructured.cu
 
 struct tns_handle {
     std::string err;
@@ -84,6 +85,10 @@ struct tns_handle {
     long long kcount[K_NKERNEL] = {0};
     long long launches = 0;
     tns_adjoint_state* adj = nullptr;  // discrete adjoint buffers (tns_adjoint_enable)
+    // a general quad mesh (not one i x j block): cells in reverse Cuthill-McKee order,
+    // ni = NELES and nj = 1, laid out and iterated by tns_unstructured.cu
+    bool unstructured = false;
+    tns_umesh_state* umesh = nullptr;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];

@@ -1,0 +1,101 @@
+// tns_umesh.h -- general quadrilateral meshes: the device view of a mesh that is not one
+// structured i x j block, and the runtime entry points of tns_unstructured.cu.
+//
+// The reference works on any quad connectivity (geometry.f90:31-52 reads NOD(:,1:4) and
+// NC1..NC4 as given; every stencil gathers through NCk(I)).  Such a mesh is laid out
+// by a reverse Cuthill-McKee renumbering of its cells, so that the neighbours a cell
+// gathers sit close in memory; ghosts are slots NE..NE+NGHOSTS-1 in bc.in order, nodes
+// keep their ids.  Every kernel gathers through index arrays.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/tnsgpu.h"
+#include "tns_device.cuh"
+
+struct tns_handle;
+
+namespace tns {
+
+// Static per-cell geometry [UCG_N][ne] (geometry.f90:55-149 with the gradient
+// coefficients of source_terms.f90:24-60, as in source_terms()).
+enum UCellGeo {
+    UCG_SX1, UCG_SX2, UCG_SX3, UCG_SX4, UCG_SY1, UCG_SY2, UCG_SY3, UCG_SY4,
+    UCG_GA, UCG_GB, UCG_GC, UCG_GD, UCG_VOL, UCG_RVOL, UCG_YCC, UCG_RYCC, UCG_N
+};
+// Static geometry of face k (0..3) of each cell for the viscous flux (viscous.f90:130-217,
+// A = the cell, C = NC_k, B = node N_k, D = node N_k+1): [UFG_N][4][ne], the
+// diamond-gradient coefficients and 1/YAVG (0 where YAVG is below the axis threshold).
+enum UFaceGeo { UFG_GA, UFG_GB, UFG_GC, UFG_GD, UFG_RYAVG, UFG_N };
+// Per-slot (cells, then ghosts) primitive and flux field set of one stage [UW_N][ne+ng].
+enum USlot {
+    UW_F1, UW_F2, UW_F3, UW_F4, UW_F5, UW_G1, UW_G2, UW_G3, UW_G4, UW_G5,
+    UW_U, UW_V, UW_T, UW_P, UW_RHO, UW_RI, UW_QM, UW_N
+};
+
+struct UMesh {
+    int ne, ng, nnode, nport;
+    const int* nc;        // [4][ne] neighbour slot: a cell 0..ne-1 or a ghost ne+line
+    const int* nod;       // [4][ne] 0-based node ids
+    const double* cg;     // [UCG_N][ne]
+    const double* fg;     // [UFG_N][4][ne]
+    const double* cfldl;  // [ne] CFL*DL
+    const int* gpar;      // [ng] parent cell
+    const int* gopp;      // [ng] the parent's neighbour across the face opposite the ghost
+    const int* gtype;     // [ng] BC type
+    const int* gside;     // [ng] NSIDE
+    const double* gsx;    // [ng] the parent's face vector on the ghost's side
+    const double* gsy;
+    const double* gyc;    // [ng] mirrored ghost centroid y (geometry.f90:114-142)
+    const double* ginj;   // [ng] type-6 burn-rate multiplier
+    double* gport;        // [ng] type-6 port mass flux of the current stage input
+    const int* nptr;      // [nnode+1] contributions of each node (cells by id, then ghosts)
+    const int* nslot;     // contributing slot
+    const int* nreset;    // 0, or the BC type (4, 5) whose reset follows the contribution
+    const int* pghost;    // [nport] ghost line of each type-6 ghost
+    const int* pptr;      // [nport+1] the cells of its port line, from the parent across
+    const int* pcell;
+    const double* pdely;  // DELY of each of those cells for the ghost's side
+};
+
+struct StageArgsU {
+    const double* W;     // slot field set of the stage input
+    const double* qold;  // [5][ne] state at the start of the iteration
+    double* qout;        // [5][ne] stage output (may alias qold: own-cell reads only)
+    const double* d;     // [5][ne]
+    const double* vis;   // [4][ne]
+    const double* dt;    // [ne] (LOCAL=1)
+    const double* dtmin; // (LOCAL=0)
+    double alpha;
+    unsigned long long* cdiff;
+    unsigned int* status;
+};
+
+void launch_u_prim(const Params& P, const UMesh& M, const double* q, double* W, cudaStream_t s);
+void launch_u_gport(const Params& P, const UMesh& M, const double* q, cudaStream_t s);
+void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, double* d,
+                          double* dt, const double* dtmin, cudaStream_t s);
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vis,
+                      cudaStream_t s);
+void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s);
+void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s);
+void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_t s);
+void launch_u_boundary_sums(const Params& P, const UMesh& M, const double* W, int type, int side,
+                            double* out, cudaStream_t s);
+
+}  // namespace tns
+
+namespace tns_rt {
+// Host layout of a general mesh (after build_mesh found no structured block): validates
+// the arrays as build_mesh does, renumbers the cells, computes the geometry.
+int umesh_build(tns_handle* h, const tns_mesh* m);
+int umesh_upload(tns_handle* h);
+void enqueue_iteration_u(tns_handle* h, bool monitor);
+// U, V, T, P of cells and ghosts of the last stage's input into h->primout ([4][ne+ng],
+// slot order)
+int umesh_primitives(tns_handle* h);
+int umesh_node_averages(tns_handle* h, double* dev_out);  // [4][nnode]: P, U, V, T
+int umesh_boundary_sums(tns_handle* h, int type, int side, double* dev_out);
+int umesh_set_injection(tns_handle* h, const double* scale);
+void umesh_release(tns_handle* h);
+}  // namespace tns_rt

@@ -1,0 +1,826 @@
+// tns_unstructured.cu -- the FP64 RK4 iteration on a general quadrilateral mesh (any
+// NOD / NC1..NC4 connectivity), by gather through index arrays.
+//
+// Per iteration (turbnstwod.f90:95-168), every kernel one thread per cell, slot or node:
+//   [dtmin]            global time step (LOCAL=0)
+//   k_u_diss1/2        DT, sensors and Laplacians, then the JST blend (solver_state.f90:70-225)
+//   [k_u_gport]        type-6 port mass flux of the stage input (boundary.f90:168-223)
+//   k_u_prim           primitives and fluxes of every cell and ghost (turbnstwod.f90:204-227,
+//                      boundary.f90:24-327) into a slot field set W
+//   k_u_node_avg       NODAL_AVERAGE with the bc.in-order resets (viscous.f90:40-124), stage 1
+//   k_u_visc           the four faces of every cell (viscous.f90:62-70,130-217), stage 1
+//   k_u_stage          source, residual and update (source_terms.f90:24-104, residual.f90:23-83)
+// the prim -> stage pair once per RK stage.  The host side lays the mesh out: cells in
+// reverse Cuthill-McKee order (neighbours near in memory), ghosts after them in bc.in
+// order, the static geometry computed once with the reference's formulas
+// (geometry.f90:55-149).
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <unordered_map>
+#include <vector>
+
+#include "tns_handle.h"
+#include "tns_umesh.h"
+#include "tns_tile.cuh"
+
+namespace tns {
+
+constexpr int UT = 256;  // threads per block of every kernel here
+
+__device__ __forceinline__ void u_cell_prim(const Params& P, const double* __restrict__ q, int ne, int c,
+                                            Prim& p) {
+    primitive(P, q[c], q[ne + c], q[2 * ne + c], q[3 * ne + c], q[4 * ne + c], p);
+}
+
+// Primitive / flux field set of every slot: cells from the state, ghosts by their BC
+// from the parent and (type 3) the parent's opposite neighbour.
+__global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* __restrict__ q,
+                                               double* __restrict__ W) {
+    const int s = blockIdx.x * UT + threadIdx.x;
+    const int ns = M.ne + M.ng;
+    if (s >= ns) return;
+    Prim p;
+    if (s < M.ne) {
+        u_cell_prim(P, q, M.ne, s, p);
+    } else {
+        const int L = s - M.ne;
+        const int par = M.gpar[L], type = M.gtype[L];
+        Prim pa, op;
+        u_cell_prim(P, q, M.ne, par, pa);
+        if (type == 3) u_cell_prim(P, q, M.ne, M.gopp[L], op);
+        else op = pa;
+        boundary_ghost(P, type, pa, op, M.gsx[L], M.gsy[L], M.gyc[L], M.cg[UCG_YCC * M.ne + par],
+                       type == 6 ? M.gport[L] : 0.0, M.ginj[L], p);
+    }
+    const size_t n = (size_t)ns;
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        W[(UW_F1 + m) * n + s] = p.f[m];
+        W[(UW_G1 + m) * n + s] = p.g[m];
+    }
+    W[UW_U * n + s] = p.u;
+    W[UW_V * n + s] = p.v;
+    W[UW_T * n + s] = p.t;
+    W[UW_P * n + s] = p.p;
+    W[UW_RHO * n + s] = p.rho;
+    W[UW_RI * n + s] = p.ri;
+    W[UW_QM * n + s] = p.qm;
+}
+
+// Port mass flux of each type-6 ghost: the sum of C1*U*DELY (*YCC) along its port line
+// in the line's order (the walk of the oracle's repaired COMPUTE_GPORT).
+__global__ void __launch_bounds__(UT) k_u_gport(Params P, UMesh M, const double* __restrict__ q) {
+    const int k = blockIdx.x * UT + threadIdx.x;
+    if (k >= M.nport) return;
+    double sum = 0.0;
+    for (int e = M.pptr[k]; e < M.pptr[k + 1]; e++) {
+        const int c = M.pcell[e];
+        const double c1 = q[c], u = q[M.ne + c] / c1;
+        double term = c1 * u * M.pdely[e];
+        if (P.iaxis == 1) term = term * M.cg[UCG_YCC * M.ne + c];
+        sum = (e == M.pptr[k]) ? term : sum + term;
+    }
+    M.gport[M.pghost[k]] = sum;
+}
+
+__device__ __forceinline__ double u_pressure(const Params& P, const double* __restrict__ q, int ne, int c) {
+    const double RHO = q[c];
+    const double rr = 1.0 / RHO;
+    const double U = q[ne + c] * rr, V = q[2 * ne + c] * rr;
+    const double E = q[3 * ne + c] * rr;
+    const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
+    return RHO * P.rr * T;
+}
+
+enum UAux { UA_ANU, UA_ANURT, UA_VBD, UA_D2Q, UA_N = UA_D2Q + 5 };
+
+// DISSIPATION, first pass (solver_state.f90:78-160): DT (turbnstwod.f90:97-108), VOL/DT,
+// the pressure and turbulence sensors and the Laplacians; a ghost neighbour holds a
+// copy of its parent (this cell).
+__global__ void __launch_bounds__(UT) k_u_diss1(Params P, UMesh M, const double* __restrict__ q,
+                                                double* __restrict__ aux, double* __restrict__ dt,
+                                                const double* __restrict__ dtmin) {
+    const int I = blockIdx.x * UT + threadIdx.x;
+    const int ne = M.ne;
+    if (I >= ne) return;
+    int nb[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int n = M.nc[k * ne + I];
+        nb[k] = n < ne ? n : I;
+    }
+    const double PIE = u_pressure(P, q, ne, I);
+    double Pn[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) Pn[k] = nb[k] == I ? PIE : u_pressure(P, q, ne, nb[k]);
+    const double* C5 = q + 4 * ne;
+    const double C1I = q[I], C5I = C5[I];
+    double ANUN = fabs(Pn[0] - PIE) + fabs(Pn[1] - PIE) + fabs(Pn[2] - PIE) + fabs(Pn[3] - PIE);
+    double ANUD = fabs(Pn[0] + PIE) + fabs(Pn[1] + PIE) + fabs(Pn[2] + PIE) + fabs(Pn[3] + PIE);
+    aux[UA_ANU * ne + I] = ANUN / ANUD;
+    ANUN = fabs(C5[nb[0]] - C5I) + fabs(C5[nb[1]] - C5I) + fabs(C5[nb[2]] - C5I) + fabs(C5[nb[3]] - C5I);
+    ANUD = fabs(C5[nb[0]] + C5I) + fabs(C5[nb[1]] + C5I) + fabs(C5[nb[2]] + C5I) + fabs(C5[nb[3]] + C5I);
+    aux[UA_ANURT * ne + I] = ANUN / dmax1(ANUD, 8.0 * C1I * P.rtol);
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        const double* Cm = q + m * ne;
+        aux[(UA_D2Q + m) * ne + I] = Cm[nb[0]] + Cm[nb[1]] + Cm[nb[2]] + Cm[nb[3]] - 4.0 * Cm[I];
+    }
+    double DT;
+    if (P.local) {
+        const double RHO = q[I];
+        const double rr = 1.0 / RHO;
+        const double U = q[ne + I] * rr, V = q[2 * ne + I] * rr;
+        const double VEL = sqrt(U * U + V * V);
+        const double E = q[3 * ne + I] * rr;
+        const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
+        DT = M.cfldl[I] / (fabs(VEL) + sqrt(P.gamrr * T));
+        dt[I] = DT;
+    } else {
+        DT = *dtmin;
+    }
+    aux[UA_VBD * ne + I] = M.cg[UCG_VOL * ne + I] / DT;
+}
+
+// DISSIPATION, the blend (solver_state.f90:162-225).  A ghost face contributes exactly
+// zero (its state and Laplacian are the cell's own), so it is skipped.
+__global__ void __launch_bounds__(UT) k_u_diss2(UMesh M, const double* __restrict__ q,
+                                                const double* __restrict__ aux, double* __restrict__ d) {
+    const int I = blockIdx.x * UT + threadIdx.x;
+    const int ne = M.ne;
+    if (I >= ne) return;
+    int nb[4];
+    bool has[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        nb[k] = M.nc[k * ne + I];
+        has[k] = nb[k] < ne;
+        if (!has[k]) nb[k] = I;
+    }
+    const double VOLBYDT = aux[UA_VBD * ne + I];
+    const double ANUI = aux[UA_ANU * ne + I], ANURTI = aux[UA_ANURT * ne + I];
+    double D2c[4], D4c[4], D2t[4], D4t[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double D24N = HALF * (VOLBYDT + aux[UA_VBD * ne + nb[k]]);
+        double E2N = C02 * dmax1(ANUI, aux[UA_ANU * ne + nb[k]]);
+        double E4N = dmax1(0.0, C04 - E2N);
+        D2c[k] = E2N * D24N;
+        D4c[k] = E4N * D24N;
+        E2N = C02 * dmax1(ANURTI, aux[UA_ANURT * ne + nb[k]]);
+        E4N = dmax1(0.0, C04 - E2N);
+        D2t[k] = E2N * D24N;
+        D4t[k] = E4N * D24N;
+    }
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        const double* Cm = q + m * ne;
+        const double* Qm = aux + (UA_D2Q + m) * ne;
+        const double CI = Cm[I], D2I = Qm[I];
+        double D2 = 0.0, D4 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!has[k]) continue;
+            const double a2 = (m == 4) ? D2t[k] : D2c[k];
+            const double a4 = (m == 4) ? D4t[k] : D4c[k];
+            D2 = D2 + a2 * (Cm[nb[k]] - CI);
+            D4 = D4 + a4 * (Qm[nb[k]] - D2I);
+        }
+        d[m * ne + I] = D2 - D4;
+    }
+}
+
+// NODAL_AVERAGE_ELEMENTS / _GHOSTS / finalize (viscous.f90:40-124): each node sums its
+// contributions in the reference's visit order (cells by id, then ghosts in bc.in order),
+// with a type-4 ghost zeroing VN and a type-5 ghost zeroing UN, VN and setting RN after
+// its contribution; out [5][nnode] = U, V, T, RHO, RI averages.
+__global__ void __launch_bounds__(UT) k_u_node_avg(Params P, UMesh M, const double* __restrict__ W,
+                                                   double* __restrict__ na) {
+    const int n = blockIdx.x * UT + threadIdx.x;
+    if (n >= M.nnode) return;
+    const size_t ns = (size_t)M.ne + M.ng;
+    double un = 0.0, vn = 0.0, tn = 0.0, rhon = 0.0, rn = 0.0;
+    const int e0 = M.nptr[n], e1 = M.nptr[n + 1];
+    for (int e = e0; e < e1; e++) {
+        const int s = M.nslot[e];
+        un = un + W[UW_U * ns + s];
+        vn = vn + W[UW_V * ns + s];
+        tn = tn + W[UW_T * ns + s];
+        rhon = rhon + W[UW_RHO * ns + s];
+        rn = rn + W[UW_RI * ns + s];
+        const int r = M.nreset[e];
+        if (r == 4) {
+            vn = 0.0;
+        } else if (r == 5) {
+            un = 0.0;
+            vn = 0.0;
+            rn = P.rtol_rtred;
+        }
+    }
+    const double DF = (double)(e1 - e0);
+    const size_t nn = (size_t)M.nnode;
+    na[n] = un / DF;
+    na[nn + n] = vn / DF;
+    na[2 * nn + n] = tn / DF;
+    na[3 * nn + n] = rhon / DF;
+    na[4 * nn + n] = dmax1(P.rtol, rn / DF);
+}
+
+// COMPUTE_VISCOUS face loop (viscous.f90:62-70): faces 1..4 of every cell in its own
+// orientation, face 1 assigning and the others adding.
+__global__ void __launch_bounds__(UT) k_u_visc(Params P, UMesh M, const double* __restrict__ W,
+                                               const double* __restrict__ na, double* __restrict__ vis) {
+    const int I = blockIdx.x * UT + threadIdx.x;
+    const int ne = M.ne;
+    if (I >= ne) return;
+    const size_t ns = (size_t)ne + M.ng, nn = (size_t)M.nnode;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int k = 0; k < 4; k++) {
+        const int nbn = M.nod[k * ne + I], ndn = M.nod[((k + 1) & 3) * ne + I];
+        const int cc = M.nc[k * ne + I];
+        FaceVals f;
+        f.ua = W[UW_U * ns + I]; f.va = W[UW_V * ns + I]; f.ta = W[UW_T * ns + I];
+        f.uc = W[UW_U * ns + cc]; f.vc = W[UW_V * ns + cc]; f.tc = W[UW_T * ns + cc];
+        f.ub = na[nbn]; f.vb = na[nn + nbn]; f.tb = na[2 * nn + nbn];
+        f.ud = na[ndn]; f.vd = na[nn + ndn]; f.td = na[2 * nn + ndn];
+        f.rhoa = W[UW_RHO * ns + I]; f.rhoc = W[UW_RHO * ns + cc];
+        f.rhob = na[3 * nn + nbn]; f.rhod = na[3 * nn + ndn];
+        f.ra = W[UW_RI * ns + I]; f.rc = W[UW_RI * ns + cc];
+        f.rb = na[4 * nn + nbn]; f.rd = na[4 * nn + ndn];
+        const double* G = M.fg + (size_t)k * ne + I;
+        const size_t st = (size_t)4 * ne;
+        double out[4];
+        viscous_face(P, f, M.cg[(UCG_SX1 + k) * ne + I], M.cg[(UCG_SY1 + k) * ne + I], G[UFG_GA * st],
+                     G[UFG_GB * st], G[UFG_GC * st], G[UFG_GD * st],
+                     P.iaxis == 1 ? G[UFG_RYAVG * st] : 0.0, out);
+#pragma unroll
+        for (int m = 0; m < 4; m++) acc[m] = k == 0 ? out[m] : acc[m] + out[m];
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) vis[m * ne + I] = acc[m];
+}
+
+// One RK stage of every cell: source terms, flux residual, update (source_terms.f90:24-104,
+// residual.f90:23-83), with the CDIFF reduction and the finite check where asked.
+__global__ void __launch_bounds__(UT) k_u_stage(Params P, UMesh M, StageArgsU A) {
+    const int I = blockIdx.x * UT + threadIdx.x;
+    const int ne = M.ne;
+    const size_t ns = (size_t)ne + M.ng;
+    const double* W = A.W;
+    double dv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (I < ne) {
+        int nb[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) nb[k] = M.nc[k * ne + I];
+        const double* G = M.cg + I;
+        double src3, src5;
+        {
+            SrcIn s;
+            s.ga = G[UCG_GA * ne]; s.gb = G[UCG_GB * ne]; s.gc = G[UCG_GC * ne]; s.gd = G[UCG_GD * ne];
+            s.ua = W[UW_U * ns + nb[0]]; s.ub = W[UW_U * ns + nb[1]];
+            s.uc = W[UW_U * ns + nb[2]]; s.ud = W[UW_U * ns + nb[3]];
+            s.va = W[UW_V * ns + nb[0]]; s.vb = W[UW_V * ns + nb[1]];
+            s.vc = W[UW_V * ns + nb[2]]; s.vd = W[UW_V * ns + nb[3]];
+            s.ra = W[UW_RI * ns + nb[0]]; s.rb = W[UW_RI * ns + nb[1]];
+            s.rc = W[UW_RI * ns + nb[2]]; s.rd = W[UW_RI * ns + nb[3]];
+            s.qa = W[UW_QM * ns + nb[0]]; s.qb = W[UW_QM * ns + nb[1]];
+            s.qc = W[UW_QM * ns + nb[2]]; s.qd = W[UW_QM * ns + nb[3]];
+            source_terms(P, s, W[UW_RHO * ns + I], W[UW_RI * ns + I], W[UW_T * ns + I], W[UW_P * ns + I],
+                         W[UW_V * ns + I], G[UCG_YCC * ne], G[UCG_RYCC * ne], src3, src5);
+        }
+        double R[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            const double* F = W + (UW_F1 + m) * ns;
+            const double* Gm = W + (UW_G1 + m) * ns;
+            const double FI = F[I], GI = Gm[I];
+            R[m] = HALF * ((FI + F[nb[0]]) * G[UCG_SX1 * ne] + (GI + Gm[nb[0]]) * G[UCG_SY1 * ne] +
+                           (FI + F[nb[1]]) * G[UCG_SX2 * ne] + (GI + Gm[nb[1]]) * G[UCG_SY2 * ne] +
+                           (FI + F[nb[2]]) * G[UCG_SX3 * ne] + (GI + Gm[nb[2]]) * G[UCG_SY3 * ne] +
+                           (FI + F[nb[3]]) * G[UCG_SX4 * ne] + (GI + Gm[nb[3]]) * G[UCG_SY4 * ne]);
+        }
+        const double VOL = G[UCG_VOL * ne];
+        R[4] = R[4] - VOL * src5;
+        if (P.iaxis == 1) R[2] = R[2] - VOL * src3;
+        const double DT = P.local ? A.dt[I] : *A.dtmin;
+        const double DTBYVOL = DT * G[UCG_RVOL * ne];
+        const double al = A.alpha;
+        double Cn[5], Co[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) Co[m] = A.qold[m * ne + I];
+        Cn[0] = Co[0] - al * DTBYVOL * (R[0] - A.d[I]);
+        Cn[1] = Co[1] - al * DTBYVOL * (R[1] - A.vis[I] - A.d[ne + I]);
+        Cn[2] = Co[2] - al * DTBYVOL * (R[2] - A.vis[ne + I] - A.d[2 * ne + I]);
+        Cn[3] = Co[3] - al * DTBYVOL * (R[3] - A.vis[2 * ne + I] - A.d[3 * ne + I]);
+        Cn[4] = Co[4] - al * DTBYVOL * CFLTURB * (R[4] - A.vis[3 * ne + I] - A.d[4 * ne + I]);
+        Cn[4] = Cn[0] * dmax1(P.rtol, Cn[4] / Cn[0]);
+#pragma unroll
+        for (int m = 0; m < 5; m++) A.qout[m * ne + I] = Cn[m];
+        if (A.status) {
+            bool bad = false;
+#pragma unroll
+            for (int m = 0; m < 5; m++) bad |= !isfinite(Cn[m]);
+            if (bad) atomicOr(A.status, 1u);
+        }
+#pragma unroll
+        for (int m = 0; m < 5; m++) dv[m] = fabs(Co[m] - Cn[m]);
+    }
+    if (A.cdiff) {
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            double v = dv[m];
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if ((threadIdx.x & 31) == 0) atomicMax(&A.cdiff[m], (unsigned long long)__double_as_longlong(v));
+        }
+    }
+}
+
+// POSTPROCESS node averages (solver_state.f90:237-281): P, U, V, T of the contributions
+// in the same visit order, divided by their count; out [4][nnode].
+__global__ void __launch_bounds__(UT) k_u_post_avg(UMesh M, const double* __restrict__ W,
+                                                   double* __restrict__ out) {
+    const int n = blockIdx.x * UT + threadIdx.x;
+    if (n >= M.nnode) return;
+    const size_t ns = (size_t)M.ne + M.ng, nn = (size_t)M.nnode;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    const int e0 = M.nptr[n], e1 = M.nptr[n + 1];
+    for (int e = e0; e < e1; e++) {
+        const int sl = M.nslot[e];
+        s[0] += W[UW_P * ns + sl];
+        s[1] += W[UW_U * ns + sl];
+        s[2] += W[UW_V * ns + sl];
+        s[3] += W[UW_T * ns + sl];
+    }
+    const double d = (double)(e1 - e0);
+#pragma unroll
+    for (int f = 0; f < 4; f++) out[f * nn + n] = s[f] / d;
+}
+
+__global__ void __launch_bounds__(UT) k_u_prim_out(UMesh M, const double* __restrict__ W,
+                                                   double* __restrict__ out) {
+    const int s = blockIdx.x * UT + threadIdx.x;
+    const size_t ns = (size_t)M.ne + M.ng;
+    if (s >= (int)ns) return;
+    out[s] = W[UW_U * ns + s];
+    out[ns + s] = W[UW_V * ns + s];
+    out[2 * ns + s] = W[UW_T * ns + s];
+    out[3 * ns + s] = W[UW_P * ns + s];
+}
+
+// Boundary-face sums over the ghosts whose BC type / side match (0 = any), with the face
+// state (parent + ghost)/2, as k_boundary_sums.
+__global__ void __launch_bounds__(UT) k_u_bsums(Params P, UMesh M, const double* __restrict__ W, int type,
+                                                int side, double* __restrict__ out) {
+    const int L = blockIdx.x * UT + threadIdx.x;
+    const size_t ns = (size_t)M.ne + M.ng;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (L < M.ng && (type == 0 || M.gtype[L] == type) && (side == 0 || M.gside[L] == side)) {
+        const size_t cp = (size_t)M.gpar[L], cg = (size_t)M.ne + L;
+        const double sx = M.gsx[L], sy = M.gsy[L];
+        const double u = 0.5 * (W[UW_U * ns + cp] + W[UW_U * ns + cg]);
+        const double vv = 0.5 * (W[UW_V * ns + cp] + W[UW_V * ns + cg]);
+        const double tp = W[UW_T * ns + cp], tg = W[UW_T * ns + cg];
+        const double pp = W[UW_P * ns + cp], pg = W[UW_P * ns + cg];
+        const double pf = 0.5 * (pp + pg);
+        const double rho = 0.5 * (pp / (P.rr * tp) + pg / (P.rr * tg));
+        v[0] = pf * sx;
+        v[1] = pf * sy;
+        v[2] = rho * (u * sx + vv * sy);
+        v[3] = sqrt(sx * sx + sy * sy);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x != 0.0) atomicAdd(&out[q], x);
+    }
+}
+
+static unsigned blocks(long long n) { return (unsigned)((n + UT - 1) / UT); }
+
+void launch_u_prim(const Params& P, const UMesh& M, const double* q, double* W, cudaStream_t s) {
+    k_u_prim<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(P, M, q, W);
+}
+void launch_u_gport(const Params& P, const UMesh& M, const double* q, cudaStream_t s) {
+    if (M.nport > 0) k_u_gport<<<blocks(M.nport), UT, 0, s>>>(P, M, q);
+}
+void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, double* d,
+                          double* dt, const double* dtmin, cudaStream_t s) {
+    k_u_diss1<<<blocks(M.ne), UT, 0, s>>>(P, M, q, aux, dt, dtmin);
+    k_u_diss2<<<blocks(M.ne), UT, 0, s>>>(M, q, aux, d);
+}
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vis,
+                      cudaStream_t s) {
+    k_u_node_avg<<<blocks(M.nnode), UT, 0, s>>>(P, M, W, na);
+    k_u_visc<<<blocks(M.ne), UT, 0, s>>>(P, M, W, na, vis);
+}
+void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s) {
+    k_u_stage<<<blocks(M.ne), UT, 0, s>>>(P, M, A);
+}
+void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s) {
+    k_u_post_avg<<<blocks(M.nnode), UT, 0, s>>>(M, W, out);
+}
+void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_t s) {
+    k_u_prim_out<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(M, W, out);
+}
+void launch_u_boundary_sums(const Params& P, const UMesh& M, const double* W, int type, int side,
+                            double* out, cudaStream_t s) {
+    if (M.ng > 0) k_u_bsums<<<blocks(M.ng), UT, 0, s>>>(P, M, W, type, side, out);
+}
+
+}  // namespace tns
+
+// ------------------------------------------------------------------ host runtime
+
+struct tns_umesh_state {
+    tns::UMesh M{};
+    DevBuf<int> nc, nod, gpar, gopp, gtype, gside, nptr, nslot, nreset, pghost, pptr, pcell;
+    DevBuf<double> cg, fg, cfldl, gsx, gsy, gyc, ginj, gport, pdely, W, aux, na;
+    // host layout, uploaded by umesh_upload
+    std::vector<int> hnc, hnod, hgpar, hgopp, hgtype, hgside, hnptr, hnslot, hnreset, hpghost, hpptr, hpcell;
+    std::vector<double> hcg, hfg, hcfldl, hgsx, hgsy, hgyc, hginj, hpdely;
+};
+
+namespace tns_rt {
+
+namespace {
+
+// Reverse Cuthill-McKee order of the cells over the cell-to-cell adjacency of NC1..NC4:
+// breadth-first from a least-connected cell of each component, neighbours by ascending
+// degree, the whole order reversed.  Returns new index -> cell.
+std::vector<int> rcm_order(int ne, const std::vector<int>& adj /* [ne][4], -1 = none */) {
+    std::vector<int> deg(ne, 0);
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) deg[c] += adj[4 * c + k] >= 0;
+    std::vector<int> by_deg(ne);
+    std::iota(by_deg.begin(), by_deg.end(), 0);
+    std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    std::vector<char> seen(ne, 0);
+    std::vector<int> order;
+    order.reserve(ne);
+    for (int start : by_deg) {
+        if (seen[start]) continue;
+        size_t head = order.size();
+        order.push_back(start);
+        seen[start] = 1;
+        while (head < order.size()) {
+            const int c = order[head++];
+            int nb[4], n = 0;
+            for (int k = 0; k < 4; k++) {
+                const int v = adj[4 * c + k];
+                if (v >= 0 && !seen[v]) nb[n++] = v;
+            }
+            std::sort(nb, nb + n, [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+            for (int k = 0; k < n; k++) {
+                if (seen[nb[k]]) continue;
+                seen[nb[k]] = 1;
+                order.push_back(nb[k]);
+            }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+}  // namespace
+
+int umesh_build(tns_handle* h, const tns_mesh* m) {
+    using namespace tns;
+    const int ne = m->neles, ng = m->nghosts, nn = m->nods;
+    const int* ncs[4] = {m->nc1, m->nc2, m->nc3, m->nc4};
+    auto NOD = [&](int c, int k) { return m->nod[(size_t)k * m->ld_nod + c] - 1; };
+    std::unordered_map<int, int> line_of;
+    line_of.reserve((size_t)ng * 2 + 1);
+    int maxid = ne;
+    for (int L = 0; L < ng; L++) {
+        line_of.emplace(m->nghost[L], L);
+        maxid = std::max(maxid, m->nghost[L]);
+    }
+    // every cell face has a cell or a ghost behind it (checked by build_mesh); reject
+    // what this layout cannot express
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) {
+            const int v = ncs[k][c];
+            if (!(v >= 1 && v <= ne) && !line_of.count(v))
+                return h->fail(TNS_ERR_MESH, "cell %d face %d: neighbour %d is neither a cell nor a ghost", c + 1,
+                               k + 1, v);
+        }
+    std::vector<int> adj((size_t)4 * ne, -1);
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) {
+            const int v = ncs[k][c];
+            if (v >= 1 && v <= ne) adj[4 * (size_t)c + k] = v - 1;
+        }
+    std::vector<int> cell_of = rcm_order(ne, adj), new_of(ne);
+    for (int k = 0; k < ne; k++) new_of[cell_of[k]] = k;
+
+    tns_umesh_state* u = new tns_umesh_state();
+    h->umesh = u;
+    auto slot = [&](int v) { return (v >= 1 && v <= ne) ? new_of[v - 1] : ne + line_of.at(v); };
+    const int iaxis = h->P.iaxis;
+    // geometry of the cells in original numbering (geometry.f90:55-105)
+    std::vector<double> xcc(ne), ycc(ne), vol(ne), dl(ne), sx((size_t)4 * ne), sy((size_t)4 * ne);
+    for (int c = 0; c < ne; c++) {
+        double X[4], Y[4];
+        for (int k = 0; k < 4; k++) {
+            const int n = NOD(c, k);
+            X[k] = m->x[n];
+            Y[k] = m->y[n];
+            if (!std::isfinite(X[k]) || !std::isfinite(Y[k]))
+                return h->fail(TNS_ERR_MESH, "cell %d has a non-finite node coordinate", c + 1);
+        }
+        xcc[c] = (X[0] + X[1] + X[2] + X[3]) * 0.25;
+        ycc[c] = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
+        const double DL12 = std::sqrt((X[0] - X[1]) * (X[0] - X[1]) + (Y[0] - Y[1]) * (Y[0] - Y[1]));
+        const double DL23 = std::sqrt((X[1] - X[2]) * (X[1] - X[2]) + (Y[1] - Y[2]) * (Y[1] - Y[2]));
+        const double DL34 = std::sqrt((X[2] - X[3]) * (X[2] - X[3]) + (Y[2] - Y[3]) * (Y[2] - Y[3]));
+        const double DL41 = std::sqrt((X[3] - X[0]) * (X[3] - X[0]) + (Y[3] - Y[0]) * (Y[3] - Y[0]));
+        dl[c] = std::min(std::min(std::min(DL12, DL23), DL34), DL41);
+        for (int k = 0; k < 4; k++) face_vector(iaxis, k + 1, X, Y, sx[4 * (size_t)c + k], sy[4 * (size_t)c + k]);
+        double v = HALF * ((X[2] - X[0]) * (Y[3] - Y[1]) - (X[3] - X[1]) * (Y[2] - Y[0]));
+        if (iaxis == 1) v = v * ycc[c];
+        if (v == 0.0) return h->fail(TNS_ERR_MESH, "cell %d has zero volume (collapsed or on the axis)", c + 1);
+        vol[c] = v < 0.0 ? -v : v;
+    }
+    // mirrored ghost centroids (geometry.f90:107-149)
+    std::vector<double> gxc(ng), gyc(ng);
+    for (int L = 0; L < ng; L++) {
+        const int p = m->nparent[L] - 1, s = m->nside[L];
+        const int na = NOD(p, s - 1), nb = NOD(p, s & 3);
+        const double xf = HALF * (m->x[na] + m->x[nb]), yf = HALF * (m->y[na] + m->y[nb]);
+        gxc[L] = 2.0 * xf - xcc[p];
+        gyc[L] = 2.0 * yf - ycc[p];
+    }
+    auto centroid = [&](int v, double& x, double& y) {  // a Fortran id: cell or ghost
+        if (v >= 1 && v <= ne) { x = xcc[v - 1]; y = ycc[v - 1]; }
+        else { const int L = line_of.at(v); x = gxc[L]; y = gyc[L]; }
+    };
+    auto grad = [](double xa, double ya, double xb, double yb, double xc, double yc, double xd, double yd,
+                   double* out, size_t stride) {
+        const double ybd = yb - yd, yac = ya - yc, xbd = xb - xd, xac = xa - xc;
+        const double iDNR = 1.0 / (xac * ybd - xbd * yac);
+        out[0] = ybd * iDNR;
+        out[stride] = -yac * iDNR;
+        out[2 * stride] = -xbd * iDNR;
+        out[3 * stride] = xac * iDNR;
+    };
+    u->hnc.assign((size_t)4 * ne, 0);
+    u->hnod.assign((size_t)4 * ne, 0);
+    u->hcg.assign((size_t)UCG_N * ne, 0.0);
+    u->hfg.assign((size_t)UFG_N * 4 * ne, 0.0);
+    u->hcfldl.assign(ne, 0.0);
+    for (int k = 0; k < ne; k++) {
+        const int c = cell_of[k];
+        for (int f = 0; f < 4; f++) {
+            u->hnc[(size_t)f * ne + k] = slot(ncs[f][c]);
+            u->hnod[(size_t)f * ne + k] = NOD(c, f);
+            u->hcg[(size_t)(UCG_SX1 + f) * ne + k] = sx[4 * (size_t)c + f];
+            u->hcg[(size_t)(UCG_SY1 + f) * ne + k] = sy[4 * (size_t)c + f];
+        }
+        double xa, ya, xb, yb, xc, yc, xd, yd;
+        centroid(ncs[0][c], xa, ya);
+        centroid(ncs[1][c], xb, yb);
+        centroid(ncs[2][c], xc, yc);
+        centroid(ncs[3][c], xd, yd);
+        grad(xa, ya, xb, yb, xc, yc, xd, yd, &u->hcg[(size_t)UCG_GA * ne + k], ne);
+        u->hcg[(size_t)UCG_VOL * ne + k] = vol[c];
+        u->hcg[(size_t)UCG_RVOL * ne + k] = 1.0 / vol[c];
+        u->hcg[(size_t)UCG_YCC * ne + k] = ycc[c];
+        u->hcg[(size_t)UCG_RYCC * ne + k] = 1.0 / ycc[c];
+        u->hcfldl[k] = h->P.cfl * dl[c];
+        // faces for the viscous flux: A = the cell, C = NC_f, B = N_f, D = N_f+1
+        for (int f = 0; f < 4; f++) {
+            double xcn, ycn;
+            centroid(ncs[f][c], xcn, ycn);
+            const int nb = NOD(c, f), nd = NOD(c, (f + 1) & 3);
+            const size_t st = (size_t)4 * ne, at = (size_t)f * ne + k;
+            grad(xcc[c], ycc[c], m->x[nb], m->y[nb], xcn, ycn, m->x[nd], m->y[nd], &u->hfg[UFG_GA * st + at], st);
+            const double yavg = HALF * (m->y[nb] + m->y[nd]);
+            u->hfg[UFG_RYAVG * st + at] = (iaxis == 1 && !(yavg < YAXIS_THRESH)) ? 1.0 / yavg : 0.0;
+        }
+    }
+    // ghosts in bc.in order
+    static const int OPP[5] = {0, 3, 4, 1, 2};  // side -> the opposite face
+    u->hgpar.assign(ng, 0); u->hgopp.assign(ng, 0); u->hgtype.assign(ng, 0); u->hgside.assign(ng, 0);
+    u->hgsx.assign(ng, 0.0); u->hgsy.assign(ng, 0.0); u->hgyc.assign(ng, 0.0); u->hginj.assign(ng, 1.0);
+    for (int L = 0; L < ng; L++) {
+        const int p = m->nparent[L] - 1, s = m->nside[L], ty = m->ntype[L];
+        u->hgpar[L] = new_of[p];
+        u->hgtype[L] = ty;
+        u->hgside[L] = s;
+        u->hgsx[L] = sx[4 * (size_t)p + s - 1];
+        u->hgsy[L] = sy[4 * (size_t)p + s - 1];
+        u->hgyc[L] = gyc[L];
+        const int o = ncs[OPP[s] - 1][p];
+        if (ty == 3 && !(o >= 1 && o <= ne))
+            return h->fail(TNS_ERR_UNSUPPORTED,
+                           "bc.in line %d: type-3 ghost whose parent %d has no cell across the opposite face", L + 1,
+                           p + 1);
+        u->hgopp[L] = (o >= 1 && o <= ne) ? new_of[o - 1] : new_of[p];
+    }
+    // node contributions in the reference's visit order (viscous.f90:77-124,
+    // solver_state.f90:237-262): cells by id, then the ghosts in bc.in order
+    std::vector<int> cnt(nn, 0);
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) cnt[NOD(c, k)]++;
+    for (int L = 0; L < ng; L++) {
+        const int p = m->nparent[L] - 1, s = m->nside[L];
+        cnt[NOD(p, s - 1)]++;
+        cnt[NOD(p, s & 3)]++;
+    }
+    u->hnptr.assign(nn + 1, 0);
+    for (int n = 0; n < nn; n++) u->hnptr[n + 1] = u->hnptr[n] + cnt[n];
+    for (int n = 0; n < nn; n++)
+        if (cnt[n] == 0) return h->fail(TNS_ERR_MESH, "node %d belongs to no cell", n + 1);
+    u->hnslot.assign(u->hnptr[nn], 0);
+    u->hnreset.assign(u->hnptr[nn], 0);
+    std::vector<int> fill(u->hnptr.begin(), u->hnptr.end() - 1);
+    for (int c = 0; c < ne; c++)
+        for (int k = 0; k < 4; k++) {
+            const int n = NOD(c, k);
+            u->hnslot[fill[n]++] = new_of[c];
+        }
+    for (int L = 0; L < ng; L++) {
+        const int p = m->nparent[L] - 1, s = m->nside[L], ty = m->ntype[L];
+        for (int n : {NOD(p, s - 1), NOD(p, s & 3)}) {
+            u->hnreset[fill[n]] = (ty == 4 || ty == 5) ? ty : 0;
+            u->hnslot[fill[n]++] = ne + L;
+        }
+    }
+    // port lines of the type-6 ghosts: from the parent straight across the mesh through
+    // the face opposite NSIDE until a ghost is reached
+    u->hpptr.assign(1, 0);
+    for (int L = 0; L < ng; L++) {
+        if (m->ntype[L] != 6) continue;
+        const int s = m->nside[L];
+        int v = m->nparent[L], steps = 0;
+        while (v >= 1 && v <= ne && steps <= ne) {
+            const int c = v - 1;
+            double Y[4];
+            for (int k = 0; k < 4; k++) Y[k] = m->y[NOD(c, k)];
+            double dely;  // boundary.f90:183-214
+            if (s == 1) dely = HALF * ((Y[0] + Y[1]) - (Y[2] + Y[3]));
+            else if (s == 2) dely = HALF * ((Y[1] + Y[2]) - (Y[0] + Y[3]));
+            else if (s == 3) dely = HALF * ((Y[2] + Y[3]) - (Y[0] + Y[1]));
+            else dely = HALF * ((Y[3] + Y[0]) - (Y[1] + Y[2]));
+            u->hpcell.push_back(new_of[c]);
+            u->hpdely.push_back(dely);
+            v = ncs[OPP[s] - 1][c];
+            steps++;
+        }
+        u->hpghost.push_back(L);
+        u->hpptr.push_back((int)u->hpcell.size());
+    }
+    h->ni = ne;
+    h->nj = 1;
+    h->neles = ne;
+    h->nods = nn;
+    h->nghosts = ng;
+    h->maxid = maxid;
+    h->unstructured = true;
+    h->identity = true;
+    for (int k = 0; k < ne; k++)
+        if (cell_of[k] != k) { h->identity = false; break; }
+    h->cell_of.swap(cell_of);
+    h->ghost_line.resize(ng);
+    std::iota(h->ghost_line.begin(), h->ghost_line.end(), 0);
+    h->ghost_id.assign(m->nghost, m->nghost + ng);
+    h->node_of.resize(nn);
+    std::iota(h->node_of.begin(), h->node_of.end(), 1);
+    h->M = Mesh{};
+    h->M.ni = ne;
+    h->M.nj = 1;
+    return TNS_OK;
+}
+
+int umesh_upload(tns_handle* h) {
+    tns_umesh_state* u = h->umesh;
+    int rc;
+    auto upi = [&](DevBuf<int>& b, const std::vector<int>& v) {
+        int r = h->cuda(b.alloc(v.size()), "cudaMalloc");
+        if (!r && !v.empty()) r = h->cuda(cudaMemcpy(b.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+        return r;
+    };
+    auto upd = [&](DevBuf<double>& b, const std::vector<double>& v) {
+        int r = h->cuda(b.alloc(v.size()), "cudaMalloc");
+        if (!r && !v.empty()) r = h->cuda(cudaMemcpy(b.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        return r;
+    };
+    const int ne = h->neles, ng = h->nghosts, nn = h->nods;
+    if ((rc = upi(u->nc, u->hnc)) || (rc = upi(u->nod, u->hnod)) || (rc = upi(u->gpar, u->hgpar)) ||
+        (rc = upi(u->gopp, u->hgopp)) || (rc = upi(u->gtype, u->hgtype)) || (rc = upi(u->gside, u->hgside)) ||
+        (rc = upi(u->nptr, u->hnptr)) || (rc = upi(u->nslot, u->hnslot)) || (rc = upi(u->nreset, u->hnreset)) ||
+        (rc = upi(u->pghost, u->hpghost)) || (rc = upi(u->pptr, u->hpptr)) || (rc = upi(u->pcell, u->hpcell)) ||
+        (rc = upd(u->cg, u->hcg)) || (rc = upd(u->fg, u->hfg)) || (rc = upd(u->cfldl, u->hcfldl)) ||
+        (rc = upd(u->gsx, u->hgsx)) || (rc = upd(u->gsy, u->hgsy)) || (rc = upd(u->gyc, u->hgyc)) ||
+        (rc = upd(u->ginj, u->hginj)) || (rc = upd(u->pdely, u->hpdely)))
+        return rc;
+    if ((rc = h->cuda(u->gport.alloc(ng), "cudaMalloc")) ||
+        (rc = h->cuda(u->W.alloc((size_t)tns::UW_N * ((size_t)ne + ng)), "cudaMalloc")) ||
+        (rc = h->cuda(u->aux.alloc((size_t)tns::UA_N * ne), "cudaMalloc")) ||
+        (rc = h->cuda(u->na.alloc((size_t)5 * nn), "cudaMalloc")) ||
+        (rc = h->cuda(cudaMemset(u->gport.p, 0, std::max(ng, 1) * 8), "cudaMemset")))
+        return rc;
+    tns::UMesh& M = u->M;
+    M.ne = ne; M.ng = ng; M.nnode = nn; M.nport = (int)u->hpghost.size();
+    M.nc = u->nc.p; M.nod = u->nod.p; M.cg = u->cg.p; M.fg = u->fg.p; M.cfldl = u->cfldl.p;
+    M.gpar = u->gpar.p; M.gopp = u->gopp.p; M.gtype = u->gtype.p; M.gside = u->gside.p;
+    M.gsx = u->gsx.p; M.gsy = u->gsy.p; M.gyc = u->gyc.p; M.ginj = u->ginj.p; M.gport = u->gport.p;
+    M.nptr = u->nptr.p; M.nslot = u->nslot.p; M.nreset = u->nreset.p;
+    M.pghost = u->pghost.p; M.pptr = u->pptr.p; M.pcell = u->pcell.p; M.pdely = u->pdely.p;
+    // the time-step kernels read CFL*DL through the structured view
+    h->M.cfldl = u->cfldl.p;
+    for (auto* v : {&u->hnc, &u->hnod, &u->hgpar, &u->hgopp, &u->hgside, &u->hnptr, &u->hnslot, &u->hnreset,
+                    &u->hpghost, &u->hpptr, &u->hpcell})
+        std::vector<int>().swap(*v);
+    for (auto* v : {&u->hcg, &u->hfg, &u->hcfldl, &u->hgsx, &u->hgsy, &u->hgyc, &u->hpdely})
+        std::vector<double>().swap(*v);
+    return TNS_OK;
+}
+
+// One FP64 RK4 iteration (turbnstwod.f90:97-168) in the buffers of the structured path:
+// A = state, B / C = stage scratch, D, VIS, DT.
+void enqueue_iteration_u(tns_handle* h, bool monitor) {
+    const tns::Params& P = h->P;
+    tns_umesh_state* u = h->umesh;
+    const tns::UMesh& M = u->M;
+    cudaStream_t s = h->stream;
+    double *A = h->qa.p, *B = h->qb.p, *Cq = h->qc.p;
+    static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
+    const double* in[4] = {A, B, Cq, B};
+    double* out[4] = {B, Cq, B, A};
+    if (!P.local) {
+        tns::launch_time_step_scratch(P, A, M.cfldl, M.ne, h->dt.p, h->partial.p, h->counter.p, h->dtmin.p,
+                                      tns::dtmin_blocks(h->M), s);
+        h->launches++;
+    }
+    tns::launch_u_dissipation(P, M, A, u->aux.p, h->d.p, h->dt.p, h->dtmin.p, s);
+    h->launches += 2;
+    if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
+    for (int st = 0; st < 4; st++) {
+        if (M.nport) {
+            tns::launch_u_gport(P, M, in[st], s);
+            h->launches++;
+        }
+        tns::launch_u_prim(P, M, in[st], u->W.p, s);
+        h->launches++;
+        if (st == 0) {
+            tns::launch_u_viscous(P, M, u->W.p, u->na.p, h->vis.p, s);
+            h->launches += 2;
+        }
+        tns::StageArgsU S{u->W.p, A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p, alpha[st],
+                          (monitor && st == 3) ? h->cdiff.p : nullptr, st == 3 ? h->status.p : nullptr};
+        tns::launch_u_stage(P, M, S, s);
+        h->launches++;
+    }
+}
+
+int umesh_primitives(tns_handle* h) {
+    tns_umesh_state* u = h->umesh;
+    const size_t nt = (size_t)h->neles + h->nghosts;
+    int rc;
+    if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
+    // the last stage read B: its primitives and ghosts again from B
+    tns::launch_u_gport(h->P, u->M, h->qb.p, h->stream);
+    tns::launch_u_prim(h->P, u->M, h->qb.p, u->W.p, h->stream);
+    tns::launch_u_prim_out(u->M, u->W.p, h->primout.p, h->stream);
+    return h->cuda(cudaGetLastError(), "kernel launch");
+}
+
+int umesh_node_averages(tns_handle* h, double* dev_out) {
+    tns_umesh_state* u = h->umesh;
+    int rc;
+    if ((rc = umesh_primitives(h))) return rc;
+    tns::launch_u_post_average(u->M, u->W.p, dev_out, h->stream);
+    return h->cuda(cudaGetLastError(), "kernel launch");
+}
+
+int umesh_boundary_sums(tns_handle* h, int type, int side, double* dev_out) {
+    tns_umesh_state* u = h->umesh;
+    int rc;
+    if ((rc = umesh_primitives(h))) return rc;
+    tns::launch_u_boundary_sums(h->P, u->M, u->W.p, type, side, dev_out, h->stream);
+    return h->cuda(cudaGetLastError(), "kernel launch");
+}
+
+int umesh_set_injection(tns_handle* h, const double* scale) {
+    tns_umesh_state* u = h->umesh;
+    return h->cuda(cudaMemcpy(u->ginj.p, scale, (size_t)h->nghosts * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+void umesh_release(tns_handle* h) {
+    tns_umesh_state* u = h->umesh;
+    if (!u) return;
+    for (auto* b : {&u->nc, &u->nod, &u->gpar, &u->gopp, &u->gtype, &u->gside, &u->nptr, &u->nslot, &u->nreset,
+                    &u->pghost, &u->pptr, &u->pcell})
+        b->release();
+    for (auto* b : {&u->cg, &u->fg, &u->cfldl, &u->gsx, &u->gsy, &u->gyc, &u->ginj, &u->gport, &u->pdely, &u->W,
+                    &u->aux, &u->na})
+        b->release();
+    delete u;
+    h->umesh = nullptr;
+}
+
+}  // namespace tns_rt

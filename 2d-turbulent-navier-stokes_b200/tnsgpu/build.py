@@ -6,7 +6,8 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
-SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu", "tns_batch_api.cu", "tns_adjoint.cu")
+SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu", "tns_batch_api.cu", "tns_adjoint.cu",
+           "tns_unstructured.cu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 # the mixed-precision kernels: FP32 division and square root to 2 ulp and FP32

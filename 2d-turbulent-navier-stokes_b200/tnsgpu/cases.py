@@ -1,6 +1,6 @@
-"""Structured quadrilateral meshes and flow cases for the solver.
+"""Quadrilateral meshes and flow cases for the solver.
 
-Every mesh is one i x j block numbered the way the reference's grid generators number
+Every mesh but ``multiblock_mesh``'s is one i x j block numbered the way the reference's grid generators number
 theirs (utils/gridgen/ramp.f90:53-63, examples/case1/grid.in): node (i, j) has id
 ``i*(NJ+1) + j + 1``, cell (i, j) has id ``i*NJ + j + 1`` (j fastest), and cell (i, j)
 has nodes N1=(i,j), N2=(i+1,j), N3=(i+1,j+1), N4=(i,j+1) -- faces 1..4 are the j-,
@@ -23,6 +23,8 @@ Cases (sizes as named in the solver's benchmark configurations):
                  reference's example case (axis 4 / wall 5 / inlet 2 / outflow 3).
   ramp_sweep  -- a seeded parameter sweep of ramp cases (mesh size, ramp angle, P0,
                  T0) for the batched solver.
+  backstep    -- a general (multi-block) mesh: a 2-D backward-facing step of three
+                 blocks, one of them numbered from another corner (``multiblock_mesh``).
 """
 from __future__ import annotations
 
@@ -195,6 +197,96 @@ def nozzle_2d_mesh(nx: int = 115, ny: int = 50, beta: float = 2.0) -> Mesh:
 
 
 # ---------------------------------------------------------------- flow settings
+
+def multiblock_mesh(blocks, bc_type: Callable[[float, float], int], rotate=None) -> Mesh:
+    """A general quadrilateral mesh from several structured blocks of nodes.
+
+    ``blocks`` are (xn_mm, yn_mm) node arrays of shape (NI+1, NJ+1), each oriented like
+    ``structured_mesh`` (cell (i, j) has nodes (i,j), (i+1,j), (i+1,j+1), (i,j+1), counter-
+    clockwise).  Nodes with equal coordinates are one node, so blocks join where their
+    node rows coincide.  Cells are numbered block by block (j fastest); ``rotate[b]``
+    shifts the local node order of block b's cells cyclically (its faces 1..4 start at
+    another corner), as grids converted from other generators number them.  Faces that
+    no other cell shares get ghosts, numbered NELES+1.. in cell order, faces ascending,
+    with BC type ``bc_type(x_mid_mm, y_mid_mm)`` of the face midpoint.  The result is one
+    grid.in / bc.in as the reference reads them (geometry.f90:31-52), not one i x j block.
+    """
+    node_id: dict = {}
+    xs, ys = [], []
+
+    def node(x, y):
+        k = (float(x), float(y))
+        if k not in node_id:
+            node_id[k] = len(xs) + 1
+            xs.append(float(x))
+            ys.append(float(y))
+        return node_id[k]
+
+    nod = []
+    for b, (xn, yn) in enumerate(blocks):
+        ni, nj = xn.shape[0] - 1, xn.shape[1] - 1
+        r = 0 if rotate is None else int(rotate[b]) % 4
+        for i in range(ni):
+            for j in range(nj):
+                q = [node(xn[i, j], yn[i, j]), node(xn[i + 1, j], yn[i + 1, j]),
+                     node(xn[i + 1, j + 1], yn[i + 1, j + 1]), node(xn[i, j + 1], yn[i, j + 1])]
+                nod.append(q[r:] + q[:r])
+    nod = np.asarray(nod, np.int32)
+    neles = nod.shape[0]
+    edge: dict = {}
+    for c in range(neles):
+        for k in range(4):
+            a, b2 = int(nod[c, k]), int(nod[c, (k + 1) % 4])
+            edge.setdefault((min(a, b2), max(a, b2)), []).append((c, k))
+    nc = np.zeros((neles, 4), np.int32)
+    for faces in edge.values():
+        if len(faces) > 2:
+            raise ValueError("an edge is shared by more than two cells")
+        if len(faces) == 2:
+            (c1, k1), (c2, k2) = faces
+            nc[c1, k1] = c2 + 1
+            nc[c2, k2] = c1 + 1
+    xm, ym = np.asarray(xs), np.asarray(ys)
+    par, gid, typ, side = [], [], [], []
+    for c in range(neles):
+        for k in range(4):
+            if nc[c, k] == 0:
+                g = neles + 1 + len(gid)
+                nc[c, k] = g
+                a, b2 = nod[c, k] - 1, nod[c, (k + 1) % 4] - 1
+                par.append(c + 1)
+                gid.append(g)
+                side.append(k + 1)
+                typ.append(int(bc_type(0.5 * (xm[a] + xm[b2]), 0.5 * (ym[a] + ym[b2]))))
+    i32 = lambda v: np.asarray(v, np.int32)
+    return Mesh(x=xm * MM_TO_M, y=ym * MM_TO_M, nod=nod, nc=nc, nparent=i32(par), nghost=i32(gid),
+                ntype=i32(typ), nside=i32(side), x_mm=xm, y_mm=ym, shape=None)
+
+
+def backstep_mesh(nx_in: int = 32, nx_out: int = 96, ny_up: int = 24, ny_low: int = 12,
+                  length_in: float = 0.2, length_out: float = 0.8, height: float = 0.3,
+                  step: float = 0.1) -> Mesh:
+    """Backward-facing step, 2-D, three blocks: the inlet channel above the step
+    (``length_in`` long, y from ``step`` to ``height``), and downstream of it an upper
+    and a lower block (y above and below ``step``); the lower block's cells number their
+    nodes from another corner.  Inlet (x=0) type 2, outlet type 3, every other face a
+    type-5 wall (channel top and bottom, the step face)."""
+    L1, L = length_in * 1000.0, (length_in + length_out) * 1000.0
+    h, H = step * 1000.0, height * 1000.0
+    grid = lambda x0, x1, nx, y0, y1, ny: np.meshgrid(np.linspace(x0, x1, nx + 1), np.linspace(y0, y1, ny + 1),
+                                                      indexing="ij")
+    blocks = [grid(0.0, L1, nx_in, h, H, ny_up), grid(L1, L, nx_out, h, H, ny_up),
+              grid(L1, L, nx_out, 0.0, h, ny_low)]
+
+    def bc(x, y):
+        if x == 0.0:
+            return 2
+        if x == L:
+            return 3
+        return 5
+
+    return multiblock_mesh(blocks, bc, rotate=[0, 0, 1])
+
 
 def ramp_flow(niter: int = 2000, p0: float = 873500.0, t0: float = 298.0) -> Flow:
     """flow.in of the 2-D ramp case: ``grid.in bc.in 1.4 28.96 1 N 1 0.25 0.72 0.9

@@ -134,3 +134,21 @@ def test_case1_drop_in_main(tmp_path):
     vals = np.array([[float(x) for x in l.split()] for l in tec[2:2 + mesh.nods]])
     for col, refv in ((2, un), (3, vn), (4, pn * 1e-5), (7, tn)):
         assert np.max(np.abs(vals[:, col] - refv)) <= TOL * np.max(np.abs(refv)), col
+
+
+def test_oracle_is_numbering_invariant_on_case1():
+    """The oracle on case1 with permuted cell / node ids and rotated local node order
+    (tests/meshperm.py) gives the original solution up to summation order: this holds the
+    renumbering helper the general-mesh GPU tests use."""
+    from meshperm import permute_mesh
+    mesh, flow, g = load_case1()
+    ri = float(g["rinit"])
+    pm, perm = permute_mesh(mesh, seed=1)
+    a = Oracle(pm, flow, ri)
+    a.set_state(formats.cold_state(flow, pm.neles, ri))
+    ha = a.iterate(100, 50)
+    b = Oracle(mesh, flow, ri)
+    b.set_state(formats.cold_state(flow, mesh.neles, ri))
+    hb = b.iterate(100, 50)
+    assert np.all(_rel(a.state()[:, perm], b.state()) <= 1e-10)
+    assert np.max(np.abs(ha - hb) / np.abs(hb)) <= 1e-10

@@ -1,0 +1,148 @@
+"""General quadrilateral meshes through the C ABI: meshes that are not one structured
+i x j block (the reference reads any NOD / NC1..NC4, geometry.f90:31-52) run on the
+gather-indexed kernels (csrc/tns_unstructured.cu) and must match the oracle on the same
+mesh to <= 1e-10 relative (max-norm per variable), like the structured path.
+
+Meshes: the reference's examples/case1 with its cell and node ids permuted and every
+cell's faces starting at another corner (tests/meshperm.py); the same with ids only
+permuted (still one block: the structured path with its permutation); a three-block
+backward-facing step (cases.backstep_mesh); axisymmetric and port / boundary-layer
+variants renumbered the same way."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from meshperm import permute_mesh
+from oracle.pyoracle import Oracle
+from test_case1 import load_case1
+from tnsgpu import cases, formats
+from tnsgpu.solver import Solver
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def rel(a, b):
+    a, b = np.atleast_2d(a), np.atleast_2d(b)
+    return np.max(np.abs(a - b), axis=1) / np.maximum(np.max(np.abs(b), axis=1), 1e-300)
+
+
+def _compare(mesh, flow, c0, ri, niter, mon, label):
+    s = Solver(mesh, flow, ri)
+    s.upload(c0)
+    hist = s.run(niter, mon)
+    q = s.download()
+    prim = s.primitives()
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    ref_hist = o.iterate(niter, mon)
+    err = rel(q, o.state())
+    herr = np.max(np.abs(hist - ref_hist) / np.abs(ref_hist)) if len(ref_hist) else 0.0
+    nn = o.nn
+    perr = rel(prim[:, :nn], np.stack([o.fetch(k)[:nn] for k in "UVTP"]))
+    print(f"{label}: {mesh.neles} cells x {niter} iterations, Q rel err {err}, CDIFF {herr:.3e}, "
+          f"primitives {perr.max():.3e}")
+    assert hist.shape == ref_hist.shape
+    assert np.all(err <= TOL), err
+    assert herr <= TOL
+    assert np.all(perr <= TOL), perr
+    return s, o
+
+
+def _cold(mesh, flow):
+    ri = formats.rinit_cold(flow)
+    return formats.cold_state(flow, mesh.neles, ri), ri
+
+
+def test_case1_renumbered_and_rotated_takes_the_general_path():
+    mesh, flow, g = load_case1()
+    pm, _ = permute_mesh(mesh, seed=1)
+    c0, ri = _cold(pm, flow)
+    s, o = _compare(pm, flow, c0, ri, 200, 50, "case1 permuted + rotated")
+    # POSTPROCESS node averages and boundary integrals of the last stage
+    pn, un, vn, tn = o.postprocess()
+    na = s.node_averages()
+    for got, ref in zip(na, (pn, un, vn, tn)):
+        assert np.max(np.abs(got - ref)) <= TOL * np.max(np.abs(ref))
+    s.close()
+
+
+def test_case1_renumbered_without_rotation_stays_structured():
+    mesh, flow, g = load_case1()
+    pm, _ = permute_mesh(mesh, seed=2, rotate=False)
+    c0, ri = _cold(pm, flow)
+    s, _ = _compare(pm, flow, c0, ri, 200, 50, "case1 permuted")
+    s.close()
+
+
+def test_case1_one_iteration_frozen_terms():
+    """D, VIS and DT of the first iteration, cell by cell, on the general path."""
+    mesh, flow, g = load_case1()
+    pm, _ = permute_mesh(mesh, seed=3)
+    c0, ri = _cold(pm, flow)
+    s = Solver(pm, flow, ri)
+    s.upload(c0)
+    s.run(1, 0)
+    o = Oracle(pm, flow, ri)
+    o.set_state(c0)
+    o.iterate(1, 0)
+    ne = pm.neles
+    assert np.all(rel(s.debug(0), np.stack([o.fetch(f"D24{k}")[:ne] for k in range(1, 6)])) < 1e-11)
+    assert np.all(rel(s.debug(1), np.stack([o.fetch(k)[:ne] for k in ("VISU", "VISV", "VIST", "VISR")])) < 1e-11)
+    assert np.all(rel(s.debug(2), o.fetch("DT")[None, :ne]) < 1e-13)
+    s.close()
+
+
+@pytest.mark.parametrize("local", [1, 0])
+def test_backward_facing_step_three_blocks(local):
+    mesh, flow = cases.backstep_mesh(32, 96, 24, 12), cases.ramp_flow()
+    flow.istart = 0
+    flow.local = local
+    c0, ri = _cold(mesh, flow)
+    s, _ = _compare(mesh, flow, c0, ri, 200, 50, f"backstep LOCAL={local}")
+    s.close()
+
+
+def _bl_ramp():
+    m = cases.ramp_mesh(24, 12)
+    m.ntype[m.ntype == 2] = 7
+    f = cases.ramp_flow()
+    f.pinf, f.aminf, f.deltabl = 8.6e5, 0.05, 0.01
+    return m, f
+
+
+@pytest.mark.parametrize("kind", ["port_type4_axis", "plume_type4_axis", "bl_inlet"])
+def test_renumbered_axisymmetric_port_and_inlet_cases(kind):
+    if kind == "port_type4_axis":
+        mesh, flow = cases.port_mesh(40, 16), cases.port_flow()
+    elif kind == "plume_type4_axis":
+        mesh, flow = cases.nozzle_plume_mesh(48, 20), cases.nozzle_plume_flow()
+    else:
+        mesh, flow = _bl_ramp()
+    if kind != "bl_inlet":
+        mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4  # well-conditioned axis
+    pm, _ = permute_mesh(mesh, seed=4)
+    c0, ri = _cold(pm, flow)
+    s, _ = _compare(pm, flow, c0, ri, 20, 10, kind)
+    if kind == "port_type4_axis":
+        # the port line of each type-6 ghost, walked across a renumbered mesh
+        assert np.any(pm.ntype == 6)
+    s.close()
+
+
+def test_drop_in_main_on_a_general_mesh(tmp_path):
+    mesh, flow = cases.backstep_mesh(16, 48, 12, 6), cases.ramp_flow(300)
+    flow.istart = 0
+    formats.write_case(str(tmp_path), mesh, flow)
+    r = subprocess.run([os.path.join(os.path.dirname(HERE), "2d-turbulent-navier-stokes_b200", "mains",
+                                     "twodturb")], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    cfin, *_ = formats.read_restart(str(tmp_path / "restart.in"), mesh.neles)
+    c0, ri = _cold(mesh, flow)
+    o = Oracle(mesh, flow, ri)
+    o.set_state(c0)
+    o.iterate(300, 1000)
+    assert np.all(rel(cfin, o.state()) <= TOL)

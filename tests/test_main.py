@@ -19,9 +19,10 @@ def _run(exe, cwd):
                           timeout=600)
 
 
-def test_main_rejects_unstructured_mesh_before_touching_cuda(tmp_path):
-    m = cases.ramp_mesh(6, 4)
-    m.nc[9, 1], m.nc[9, 2] = m.nc[9, 2], m.nc[9, 1]
+def test_main_rejects_a_mesh_it_cannot_lay_out_before_touching_cuda(tmp_path):
+    # one row of cells: the type-3 ghosts have no cell across the opposite face
+    xn, yn = np.meshgrid(np.linspace(0.0, 600.0, 7), np.linspace(0.0, 100.0, 2), indexing="ij")
+    m = cases.multiblock_mesh([(xn, yn)], lambda x, y: 2 if x == 0.0 else 3)
     f = cases.ramp_flow(10)
     f.istart = 0
     formats.write_case(str(tmp_path), m, f)
