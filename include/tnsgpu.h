@@ -23,7 +23,7 @@ extern "C" {
 #define TNS_OK 0
 #define TNS_ERR_ARG (-1)          /* null pointer / bad size */
 #define TNS_ERR_MESH (-2)         /* inconsistent grid.in / bc.in arrays */
-#define TNS_ERR_UNSUPPORTED (-3)  /* mesh is not one structured i x j block */
+#define TNS_ERR_UNSUPPORTED (-3)  /* a case the layout cannot express (see tns_create) */
 #define TNS_ERR_CUDA (-4)         /* CUDA runtime error */
 #define TNS_ERR_NONFINITE (-5)    /* state became NaN / Inf */
 #define TNS_ERR_STATE (-6)        /* call out of order (e.g. no state uploaded) */
@@ -54,8 +54,14 @@ typedef struct tns_params {
 
 typedef struct tns_handle tns_handle;
 
-/* Builds the device mesh: validates the arrays, detects the structured i x j block,
- * computes DL and the ghost centroids (geometry.f90:55-149) and uploads everything.
+/* Builds the device mesh: validates the arrays, computes the geometry
+ * (geometry.f90:55-149) and uploads everything.  A mesh whose cells form one structured
+ * i x j block (any numbering) runs on the tiled kernels; any other quadrilateral mesh
+ * (the reference reads any NOD / NC1..NC4) on the gather-indexed kernels, its cells
+ * renumbered by reverse Cuthill-McKee on the device (the ABI's arrays keep the caller's
+ * ids).  TNS_ERR_UNSUPPORTED: a general mesh with mixed precision, or with a type-3 ghost
+ * whose parent has no cell across the opposite face; the adjoint and the batch API also
+ * refuse general meshes with it.
  * Replaces: CALL COMPUTE_GEOMETRY's consumers + the module state setup
  * (turbnstwod.f90:32-48). */
 int tns_create(const tns_mesh *mesh, const tns_params *params, tns_handle **out);
