@@ -463,7 +463,7 @@ void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) 
         launch(h, K_STAGE, [&] {
             tns::launch_stage_mx(P, M, A, in[st], out[st], st == 3 ? Aout : nullptr, h->df.p, h->visf.p,
                                  h->dtf.p, h->dtmin.p, alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
-                                 st == 3 ? h->status.p : nullptr, s);
+                                 st == 3 ? h->status.p : nullptr, h->status.p, s);
         });
     }
 }

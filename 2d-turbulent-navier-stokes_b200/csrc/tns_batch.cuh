@@ -47,6 +47,7 @@ struct StageArgsMx {
     float alpha;
     unsigned long long* cdiff;
     unsigned int* status;
+    unsigned int* error;  // bit 1: a tile's static-block copy did not complete
 };
 
 struct BatchCase {

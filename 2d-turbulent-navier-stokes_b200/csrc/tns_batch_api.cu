@@ -126,7 +126,8 @@ BatchCase describe(tns_batch* b, int k) {
                 for (int st = 0; st < 4; st++)
                     c.stage_mx[par][mon][st] = tns::StageArgsMx{
                         q[par], in[st], out[st], st == 3 ? q[1 - par] : nullptr, h->df.p, h->visf.p, h->dtf.p,
-                        h->dtmin.p, alpha[st], (mon && st == 3) ? cdiff : nullptr, st == 3 ? status : nullptr};
+                        h->dtmin.p, alpha[st], (mon && st == 3) ? cdiff : nullptr, st == 3 ? status : nullptr,
+                        status};
     }
     return c;
 }

@@ -57,7 +57,7 @@ void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* v
 void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,
                      float* dqout, double* qout, const float* d, const float* vis, const float* dt,
                      const double* dtmin, double alpha, unsigned long long* cdiff,
-                     unsigned int* status, cudaStream_t s);
+                     unsigned int* status, unsigned int* error, cudaStream_t s);
 void launch_gport_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,
                      const int* ghosts, int nport, double* gport, cudaStream_t s);
 void launch_prim_out_mx(const Params& P, const Mesh& M, const double* cold, const float* dq,

@@ -39,14 +39,14 @@ __device__ __forceinline__ float tanh_f32(float x) {
 // ------------------------------------------------------------------ stage kernel
 
 struct StageSmemMx {
+    double st[STILE];      // the tile's static block (tns_tile.cuh), one bulk copy
     float2 fg[5][NSLOT];   // (F_m - Fref_m, G_m - Gref_m)
     double2 uv[NSLOT];     // (U, V)
     double2 rq[NSLOT];     // (C5/C1, |V|)
-    double2 xy[NSLOT];     // centroid
     double p[NSLOT];       // pressure (FP64: the axisymmetric radial balance cancels)
     float2 tr[NSLOT];      // (T, RHO)
     double fref[5], gref[5];
-    double nx[NNODE], ny[NNODE];
+    unsigned long long bar;  // completion of the static block's copy
 };
 
 size_t stage_mx_smem_bytes() { return sizeof(StageSmemMx); }
@@ -85,7 +85,12 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     pdl_trigger();
-    load_nodes(M, i0, j0, S.nx, S.ny);
+    // the static block is written by nothing: its copy overlaps the previous kernel's tail
+    if (tid == 0) {
+        bulk_barrier_init(&S.bar);
+        const size_t tile = (size_t)by * ((M.nj + TJ - 1) / TJ) + bx;
+        bulk_copy_start(S.st, M.stile + tile * STILE, STILE * sizeof(double), &S.bar);
+    }
     pdl_wait();
     if (tid == 0) {
         // tile reference flux: the first cell of the tile
@@ -101,19 +106,20 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
         Prim p;
-        if (kind == 0) {
+        if (kind == 0)
             cell_prim(P, st, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-            const int n1 = li * NW + lj;
-            S.xy[s] = make_double2((S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25,
-                                   (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25);
-        } else {
+        else
             ghost_state(P, M, st, kind, along, p);
-            const int g = M.ghost_index(kind, along);
-            S.xy[s] = make_double2(M.gxc[g], M.gyc[g]);
-        }
         put_slot_mx(S, s, p);
     }
     __syncthreads();
+    if (!bulk_wait(&S.bar)) {
+        // the copy did not complete: report it, give it one more bounded wait (it writes
+        // this block's shared memory) and leave the tile
+        if (tid == 0) atomicOr(A.error, 2u);
+        bulk_wait(&S.bar);
+        return;
+    }
 
     const int tj = threadIdx.x, ti = threadIdx.y;
     const int i = i0 + ti, j = j0 + tj;
@@ -123,14 +129,17 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
         const size_t cell = (size_t)i * M.nj + j;
         const int c = (ti + 1) * SW + (tj + 1);
         const int nb[4] = {c - 1, c + SW, c + 1, c - SW};
-        const int n1 = (ti + 1) * NW + (tj + 1);
-        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
-        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
+        const int n1 = ti * SNW + tj;  // node 1 of the cell in the static block
+        const int gc = 2 * SNN + ti * TJ + tj;
+        const double* X0 = S.st;
+        const double* Y0 = S.st + SNN;
+        const double X[4] = {X0[n1], X0[n1 + SNW], X0[n1 + SNW + 1], X0[n1 + 1]};
+        const double Y[4] = {Y0[n1], Y0[n1 + SNW], Y0[n1 + SNW + 1], Y0[n1 + 1]};
         double SX[4], SY[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) face_vector(P.iaxis, k + 1, X, Y, SX[k], SY[k]);
-        const double2 xyc = S.xy[c];
-        const double VOL = cell_volume(P.iaxis, X, Y, xyc.y);
+        const double ycc = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
+        const double VOL = M.cvol[cell];
         const double sumx = SX[0] + SX[1] + SX[2] + SX[3], sumy = SY[0] + SY[1] + SY[2] + SY[3];
         float sx[4], sy[4];
 #pragma unroll
@@ -149,27 +158,22 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             R64[m] = S.fref[m] * sumx + S.gref[m] * sumy;
         }
 
-        // source terms (source_terms.f90:24-104): FP64 stencil differences, FP32 rest
+        // source terms (source_terms.f90:24-104): FP64 stencil differences, FP32 rest,
+        // the gradient through the tile's stored coefficients
         {
             const int a = nb[0], b = nb[1], cc = nb[2], d = nb[3];
-            const double2 xa = S.xy[a], xb = S.xy[b], xc = S.xy[cc], xd = S.xy[d];
-            const double ybd = xb.y - xd.y, yac = xa.y - xc.y, xbd = xb.x - xd.x, xac = xa.x - xc.x;
-            const float idnr = (float)(1.0 / (xac * ybd - xbd * yac));
-            const float fybd = (float)ybd, fyac = (float)yac, fxbd = (float)xbd, fxac = (float)xac;
+            const float ga = (float)S.st[gc + ST_GA * NTHREADS], gb = (float)S.st[gc + ST_GB * NTHREADS];
+            const float gcf = (float)S.st[gc + ST_GC * NTHREADS], gd = (float)S.st[gc + ST_GD * NTHREADS];
             const double2 ua = S.uv[a], ub = S.uv[b], uc = S.uv[cc], ud = S.uv[d];
             const double2 ra = S.rq[a], rb = S.rq[b], rc = S.rq[cc], rd = S.rq[d];
             const float dqac = (float)(ra.y - rc.y), dqbd = (float)(rb.y - rd.y);
             const float drac = (float)(ra.x - rc.x), drbd = (float)(rb.x - rd.x);
             const float duac = (float)(ua.x - uc.x), dubd = (float)(ub.x - ud.x);
             const float dvac = (float)(ua.y - uc.y), dvbd = (float)(ub.y - ud.y);
-            const float DQX = (dqac * fybd - dqbd * fyac) * idnr;
-            const float DRX = (drac * fybd - drbd * fyac) * idnr;
-            const float DUX = (duac * fybd - dubd * fyac) * idnr;
-            const float DVX = (dvac * fybd - dvbd * fyac) * idnr;
-            const float DQY = (-dqac * fxbd + dqbd * fxac) * idnr;
-            const float DRY = (-drac * fxbd + drbd * fxac) * idnr;
-            const float DUY = (-duac * fxbd + dubd * fxac) * idnr;
-            const float DVY = (-dvac * fxbd + dvbd * fxac) * idnr;
+            const float DQX = dqac * ga + dqbd * gb, DQY = dqac * gcf + dqbd * gd;
+            const float DRX = drac * ga + drbd * gb, DRY = drac * gcf + drbd * gd;
+            const float DUX = duac * ga + dubd * gb, DUY = duac * gcf + dubd * gd;
+            const float DVX = dvac * ga + dvbd * gb, DVY = dvac * gcf + dvbd * gd;
             const float2 trc = S.tr[c];
             const float RHO = trc.y, RI = (float)S.rq[c].x, T = trc.x;
             const float AMU = (float)P.suth_amol * pow06f(T);
@@ -195,8 +199,8 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             float PK, src5;
             const float volf = (float)VOL;
             if (P.iaxis == 1) {
-                const double ycc = xyc.y;
-                const float VBYY = (ycc < YAXIS_THRESH) ? DVY : (float)(S.uv[c].y / ycc);
+                const double rycc = S.st[gc + ST_RYCC * NTHREADS];
+                const float VBYY = (ycc < YAXIS_THRESH) ? DVY : (float)(S.uv[c].y * rycc);
                 const float DIVVEL = DUX + DVY + VBYY;
                 PK = AMUT / RHO *
                      (DUX * DUX + DVY * DVY + VBYY * VBYY + DUX * DUX + DVY * DVY + VBYY * VBYY +
@@ -206,8 +210,8 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
                         RHO * (float)CONST3 * DEE) * pw;
                 const float TTT = (AMU + AMUT) * (VBYY + VBYY - DIV23 * DIVVEL);
                 // SOURCE3 = (P - TTT)/YCC: the P part cancels the reference flux in FP64
-                R64[2] -= VOL * (S.p[c] / ycc);
-                R[2] += volf * (TTT / (float)ycc);
+                R64[2] -= VOL * (S.p[c] * rycc);
+                R[2] += volf * (TTT * (float)rycc);
             } else {
                 const float DIVVEL = DUX + DVY;
                 PK = AMUT / RHO *
@@ -224,7 +228,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
 
         // update (residual.f90:67-83) as an FP32 increment on the FP64 state
         const float DT = P.local ? A.dt[cell] : (float)*A.dtmin;
-        const float dtv = -A.alpha * (DT / (float)VOL);
+        const float dtv = -A.alpha * (DT * (float)S.st[gc + ST_RVOL * NTHREADS]);
         float inc[5];
         inc[0] = dtv * (R[0] - A.d[cell]);
         inc[1] = dtv * (R[1] - A.vis[cell] - A.d[ncell + cell]);
@@ -284,31 +288,21 @@ constexpr int NIFM = (TI + 1) * TJ;
 constexpr int NJFM = TI * (TJ + 1);
 
 struct ViscSmemMx {
-    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT], xc[NSLOT], yc[NSLOT];
+    double u[NSLOT], v[NSLOT], t[NSLOT], rho[NSLOT], ri[NSLOT];
     double au[NAVG], av[NAVG], at[NAVG], arho[NAVG], ar[NAVG];
     float fi[4][NIFM], fj[4][NJFM];
-    double nx[NNODE], ny[NNODE];
 };
 
 size_t visc_mx_smem_bytes() { return sizeof(ViscSmemMx); }
 
-// One face of viscous.f90:130-217: FP64 geometry and stencil differences, FP32 rest.
+// One face of viscous.f90:130-217: FP64 stencil differences, FP32 rest; the face vector
+// and diamond-gradient coefficients from the face's stored row fg[k * nf] (FG_*).
 __device__ __forceinline__ void face_flux_mx(const Params& P, const ViscSmemMx& S, int sa, int sc,
-                                             int ab, int ad, int nb, int nd, float out[4]) {
-    const double xb = S.nx[nb], yb = S.ny[nb], xd = S.nx[nd], yd = S.ny[nd];
-    double SXd, SYd;
-    if (P.iaxis == 1) {
-        SXd = (yd - yb) * (yb + yd) * HALF;
-        SYd = -(xd - xb) * (yb + yd) * HALF;
-    } else {
-        SXd = (yd - yb);
-        SYd = -(xd - xb);
-    }
-    const float sx = (float)SXd, sy = (float)SYd;
-    const double xa = S.xc[sa], ya = S.yc[sa], xc = S.xc[sc], yc = S.yc[sc];
-    const double ybd = yb - yd, yac = ya - yc, xbd = xb - xd, xac = xa - xc;
-    const float idnr = (float)(1.0 / (xac * ybd - xbd * yac));
-    const float fybd = (float)ybd, fyac = (float)yac, fxbd = (float)xbd, fxac = (float)xac;
+                                             int ab, int ad, const double* __restrict__ fg, size_t nf,
+                                             float out[4]) {
+    const float sx = (float)fg[FG_SX * nf], sy = (float)fg[FG_SY * nf];
+    const float ga = (float)fg[FG_GA * nf], gb = (float)fg[FG_GB * nf];
+    const float gc = (float)fg[FG_GC * nf], gd = (float)fg[FG_GD * nf];
     const double ua = S.u[sa], va = S.v[sa], ta = S.t[sa], uc = S.u[sc], vc = S.v[sc], tc = S.t[sc];
     const double ub = S.au[ab], vb = S.av[ab], tb = S.at[ab], ud = S.au[ad], vd = S.av[ad], td = S.at[ad];
     const double ra = S.ri[sa], rc = S.ri[sc], rb = S.ar[ab], rd = S.ar[ad];
@@ -316,14 +310,10 @@ __device__ __forceinline__ void face_flux_mx(const Params& P, const ViscSmemMx& 
     const float dvac = (float)(va - vc), dvbd = (float)(vb - vd);
     const float dtac = (float)(ta - tc), dtbd = (float)(tb - td);
     const float drac = (float)(ra - rc), drbd = (float)(rb - rd);
-    const float DUX = (duac * fybd - dubd * fyac) * idnr;
-    const float DVX = (dvac * fybd - dvbd * fyac) * idnr;
-    const float DTX = (dtac * fybd - dtbd * fyac) * idnr;
-    const float DRX = (drac * fybd - drbd * fyac) * idnr;
-    const float DUY = (-duac * fxbd + dubd * fxac) * idnr;
-    const float DVY = (-dvac * fxbd + dvbd * fxac) * idnr;
-    const float DTY = (-dtac * fxbd + dtbd * fxac) * idnr;
-    const float DRY = (-drac * fxbd + drbd * fxac) * idnr;
+    const float DUX = duac * ga + dubd * gb, DUY = duac * gc + dubd * gd;
+    const float DVX = dvac * ga + dvbd * gb, DVY = dvac * gc + dvbd * gd;
+    const float DTX = dtac * ga + dtbd * gb, DTY = dtac * gc + dtbd * gd;
+    const float DRX = drac * ga + drbd * gb, DRY = drac * gc + drbd * gd;
     const float UAVG = (float)(QUARTER * (ua + ub + uc + ud));
     const float VAVG = (float)(QUARTER * (va + vb + vc + vd));
     const float TAVG = (float)(QUARTER * (ta + tb + tc + td));
@@ -331,8 +321,8 @@ __device__ __forceinline__ void face_flux_mx(const Params& P, const ViscSmemMx& 
     const float RAVG = (float)(QUARTER * (ra + rb + rc + rd));
     float DIVVEL;
     if (P.iaxis == 1) {
-        const double YAVG = HALF * (yb + yd);
-        const float VBYY = (YAVG < YAXIS_THRESH) ? DVY : (float)(QUARTER * (va + vb + vc + vd) / YAVG);
+        const double ryavg = fg[FG_RYAVG * nf];
+        const float VBYY = (ryavg == 0.0) ? DVY : (float)(QUARTER * (va + vb + vc + vd) * ryavg);
         DIVVEL = DUX + DVY + VBYY;
     } else {
         DIVVEL = DUX + DVY;
@@ -366,26 +356,17 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     pdl_trigger();
-    load_nodes(M, i0, j0, S.nx, S.ny, VNT);
     pdl_wait();
-    __syncthreads();
     for (int s = tid; s < NSLOT; s += VNT) {
         const int li = s / SW, lj = s % SW;
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
         Prim p;
-        if (kind == 0) {
+        if (kind == 0)
             cell_prim(P, q, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-            const int n1 = li * NW + lj;
-            S.xc[s] = (S.nx[n1] + S.nx[n1 + NW] + S.nx[n1 + NW + 1] + S.nx[n1 + 1]) * 0.25;
-            S.yc[s] = (S.ny[n1] + S.ny[n1 + NW] + S.ny[n1 + NW + 1] + S.ny[n1 + 1]) * 0.25;
-        } else {
+        else
             ghost_state(P, M, q, ncell, kind, along, p);
-            const int g = M.ghost_index(kind, along);
-            S.xc[s] = M.gxc[g];
-            S.yc[s] = M.gyc[g];
-        }
         S.u[s] = p.u; S.v[s] = p.v; S.t[s] = p.t; S.rho[s] = p.rho; S.ri[s] = p.ri;
     }
     __syncthreads();
@@ -434,8 +415,11 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
     __syncthreads();
     // all faces of the tile in one loop (i-faces first): at most three faces per thread,
     // one inlined copy of the face flux
+    const size_t nfi = (size_t)(M.ni + 1) * M.nj, nfj = (size_t)M.ni * (M.nj + 1);
     for (int f = tid; f < NIFM + NJFM; f += VNT) {
-        int sa, sc, ab, ad, nb, nd;
+        int sa, sc, ab, ad;
+        const double* fg;
+        size_t nf;
         if (f < NIFM) {
             // i-face: orientation of cell (i-1, j) as its face 2, or of (0, j) as its face 4
             const int ii = f / TJ, jj = f % TJ;
@@ -443,12 +427,13 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
             if (i > M.ni || j >= M.nj) continue;
             const int sL = ii * SW + jj + 1, sR = sL + SW;  // cells (i-1, j), (i, j)
             const int aLo = ii * AW + jj, aHi = aLo + 1;    // nodes (i, j), (i, j+1)
-            const int nLo = (ii + 1) * NW + jj + 1, nHi = nLo + 1;
             if (i == 0) {  // face 4: B=N4, D=N1
-                sa = sR; sc = sL; ab = aHi; ad = aLo; nb = nHi; nd = nLo;
+                sa = sR; sc = sL; ab = aHi; ad = aLo;
             } else {  // face 2: B=N2, D=N3
-                sa = sL; sc = sR; ab = aLo; ad = aHi; nb = nLo; nd = nHi;
+                sa = sL; sc = sR; ab = aLo; ad = aHi;
             }
+            fg = M.fgi + ((size_t)i * M.nj + j);
+            nf = nfi;
         } else {
             // j-face: orientation of cell (i, j-1) as its face 3, or of (i, 0) as its face 1
             const int g = f - NIFM;
@@ -457,15 +442,16 @@ __device__ __forceinline__ void viscous_mx_tile(const Params& P, const Mesh& M, 
             if (i >= M.ni || j > M.nj) continue;
             const int sB = (ii + 1) * SW + jj, sT = sB + 1;  // cells (i, j-1), (i, j)
             const int aL = ii * AW + jj, aR = aL + AW;       // nodes (i, j), (i+1, j)
-            const int nL = (ii + 1) * NW + jj + 1, nR = nL + NW;
             if (j == 0) {  // face 1: B=N1, D=N2
-                sa = sT; sc = sB; ab = aL; ad = aR; nb = nL; nd = nR;
+                sa = sT; sc = sB; ab = aL; ad = aR;
             } else {  // face 3: B=N3, D=N4
-                sa = sB; sc = sT; ab = aR; ad = aL; nb = nR; nd = nL;
+                sa = sB; sc = sT; ab = aR; ad = aL;
             }
+            fg = M.fgj + ((size_t)i * (M.nj + 1) + j);
+            nf = nfj;
         }
         float out[4];
-        face_flux_mx(P, S, sa, sc, ab, ad, nb, nd, out);
+        face_flux_mx(P, S, sa, sc, ab, ad, fg, nf, out);
         if (f < NIFM) {
 #pragma unroll
             for (int k = 0; k < 4; k++) S.fi[k][f] = out[k];
@@ -505,7 +491,6 @@ struct DissSmemMx {
     double c[5][NDSLOTM];
     double p[NDSLOTM];
     float vbd[NRSLOTM], anu[NRSLOTM], anurt[NRSLOTM], d2q[5][NRSLOTM];
-    double nx[NNODE], ny[NNODE];
 };
 
 size_t diss_mx_smem_bytes() { return sizeof(DissSmemMx); }
@@ -529,7 +514,6 @@ __device__ __forceinline__ void dissipation_mx_tile(const Params& P, const Mesh&
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     pdl_trigger();
-    load_nodes(M, i0, j0, S.nx, S.ny);
     pdl_wait();
     for (int s = tid; s < NDSLOTM; s += NTHREADS) {
         const int i = i0 - 2 + s / DWM, j = j0 - 2 + s % DWM;
@@ -580,11 +564,7 @@ __device__ __forceinline__ void dissipation_mx_tile(const Params& P, const Mesh&
         } else {
             DT = *dtmin;
         }
-        const int n1 = ri * NW + rj;
-        const double X[4] = {S.nx[n1], S.nx[n1 + NW], S.nx[n1 + NW + 1], S.nx[n1 + 1]};
-        const double Y[4] = {S.ny[n1], S.ny[n1 + NW], S.ny[n1 + NW + 1], S.ny[n1 + 1]};
-        const double ycc = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
-        S.vbd[s] = (float)(cell_volume(P.iaxis, X, Y, ycc) / DT);
+        S.vbd[s] = (float)(M.cvol[c] / DT);
     }
     __syncthreads();
     const int tj = threadIdx.x, ti = threadIdx.y;
@@ -790,8 +770,8 @@ void launch_viscous_mx(const Params& P, const Mesh& M, const double* q, float* v
 void launch_stage_mx(const Params& P, const Mesh& M, const double* cold, const float* dqin,
                      float* dqout, double* qout, const float* d, const float* vis, const float* dt,
                      const double* dtmin, double alpha, unsigned long long* cdiff,
-                     unsigned int* status, cudaStream_t s) {
-    StageArgsMx A{cold, dqin, dqout, qout, d, vis, dt, dtmin, (float)alpha, cdiff, status};
+                     unsigned int* status, unsigned int* error, cudaStream_t s) {
+    StageArgsMx A{cold, dqin, dqout, qout, d, vis, dt, dtmin, (float)alpha, cdiff, status, error};
     launch_tile(cdiff ? k_stage_mx<1> : k_stage_mx<0>, tile_grid_mx(M), dim3(TJ, TI), stage_mx_smem_bytes(), s,
                 P, M, A);
 }
