@@ -12,6 +12,7 @@
 // others carry on.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -48,8 +49,15 @@ struct tns_batch {
     // schedule: 0 = one launch per phase over the tile table of all active cases;
     // 1 = each case's own single-case launches on one of several streams, captured as
     // parallel branches of one graph (cases run concurrently, kernels as for tns_run);
-    // 2 = as 1, with BLOCK unmonitored iterations per graph
+    // 2 = as 1, with BLOCK unmonitored iterations per graph; 3 = one persistent
+    // cooperative launch per run of up to PERSIST unmonitored iterations (grid barriers
+    // between the phases), monitored iterations as schedule 0
     int mode = 0;
+    static constexpr int PERSIST = 256;
+    int persist_grid = 0;               // resident blocks of the persistent kernel
+    DevBuf<unsigned int> d_bar;         // its grid barrier: arrival counter, generation
+    DevBuf<unsigned int> d_error;       // bit 2: a grid barrier gave up
+    unsigned int* h_error = nullptr;    // pinned
     std::vector<cudaStream_t> branch;
     std::vector<int> branch_of;  // case -> branch stream (largest cases spread first)
     std::vector<cudaEvent_t> join;
@@ -270,9 +278,12 @@ void enqueue_branches(tns_batch* b, int parity, bool monitor, int iters = 1) {
 int fetch_monitor(tns_batch* b, bool monitor) {
     const int n = (int)b->cases.size();
     int rc;
-    if (b->mode == 0) {  // the tile-table kernels write the batch's own status and CDIFF slots
+    if (b->mode == 0 || b->mode == 3) {  // the tile-table kernels write the batch's own slots
         if ((rc = b->cuda(cudaMemcpyAsync(b->h_status, b->d_status.p, n * sizeof(unsigned int),
                                           cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
+            return rc;
+        if (b->mode == 3 && (rc = b->cuda(cudaMemcpyAsync(b->h_error, b->d_error.p, sizeof(unsigned int),
+                                                          cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
             return rc;
         if (monitor && (rc = b->cuda(cudaMemcpyAsync(b->h_cdiff, b->d_cdiff.p, 5 * n * sizeof(unsigned long long),
                                                      cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync")))
@@ -314,7 +325,7 @@ int ensure_batch_graph(tns_batch* b, int monitor, int parity) {
     int rc;
     if ((rc = b->cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
     const long long before = b->launches;
-    if (b->mode >= 1)
+    if (b->mode == 1 || b->mode == 2)
         enqueue_branches(b, parity, monitor != 0);
     else
         enqueue_batch_iteration(b, parity, monitor != 0);
@@ -471,7 +482,18 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
             for (int j = it; j < it + tns_batch::BLOCK; j++)
                 if (monitored(j)) step = 1;
         }
-        if (step > 1) {
+        if (b->mode == 3 && !monitor) {
+            // the run of unmonitored iterations from here, in one persistent launch
+            step = 1;
+            while (step < tns_batch::PERSIST && it + step <= niter && !monitored(it + step)) step++;
+            const int grid = std::min(b->persist_grid, 2 * b->ntiles);
+            if ((rc = b->cuda(cudaMemsetAsync(b->d_bar.p, 0, 2 * sizeof(unsigned int), b->stream), "cudaMemsetAsync")) ||
+                (rc = b->cuda(tns::launch_persistent(b->precision == 1, b->d_desc.p, b->d_tiles.p, b->d_active.p,
+                                                     b->ntiles, step, parity, grid, b->d_bar.p, b->d_error.p,
+                                                     b->stream), "persistent launch")))
+                return rc;
+            b->launches++;
+        } else if (step > 1) {
             if ((rc = ensure_block_graph(b, parity))) return rc;
             if ((rc = b->cuda(cudaGraphLaunch(b->block[parity], b->stream), "cudaGraphLaunch"))) return rc;
             b->launches += b->per_block;
@@ -489,6 +511,8 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
         // residual records, status words and the masks, at the monitor cadence and at the end
         if ((rc = fetch_monitor(b, monitor))) return rc;
         if ((rc = b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize"))) return rc;
+        if (b->mode == 3 && (*b->h_error & 4u))
+            return b->fail(TNS_ERR_CUDA, "a grid barrier of the persistent batch launch did not complete in its bounded wait");
         for (int k = 0; k < n; k++) {
             if (!b->active[k]) continue;
             if (b->h_status[k] & 3u) {
@@ -540,8 +564,29 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
 
 int tns_batch_set_schedule(tns_batch* b, int schedule) {
     if (!b) return TNS_ERR_ARG;
-    if (schedule < 0 || schedule > 2) return b->fail(TNS_ERR_ARG, "schedule %d is not 0, 1 or 2", schedule);
+    if (schedule < 0 || schedule > 3) return b->fail(TNS_ERR_ARG, "schedule %d is not 0, 1, 2 or 3", schedule);
     int rc;
+    if (schedule == 3) {
+        for (size_t k = 0; k < b->cases.size(); k++) {
+            const tns_handle* h = b->cases[k];
+            if (!h->P.local || !h->port_ghosts.empty())
+                return b->fail(TNS_ERR_UNSUPPORTED,
+                               "schedule 3 needs LOCAL=1 and no type-6 port in every case (case %zu)", k);
+        }
+        int dev = 0, coop = 0;
+        if ((rc = b->cuda(cudaGetDevice(&dev), "cudaGetDevice")) ||
+            (rc = b->cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute")))
+            return rc;
+        b->persist_grid = coop ? tns::persistent_grid(b->precision == 1) : 0;
+        if (b->persist_grid <= 0)
+            return b->fail(TNS_ERR_UNSUPPORTED, "schedule 3 needs a cooperative launch of the persistent kernel");
+        if (!b->d_bar.p && ((rc = b->cuda(b->d_bar.alloc(2), "cudaMalloc")) ||
+                            (rc = b->cuda(b->d_error.alloc(1), "cudaMalloc")) ||
+                            (rc = b->cuda(cudaMemset(b->d_error.p, 0, sizeof(unsigned int)), "cudaMemset")) ||
+                            (rc = b->cuda(cudaMallocHost((void**)&b->h_error, sizeof(unsigned int)), "cudaMallocHost"))))
+            return rc;
+        *b->h_error = 0;
+    }
     if (schedule >= 1 && b->branch.empty()) {
         const int n = (int)b->cases.size();
         const int nb = std::min<int>(n, 64);
@@ -587,6 +632,9 @@ void tns_batch_destroy(tns_batch* b) {
     b->d_tiles.release();
     b->d_cdiff.release();
     b->d_status.release();
+    b->d_bar.release();
+    b->d_error.release();
+    if (b->h_error) cudaFreeHost(b->h_error);
     if (b->h_cdiff) cudaFreeHost(b->h_cdiff);
     if (b->h_status) cudaFreeHost(b->h_status);
     for (cudaStream_t st : b->branch)

@@ -11,6 +11,8 @@
 //   [k_gport]      type-6 port mass flux of the stage input (only if such ghosts exist)
 // Ghost cells are never stored: each tile evaluates the BC of the ghosts in its halo
 // from the parent and the parent's opposite neighbour, both already in the tile.
+#include <algorithm>
+
 #include "tns_device.cuh"
 #include "tns_kernels.h"
 #include "tns_tile.cuh"
@@ -778,6 +780,42 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_
     stage_tile(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
 }
 
+// Persistent batched iterations (schedule 3): one cooperative launch advances every
+// active case by `iters` unmonitored RK4 iterations.  Its blocks walk the tile table
+// phase by phase -- dissipation and viscous flux together (both read Q_old only and
+// write disjoint arrays), then the four stages -- with a grid barrier between phases
+// (bounded waits: a barrier that gives up sets error bit 2 and the kernel returns).  A
+// block that finishes a tile synchronises before the next, whose static-block copy
+// reuses the tile's shared memory and barrier.  Cases need LOCAL=1 and no type-6 port
+// (those add per-case reductions between the phases).
+#ifndef TNS_PERSIST_MINB
+#define TNS_PERSIST_MINB 2
+#endif
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_PERSIST_MINB))
+k_batch_persistent(const BatchCase* __restrict__ cases, const int4* __restrict__ tiles,
+                   const int* __restrict__ active, int ntiles, int iters, unsigned int* bar,
+                   unsigned int* error) {
+    for (int it = 0; it < iters; it++) {
+        for (int ph = 0; ph < 5; ph++) {
+            const int nwork = ph == 0 ? 2 * ntiles : ntiles;
+            for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+                const int4 t = tiles[w % ntiles];
+                if (active[t.x]) {
+                    const BatchCase& c = cases[t.x];
+                    if (ph == 0 && w < ntiles) dissipation_tile<double>(c.P, c.M, c.diss, t.y, t.z);
+                    else if (ph == 0) viscous_tile(c.P, c.M, c.q, c.vis, t.y, t.z);
+                    else stage_tile(c.P, c.M, c.stage[0][ph - 1], t.y, t.z);
+                }
+                __syncthreads();
+            }
+            if (!grid_barrier(bar, bar + 1)) {
+                if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(error, 4u);
+                return;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- math check
 
 // Evaluates one of the FP64 helpers the kernels use, elementwise, for testing their
@@ -821,8 +859,37 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(k_viscous_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)visc_smem_bytes());
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)persistent_smem_bytes(false));
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_stage_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)stage_smem_bytes());
+}
+
+size_t persistent_smem_bytes(bool mixed) {
+    if (mixed) return std::max(stage_mx_smem_bytes(), std::max(visc_mx_smem_bytes(), diss_mx_smem_bytes()));
+    return std::max(stage_smem_bytes(), std::max(visc_smem_bytes(), diss_smem_bytes()));
+}
+
+int persistent_grid(bool mixed) {
+    int per_sm = 0, dev = 0, sms = 0;
+    const void* k = mixed ? persistent_kernel_mx() : (const void*)k_batch_persistent;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NTHREADS, persistent_smem_bytes(mixed)) !=
+            cudaSuccess)
+        return 0;
+    return per_sm * sms;
+}
+
+cudaError_t launch_persistent(bool mixed, const BatchCase* cases, const int4* tiles, const int* active,
+                              int ntiles, int iters, int parity, int grid, unsigned int* bar,
+                              unsigned int* error, cudaStream_t s) {
+    if (mixed) return launch_persistent_mx(cases, tiles, active, ntiles, iters, parity, grid, bar, error, s);
+    void* args[] = {(void*)&cases, (void*)&tiles, (void*)&active, (void*)&ntiles, (void*)&iters, (void*)&bar,
+                    (void*)&error};
+    return cudaLaunchCooperativeKernel((const void*)k_batch_persistent, dim3(grid), dim3(TJ, TI), args,
+                                       persistent_smem_bytes(false), s);
 }
 
 void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,

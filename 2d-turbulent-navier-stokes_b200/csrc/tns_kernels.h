@@ -47,6 +47,23 @@ void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* acti
 void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
                      int kernel, int parity, int stage, int monitor, cudaStream_t s);
 
+// persistent batched iterations (schedule 3): dynamic shared memory, the resident grid
+// (blocks per SM x SMs, 0 if unknown) and the cooperative launch of `iters` unmonitored
+// iterations; bar = arrival counter and generation (zero before the launch), error bit 2
+// = a grid barrier gave up
+size_t persistent_smem_bytes(bool mixed);
+int persistent_grid(bool mixed);
+cudaError_t launch_persistent(bool mixed, const BatchCase* cases, const int4* tiles, const int* active,
+                              int ntiles, int iters, int parity, int grid, unsigned int* bar,
+                              unsigned int* error, cudaStream_t s);
+const void* persistent_kernel_mx();
+cudaError_t launch_persistent_mx(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                                 int iters, int parity, int grid, unsigned int* bar, unsigned int* error,
+                                 cudaStream_t s);
+size_t stage_mx_smem_bytes();
+size_t visc_mx_smem_bytes();
+size_t diss_mx_smem_bytes();
+
 // mixed FP32/FP64 path (tns_kernels_mx.cu)
 cudaError_t configure_kernels_mx();
 void launch_dissipation_mx(const Params& P, const Mesh& M, const double* q, float* d, float* dt,

@@ -720,6 +720,51 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_BATCH_MINB))
     stage_mx_tile(c.P, c.M, c.stage_mx[parity][monitor][stage], t.y, t.z);
 }
 
+// Persistent batched iterations of the mixed path (schedule 3), as k_batch_persistent:
+// the state parity alternates from `parity` with every iteration.
+#ifndef TNS_PERSIST_MX_MINB
+#define TNS_PERSIST_MX_MINB 2
+#endif
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_PERSIST_MX_MINB))
+k_batch_persistent_mx(const BatchCase* __restrict__ cases, const int4* __restrict__ tiles,
+                      const int* __restrict__ active, int ntiles, int iters, int parity0, unsigned int* bar,
+                      unsigned int* error) {
+    for (int it = 0; it < iters; it++) {
+        const int parity = parity0 ^ (it & 1);
+        for (int ph = 0; ph < 5; ph++) {
+            const int nwork = ph == 0 ? 2 * ntiles : ntiles;
+            for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+                const int4 t = tiles[w % ntiles];
+                if (active[t.x]) {
+                    const BatchCase& c = cases[t.x];
+                    if (ph == 0 && w < ntiles)
+                        dissipation_mx_tile(c.P, c.M, c.qmx[parity], c.df, c.dtf, c.dtmin, t.y, t.z);
+                    else if (ph == 0)
+                        viscous_mx_tile(c.P, c.M, c.qmx[parity], c.visf, t.y, t.z);
+                    else
+                        stage_mx_tile(c.P, c.M, c.stage_mx[parity][0][ph - 1], t.y, t.z);
+                }
+                __syncthreads();
+            }
+            if (!grid_barrier(bar, bar + 1)) {
+                if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(error, 4u);
+                return;
+            }
+        }
+    }
+}
+
+const void* persistent_kernel_mx() { return (const void*)k_batch_persistent_mx; }
+
+cudaError_t launch_persistent_mx(const BatchCase* cases, const int4* tiles, const int* active, int ntiles,
+                                 int iters, int parity, int grid, unsigned int* bar, unsigned int* error,
+                                 cudaStream_t s) {
+    void* args[] = {(void*)&cases, (void*)&tiles, (void*)&active, (void*)&ntiles, (void*)&iters,
+                    (void*)&parity, (void*)&bar, (void*)&error};
+    return cudaLaunchCooperativeKernel((const void*)k_batch_persistent_mx, dim3(grid), dim3(TJ, TI), args,
+                                       persistent_smem_bytes(true), s);
+}
+
 // ------------------------------------------------------------------ launchers
 
 static dim3 tile_grid_mx(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
@@ -742,6 +787,9 @@ cudaError_t configure_kernels_mx() {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_viscous_mx_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)visc_mx_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_batch_persistent_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)persistent_smem_bytes(true));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_stage_mx_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)stage_mx_smem_bytes());

@@ -124,6 +124,37 @@ __device__ __forceinline__ bool bulk_wait(unsigned long long* bar, int max_polls
     return false;
 }
 
+// Grid-wide barrier of a cooperative launch (every block resident): an arrival counter
+// and a generation word in global memory, both zero before the launch.  The last block
+// to arrive resets the counter and advances the generation; the others poll the
+// generation at most max_polls times.  Returns false when the wait gave up (the caller
+// reports it and leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen, int max_polls = 1 << 22) {
+    __shared__ int passed;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const unsigned int g = *(volatile unsigned int*)gen;
+        __threadfence();
+        const unsigned int nb = gridDim.x * gridDim.y;
+        if (atomicAdd(count, 1u) == nb - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+            passed = 1;
+        } else {
+            int k = 0;
+            while (*(volatile unsigned int*)gen == g && k < max_polls) {
+                __nanosleep(64);
+                k++;
+            }
+            passed = *(volatile unsigned int*)gen != g;
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return passed != 0;
+}
+
 // Launch of a tile kernel that may overlap its predecessor's tail (see pdl_wait).
 template <class... Exp, class... Act>
 inline cudaError_t launch_tile(void (*kernel)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,

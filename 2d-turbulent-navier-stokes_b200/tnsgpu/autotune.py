@@ -3,9 +3,11 @@
 The tile kernels are compiled for three tile heights -- TI = 4, 8 or 16 rows of 32
 cells per thread block (``libtnsgpu_ti4.so``, ``libtnsgpu.so``, ``libtnsgpu_ti16.so``;
 each build keeps the threads resident per SM of the TI = 8 tuning).  A batch can also
-run any of three schedules (0: one launch per kernel phase over the tiles of all cases;
+run any of four schedules (0: one launch per kernel phase over the tiles of all cases;
 1: the cases' own launches on parallel branches of one CUDA graph; 2: as 1 with 8
-iterations per graph).  ``tune_batch`` and
+iterations per graph; 3: one persistent cooperative launch per run of unmonitored
+iterations, grid barriers between the phases -- refused, and skipped here, when a case
+has LOCAL=0 or a type-6 port).  ``tune_batch`` and
 ``tune_case`` time a few iterations of the caller's cases under every combination and
 return the fastest.
 
@@ -45,7 +47,7 @@ def _time_batch(solvers: Sequence[Solver], schedule: int, iters: int, warmup: in
 
 
 def tune_batch(make_solvers: Callable[[str], List[Solver]], iters: int = 40, warmup: int = 16,
-               tile_heights: Iterable[int] = TILE_HEIGHTS, schedules: Sequence[int] = (0, 1, 2),
+               tile_heights: Iterable[int] = TILE_HEIGHTS, schedules: Sequence[int] = (0, 1, 2, 3),
                cache: Optional[str] = None, key: Optional[str] = None) -> dict:
     """make_solvers(lib_path) builds the batch's cases (state uploaded) from that library
     build.  Times ``iters`` iterations after ``warmup`` (enough to capture every graph a

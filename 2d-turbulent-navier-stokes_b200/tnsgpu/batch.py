@@ -43,7 +43,11 @@ class Batch:
         self._check(rc)
         self.reference = np.zeros((len(self.solvers), 5))
         if schedule:
-            self.schedule = schedule
+            try:
+                self.schedule = schedule
+            except _lib.TnsError:
+                self.close()
+                raise
 
     def _check(self, rc: int):
         if rc != _lib.TNS_OK:

@@ -281,6 +281,9 @@ def run_ours(args, rank, world, dev):
     adj = None
     if world == 1 and not args.no_adjoint:
         adj = adjoint_timing(torch, dev)
+    bat = None
+    if world == 1 and not args.no_batch:
+        bat = batch_timing()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -304,6 +307,7 @@ def run_ours(args, rank, world, dev):
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         "other_precision": other,
         "adjoint": adj,
+        "batch": bat,
         "cpu_baseline": cpu,
     }
     if rank == 0:
@@ -389,6 +393,82 @@ def adjoint_timing(torch, dev, K=50, W=5):
             "kernels_per_transient_step": int(per_step)}
 
 
+def batch_timing(niter=200, monitor=100, stop_ratio=1.0e-5, warmup=16, ncases=64):
+    """The batched-sweep workload: ``ncases`` ramp cases from cases.ramp_sweep(seed=0)
+    (96x32 .. 512x192 cells, ramp angle, P0, T0 drawn per case), mixed FP32/FP64, cold
+    start, convergence masking at ``stop_ratio``.  Each arm first runs ``warmup``
+    untimed iterations (graph capture, kernel attributes), then ``niter`` iterations
+    with a residual record every ``monitor``: the cases one after another through
+    tns_run (the stop criterion checked at every record), and the same cases as one
+    batch under schedule 2 (per-case graph branches) and schedule 3 (one persistent
+    cooperative launch per run of unmonitored iterations).  Wall time with the device
+    synchronised; the default tile height (no autotuning)."""
+    import numpy as np
+    from tnsgpu import cases, formats
+    from tnsgpu.batch import Batch
+    from tnsgpu.solver import Solver
+    sw = cases.ramp_sweep(ncases, seed=0)
+    cells = np.array([c.nx * c.ny for c in sw], dtype=np.float64)
+
+    def members(solo_warmup):
+        out = []
+        for c in sw:
+            mesh, flow = c.mesh(), c.flow()
+            ri = formats.rinit_cold(flow)
+            s = Solver(mesh, flow, ri, precision=1)
+            s.upload(formats.cold_state(flow, mesh.neles, ri))
+            if solo_warmup:
+                s.run(warmup, 0)
+            out.append(s)
+        return out
+
+    seq = members(True)
+    t0 = time.perf_counter()
+    it_seq = []
+    for s in seq:
+        ref = s.run(1, 1)[0]
+        it = 1
+        while it < niter:
+            n = min(monitor - it % monitor, niter - it)
+            rec = s.run(n, n)
+            it += n
+            if it % monitor == 0 and np.max(rec[-1] / ref) <= stop_ratio:
+                break
+        it_seq.append(it)
+    t_seq = time.perf_counter() - t0
+    q_seq = [s.download() for s in seq]
+    for s in seq:
+        s.close()
+    out = {"workload": f"{ncases} ramp cases of cases.ramp_sweep(seed=0), 96x32..512x192, mixed FP32/FP64, "
+                       f"cold start + {warmup} untimed iterations",
+           "cells_total": int(cells.sum()), "niter": niter, "monitor": monitor, "stop_ratio": stop_ratio,
+           "sequential_s": round(t_seq, 4), "sequential_cell_iter_per_s": float(np.sum(cells * it_seq) / t_seq)}
+    best = None
+    for sched in (2, 3):
+        bat = members(False)
+        b = Batch(bat, schedule=sched)
+        # the warm-up on the batch itself captures this schedule's graphs (monitored and
+        # not, both state parities) and leaves every case where the sequential arm began
+        b.run(warmup, warmup // 2)
+        l0 = b.launch_count()
+        t0 = time.perf_counter()
+        r = b.run(niter, monitor, stop_ratio)
+        dt = time.perf_counter() - t0
+        launches = b.launch_count() - l0
+        b.close()
+        same = all(np.array_equal(s.download(), q) for s, q in zip(bat, q_seq))
+        its = [int(v) for v in r.iterations]
+        for s in bat:
+            s.close()
+        out[f"schedule_{sched}"] = {"s": round(dt, 4), "launches": int(launches),
+                                    "cell_iter_per_s": float(np.sum(cells * np.array(its)) / dt),
+                                    "iterations_equal_sequential": its == it_seq,
+                                    "states_bitwise_equal_sequential": bool(same)}
+        best = dt if best is None else min(best, dt)
+    out["speedup_vs_sequential"] = round(t_seq / best, 3)
+    return out
+
+
 def cpu_baseline(mesh, flow, c0, rinit, budget_s=15.0):
     """The oracle (FP64 C restatement of the reference, single thread) on this host."""
     from oracle.pyoracle import Oracle
@@ -450,6 +530,7 @@ def main():
     ap.add_argument("--case", default="nozzle_plume_1024x384")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/primal timing")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-case sweep timing")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint/primal timing (K = --steps, W = --warmup), for profiling")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",

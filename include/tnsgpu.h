@@ -264,8 +264,13 @@ int tns_batch_set_active(tns_batch *b, const int *active);
  * the tiles of all active cases; 1 = every case's own tns_run launches, the cases on
  * parallel branches of one CUDA graph so they run concurrently; 2 = as 1, with 8
  * unmonitored iterations per graph so each case runs ahead without a join between
- * iterations.  Results are identical; which is fastest depends on the case mix
- * (tnsgpu.autotune measures them). */
+ * iterations; 3 = one persistent cooperative launch per run of up to 256 unmonitored
+ * iterations, its blocks walking the tile table of all active cases phase by phase with
+ * grid barriers between the phases (monitored iterations as schedule 0); it needs
+ * LOCAL=1 and no type-6 port in every case (TNS_ERR_UNSUPPORTED otherwise), and a grid
+ * barrier that does not complete in its bounded wait ends the run with TNS_ERR_CUDA.
+ * Results are identical; which is fastest depends on the case mix (tnsgpu.autotune
+ * measures them). */
 int tns_batch_set_schedule(tns_batch *b, int schedule);
 int tns_batch_get_schedule(tns_batch *b);
 int tns_batch_get_active(tns_batch *b, int *active);

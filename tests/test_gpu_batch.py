@@ -223,9 +223,9 @@ def test_autotune_batch_picks_a_timed_configuration():
         return out
 
     r = autotune.tune_batch(make, iters=3, warmup=1)
-    assert r["ti"] in (4, 8, 16) and r["schedule"] in (0, 1, 2)
+    assert r["ti"] in (4, 8, 16) and r["schedule"] in (0, 1, 2, 3)
     timed = [t for t in r["trials"] if "s_per_iter" in t]
-    assert len(timed) == 9 and r["s_per_iter"] == min(t["s_per_iter"] for t in timed)
+    assert len(timed) == 12 and r["s_per_iter"] == min(t["s_per_iter"] for t in timed)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -250,3 +250,48 @@ def test_schedule2_iteration_blocks_and_parity_offset(precision):
         np.testing.assert_array_equal(r.records[k], rec, err_msg=name)
         s.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_schedule_equals_solo_runs(precision):
+    """Schedule 3: unmonitored runs of iterations in one cooperative launch (grid
+    barriers between the phases), monitored iterations as schedule 0; members equal
+    their solo runs bit for bit, across calls of odd and even length."""
+    mem = _members(precision, pick=[0, 1, 2, 3])  # LOCAL=1, no port
+    solvers = []
+    for name, mesh, flow, c0, ri in mem:
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        solvers.append(s)
+    b = Batch(solvers, schedule=3)
+    assert b.schedule == 3
+    l0 = b.launch_count()
+    r1 = b.run(37, monitor_every=10)
+    r2 = b.run(4, monitor_every=0)
+    assert list(r1.iterations) == [37] * len(mem) and list(r2.iterations) == [4] * len(mem)
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        (q, prim), rec = _solo(mesh, flow, c0, ri, precision, [37, 4], monitor=10)
+        np.testing.assert_array_equal(solvers[k].download(), q, err_msg=name)
+        np.testing.assert_array_equal(solvers[k].primitives(), prim, err_msg=name)
+        np.testing.assert_array_equal(r1.records[k], rec[0], err_msg=name)
+    # 41 iterations, 3 of them monitored: a handful of persistent launches, not 6 a case
+    assert b.launch_count() - l0 < 40
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+def test_persistent_schedule_refuses_what_it_cannot_run():
+    for pick in ([4], [5]):  # LOCAL=0; a type-6 port
+        mem = _members(0, pick=pick)
+        solvers = []
+        for name, mesh, flow, c0, ri in mem:
+            s = Solver(mesh, flow, ri)
+            s.upload(c0)
+            solvers.append(s)
+        with pytest.raises(_lib.TnsError) as e:
+            Batch(solvers, schedule=3)
+        assert "schedule 3" in str(e.value)
+        for s in solvers:
+            s.close()
+
