@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_
 // reuses the tile's shared memory and barrier.  Cases need LOCAL=1 and no type-6 port
 // (those add per-case reductions between the phases).
 #ifndef TNS_PERSIST_MINB
-#define TNS_PERSIST_MINB 2
+#define TNS_PERSIST_MINB 3
 #endif
 __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_PERSIST_MINB))
 k_batch_persistent(const BatchCase* __restrict__ cases, const int4* __restrict__ tiles,

@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_BATCH_MINB))
 // Persistent batched iterations of the mixed path (schedule 3), as k_batch_persistent:
 // the state parity alternates from `parity` with every iteration.
 #ifndef TNS_PERSIST_MX_MINB
-#define TNS_PERSIST_MX_MINB 2
+#define TNS_PERSIST_MX_MINB 4
 #endif
 __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_PERSIST_MX_MINB))
 k_batch_persistent_mx(const BatchCase* __restrict__ cases, const int4* __restrict__ tiles,

@@ -401,8 +401,10 @@ def batch_timing(niter=200, monitor=100, stop_ratio=1.0e-5, warmup=16, ncases=64
     with a residual record every ``monitor``: the cases one after another through
     tns_run (the stop criterion checked at every record), and the same cases as one
     batch under schedule 2 (per-case graph branches) and schedule 3 (one persistent
-    cooperative launch per run of unmonitored iterations).  Wall time with the device
-    synchronised; the default tile height (no autotuning)."""
+    cooperative launch per run of unmonitored iterations) at the default tile height, and
+    under the tile height and schedule tnsgpu.autotune picks by timing a few iterations
+    of the sweep (its tuning time reported apart).  Wall time with the device
+    synchronised."""
     import numpy as np
     from tnsgpu import cases, formats
     from tnsgpu.batch import Batch
@@ -410,12 +412,12 @@ def batch_timing(niter=200, monitor=100, stop_ratio=1.0e-5, warmup=16, ncases=64
     sw = cases.ramp_sweep(ncases, seed=0)
     cells = np.array([c.nx * c.ny for c in sw], dtype=np.float64)
 
-    def members(solo_warmup):
+    def members(solo_warmup, lib=None):
         out = []
         for c in sw:
             mesh, flow = c.mesh(), c.flow()
             ri = formats.rinit_cold(flow)
-            s = Solver(mesh, flow, ri, precision=1)
+            s = Solver(mesh, flow, ri, precision=1, lib=lib)
             s.upload(formats.cold_state(flow, mesh.neles, ri))
             if solo_warmup:
                 s.run(warmup, 0)
@@ -443,9 +445,16 @@ def batch_timing(niter=200, monitor=100, stop_ratio=1.0e-5, warmup=16, ncases=64
                        f"cold start + {warmup} untimed iterations",
            "cells_total": int(cells.sum()), "niter": niter, "monitor": monitor, "stop_ratio": stop_ratio,
            "sequential_s": round(t_seq, 4), "sequential_cell_iter_per_s": float(np.sum(cells * it_seq) / t_seq)}
+    from tnsgpu import autotune
+    t0 = time.perf_counter()
+    choice = autotune.tune_batch(lambda lib: members(False, lib), iters=20, warmup=8)
+    out["tuned"] = {"ti": choice["ti"], "schedule": choice["schedule"], "tuning_s": round(time.perf_counter() - t0, 2),
+                    "trials": [{k: (round(v, 7) if isinstance(v, float) else v) for k, v in t.items()}
+                               for t in choice["trials"]]}
     best = None
-    for sched in (2, 3):
-        bat = members(False)
+    arms = [(2, None, "schedule_2"), (3, None, "schedule_3"), (choice["schedule"], choice["lib"], "tuned_run")]
+    for sched, lib, key in arms:
+        bat = members(False, lib)
         b = Batch(bat, schedule=sched)
         # the warm-up on the batch itself captures this schedule's graphs (monitored and
         # not, both state parities) and leaves every case where the sequential arm began
@@ -456,14 +465,16 @@ def batch_timing(niter=200, monitor=100, stop_ratio=1.0e-5, warmup=16, ncases=64
         dt = time.perf_counter() - t0
         launches = b.launch_count() - l0
         b.close()
-        same = all(np.array_equal(s.download(), q) for s, q in zip(bat, q_seq))
+        qb = [s.download() for s in bat]
+        same = all(np.array_equal(a, q) for a, q in zip(qb, q_seq))
+        diff = max(float(np.max(np.max(np.abs(a - q), axis=1) / np.max(np.abs(q), axis=1))) for a, q in zip(qb, q_seq))
         its = [int(v) for v in r.iterations]
         for s in bat:
             s.close()
-        out[f"schedule_{sched}"] = {"s": round(dt, 4), "launches": int(launches),
-                                    "cell_iter_per_s": float(np.sum(cells * np.array(its)) / dt),
-                                    "iterations_equal_sequential": its == it_seq,
-                                    "states_bitwise_equal_sequential": bool(same)}
+        out[key] = {"schedule": sched, "s": round(dt, 4), "launches": int(launches),
+                    "cell_iter_per_s": float(np.sum(cells * np.array(its)) / dt),
+                    "iterations_equal_sequential": its == it_seq,
+                    "states_bitwise_equal_sequential": bool(same), "state_rel_diff_max": diff}
         best = dt if best is None else min(best, dt)
     out["speedup_vs_sequential"] = round(t_seq / best, 3)
     return out
