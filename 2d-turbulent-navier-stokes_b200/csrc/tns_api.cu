@@ -852,27 +852,66 @@ int tns_node_averages(tns_handle* h, double* pn, double* un, double* vn, double*
     return TNS_OK;
 }
 
-int tns_boundary_integrals(tns_handle* h, int type, int side, double out[4]) {
-    if (!h || !out || type < 0 || type > 7 || side < 0 || side > 4) return TNS_ERR_ARG;
-    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_boundary_integrals: no iteration has run");
+}  // extern "C"
+
+namespace {
+// Boundary-face sums (mode 0: out[4]; mode 1: out[2]) of the last stage's state.
+int boundary_sums(tns_handle* h, int type, int side, int mode, double* out, int nout) {
     int rc;
     DevBuf<double> acc;
     if ((rc = h->cuda(acc.alloc(4), "cudaMalloc"))) return rc;
     cudaMemsetAsync(acc.p, 0, 4 * sizeof(double), h->stream);
     if (h->unstructured) {
-        rc = tns_rt::umesh_boundary_sums(h, type, side, acc.p);
+        rc = tns_rt::umesh_boundary_sums(h, type, side, mode, acc.p);
     } else if (!(rc = fill_primitives(h))) {
-        tns::launch_boundary_sums(h->P, h->M, h->primout.p, type, side, acc.p, h->stream);
+        tns::launch_boundary_sums(h->P, h->M, h->primout.p, type, side, mode, acc.p, h->stream);
     }
-    if (rc) {
-        acc.release();
-        return rc;
-    }
-    rc = h->cuda(cudaMemcpyAsync(out, acc.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
-                 "cudaMemcpyAsync");
+    if (!rc)
+        rc = h->cuda(cudaMemcpyAsync(out, acc.p, nout * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                     "cudaMemcpyAsync");
     if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     acc.release();
     return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int tns_boundary_integrals(tns_handle* h, int type, int side, double out[4]) {
+    if (!h || !out || type < 0 || type > 7 || side < 0 || side > 4) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_boundary_integrals: no iteration has run");
+    return boundary_sums(h, type, side, 0, out, 4);
+}
+
+int tns_total_pressure_sums(tns_handle* h, int type, int side, double out[2]) {
+    if (!h || !out || type < 0 || type > 7 || side < 0 || side > 4) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_total_pressure_sums: no iteration has run");
+    return boundary_sums(h, type, side, 1, out, 2);
+}
+
+int tns_boundary_face_states(tns_handle* h, double* out) {
+    if (!h || !out) return TNS_ERR_ARG;
+    if (!h->have_run) return h->fail(TNS_ERR_STATE, "tns_boundary_face_states: no iteration has run");
+    const size_t ng = (size_t)h->nghosts;
+    if (ng == 0) return TNS_OK;
+    int rc;
+    DevBuf<double> dv;
+    if ((rc = h->cuda(dv.alloc(5 * ng), "cudaMalloc"))) return rc;
+    if (h->unstructured) {
+        rc = tns_rt::umesh_face_states(h, dv.p);
+    } else if (!(rc = fill_primitives(h))) {
+        tns::launch_face_states(h->P, h->M, h->primout.p, dv.p, h->stream);
+    }
+    std::vector<double> hb(5 * ng);
+    if (!rc)
+        rc = h->cuda(cudaMemcpyAsync(hb.data(), dv.p, 5 * ng * 8, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+    if (!rc) rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    dv.release();
+    if (rc) return rc;
+    // device ghost order -> bc.in line order
+    for (int f = 0; f < 5; f++)
+        for (size_t g = 0; g < ng; g++) out[f * ng + h->ghost_line[g]] = hb[f * ng + g];
+    return TNS_OK;
 }
 
 int tns_debug_fetch(tns_handle* h, int which, double* out) {

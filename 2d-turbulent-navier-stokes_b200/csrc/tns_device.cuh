@@ -399,6 +399,30 @@ struct FaceIn {
     double rhoa, rhob, rhoc, rhod, ra, rb, rc, rd;
 };
 
+// Sums of one boundary face with the face state (parent + ghost)/2 (U, V averaged; T, P
+// of both sides).  mode 0: v = P*SX, P*SY, RHO*(U*SX+V*SY), |S|; mode 1: v[0] = P0*|MDOT|,
+// v[1] = |MDOT| with the face's total pressure P0 = P (1 + (GAMA-1)/2 M^2)^(GAMA/(GAMA-1)),
+// M^2 = (U^2+V^2)/(GAMA RR T) and mass flux MDOT = RHO (U SX + V SY); RHO is the average of
+// P/(RR*T) on both sides.
+__device__ __forceinline__ void face_sums(const Params& P, int mode, double u, double vv, double tp, double tg,
+                                          double pp, double pg, double sx, double sy, double v[4]) {
+    const double pf = 0.5 * (pp + pg);
+    const double rho = 0.5 * (pp / (P.rr * tp) + pg / (P.rr * tg));
+    if (mode == 1) {
+        const double tf = 0.5 * (tp + tg);
+        const double m2 = (u * u + vv * vv) / (P.gama * P.rr * tf);
+        const double p0 = pf * pow(1.0 + 0.5 * (P.gama - 1.0) * m2, P.gama / (P.gama - 1.0));
+        const double md = fabs(rho * (u * sx + vv * sy));
+        v[0] = p0 * md;
+        v[1] = md;
+        return;
+    }
+    v[0] = pf * sx;
+    v[1] = pf * sy;
+    v[2] = rho * (u * sx + vv * sy);
+    v[3] = sqrt(sx * sx + sy * sy);
+}
+
 // One face from its stored geometry (FG_*): the flux of viscous.f90:130-217 with the
 // diamond gradient from the coefficients.  Assigns vis[0..3].
 struct FaceVals {

@@ -704,10 +704,12 @@ __global__ void k_node_average(Mesh M, const double* __restrict__ prim, double* 
 }
 
 // Boundary-face sums over the ghosts whose BC type / side match (0 = any), with the face
-// state (parent + ghost)/2: [0] sum P*SX, [1] sum P*SY, [2] sum RHO*(U*SX+V*SY),
-// [3] sum |S|.  One warp per 32 faces; one atomicAdd per warp and quantity.
+// state (parent + ghost)/2.  mode 0: [0] sum P*SX, [1] sum P*SY, [2] sum RHO*(U*SX+V*SY),
+// [3] sum |S|; mode 1: [0] sum P0*|MDOT|, [1] sum |MDOT| with the face's total pressure
+// P0 = P (1 + (GAMA-1)/2 M^2)^(GAMA/(GAMA-1)), M^2 = (U^2+V^2)/(GAMA RR T), and mass flux
+// MDOT = RHO (U SX + V SY).  One warp per 32 faces; one atomicAdd per warp and quantity.
 __global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ prim, int type,
-                                int side, double* __restrict__ out) {
+                                int side, int mode, double* __restrict__ out) {
     const size_t ncell = (size_t)M.ni * M.nj, ntot = ncell + M.nghosts();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -730,14 +732,8 @@ __global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ pri
             double sx, sy;
             face_vector(P.iaxis, sd, X, Y, sx, sy);
             const double u = 0.5 * (prim[cp] + prim[cg]), vv = 0.5 * (prim[ntot + cp] + prim[ntot + cg]);
-            const double tp = prim[2 * ntot + cp], tg = prim[2 * ntot + cg];
-            const double pp = prim[3 * ntot + cp], pg = prim[3 * ntot + cg];
-            const double pf = 0.5 * (pp + pg);
-            const double rho = 0.5 * (pp / (P.rr * tp) + pg / (P.rr * tg));
-            v[0] = pf * sx;
-            v[1] = pf * sy;
-            v[2] = rho * (u * sx + vv * sy);
-            v[3] = sqrt(sx * sx + sy * sy);
+            face_sums(P, mode, u, vv, prim[2 * ntot + cp], prim[2 * ntot + cg], prim[3 * ntot + cp],
+                      prim[3 * ntot + cg], sx, sy, v);
         }
     }
 #pragma unroll
@@ -746,6 +742,36 @@ __global__ void k_boundary_sums(Params P, Mesh M, const double* __restrict__ pri
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
         if ((threadIdx.x & 31) == 0 && x != 0.0) atomicAdd(&out[q], x);
     }
+}
+
+// Face state (parent + ghost)/2 of every ghost in device order: out [5][nghosts] = U, V,
+// P, RHO (the average of P/(RR*T) on both sides), T.
+__global__ void k_face_states(Params P, Mesh M, const double* __restrict__ prim, double* __restrict__ out) {
+    const size_t ncell = (size_t)M.ni * M.nj, ng = M.nghosts(), ntot = ncell + ng;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (int)ng) return;
+    int sd, along;
+    if (g < M.ni) { sd = 1; along = g; }
+    else if (g < M.ni + M.nj) { sd = 2; along = g - M.ni; }
+    else if (g < 2 * M.ni + M.nj) { sd = 3; along = g - M.ni - M.nj; }
+    else { sd = 4; along = g - 2 * M.ni - M.nj; }
+    int ip, jp;
+    if (sd == 1) { ip = along; jp = 0; }
+    else if (sd == 2) { ip = M.ni - 1; jp = along; }
+    else if (sd == 3) { ip = along; jp = M.nj - 1; }
+    else { ip = 0; jp = along; }
+    const size_t cp = (size_t)ip * M.nj + jp, cg = ncell + g;
+    const double tp = prim[2 * ntot + cp], tgh = prim[2 * ntot + cg];
+    const double pp = prim[3 * ntot + cp], pgh = prim[3 * ntot + cg];
+    out[g] = 0.5 * (prim[cp] + prim[cg]);
+    out[ng + g] = 0.5 * (prim[ntot + cp] + prim[ntot + cg]);
+    out[2 * ng + g] = 0.5 * (pp + pgh);
+    out[3 * ng + g] = 0.5 * (pp / (P.rr * tp) + pgh / (P.rr * tgh));
+    out[4 * ng + g] = 0.5 * (tp + tgh);
+}
+
+void launch_face_states(const Params& P, const Mesh& M, const double* prim, double* out, cudaStream_t s) {
+    k_face_states<<<(M.nghosts() + 255) / 256, 256, 0, s>>>(P, M, prim, out);
 }
 
 // ------------------------------------------------------------ batched kernels
@@ -950,8 +976,8 @@ void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStr
 }
 
 void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
-                          double* out, cudaStream_t s) {
-    k_boundary_sums<<<(M.nghosts() + 255) / 256, 256, 0, s>>>(P, M, prim, type, side, out);
+                          int mode, double* out, cudaStream_t s) {
+    k_boundary_sums<<<(M.nghosts() + 255) / 256, 256, 0, s>>>(P, M, prim, type, side, mode, out);
 }
 
 void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* out,

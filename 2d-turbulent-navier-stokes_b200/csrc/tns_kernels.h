@@ -35,8 +35,10 @@ void launch_prim_out(const Params& P, const Mesh& M, const double* q, double* ou
                      cudaStream_t s);
 
 void launch_node_average(const Mesh& M, const double* prim, double* out, cudaStream_t s);
+// mode 0: force / mass flow / area sums (out[4]); mode 1: total-pressure sums (out[2])
 void launch_boundary_sums(const Params& P, const Mesh& M, const double* prim, int type, int side,
-                          double* out, cudaStream_t s);
+                          int mode, double* out, cudaStream_t s);
+void launch_face_states(const Params& P, const Mesh& M, const double* prim, double* out, cudaStream_t s);
 
 // accuracy check of the FP64 helpers (fn 0 = pow06, 1 = tanh_ratio)
 void launch_debug_math(int fn, long long n, const double* a, const double* b, double* out, cudaStream_t s);

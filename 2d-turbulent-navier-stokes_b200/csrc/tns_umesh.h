@@ -81,7 +81,8 @@ void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaSt
 void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s);
 void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_t s);
 void launch_u_boundary_sums(const Params& P, const UMesh& M, const double* W, int type, int side,
-                            double* out, cudaStream_t s);
+                            int mode, double* out, cudaStream_t s);
+void launch_u_face_states(const Params& P, const UMesh& M, const double* W, double* out, cudaStream_t s);
 
 }  // namespace tns
 
@@ -95,7 +96,8 @@ void enqueue_iteration_u(tns_handle* h, bool monitor);
 // slot order)
 int umesh_primitives(tns_handle* h);
 int umesh_node_averages(tns_handle* h, double* dev_out);  // [4][nnode]: P, U, V, T
-int umesh_boundary_sums(tns_handle* h, int type, int side, double* dev_out);
+int umesh_boundary_sums(tns_handle* h, int type, int side, int mode, double* dev_out);
+int umesh_face_states(tns_handle* h, double* dev_out);  // [5][ng], bc.in order
 int umesh_set_injection(tns_handle* h, const double* scale);
 void umesh_release(tns_handle* h);
 }  // namespace tns_rt

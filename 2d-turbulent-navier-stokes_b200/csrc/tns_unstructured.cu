@@ -371,8 +371,24 @@ __global__ void __launch_bounds__(UT) k_u_prim_out(UMesh M, const double* __rest
 
 // Boundary-face sums over the ghosts whose BC type / side match (0 = any), with the face
 // state (parent + ghost)/2, as k_boundary_sums.
+// Face state (parent + ghost)/2 of every ghost (bc.in order): out [5][ng] = U, V, P, RHO, T.
+__global__ void __launch_bounds__(UT) k_u_face_states(Params P, UMesh M, const double* __restrict__ W,
+                                                      double* __restrict__ out) {
+    const int L = blockIdx.x * UT + threadIdx.x;
+    if (L >= M.ng) return;
+    const size_t ns = (size_t)M.ne + M.ng, ng = (size_t)M.ng;
+    const size_t cp = (size_t)M.gpar[L], cg = (size_t)M.ne + L;
+    const double tp = W[UW_T * ns + cp], tgh = W[UW_T * ns + cg];
+    const double pp = W[UW_P * ns + cp], pgh = W[UW_P * ns + cg];
+    out[L] = 0.5 * (W[UW_U * ns + cp] + W[UW_U * ns + cg]);
+    out[ng + L] = 0.5 * (W[UW_V * ns + cp] + W[UW_V * ns + cg]);
+    out[2 * ng + L] = 0.5 * (pp + pgh);
+    out[3 * ng + L] = 0.5 * (pp / (P.rr * tp) + pgh / (P.rr * tgh));
+    out[4 * ng + L] = 0.5 * (tp + tgh);
+}
+
 __global__ void __launch_bounds__(UT) k_u_bsums(Params P, UMesh M, const double* __restrict__ W, int type,
-                                                int side, double* __restrict__ out) {
+                                                int side, int mode, double* __restrict__ out) {
     const int L = blockIdx.x * UT + threadIdx.x;
     const size_t ns = (size_t)M.ne + M.ng;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -381,14 +397,8 @@ __global__ void __launch_bounds__(UT) k_u_bsums(Params P, UMesh M, const double*
         const double sx = M.gsx[L], sy = M.gsy[L];
         const double u = 0.5 * (W[UW_U * ns + cp] + W[UW_U * ns + cg]);
         const double vv = 0.5 * (W[UW_V * ns + cp] + W[UW_V * ns + cg]);
-        const double tp = W[UW_T * ns + cp], tg = W[UW_T * ns + cg];
-        const double pp = W[UW_P * ns + cp], pg = W[UW_P * ns + cg];
-        const double pf = 0.5 * (pp + pg);
-        const double rho = 0.5 * (pp / (P.rr * tp) + pg / (P.rr * tg));
-        v[0] = pf * sx;
-        v[1] = pf * sy;
-        v[2] = rho * (u * sx + vv * sy);
-        v[3] = sqrt(sx * sx + sy * sy);
+        face_sums(P, mode, u, vv, W[UW_T * ns + cp], W[UW_T * ns + cg], W[UW_P * ns + cp], W[UW_P * ns + cg], sx,
+                  sy, v);
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -426,8 +436,11 @@ void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_
     k_u_prim_out<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(M, W, out);
 }
 void launch_u_boundary_sums(const Params& P, const UMesh& M, const double* W, int type, int side,
-                            double* out, cudaStream_t s) {
-    if (M.ng > 0) k_u_bsums<<<blocks(M.ng), UT, 0, s>>>(P, M, W, type, side, out);
+                            int mode, double* out, cudaStream_t s) {
+    if (M.ng > 0) k_u_bsums<<<blocks(M.ng), UT, 0, s>>>(P, M, W, type, side, mode, out);
+}
+void launch_u_face_states(const Params& P, const UMesh& M, const double* W, double* out, cudaStream_t s) {
+    if (M.ng > 0) k_u_face_states<<<blocks(M.ng), UT, 0, s>>>(P, M, W, out);
 }
 
 }  // namespace tns
@@ -797,11 +810,19 @@ int umesh_node_averages(tns_handle* h, double* dev_out) {
     return h->cuda(cudaGetLastError(), "kernel launch");
 }
 
-int umesh_boundary_sums(tns_handle* h, int type, int side, double* dev_out) {
+int umesh_boundary_sums(tns_handle* h, int type, int side, int mode, double* dev_out) {
     tns_umesh_state* u = h->umesh;
     int rc;
     if ((rc = umesh_primitives(h))) return rc;
-    tns::launch_u_boundary_sums(h->P, u->M, u->W.p, type, side, dev_out, h->stream);
+    tns::launch_u_boundary_sums(h->P, u->M, u->W.p, type, side, mode, dev_out, h->stream);
+    return h->cuda(cudaGetLastError(), "kernel launch");
+}
+
+int umesh_face_states(tns_handle* h, double* dev_out) {
+    tns_umesh_state* u = h->umesh;
+    int rc;
+    if ((rc = umesh_primitives(h))) return rc;
+    tns::launch_u_face_states(h->P, u->M, u->W.p, dev_out, h->stream);
     return h->cuda(cudaGetLastError(), "kernel launch");
 }
 

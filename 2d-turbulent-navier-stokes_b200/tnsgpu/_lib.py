@@ -37,7 +37,7 @@ EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run
            "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
-           "tns_boundary_integrals", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
+           "tns_boundary_integrals", "tns_total_pressure_sums", "tns_boundary_face_states", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
            "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule",
            "tns_batch_launch_count", "tns_debug_math", "tns_batch_last_error", "tns_batch_destroy",
            "tns_adjoint_enable", "tns_adjoint_step", "tns_adjoint_step_next", "tns_adjoint_sensitivity_size",
@@ -92,6 +92,8 @@ def load(path: str = None):
     L.tns_debug_fetch.argtypes = [vp, ip, dp]
     L.tns_node_averages.argtypes = [vp, dp, dp, dp, dp]
     L.tns_boundary_integrals.argtypes = [vp, ip, ip, dp]
+    L.tns_total_pressure_sums.argtypes = [vp, ip, ip, dp]
+    L.tns_boundary_face_states.argtypes = [vp, dp]
     L.tns_set_stream.argtypes = [vp, vp]
     L.tns_profile.argtypes = [vp, ip]
     L.tns_kernel_times.argtypes = [vp, ip, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]

@@ -132,6 +132,31 @@ class Solver:
         self._check(self.L.tns_boundary_integrals(self.h, int(btype), int(side), out.ctypes.data))
         return out
 
+    def total_pressure_sums(self, btype: int = 0, side: int = 0) -> np.ndarray:
+        """[sum P0*|MDOT|, sum |MDOT|] over the matching boundary faces (on the GPU)."""
+        out = np.zeros(2)
+        self._check(self.L.tns_total_pressure_sums(self.h, int(btype), int(side), out.ctypes.data))
+        return out
+
+    def total_pressure_loss(self, inlet=(0, 4), outlet=(0, 2)) -> float:
+        """1 - (mass-weighted outlet total pressure) / (mass-weighted inlet total pressure),
+        the face sets given as (BC type, side), 0 = any."""
+        i, o = self.total_pressure_sums(*inlet), self.total_pressure_sums(*outlet)
+        return float(1.0 - (o[0] / o[1]) / (i[0] / i[1]))
+
+    def boundary_face_states(self) -> np.ndarray:
+        """[5, NGHOSTS] U, V, P, RHO, T of every boundary face in bc.in order (on the GPU)."""
+        out = np.zeros((5, self.mesh.nghosts))
+        self._check(self.L.tns_boundary_face_states(self.h, out.ctypes.data))
+        return out
+
+    def wall_pressure(self, wall_type: int = 5, side: Optional[int] = None) -> np.ndarray:
+        """Face pressure of the faces of BC ``wall_type`` (and ``side``), in bc.in order."""
+        sel = self.mesh.ntype == wall_type
+        if side is not None:
+            sel &= self.mesh.nside == side
+        return self.boundary_face_states()[2][sel]
+
     def debug(self, which: int) -> np.ndarray:
         cnt = {0: 5, 1: 4, 2: 1}[which]
         out = np.zeros((cnt, self.mesh.neles))

@@ -115,6 +115,20 @@ int tns_node_averages(tns_handle *h, double *pn, double *un, double *vn, double 
  * counterpart (THRUST is declared in solver_state.f90:40 but never computed). */
 int tns_boundary_integrals(tns_handle *h, int type, int side, double out[4]);
 
+/* Mass-weighted total pressure over the same faces (NTYPE == type, NSIDE == side, 0 =
+ * any), on the GPU: out[0] = sum P0*|MDOT|, out[1] = sum |MDOT| with the face's total
+ * pressure P0 = P (1 + (GAMA-1)/2 M^2)^(GAMA/(GAMA-1)), M^2 = (U^2+V^2)/(GAMA RR T) and
+ * mass flux MDOT = RHO (U SX + V SY) of the face state above.  The total-pressure loss
+ * between an inlet and an outlet face set is 1 - (o[0]/o[1]) / (i[0]/i[1]).  No
+ * reference counterpart (an objective of the discrete adjoint). */
+int tns_total_pressure_sums(tns_handle *h, int type, int side, double out[2]);
+
+/* The face state of every boundary face, in bc.in order, computed on the GPU: out
+ * [5][NGHOSTS] = U, V, P, RHO, T of (parent + ghost)/2 of the last stage (RHO the average
+ * of P/(RR*T) on both sides).  The wall pressure distribution is out[2] on the wall
+ * lines.  No reference counterpart. */
+int tns_boundary_face_states(tns_handle *h, double *out);
+
 /* Frozen terms of the last iteration, for checking: which = 0: D241..D245 (5 arrays),
  * 1: VISU, VISV, VIST, VISR (4), 2: DT (1).  out holds count*NELES doubles, cell order
  * 1..NELES per array. */

@@ -46,3 +46,52 @@ def _force_any(mesh, prims, flow, side):
     sx, sy, _, _ = objectives.face_vectors(mesh, flow.iaxis)
     sel = np.ones(mesh.nghosts, bool) if side is None else mesh.nside == side
     return np.sum(pf[sel] * sx[sel]), np.sum(pf[sel] * sy[sel])
+
+
+def _host_tp_sums(mesh, prims, flow, sel):
+    """Host restatement of tns_total_pressure_sums over the bc.in lines ``sel``."""
+    uf, vf, pf, rhof, tf = objectives._face_state(mesh, prims, flow.amol)
+    sx, sy, _, _ = objectives.face_vectors(mesh, flow.iaxis)
+    rr = objectives.RUNIV / flow.amol
+    g = flow.gama
+    m2 = (uf * uf + vf * vf) / (g * rr * tf)
+    p0 = pf * (1.0 + 0.5 * (g - 1.0) * m2) ** (g / (g - 1.0))
+    md = np.abs(rhof * (uf * sx + vf * sy))
+    return np.array([np.sum((p0 * md)[sel]), np.sum(md[sel])])
+
+
+@pytest.mark.parametrize("kind", ["nozzle2d", "plume_axi", "backstep_general"])
+def test_face_states_and_total_pressure_loss_on_the_gpu(kind):
+    """tns_boundary_face_states (the wall pressure distribution) and
+    tns_total_pressure_sums (the total-pressure loss objective) against the host
+    objectives on the same downloaded primitives, on a structured 2-D channel, an
+    axisymmetric mesh and a general (three-block) mesh."""
+    if kind == "nozzle2d":
+        mesh, flow = cases.nozzle_2d_mesh(30, 14), cases.nozzle_2d_flow()
+    elif kind == "plume_axi":
+        mesh, flow = cases.nozzle_plume_mesh(48, 20), cases.nozzle_plume_flow()
+        mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    else:
+        mesh, flow = cases.backstep_mesh(16, 48, 12, 6), cases.ramp_flow()
+        flow.istart = 0
+    ri = formats.rinit_cold(flow)
+    s = Solver(mesh, flow, ri)
+    s.upload(formats.cold_state(flow, mesh.neles, ri))
+    s.run(60, 0)
+    prims = s.primitives()
+    fs = s.boundary_face_states()
+    ref = np.stack(objectives._face_state(mesh, prims, flow.amol))  # U, V, P, RHO, T
+    for k in range(5):
+        assert np.max(np.abs(fs[k] - ref[k])) <= 1e-13 * np.max(np.abs(ref[k])) + 1e-300, k
+    walls = mesh.ntype == 5
+    assert np.array_equal(s.wall_pressure(5), fs[2][walls])
+    # inlet = the type-2 faces, outlet = the type-3 faces (valid on any numbering)
+    for btype in (2, 3):
+        got = s.total_pressure_sums(btype, 0)
+        want = _host_tp_sums(mesh, prims, flow, mesh.ntype == btype)
+        assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want)), (btype, got, want)
+    loss = s.total_pressure_loss((2, 0), (3, 0))
+    i, o = _host_tp_sums(mesh, prims, flow, mesh.ntype == 2), _host_tp_sums(mesh, prims, flow, mesh.ntype == 3)
+    want = 1.0 - (o[0] / o[1]) / (i[0] / i[1])
+    assert abs(loss - want) <= 1e-10 * max(abs(want), 1e-12), (loss, want)
+    s.close()
