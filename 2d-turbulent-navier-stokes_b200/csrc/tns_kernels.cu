@@ -11,7 +11,10 @@
 //   [k_gport]      type-6 port mass flux of the stage input (only if such ghosts exist)
 // Ghost cells are never stored: each tile evaluates the BC of the ghosts in its halo
 // from the parent and the parent's opposite neighbour, both already in the tile.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <cstring>
 
 #include "tns_device.cuh"
 #include "tns_kernels.h"
@@ -23,33 +26,65 @@ namespace tns {
 // ------------------------------------------------------------------ stage kernel
 
 // Shared-memory fields of the stage tile, paired for 16-byte loads; the tile's static
-// block (nodes, gradient coefficients, 1/VOL, 1/YCC) arrives by one bulk copy.
-struct StageSmem {
-    double st[STILE];      // static block (tns_tile.cuh)
-    double2 fg[5][NSLOT];  // (F_m, G_m)
-    double2 uv[NSLOT];     // (U, V)
-    double2 rq[NSLOT];     // (C5/C1, |V|)
-    double2 tp[NSLOT];     // (T, P)
-    double rho[NSLOT];
-    unsigned long long bar;  // completion of the static block's copy
+// block (nodes, gradient coefficients, 1/VOL, 1/YCC) arrives by one bulk copy.  The TMA
+// variant also receives the five Q planes of the tile's halo box by one tiled tensor
+// copy: rows i0-1 .. i0+TI, columns j0-2 .. j0+TJ+1 (the box starts one column early so
+// that its first column is a multiple of 16 bytes; out-of-mesh positions arrive as
+// zeros), and reads RHO of its cells from there.
+// Off by default: measured on 1024 x 384 (B200, FP64), the TMA variant took 157-159 us
+// for a RK4 iteration's four stage launches against 145 us with plain loads (same
+// results bit for bit).  A block waits for its whole box before its first slot, where
+// plain loads let each warp start as its own rows arrive.
+#ifndef TNS_STAGE_TMA
+#define TNS_STAGE_TMA 0
+#endif
+// Three blocks of the TMA variant fit an SM at TI >= 8 (at TI = 4 its box would cost the
+// sixth block).
+#define TNS_STAGE_TMA_ON (TNS_STAGE_TMA && TNS_TI >= 8)
+constexpr int QH = TI + 2, QW = TJ + 4;
+static_assert(QW % 2 == 0, "the Q box rows must be a multiple of 16 bytes");
+
+template <bool TMA>
+struct StageSmemT {
+    double qs[TMA ? 5 * QH * QW : 2];  // (TMA) Q planes [5][QH][QW], 128-byte aligned
+    double st[STILE];                  // static block (tns_tile.cuh)
+    double2 fg[5][NSLOT];              // (F_m, G_m)
+    double2 uv[NSLOT];                 // (U, V)
+    double2 rq[NSLOT];                 // (C5/C1, |V|)
+    double2 tp[NSLOT];                 // (T, P)
+    double rho[TMA ? 2 : NSLOT];
+    unsigned long long bar;   // completion of the static block's copy
+    unsigned long long qbar;  // (TMA) completion of the Q box
 };
+using StageSmem = StageSmemT<false>;
+static_assert(sizeof(double) * 5 * QH * QW % 16 == 0, "the static block follows the Q box at 16 bytes");
 
 size_t stage_smem_bytes() { return sizeof(StageSmem); }
+#if TNS_STAGE_TMA_ON
+// (+128: the kernel aligns the Q box to 128 bytes inside its dynamic shared memory)
+static size_t stage_tma_smem_bytes() { return sizeof(StageSmemT<true>) + 128; }
+#endif
 
-__device__ __forceinline__ void put_slot(StageSmem& S, int s, const Prim& p) {
+template <bool TMA>
+__device__ __forceinline__ void put_slot(StageSmemT<TMA>& S, int s, const Prim& p) {
 #pragma unroll
     for (int m = 0; m < 5; m++) S.fg[m][s] = make_double2(p.f[m], p.g[m]);
     S.uv[s] = make_double2(p.u, p.v);
     S.rq[s] = make_double2(p.ri, p.qm);
     S.tp[s] = make_double2(p.t, p.p);
-    S.rho[s] = p.rho;
+    if (!TMA) S.rho[s] = p.rho;
 }
 
 // One RK stage (turbnstwod.f90:204-227, boundary.f90:24-48, source_terms.f90:24-104,
 // residual.f90:23-83) on a TI x TJ tile with its halo staged in shared memory.
-__device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const StageArgs& A, int bx, int by) {
+// TMA: qmap is the tensor map of A.qin ([5][NI][NJ] doubles, box [5][QH][QW]).
+template <bool TMA>
+__device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const StageArgs& A, int bx, int by,
+                                           const CUtensorMap* qmap = nullptr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    unsigned char* base = smem_raw;
+    if (TMA) base += (128u - ((unsigned)__cvta_generic_to_shared(smem_raw) & 127u)) & 127u;
+    StageSmemT<TMA>& S = *reinterpret_cast<StageSmemT<TMA>*>(base);
     const size_t ncell = (size_t)M.ni * M.nj;
     const int j0 = bx * TJ, i0 = by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
@@ -57,21 +92,43 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
     // the static block is written by nothing: its copy overlaps the previous kernel's tail
     if (tid == 0) {
         bulk_barrier_init(&S.bar);
+        if (TMA) bulk_barrier_init(&S.qbar);
         const size_t tile = (size_t)by * ((M.nj + TJ - 1) / TJ) + bx;
         bulk_copy_start(S.st, M.stile + tile * STILE, STILE * sizeof(double), &S.bar);
     }
     pdl_wait();
+    if (TMA && tid == 0)
+        tensor_copy_3d_start(S.qs, qmap, j0 - 2, i0 - 1, 0, (unsigned)(sizeof(double) * 5 * QH * QW), &S.qbar);
     __syncthreads();
+    if (TMA) {
+        // a block-uniform decision: every thread leaves, or none
+        const bool ok = bulk_wait(&S.qbar);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(A.error, 2u);
+            bulk_wait(&S.qbar);
+            bulk_wait(&S.bar);
+            return;
+        }
+    }
+    // primitives of a cell of the Q box, by mesh position
+    auto box_prim = [&](int ci, int cj, Prim& q) {
+        const double* b = S.qs + (ci - i0 + 1) * QW + (cj - j0 + 2);
+        primitive(P, b[0], b[QH * QW], b[2 * QH * QW], b[3 * QH * QW], b[4 * QH * QW], q);
+    };
     for (int s = tid; s < NSLOT; s += NTHREADS) {
         const int li = s / SW, lj = s % SW;
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
         Prim p;
-        if (kind == 0)
+        if (TMA) {
+            if (kind == 0) box_prim(i0 - 1 + li, j0 - 1 + lj, p);
+            else ghost_state_at(P, M, kind, along, box_prim, p);
+        } else if (kind == 0) {
             cell_prim(P, A.qin, ncell, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-        else
+        } else {
             ghost_state(P, M, A.qin, ncell, kind, along, p);
+        }
         put_slot(S, s, p);
     }
     __syncthreads();
@@ -111,7 +168,8 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
             s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
             const double2 tp = S.tp[c];
             const double YCCI = (Y0[n1] + Y0[n1 + SNW] + Y0[n1 + SNW + 1] + Y0[n1 + 1]) * 0.25;
-            source_terms(P, s, S.rho[c], S.rq[c].x, tp.x, tp.y, S.uv[c].y, YCCI,
+            const double RHOC = TMA ? S.qs[(ti + 1) * QW + tj + 2] : S.rho[c];
+            source_terms(P, s, RHOC, S.rq[c].x, tp.x, tp.y, S.uv[c].y, YCCI,
                          S.st[gc + ST_RYCC * NTHREADS], src3, src5);
         }
 
@@ -178,11 +236,12 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
 
 // Specialised on the residual monitor, so the CDIFF reduction is compiled only where it
 // runs.
-template <int MONITOR>
-__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MINB)) k_stage(Params P, Mesh M, StageArgs A) {
+template <int MONITOR, bool TMA>
+__global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MINB))
+k_stage(Params P, Mesh M, StageArgs A, const __grid_constant__ CUtensorMap qmap) {
     StageArgs Ac = A;
     if (!MONITOR) Ac.cdiff = nullptr;
-    stage_tile(P, M, Ac, blockIdx.x, blockIdx.y);
+    stage_tile<TMA>(P, M, Ac, blockIdx.x, blockIdx.y, &qmap);
 }
 
 // ---------------------------------------------------------------- viscous kernel
@@ -803,7 +862,7 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_
     const int4 t = tiles[blockIdx.x];
     if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
-    stage_tile(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
+    stage_tile<false>(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
 }
 
 // Persistent batched iterations (schedule 3): one cooperative launch advances every
@@ -830,7 +889,7 @@ k_batch_persistent(const BatchCase* __restrict__ cases, const int4* __restrict__
                     const BatchCase& c = cases[t.x];
                     if (ph == 0 && w < ntiles) dissipation_tile<double>(c.P, c.M, c.diss, t.y, t.z);
                     else if (ph == 0) viscous_tile(c.P, c.M, c.q, c.vis, t.y, t.z);
-                    else stage_tile(c.P, c.M, c.stage[0][ph - 1], t.y, t.z);
+                    else stage_tile<false>(c.P, c.M, c.stage[0][ph - 1], t.y, t.z);
                 }
                 __syncthreads();
             }
@@ -862,14 +921,53 @@ void launch_debug_math(int fn, long long n, const double* a, const double* b, do
 
 static dim3 tile_grid(const Mesh& M) { return dim3((M.nj + TJ - 1) / TJ, (M.ni + TI - 1) / TI); }
 
+#if TNS_STAGE_TMA_ON
+// The driver's tensor-map encoder, looked up once through the runtime.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of a state array [5][NI][NJ] for the stage's Q box; false (the caller takes
+// the plain-load kernel) where TMA cannot address it: NJ odd (rows not a multiple of 16
+// bytes) or the array not 16-byte aligned.
+static bool stage_q_map(const Mesh& M, const double* q, CUtensorMap* map) {
+    if (M.nj % 2 != 0 || (reinterpret_cast<uintptr_t>(q) & 15) != 0) return false;
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)M.nj, (cuuint64_t)M.ni, 5};
+    const cuuint64_t strides[2] = {(cuuint64_t)M.nj * sizeof(double), (cuuint64_t)M.ni * M.nj * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)QW, (cuuint32_t)QH, 5};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(q), dims, strides, box, elem,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+#endif
+
 cudaError_t configure_kernels() {
     cudaError_t e;
-    e = cudaFuncSetAttribute(k_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_stage<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stage_smem_bytes());
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_stage<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stage_smem_bytes());
     if (e != cudaSuccess) return e;
+#if TNS_STAGE_TMA_ON
+    e = cudaFuncSetAttribute(k_stage<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage_tma_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_stage<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage_tma_smem_bytes());
+    if (e != cudaSuccess) return e;
+#endif
     e = cudaFuncSetAttribute(k_viscous, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)visc_smem_bytes());
     if (e != cudaSuccess) return e;
@@ -950,7 +1048,17 @@ void launch_stage(const Params& P, const Mesh& M, const double* qin, const doubl
                   const double* dtmin, double alpha, unsigned long long* cdiff,
                   unsigned int* status, unsigned int* error, cudaStream_t s) {
     StageArgs A{qin, qold, qout, d, vis, dt, dtmin, alpha, cdiff, status, error};
-    launch_tile(cdiff ? k_stage<1> : k_stage<0>, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s, P, M, A);
+    CUtensorMap qmap;
+#if TNS_STAGE_TMA_ON
+    if (stage_q_map(M, qin, &qmap)) {
+        launch_tile(cdiff ? k_stage<1, true> : k_stage<0, true>, tile_grid(M), dim3(TJ, TI),
+                    stage_tma_smem_bytes(), s, P, M, A, qmap);
+        return;
+    }
+#endif
+    memset(&qmap, 0, sizeof(qmap));
+    launch_tile(cdiff ? k_stage<1, false> : k_stage<0, false>, tile_grid(M), dim3(TJ, TI), stage_smem_bytes(), s,
+                P, M, A, qmap);
 }
 
 int dtmin_blocks(const Mesh& M) {

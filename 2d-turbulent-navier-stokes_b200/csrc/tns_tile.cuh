@@ -5,6 +5,8 @@
 
 #include <utility>
 
+#include <cuda.h>
+
 #include "tns_device.cuh"
 
 namespace tns {
@@ -108,6 +110,22 @@ __device__ __forceinline__ void bulk_copy_start(void* dst, const void* src, unsi
                  ::"r"(b), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
+}
+// One-shot tiled tensor copy global -> shared (cp.async.bulk.tensor, 3-D, no multicast):
+// the box of `map` at element coordinates (x, y, z), x the innermost; x * element size a
+// multiple of 16 bytes; the shared destination 128-byte aligned; `bytes` the whole box
+// (out-of-range elements arrive as zeros and count).  `map` is the address of a
+// __grid_constant__ kernel parameter.  One thread, after bulk_barrier_init.
+__device__ __forceinline__ void tensor_copy_3d_start(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                                     unsigned bytes, unsigned long long* bar) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];"
+                 ::"r"(d), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(b)
+                 : "memory");
 }
 // Waits for phase 0 of the barrier with a bounded number of polls; false if the copy did
 // not complete in that many (the caller reports it and skips the tile).
@@ -216,10 +234,11 @@ __device__ __forceinline__ int classify(const Mesh& M, int i, int j, int& along)
 }
 
 // BC state of the ghost on `side` at `along`, from the parent and the parent's opposite
-// neighbour read straight from the state array (bit-identical to their PRIMITIVE_VARS).
-template <class St>
-__device__ void ghost_state(const Params& P, const Mesh& M, const St& st, int side, int along,
-                            Prim& gh) {
+// neighbour, whose primitives cell(i, j, Prim&) evaluates (bit-identical to their
+// PRIMITIVE_VARS).
+template <class CellPrim>
+__device__ void ghost_state_at(const Params& P, const Mesh& M, int side, int along, CellPrim cell,
+                               Prim& gh) {
     int ip, jp, io, jo;
     if (side == 1) { ip = along; jp = 0; io = along; jo = 1; }
     else if (side == 2) { ip = M.ni - 1; jp = along; io = M.ni - 2; jo = along; }
@@ -228,8 +247,8 @@ __device__ void ghost_state(const Params& P, const Mesh& M, const St& st, int si
     const int g = M.ghost_index(side, along);
     const int type = M.gtype[g];
     Prim par, opp;
-    cell_prim(P, st, (size_t)ip * M.nj + jp, par);
-    if (type == 3) cell_prim(P, st, (size_t)io * M.nj + jo, opp);
+    cell(ip, jp, par);
+    if (type == 3) cell(io, jo, opp);
     else opp = par;
     const size_t n1 = (size_t)ip * (M.nj + 1) + jp;
     const double X[4] = {M.x[n1], M.x[n1 + M.nj + 1], M.x[n1 + M.nj + 2], M.x[n1 + 1]};
@@ -239,6 +258,14 @@ __device__ void ghost_state(const Params& P, const Mesh& M, const St& st, int si
     const double ycc_p = (Y[0] + Y[1] + Y[2] + Y[3]) * 0.25;
     boundary_ghost(P, type, par, opp, psx, psy, M.gyc[g], ycc_p, type == 6 ? M.gport[g] : 0.0,
                    M.ginj[g], gh);
+}
+
+// The same, with both cells read straight from the state array.
+template <class St>
+__device__ __forceinline__ void ghost_state(const Params& P, const Mesh& M, const St& st, int side, int along,
+                                            Prim& gh) {
+    ghost_state_at(P, M, side, along,
+                   [&](int i, int j, Prim& p) { cell_prim(P, st, (size_t)i * M.nj + j, p); }, gh);
 }
 
 __device__ __forceinline__ void ghost_state(const Params& P, const Mesh& M, const double* __restrict__ q,

@@ -17,10 +17,14 @@ AMACHINIT and the displacements of the 64 ramp-wall nodes i = 260, 264, ..., 512
    primal on the GPU through the C ABI with a checkpoint (or a record of the forward
    values) per iteration, reverse sweep of CUDA adjoint steps (tnsgpu.adjoint).  Two objectives: the wall pressure force (y) and the
    total-pressure loss between the inlet (side 4) and the outlet (side 2).
-3. Central finite differences (relative step 1e-6 and 2e-6; node displacement 3e-7 m
-   and 6e-7 m) of both objectives for 4 parameters -- P0, T0, AMACHINIT and wall node
-   i = 388 -- on the GPU FP64 path, and with ``--oracle-fd`` on the oracle (C, host
-   cores, one process per evaluation).
+3. Central finite differences of both objectives for 4 parameters -- P0, T0, AMACHINIT
+   and wall node i = 388 -- on the GPU FP64 path, and with ``--oracle-fd`` on the
+   oracle (C, host cores, one process per evaluation), at steps h and 3h with the
+   Richardson value D(h) + (D(h) - D(3h)) / 8.  h is relative 1e-3 for P0 and
+   AMACHINIT, 1e-2 for T0 (J is nearly independent of T0, so a smaller step returns
+   rounding noise) and 3e-7 m for the node.
+4. With ``--step-study``: the GPU central differences of T0, P0 and AMACHINIT over
+   relative steps 3e-2 .. 1e-7, and of the node over 1e-8 .. 1e-4 m.
 
 Prints one JSON object.
 """
@@ -90,6 +94,7 @@ def main():
     ap.add_argument("--transient-iters", type=int, default=500)
     ap.add_argument("--fixed-point-iters", type=int, default=200)
     ap.add_argument("--oracle-fd", action="store_true")
+    ap.add_argument("--step-study", action="store_true")
     a = ap.parse_args()
     # the oracle pool starts before any CUDA work
     pool = cf.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
@@ -149,7 +154,7 @@ def main():
 
     # 3. finite differences on the GPU FP64 path (and the oracle)
     base = {"p0": flow.p0, "t0": flow.t0, "am": flow.amachinit, "dy": float(dy[CHECK_NODE])}
-    steps = {"p0": 1e-6 * flow.p0, "t0": 1e-6 * flow.t0, "am": 1e-6 * flow.amachinit, "dy": 3e-7}
+    steps = {"p0": 1e-3 * flow.p0, "t0": 1e-2 * flow.t0, "am": 1e-3 * flow.amachinit, "dy": 3e-7}
 
     def gpu_J(obj, which, value):
         kw = {"p0": None, "t0": None, "amachinit": None, "dy": dy}
@@ -169,7 +174,7 @@ def main():
         for which in base:
             adj = grads[obj]["dJ_ddy"][CHECK_NODE] if which == "dy" else grads[obj][key[which]]
             row = {"adjoint": float(adj)}
-            for mult in (1, 2):
+            for mult in (1, 3):
                 hh = mult * steps[which]
                 row[f"gpu_fd_h{mult}"] = (gpu_J(obj, which, base[which] + hh) -
                                           gpu_J(obj, which, base[which] - hh)) / (2 * hh)
@@ -177,20 +182,38 @@ def main():
                     for sgn in (1, -1):
                         jobs.append(((obj, which, mult, sgn),
                                      pool.submit(_oracle_objective, (which, base[which] + sgn * hh, N, obj))))
+            row["gpu_richardson"] = row["gpu_fd_h1"] + (row["gpu_fd_h1"] - row["gpu_fd_h3"]) / 8.0
             row["rel_diff_gpu_fd"] = abs(row["adjoint"] - row["gpu_fd_h1"]) / max(abs(row["gpu_fd_h1"]), 1e-300)
+            row["rel_diff_gpu_richardson"] = abs(row["adjoint"] - row["gpu_richardson"]) / \
+                max(abs(row["gpu_richardson"]), 1e-300)
             fd[f"{obj}/{which}"] = row
     if pool is not None:
         vals = {k: f.result() for k, f in jobs}
         for obj in objectives:
             for which in base:
                 row = fd[f"{obj}/{which}"]
-                for mult in (1, 2):
+                for mult in (1, 3):
                     hh = mult * steps[which]
                     row[f"oracle_fd_h{mult}"] = (vals[(obj, which, mult, 1)] - vals[(obj, which, mult, -1)]) / (2 * hh)
                 row["rel_diff_oracle_fd"] = abs(row["adjoint"] - row["oracle_fd_h1"]) / \
                     max(abs(row["oracle_fd_h1"]), 1e-300)
         pool.shutdown()
     out["finite_differences"] = fd
+    if a.step_study:
+        study = {}
+        for obj in objectives:
+            for which in base:
+                adj = grads[obj]["dJ_ddy"][CHECK_NODE] if which == "dy" else grads[obj][key[which]]
+                rels = (1e-8, 3e-8, 1e-7, 3e-7, 1e-6, 3e-6, 1e-5, 3e-5, 1e-4) if which == "dy" else \
+                    (3e-2, 1e-2, 3e-3, 1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7)
+                rows = []
+                for rel in rels:
+                    hh = rel if which == "dy" else rel * base[which]
+                    c = (gpu_J(obj, which, base[which] + hh) - gpu_J(obj, which, base[which] - hh)) / (2 * hh)
+                    rows.append({"step": rel, "central": c,
+                                 "rel_diff": abs(float(adj) - c) / max(abs(c), 1e-300)})
+                study[f"{obj}/{which}"] = {"adjoint": float(adj), "rows": rows}
+        out["step_study"] = study
     print(json.dumps(out))
 
 
