@@ -374,6 +374,11 @@ int alloc_state(tns_handle* h) {
         if ((rc = h->cuda(cudaMemset(h->dtf.p, 0, nc * 4), "cudaMemset")) ||
             (rc = h->cuda(cudaMemset(h->visf.p, 0, 4 * nc * 4), "cudaMemset")))
             return rc;
+        const size_t ntiles = (size_t)((h->nj + tns::TJ - 1) / tns::TJ) * ((h->ni + tns::TI - 1) / tns::TI);
+        if ((rc = h->cuda(h->tref.alloc(ntiles * tns::TREF_WORDS), "cudaMalloc")) ||
+            (rc = h->cuda(cudaMemset(h->tref.p, 0, ntiles * tns::TREF_WORDS * 8), "cudaMemset")))
+            return rc;
+        h->M.tref = reinterpret_cast<tns::TileRefMx*>(h->tref.p);
     } else if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qb.alloc(5 * nc), "cudaMalloc")) ||
                (rc = h->cuda(h->qc.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->d.alloc(5 * nc), "cudaMalloc")) ||
                (rc = h->cuda(h->vis.alloc(4 * nc), "cudaMalloc")) || (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc"))) {
@@ -1052,7 +1057,7 @@ void tns_destroy(tns_handle* h) {
         if (g) cudaGraphExecDestroy(g);
     if (h->graph_mon) cudaGraphExecDestroy(h->graph_mon);
     h->qa2.release(); h->dqb.release(); h->dqc.release(); h->df.release(); h->visf.release();
-    h->dtf.release();
+    h->dtf.release(); h->tref.release();
     for (auto* b : {&h->x, &h->y, &h->cfldl, &h->gxc, &h->gyc, &h->ginj, &h->gport, &h->qa, &h->qb,
                     &h->qc, &h->d, &h->vis, &h->dt, &h->dtmin, &h->partial, &h->primout, &h->cvol,
                     &h->stile, &h->fgi, &h->fgj})

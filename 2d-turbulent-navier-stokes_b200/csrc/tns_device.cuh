@@ -69,6 +69,8 @@ enum FaceGeo { FG_SX, FG_SY, FG_GA, FG_GB, FG_GC, FG_GD, FG_RYAVG, FG_N };
 
 // Ghost-side numbering: side 1 (j=-1) and 3 (j=NJ) are indexed by i, sides 2 (i=NI)
 // and 4 (i=-1) by j; the four runs are stored back to back.
+struct TileRefMx;
+
 struct Mesh {
     int ni, nj;             // cells in i and j
     const double* x;        // node x [(ni+1)*(nj+1)], node (i,j) at i*(nj+1)+j
@@ -84,6 +86,9 @@ struct Mesh {
     const double* stile;    // static data of the stage tiles, one block per tile (tns_tile.cuh)
     const double* fgi;      // [FG_N][(ni+1)*nj] static i-face geometry
     const double* fgj;      // [FG_N][ni*(nj+1)] static j-face geometry
+    // (mixed precision) each stage tile's reference state for the current iteration,
+    // written by the dissipation kernel from Q_old, read by the four stages
+    TileRefMx* tref = nullptr;
     __host__ __device__ int ghost_index(int side, int along) const {
         return side == 1 ? along : side == 2 ? ni + along : side == 3 ? ni + nj + along
                                                                       : 2 * ni + nj + along;
@@ -171,6 +176,36 @@ TNS_HD void primitive(const Params& P, double c1, double c2, double c3,
     s.ri = RT;
     s.c5 = c5;
     s.qm = sqrt(s.u * s.u + s.v * s.v);
+}
+
+// The mixed path's reference state of a stage tile: a FP64 state of the tile (its first
+// cell's Q_old), its primitives and fluxes, and the primitives in FP32 that the
+// deviation formulas multiply by.  Any state of the tile serves: the kernels only form
+// differences from it.
+struct TileRefMx {
+    double c[5];  // conservative state
+    Prim q;       // its primitives and fluxes
+    float rho, u, v, e, t, ri, qm, c2, c3, c4p, c5;  // (e = C4/C1, c4p = C4 + P)
+    float pad;
+};
+static_assert(sizeof(TileRefMx) % 8 == 0, "a tile reference is copied as 8-byte words");
+constexpr int TREF_WORDS = (int)(sizeof(TileRefMx) / 8);
+
+TNS_HD void make_tile_ref(const Params& P, const double c[5], TileRefMx& R) {
+    for (int m = 0; m < 5; m++) R.c[m] = c[m];
+    primitive(P, c[0], c[1], c[2], c[3], c[4], R.q);
+    R.rho = (float)c[0];
+    R.u = (float)R.q.u;
+    R.v = (float)R.q.v;
+    R.e = (float)(c[3] / c[0]);
+    R.t = (float)R.q.t;
+    R.ri = (float)R.q.ri;
+    R.qm = (float)R.q.qm;
+    R.c2 = (float)c[1];
+    R.c3 = (float)c[2];
+    R.c4p = (float)(c[3] + R.q.p);
+    R.c5 = (float)c[4];
+    R.pad = 0.0f;
 }
 
 // Conservative + flux tail shared by BC types 2,3,4,6,7 (e.g. boundary.f90:62-70).

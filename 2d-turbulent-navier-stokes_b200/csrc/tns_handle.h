@@ -67,6 +67,7 @@ struct tns_handle {
     int cur = 0;  // mixed: which of qa / qa2 holds the state
     DevBuf<double> qa2;
     DevBuf<float> dqb, dqc, df, visf, dtf;
+    DevBuf<double> tref;  // per stage tile reference state (TileRefMx words)
     cudaGraphExec_t graph_mx[2] = {nullptr, nullptr};
     // monitored iteration (CDIFF reduction in stage 4): FP64, mixed per parity
     cudaGraphExec_t graph_mon = nullptr;

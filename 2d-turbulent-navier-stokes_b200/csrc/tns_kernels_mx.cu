@@ -1,15 +1,17 @@
 // tns_kernels_mx.cu -- mixed FP32/FP64 kernels of one RK4 iteration.
 //
-// What stays FP64: the state Q (and every stage state COLD + dQ), primitive variables,
-// geometry (node coordinates, surface vectors, volumes, centroids), every difference of
-// nearly equal quantities (gradient stencils, node averages), the part of the flux
-// residual that cancels (a per-tile reference flux times the closed-contour sum of S),
-// the state accumulation and the residual monitor.  What is FP32: the stage increments
-// dQ, the dissipation D, the viscous flux VIS and DT as stored, the flux deviations from
-// the tile reference, and the flux / source / viscous arithmetic with its
-// transcendentals (T**0.6, tanh, sqrt).
+// What stays FP64: the state Q (and every stage state COLD + dQ), each stage tile's
+// reference state with its primitives and fluxes, ghost states, the viscous and
+// dissipation kernels' primitives, geometry (node coordinates, surface vectors,
+// volumes, centroids), the differences of nearly equal quantities in the viscous and
+// dissipation kernels (gradient stencils, node averages), the part of the flux residual
+// that cancels (the reference flux times the closed-contour sum of S), the state
+// accumulation and the residual monitor.  What is FP32: the stage increments dQ, the
+// dissipation D, the viscous flux VIS and DT as stored, the stage slots as deviations
+// from the tile reference (primitives, fluxes and the source stencils), and the
+// source / viscous arithmetic with its transcendentals (T**0.6, tanh, sqrt).
 //
-// Storing flux deviations instead of fluxes keeps the FP32 rounding of the residual
+// Working with deviations instead of values keeps the FP32 rounding of the residual
 // proportional to the flow's variation inside a tile rather than to the pressure and
 // total-enthalpy levels, so the iteration can still converge by RTRED=1e-5 and more.
 #include "tns_device.cuh"
@@ -41,23 +43,59 @@ __device__ __forceinline__ float tanh_f32(float x) {
 struct StageSmemMx {
     double st[STILE];      // the tile's static block (tns_tile.cuh), one bulk copy
     float2 fg[5][NSLOT];   // (F_m - Fref_m, G_m - Gref_m)
-    double2 uv[NSLOT];     // (U, V)
-    double2 rq[NSLOT];     // (C5/C1, |V|)
-    double p[NSLOT];       // pressure (FP64: the axisymmetric radial balance cancels)
+    float2 duv[NSLOT];     // (U - Uref, V - Vref)
+    float2 drq[NSLOT];     // (C5/C1 - ref, |V| - ref)
+    float dp[NSLOT];       // P - Pref
     float2 tr[NSLOT];      // (T, RHO)
-    double fref[5], gref[5];
+    TileRefMx ref;           // the tile's reference state (written by the dissipation kernel)
     unsigned long long bar;  // completion of the static block's copy
 };
 
 size_t stage_mx_smem_bytes() { return sizeof(StageSmemMx); }
 
-__device__ __forceinline__ void put_slot_mx(StageSmemMx& S, int s, const Prim& p) {
+// Slot of a cell from its state's deviation from the tile reference, dC = C - Cref, all in
+// FP32: every quantity the residual and the sources difference is formed as a deviation
+// by exact algebra (dU = (dC2 - Uref dC1) / C1, d(C2 U) = dC2 U + C2ref dU, P - Pref =
+// R (dC1 T + C1ref dT), |V| - |V|ref = (|V|^2 - |V|ref^2) / (|V| + |V|ref), ...), so its
+// FP32 rounding is a fraction of the deviation, as for a FP64 value rounded after the
+// subtraction.
+__device__ __forceinline__ void put_slot_dev_mx(const Params& P, StageSmemMx& S, int s, float d1, float d2,
+                                                float d3, float d4, float d5) {
+    const TileRefMx& R = S.ref;
+    const float rho = R.rho + d1;
+    const float rr = 1.0f / rho;
+    const float du = (d2 - R.u * d1) * rr;
+    const float dv = (d3 - R.v * d1) * rr;
+    const float de = (d4 - R.e * d1) * rr;
+    const float dri = (d5 - R.ri * d1) * rr;
+    const float u = R.u + du, v = R.v + dv;
+    const float dq2 = du * (u + R.u) + dv * (v + R.v);  // |V|^2 - |V|ref^2
+    const float dt = (de - 0.5f * dq2) * (float)P.inv_cv;
+    const float t = R.t + dt;
+    const float dp = (float)P.rr * (d1 * t + R.rho * dt);
+    const float qm = sqrtf(u * u + v * v);
+    const float qs = qm + R.qm;
+    const float dqm = qs > 0.0f ? dq2 / qs : 0.0f;
+    const float f2 = d2 * v + R.c2 * dv;  // d(C2 V) = d(C3 U)
+    S.fg[0][s] = make_float2(d2, d3);
+    S.fg[1][s] = make_float2(d2 * u + R.c2 * du + dp, f2);
+    S.fg[2][s] = make_float2(f2, d3 * v + R.c3 * dv + dp);
+    S.fg[3][s] = make_float2((d4 + dp) * u + R.c4p * du, (d4 + dp) * v + R.c4p * dv);
+    S.fg[4][s] = make_float2(d5 * u + R.c5 * du, d5 * v + R.c5 * dv);
+    S.duv[s] = make_float2(du, dv);
+    S.drq[s] = make_float2(dri, dqm);
+    S.dp[s] = dp;
+    S.tr[s] = make_float2(t, rho);
+}
+
+// Slot of a ghost: its BC state in FP64, then the deviations.
+__device__ __forceinline__ void put_slot_ghost_mx(StageSmemMx& S, int s, const Prim& p) {
+    const Prim& r = S.ref.q;
 #pragma unroll
-    for (int m = 0; m < 5; m++)
-        S.fg[m][s] = make_float2((float)(p.f[m] - S.fref[m]), (float)(p.g[m] - S.gref[m]));
-    S.uv[s] = make_double2(p.u, p.v);
-    S.rq[s] = make_double2(p.ri, p.qm);
-    S.p[s] = p.p;
+    for (int m = 0; m < 5; m++) S.fg[m][s] = make_float2((float)(p.f[m] - r.f[m]), (float)(p.g[m] - r.g[m]));
+    S.duv[s] = make_float2((float)(p.u - r.u), (float)(p.v - r.v));
+    S.drq[s] = make_float2((float)(p.ri - r.ri), (float)(p.qm - r.qm));
+    S.dp[s] = (float)(p.p - r.p);
     S.tr[s] = make_float2((float)p.t, (float)p.rho);
 }
 
@@ -92,12 +130,10 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
         bulk_copy_start(S.st, M.stile + tile * STILE, STILE * sizeof(double), &S.bar);
     }
     pdl_wait();
-    if (tid == 0) {
-        // tile reference flux: the first cell of the tile
-        Prim r;
-        cell_prim(P, st, (size_t)i0 * M.nj + j0, r);
-#pragma unroll
-        for (int m = 0; m < 5; m++) { S.fref[m] = r.f[m]; S.gref[m] = r.g[m]; }
+    if (tid < TREF_WORDS) {
+        const size_t tile = (size_t)by * ((M.nj + TJ - 1) / TJ) + bx;
+        reinterpret_cast<unsigned long long*>(&S.ref)[tid] =
+            reinterpret_cast<const unsigned long long*>(M.tref + tile)[tid];
     }
     __syncthreads();
     for (int s = tid; s < NSLOT; s += NTHREADS) {
@@ -105,12 +141,20 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
         if (kind < 0) continue;
-        Prim p;
-        if (kind == 0)
-            cell_prim(P, st, (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj), p);
-        else
+        if (kind == 0) {
+            const size_t cell = (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj);
+            float d[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++) {
+                d[m] = (float)(st.cold[m * ncell + cell] - S.ref.c[m]);
+                if (st.dq) d[m] += st.dq[m * ncell + cell];
+            }
+            put_slot_dev_mx(P, S, s, d[0], d[1], d[2], d[3], d[4]);
+        } else {
+            Prim p;
             ghost_state(P, M, st, kind, along, p);
-        put_slot_mx(S, s, p);
+            put_slot_ghost_mx(S, s, p);
+        }
     }
     __syncthreads();
     if (!bulk_wait(&S.bar)) {
@@ -155,7 +199,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             R[m] = 0.5f * ((I.x + a.x) * sx[0] + (I.y + a.y) * sy[0] + (I.x + b.x) * sx[1] +
                            (I.y + b.y) * sy[1] + (I.x + e.x) * sx[2] + (I.y + e.y) * sy[2] +
                            (I.x + d.x) * sx[3] + (I.y + d.y) * sy[3]);
-            R64[m] = S.fref[m] * sumx + S.gref[m] * sumy;
+            R64[m] = S.ref.q.f[m] * sumx + S.ref.q.g[m] * sumy;
         }
 
         // source terms (source_terms.f90:24-104): FP64 stencil differences, FP32 rest,
@@ -164,18 +208,18 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             const int a = nb[0], b = nb[1], cc = nb[2], d = nb[3];
             const float ga = (float)S.st[gc + ST_GA * NTHREADS], gb = (float)S.st[gc + ST_GB * NTHREADS];
             const float gcf = (float)S.st[gc + ST_GC * NTHREADS], gd = (float)S.st[gc + ST_GD * NTHREADS];
-            const double2 ua = S.uv[a], ub = S.uv[b], uc = S.uv[cc], ud = S.uv[d];
-            const double2 ra = S.rq[a], rb = S.rq[b], rc = S.rq[cc], rd = S.rq[d];
-            const float dqac = (float)(ra.y - rc.y), dqbd = (float)(rb.y - rd.y);
-            const float drac = (float)(ra.x - rc.x), drbd = (float)(rb.x - rd.x);
-            const float duac = (float)(ua.x - uc.x), dubd = (float)(ub.x - ud.x);
-            const float dvac = (float)(ua.y - uc.y), dvbd = (float)(ub.y - ud.y);
+            const float2 ua = S.duv[a], ub = S.duv[b], uc = S.duv[cc], ud = S.duv[d];
+            const float2 ra = S.drq[a], rb = S.drq[b], rc = S.drq[cc], rd = S.drq[d];
+            const float dqac = ra.y - rc.y, dqbd = rb.y - rd.y;
+            const float drac = ra.x - rc.x, drbd = rb.x - rd.x;
+            const float duac = ua.x - uc.x, dubd = ub.x - ud.x;
+            const float dvac = ua.y - uc.y, dvbd = ub.y - ud.y;
             const float DQX = dqac * ga + dqbd * gb, DQY = dqac * gcf + dqbd * gd;
             const float DRX = drac * ga + drbd * gb, DRY = drac * gcf + drbd * gd;
             const float DUX = duac * ga + dubd * gb, DUY = duac * gcf + dubd * gd;
             const float DVX = dvac * ga + dvbd * gb, DVY = dvac * gcf + dvbd * gd;
             const float2 trc = S.tr[c];
-            const float RHO = trc.y, RI = (float)S.rq[c].x, T = trc.x;
+            const float RHO = trc.y, RI = S.ref.ri + S.drq[c].x, T = trc.x;
             const float AMU = (float)P.suth_amol * pow06f(T);
             const float CHI = RHO * RI / ((float)CMU * AMU);
             const float chi2 = CHI * CHI;
@@ -200,7 +244,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             const float volf = (float)VOL;
             if (P.iaxis == 1) {
                 const double rycc = S.st[gc + ST_RYCC * NTHREADS];
-                const float VBYY = (ycc < YAXIS_THRESH) ? DVY : (float)(S.uv[c].y * rycc);
+                const float VBYY = (ycc < YAXIS_THRESH) ? DVY : (S.ref.v + S.duv[c].y) * (float)rycc;
                 const float DIVVEL = DUX + DVY + VBYY;
                 PK = AMUT / RHO *
                      (DUX * DUX + DVY * DVY + VBYY * VBYY + DUX * DUX + DVY * DVY + VBYY * VBYY +
@@ -209,9 +253,10 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
                 src5 = (RHO * ((float)CONST1 - (float)CONST2 * FR2) * sqrtf(RI * PK) -
                         RHO * (float)CONST3 * DEE) * pw;
                 const float TTT = (AMU + AMUT) * (VBYY + VBYY - DIV23 * DIVVEL);
-                // SOURCE3 = (P - TTT)/YCC: the P part cancels the reference flux in FP64
-                R64[2] -= VOL * (S.p[c] * rycc);
-                R[2] += volf * (TTT * (float)rycc);
+                // SOURCE3 = (P - TTT)/YCC: the reference pressure's part cancels the
+                // reference flux in FP64
+                R64[2] -= VOL * (S.ref.q.p * rycc);
+                R[2] += volf * ((TTT - S.dp[c]) * (float)rycc);
             } else {
                 const float DIVVEL = DUX + DVY;
                 PK = AMUT / RHO *
@@ -565,6 +610,13 @@ __device__ __forceinline__ void dissipation_mx_tile(const Params& P, const Mesh&
             DT = *dtmin;
         }
         S.vbd[s] = (float)(M.cvol[c] / DT);
+    }
+    if (tid == NTHREADS - 1) {
+        // the tile's reference state for this iteration's stages (its first cell), by the
+        // last warp, which has no second ring slot to wait for
+        const int d0 = 2 * DWM + 2;
+        const double c[5] = {S.c[0][d0], S.c[1][d0], S.c[2][d0], S.c[3][d0], S.c[4][d0]};
+        make_tile_ref(P, c, M.tref[(size_t)by * ((M.nj + TJ - 1) / TJ) + bx]);
     }
     __syncthreads();
     const int tj = threadIdx.x, ti = threadIdx.y;
