@@ -10,6 +10,7 @@
 #pragma once
 
 #include "tns_device.cuh"
+#include "tns_tile.cuh"
 
 namespace tns {
 
@@ -64,5 +65,22 @@ struct BatchCase {
     StageArgsMx stage_mx[2][2][4];  // [parity][monitor][stage]
     const double* dtmin;
 };
+
+// The batched stage kernels copy their case's arguments into shared memory: loads from
+// constant shared addresses instead of through a descriptor pointer held in registers.
+// The mixed one then runs 4 blocks per SM like the single-case kernel (64-case sweep,
+// schedule 0: 0.235 -> 0.206 s); the viscous kernels are better off without (spills).
+#ifndef TNS_BATCH_SMEM_ARGS
+#define TNS_BATCH_SMEM_ARGS 1
+#endif
+static_assert(sizeof(Params) % 8 == 0 && sizeof(Mesh) % 8 == 0 && sizeof(StageArgs) % 4 == 0 &&
+                  sizeof(StageArgsMx) % 4 == 0,
+              "descriptors are copied as 4-byte words and laid out at 8-byte offsets");
+// Block-wide copy of a descriptor (a multiple of 4 bytes) into shared memory.
+__device__ __forceinline__ void copy_words(void* dst, const void* src, size_t bytes, int tid) {
+    const unsigned* s = reinterpret_cast<const unsigned*>(src);
+    unsigned* d = reinterpret_cast<unsigned*>(dst);
+    for (int k = tid; k < (int)(bytes / 4); k += NTHREADS) d[k] = s[k];
+}
 
 }  // namespace tns

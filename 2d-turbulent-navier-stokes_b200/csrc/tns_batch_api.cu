@@ -23,6 +23,10 @@
 
 using tns::BatchCase;
 
+#ifndef TNS_BATCH_BLOCK
+#define TNS_BATCH_BLOCK 8
+#endif
+
 struct tns_batch {
     std::string err;
     std::vector<tns_handle*> cases;
@@ -43,7 +47,7 @@ struct tns_batch {
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [monitor][parity]
     // schedule 2: BLOCK unmonitored iterations in one graph per starting parity; each
     // case's chain runs ahead on its stream with no join between the iterations
-    static constexpr int BLOCK = 8;
+    static constexpr int BLOCK = TNS_BATCH_BLOCK;
     cudaGraphExec_t block[2] = {nullptr, nullptr};
     long long per_block = 0;
     // schedule: 0 = one launch per phase over the tile table of all active cases;

@@ -862,7 +862,24 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_BATCH_MINB)) k_
     const int4 t = tiles[blockIdx.x];
     if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
+#if TNS_BATCH_SMEM_ARGS
+    // the case's arguments copied into shared memory (raw storage, never constructed):
+    // loads from constant shared addresses instead of through the descriptor pointer
+    __shared__ __align__(16) unsigned char sargs[sizeof(Params) + sizeof(Mesh) + sizeof(StageArgs)];
+    Params& sP = *reinterpret_cast<Params*>(sargs);
+    Mesh& sM = *reinterpret_cast<Mesh*>(sargs + sizeof(Params));
+    StageArgs& sA = *reinterpret_cast<StageArgs*>(sargs + sizeof(Params) + sizeof(Mesh));
+    {
+        const int tid = threadIdx.y * TJ + threadIdx.x;
+        copy_words(&sP, &c.P, sizeof(Params), tid);
+        copy_words(&sM, &c.M, sizeof(Mesh), tid);
+        copy_words(&sA, &c.stage[monitor][stage], sizeof(StageArgs), tid);
+        __syncthreads();
+    }
+    stage_tile<false>(sP, sM, sA, t.y, t.z);
+#else
     stage_tile<false>(c.P, c.M, c.stage[monitor][stage], t.y, t.z);
+#endif
 }
 
 // Persistent batched iterations (schedule 3): one cooperative launch advances every
@@ -1020,11 +1037,11 @@ void launch_batch_f64(const BatchCase* cases, const int4* tiles, const int* acti
                       int kernel, int stage, int monitor, cudaStream_t s) {
     const dim3 blk(TJ, TI);
     if (kernel == 0)
-        k_dissipation_batch<<<ntiles, blk, diss_smem_bytes(), s>>>(cases, tiles, active);
+        launch_tile(k_dissipation_batch, dim3(ntiles), blk, diss_smem_bytes(), s, cases, tiles, active);
     else if (kernel == 1)
-        k_viscous_batch<<<ntiles, dim3(TJ, VROWS), visc_smem_bytes(), s>>>(cases, tiles, active);
+        launch_tile(k_viscous_batch, dim3(ntiles), dim3(TJ, VROWS), visc_smem_bytes(), s, cases, tiles, active);
     else
-        k_stage_batch<<<ntiles, blk, stage_smem_bytes(), s>>>(cases, tiles, active, stage, monitor);
+        launch_tile(k_stage_batch, dim3(ntiles), blk, stage_smem_bytes(), s, cases, tiles, active, stage, monitor);
 }
 
 void launch_dissipation(const Params& P, const Mesh& M, const double* q, double* d, double* dt,

@@ -102,16 +102,16 @@ __device__ __forceinline__ void put_slot_ghost_mx(StageSmemMx& S, int s, const P
 #ifndef TNS_STAGE_MX_MINB
 #define TNS_STAGE_MX_MINB 4
 #endif
-// the batched stage kernel reads its arguments from global descriptors, which costs
-// registers: at 4 blocks/SM it spills
+// the batched kernels at 4 blocks/SM as the single-case ones (the stage kernel with its
+// arguments in shared memory, TNS_BATCH_SMEM_ARGS)
 #ifndef TNS_STAGE_MX_BATCH_MINB
-#define TNS_STAGE_MX_BATCH_MINB 3
+#define TNS_STAGE_MX_BATCH_MINB 4
 #endif
 #ifndef TNS_VISC_MX_MINB
 #define TNS_VISC_MX_MINB 4  // 64 registers with small spills beat 80 registers at 3 blocks/SM
 #endif
 #ifndef TNS_VISC_MX_BATCH_MINB
-#define TNS_VISC_MX_BATCH_MINB 3
+#define TNS_VISC_MX_BATCH_MINB 4
 #endif
 // One stage on tile (bx, by) of a mesh; the single-case and the batched kernels wrap it.
 __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, const StageArgsMx& A,
@@ -769,7 +769,25 @@ __global__ void __launch_bounds__(NTHREADS, TNS_PER_SM(TNS_STAGE_MX_BATCH_MINB))
     const int4 t = tiles[blockIdx.x];
     if (!active[t.x]) return;
     const BatchCase& c = cases[t.x];
+#if TNS_BATCH_SMEM_ARGS
+    // the case's arguments in shared memory: constant-address loads instead of loads
+    // through a descriptor pointer held in registers
+    // (raw storage: the structs are copied in, never constructed)
+    __shared__ __align__(16) unsigned char sargs[sizeof(Params) + sizeof(Mesh) + sizeof(StageArgsMx)];
+    Params& sP = *reinterpret_cast<Params*>(sargs);
+    Mesh& sM = *reinterpret_cast<Mesh*>(sargs + sizeof(Params));
+    StageArgsMx& sA = *reinterpret_cast<StageArgsMx*>(sargs + sizeof(Params) + sizeof(Mesh));
+    {
+        const int tid = threadIdx.y * TJ + threadIdx.x;
+        copy_words(&sP, &c.P, sizeof(Params), tid);
+        copy_words(&sM, &c.M, sizeof(Mesh), tid);
+        copy_words(&sA, &c.stage_mx[parity][monitor][stage], sizeof(StageArgsMx), tid);
+        __syncthreads();
+    }
+    stage_mx_tile(sP, sM, sA, t.y, t.z);
+#else
     stage_mx_tile(c.P, c.M, c.stage_mx[parity][monitor][stage], t.y, t.z);
+#endif
 }
 
 // Persistent batched iterations of the mixed path (schedule 3), as k_batch_persistent:
@@ -851,11 +869,13 @@ void launch_batch_mx(const BatchCase* cases, const int4* tiles, const int* activ
                      int kernel, int parity, int stage, int monitor, cudaStream_t s) {
     const dim3 blk(TJ, TI);
     if (kernel == 0)
-        k_dissipation_mx_batch<<<ntiles, blk, diss_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
+        launch_tile(k_dissipation_mx_batch, dim3(ntiles), blk, diss_mx_smem_bytes(), s, cases, tiles, active, parity);
     else if (kernel == 1)
-        k_viscous_mx_batch<<<ntiles, dim3(TJ, VROWS), visc_mx_smem_bytes(), s>>>(cases, tiles, active, parity);
+        launch_tile(k_viscous_mx_batch, dim3(ntiles), dim3(TJ, VROWS), visc_mx_smem_bytes(), s, cases, tiles, active,
+                    parity);
     else
-        k_stage_mx_batch<<<ntiles, blk, stage_mx_smem_bytes(), s>>>(cases, tiles, active, parity, stage, monitor);
+        launch_tile(k_stage_mx_batch, dim3(ntiles), blk, stage_mx_smem_bytes(), s, cases, tiles, active, parity, stage,
+                    monitor);
 }
 
 void launch_dissipation_mx2(const Params& P, const Mesh& M, const double* q, float* d, float* dt,

@@ -18,7 +18,7 @@ namespace tns {
 #define TNS_STAGE_MINB 3
 #endif
 #ifndef TNS_STAGE_BATCH_MINB
-#define TNS_STAGE_BATCH_MINB 2
+#define TNS_STAGE_BATCH_MINB 3  // with its arguments in shared memory (tns_batch.cuh)
 #endif
 #ifndef TNS_VISC_MINB
 #define TNS_VISC_MINB 3  // 80 registers: 3 blocks/SM beat 2 blocks without the cap

@@ -231,7 +231,8 @@ int tns_adjoint_step_next(tns_handle *h, const double *d_q, const double *d_q_ne
  * writes Q_{n+1} to d_q_next and the iteration's forward values -- stage inputs 1-3, D,
  * VIS, DT, DTMIN, the port mass flux of each stage -- to d_rec
  * (tns_adjoint_record_size doubles).  tns_adjoint_step_recorded(h, Q_n, rec_n, ...)
- * then skips the recomputation (same results as tns_adjoint_step). */
+ * then skips the recomputation (same results as tns_adjoint_step).  d_q_next may equal
+ * d_q (the last stage reads only each cell's own old value); d_rec must overlap neither. */
 long long tns_adjoint_record_size(tns_handle *h);
 int tns_adjoint_record(tns_handle *h, const double *d_q, double *d_q_next, double *d_rec);
 int tns_adjoint_step_recorded(tns_handle *h, const double *d_q, const double *d_rec, double *d_lam, int flags);
