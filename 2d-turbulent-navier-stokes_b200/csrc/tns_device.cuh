@@ -146,6 +146,32 @@ TNS_HD double amu_of(const Params& P, double T) {
     return P.suth_amol * pow06(T);
 }
 
+// A value made opaque to the optimizer (device code; the identity on the host).  The
+// compiler fuses a multiply into a later add (FMA contraction) or not depending on how
+// many uses the product has, so a value whose uses differ between kernels (a slot kept in
+// a register for the thread's own cell in one, only stored in another) could round
+// differently in each.  Passing it through kept() rounds it once, the same way in every
+// kernel and build, which keeps the tile-height builds and the batched kernels
+// bit-identical to one another.
+TNS_HD double kept(double x) {
+#ifdef __CUDA_ARCH__
+    double r;
+    asm("mov.b64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+#else
+    return x;
+#endif
+}
+TNS_HD float kept(float x) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("mov.b32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return x;
+#endif
+}
+
 // Primitive variables and fluxes of one interior cell (turbnstwod.f90:204-227).
 struct Prim {
     double u, v, t, p, rho, ri, c5, qm;
@@ -161,7 +187,7 @@ TNS_HD void primitive(const Params& P, double c1, double c2, double c3,
     s.v = c3 * rr;
     const double E = c4 * rr;
     s.t = (E - 0.5 * (s.u * s.u + s.v * s.v)) * P.inv_cv;
-    s.p = RHO * P.rr * s.t;
+    s.p = kept(RHO * P.rr * s.t);
     s.f[0] = c2;
     s.f[1] = RHO * s.u * s.u + s.p;
     s.f[2] = RHO * s.u * s.v;

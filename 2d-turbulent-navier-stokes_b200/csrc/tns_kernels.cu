@@ -30,7 +30,7 @@ namespace tns {
 // variant also receives the five Q planes of the tile's halo box by one tiled tensor
 // copy: rows i0-1 .. i0+TI, columns j0-2 .. j0+TJ+1 (the box starts one column early so
 // that its first column is a multiple of 16 bytes; out-of-mesh positions arrive as
-// zeros), and reads RHO of its cells from there.
+// zeros), and evaluates its slots from there.
 // Off by default: measured on 1024 x 384 (B200, FP64), the TMA variant took 157-159 us
 // for a RK4 iteration's four stage launches against 145 us with plain loads (same
 // results bit for bit).  A block waits for its whole box before its first slot, where
@@ -44,6 +44,11 @@ namespace tns {
 constexpr int QH = TI + 2, QW = TJ + 4;
 static_assert(QW % 2 == 0, "the Q box rows must be a multiple of 16 bytes");
 
+// Slot order: each thread first evaluates the slot of its own cell and keeps that cell's
+// T, P and RHO in registers (the only slot values read for the cell alone), then the
+// first NRING threads evaluate the halo ring's slots (tns_tile.cuh).
+static_assert(NRING <= NTHREADS, "one ring slot per thread at most");
+
 template <bool TMA>
 struct StageSmemT {
     double qs[TMA ? 5 * QH * QW : 2];  // (TMA) Q planes [5][QH][QW], 128-byte aligned
@@ -51,8 +56,6 @@ struct StageSmemT {
     double2 fg[5][NSLOT];              // (F_m, G_m)
     double2 uv[NSLOT];                 // (U, V)
     double2 rq[NSLOT];                 // (C5/C1, |V|)
-    double2 tp[NSLOT];                 // (T, P)
-    double rho[TMA ? 2 : NSLOT];
     unsigned long long bar;   // completion of the static block's copy
     unsigned long long qbar;  // (TMA) completion of the Q box
 };
@@ -71,8 +74,6 @@ __device__ __forceinline__ void put_slot(StageSmemT<TMA>& S, int s, const Prim& 
     for (int m = 0; m < 5; m++) S.fg[m][s] = make_double2(p.f[m], p.g[m]);
     S.uv[s] = make_double2(p.u, p.v);
     S.rq[s] = make_double2(p.ri, p.qm);
-    S.tp[s] = make_double2(p.t, p.p);
-    if (!TMA) S.rho[s] = p.rho;
 }
 
 // One RK stage (turbnstwod.f90:204-227, boundary.f90:24-48, source_terms.f90:24-104,
@@ -115,12 +116,11 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
         const double* b = S.qs + (ci - i0 + 1) * QW + (cj - j0 + 2);
         primitive(P, b[0], b[QH * QW], b[2 * QH * QW], b[3 * QH * QW], b[4 * QH * QW], q);
     };
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
-        const int li = s / SW, lj = s % SW;
+    // the slot at (li, lj): false where the position is neither a cell nor a ghost
+    auto slot_prim = [&](int li, int lj, Prim& p) -> bool {
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
-        if (kind < 0) continue;
-        Prim p;
+        if (kind < 0) return false;
         if (TMA) {
             if (kind == 0) box_prim(i0 - 1 + li, j0 - 1 + lj, p);
             else ghost_state_at(P, M, kind, along, box_prim, p);
@@ -129,7 +129,24 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
         } else {
             ghost_state(P, M, A.qin, ncell, kind, along, p);
         }
-        put_slot(S, s, p);
+        return true;
+    };
+    // own cell first (its T, P, RHO kept), then the ring
+    double own_t = 0.0, own_p = 0.0, own_rho = 0.0;
+    {
+        Prim p;
+        if (slot_prim(threadIdx.y + 1, threadIdx.x + 1, p)) {
+            put_slot(S, (threadIdx.y + 1) * SW + threadIdx.x + 1, p);
+            own_t = kept(p.t);
+            own_p = kept(p.p);
+            own_rho = kept(p.rho);
+        }
+    }
+    if (tid < NRING) {
+        int li, lj;
+        ring_slot(tid, li, lj);
+        Prim p;
+        if (slot_prim(li, lj, p)) put_slot(S, li * SW + lj, p);
     }
     __syncthreads();
     if (!bulk_wait(&S.bar)) {
@@ -166,9 +183,9 @@ __device__ __forceinline__ void stage_tile(const Params& P, const Mesh& M, const
             s.va = ua.y; s.vb = ub.y; s.vc = uc.y; s.vd = ud.y;
             s.ra = ra.x; s.rb = rb.x; s.rc = rc.x; s.rd = rd.x;
             s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
-            const double2 tp = S.tp[c];
+            const double2 tp = make_double2(own_t, own_p);
+            const double RHOC = own_rho;
             const double YCCI = (Y0[n1] + Y0[n1 + SNW] + Y0[n1 + SNW + 1] + Y0[n1 + 1]) * 0.25;
-            const double RHOC = TMA ? S.qs[(ti + 1) * QW + tj + 2] : S.rho[c];
             source_terms(P, s, RHOC, S.rq[c].x, tp.x, tp.y, S.uv[c].y, YCCI,
                          S.st[gc + ST_RYCC * NTHREADS], src3, src5);
         }

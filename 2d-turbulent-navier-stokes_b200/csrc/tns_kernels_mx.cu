@@ -40,13 +40,14 @@ __device__ __forceinline__ float tanh_f32(float x) {
 
 // ------------------------------------------------------------------ stage kernel
 
+// Slot order: each thread first evaluates its own cell's slot and keeps that cell's T,
+// RHO and P - Pref (read for the cell alone) in registers, then the first NRING threads
+// evaluate the halo ring (tns_tile.cuh).
 struct StageSmemMx {
     double st[STILE];      // the tile's static block (tns_tile.cuh), one bulk copy
     float2 fg[5][NSLOT];   // (F_m - Fref_m, G_m - Gref_m)
     float2 duv[NSLOT];     // (U - Uref, V - Vref)
     float2 drq[NSLOT];     // (C5/C1 - ref, |V| - ref)
-    float dp[NSLOT];       // P - Pref
-    float2 tr[NSLOT];      // (T, RHO)
     TileRefMx ref;           // the tile's reference state (written by the dissipation kernel)
     unsigned long long bar;  // completion of the static block's copy
 };
@@ -60,7 +61,7 @@ size_t stage_mx_smem_bytes() { return sizeof(StageSmemMx); }
 // FP32 rounding is a fraction of the deviation, as for a FP64 value rounded after the
 // subtraction.
 __device__ __forceinline__ void put_slot_dev_mx(const Params& P, StageSmemMx& S, int s, float d1, float d2,
-                                                float d3, float d4, float d5) {
+                                                float d3, float d4, float d5, float3& own) {
     const TileRefMx& R = S.ref;
     const float rho = R.rho + d1;
     const float rr = 1.0f / rho;
@@ -72,7 +73,7 @@ __device__ __forceinline__ void put_slot_dev_mx(const Params& P, StageSmemMx& S,
     const float dq2 = du * (u + R.u) + dv * (v + R.v);  // |V|^2 - |V|ref^2
     const float dt = (de - 0.5f * dq2) * (float)P.inv_cv;
     const float t = R.t + dt;
-    const float dp = (float)P.rr * (d1 * t + R.rho * dt);
+    const float dp = kept((float)P.rr * (d1 * t + R.rho * dt));
     const float qm = sqrtf(u * u + v * v);
     const float qs = qm + R.qm;
     const float dqm = qs > 0.0f ? dq2 / qs : 0.0f;
@@ -84,19 +85,18 @@ __device__ __forceinline__ void put_slot_dev_mx(const Params& P, StageSmemMx& S,
     S.fg[4][s] = make_float2(d5 * u + R.c5 * du, d5 * v + R.c5 * dv);
     S.duv[s] = make_float2(du, dv);
     S.drq[s] = make_float2(dri, dqm);
-    S.dp[s] = dp;
-    S.tr[s] = make_float2(t, rho);
+    own = make_float3(kept(t), kept(rho), kept(dp));
 }
 
 // Slot of a ghost: its BC state in FP64, then the deviations.
-__device__ __forceinline__ void put_slot_ghost_mx(StageSmemMx& S, int s, const Prim& p) {
+__device__ __forceinline__ void put_slot_ghost_mx(StageSmemMx& S, int s, const Prim& p, float3& own) {
     const Prim& r = S.ref.q;
 #pragma unroll
     for (int m = 0; m < 5; m++) S.fg[m][s] = make_float2((float)(p.f[m] - r.f[m]), (float)(p.g[m] - r.g[m]));
     S.duv[s] = make_float2((float)(p.u - r.u), (float)(p.v - r.v));
     S.drq[s] = make_float2((float)(p.ri - r.ri), (float)(p.qm - r.qm));
-    S.dp[s] = (float)(p.p - r.p);
-    S.tr[s] = make_float2((float)p.t, (float)p.rho);
+    const float dp = (float)(p.p - r.p);
+    own = make_float3(kept((float)p.t), kept((float)p.rho), kept(dp));
 }
 
 #ifndef TNS_STAGE_MX_MINB
@@ -136,11 +136,13 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             reinterpret_cast<const unsigned long long*>(M.tref + tile)[tid];
     }
     __syncthreads();
-    for (int s = tid; s < NSLOT; s += NTHREADS) {
-        const int li = s / SW, lj = s % SW;
+    // the slot at (li, lj) (nothing where the position is neither a cell nor a ghost);
+    // own: its T, RHO, P - Pref
+    auto slot = [&](int li, int lj, float3& own) {
         int along = 0;
         const int kind = classify(M, i0 - 1 + li, j0 - 1 + lj, along);
-        if (kind < 0) continue;
+        if (kind < 0) return;
+        const int s = li * SW + lj;
         if (kind == 0) {
             const size_t cell = (size_t)(i0 - 1 + li) * M.nj + (j0 - 1 + lj);
             float d[5];
@@ -149,12 +151,21 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
                 d[m] = (float)(st.cold[m * ncell + cell] - S.ref.c[m]);
                 if (st.dq) d[m] += st.dq[m * ncell + cell];
             }
-            put_slot_dev_mx(P, S, s, d[0], d[1], d[2], d[3], d[4]);
+            put_slot_dev_mx(P, S, s, d[0], d[1], d[2], d[3], d[4], own);
         } else {
             Prim p;
             ghost_state(P, M, st, kind, along, p);
-            put_slot_ghost_mx(S, s, p);
+            put_slot_ghost_mx(S, s, p, own);
         }
+    };
+    // own cell first (its T, RHO, P - Pref kept), then the ring
+    float3 own = make_float3(0.0f, 0.0f, 0.0f);
+    slot(threadIdx.y + 1, threadIdx.x + 1, own);
+    if (tid < NRING) {
+        int li, lj;
+        ring_slot(tid, li, lj);
+        float3 o;
+        slot(li, lj, o);
     }
     __syncthreads();
     if (!bulk_wait(&S.bar)) {
@@ -218,7 +229,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
             const float DRX = drac * ga + drbd * gb, DRY = drac * gcf + drbd * gd;
             const float DUX = duac * ga + dubd * gb, DUY = duac * gcf + dubd * gd;
             const float DVX = dvac * ga + dvbd * gb, DVY = dvac * gcf + dvbd * gd;
-            const float2 trc = S.tr[c];
+            const float2 trc = make_float2(own.x, own.y);
             const float RHO = trc.y, RI = S.ref.ri + S.drq[c].x, T = trc.x;
             const float AMU = (float)P.suth_amol * pow06f(T);
             const float CHI = RHO * RI / ((float)CMU * AMU);
@@ -256,7 +267,7 @@ __device__ __forceinline__ void stage_mx_tile(const Params& P, const Mesh& M, co
                 // SOURCE3 = (P - TTT)/YCC: the reference pressure's part cancels the
                 // reference flux in FP64
                 R64[2] -= VOL * (S.ref.q.p * rycc);
-                R[2] += volf * ((TTT - S.dp[c]) * (float)rycc);
+                R[2] += volf * ((TTT - own.z) * (float)rycc);
             } else {
                 const float DIVVEL = DUX + DVY;
                 PK = AMUT / RHO *

@@ -47,6 +47,16 @@ constexpr int SW = TJ + 2;
 constexpr int NSLOT = (TI + 2) * SW;
 constexpr int NW = TJ + 3;
 constexpr int NNODE = (TI + 3) * NW;
+// The halo ring of the slot grid, 2 (TI + 2) + 2 TJ + 4 positions as ring slots r:
+// position (li, lj) of r runs along the first and last slot rows, then along the first
+// and last slot columns between them.
+constexpr int NRING = 2 * SW + 2 * TI;
+__device__ __forceinline__ void ring_slot(int r, int& li, int& lj) {
+    if (r < SW) { li = 0; lj = r; }
+    else if (r < 2 * SW) { li = TI + 1; lj = r - SW; }
+    else if (r < 2 * SW + TI) { li = 1 + r - 2 * SW; lj = 0; }
+    else { li = 1 + r - 2 * SW - TI; lj = SW - 1; }
+}
 constexpr int AW = TJ + 1;  // node-average grid (TI+1) x (TJ+1)
 constexpr int NAVG = (TI + 1) * AW;
 
