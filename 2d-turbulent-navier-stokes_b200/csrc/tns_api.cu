@@ -976,7 +976,7 @@ int tns_kernel_times(tns_handle* h, int kernel, double* ms, long long* launches)
 long long tns_launch_count(tns_handle* h) { return h ? h->launches : -1; }
 
 int tns_debug_math(int fn, long long n, const double* a, const double* b, double* out) {
-    if ((fn != 0 && fn != 1) || n < 0 || (n > 0 && (!a || !out || (fn == 1 && !b)))) return TNS_ERR_ARG;
+    if (fn < 0 || fn > 2 || n < 0 || (n > 0 && (!a || !out || (fn == 1 && !b)))) return TNS_ERR_ARG;
     if (n == 0) return TNS_OK;
     double* d = nullptr;
     const size_t bytes = (size_t)n * sizeof(double);

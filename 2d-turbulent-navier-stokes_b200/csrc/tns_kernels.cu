@@ -938,12 +938,12 @@ k_batch_persistent(const BatchCase* __restrict__ cases, const int4* __restrict__
 // ---------------------------------------------------------------- math check
 
 // Evaluates one of the FP64 helpers the kernels use, elementwise, for testing their
-// accuracy: fn 0 = pow06(a), 1 = tanh_ratio(a, b).
+// accuracy: fn 0 = pow06(a), 1 = tanh_ratio(a, b), 2 = expm1_nonneg(a).
 __global__ void k_debug_math(int fn, long long n, const double* __restrict__ a, const double* __restrict__ b,
                              double* __restrict__ out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = fn == 0 ? pow06(a[i]) : tanh_ratio(a[i], b[i]);
+    out[i] = fn == 0 ? pow06(a[i]) : (fn == 1 ? tanh_ratio(a[i], b[i]) : expm1_nonneg(a[i]));
 }
 
 void launch_debug_math(int fn, long long n, const double* a, const double* b, double* out, cudaStream_t s) {

@@ -136,7 +136,8 @@ int tns_debug_fetch(tns_handle *h, int which, double *out);
 
 /* Accuracy check of the FP64 helpers the kernels use in place of library calls,
  * elementwise on n host values: fn 0 = T**0.6 (viscosity law, viscous.f90:188),
- * fn 1 = tanh(a)/tanh(b) (damping ratios, viscous.f90:191, source_terms.f90:64-67).
+ * fn 1 = tanh(a)/tanh(b) (damping ratios, viscous.f90:191, source_terms.f90:64-67),
+ * fn 2 = expm1(a) for 0 <= a <= 40 (the function behind fn 1).
  * For tests; allocates and frees its own device memory. */
 int tns_debug_math(int fn, long long n, const double *a, const double *b, double *out);
 

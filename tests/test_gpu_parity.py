@@ -212,8 +212,8 @@ def test_graph_replay_equals_direct_launches():
 
 def test_fp64_math_helpers_match_libm():
     """The kernels compute T**0.6 by two Newton steps from a single-precision estimate
-    and tanh(a)/tanh(b) through expm1; both agree with numpy's pow / tanh to a few ulp
-    over the temperatures and damping arguments the solver meets."""
+    and tanh(a)/tanh(b) through their own expm1; all agree with numpy's pow / tanh /
+    expm1 to a few ulp over the temperatures and damping arguments the solver meets."""
     from tnsgpu import _lib
     L = _lib.load()
     t = np.concatenate([np.logspace(0, 4, 20000), np.random.default_rng(0).uniform(100, 4000, 20000)])
@@ -228,3 +228,11 @@ def test_fp64_math_helpers_match_libm():
     assert L.tns_debug_math(1, a.size, a.ctypes.data, b.ctypes.data, out.ctypes.data) == 0
     ref = np.tanh(a) / np.tanh(b)
     assert np.max(np.abs(out - ref) / np.abs(ref)) < 16 * np.finfo(float).eps
+    # the expm1 behind it (Cody-Waite reduction + Taylor series) over its range [0, 40]
+    x = np.concatenate([[0.0, 40.0, np.log(2) / 2, 5e-324], 10 ** rng.uniform(-300, -1, 20000),
+                        rng.uniform(0, 1, 20000), rng.uniform(0, 40, 20000)])
+    out = np.zeros_like(x)
+    assert L.tns_debug_math(2, x.size, x.ctypes.data, None, out.ctypes.data) == 0
+    ref = np.expm1(x)
+    nz = ref != 0
+    assert out[0] == 0.0 and np.max(np.abs(out[nz] - ref[nz]) / ref[nz]) < 2 * np.finfo(float).eps
