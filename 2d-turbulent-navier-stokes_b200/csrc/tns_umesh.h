@@ -56,6 +56,13 @@ struct UMesh {
     const int* pptr;      // [nport+1] the cells of its port line, from the parent across
     const int* pcell;
     const double* pdely;  // DELY of each of those cells for the ghost's side
+    // viscous faces: each face evaluated once, in the orientation of its owner cell (the
+    // lower id of two cells; the cell of a ghost face); fcell[e] = 4 * owner + face, and
+    // per cell face fref[k][ne] = e (the cell owns it) or ~e (its neighbour does: the cell
+    // adds -F_e)
+    int nface;
+    const int* fcell;
+    const int* fref;
 };
 
 struct StageArgsU {
@@ -75,7 +82,7 @@ void launch_u_prim(const Params& P, const UMesh& M, const double* q, double* W, 
 void launch_u_gport(const Params& P, const UMesh& M, const double* q, cudaStream_t s);
 void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, double* d,
                           double* dt, const double* dtmin, cudaStream_t s);
-void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vis,
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, double* vis,
                       cudaStream_t s);
 void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s);
 void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s);

@@ -8,7 +8,8 @@
 //   k_u_prim           primitives and fluxes of every cell and ghost (turbnstwod.f90:204-227,
 //                      boundary.f90:24-327) into a slot field set W
 //   k_u_node_avg       NODAL_AVERAGE with the bc.in-order resets (viscous.f90:40-124), stage 1
-//   k_u_visc           the four faces of every cell (viscous.f90:62-70,130-217), stage 1
+//   k_u_vface/vsum     every face once, then the four faces of every cell in order
+//                      (viscous.f90:62-70,130-217), stage 1
 //   k_u_stage          source, residual and update (source_terms.f90:24-104, residual.f90:23-83)
 // the prim -> stage pair once per RK stage.  The host side lays the mesh out: cells in
 // reverse Cuthill-McKee order (neighbours near in memory), ghosts after them in bc.in
@@ -202,14 +203,29 @@ __global__ void __launch_bounds__(UT) k_u_node_avg(Params P, UMesh M, const doub
     const size_t ns = (size_t)M.ne + M.ng;
     double un = 0.0, vn = 0.0, tn = 0.0, rhon = 0.0, rn = 0.0;
     const int e0 = M.nptr[n], e1 = M.nptr[n + 1];
-    for (int e = e0; e < e1; e++) {
-        const int s = M.nslot[e];
-        un = un + W[UW_U * ns + s];
-        vn = vn + W[UW_V * ns + s];
-        tn = tn + W[UW_T * ns + s];
-        rhon = rhon + W[UW_RHO * ns + s];
-        rn = rn + W[UW_RI * ns + s];
-        const int r = M.nreset[e];
+    // the first NB contributions' values are loaded together, then summed in order
+    constexpr int NB = 4;
+    double w[NB][5];
+    int rs[NB];
+#pragma unroll
+    for (int q = 0; q < NB; q++) {
+        rs[q] = 0;
+        if (e0 + q < e1) {
+            const int sl = M.nslot[e0 + q];
+            rs[q] = M.nreset[e0 + q];
+            w[q][0] = W[UW_U * ns + sl];
+            w[q][1] = W[UW_V * ns + sl];
+            w[q][2] = W[UW_T * ns + sl];
+            w[q][3] = W[UW_RHO * ns + sl];
+            w[q][4] = W[UW_RI * ns + sl];
+        }
+    }
+    auto add = [&](const double* v, int r) {
+        un = un + v[0];
+        vn = vn + v[1];
+        tn = tn + v[2];
+        rhon = rhon + v[3];
+        rn = rn + v[4];
         if (r == 4) {
             vn = 0.0;
         } else if (r == 5) {
@@ -217,6 +233,15 @@ __global__ void __launch_bounds__(UT) k_u_node_avg(Params P, UMesh M, const doub
             vn = 0.0;
             rn = P.rtol_rtred;
         }
+    };
+#pragma unroll
+    for (int q = 0; q < NB; q++)
+        if (e0 + q < e1) add(w[q], rs[q]);
+    for (int e = e0 + NB; e < e1; e++) {
+        const int sl = M.nslot[e];
+        const double v[5] = {W[UW_U * ns + sl], W[UW_V * ns + sl], W[UW_T * ns + sl], W[UW_RHO * ns + sl],
+                             W[UW_RI * ns + sl]};
+        add(v, M.nreset[e]);
     }
     const double DF = (double)(e1 - e0);
     const size_t nn = (size_t)M.nnode;
@@ -227,36 +252,57 @@ __global__ void __launch_bounds__(UT) k_u_node_avg(Params P, UMesh M, const doub
     na[4 * nn + n] = dmax1(P.rtol, rn / DF);
 }
 
-// COMPUTE_VISCOUS face loop (viscous.f90:62-70): faces 1..4 of every cell in its own
-// orientation, face 1 assigning and the others adding.
-__global__ void __launch_bounds__(UT) k_u_visc(Params P, UMesh M, const double* __restrict__ W,
-                                               const double* __restrict__ na, double* __restrict__ vis) {
+// COMPUTE_VISCOUS (viscous.f90:62-70, 130-217) in two passes.  k_u_vface evaluates each
+// face once, in the orientation of the cell that owns it (A = that cell, C = its
+// neighbour across face k, B = node k, D = node k+1); in the neighbour's orientation the
+// face has the same gradient and averages and the opposite face vector, so its flux is
+// the negative.  k_u_vsum then gives every cell its four faces in order, face 1
+// assigning and the others adding, as the reference's loop does.
+__global__ void __launch_bounds__(UT) k_u_vface(Params P, UMesh M, const double* __restrict__ W,
+                                                const double* __restrict__ na, double* __restrict__ vf) {
+    const int e = blockIdx.x * UT + threadIdx.x;
+    if (e >= M.nface) return;
+    const int ne = M.ne;
+    const int I = M.fcell[e] >> 2, k = M.fcell[e] & 3;
+    const size_t ns = (size_t)ne + M.ng, nn = (size_t)M.nnode;
+    const int nbn = M.nod[k * ne + I], ndn = M.nod[((k + 1) & 3) * ne + I];
+    const int cc = M.nc[k * ne + I];
+    FaceVals f;
+    f.ua = W[UW_U * ns + I]; f.va = W[UW_V * ns + I]; f.ta = W[UW_T * ns + I];
+    f.uc = W[UW_U * ns + cc]; f.vc = W[UW_V * ns + cc]; f.tc = W[UW_T * ns + cc];
+    f.ub = na[nbn]; f.vb = na[nn + nbn]; f.tb = na[2 * nn + nbn];
+    f.ud = na[ndn]; f.vd = na[nn + ndn]; f.td = na[2 * nn + ndn];
+    f.rhoa = W[UW_RHO * ns + I]; f.rhoc = W[UW_RHO * ns + cc];
+    f.rhob = na[3 * nn + nbn]; f.rhod = na[3 * nn + ndn];
+    f.ra = W[UW_RI * ns + I]; f.rc = W[UW_RI * ns + cc];
+    f.rb = na[4 * nn + nbn]; f.rd = na[4 * nn + ndn];
+    const double* G = M.fg + (size_t)k * ne + I;
+    const size_t st = (size_t)4 * ne;
+    double out[4];
+    viscous_face(P, f, M.cg[(UCG_SX1 + k) * ne + I], M.cg[(UCG_SY1 + k) * ne + I], G[UFG_GA * st],
+                 G[UFG_GB * st], G[UFG_GC * st], G[UFG_GD * st], P.iaxis == 1 ? G[UFG_RYAVG * st] : 0.0, out);
+    const size_t nf = (size_t)M.nface;
+#pragma unroll
+    for (int m = 0; m < 4; m++) vf[m * nf + e] = out[m];
+}
+
+__global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict__ vf, double* __restrict__ vis) {
     const int I = blockIdx.x * UT + threadIdx.x;
     const int ne = M.ne;
     if (I >= ne) return;
-    const size_t ns = (size_t)ne + M.ng, nn = (size_t)M.nnode;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-    for (int k = 0; k < 4; k++) {
-        const int nbn = M.nod[k * ne + I], ndn = M.nod[((k + 1) & 3) * ne + I];
-        const int cc = M.nc[k * ne + I];
-        FaceVals f;
-        f.ua = W[UW_U * ns + I]; f.va = W[UW_V * ns + I]; f.ta = W[UW_T * ns + I];
-        f.uc = W[UW_U * ns + cc]; f.vc = W[UW_V * ns + cc]; f.tc = W[UW_T * ns + cc];
-        f.ub = na[nbn]; f.vb = na[nn + nbn]; f.tb = na[2 * nn + nbn];
-        f.ud = na[ndn]; f.vd = na[nn + ndn]; f.td = na[2 * nn + ndn];
-        f.rhoa = W[UW_RHO * ns + I]; f.rhoc = W[UW_RHO * ns + cc];
-        f.rhob = na[3 * nn + nbn]; f.rhod = na[3 * nn + ndn];
-        f.ra = W[UW_RI * ns + I]; f.rc = W[UW_RI * ns + cc];
-        f.rb = na[4 * nn + nbn]; f.rd = na[4 * nn + ndn];
-        const double* G = M.fg + (size_t)k * ne + I;
-        const size_t st = (size_t)4 * ne;
-        double out[4];
-        viscous_face(P, f, M.cg[(UCG_SX1 + k) * ne + I], M.cg[(UCG_SY1 + k) * ne + I], G[UFG_GA * st],
-                     G[UFG_GB * st], G[UFG_GC * st], G[UFG_GD * st],
-                     P.iaxis == 1 ? G[UFG_RYAVG * st] : 0.0, out);
+    const size_t nf = (size_t)M.nface;
+    int r[4];
 #pragma unroll
-        for (int m = 0; m < 4; m++) acc[m] = k == 0 ? out[m] : acc[m] + out[m];
+    for (int k = 0; k < 4; k++) r[k] = M.fref[k * ne + I];
+    double acc[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int e = r[k] >= 0 ? r[k] : ~r[k];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const double v = r[k] >= 0 ? vf[m * nf + e] : -vf[m * nf + e];
+            acc[m] = k == 0 ? v : acc[m] + v;
+        }
     }
 #pragma unroll
     for (int m = 0; m < 4; m++) vis[m * ne + I] = acc[m];
@@ -421,10 +467,11 @@ void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, doub
     k_u_diss1<<<blocks(M.ne), UT, 0, s>>>(P, M, q, aux, dt, dtmin);
     k_u_diss2<<<blocks(M.ne), UT, 0, s>>>(M, q, aux, d);
 }
-void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vis,
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, double* vis,
                       cudaStream_t s) {
     k_u_node_avg<<<blocks(M.nnode), UT, 0, s>>>(P, M, W, na);
-    k_u_visc<<<blocks(M.ne), UT, 0, s>>>(P, M, W, na, vis);
+    k_u_vface<<<blocks(M.nface), UT, 0, s>>>(P, M, W, na, vf);
+    k_u_vsum<<<blocks(M.ne), UT, 0, s>>>(M, vf, vis);
 }
 void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s) {
     k_u_stage<<<blocks(M.ne), UT, 0, s>>>(P, M, A);
@@ -449,10 +496,11 @@ void launch_u_face_states(const Params& P, const UMesh& M, const double* W, doub
 
 struct tns_umesh_state {
     tns::UMesh M{};
-    DevBuf<int> nc, nod, gpar, gopp, gtype, gside, nptr, nslot, nreset, pghost, pptr, pcell;
-    DevBuf<double> cg, fg, cfldl, gsx, gsy, gyc, ginj, gport, pdely, W, aux, na;
+    DevBuf<int> nc, nod, gpar, gopp, gtype, gside, nptr, nslot, nreset, pghost, pptr, pcell, fcell, fref;
+    DevBuf<double> cg, fg, cfldl, gsx, gsy, gyc, ginj, gport, pdely, W, aux, na, vf;
     // host layout, uploaded by umesh_upload
-    std::vector<int> hnc, hnod, hgpar, hgopp, hgtype, hgside, hnptr, hnslot, hnreset, hpghost, hpptr, hpcell;
+    std::vector<int> hnc, hnod, hgpar, hgopp, hgtype, hgside, hnptr, hnslot, hnreset, hpghost, hpptr, hpcell,
+        hfcell, hfref;
     std::vector<double> hcg, hfg, hcfldl, hgsx, hgsy, hgyc, hginj, hpdely;
 };
 
@@ -528,6 +576,23 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
         }
     std::vector<int> cell_of = rcm_order(ne, adj), new_of(ne);
     for (int k = 0; k < ne; k++) new_of[cell_of[k]] = k;
+    // nodes in the order the renumbered cells first reach them, so that a node's
+    // contributions and a face's two nodes sit near the cells that read them
+    std::vector<int> node_new(nn, -1), node_old;
+    node_old.reserve(nn);
+    for (int k = 0; k < ne; k++)
+        for (int f = 0; f < 4; f++) {
+            const int n = NOD(cell_of[k], f);
+            if (n < 0 || n >= nn)
+                return h->fail(TNS_ERR_MESH, "cell %d: node %d out of range", cell_of[k] + 1, n + 1);
+            if (node_new[n] < 0) {
+                node_new[n] = (int)node_old.size();
+                node_old.push_back(n);
+            }
+        }
+    for (int n = 0; n < nn; n++)
+        if (node_new[n] < 0) return h->fail(TNS_ERR_MESH, "node %d belongs to no cell", n + 1);
+    auto NODN = [&](int c, int k) { return node_new[NOD(c, k)]; };  // renumbered node
 
     tns_umesh_state* u = new tns_umesh_state();
     h->umesh = u;
@@ -588,7 +653,7 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
         const int c = cell_of[k];
         for (int f = 0; f < 4; f++) {
             u->hnc[(size_t)f * ne + k] = slot(ncs[f][c]);
-            u->hnod[(size_t)f * ne + k] = NOD(c, f);
+            u->hnod[(size_t)f * ne + k] = NODN(c, f);
             u->hcg[(size_t)(UCG_SX1 + f) * ne + k] = sx[4 * (size_t)c + f];
             u->hcg[(size_t)(UCG_SY1 + f) * ne + k] = sy[4 * (size_t)c + f];
         }
@@ -614,6 +679,33 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
             u->hfg[UFG_RYAVG * st + at] = (iaxis == 1 && !(yavg < YAXIS_THRESH)) ? 1.0 / yavg : 0.0;
         }
     }
+    // viscous faces: a face between two cells is evaluated once, by the lower id, when the
+    // other cell meets it with its nodes in the opposite order (both cells oriented alike);
+    // otherwise, and for ghost faces, each cell evaluates its own
+    u->hfref.assign((size_t)4 * ne, 0);
+    u->hfcell.clear();
+    u->hfcell.reserve((size_t)2 * ne + ng);
+    {
+        std::vector<char> done((size_t)4 * ne, 0);
+        for (int k = 0; k < ne; k++)
+            for (int f = 0; f < 4; f++) {
+                if (done[(size_t)f * ne + k]) continue;
+                const int e = (int)u->hfcell.size();
+                u->hfcell.push_back(4 * k + f);
+                u->hfref[(size_t)f * ne + k] = e;
+                done[(size_t)f * ne + k] = 1;
+                const int v = u->hnc[(size_t)f * ne + k];
+                if (v >= ne || v <= k) continue;
+                const int nb = u->hnod[(size_t)f * ne + k], nd = u->hnod[(size_t)((f + 1) & 3) * ne + k];
+                for (int g = 0; g < 4; g++)
+                    if (!done[(size_t)g * ne + v] && u->hnc[(size_t)g * ne + v] == k &&
+                        u->hnod[(size_t)g * ne + v] == nd && u->hnod[(size_t)((g + 1) & 3) * ne + v] == nb) {
+                        u->hfref[(size_t)g * ne + v] = ~e;
+                        done[(size_t)g * ne + v] = 1;
+                        break;
+                    }
+            }
+    }
     // ghosts in bc.in order
     static const int OPP[5] = {0, 3, 4, 1, 2};  // side -> the opposite face
     u->hgpar.assign(ng, 0); u->hgopp.assign(ng, 0); u->hgtype.assign(ng, 0); u->hgside.assign(ng, 0);
@@ -637,27 +729,25 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
     // solver_state.f90:237-262): cells by id, then the ghosts in bc.in order
     std::vector<int> cnt(nn, 0);
     for (int c = 0; c < ne; c++)
-        for (int k = 0; k < 4; k++) cnt[NOD(c, k)]++;
+        for (int k = 0; k < 4; k++) cnt[NODN(c, k)]++;
     for (int L = 0; L < ng; L++) {
         const int p = m->nparent[L] - 1, s = m->nside[L];
-        cnt[NOD(p, s - 1)]++;
-        cnt[NOD(p, s & 3)]++;
+        cnt[NODN(p, s - 1)]++;
+        cnt[NODN(p, s & 3)]++;
     }
     u->hnptr.assign(nn + 1, 0);
     for (int n = 0; n < nn; n++) u->hnptr[n + 1] = u->hnptr[n] + cnt[n];
-    for (int n = 0; n < nn; n++)
-        if (cnt[n] == 0) return h->fail(TNS_ERR_MESH, "node %d belongs to no cell", n + 1);
     u->hnslot.assign(u->hnptr[nn], 0);
     u->hnreset.assign(u->hnptr[nn], 0);
     std::vector<int> fill(u->hnptr.begin(), u->hnptr.end() - 1);
     for (int c = 0; c < ne; c++)
         for (int k = 0; k < 4; k++) {
-            const int n = NOD(c, k);
+            const int n = NODN(c, k);
             u->hnslot[fill[n]++] = new_of[c];
         }
     for (int L = 0; L < ng; L++) {
         const int p = m->nparent[L] - 1, s = m->nside[L], ty = m->ntype[L];
-        for (int n : {NOD(p, s - 1), NOD(p, s & 3)}) {
+        for (int n : {NODN(p, s - 1), NODN(p, s & 3)}) {
             u->hnreset[fill[n]] = (ty == 4 || ty == 5) ? ty : 0;
             u->hnslot[fill[n]++] = ne + L;
         }
@@ -701,7 +791,7 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
     std::iota(h->ghost_line.begin(), h->ghost_line.end(), 0);
     h->ghost_id.assign(m->nghost, m->nghost + ng);
     h->node_of.resize(nn);
-    std::iota(h->node_of.begin(), h->node_of.end(), 1);
+    for (int k = 0; k < nn; k++) h->node_of[k] = node_old[k] + 1;
     h->M = Mesh{};
     h->M.ni = ne;
     h->M.nj = 1;
@@ -726,6 +816,7 @@ int umesh_upload(tns_handle* h) {
         (rc = upi(u->gopp, u->hgopp)) || (rc = upi(u->gtype, u->hgtype)) || (rc = upi(u->gside, u->hgside)) ||
         (rc = upi(u->nptr, u->hnptr)) || (rc = upi(u->nslot, u->hnslot)) || (rc = upi(u->nreset, u->hnreset)) ||
         (rc = upi(u->pghost, u->hpghost)) || (rc = upi(u->pptr, u->hpptr)) || (rc = upi(u->pcell, u->hpcell)) ||
+        (rc = upi(u->fcell, u->hfcell)) || (rc = upi(u->fref, u->hfref)) ||
         (rc = upd(u->cg, u->hcg)) || (rc = upd(u->fg, u->hfg)) || (rc = upd(u->cfldl, u->hcfldl)) ||
         (rc = upd(u->gsx, u->hgsx)) || (rc = upd(u->gsy, u->hgsy)) || (rc = upd(u->gyc, u->hgyc)) ||
         (rc = upd(u->ginj, u->hginj)) || (rc = upd(u->pdely, u->hpdely)))
@@ -734,6 +825,7 @@ int umesh_upload(tns_handle* h) {
         (rc = h->cuda(u->W.alloc((size_t)tns::UW_N * ((size_t)ne + ng)), "cudaMalloc")) ||
         (rc = h->cuda(u->aux.alloc((size_t)tns::UA_N * ne), "cudaMalloc")) ||
         (rc = h->cuda(u->na.alloc((size_t)5 * nn), "cudaMalloc")) ||
+        (rc = h->cuda(u->vf.alloc((size_t)4 * std::max<size_t>(u->hfcell.size(), 1)), "cudaMalloc")) ||
         (rc = h->cuda(cudaMemset(u->gport.p, 0, std::max(ng, 1) * 8), "cudaMemset")))
         return rc;
     tns::UMesh& M = u->M;
@@ -743,10 +835,11 @@ int umesh_upload(tns_handle* h) {
     M.gsx = u->gsx.p; M.gsy = u->gsy.p; M.gyc = u->gyc.p; M.ginj = u->ginj.p; M.gport = u->gport.p;
     M.nptr = u->nptr.p; M.nslot = u->nslot.p; M.nreset = u->nreset.p;
     M.pghost = u->pghost.p; M.pptr = u->pptr.p; M.pcell = u->pcell.p; M.pdely = u->pdely.p;
+    M.nface = (int)u->hfcell.size(); M.fcell = u->fcell.p; M.fref = u->fref.p;
     // the time-step kernels read CFL*DL through the structured view
     h->M.cfldl = u->cfldl.p;
     for (auto* v : {&u->hnc, &u->hnod, &u->hgpar, &u->hgopp, &u->hgside, &u->hnptr, &u->hnslot, &u->hnreset,
-                    &u->hpghost, &u->hpptr, &u->hpcell})
+                    &u->hpghost, &u->hpptr, &u->hpcell, &u->hfcell, &u->hfref})
         std::vector<int>().swap(*v);
     for (auto* v : {&u->hcg, &u->hfg, &u->hcfldl, &u->hgsx, &u->hgsy, &u->hgyc, &u->hpdely})
         std::vector<double>().swap(*v);
@@ -764,13 +857,24 @@ void enqueue_iteration_u(tns_handle* h, bool monitor) {
     static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
     const double* in[4] = {A, B, Cq, B};
     double* out[4] = {B, Cq, B, A};
+    // the dissipation (with DTMIN before it, LOCAL=0) reads only Q_old and writes D, DT
+    // and its own scratch: it runs on the side stream beside stage 1's field set and the
+    // viscous flux, joined before stage 1
+    const bool fork = !h->profile && h->side;
+    cudaStream_t sd = s;
+    if (fork) {
+        cudaEventRecord(h->fork, s);
+        cudaStreamWaitEvent(h->side, h->fork, 0);
+        sd = h->side;
+    }
     if (!P.local) {
         tns::launch_time_step_scratch(P, A, M.cfldl, M.ne, h->dt.p, h->partial.p, h->counter.p, h->dtmin.p,
-                                      tns::dtmin_blocks(h->M), s);
+                                      tns::dtmin_blocks(h->M), sd);
         h->launches++;
     }
-    tns::launch_u_dissipation(P, M, A, u->aux.p, h->d.p, h->dt.p, h->dtmin.p, s);
+    tns::launch_u_dissipation(P, M, A, u->aux.p, h->d.p, h->dt.p, h->dtmin.p, sd);
     h->launches += 2;
+    if (fork) cudaEventRecord(h->join, sd);
     if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
     for (int st = 0; st < 4; st++) {
         if (M.nport) {
@@ -780,8 +884,9 @@ void enqueue_iteration_u(tns_handle* h, bool monitor) {
         tns::launch_u_prim(P, M, in[st], u->W.p, s);
         h->launches++;
         if (st == 0) {
-            tns::launch_u_viscous(P, M, u->W.p, u->na.p, h->vis.p, s);
-            h->launches += 2;
+            tns::launch_u_viscous(P, M, u->W.p, u->na.p, u->vf.p, h->vis.p, s);
+            h->launches += 3;
+            if (fork) cudaStreamWaitEvent(s, h->join, 0);
         }
         tns::StageArgsU S{u->W.p, A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p, alpha[st],
                           (monitor && st == 3) ? h->cdiff.p : nullptr, st == 3 ? h->status.p : nullptr};
@@ -835,10 +940,10 @@ void umesh_release(tns_handle* h) {
     tns_umesh_state* u = h->umesh;
     if (!u) return;
     for (auto* b : {&u->nc, &u->nod, &u->gpar, &u->gopp, &u->gtype, &u->gside, &u->nptr, &u->nslot, &u->nreset,
-                    &u->pghost, &u->pptr, &u->pcell})
+                    &u->pghost, &u->pptr, &u->pcell, &u->fcell, &u->fref})
         b->release();
     for (auto* b : {&u->cg, &u->fg, &u->cfldl, &u->gsx, &u->gsy, &u->gyc, &u->ginj, &u->gport, &u->pdely, &u->W,
-                    &u->aux, &u->na})
+                    &u->aux, &u->na, &u->vf})
         b->release();
     delete u;
     h->umesh = nullptr;
