@@ -25,6 +25,9 @@ Cases (sizes as named in the solver's benchmark configurations):
                  T0) for the batched solver.
   backstep    -- a general (multi-block) mesh: a 2-D backward-facing step of three
                  blocks, one of them numbered from another corner (``multiblock_mesh``).
+  renumbered  -- any mesh with its cell and node ids shuffled and each cell's faces
+                 starting at another corner: the same cells in GAMBIT-like numbering,
+                 which the solver runs on its general-mesh path (``renumbered_mesh``).
 """
 from __future__ import annotations
 
@@ -377,3 +380,39 @@ CASES = {
     "port_4096x1536": lambda: (port_mesh(4096, 1536), port_flow()),
     "nozzle_2d_115x50": lambda: (nozzle_2d_mesh(115, 50), nozzle_2d_flow()),
 }
+
+
+def renumbered_mesh(mesh: Mesh, seed: int = 0, rotate: bool = True):
+    """The same cells, nodes and ghosts under random ids (``default_rng(seed)``) and,
+    with ``rotate``, each cell's local node order shifted by a random 0..3 (its NC and
+    its ghosts' NSIDE follow).  Ghost ids and the bc.in line order are kept.  Returns
+    (mesh, cell_perm) where new cell id cell_perm[c] + 1 holds old cell c + 1, so a state
+    q of the old numbering is ``q_new[:, cell_perm] = q``."""
+    rng = np.random.default_rng(seed)
+    ne, nn = mesh.neles, mesh.nods
+    cperm = rng.permutation(ne)          # old cell c -> new index cperm[c]
+    nperm = rng.permutation(nn)          # old node n -> new index nperm[n]
+    rot = rng.integers(0, 4, ne) if rotate else np.zeros(ne, int)
+    inv = np.argsort(cperm)              # new index -> old cell
+    r = rot[inv]
+    cols = (np.arange(4)[None, :] + r[:, None]) % 4
+    old_nod = mesh.nod[inv[:, None], cols]
+    old_nc = mesh.nc[inv[:, None], cols]
+    nod = nperm[old_nod - 1] + 1
+    nc = np.where(old_nc <= ne, cperm[np.clip(old_nc, 1, ne) - 1] + 1, old_nc)
+    x = np.zeros(nn)
+    y = np.zeros(nn)
+    x[nperm] = mesh.x
+    y[nperm] = mesh.y
+    xm = ym = None
+    if mesh.x_mm is not None:
+        xm = np.zeros(nn)
+        ym = np.zeros(nn)
+        xm[nperm] = mesh.x_mm
+        ym[nperm] = mesh.y_mm
+    par = mesh.nparent - 1
+    side = ((mesh.nside - 1 - rot[par]) % 4 + 1).astype(np.int32)
+    out = dataclasses.replace(mesh, x=x, y=y, x_mm=xm, y_mm=ym, nod=nod.astype(np.int32),
+                              nc=nc.astype(np.int32), nparent=(cperm[par] + 1).astype(np.int32),
+                              nside=side, shape=None)
+    return out, cperm

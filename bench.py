@@ -278,6 +278,24 @@ def run_ours(args, rank, world, dev):
         other = {"precision": "fp64" if prec else "mixed", "value": replica_rate(mesh.neles, ms2 * 1e-3, world),
                  "ms_per_step": round(ms2, 5), "mixed_over_fp64": (ms2 / ms) if prec == 0 else (ms / ms2)}
 
+    # the same workload through the general-mesh (gather) path: cell and node ids
+    # shuffled and every cell's faces rotated, FP64
+    gen = None
+    if not args.no_general and prec == 0:
+        from tnsgpu import cases as cs
+        gmesh, gperm = cs.renumbered_mesh(mesh, seed=3)
+        gq = np.empty_like(c0)
+        gq[:, gperm] = c0
+        s3 = Solver(gmesh, flow, rinit, precision=0)
+        s3.set_stream(stream.cuda_stream)
+        s3.upload(gq)
+        ms3, l3 = time_steps(s3, stream, flush, min(K, 300), W, world, torch)
+        s3.close()
+        gen = {"workload": wname + ", cell and node ids shuffled, faces rotated (general-mesh path)",
+               "value": replica_rate(mesh.neles, ms3 * 1e-3, world), "ms_per_step": round(ms3, 5),
+               "steps": min(K, 300), "launches_per_step": l3 / min(K, 300),
+               "over_structured": ms3 / ms}
+
     adj = None
     if world == 1 and not args.no_adjoint:
         adj = adjoint_timing(torch, dev)
@@ -306,6 +324,7 @@ def run_ours(args, rank, world, dev):
         "device_ms_per_iteration_profiled": round(total_kms, 5),
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         "other_precision": other,
+        "general_mesh": gen,
         "adjoint": adj,
         "batch": bat,
         "cpu_baseline": cpu,
@@ -542,6 +561,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/primal timing")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-case sweep timing")
+    ap.add_argument("--no-general", action="store_true",
+                    help="skip the timing of the same workload on the general-mesh path")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint/primal timing (K = --steps, W = --warmup), for profiling")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
