@@ -3,9 +3,11 @@
 //
 // The reference works on any quad connectivity (geometry.f90:31-52 reads NOD(:,1:4) and
 // NC1..NC4 as given; every stencil gathers through NCk(I)).  Such a mesh is laid out
-// by a reverse Cuthill-McKee renumbering of its cells, so that the neighbours a cell
-// gathers sit close in memory; ghosts are slots NE..NE+NGHOSTS-1 in bc.in order, nodes
-// keep their ids.  Every kernel gathers through index arrays.
+// with its cells in the order of their centroids along a Hilbert curve, so that the
+// neighbours a cell gathers sit close in memory and each run of 256 cells is a compact
+// chunk with a short halo; ghosts are slots NE..NE+NGHOSTS-1 in bc.in order, nodes are
+// renumbered in the order the cells first reach them.  Kernels gather through index
+// arrays; the RK stages stage each chunk and its halo in shared memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -63,10 +65,18 @@ struct UMesh {
     int nface;
     const int* fcell;
     const int* fref;
+    // stage chunks: chunk b holds cells UT b .. UT b + UT - 1 and the halo slots
+    // cslot[cptr[b] .. cptr[b+1]) (cells of other chunks and ghosts its cells touch);
+    // lnb[k][ne] is the local slot of each cell's face-k neighbour (below UT: a cell of
+    // the chunk, UT + h: halo slot h); hmax the largest halo
+    int nchunk, hmax;
+    const int* cptr;
+    const int* cslot;
+    const int* lnb;
 };
+constexpr int UT = 256;  // threads per block of the general-mesh kernels, cells per stage chunk
 
 struct StageArgsU {
-    const double* W;     // slot field set of the stage input
     const double* qold;  // [5][ne] state at the start of the iteration
     double* qout;        // [5][ne] stage output (may alias qold: own-cell reads only)
     const double* d;     // [5][ne]
@@ -84,7 +94,10 @@ void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, doub
                           double* dt, const double* dtmin, cudaStream_t s);
 void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, double* vis,
                       cudaStream_t s);
-void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s);
+// one RK stage on state q, chunk by chunk; configure_u_chunk once per mesh
+void launch_u_stage_chunk(const Params& P, const UMesh& M, const StageArgsU& A, const double* q, cudaStream_t s);
+cudaError_t configure_u_chunk(const UMesh& M);
+size_t u_chunk_smem_bytes(const UMesh& M);
 void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s);
 void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_t s);
 void launch_u_boundary_sums(const Params& P, const UMesh& M, const double* W, int type, int side,

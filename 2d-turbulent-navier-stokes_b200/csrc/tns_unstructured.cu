@@ -10,11 +10,12 @@
 //   k_u_node_avg       NODAL_AVERAGE with the bc.in-order resets (viscous.f90:40-124), stage 1
 //   k_u_vface/vsum     every face once, then the four faces of every cell in order
 //                      (viscous.f90:62-70,130-217), stage 1
-//   k_u_stage          source, residual and update (source_terms.f90:24-104, residual.f90:23-83)
-// the prim -> stage pair once per RK stage.  The host side lays the mesh out: cells in
-// reverse Cuthill-McKee order (neighbours near in memory), ghosts after them in bc.in
-// order, the static geometry computed once with the reference's formulas
-// (geometry.f90:55-149).
+//   k_u_stage_chunk    per chunk of 256 cells: primitives and fluxes of its cells and halo
+//                      into shared memory, then source, residual and update
+//                      (source_terms.f90:24-104, residual.f90:23-83), each RK stage
+// The host side lays the mesh out: cells in Hilbert-curve order of their centroids
+// (neighbours near in memory, compact chunks), ghosts after them in bc.in order, the
+// static geometry computed once with the reference's formulas (geometry.f90:55-149).
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -27,21 +28,16 @@
 
 namespace tns {
 
-constexpr int UT = 256;  // threads per block of every kernel here
 
 __device__ __forceinline__ void u_cell_prim(const Params& P, const double* __restrict__ q, int ne, int c,
                                             Prim& p) {
     primitive(P, q[c], q[ne + c], q[2 * ne + c], q[3 * ne + c], q[4 * ne + c], p);
 }
 
-// Primitive / flux field set of every slot: cells from the state, ghosts by their BC
-// from the parent and (type 3) the parent's opposite neighbour.
-__global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* __restrict__ q,
-                                               double* __restrict__ W) {
-    const int s = blockIdx.x * UT + threadIdx.x;
-    const int ns = M.ne + M.ng;
-    if (s >= ns) return;
-    Prim p;
+// Primitives and fluxes of slot s: a cell from the state, a ghost by its BC from the
+// parent and (type 3) the parent's opposite neighbour.
+__device__ __forceinline__ void u_slot_prim(const Params& P, const UMesh& M, const double* __restrict__ q, int s,
+                                            Prim& p) {
     if (s < M.ne) {
         u_cell_prim(P, q, M.ne, s, p);
     } else {
@@ -54,6 +50,16 @@ __global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* 
         boundary_ghost(P, type, pa, op, M.gsx[L], M.gsy[L], M.gyc[L], M.cg[UCG_YCC * M.ne + par],
                        type == 6 ? M.gport[L] : 0.0, M.ginj[L], p);
     }
+}
+
+// Primitive / flux field set of every slot.
+__global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* __restrict__ q,
+                                               double* __restrict__ W) {
+    const int s = blockIdx.x * UT + threadIdx.x;
+    const int ns = M.ne + M.ng;
+    if (s >= ns) return;
+    Prim p;
+    u_slot_prim(P, M, q, s, p);
     const size_t n = (size_t)ns;
 #pragma unroll
     for (int m = 0; m < 5; m++) {
@@ -308,44 +314,71 @@ __global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict
     for (int m = 0; m < 4; m++) vis[m * ne + I] = acc[m];
 }
 
-// One RK stage of every cell: source terms, flux residual, update (source_terms.f90:24-104,
-// residual.f90:23-83), with the CDIFF reduction and the finite check where asked.
-__global__ void __launch_bounds__(UT) k_u_stage(Params P, UMesh M, StageArgsU A) {
-    const int I = blockIdx.x * UT + threadIdx.x;
-    const int ne = M.ne;
-    const size_t ns = (size_t)ne + M.ng;
-    const double* W = A.W;
+// One RK stage of one chunk of UT cells (source_terms.f90:24-104, residual.f90:23-83),
+// with the primitives and fluxes of the chunk's cells and halo staged in shared memory
+// instead of a field set in global memory: each thread evaluates its own cell (keeping
+// its T, P, RHO) and the threads then share the halo slots.  (It gives bitwise the
+// results of a slot field set in global memory gathered per cell.)  Shared memory:
+// (UT + hmax) slots of (F_m, G_m) x 5, (U, V), (C5/C1, |V|).
+__global__ void __launch_bounds__(UT, 3) k_u_stage_chunk(Params P, UMesh M, StageArgsU A,
+                                                         const double* __restrict__ q) {
+    extern __shared__ double2 usm[];
+    const int ns = UT + M.hmax;
+    double2* fg = usm;
+    double2* uv = usm + 5 * ns;
+    double2* rq = uv + ns;
+    const int ne = M.ne, t = threadIdx.x;
+    const int c0 = blockIdx.x * UT, I = c0 + t;
+    const int h0 = M.cptr[blockIdx.x], nh = M.cptr[blockIdx.x + 1] - h0;
+    auto put = [&](int s, const Prim& p) {
+#pragma unroll
+        for (int m = 0; m < 5; m++) fg[m * ns + s] = make_double2(p.f[m], p.g[m]);
+        uv[s] = make_double2(p.u, p.v);
+        rq[s] = make_double2(p.ri, p.qm);
+    };
+    double own_t = 0.0, own_p = 0.0, own_rho = 0.0;
+    if (I < ne) {
+        Prim p;
+        u_cell_prim(P, q, ne, I, p);
+        put(t, p);
+        own_t = kept(p.t);
+        own_p = kept(p.p);
+        own_rho = kept(p.rho);
+    }
+    for (int h = t; h < nh; h += UT) {
+        Prim p;
+        u_slot_prim(P, M, q, M.cslot[h0 + h], p);
+        put(UT + h, p);
+    }
+    __syncthreads();
     double dv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (I < ne) {
         int nb[4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) nb[k] = M.nc[k * ne + I];
+        for (int k = 0; k < 4; k++) nb[k] = M.lnb[k * ne + I];
         const double* G = M.cg + I;
         double src3, src5;
         {
             SrcIn s;
             s.ga = G[UCG_GA * ne]; s.gb = G[UCG_GB * ne]; s.gc = G[UCG_GC * ne]; s.gd = G[UCG_GD * ne];
-            s.ua = W[UW_U * ns + nb[0]]; s.ub = W[UW_U * ns + nb[1]];
-            s.uc = W[UW_U * ns + nb[2]]; s.ud = W[UW_U * ns + nb[3]];
-            s.va = W[UW_V * ns + nb[0]]; s.vb = W[UW_V * ns + nb[1]];
-            s.vc = W[UW_V * ns + nb[2]]; s.vd = W[UW_V * ns + nb[3]];
-            s.ra = W[UW_RI * ns + nb[0]]; s.rb = W[UW_RI * ns + nb[1]];
-            s.rc = W[UW_RI * ns + nb[2]]; s.rd = W[UW_RI * ns + nb[3]];
-            s.qa = W[UW_QM * ns + nb[0]]; s.qb = W[UW_QM * ns + nb[1]];
-            s.qc = W[UW_QM * ns + nb[2]]; s.qd = W[UW_QM * ns + nb[3]];
-            source_terms(P, s, W[UW_RHO * ns + I], W[UW_RI * ns + I], W[UW_T * ns + I], W[UW_P * ns + I],
-                         W[UW_V * ns + I], G[UCG_YCC * ne], G[UCG_RYCC * ne], src3, src5);
+            const double2 ua = uv[nb[0]], ub = uv[nb[1]], uc = uv[nb[2]], ud = uv[nb[3]];
+            const double2 ra = rq[nb[0]], rb = rq[nb[1]], rc = rq[nb[2]], rd = rq[nb[3]];
+            s.ua = ua.x; s.ub = ub.x; s.uc = uc.x; s.ud = ud.x;
+            s.va = ua.y; s.vb = ub.y; s.vc = uc.y; s.vd = ud.y;
+            s.ra = ra.x; s.rb = rb.x; s.rc = rc.x; s.rd = rd.x;
+            s.qa = ra.y; s.qb = rb.y; s.qc = rc.y; s.qd = rd.y;
+            source_terms(P, s, own_rho, rq[t].x, own_t, own_p, uv[t].y, G[UCG_YCC * ne], G[UCG_RYCC * ne], src3,
+                         src5);
         }
         double R[5];
 #pragma unroll
         for (int m = 0; m < 5; m++) {
-            const double* F = W + (UW_F1 + m) * ns;
-            const double* Gm = W + (UW_G1 + m) * ns;
-            const double FI = F[I], GI = Gm[I];
-            R[m] = HALF * ((FI + F[nb[0]]) * G[UCG_SX1 * ne] + (GI + Gm[nb[0]]) * G[UCG_SY1 * ne] +
-                           (FI + F[nb[1]]) * G[UCG_SX2 * ne] + (GI + Gm[nb[1]]) * G[UCG_SY2 * ne] +
-                           (FI + F[nb[2]]) * G[UCG_SX3 * ne] + (GI + Gm[nb[2]]) * G[UCG_SY3 * ne] +
-                           (FI + F[nb[3]]) * G[UCG_SX4 * ne] + (GI + Gm[nb[3]]) * G[UCG_SY4 * ne]);
+            const double2* F = fg + m * ns;
+            const double2 Fi = F[t], a = F[nb[0]], b = F[nb[1]], e = F[nb[2]], d = F[nb[3]];
+            R[m] = HALF * ((Fi.x + a.x) * G[UCG_SX1 * ne] + (Fi.y + a.y) * G[UCG_SY1 * ne] +
+                           (Fi.x + b.x) * G[UCG_SX2 * ne] + (Fi.y + b.y) * G[UCG_SY2 * ne] +
+                           (Fi.x + e.x) * G[UCG_SX3 * ne] + (Fi.y + e.y) * G[UCG_SY3 * ne] +
+                           (Fi.x + d.x) * G[UCG_SX4 * ne] + (Fi.y + d.y) * G[UCG_SY4 * ne]);
         }
         const double VOL = G[UCG_VOL * ne];
         R[4] = R[4] - VOL * src5;
@@ -382,6 +415,8 @@ __global__ void __launch_bounds__(UT) k_u_stage(Params P, UMesh M, StageArgsU A)
         }
     }
 }
+
+size_t u_chunk_smem_bytes(const UMesh& M) { return sizeof(double2) * 7 * ((size_t)UT + M.hmax); }
 
 // POSTPROCESS node averages (solver_state.f90:237-281): P, U, V, T of the contributions
 // in the same visit order, divided by their count; out [4][nnode].
@@ -473,8 +508,12 @@ void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* 
     k_u_vface<<<blocks(M.nface), UT, 0, s>>>(P, M, W, na, vf);
     k_u_vsum<<<blocks(M.ne), UT, 0, s>>>(M, vf, vis);
 }
-void launch_u_stage(const Params& P, const UMesh& M, const StageArgsU& A, cudaStream_t s) {
-    k_u_stage<<<blocks(M.ne), UT, 0, s>>>(P, M, A);
+void launch_u_stage_chunk(const Params& P, const UMesh& M, const StageArgsU& A, const double* q, cudaStream_t s) {
+    k_u_stage_chunk<<<M.nchunk, UT, u_chunk_smem_bytes(M), s>>>(P, M, A, q);
+}
+cudaError_t configure_u_chunk(const UMesh& M) {
+    return cudaFuncSetAttribute(k_u_stage_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)u_chunk_smem_bytes(M));
 }
 void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s) {
     k_u_post_avg<<<blocks(M.nnode), UT, 0, s>>>(M, W, out);
@@ -496,11 +535,13 @@ void launch_u_face_states(const Params& P, const UMesh& M, const double* W, doub
 
 struct tns_umesh_state {
     tns::UMesh M{};
-    DevBuf<int> nc, nod, gpar, gopp, gtype, gside, nptr, nslot, nreset, pghost, pptr, pcell, fcell, fref;
+    DevBuf<int> nc, nod, gpar, gopp, gtype, gside, nptr, nslot, nreset, pghost, pptr, pcell, fcell, fref, cptr,
+        cslot, lnb;
     DevBuf<double> cg, fg, cfldl, gsx, gsy, gyc, ginj, gport, pdely, W, aux, na, vf;
     // host layout, uploaded by umesh_upload
     std::vector<int> hnc, hnod, hgpar, hgopp, hgtype, hgside, hnptr, hnslot, hnreset, hpghost, hpptr, hpcell,
-        hfcell, hfref;
+        hfcell, hfref, hcptr, hcslot, hlnb;
+    int hmax = 0;
     std::vector<double> hcg, hfg, hcfldl, hgsx, hgsy, hgyc, hginj, hpdely;
 };
 
@@ -508,40 +549,45 @@ namespace tns_rt {
 
 namespace {
 
-// Reverse Cuthill-McKee order of the cells over the cell-to-cell adjacency of NC1..NC4:
-// breadth-first from a least-connected cell of each component, neighbours by ascending
-// degree, the whole order reversed.  Returns new index -> cell.
-std::vector<int> rcm_order(int ne, const std::vector<int>& adj /* [ne][4], -1 = none */) {
-    std::vector<int> deg(ne, 0);
-    for (int c = 0; c < ne; c++)
-        for (int k = 0; k < 4; k++) deg[c] += adj[4 * c + k] >= 0;
-    std::vector<int> by_deg(ne);
-    std::iota(by_deg.begin(), by_deg.end(), 0);
-    std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-    std::vector<char> seen(ne, 0);
-    std::vector<int> order;
-    order.reserve(ne);
-    for (int start : by_deg) {
-        if (seen[start]) continue;
-        size_t head = order.size();
-        order.push_back(start);
-        seen[start] = 1;
-        while (head < order.size()) {
-            const int c = order[head++];
-            int nb[4], n = 0;
-            for (int k = 0; k < 4; k++) {
-                const int v = adj[4 * c + k];
-                if (v >= 0 && !seen[v]) nb[n++] = v;
+// Position along the Hilbert curve of order 20 (2^20 x 2^20 cells) of the point (x, y),
+// 0 <= x, y < 2^20: the classical quadrant recursion, with each sub-square rotated or
+// reflected so that the curve stays continuous.
+unsigned long long hilbert_index(unsigned x, unsigned y) {
+    constexpr unsigned N = 1u << 20;
+    unsigned long long d = 0;
+    for (unsigned s = N / 2; s > 0; s /= 2) {
+        const unsigned rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
+        d += (unsigned long long)s * s * ((3u * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) {
+                x = N - 1 - x;
+                y = N - 1 - y;
             }
-            std::sort(nb, nb + n, [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
-            for (int k = 0; k < n; k++) {
-                if (seen[nb[k]]) continue;
-                seen[nb[k]] = 1;
-                order.push_back(nb[k]);
-            }
+            const unsigned t = x;
+            x = y;
+            y = t;
         }
     }
-    std::reverse(order.begin(), order.end());
+    return d;
+}
+
+// Cells in the order of their centroids along a Hilbert curve over the mesh's bounding
+// box (ties by id): consecutive cells form compact patches, so a run of 256 of them has
+// a short halo, and neighbours sit nearby in memory.  Returns new index -> cell.
+std::vector<int> hilbert_order(const std::vector<double>& xc, const std::vector<double>& yc) {
+    const int ne = (int)xc.size();
+    double x0 = xc[0], x1 = xc[0], y0 = yc[0], y1 = yc[0];
+    for (int c = 1; c < ne; c++) {
+        x0 = std::min(x0, xc[c]); x1 = std::max(x1, xc[c]);
+        y0 = std::min(y0, yc[c]); y1 = std::max(y1, yc[c]);
+    }
+    const double sx = x1 > x0 ? 1048575.0 / (x1 - x0) : 0.0, sy = y1 > y0 ? 1048575.0 / (y1 - y0) : 0.0;
+    std::vector<unsigned long long> key(ne);
+    for (int c = 0; c < ne; c++)
+        key[c] = hilbert_index((unsigned)((xc[c] - x0) * sx), (unsigned)((yc[c] - y0) * sy));
+    std::vector<int> order(ne);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
     return order;
 }
 
@@ -568,13 +614,21 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
                 return h->fail(TNS_ERR_MESH, "cell %d face %d: neighbour %d is neither a cell nor a ghost", c + 1,
                                k + 1, v);
         }
-    std::vector<int> adj((size_t)4 * ne, -1);
-    for (int c = 0; c < ne; c++)
+    std::vector<double> xc0(ne), yc0(ne);
+    for (int c = 0; c < ne; c++) {
+        double sx = 0.0, sy = 0.0;
         for (int k = 0; k < 4; k++) {
-            const int v = ncs[k][c];
-            if (v >= 1 && v <= ne) adj[4 * (size_t)c + k] = v - 1;
+            const int n = NOD(c, k);
+            if (n < 0 || n >= nn) return h->fail(TNS_ERR_MESH, "cell %d: node %d out of range", c + 1, n + 1);
+            sx += m->x[n];
+            sy += m->y[n];
         }
-    std::vector<int> cell_of = rcm_order(ne, adj), new_of(ne);
+        xc0[c] = sx * 0.25;
+        yc0[c] = sy * 0.25;
+        if (!std::isfinite(xc0[c]) || !std::isfinite(yc0[c]))
+            return h->fail(TNS_ERR_MESH, "cell %d has a non-finite node coordinate", c + 1);
+    }
+    std::vector<int> cell_of = hilbert_order(xc0, yc0), new_of(ne);
     for (int k = 0; k < ne; k++) new_of[cell_of[k]] = k;
     // nodes in the order the renumbered cells first reach them, so that a node's
     // contributions and a face's two nodes sit near the cells that read them
@@ -583,8 +637,6 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
     for (int k = 0; k < ne; k++)
         for (int f = 0; f < 4; f++) {
             const int n = NOD(cell_of[k], f);
-            if (n < 0 || n >= nn)
-                return h->fail(TNS_ERR_MESH, "cell %d: node %d out of range", cell_of[k] + 1, n + 1);
             if (node_new[n] < 0) {
                 node_new[n] = (int)node_old.size();
                 node_old.push_back(n);
@@ -706,6 +758,39 @@ int umesh_build(tns_handle* h, const tns_mesh* m) {
                     }
             }
     }
+    // stage chunks of UT consecutive cells: each chunk's halo (the slots its cells touch
+    // outside it, in first-touch order) and every cell face's local neighbour slot
+    {
+        const int nch = (ne + UT - 1) / UT;
+        u->hcptr.assign(nch + 1, 0);
+        u->hcslot.clear();
+        u->hlnb.assign((size_t)4 * ne, 0);
+        std::vector<int> tag((size_t)ne + ng, -1), loc((size_t)ne + ng, 0);
+        int hmax = 0;
+        for (int b = 0; b < nch; b++) {
+            const int c0 = b * UT, c1 = std::min(ne, c0 + UT);
+            for (int k = c0; k < c1; k++)
+                for (int f = 0; f < 4; f++) {
+                    const int v = u->hnc[(size_t)f * ne + k];
+                    int l;
+                    if (v >= c0 && v < c1) {
+                        l = v - c0;
+                    } else {
+                        if (tag[v] != b) {
+                            tag[v] = b;
+                            loc[v] = UT + (int)u->hcslot.size() - u->hcptr[b];
+                            u->hcslot.push_back(v);
+                        }
+                        l = loc[v];
+                    }
+                    u->hlnb[(size_t)f * ne + k] = l;
+                }
+            u->hcptr[b + 1] = (int)u->hcslot.size();
+            hmax = std::max(hmax, u->hcptr[b + 1] - u->hcptr[b]);
+        }
+        // at most 4 UT halo slots: (UT + hmax) slots of 112 bytes fit a block's shared memory
+        u->hmax = hmax;
+    }
     // ghosts in bc.in order
     static const int OPP[5] = {0, 3, 4, 1, 2};  // side -> the opposite face
     u->hgpar.assign(ng, 0); u->hgopp.assign(ng, 0); u->hgtype.assign(ng, 0); u->hgside.assign(ng, 0);
@@ -817,6 +902,7 @@ int umesh_upload(tns_handle* h) {
         (rc = upi(u->nptr, u->hnptr)) || (rc = upi(u->nslot, u->hnslot)) || (rc = upi(u->nreset, u->hnreset)) ||
         (rc = upi(u->pghost, u->hpghost)) || (rc = upi(u->pptr, u->hpptr)) || (rc = upi(u->pcell, u->hpcell)) ||
         (rc = upi(u->fcell, u->hfcell)) || (rc = upi(u->fref, u->hfref)) ||
+        (rc = upi(u->cptr, u->hcptr)) || (rc = upi(u->cslot, u->hcslot)) || (rc = upi(u->lnb, u->hlnb)) ||
         (rc = upd(u->cg, u->hcg)) || (rc = upd(u->fg, u->hfg)) || (rc = upd(u->cfldl, u->hcfldl)) ||
         (rc = upd(u->gsx, u->hgsx)) || (rc = upd(u->gsy, u->hgsy)) || (rc = upd(u->gyc, u->hgyc)) ||
         (rc = upd(u->ginj, u->hginj)) || (rc = upd(u->pdely, u->hpdely)))
@@ -836,10 +922,13 @@ int umesh_upload(tns_handle* h) {
     M.nptr = u->nptr.p; M.nslot = u->nslot.p; M.nreset = u->nreset.p;
     M.pghost = u->pghost.p; M.pptr = u->pptr.p; M.pcell = u->pcell.p; M.pdely = u->pdely.p;
     M.nface = (int)u->hfcell.size(); M.fcell = u->fcell.p; M.fref = u->fref.p;
+    M.nchunk = (int)u->hcptr.size() - 1; M.hmax = u->hmax;
+    M.cptr = u->cptr.p; M.cslot = u->cslot.p; M.lnb = u->lnb.p;
+    if ((rc = h->cuda(tns::configure_u_chunk(M), "cudaFuncSetAttribute"))) return rc;
     // the time-step kernels read CFL*DL through the structured view
     h->M.cfldl = u->cfldl.p;
     for (auto* v : {&u->hnc, &u->hnod, &u->hgpar, &u->hgopp, &u->hgside, &u->hnptr, &u->hnslot, &u->hnreset,
-                    &u->hpghost, &u->hpptr, &u->hpcell, &u->hfcell, &u->hfref})
+                    &u->hpghost, &u->hpptr, &u->hpcell, &u->hfcell, &u->hfref, &u->hcptr, &u->hcslot, &u->hlnb})
         std::vector<int>().swap(*v);
     for (auto* v : {&u->hcg, &u->hfg, &u->hcfldl, &u->hgsx, &u->hgsy, &u->hgyc, &u->hpdely})
         std::vector<double>().swap(*v);
@@ -881,16 +970,19 @@ void enqueue_iteration_u(tns_handle* h, bool monitor) {
             tns::launch_u_gport(P, M, in[st], s);
             h->launches++;
         }
-        tns::launch_u_prim(P, M, in[st], u->W.p, s);
-        h->launches++;
+        // the field set W: stage 1's feeds the viscous flux; the chunked stage needs none
+        if (st == 0) {
+            tns::launch_u_prim(P, M, in[st], u->W.p, s);
+            h->launches++;
+        }
         if (st == 0) {
             tns::launch_u_viscous(P, M, u->W.p, u->na.p, u->vf.p, h->vis.p, s);
             h->launches += 3;
             if (fork) cudaStreamWaitEvent(s, h->join, 0);
         }
-        tns::StageArgsU S{u->W.p, A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p, alpha[st],
+        tns::StageArgsU S{A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p, alpha[st],
                           (monitor && st == 3) ? h->cdiff.p : nullptr, st == 3 ? h->status.p : nullptr};
-        tns::launch_u_stage(P, M, S, s);
+        tns::launch_u_stage_chunk(P, M, S, in[st], s);
         h->launches++;
     }
 }
@@ -940,7 +1032,7 @@ void umesh_release(tns_handle* h) {
     tns_umesh_state* u = h->umesh;
     if (!u) return;
     for (auto* b : {&u->nc, &u->nod, &u->gpar, &u->gopp, &u->gtype, &u->gside, &u->nptr, &u->nslot, &u->nreset,
-                    &u->pghost, &u->pptr, &u->pcell, &u->fcell, &u->fref})
+                    &u->pghost, &u->pptr, &u->pcell, &u->fcell, &u->fref, &u->cptr, &u->cslot, &u->lnb})
         b->release();
     for (auto* b : {&u->cg, &u->fg, &u->cfldl, &u->gsx, &u->gsy, &u->gyc, &u->ginj, &u->gport, &u->pdely, &u->W,
                     &u->aux, &u->na, &u->vf})
