@@ -47,3 +47,25 @@ def test_ramp_first_cell_height():
     ni, nj = m.shape
     y = m.y.reshape(ni + 1, nj + 1)
     assert abs((y[0, 1] - y[0, 0]) - 1.0e-5) < 1e-9
+
+
+def test_renumbered_mesh_is_the_same_mesh():
+    """cases.renumbered_mesh shuffles cell and node ids and rotates each cell's faces:
+    every cell keeps its corner coordinates in cyclic order, every face still meets the
+    neighbour (or ghost) it met before, and each ghost keeps its parent face."""
+    m = cases.port_mesh(24, 10)
+    g, perm = cases.renumbered_mesh(m, seed=5)
+    ne = m.neles
+    assert g.neles == ne and g.nods == m.nods and g.nghosts == m.nghosts
+    for c in range(ne):
+        k = perm[c]
+        old = [(m.x[n - 1], m.y[n - 1]) for n in m.nod[c]]
+        new = [(g.x[n - 1], g.y[n - 1]) for n in g.nod[k]]
+        r = old.index(new[0])
+        assert new == old[r:] + old[:r]
+        for f in range(4):  # face f of the new cell is face (f + r) % 4 of the old one
+            v_old, v_new = m.nc[c, (f + r) % 4], g.nc[k, f]
+            assert v_new == (perm[v_old - 1] + 1 if v_old <= ne else v_old)
+    for L in range(m.nghosts):
+        p_new, s_new = g.nparent[L] - 1, g.nside[L] - 1
+        assert g.nc[p_new, s_new] == m.nghost[L]
