@@ -249,13 +249,16 @@ __global__ void __launch_bounds__(UT) k_u_node_avg(Params P, UMesh M, const doub
                              W[UW_RI * ns + sl]};
         add(v, M.nreset[e]);
     }
-    const double DF = (double)(e1 - e0);
+    // one reciprocal of the contribution count (exact for 1, 2 and 4), as the
+    // structured kernel
+    const int cnt = e1 - e0;
+    const double idf = cnt == 4 ? 0.25 : 1.0 / (double)cnt;
     const size_t nn = (size_t)M.nnode;
-    na[n] = un / DF;
-    na[nn + n] = vn / DF;
-    na[2 * nn + n] = tn / DF;
-    na[3 * nn + n] = rhon / DF;
-    na[4 * nn + n] = dmax1(P.rtol, rn / DF);
+    na[n] = un * idf;
+    na[nn + n] = vn * idf;
+    na[2 * nn + n] = tn * idf;
+    na[3 * nn + n] = rhon * idf;
+    na[4 * nn + n] = dmax1(P.rtol, rn * idf);
 }
 
 // COMPUTE_VISCOUS (viscous.f90:62-70, 130-217) in two passes.  k_u_vface evaluates each

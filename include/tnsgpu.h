@@ -58,8 +58,8 @@ typedef struct tns_handle tns_handle;
  * (geometry.f90:55-149) and uploads everything.  A mesh whose cells form one structured
  * i x j block (any numbering) runs on the tiled kernels; any other quadrilateral mesh
  * (the reference reads any NOD / NC1..NC4) on the gather-indexed kernels, its cells
- * renumbered by reverse Cuthill-McKee on the device (the ABI's arrays keep the caller's
- * ids).  TNS_ERR_UNSUPPORTED: a general mesh with mixed precision, or with a type-3 ghost
+ * ordered along a Hilbert curve and its nodes renumbered on the device (the ABI's
+ * arrays keep the caller's ids).  TNS_ERR_UNSUPPORTED: a general mesh with mixed precision, or with a type-3 ghost
  * whose parent has no cell across the opposite face; the adjoint and the batch API also
  * refuse general meshes with it.
  * Replaces: CALL COMPUTE_GEOMETRY's consumers + the module state setup
