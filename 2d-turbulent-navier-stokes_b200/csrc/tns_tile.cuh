@@ -1,5 +1,5 @@
-// tns_tile.cuh -- tile geometry and the helpers every tile kernel shares: node staging,
-// halo classification, primitive variables of a cell, and the ghost state of a halo
+// tns_tile.cuh -- tile geometry and the helpers every tile kernel shares: bulk copies,
+// programmatic dependent launch, halo classification, primitive variables of a cell, and the ghost state of a halo
 // position (BC of boundary.f90:24-327 from the parent and its opposite neighbour).
 #pragma once
 
@@ -42,11 +42,9 @@ constexpr int VROWS = TI + TNS_VISC_EXTRA_ROW;
 constexpr int VNT = TJ * VROWS;
 
 
-// Halo-1 slot grid (TI+2) x (TJ+2), node grid (TI+3) x (TJ+3) (nodes of every halo cell).
+// Halo-1 slot grid (TI+2) x (TJ+2).
 constexpr int SW = TJ + 2;
 constexpr int NSLOT = (TI + 2) * SW;
-constexpr int NW = TJ + 3;
-constexpr int NNODE = (TI + 3) * NW;
 // The halo ring of the slot grid, 2 (TI + 2) + 2 TJ + 4 positions as ring slots r:
 // position (li, lj) of r runs along the first and last slot rows, then along the first
 // and last slot columns between them.
@@ -71,24 +69,11 @@ enum StageTileField { ST_GA, ST_GB, ST_GC, ST_GD, ST_RVOL, ST_RYCC, ST_NF };
 constexpr int STILE = 2 * SNN + ST_NF * TI * TJ;
 static_assert(STILE % 2 == 0, "a stage tile block must be a multiple of 16 bytes");
 
-__device__ __forceinline__ void load_nodes(const Mesh& M, int i0, int j0, double* snx, double* sny,
-                                           int nthreads = NTHREADS) {
-    const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int s = tid; s < NNODE; s += nthreads) {
-        const int a = i0 - 1 + s / NW, b = j0 - 1 + s % NW;
-        if (a >= 0 && a <= M.ni && b >= 0 && b <= M.nj) {
-            const size_t n = (size_t)a * (M.nj + 1) + b;
-            snx[s] = M.x[n];
-            sny[s] = M.y[n];
-        }
-    }
-}
-
 // Programmatic dependent launch: a tile kernel lets the next kernel in the stream start
 // as soon as all its blocks are running (pdl_trigger), and waits for the previous one
 // to finish, with its memory visible, before it touches data that kernel produced
-// (pdl_wait).  The node coordinates, which nothing writes, load before the wait.  Both
-// are no-ops when the kernel was not launched with the attribute.
+// (pdl_wait).  Static data, which nothing writes, may load before the wait.  Both are
+// no-ops when the kernel was not launched with the attribute.
 #ifndef TNS_PDL
 #define TNS_PDL 1
 #endif
