@@ -405,21 +405,6 @@ int alloc_state(tns_handle* h) {
 namespace tns_rt {
 
 // Timed launch wrapper: events around the launch when profiling.
-template <class F>
-void launch(tns_handle* h, int kid, F&& f) {
-    if (h->profile) cudaEventRecord(h->ev[0], h->stream);
-    f();
-    h->launches++;
-    if (h->profile) {
-        cudaEventRecord(h->ev[1], h->stream);
-        cudaEventSynchronize(h->ev[1]);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
-        h->kms[kid] += ms;
-        h->kcount[kid]++;
-    }
-}
-
 // The two pre-passes of an iteration read only Q_old and write disjoint arrays: the
 // dissipation (with DTMIN before it, LOCAL=0) on the side stream, the frozen viscous flux
 // (with stage 1's port columns before it) on the main stream, joined before stage 1.

@@ -111,6 +111,22 @@ struct tns_handle {
 
 
 namespace tns_rt {
+// Enqueues f() (nk kernel launches of kernel kind kid) on h->stream; with per-kernel
+// profiling on (tns_profile), brackets it with CUDA events and adds its device time.
+template <class F>
+void launch(tns_handle* h, int kid, F&& f, int nk = 1) {
+    if (h->profile) cudaEventRecord(h->ev[0], h->stream);
+    f();
+    h->launches += nk;
+    if (h->profile) {
+        cudaEventRecord(h->ev[1], h->stream);
+        cudaEventSynchronize(h->ev[1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        h->kms[kid] += ms;
+        h->kcount[kid]++;
+    }
+}
 // One RK4 iteration of a handle on h->stream (tns_api.cu): FP64 in place, mixed from
 // state buffer A to Aout.  The batch runtime captures these per case.
 void enqueue_iteration_f64(tns_handle* h, bool monitor);

@@ -959,34 +959,28 @@ void enqueue_iteration_u(tns_handle* h, bool monitor) {
         cudaStreamWaitEvent(h->side, h->fork, 0);
         sd = h->side;
     }
-    if (!P.local) {
-        tns::launch_time_step_scratch(P, A, M.cfldl, M.ne, h->dt.p, h->partial.p, h->counter.p, h->dtmin.p,
-                                      tns::dtmin_blocks(h->M), sd);
-        h->launches++;
-    }
-    tns::launch_u_dissipation(P, M, A, u->aux.p, h->d.p, h->dt.p, h->dtmin.p, sd);
-    h->launches += 2;
+    // (with per-kernel profiling everything runs in order on h->stream, each launch timed)
+    if (!P.local)
+        launch(h, K_DTMIN, [&] {
+            tns::launch_time_step_scratch(P, A, M.cfldl, M.ne, h->dt.p, h->partial.p, h->counter.p, h->dtmin.p,
+                                          tns::dtmin_blocks(h->M), sd);
+        });
+    launch(h, K_DISS, [&] { tns::launch_u_dissipation(P, M, A, u->aux.p, h->d.p, h->dt.p, h->dtmin.p, sd); }, 2);
     if (fork) cudaEventRecord(h->join, sd);
     if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
     for (int st = 0; st < 4; st++) {
-        if (M.nport) {
-            tns::launch_u_gport(P, M, in[st], s);
-            h->launches++;
-        }
-        // the field set W: stage 1's feeds the viscous flux; the chunked stage needs none
+        if (M.nport) launch(h, K_GPORT, [&] { tns::launch_u_gport(P, M, in[st], s); });
         if (st == 0) {
-            tns::launch_u_prim(P, M, in[st], u->W.p, s);
-            h->launches++;
-        }
-        if (st == 0) {
-            tns::launch_u_viscous(P, M, u->W.p, u->na.p, u->vf.p, h->vis.p, s);
-            h->launches += 3;
+            // stage 1's field set W feeds the viscous flux (the chunked stages need none)
+            launch(h, K_VISC, [&] {
+                tns::launch_u_prim(P, M, in[st], u->W.p, s);
+                tns::launch_u_viscous(P, M, u->W.p, u->na.p, u->vf.p, h->vis.p, s);
+            }, 4);
             if (fork) cudaStreamWaitEvent(s, h->join, 0);
         }
         tns::StageArgsU S{A, out[st], h->d.p, h->vis.p, h->dt.p, h->dtmin.p, alpha[st],
                           (monitor && st == 3) ? h->cdiff.p : nullptr, st == 3 ? h->status.p : nullptr};
-        tns::launch_u_stage_chunk(P, M, S, in[st], s);
-        h->launches++;
+        launch(h, K_STAGE, [&] { tns::launch_u_stage_chunk(P, M, S, in[st], s); });
     }
 }
 

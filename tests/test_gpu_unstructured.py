@@ -209,3 +209,25 @@ def test_full_size_renumbered_nozzle_plume_matches_the_structured_path():
     # (the oracle's own response to a 1e-15 perturbation, test_gpu_parity.py)
     assert np.all(err[:4] <= TOL) and err[4] <= 1e-4, err
     assert np.all(herr[:4] <= 1e-8) and herr[4] <= 1e-3, herr
+
+
+def test_general_path_per_kernel_profile():
+    """tns_profile on a general mesh: every launch of the iteration timed in order on the
+    handle's stream (dissipation, viscous flux with stage 1's field set, the four chunked
+    stages), with the same state as an unprofiled run."""
+    mesh, flow = cases.backstep_mesh(32, 96, 24, 12), cases.ramp_flow()
+    flow.istart = 0
+    c0, ri = _cold(mesh, flow)
+    a = Solver(mesh, flow, ri)
+    a.upload(c0)
+    a.run(7, 0)
+    b = Solver(mesh, flow, ri)
+    b.upload(c0)
+    b.profile(True)
+    b.run(7, 0)
+    assert np.array_equal(a.download(), b.download())
+    kt = b.kernel_times()
+    assert kt["dissipation"][1] == 7 and kt["viscous"][1] == 7 and kt["stage"][1] == 28
+    assert all(kt[k][0] > 0 for k in ("dissipation", "viscous", "stage"))
+    a.close()
+    b.close()
