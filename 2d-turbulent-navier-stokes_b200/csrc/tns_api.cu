@@ -379,6 +379,8 @@ int alloc_state(tns_handle* h) {
             (rc = h->cuda(cudaMemset(h->tref.p, 0, ntiles * tns::TREF_WORDS * 8), "cudaMemset")))
             return rc;
         h->M.tref = reinterpret_cast<tns::TileRefMx*>(h->tref.p);
+        // a general mesh's global time step (LOCAL=0) writes the FP64 per-cell DT
+        if (h->unstructured && (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc"))) return rc;
     } else if ((rc = h->cuda(h->qa.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->qb.alloc(5 * nc), "cudaMalloc")) ||
                (rc = h->cuda(h->qc.alloc(5 * nc), "cudaMalloc")) || (rc = h->cuda(h->d.alloc(5 * nc), "cudaMalloc")) ||
                (rc = h->cuda(h->vis.alloc(4 * nc), "cudaMalloc")) || (rc = h->cuda(h->dt.alloc(nc), "cudaMalloc"))) {
@@ -404,7 +406,6 @@ int alloc_state(tns_handle* h) {
 
 namespace tns_rt {
 
-// Timed launch wrapper: events around the launch when profiling.
 // The two pre-passes of an iteration read only Q_old and write disjoint arrays: the
 // dissipation (with DTMIN before it, LOCAL=0) on the side stream, the frozen viscous flux
 // (with stage 1's port columns before it) on the main stream, joined before stage 1.
@@ -428,6 +429,10 @@ void prepass(tns_handle* h, Diss&& diss, Visc&& visc) {
 // dQ_B, dQ_C between the stages).  The previous state survives in `in`, so the last
 // stage's input (in + dQ_B) can be reconstructed for tns_download_primitives.
 void enqueue_iteration_mx(tns_handle* h, bool monitor, double* A, double* Aout) {
+    if (h->unstructured) {
+        enqueue_iteration_u_mx(h, monitor, A, Aout);
+        return;
+    }
     const Params& P = h->P;
     const Mesh& M = h->M;
     const int np = (int)h->port_ghosts.size();
@@ -517,12 +522,7 @@ int tns_create(const tns_mesh* mesh, const tns_params* params, tns_handle** out)
     // host-side validation and layout first: mesh errors are reported without a GPU.  A
     // mesh that is not one structured block takes the general (gather) layout, FP64 only.
     rc = build_mesh(h, mesh);
-    if (rc == TNS_ERR_UNSUPPORTED) {
-        const std::string why = h->err;
-        if (h->precision != 0)
-            return h->fail(TNS_ERR_UNSUPPORTED, "mixed precision needs one structured i x j block (%s)", why.c_str());
-        rc = tns_rt::umesh_build(h, mesh);
-    }
+    if (rc == TNS_ERR_UNSUPPORTED) rc = tns_rt::umesh_build(h, mesh);
     if (rc) return rc;
     if ((rc = h->cuda(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
     h->stream = h->own;

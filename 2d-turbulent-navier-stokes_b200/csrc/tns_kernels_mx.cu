@@ -16,27 +16,11 @@
 // total-enthalpy levels, so the iteration can still converge by RTRED=1e-5 and more.
 #include "tns_device.cuh"
 #include "tns_kernels.h"
+#include "tns_mx.cuh"
 #include "tns_tile.cuh"
 #include "tns_batch.cuh"
 
 namespace tns {
-
-__device__ __forceinline__ float pow06f(float T) { return __expf(0.6f * __logf(T)); }
-
-// tanh for the FP32 path: the Maclaurin series x - x^3/3 + 2x^5/15 - 17x^7/315 +
-// 62x^9/2835 - 1382x^11/155925 + 21844x^13/6081075 for |x| < 1/4 (the first omitted
-// term is below 2e-12 relative there), and the identity tanh|x| = 1 - 2/(exp(2|x|)+1)
-// above, where its cancellation costs at most ~5e-7 relative.
-__device__ __forceinline__ float tanh_f32(float x) {
-    const float ax = fabsf(x);
-    if (ax < 0.25f) {
-        const float x2 = x * x;
-        return x * (1.0f + x2 * (-1.0f / 3.0f + x2 * (2.0f / 15.0f + x2 * (-17.0f / 315.0f +
-                    x2 * (62.0f / 2835.0f + x2 * (-1382.0f / 155925.0f + x2 * (21844.0f / 6081075.0f)))))));
-    }
-    const float r = 1.0f - __fdividef(2.0f, __expf(2.0f * ax) + 1.0f);
-    return copysignf(r, x);
-}
 
 // ------------------------------------------------------------------ stage kernel
 

@@ -89,6 +89,15 @@ struct StageArgsU {
 };
 
 void launch_u_prim(const Params& P, const UMesh& M, const double* q, double* W, cudaStream_t s);
+// the same for the mixed path's stage input COLD + dQ (dq null: COLD)
+void launch_u_prim_mx(const Params& P, const UMesh& M, const double* cold, const float* dq, double* W,
+                      cudaStream_t s);
+void launch_u_gport_mx(const Params& P, const UMesh& M, const double* cold, const float* dq, cudaStream_t s);
+// mixed path: D, DT (dissipation) and VIS (viscous) stored in FP32
+void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, float* d, float* dt,
+                          const double* dtmin, cudaStream_t s);
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, float* vis,
+                      cudaStream_t s);
 void launch_u_gport(const Params& P, const UMesh& M, const double* q, cudaStream_t s);
 void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, double* d,
                           double* dt, const double* dtmin, cudaStream_t s);
@@ -97,6 +106,12 @@ void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* 
 // one RK stage on state q, chunk by chunk; configure_u_chunk once per mesh
 void launch_u_stage_chunk(const Params& P, const UMesh& M, const StageArgsU& A, const double* q, cudaStream_t s);
 cudaError_t configure_u_chunk(const UMesh& M);
+// the mixed FP32/FP64 stage (tns_unstructured_mx.cu): A.cold + A.dqin in, A.dqout or
+// (stage 4) A.qout out; configure_u_chunk_mx once per mesh
+struct StageArgsMx;
+void launch_u_stage_chunk_mx(const Params& P, const UMesh& M, const StageArgsMx& A, cudaStream_t s);
+cudaError_t configure_u_chunk_mx(const UMesh& M);
+size_t u_chunk_mx_smem_bytes(const UMesh& M);
 size_t u_chunk_smem_bytes(const UMesh& M);
 void launch_u_post_average(const UMesh& M, const double* W, double* out, cudaStream_t s);
 void launch_u_prim_out(const UMesh& M, const double* W, double* out, cudaStream_t s);
@@ -112,6 +127,9 @@ namespace tns_rt {
 int umesh_build(tns_handle* h, const tns_mesh* m);
 int umesh_upload(tns_handle* h);
 void enqueue_iteration_u(tns_handle* h, bool monitor);
+// the mixed-precision iteration from state buffer A to Aout (FP32 increments between
+// the stages, as the structured mixed path)
+void enqueue_iteration_u_mx(tns_handle* h, bool monitor, double* A, double* Aout);
 // U, V, T, P of cells and ghosts of the last stage's input into h->primout ([4][ne+ng],
 // slot order)
 int umesh_primitives(tns_handle* h);

@@ -29,23 +29,25 @@
 namespace tns {
 
 
-__device__ __forceinline__ void u_cell_prim(const Params& P, const double* __restrict__ q, int ne, int c,
-                                            Prim& p) {
-    primitive(P, q[c], q[ne + c], q[2 * ne + c], q[3 * ne + c], q[4 * ne + c], p);
+// The state of a general mesh is read through an accessor (tns_tile.cuh): StateF64 (an
+// FP64 array [5][ne]) or StateMixed (FP64 COLD plus an FP32 stage increment).
+template <class St>
+__device__ __forceinline__ void u_cell_prim(const Params& P, const St& st, int c, Prim& p) {
+    primitive(P, st.c(0, c), st.c(1, c), st.c(2, c), st.c(3, c), st.c(4, c), p);
 }
 
 // Primitives and fluxes of slot s: a cell from the state, a ghost by its BC from the
 // parent and (type 3) the parent's opposite neighbour.
-__device__ __forceinline__ void u_slot_prim(const Params& P, const UMesh& M, const double* __restrict__ q, int s,
-                                            Prim& p) {
+template <class St>
+__device__ __forceinline__ void u_slot_prim(const Params& P, const UMesh& M, const St& st, int s, Prim& p) {
     if (s < M.ne) {
-        u_cell_prim(P, q, M.ne, s, p);
+        u_cell_prim(P, st, s, p);
     } else {
         const int L = s - M.ne;
         const int par = M.gpar[L], type = M.gtype[L];
         Prim pa, op;
-        u_cell_prim(P, q, M.ne, par, pa);
-        if (type == 3) u_cell_prim(P, q, M.ne, M.gopp[L], op);
+        u_cell_prim(P, st, par, pa);
+        if (type == 3) u_cell_prim(P, st, M.gopp[L], op);
         else op = pa;
         boundary_ghost(P, type, pa, op, M.gsx[L], M.gsy[L], M.gyc[L], M.cg[UCG_YCC * M.ne + par],
                        type == 6 ? M.gport[L] : 0.0, M.ginj[L], p);
@@ -53,13 +55,13 @@ __device__ __forceinline__ void u_slot_prim(const Params& P, const UMesh& M, con
 }
 
 // Primitive / flux field set of every slot.
-__global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* __restrict__ q,
-                                               double* __restrict__ W) {
+template <class St>
+__global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, St st, double* __restrict__ W) {
     const int s = blockIdx.x * UT + threadIdx.x;
     const int ns = M.ne + M.ng;
     if (s >= ns) return;
     Prim p;
-    u_slot_prim(P, M, q, s, p);
+    u_slot_prim(P, M, st, s, p);
     const size_t n = (size_t)ns;
 #pragma unroll
     for (int m = 0; m < 5; m++) {
@@ -77,13 +79,14 @@ __global__ void __launch_bounds__(UT) k_u_prim(Params P, UMesh M, const double* 
 
 // Port mass flux of each type-6 ghost: the sum of C1*U*DELY (*YCC) along its port line
 // in the line's order (the walk of the oracle's repaired COMPUTE_GPORT).
-__global__ void __launch_bounds__(UT) k_u_gport(Params P, UMesh M, const double* __restrict__ q) {
+template <class St>
+__global__ void __launch_bounds__(UT) k_u_gport(Params P, UMesh M, St st) {
     const int k = blockIdx.x * UT + threadIdx.x;
     if (k >= M.nport) return;
     double sum = 0.0;
     for (int e = M.pptr[k]; e < M.pptr[k + 1]; e++) {
         const int c = M.pcell[e];
-        const double c1 = q[c], u = q[M.ne + c] / c1;
+        const double c1 = st.c(0, c), u = st.c(1, c) / c1;
         double term = c1 * u * M.pdely[e];
         if (P.iaxis == 1) term = term * M.cg[UCG_YCC * M.ne + c];
         sum = (e == M.pptr[k]) ? term : sum + term;
@@ -105,8 +108,9 @@ enum UAux { UA_ANU, UA_ANURT, UA_VBD, UA_D2Q, UA_N = UA_D2Q + 5 };
 // DISSIPATION, first pass (solver_state.f90:78-160): DT (turbnstwod.f90:97-108), VOL/DT,
 // the pressure and turbulence sensors and the Laplacians; a ghost neighbour holds a
 // copy of its parent (this cell).
+template <class OutT>
 __global__ void __launch_bounds__(UT) k_u_diss1(Params P, UMesh M, const double* __restrict__ q,
-                                                double* __restrict__ aux, double* __restrict__ dt,
+                                                double* __restrict__ aux, OutT* __restrict__ dt,
                                                 const double* __restrict__ dtmin) {
     const int I = blockIdx.x * UT + threadIdx.x;
     const int ne = M.ne;
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(UT) k_u_diss1(Params P, UMesh M, const double*
         const double E = q[3 * ne + I] * rr;
         const double T = (E - 0.5 * (U * U + V * V)) * P.inv_cv;
         DT = M.cfldl[I] / (fabs(VEL) + sqrt(P.gamrr * T));
-        dt[I] = DT;
+        dt[I] = (OutT)DT;
     } else {
         DT = *dtmin;
     }
@@ -152,8 +156,9 @@ __global__ void __launch_bounds__(UT) k_u_diss1(Params P, UMesh M, const double*
 
 // DISSIPATION, the blend (solver_state.f90:162-225).  A ghost face contributes exactly
 // zero (its state and Laplacian are the cell's own), so it is skipped.
+template <class OutT>
 __global__ void __launch_bounds__(UT) k_u_diss2(UMesh M, const double* __restrict__ q,
-                                                const double* __restrict__ aux, double* __restrict__ d) {
+                                                const double* __restrict__ aux, OutT* __restrict__ d) {
     const int I = blockIdx.x * UT + threadIdx.x;
     const int ne = M.ne;
     if (I >= ne) return;
@@ -194,7 +199,7 @@ __global__ void __launch_bounds__(UT) k_u_diss2(UMesh M, const double* __restric
             D2 = D2 + a2 * (Cm[nb[k]] - CI);
             D4 = D4 + a4 * (Qm[nb[k]] - D2I);
         }
-        d[m * ne + I] = D2 - D4;
+        d[m * ne + I] = (OutT)(D2 - D4);
     }
 }
 
@@ -295,7 +300,8 @@ __global__ void __launch_bounds__(UT) k_u_vface(Params P, UMesh M, const double*
     for (int m = 0; m < 4; m++) vf[m * nf + e] = out[m];
 }
 
-__global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict__ vf, double* __restrict__ vis) {
+template <class OutT>
+__global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict__ vf, OutT* __restrict__ vis) {
     const int I = blockIdx.x * UT + threadIdx.x;
     const int ne = M.ne;
     if (I >= ne) return;
@@ -314,7 +320,7 @@ __global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict
         }
     }
 #pragma unroll
-    for (int m = 0; m < 4; m++) vis[m * ne + I] = acc[m];
+    for (int m = 0; m < 4; m++) vis[m * ne + I] = (OutT)acc[m];
 }
 
 // One RK stage of one chunk of UT cells (source_terms.f90:24-104, residual.f90:23-83),
@@ -342,7 +348,7 @@ __global__ void __launch_bounds__(UT, 3) k_u_stage_chunk(Params P, UMesh M, Stag
     double own_t = 0.0, own_p = 0.0, own_rho = 0.0;
     if (I < ne) {
         Prim p;
-        u_cell_prim(P, q, ne, I, p);
+        u_cell_prim(P, StateF64{q, (size_t)ne}, I, p);
         put(t, p);
         own_t = kept(p.t);
         own_p = kept(p.p);
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(UT, 3) k_u_stage_chunk(Params P, UMesh M, Stag
     }
     for (int h = t; h < nh; h += UT) {
         Prim p;
-        u_slot_prim(P, M, q, M.cslot[h0 + h], p);
+        u_slot_prim(P, M, StateF64{q, (size_t)ne}, M.cslot[h0 + h], p);
         put(UT + h, p);
     }
     __syncthreads();
@@ -495,17 +501,35 @@ __global__ void __launch_bounds__(UT) k_u_bsums(Params P, UMesh M, const double*
 static unsigned blocks(long long n) { return (unsigned)((n + UT - 1) / UT); }
 
 void launch_u_prim(const Params& P, const UMesh& M, const double* q, double* W, cudaStream_t s) {
-    k_u_prim<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(P, M, q, W);
+    k_u_prim<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(P, M, StateF64{q, (size_t)M.ne}, W);
+}
+void launch_u_prim_mx(const Params& P, const UMesh& M, const double* cold, const float* dq, double* W,
+                      cudaStream_t s) {
+    k_u_prim<<<blocks((long long)M.ne + M.ng), UT, 0, s>>>(P, M, StateMixed{cold, dq, (size_t)M.ne}, W);
 }
 void launch_u_gport(const Params& P, const UMesh& M, const double* q, cudaStream_t s) {
-    if (M.nport > 0) k_u_gport<<<blocks(M.nport), UT, 0, s>>>(P, M, q);
+    if (M.nport > 0) k_u_gport<<<blocks(M.nport), UT, 0, s>>>(P, M, StateF64{q, (size_t)M.ne});
+}
+void launch_u_gport_mx(const Params& P, const UMesh& M, const double* cold, const float* dq, cudaStream_t s) {
+    if (M.nport > 0) k_u_gport<<<blocks(M.nport), UT, 0, s>>>(P, M, StateMixed{cold, dq, (size_t)M.ne});
 }
 void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, double* d,
                           double* dt, const double* dtmin, cudaStream_t s) {
     k_u_diss1<<<blocks(M.ne), UT, 0, s>>>(P, M, q, aux, dt, dtmin);
     k_u_diss2<<<blocks(M.ne), UT, 0, s>>>(M, q, aux, d);
 }
+void launch_u_dissipation(const Params& P, const UMesh& M, const double* q, double* aux, float* d, float* dt,
+                          const double* dtmin, cudaStream_t s) {
+    k_u_diss1<<<blocks(M.ne), UT, 0, s>>>(P, M, q, aux, dt, dtmin);
+    k_u_diss2<<<blocks(M.ne), UT, 0, s>>>(M, q, aux, d);
+}
 void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, double* vis,
+                      cudaStream_t s) {
+    k_u_node_avg<<<blocks(M.nnode), UT, 0, s>>>(P, M, W, na);
+    k_u_vface<<<blocks(M.nface), UT, 0, s>>>(P, M, W, na, vf);
+    k_u_vsum<<<blocks(M.ne), UT, 0, s>>>(M, vf, vis);
+}
+void launch_u_viscous(const Params& P, const UMesh& M, const double* W, double* na, double* vf, float* vis,
                       cudaStream_t s) {
     k_u_node_avg<<<blocks(M.nnode), UT, 0, s>>>(P, M, W, na);
     k_u_vface<<<blocks(M.nface), UT, 0, s>>>(P, M, W, na, vf);
@@ -927,7 +951,9 @@ int umesh_upload(tns_handle* h) {
     M.nface = (int)u->hfcell.size(); M.fcell = u->fcell.p; M.fref = u->fref.p;
     M.nchunk = (int)u->hcptr.size() - 1; M.hmax = u->hmax;
     M.cptr = u->cptr.p; M.cslot = u->cslot.p; M.lnb = u->lnb.p;
-    if ((rc = h->cuda(tns::configure_u_chunk(M), "cudaFuncSetAttribute"))) return rc;
+    if ((rc = h->cuda(tns::configure_u_chunk(M), "cudaFuncSetAttribute")) ||
+        (rc = h->cuda(tns::configure_u_chunk_mx(M), "cudaFuncSetAttribute")))
+        return rc;
     // the time-step kernels read CFL*DL through the structured view
     h->M.cfldl = u->cfldl.p;
     for (auto* v : {&u->hnc, &u->hnod, &u->hgpar, &u->hgopp, &u->hgside, &u->hnptr, &u->hnslot, &u->hnreset,
@@ -984,14 +1010,61 @@ void enqueue_iteration_u(tns_handle* h, bool monitor) {
     }
 }
 
+void enqueue_iteration_u_mx(tns_handle* h, bool monitor, double* A, double* Aout) {
+    const tns::Params& P = h->P;
+    tns_umesh_state* u = h->umesh;
+    const tns::UMesh& M = u->M;
+    cudaStream_t s = h->stream;
+    static const double alpha[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};  // constants.f90:30-33
+    const float* in[4] = {nullptr, h->dqb.p, h->dqc.p, h->dqb.p};
+    float* out[4] = {h->dqb.p, h->dqc.p, h->dqb.p, nullptr};
+    // as the FP64 iteration: the dissipation (D, DT in FP32) on the side stream beside
+    // stage 1's field set and the viscous flux (VIS in FP32), from the FP64 Q_old
+    const bool fork = !h->profile && h->side;
+    cudaStream_t sd = s;
+    if (fork) {
+        cudaEventRecord(h->fork, s);
+        cudaStreamWaitEvent(h->side, h->fork, 0);
+        sd = h->side;
+    }
+    if (!P.local)
+        launch(h, K_DTMIN, [&] {
+            tns::launch_time_step_scratch(P, A, M.cfldl, M.ne, h->dt.p, h->partial.p, h->counter.p, h->dtmin.p,
+                                          tns::dtmin_blocks(h->M), sd);
+        });
+    launch(h, K_DISS, [&] { tns::launch_u_dissipation(P, M, A, u->aux.p, h->df.p, h->dtf.p, h->dtmin.p, sd); }, 2);
+    if (fork) cudaEventRecord(h->join, sd);
+    if (monitor) cudaMemsetAsync(h->cdiff.p, 0, 5 * sizeof(unsigned long long), s);
+    for (int st = 0; st < 4; st++) {
+        if (M.nport) launch(h, K_GPORT, [&] { tns::launch_u_gport_mx(P, M, A, in[st], s); });
+        if (st == 0) {
+            launch(h, K_VISC, [&] {
+                tns::launch_u_prim(P, M, A, u->W.p, s);
+                tns::launch_u_viscous(P, M, u->W.p, u->na.p, u->vf.p, h->visf.p, s);
+            }, 4);
+            if (fork) cudaStreamWaitEvent(s, h->join, 0);
+        }
+        tns::StageArgsMx S{A, in[st], out[st], st == 3 ? Aout : nullptr, h->df.p, h->visf.p, h->dtf.p, h->dtmin.p,
+                           (float)alpha[st], (monitor && st == 3) ? h->cdiff.p : nullptr,
+                           st == 3 ? h->status.p : nullptr, h->status.p};
+        launch(h, K_STAGE, [&] { tns::launch_u_stage_chunk_mx(P, M, S, s); });
+    }
+}
+
 int umesh_primitives(tns_handle* h) {
     tns_umesh_state* u = h->umesh;
     const size_t nt = (size_t)h->neles + h->nghosts;
     int rc;
     if (!h->primout.p && (rc = h->cuda(h->primout.alloc(4 * nt), "cudaMalloc"))) return rc;
-    // the last stage read B: its primitives and ghosts again from B
-    tns::launch_u_gport(h->P, u->M, h->qb.p, h->stream);
-    tns::launch_u_prim(h->P, u->M, h->qb.p, u->W.p, h->stream);
+    if (h->precision == 1) {
+        // the last stage read the previous state + dQ_B
+        tns::launch_u_gport_mx(h->P, u->M, h->other_state(), h->dqb.p, h->stream);
+        tns::launch_u_prim_mx(h->P, u->M, h->other_state(), h->dqb.p, u->W.p, h->stream);
+    } else {
+        // the last stage read B: its primitives and ghosts again from B
+        tns::launch_u_gport(h->P, u->M, h->qb.p, h->stream);
+        tns::launch_u_prim(h->P, u->M, h->qb.p, u->W.p, h->stream);
+    }
     tns::launch_u_prim_out(u->M, u->W.p, h->primout.p, h->stream);
     return h->cuda(cudaGetLastError(), "kernel launch");
 }

@@ -7,13 +7,14 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
 SOURCES = ("tns_kernels.cu", "tns_kernels_mx.cu", "tns_api.cu", "tns_batch_api.cu", "tns_adjoint.cu",
-           "tns_unstructured.cu")
+           "tns_unstructured.cu", "tns_unstructured_mx.cu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 # the mixed-precision kernels: FP32 division and square root to 2 ulp and FP32
 # denormals flushed (their FP32 parts are deviations and sources whose error budget is
 # FP32-level anyway; the FP64 parts are unaffected by these flags)
-FILE_FLAGS = {"tns_kernels_mx.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
+FILE_FLAGS = {"tns_kernels_mx.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+              "tns_unstructured_mx.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 
 
 MAINS = os.path.join(os.path.dirname(HERE), "mains")

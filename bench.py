@@ -298,11 +298,18 @@ def run_ours(args, rank, world, dev):
         kt3 = s3.kernel_times()
         s3.profile(False)
         s3.close()
+        s4 = Solver(gmesh, flow, rinit, precision=1)
+        s4.set_stream(stream.cuda_stream)
+        s4.upload(gq)
+        ms4, _ = time_steps(s4, stream, flush, min(K, 300), W, world, torch)
+        s4.close()
         gen = {"workload": wname + ", cell and node ids shuffled, faces rotated (general-mesh path)",
                "value": replica_rate(mesh.neles, ms3 * 1e-3, world), "ms_per_step": round(ms3, 5),
                "steps": min(K, 300), "launches_per_step": l3 / min(K, 300),
                "over_structured": ms3 / ms,
-               "kernel_us_per_iteration": {k: round(kt3[k][0] / 3 * 1e3, 2) for k in kt3 if kt3[k][1]}}
+               "kernel_us_per_iteration": {k: round(kt3[k][0] / 3 * 1e3, 2) for k in kt3 if kt3[k][1]},
+               "mixed": {"value": replica_rate(mesh.neles, ms4 * 1e-3, world), "ms_per_step": round(ms4, 5),
+                         "mixed_over_fp64": ms4 / ms3}}
 
     adj = None
     if world == 1 and not args.no_adjoint:

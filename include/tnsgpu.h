@@ -59,9 +59,9 @@ typedef struct tns_handle tns_handle;
  * i x j block (any numbering) runs on the tiled kernels; any other quadrilateral mesh
  * (the reference reads any NOD / NC1..NC4) on the gather-indexed kernels, its cells
  * ordered along a Hilbert curve and its nodes renumbered on the device (the ABI's
- * arrays keep the caller's ids).  TNS_ERR_UNSUPPORTED: a general mesh with mixed precision, or with a type-3 ghost
- * whose parent has no cell across the opposite face; the adjoint and the batch API also
- * refuse general meshes with it.
+ * arrays keep the caller's ids); both precisions run there.  TNS_ERR_UNSUPPORTED: a
+ * general mesh with a type-3 ghost whose parent has no cell across the opposite face;
+ * the adjoint and the batch API also refuse general meshes with it.
  * Replaces: CALL COMPUTE_GEOMETRY's consumers + the module state setup
  * (turbnstwod.f90:32-48). */
 int tns_create(const tns_mesh *mesh, const tns_params *params, tns_handle **out);

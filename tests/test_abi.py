@@ -80,7 +80,8 @@ def _strip(ni=6):
 
 def test_general_meshes_refused_where_the_layout_cannot_follow():
     """A mesh that is not one i x j block takes the general layout; it refuses, before
-    any CUDA call, a type-3 ghost with no cell to extrapolate from and mixed precision."""
+    any CUDA call, a type-3 ghost with no cell to extrapolate from, and takes mixed
+    precision (host checks pass; without a GPU the first CUDA call fails)."""
     rc, msg = _create(_strip())
     assert rc == -3 and "type-3" in msg, (rc, msg)
     f = cases.ramp_flow()
@@ -98,7 +99,7 @@ def test_general_meshes_refused_where_the_layout_cannot_follow():
     rc = L.tns_create(C.byref(m), C.byref(p), C.byref(h))
     msg = L.tns_last_error(h).decode()
     L.tns_destroy(h)
-    assert rc == -3 and "mixed precision" in msg, (rc, msg)
+    assert rc in (0, -4) and "mixed precision" not in msg, (rc, msg)
 
 
 def test_general_mesh_passes_host_checks():

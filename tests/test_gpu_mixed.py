@@ -85,3 +85,30 @@ def test_mixed_graph_replay_equals_direct_launches_and_parity_alternates():
     b.run(2, 1)
     assert np.array_equal(a.download(), b.download())
     assert np.array_equal(a.primitives(), b.primitives())
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_mixed_general_mesh_follows_fp64(name):
+    """The same cases with their ids shuffled and faces rotated (cases.renumbered_mesh),
+    so they take the general-mesh path: its mixed iteration (chunk reference states,
+    FP32 slot deviations, FP32 D / VIS / DT) follows its FP64 iteration to the same
+    tolerances, the residual record and the POSTPROCESS primitives too."""
+    mesh, flow, kind = CASES[name]()
+    if name == "plume_axis_sym":
+        mesh.ntype[(mesh.ntype == 5) & (mesh.nside == 1)] = 4
+    if kind == "noisy":
+        c0, ri = cases.noisy_restart_state(flow, mesh.neles)
+    else:
+        ri = formats.rinit_cold(flow)
+        c0 = formats.cold_state(flow, mesh.neles, ri)
+    g, perm = cases.renumbered_mesh(mesh, seed=7)
+    q0 = np.empty_like(c0)
+    q0[:, perm] = c0
+    a, b, ha, hb = _pair(g, flow, q0, ri, 50)
+    err = rel(b.download(), a.download())
+    print(f"{name} general mesh: mixed vs FP64 {err}")
+    assert np.all(err <= TOL), err
+    assert np.max(np.abs(hb - ha) / ha) <= 1e-4
+    assert np.all(rel(b.primitives(), a.primitives()) <= 1e-4)
+    a.close()
+    b.close()
