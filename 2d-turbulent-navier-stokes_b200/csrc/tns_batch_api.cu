@@ -57,6 +57,7 @@ struct tns_batch {
     // cooperative launch per run of up to PERSIST unmonitored iterations (grid barriers
     // between the phases), monitored iterations as schedule 0
     int mode = 0;
+    bool general = false;  // a case is a general mesh: per-case schedules (1, 2) only
     static constexpr int PERSIST = 256;
     int persist_grid = 0;               // resident blocks of the persistent kernel
     DevBuf<unsigned int> d_bar;         // its grid barrier: arrival counter, generation
@@ -166,7 +167,7 @@ int upload_tiles(tns_batch* b) {
     std::vector<int4> t;
     const int n = (int)b->cases.size();
     for (int k = 0; k < n; k++) {
-        if (!b->active[k]) continue;
+        if (!b->active[k] || b->cases[k]->unstructured) continue;
         const tns::Mesh& M = b->cases[k]->M;
         const int tj = (M.nj + tns::TJ - 1) / tns::TJ, ti = (M.ni + tns::TI - 1) / tns::TI;
         for (int y = 0; y < ti; y++)
@@ -357,8 +358,7 @@ int tns_batch_create(tns_handle* const* cases, int ncases, tns_batch** out) {
         for (int j = 0; j < k; j++)
             if (cases[j] == cases[k]) return b->fail(TNS_ERR_ARG, "tns_batch_create: case %d repeats case %d", k, j);
         if (!cases[k]->qa.p) return b->fail(TNS_ERR_STATE, "tns_batch_create: case %d was not created", k);
-        if (cases[k]->unstructured)
-            return b->fail(TNS_ERR_UNSUPPORTED, "tns_batch_create: case %d is not one structured i x j block", k);
+        if (cases[k]->unstructured) b->general = true;
     }
     b->cases.assign(cases, cases + ncases);
     b->precision = cases[0]->precision;
@@ -368,7 +368,8 @@ int tns_batch_create(tns_handle* const* cases, int ncases, tns_batch** out) {
                            cases[k]->precision, b->precision);
     long long ntiles = 0;
     for (tns_handle* h : b->cases)
-        ntiles += (long long)((h->M.nj + tns::TJ - 1) / tns::TJ) * ((h->M.ni + tns::TI - 1) / tns::TI);
+        if (!h->unstructured)
+            ntiles += (long long)((h->M.nj + tns::TJ - 1) / tns::TJ) * ((h->M.ni + tns::TI - 1) / tns::TI);
     if (ntiles > 0x7fffffffLL) return b->fail(TNS_ERR_TOO_LARGE, "tns_batch_create: %lld tiles", ntiles);
     int rc;
     if ((rc = b->cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate")) ||
@@ -382,8 +383,9 @@ int tns_batch_create(tns_handle* const* cases, int ncases, tns_batch** out) {
         return rc;
     b->active.assign(ncases, 1);
     b->failed.assign(ncases, 0);
-    if ((rc = upload_descriptors(b))) return rc;
-    return upload_tiles(b);
+    if ((rc = upload_descriptors(b)) || (rc = upload_tiles(b))) return rc;
+    // general meshes have no tile table: their cases run through their own iterations
+    return b->general ? tns_batch_set_schedule(b, 2) : TNS_OK;
 }
 
 int tns_batch_set_active(tns_batch* b, const int* active) {
@@ -569,6 +571,8 @@ int tns_batch_run(tns_batch* b, int niter, int monitor_every, double stop_ratio,
 int tns_batch_set_schedule(tns_batch* b, int schedule) {
     if (!b) return TNS_ERR_ARG;
     if (schedule < 0 || schedule > 3) return b->fail(TNS_ERR_ARG, "schedule %d is not 0, 1, 2 or 3", schedule);
+    if (b->general && (schedule == 0 || schedule == 3))
+        return b->fail(TNS_ERR_UNSUPPORTED, "schedule %d needs every case to be one structured i x j block", schedule);
     int rc;
     if (schedule == 3) {
         for (size_t k = 0; k < b->cases.size(); k++) {

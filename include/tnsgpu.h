@@ -61,7 +61,8 @@ typedef struct tns_handle tns_handle;
  * ordered along a Hilbert curve and its nodes renumbered on the device (the ABI's
  * arrays keep the caller's ids); both precisions run there.  TNS_ERR_UNSUPPORTED: a
  * general mesh with a type-3 ghost whose parent has no cell across the opposite face;
- * the adjoint and the batch API also refuse general meshes with it.
+ * the adjoint also refuses general meshes, and a batch holding one runs schedules 1
+ * and 2 only (tns_batch_set_schedule).
  * Replaces: CALL COMPUTE_GEOMETRY's consumers + the module state setup
  * (turbnstwod.f90:32-48). */
 int tns_create(const tns_mesh *mesh, const tns_params *params, tns_handle **out);
@@ -252,7 +253,8 @@ int tns_copy_state_device(tns_handle *h, double *d_buf, int direction);
  * differ in mesh size, geometry and parameters; they share one precision mode.  State
  * moves in and out through each member's tns_upload_state / tns_download_state /
  * tns_download_primitives, before and after tns_batch_run.  The batch borrows the
- * handles: destroy the batch first. */
+ * handles: destroy the batch first.  A batch with a general-mesh case (one that is not
+ * one structured i x j block) starts in schedule 2 and runs schedules 1 and 2 only. */
 typedef struct tns_batch tns_batch;
 
 int tns_batch_create(tns_handle *const *cases, int ncases, tns_batch **out);
@@ -285,8 +287,9 @@ int tns_batch_set_active(tns_batch *b, const int *active);
  * grid barriers between the phases (monitored iterations as schedule 0); it needs
  * LOCAL=1 and no type-6 port in every case (TNS_ERR_UNSUPPORTED otherwise), and a grid
  * barrier that does not complete in its bounded wait ends the run with TNS_ERR_CUDA.
- * Results are identical; which is fastest depends on the case mix (tnsgpu.autotune
- * measures them). */
+ * Schedules 0 and 3 need every case to be one structured i x j block
+ * (TNS_ERR_UNSUPPORTED otherwise).  Results are identical; which is fastest depends on
+ * the case mix (tnsgpu.autotune measures them). */
 int tns_batch_set_schedule(tns_batch *b, int schedule);
 int tns_batch_get_schedule(tns_batch *b);
 int tns_batch_get_active(tns_batch *b, int *active);

@@ -295,3 +295,42 @@ def test_persistent_schedule_refuses_what_it_cannot_run():
         for s in solvers:
             s.close()
 
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_with_general_meshes_equals_solo_runs(precision):
+    """A batch holding general-mesh cases (ids shuffled, faces rotated: no tile table)
+    beside structured ones runs every case through its own iteration (schedules 1 and
+    2), bit-identical to the cases run alone; the tile-table schedules are refused."""
+    mem = _members(precision, pick=[0, 2, 4])
+    runs = []
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        if k != 1:  # the nozzle stays one structured block
+            mesh, perm = cases.renumbered_mesh(mesh, seed=11 + k)
+            q = np.empty_like(c0)
+            q[:, perm] = c0
+            c0 = q
+        runs.append((name, mesh, flow, c0, ri))
+    solvers = []
+    for name, mesh, flow, c0, ri in runs:
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        solvers.append(s)
+    b = Batch(solvers)
+    assert b.schedule == 2
+    for bad in (0, 3):
+        with pytest.raises(_lib.TnsError) as e:
+            b.schedule = bad
+        assert e.value.code == _lib.TNS_ERR_UNSUPPORTED
+    r1 = b.run(3, monitor_every=0)
+    b.schedule = 1
+    r2 = b.run(10, monitor_every=5)
+    assert list(r1.iterations) == [3] * len(runs) and list(r2.iterations) == [10] * len(runs)
+    for k, (name, mesh, flow, c0, ri) in enumerate(runs):
+        (q, prim), rec = _solo(mesh, flow, c0, ri, precision, [3, 10], monitor=5)
+        np.testing.assert_array_equal(solvers[k].download(), q, err_msg=name)
+        np.testing.assert_array_equal(solvers[k].primitives(), prim, err_msg=name)
+        np.testing.assert_array_equal(r2.records[k], rec[1], err_msg=name)
+    b.close()
+    for s in solvers:
+        s.close()
