@@ -329,7 +329,12 @@ __global__ void __launch_bounds__(UT) k_u_vsum(UMesh M, const double* __restrict
 // its T, P, RHO) and the threads then share the halo slots.  (It gives bitwise the
 // results of a slot field set in global memory gathered per cell.)  Shared memory:
 // (UT + hmax) slots of (F_m, G_m) x 5, (U, V), (C5/C1, |V|).
-__global__ void __launch_bounds__(UT, 3) k_u_stage_chunk(Params P, UMesh M, StageArgsU A,
+#ifndef TNS_U_CHUNK_MINB
+// Blocks per SM the register budget is sized for; measured on a renumbered 1024 x 384
+// nozzle-plume (B200, one FP64 iteration): 2 -> 0.289 ms, 3 -> 0.294 ms, 4 -> 0.313 ms.
+#define TNS_U_CHUNK_MINB 2
+#endif
+__global__ void __launch_bounds__(UT, TNS_U_CHUNK_MINB) k_u_stage_chunk(Params P, UMesh M, StageArgsU A,
                                                          const double* __restrict__ q) {
     extern __shared__ double2 usm[];
     const int ns = UT + M.hmax;

@@ -29,7 +29,12 @@ __device__ __forceinline__ void u_cell_prim_mx(const Params& P, const St& st, in
 
 // One mixed RK stage of one chunk (source_terms.f90:24-104, residual.f90:23-83): stage
 // input COLD + dQin (dQin null in stage 1); stages 1-3 write dQout, stage 4 the state qout.
-__global__ void __launch_bounds__(UT, 4) k_u_stage_chunk_mx(Params P, UMesh M, StageArgsMx A) {
+#ifndef TNS_U_CHUNK_MX_MINB
+// Blocks per SM the register budget is sized for; measured on a renumbered 1024 x 384
+// nozzle-plume (B200, one mixed iteration): 4 -> 0.248 ms, 3 -> 0.264 ms, 5 -> 0.257 ms.
+#define TNS_U_CHUNK_MX_MINB 4
+#endif
+__global__ void __launch_bounds__(UT, TNS_U_CHUNK_MX_MINB) k_u_stage_chunk_mx(Params P, UMesh M, StageArgsMx A) {
     extern __shared__ __align__(16) unsigned char usm_raw[];
     TileRefMx& R = *reinterpret_cast<TileRefMx*>(usm_raw);
     const int ns = UT + M.hmax;
