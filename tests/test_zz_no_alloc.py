@@ -8,7 +8,8 @@ through the C ABI with device buffers it allocates itself (it is only the checke
 twice in a row, and compares DT and DTMIN with what tns_run computed for the same
 state (tns_debug_fetch).  The meshes span one reduction block (960 cells), several
 (16 384 cells: 16 partial minima, the last block's reduction through the shared array,
-the completion counter left at zero for the next call) and many (393 216 cells).
+the completion counter left at zero for the next call) and many (393 216 cells).  One
+call is also captured into a CUDA graph and replayed, the use the entry point exists for.
 
 This file is collected last so a run that stops at the first failure has run every
 other test before it.
@@ -80,6 +81,62 @@ def test_noalloc_time_step_matches_handle_path_on_two_calls(local, shape):
             assert abs(dtmin - dt.min()) <= TOL * dtmin, call
         state = s.download()  # the next call starts from a different state
     s.close()
+
+
+@pytest.mark.parametrize("local", [1, 0])
+def test_noalloc_time_step_inside_a_captured_graph(local):
+    """One call captured into a CUDA graph after a warm-up call; the graph replayed on two
+    states written into its static input, each replay against the handle path."""
+    import torch
+    mesh = cases.ramp_mesh(256, 64)  # 16 reduction blocks
+    flow = cases.ramp_flow()
+    flow.local = local
+    c0, rinit = cases.noisy_restart_state(flow, mesh.neles)
+    params = make_params(flow, rinit)
+    L = _lib.load()
+    ncell = mesh.neles
+    cfldl = torch.from_numpy(_cfldl(mesh, flow.cfl)).cuda()
+    q = torch.from_numpy(np.ascontiguousarray(c0)).cuda()
+    dt = torch.full((ncell,), math.nan, dtype=torch.float64, device="cuda")
+    dtmin = torch.full((1,), math.nan, dtype=torch.float64, device="cuda")
+
+    def call():
+        rc = L.tns_time_step_noalloc(q.data_ptr(), cfldl.data_ptr(), ncell, C.byref(params),
+                                     dt.data_ptr(), dtmin.data_ptr(),
+                                     torch.cuda.current_stream().cuda_stream)
+        assert rc == 0, _lib.ERRORS.get(rc, rc)
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        call()  # warm-up outside the capture: the scratch address is looked up here
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        call()
+
+    s = Solver(mesh, flow, rinit)
+    state = c0
+    for replay in range(2):
+        s.upload(state)
+        s.run(1, 0)
+        ref = s.debug(2)[0]
+        q.copy_(torch.from_numpy(np.ascontiguousarray(state)))
+        dt.fill_(math.nan)
+        dtmin.fill_(math.nan)
+        g.replay()
+        torch.cuda.synchronize()
+        d, m = dt.cpu().numpy(), float(dtmin.cpu().numpy()[0])
+        if local:
+            assert np.max(np.abs(d - ref) / ref) <= TOL, replay
+            assert abs(m - min(1.0e5, ref.min())) <= TOL * m, replay
+        else:
+            assert abs(m - ref[0]) <= TOL * m, replay
+            assert abs(m - d.min()) <= TOL * m, replay
+        state = s.download()
+    s.close()
+    del g
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
