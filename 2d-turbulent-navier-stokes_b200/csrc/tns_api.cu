@@ -689,6 +689,24 @@ int tns_enqueue(tns_handle* h, int niter) {
     return rc;
 }
 
+int tns_prepare(tns_handle* h) {
+    if (!h) return TNS_ERR_ARG;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_prepare: no state uploaded");
+    if (h->profile) return TNS_OK;
+    int rc;
+    if ((rc = ensure_graph(h))) return rc;
+    const long long per = h->per_iter;
+    const bool mixed = h->precision == 1;
+    for (int par = 0; par < (mixed ? 2 : 1); par++) {
+        cudaGraphExec_t* g = mixed ? &h->graph_mon_mx[par] : &h->graph_mon;
+        if (*g) continue;
+        if ((rc = capture(h, g, mixed, par, true))) return rc;
+        h->per_iter_mon = h->per_iter;
+    }
+    h->per_iter = per;
+    return TNS_OK;
+}
+
 int tns_synchronize(tns_handle* h) {
     if (!h) return TNS_ERR_ARG;
     return check_status(h);

@@ -627,6 +627,36 @@ int tns_batch_set_schedule(tns_batch* b, int schedule) {
 
 int tns_batch_get_schedule(tns_batch* b) { return b ? b->mode : TNS_ERR_ARG; }
 
+int tns_batch_prepare(tns_batch* b) {
+    if (!b) return TNS_ERR_ARG;
+    const int n = (int)b->cases.size();
+    int rc;
+    for (int k = 0; k < n; k++) {
+        tns_handle* h = b->cases[k];
+        if (!h->have_state) return b->fail(TNS_ERR_STATE, "tns_batch_prepare: case %d has no state uploaded", k);
+        if ((rc = b->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    }
+    // the descriptors and the tile table tns_batch_run would start from
+    if (b->precision == 1) {
+        const int f0 = b->cases[0]->cur ^ b->cur_at_desc[0];
+        bool same = true;
+        for (int k = 1; k < n; k++) same &= (b->cases[k]->cur ^ b->cur_at_desc[k]) == f0;
+        if (!same && (rc = upload_descriptors(b))) return rc;
+    }
+    if (b->active != b->active_at_capture && (rc = upload_tiles(b))) return rc;
+    bool any = false;
+    for (int k = 0; k < n; k++) any |= b->active[k] != 0;
+    if (!any) return TNS_OK;  // tns_batch_run launches nothing either
+    const int nparity = b->precision == 1 ? 2 : 1;
+    for (int par = 0; par < nparity; par++) {
+        // schedule 3 launches a graph only for its monitored iterations
+        if (b->mode != 3 && (rc = ensure_batch_graph(b, 0, par))) return rc;
+        if ((rc = ensure_batch_graph(b, 1, par))) return rc;
+        if (b->mode == 2 && (rc = ensure_block_graph(b, par))) return rc;
+    }
+    return TNS_OK;
+}
+
 long long tns_batch_launch_count(tns_batch* b) { return b ? b->launches : -1; }
 
 const char* tns_batch_last_error(tns_batch* b) { return b ? b->err.c_str() : "null batch"; }

@@ -34,11 +34,11 @@ NOALLOC_MAX_CELLS = 256 * 4 * 8192
 
 # every symbol include/tnsgpu.h declares
 EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
-           "tns_enqueue", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
+           "tns_enqueue", "tns_prepare", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
            "tns_boundary_integrals", "tns_total_pressure_sums", "tns_boundary_face_states", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
-           "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule",
+           "tns_batch_get_active", "tns_batch_set_schedule", "tns_batch_get_schedule", "tns_batch_prepare",
            "tns_batch_launch_count", "tns_debug_math", "tns_batch_last_error", "tns_batch_destroy",
            "tns_adjoint_enable", "tns_adjoint_step", "tns_adjoint_step_next", "tns_adjoint_sensitivity_size",
            "tns_adjoint_record_size", "tns_adjoint_record", "tns_adjoint_step_recorded",
@@ -86,6 +86,7 @@ def load(path: str = None):
     L.tns_upload_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_run.argtypes = [vp, ip, ip, dp, ip, C.POINTER(C.c_int)]
     L.tns_enqueue.argtypes = [vp, ip]
+    L.tns_prepare.argtypes = [vp]
     L.tns_synchronize.argtypes = [vp]
     L.tns_download_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_download_primitives.argtypes = [vp, dp, dp, dp, dp]
@@ -111,6 +112,7 @@ def load(path: str = None):
     L.tns_batch_set_schedule.argtypes = [vp, ip]
     L.tns_debug_math.argtypes = [ip, C.c_longlong, dp, dp, dp]
     L.tns_batch_get_schedule.argtypes = [vp]
+    L.tns_batch_prepare.argtypes = [vp]
     L.tns_batch_launch_count.argtypes = [vp]
     L.tns_batch_launch_count.restype = C.c_longlong
     L.tns_batch_last_error.argtypes = [vp]

@@ -39,6 +39,7 @@ def _time_batch(solvers: Sequence[Solver], schedule: int, iters: int, warmup: in
     b = Batch(solvers, schedule=schedule)
     try:
         b.run(warmup, 0)
+        b.prepare()
         t0 = time.perf_counter()
         b.run(iters, 0)
         return (time.perf_counter() - t0) / iters
@@ -50,10 +51,9 @@ def tune_batch(make_solvers: Callable[[str], List[Solver]], iters: int = 40, war
                tile_heights: Iterable[int] = TILE_HEIGHTS, schedules: Sequence[int] = (0, 1, 2, 3),
                cache: Optional[str] = None, key: Optional[str] = None) -> dict:
     """make_solvers(lib_path) builds the batch's cases (state uploaded) from that library
-    build.  Times ``iters`` iterations after ``warmup`` (enough to capture every graph a
-    schedule uses, including schedule 2's 8-iteration block) for every (tile height,
-    schedule)
-    and returns {"ti", "schedule", "lib", "s_per_iter", "trials"}.  With ``cache`` (a
+    build.  Times ``iters`` iterations after ``warmup`` untimed ones and
+    Batch.prepare (every graph the schedule launches captured before the timing) for
+    every (tile height, schedule) and returns {"ti", "schedule", "lib", "s_per_iter", "trials"}.  With ``cache`` (a
     JSON file) and ``key``, a stored choice is returned without timing."""
     if cache and key and os.path.exists(cache):
         with open(cache) as fh:
@@ -99,6 +99,7 @@ def tune_case(make_solver: Callable[[str], Solver], iters: int = 50, warmup: int
         s = make_solver(_lib.variant_path(ti))
         try:
             s.run(warmup, 0)
+            s.prepare()
             t0 = time.perf_counter()
             s.run(iters, 0)
             trials.append({"ti": ti, "s_per_iter": (time.perf_counter() - t0) / iters})

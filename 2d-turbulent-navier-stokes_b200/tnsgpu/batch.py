@@ -89,6 +89,12 @@ class Batch:
     def schedule(self, value: int):
         self._check(self.L.tns_batch_set_schedule(self.b, int(value)))
 
+    def prepare(self):
+        """Capture every CUDA graph run() launches under the current schedule and active
+        mask now, without running anything (tns_batch_prepare); a change of schedule or
+        mask drops them."""
+        self._check(self.L.tns_batch_prepare(self.b))
+
     def set_active(self, mask: Sequence[int]):
         m = np.ascontiguousarray(np.asarray(mask, np.int32))
         if m.shape != (self.ncases,):

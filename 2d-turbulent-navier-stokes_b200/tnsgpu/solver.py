@@ -98,6 +98,11 @@ class Solver:
         """Asynchronous iterations (no residual monitor); errors surface at synchronize()."""
         self._check(self.L.tns_enqueue(self.h, int(niter)))
 
+    def prepare(self):
+        """Capture every CUDA graph run() and enqueue() launch now, without running
+        anything, instead of inside the first call that needs each (tns_prepare)."""
+        self._check(self.L.tns_prepare(self.h))
+
     def synchronize(self):
         self._check(self.L.tns_synchronize(self.h))
 

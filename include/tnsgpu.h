@@ -88,6 +88,13 @@ int tns_run(tns_handle *h, int niter, int monitor_every, double *cdiff_out, int 
  * (non-finite state) are reported by the next tns_synchronize / tns_run. */
 int tns_enqueue(tns_handle *h, int niter);
 
+/* Captures and instantiates, without running anything, every CUDA graph that tns_run
+ * and tns_enqueue launch for this handle (the unmonitored and the monitored iteration;
+ * in mixed precision one of each per state-buffer parity).  Otherwise each is captured
+ * at its first use, inside whichever call first needs it.  Needs an uploaded state;
+ * does nothing while per-kernel profiling is on (those iterations are not graphs). */
+int tns_prepare(tns_handle *h);
+
 /* Waits for the work enqueued on the handle's stream; TNS_ERR_NONFINITE if the state
  * became NaN / Inf since the last check. */
 int tns_synchronize(tns_handle *h);
@@ -292,6 +299,14 @@ int tns_batch_set_active(tns_batch *b, const int *active);
  * the case mix (tnsgpu.autotune measures them). */
 int tns_batch_set_schedule(tns_batch *b, int schedule);
 int tns_batch_get_schedule(tns_batch *b);
+
+/* Captures and instantiates, without running anything, every CUDA graph that
+ * tns_batch_run launches under the current schedule and active mask: the monitored and
+ * the unmonitored iteration (schedules 0-2), schedule 2's 8-iteration block, in mixed
+ * precision one of each per state-buffer parity.  Otherwise each is captured at its
+ * first use inside tns_batch_run.  A change of schedule or of the active mask drops
+ * them; call it again after one. */
+int tns_batch_prepare(tns_batch *b);
 int tns_batch_get_active(tns_batch *b, int *active);
 long long tns_batch_launch_count(tns_batch *b);
 const char *tns_batch_last_error(tns_batch *b);

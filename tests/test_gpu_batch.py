@@ -334,3 +334,44 @@ def test_batch_with_general_meshes_equals_solo_runs(precision):
     b.close()
     for s in solvers:
         s.close()
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_prepare_captures_without_running(precision, schedule):
+    """tns_prepare / tns_batch_prepare capture every graph ahead of the runs: they launch
+    nothing (launch counts unchanged, states unchanged), a second call is a no-op, and
+    the runs after them equal solo runs bit for bit, across calls of odd and even
+    length (both state parities)."""
+    mem = _members(precision, pick=[0, 1, 3])  # LOCAL=1, no port: every schedule runs them
+    solvers = []
+    for name, mesh, flow, c0, ri in mem:
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        solvers.append(s)
+    b = Batch(solvers, schedule=schedule)
+    l0 = b.launch_count()
+    b.prepare()
+    b.prepare()
+    assert b.launch_count() == l0
+    for s, (name, _, _, c0, _) in zip(solvers, mem):
+        np.testing.assert_array_equal(s.download(), c0, err_msg=name)
+    r1 = b.run(3, monitor_every=0)
+    r2 = b.run(21, monitor_every=10)
+    assert list(r1.iterations) == [3] * len(mem) and list(r2.iterations) == [21] * len(mem)
+    for k, (name, mesh, flow, c0, ri) in enumerate(mem):
+        s = Solver(mesh, flow, ri, precision=precision)
+        s.upload(c0)
+        n0 = s.launch_count()
+        s.prepare()
+        s.prepare()
+        assert s.launch_count() == n0, name
+        np.testing.assert_array_equal(s.download(), c0, err_msg=name)
+        s.run(3, 0)
+        rec = s.run(21, 10)
+        np.testing.assert_array_equal(solvers[k].download(), s.download(), err_msg=name)
+        np.testing.assert_array_equal(r2.records[k], rec, err_msg=name)
+        s.close()
+    b.close()
+    for s in solvers:
+        s.close()
