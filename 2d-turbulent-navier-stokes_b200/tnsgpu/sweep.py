@@ -43,8 +43,11 @@ def _solvers(sweep, precision, lib=None):
 
 def run_sequential(solvers, niter, monitor, stop_ratio):
     """Each case alone: iteration 1 monitored (the reference), then chunks ending on the
-    monitor cadence, stopping at the criterion -- the batch's schedule, case by case."""
+    monitor cadence, stopping at the criterion -- the batch's schedule, case by case.
+    Every case's graphs are captured before the timing (Solver.prepare)."""
     iters = []
+    for s in solvers:
+        s.prepare()
     t0 = time.perf_counter()
     for s in solvers:
         ref = s.run(1, 1)[0]
@@ -61,6 +64,7 @@ def run_sequential(solvers, niter, monitor, stop_ratio):
 
 def run_batched(solvers, niter, monitor, stop_ratio, schedule=0):
     b = Batch(solvers, schedule=schedule)
+    b.prepare()  # the schedule's graphs captured before the timing
     t0 = time.perf_counter()
     r = b.run(niter, monitor, stop_ratio)
     dt = time.perf_counter() - t0
