@@ -9,7 +9,8 @@ over the tiles of all active cases, converged cases masked off) and once case by
 through tns_run with the same criterion.  Before the batched run the autotuner picks
 the tile height and the batch schedule by timing a few iterations of the sweep itself
 (its time is reported apart); the sequential solves use the default build.  Reports
-both wall times (device work synchronised, state uploads excluded), the iterations each
+both wall times (device work synchronised, state uploads and graph capture excluded),
+the iterations each
 case ran, and how far every batched final state is from its sequential counterpart
 (bit-identical in FP64; FP32 rounding of the per-tile reference flux in the mixed mode
 when the tuned tile height differs from the default).

@@ -375,3 +375,16 @@ def test_prepare_captures_without_running(precision, schedule):
     b.close()
     for s in solvers:
         s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_sweep_cli_compare_on_a_small_sweep(precision):
+    """tnsgpu.sweep.compare (the sweep CLI) on four cases of the seeded sweep: the batched
+    and sequential arms agree bit for bit (same build, no tuning) and both report their
+    times."""
+    from tnsgpu import sweep
+    r = sweep.compare(ncases=4, niter=30, stop_ratio=1.0e-5, monitor=10, seed=0, precision=precision,
+                      tune=False)
+    assert r["iterations_equal"] and r["states_bitwise_equal"] and r["state_rel_diff_max"] == 0.0
+    assert r["iterations_min_max"] == [30, 30]
+    assert r["batched_s"] > 0 and r["sequential_s"] > 0 and r["batch_launches"] > 0
