@@ -547,6 +547,55 @@ int tns_set_injection_scale(tns_handle* h, const double* scale) {
     return h->cuda(cudaMemcpy(h->ginj.p, g.data(), g.size() * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
 }
 
+namespace {
+bool page_locked(const void* p) {
+    cudaPointerAttributes at;
+    const bool ok = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return ok;
+}
+
+// The asynchronous transfers: one DMA per component on the handle's stream, page-locked
+// caller arrays in the handle's own cell order only (no staging, no scatter).
+int async_arrays_ok(tns_handle* h, const void* const* a, const char* who) {
+    if (!h->identity)
+        return h->fail(TNS_ERR_UNSUPPORTED, "%s: the mesh is renumbered on the device; use the synchronous call", who);
+    for (int m = 0; m < 5; m++)
+        if (!a[m] || !page_locked(a[m])) return h->fail(TNS_ERR_ARG, "%s: array %d is not page-locked", who, m + 1);
+    return TNS_OK;
+}
+}  // namespace
+
+int tns_upload_state_async(tns_handle* h, const double* c1, const double* c2, const double* c3,
+                           const double* c4, const double* c5) {
+    if (!h) return TNS_ERR_ARG;
+    const double* src[5] = {c1, c2, c3, c4, c5};
+    int rc;
+    if ((rc = async_arrays_ok(h, reinterpret_cast<const void* const*>(src), "tns_upload_state_async"))) return rc;
+    const size_t nc = h->ncell();
+    for (int m = 0; m < 5; m++)
+        if ((rc = h->cuda(cudaMemcpyAsync(h->state() + m * nc, src[m], nc * 8, cudaMemcpyHostToDevice, h->stream),
+                          "cudaMemcpyAsync")))
+            return rc;
+    h->have_state = true;
+    return TNS_OK;
+}
+
+int tns_download_state_async(tns_handle* h, double* c1, double* c2, double* c3, double* c4, double* c5) {
+    if (!h) return TNS_ERR_ARG;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_download_state_async: no state");
+    double* dst[5] = {c1, c2, c3, c4, c5};
+    int rc;
+    if ((rc = async_arrays_ok(h, reinterpret_cast<const void* const*>(dst), "tns_download_state_async")))
+        return rc;
+    const size_t nc = h->ncell();
+    for (int m = 0; m < 5; m++)
+        if ((rc = h->cuda(cudaMemcpyAsync(dst[m], h->state() + m * nc, nc * 8, cudaMemcpyDeviceToHost, h->stream),
+                          "cudaMemcpyAsync")))
+            return rc;
+    return TNS_OK;
+}
+
 int tns_upload_state(tns_handle* h, const double* c1, const double* c2, const double* c3,
                      const double* c4, const double* c5) {
     if (!h || !c1 || !c2 || !c3 || !c4 || !c5) return TNS_ERR_ARG;
@@ -672,6 +721,15 @@ int check_status(tns_handle* h) {
                       "cudaMemcpyAsync")))
         return rc;
     if ((rc = h->cuda(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize"))) return rc;
+    if (h->cdiff_pending) {
+        // the record of tns_enqueue_monitored has arrived: the floor tns_run applies
+        for (int m = 0; m < 5; m++) {
+            const double init = m < 4 ? 1.0e-10 : 1.0e-20;  // constants.f90:44-45
+            const double v = h->cdiff_pending[m];
+            h->cdiff_pending[m] = v >= init ? v : init;
+        }
+        h->cdiff_pending = nullptr;
+    }
     if (*h->status_host & 1u) return h->fail(TNS_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
     if (*h->status_host & 2u)
         return h->fail(TNS_ERR_CUDA, "a stage tile's static-data copy did not complete in its bounded wait");
@@ -710,6 +768,23 @@ int tns_prepare(tns_handle* h) {
 int tns_synchronize(tns_handle* h) {
     if (!h) return TNS_ERR_ARG;
     return check_status(h);
+}
+
+int tns_enqueue_monitored(tns_handle* h, double* cdiff) {
+    if (!h || !cdiff) return TNS_ERR_ARG;
+    if (!h->have_state) return h->fail(TNS_ERR_STATE, "tns_enqueue_monitored: no state uploaded");
+    if (!page_locked(cdiff)) return h->fail(TNS_ERR_ARG, "tns_enqueue_monitored: cdiff is not page-locked");
+    if (h->cdiff_pending)
+        return h->fail(TNS_ERR_STATE, "tns_enqueue_monitored: the previous record was not synchronised");
+    int rc;
+    if ((rc = enqueue_monitored(h))) return rc;
+    // the five maxima as IEEE bit patterns: a non-negative double orders like its bits
+    if ((rc = h->cuda(cudaMemcpyAsync(cdiff, h->cdiff.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                      h->stream), "cudaMemcpyAsync")))
+        return rc;
+    h->cdiff_pending = cdiff;
+    h->have_run = true;
+    return TNS_OK;
 }
 
 int tns_run(tns_handle* h, int niter, int monitor_every, double* cdiff_out, int max_records,

@@ -80,6 +80,9 @@ struct tns_handle {
     cudaGraphExec_t graph = nullptr;
     long long per_iter = 0, per_iter_mon = 0;
     unsigned int* status_host = nullptr;  // pinned
+    // caller's page-locked CDIFF record of the last tns_enqueue_monitored, given the
+    // reference's floor at the next synchronisation
+    double* cdiff_pending = nullptr;
     bool profile = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     double kms[K_NKERNEL] = {0};

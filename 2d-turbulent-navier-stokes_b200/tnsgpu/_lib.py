@@ -34,7 +34,8 @@ NOALLOC_MAX_CELLS = 256 * 4 * 8192
 
 # every symbol include/tnsgpu.h declares
 EXPORTS = ("tns_create", "tns_set_injection_scale", "tns_upload_state", "tns_run",
-           "tns_enqueue", "tns_prepare", "tns_synchronize", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
+           "tns_enqueue", "tns_prepare", "tns_synchronize", "tns_upload_state_async", "tns_enqueue_monitored",
+           "tns_download_state_async", "tns_download_state", "tns_download_primitives", "tns_debug_fetch",
            "tns_set_stream", "tns_profile", "tns_kernel_times", "tns_launch_count",
            "tns_last_error", "tns_destroy", "tns_time_step_noalloc", "tns_node_averages",
            "tns_boundary_integrals", "tns_total_pressure_sums", "tns_boundary_face_states", "tns_batch_create", "tns_batch_run", "tns_batch_set_active",
@@ -87,6 +88,9 @@ def load(path: str = None):
     L.tns_run.argtypes = [vp, ip, ip, dp, ip, C.POINTER(C.c_int)]
     L.tns_enqueue.argtypes = [vp, ip]
     L.tns_prepare.argtypes = [vp]
+    L.tns_upload_state_async.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.tns_enqueue_monitored.argtypes = [vp, vp]
+    L.tns_download_state_async.argtypes = [vp, vp, vp, vp, vp, vp]
     L.tns_synchronize.argtypes = [vp]
     L.tns_download_state.argtypes = [vp, dp, dp, dp, dp, dp]
     L.tns_download_primitives.argtypes = [vp, dp, dp, dp, dp]

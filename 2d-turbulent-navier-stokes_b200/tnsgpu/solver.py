@@ -106,6 +106,22 @@ class Solver:
     def synchronize(self):
         self._check(self.L.tns_synchronize(self.h))
 
+    def upload_async(self, ptrs):
+        """Queue the upload from five page-locked host addresses of NELES doubles and
+        return at once (tns_upload_state_async); they must stay valid until
+        synchronize()."""
+        self._check(self.L.tns_upload_state_async(self.h, *[int(p) for p in ptrs]))
+
+    def enqueue_monitored(self, cdiff_ptr):
+        """Queue one monitored iteration whose five CDIFF values arrive at the page-locked
+        address ``cdiff_ptr`` by the next synchronize() (tns_enqueue_monitored)."""
+        self._check(self.L.tns_enqueue_monitored(self.h, int(cdiff_ptr)))
+
+    def download_async(self, ptrs):
+        """Queue the download into five page-locked host addresses of NELES doubles,
+        complete at the next synchronize() (tns_download_state_async)."""
+        self._check(self.L.tns_download_state_async(self.h, *[int(p) for p in ptrs]))
+
     def upload_ptrs(self, ptrs):
         """Upload from five host addresses (e.g. page-locked buffers) of NELES doubles."""
         self._check(self.L.tns_upload_state(self.h, *[int(p) for p in ptrs]))

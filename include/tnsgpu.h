@@ -99,6 +99,23 @@ int tns_prepare(tns_handle *h);
  * became NaN / Inf since the last check. */
 int tns_synchronize(tns_handle *h);
 
+/* Asynchronous forms of tns_upload_state, tns_run(h, 1, 1, ...) and tns_download_state,
+ * for callers that keep several handles in flight (one handle's download overlapping
+ * another's upload and iteration).  Each queues its work on the handle's stream and
+ * returns at once; the results are there after the next tns_synchronize on the handle,
+ * and the host arrays must stay valid (and a download target unread) until then.  Host
+ * arrays must be page-locked (cudaHostAlloc / cudaHostRegister; TNS_ERR_ARG otherwise).
+ * The transfers need the mesh in its own cell order (a general mesh is renumbered on the
+ * device: TNS_ERR_UNSUPPORTED, use the synchronous calls).  tns_enqueue_monitored runs
+ * one monitored iteration and queues its five CDIFF values into cdiff[5]; the
+ * synchronisation applies the floor tns_run applies.  One record may be pending per
+ * handle (TNS_ERR_STATE for a second before the synchronisation). */
+int tns_upload_state_async(tns_handle *h, const double *c1, const double *c2, const double *c3,
+                           const double *c4, const double *c5);
+int tns_enqueue_monitored(tns_handle *h, double *cdiff);
+int tns_download_state_async(tns_handle *h, double *c1, double *c2, double *c3, double *c4,
+                             double *c5);
+
 /* Downloads C1..C5(1:NELES) (for restart.in, turbnstwod.f90:171-195). */
 int tns_download_state(tns_handle *h, double *c1, double *c2, double *c3, double *c4,
                        double *c5);
