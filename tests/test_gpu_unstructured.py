@@ -231,3 +231,28 @@ def test_general_path_per_kernel_profile():
     assert all(kt[k][0] > 0 for k in ("dissipation", "viscous", "stage"))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_prepare_on_a_general_mesh(precision):
+    """tns_prepare on the general path: it launches nothing, and the runs after it equal
+    the runs of a handle that captured its graphs at first use, bit for bit (both mixed
+    state parities: an odd then an even call)."""
+    mesh, flow, g = load_case1()
+    pm, _ = permute_mesh(mesh, seed=4)
+    c0, ri = _cold(pm, flow)
+    out = []
+    for prep in (True, False):
+        s = Solver(pm, flow, ri, precision=precision)
+        s.upload(c0)
+        if prep:
+            n0 = s.launch_count()
+            s.prepare()
+            s.prepare()
+            assert s.launch_count() == n0
+        rec = [s.run(7, 7), s.run(10, 5)]
+        out.append((s.download(), rec))
+        s.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
